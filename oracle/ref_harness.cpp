@@ -1,0 +1,554 @@
+// Test harness around the reference engine (PS_AGONY2D) compiled on the CPU.
+//
+// TEST INFRASTRUCTURE ONLY. It is linked into oracle/_ref/libagony_ref.so by oracle/ref_build.sh and is loaded by
+// tests/golden/make_golden.py (golden vectors), by the oracle self-checks in tests/, and by bench.py's reference arm
+// (the timed CPU baseline). Nothing in the product path loads it.
+//
+// The harness drives the reference's own public API (Simulation::update, ObjectAPI::create*, createMaterial) and,
+// for per-phase golden vectors, the same member functions Simulation::physicsStep calls
+// (PhysicsSimulation-Agony/PS_AGONY2D/Simulation.cpp:255-351), reading intermediate state in between. Private
+// members are reached by compiling this file with -fno-access-control.
+#include "PS_AGONY2D/Simulation.h"
+#include "PS_AGONY2D/FastCosSin.h"
+#include "PS_AGONY2D/Threading.h"
+#include "PS_AGONY2D/SimulationImpl/LeftOutFunctions.h"
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace PS_AGONY2D;
+
+// PolygonCapsule.cpp is not compiled (GCC rejects its goto); capsules are in no workload.
+void PS_AGONY2D::NarrowPhaseCollisionDetector::collisionPolygonCapsule(
+    std::span<const ObjectPair>, CacheLineAlignedVector<BodyCollisionData>&) {}
+
+namespace
+{
+    // IThreadingBackend (PS_AGONY2D/Threading.h:10-22): every launched task runs on its own pool thread, all
+    // concurrently, and launch() returns without waiting — the contract the reference's wave runner relies on.
+    class PoolBackend final : public Threading::IThreadingBackend
+    {
+        struct Worker
+        {
+            std::thread thread;
+            std::mutex m;
+            std::condition_variable cv;
+            Threading::TaskFn fn = nullptr;
+            void* ctx = nullptr;
+            size_t index = 0;
+            bool has = false;
+            bool stop = false;
+        };
+        std::vector<std::unique_ptr<Worker>> workers;
+
+    public:
+        explicit PoolBackend(size_t threads)
+        {
+            for (size_t i = 0; i < threads; i++)
+            {
+                workers.emplace_back(std::make_unique<Worker>());
+                Worker* w = workers.back().get();
+                w->thread = std::thread([w] {
+                    for (;;)
+                    {
+                        Threading::TaskFn fn;
+                        void* ctx;
+                        size_t index;
+                        {
+                            std::unique_lock<std::mutex> lk(w->m);
+                            w->cv.wait(lk, [w] { return w->has || w->stop; });
+                            if (w->stop && !w->has) return;
+                            fn = w->fn; ctx = w->ctx; index = w->index;
+                        }
+                        fn(ctx, index);
+                        {
+                            std::lock_guard<std::mutex> lk(w->m);
+                            w->has = false;
+                        }
+                        w->cv.notify_all();
+                    }
+                });
+            }
+        }
+        ~PoolBackend() override
+        {
+            for (auto& w : workers)
+            {
+                {
+                    std::unique_lock<std::mutex> lk(w->m);
+                    w->cv.wait(lk, [&] { return !w->has; });
+                    w->stop = true;
+                }
+                w->cv.notify_all();
+                w->thread.join();
+            }
+        }
+        size_t getThreadCount() const noexcept override { return workers.size(); }
+        void launch(size_t taskCount, Threading::TaskFn fn, void* context, std::span<const uint32_t>) override
+        {
+            for (size_t i = 0; i < taskCount; i++)
+            {
+                Worker* w = workers[i % workers.size()].get();
+                std::unique_lock<std::mutex> lk(w->m);
+                w->cv.wait(lk, [w] { return !w->has; }); // Previous task on this worker finished.
+                w->fn = fn; w->ctx = context; w->index = i; w->has = true;
+                lk.unlock();
+                w->cv.notify_all();
+            }
+        }
+    };
+
+    std::mutex g_backendMutex;
+    std::map<size_t, std::unique_ptr<PoolBackend>> g_backends;
+
+    PoolBackend* backendFor(size_t threads)
+    {
+        std::lock_guard<std::mutex> lk(g_backendMutex);
+        auto& b = g_backends[threads];
+        if (!b) b = std::make_unique<PoolBackend>(threads);
+        return b.get();
+    }
+
+    struct Harness
+    {
+        Simulation sim;
+        float dt = 1.0f / 60.0f;
+        size_t threads = 0;
+        std::map<std::string, std::vector<uint8_t>> blobs;
+
+        template <class T>
+        void put(const std::string& name, const T* data, size_t count)
+        {
+            auto& b = blobs[name];
+            b.resize(count * sizeof(T));
+            if (count) std::memcpy(b.data(), data, count * sizeof(T));
+        }
+        template <class V>
+        void putv(const std::string& name, const V& v) { put(name, v.data(), v.size()); }
+    };
+
+    void useBackend(Harness* h)
+    {
+        Threading::setThreadingBackend(backendFor(h->threads));
+    }
+
+    void dumpBodies(Harness* h, const std::string& p)
+    {
+        const BodySoA& b = h->sim.objectManager.bodies;
+        h->putv(p + "body.comX", b.comX);
+        h->putv(p + "body.comY", b.comY);
+        h->putv(p + "body.velocityX", b.velocityX);
+        h->putv(p + "body.velocityY", b.velocityY);
+        h->putv(p + "body.rotation", b.rotation);
+        h->putv(p + "body.angularVelocity", b.angularVelocity);
+        h->putv(p + "body.mass", b.mass);
+        h->putv(p + "body.invMass", b.invMass);
+        h->putv(p + "body.inertia", b.inertia);
+        h->putv(p + "body.invInertia", b.invInertia);
+        h->putv(p + "body.rotationCos", b.rotationCos);
+        h->putv(p + "body.rotationSin", b.rotationSin);
+        h->putv(p + "body.boundRadius", b.boundRadius);
+        h->putv(p + "body.sleepingTimer", b.sleepingTimer);
+        h->putv(p + "body.renderRotationWrapCount", b.renderRotationWrapCount);
+        h->putv(p + "body.localCenterOfMassX", b.localCenterOfMassX);
+        h->putv(p + "body.localCenterOfMassY", b.localCenterOfMassY);
+        h->putv(p + "body.islandId", b.islandId);
+        h->putv(p + "body.sleepIslandId", b.sleepIslandId);
+        h->put(p + "body.groupStarts", b.groupStarts, size_t(BodyGroup::Unused) + 1);
+        std::vector<uint32_t> slot(b.getCount()), gen(b.getCount());
+        for (size_t i = 0; i < b.getCount(); i++)
+        {
+            const Handle hd = b.handleAt(uint32_t(i));
+            slot[i] = hd.slot; gen[i] = hd.generation;
+        }
+        h->putv(p + "body.handleSlot", slot);
+        h->putv(p + "body.handleGen", gen);
+    }
+
+    void dumpColliders(Harness* h, const std::string& p)
+    {
+        const ObjectManager& om = h->sim.objectManager;
+        const ColliderSoA& c = om.colliders;
+        h->putv(p + "col.bodyIndex", c.bodyIndex);
+        h->putv(p + "col.localOffsetX", c.localOffsetX);
+        h->putv(p + "col.localOffsetY", c.localOffsetY);
+        h->putv(p + "col.comOffsetX", c.comOffsetX);
+        h->putv(p + "col.comOffsetY", c.comOffsetY);
+        h->putv(p + "col.localRotation", c.localRotation);
+        h->putv(p + "col.worldPosX", c.worldPosX);
+        h->putv(p + "col.worldPosY", c.worldPosY);
+        h->putv(p + "col.worldRotation", c.worldRotation);
+        h->putv(p + "col.worldRotationCos", c.worldRotationCos);
+        h->putv(p + "col.worldRotationSin", c.worldRotationSin);
+        h->putv(p + "col.materialIndex", c.materialIndex);
+        std::vector<uint32_t> st(c.getCount());
+        for (size_t i = 0; i < c.getCount(); i++) st[i] = uint32_t(c.shapeType[i]);
+        h->putv(p + "col.shapeType", st);
+        h->putv(p + "col.shapeIndex", c.shapeIndex);
+        h->putv(p + "col.aabbMinX", c.aabbMinX);
+        h->putv(p + "col.aabbMinY", c.aabbMinY);
+        h->putv(p + "col.aabbMaxX", c.aabbMaxX);
+        h->putv(p + "col.aabbMaxY", c.aabbMaxY);
+        h->putv(p + "col.minExtent", c.minExtent);
+        h->putv(p + "col.maxExtent", c.maxExtent);
+        h->put(p + "col.groupStarts", c.groups.starts, size_t(BodyGroup::Unused) + 1);
+        std::vector<uint32_t> slot(c.getCount()), gen(c.getCount());
+        for (size_t i = 0; i < c.getCount(); i++)
+        {
+            const Handle hd = c.handleAt(uint32_t(i));
+            slot[i] = hd.slot; gen[i] = hd.generation;
+        }
+        h->putv(p + "col.handleSlot", slot);
+        h->putv(p + "col.handleGen", gen);
+
+        h->putv(p + "circle.colliderIndices", om.circles.colliderIndices);
+        h->putv(p + "circle.radius", om.circles.radius);
+        h->putv(p + "box.colliderIndices", om.boxes.colliderIndices);
+        h->putv(p + "box.halfWidth", om.boxes.halfWidth);
+        h->putv(p + "box.halfHeight", om.boxes.halfHeight);
+        h->putv(p + "poly.colliderIndices", om.polygons.colliderIndices);
+        std::vector<uint32_t> counts;
+        std::vector<float> verts, norms;
+        for (const PolygonGeometry& g : om.polygons.geometry)
+        {
+            counts.push_back(uint32_t(g.size()));
+            for (size_t v = 0; v < g.size(); v++)
+            {
+                verts.push_back(g.vertices()[v].x); verts.push_back(g.vertices()[v].y);
+                norms.push_back(g.normals()[v].x); norms.push_back(g.normals()[v].y);
+            }
+        }
+        h->putv(p + "poly.counts", counts);
+        h->putv(p + "poly.vertices", verts);
+        h->putv(p + "poly.normals", norms);
+    }
+
+    // Manifolds with collider handles resolved to current dense collider indices.
+    void dumpManifolds(Harness* h, const std::string& p, std::span<const BodyCollisionData> m)
+    {
+        const HandleTable& handles = h->sim.objectManager.colliders.handles;
+        std::vector<uint32_t> a(m.size()), b(m.size()), aslot(m.size()), bslot(m.size()), cnt(m.size()), ids(2 * m.size());
+        std::vector<float> nrm(2 * m.size()), depth(m.size()), pts(4 * m.size()), imp(4 * m.size());
+        for (size_t i = 0; i < m.size(); i++)
+        {
+            const BodyCollisionData& d = m[i];
+            a[i] = handles.indexOf(d.colliderA);
+            b[i] = handles.indexOf(d.colliderB);
+            aslot[i] = d.colliderA.slot;
+            bslot[i] = d.colliderB.slot;
+            cnt[i] = d.contactCount;
+            nrm[2 * i] = d.normal.x; nrm[2 * i + 1] = d.normal.y;
+            depth[i] = d.penetration;
+            for (int k = 0; k < 2; k++)
+            {
+                const bool live = uint32_t(k) < d.contactCount;
+                pts[4 * i + 2 * k] = live ? d.contactPoints[k].x : 0.0f;
+                pts[4 * i + 2 * k + 1] = live ? d.contactPoints[k].y : 0.0f;
+                ids[2 * i + k] = live ? d.contactIds[k] : 0u;
+                imp[4 * i + 2 * k] = d.persistentContactData[k].normalImpulseAccumulator;
+                imp[4 * i + 2 * k + 1] = d.persistentContactData[k].tangentImpulseAccumulator;
+            }
+        }
+        h->putv(p + "colA", a); h->putv(p + "colB", b);
+        h->putv(p + "slotA", aslot); h->putv(p + "slotB", bslot);
+        h->putv(p + "count", cnt); h->putv(p + "normal", nrm); h->putv(p + "depth", depth);
+        h->putv(p + "points", pts); h->putv(p + "ids", ids); h->putv(p + "impulses", imp);
+    }
+
+    void dumpTree(Harness* h, const std::string& p, BroadPhaseInternal::BvhTreeType type)
+    {
+        const auto& t = h->sim.broadPhaseCollisionDetector.trees[size_t(type)];
+        h->putv(p + "sorted", t.colliderIndices);
+        h->putv(p + "morton", t.mortonCodes);
+    }
+
+    int64_t finishBody(Harness* h, std::optional<ObjectDenseIndex> idx)
+    {
+        if (!idx) return -1;
+        return int64_t(h->sim.objectManager.bodies.handleAt(*idx).slot);
+    }
+}
+
+extern "C"
+{
+    struct agref_settings
+    {
+        float dt;
+        uint32_t velocity_iterations;
+        uint32_t position_iterations;
+        float gravity_x, gravity_y;
+        int32_t ccd;
+        float sleep_speed;
+        float sleep_time;
+        int32_t threads; // Pool threads besides the calling one (0 = single-threaded).
+    };
+
+    void* agref_create(const agref_settings* s)
+    {
+        auto* h = new Harness();
+        h->dt = s->dt;
+        h->threads = size_t(s->threads < 0 ? 0 : s->threads);
+        auto& ss = h->sim.getSimulationSettings();
+        ss.clockSettings.updateInterval = s->dt;
+        ss.collisionVelocitySolvingIterations = s->velocity_iterations;
+        ss.collisionPositionSolvingIterations = s->position_iterations;
+        ss.integratorSettings.gravity = Vec2(s->gravity_x, s->gravity_y);
+        ss.continuousCollisionEnabled = s->ccd != 0;
+        ss.sleepSpeedThreshold = s->sleep_speed;
+        ss.sleepTimeThreshold = s->sleep_time;
+        return h;
+    }
+
+    void agref_destroy(void* hp) { delete static_cast<Harness*>(hp); }
+
+    uint32_t agref_material(void* hp, float elasticity, float staticFriction, float dynamicFriction)
+    {
+        Material m;
+        m.elasticity = elasticity; m.staticFriction = staticFriction; m.dynamicFriction = dynamicFriction;
+        return static_cast<Harness*>(hp)->sim.createMaterial(m);
+    }
+
+    static BodyCreateParams baseParams(float px, float py, float rot, float vx, float vy, float w, float mass, uint32_t mat)
+    {
+        BodyCreateParams b;
+        b.position = Vec2(px, py);
+        b.velocity = Vec2(vx, vy);
+        b.rotation = rot;
+        b.angularVelocity = w;
+        b.mass = mass;
+        b.materialIndex = mat;
+        return b;
+    }
+
+    // Returns the body handle slot (stable id), or -1 on failure.
+    int64_t agref_add_polygon(void* hp, const float* xy, uint32_t n, float px, float py, float rot, float vx, float vy,
+                              float w, float mass, uint32_t mat)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        std::vector<Vec2> v(n);
+        for (uint32_t i = 0; i < n; i++) v[i] = Vec2(xy[2 * i], xy[2 * i + 1]);
+        PolygonCreateParams p;
+        p.base = baseParams(px, py, rot, vx, vy, w, mass, mat);
+        p.localVertices = std::span<Vec2>(v.data(), v.size());
+        return finishBody(h, h->sim.objects().createPolygon(p));
+    }
+
+    int64_t agref_add_box(void* hp, float width, float height, float px, float py, float rot, float vx, float vy,
+                          float w, float mass, uint32_t mat)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        BoxCreateParams p;
+        p.base = baseParams(px, py, rot, vx, vy, w, mass, mat);
+        p.size = Vec2(width, height);
+        return finishBody(h, h->sim.objects().createBox(p));
+    }
+
+    int64_t agref_add_circle(void* hp, float radius, float px, float py, float rot, float vx, float vy,
+                             float w, float mass, uint32_t mat)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        CircleCreateParams p;
+        p.base = baseParams(px, py, rot, vx, vy, w, mass, mat);
+        p.radius = radius;
+        return finishBody(h, h->sim.objects().createCircle(p));
+    }
+
+    // Steps through the reference's public entry point, Simulation::update (Simulation.cpp:32-74). With
+    // updateInterval == dt every call takes exactly one fixed step (FixedClock.h:35-63).
+    void agref_update(void* hp, int32_t steps)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        useBackend(h);
+        for (int32_t i = 0; i < steps; i++) h->sim.update(h->dt);
+    }
+
+    // Wall-clock seconds for 'steps' updates (the CPU baseline timer).
+    double agref_timed_update(void* hp, int32_t steps)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        useBackend(h);
+        const auto t0 = std::chrono::steady_clock::now();
+        for (int32_t i = 0; i < steps; i++) h->sim.update(h->dt);
+        const auto t1 = std::chrono::steady_clock::now();
+        return std::chrono::duration<double>(t1 - t0).count();
+    }
+
+    uint32_t agref_body_count(void* hp) { return uint32_t(static_cast<Harness*>(hp)->sim.objectManager.bodies.getCount()); }
+    uint32_t agref_collider_count(void* hp) { return uint32_t(static_cast<Harness*>(hp)->sim.objectManager.colliders.getCount()); }
+    uint32_t agref_manifold_count(void* hp) { return uint32_t(static_cast<Harness*>(hp)->sim.getBodyCollisionData().size()); }
+
+    void agref_dump_state(void* hp, const char* prefix)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        const std::string p(prefix);
+        dumpBodies(h, p);
+        dumpColliders(h, p);
+        dumpManifolds(h, p + "man.", h->sim.getBodyCollisionData());
+    }
+
+    // Overwrites one float field of every body (used to drive the integration/wrap/cos-sin phases with chosen
+    // inputs). Returns 0 on success, -1 for an unknown field.
+    int32_t agref_set_body_field(void* hp, const char* field, const float* data)
+    {
+        BodySoA& b = static_cast<Harness*>(hp)->sim.objectManager.bodies;
+        const std::string f(field);
+        CacheLineAlignedVector<Real>* dst = nullptr;
+        if (f == "velocityX") dst = &b.velocityX;
+        else if (f == "velocityY") dst = &b.velocityY;
+        else if (f == "rotation") dst = &b.rotation;
+        else if (f == "angularVelocity") dst = &b.angularVelocity;
+        else if (f == "comX") dst = &b.comX;
+        else if (f == "comY") dst = &b.comY;
+        if (!dst) return -1;
+        std::memcpy(dst->data(), data, dst->size() * sizeof(Real));
+        return 0;
+    }
+
+    // One fixed step with taps between the phases. Mirrors the member-function sequence of Simulation::update
+    // (flushCommands, preUpdate, physicsStep, postUpdate; Simulation.cpp:32-74, 255-351, 410-451) and records:
+    //   pre.*  state entering the step          int.*  after integration, wrap, rotation cos/sin
+    //   sp.*   collider poses + AABBs           dyn.*  dynamic tree (Morton-sorted collider indices and keys)
+    //   bp.pairs  broad-phase collider pairs    np.*   narrow-phase manifolds incl. warm-start impulses
+    //   sv.*   after the contact solver         is.*   island ids        post.*  state after the step
+    void agref_phase_step(void* hp)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        useBackend(h);
+        Simulation& s = h->sim;
+        const Real dt = h->dt;
+
+        s.flushCommands();
+        s.clock.setSettings(s.simulationSettings.clockSettings);
+        s.clock.advance(dt);
+        s.preUpdate();
+
+        dumpBodies(h, "pre.");
+        dumpColliders(h, "pre.");
+        dumpManifolds(h, "pre.man.", s.narrowPhaseCollisionDetector.getBodyCollisionData());
+
+        s.simulationRunTimer += dt;
+        s.bodyCollisionSolver.resetCollisionData();
+        s.bodyCollisionSolver.setCollisionEventRecording(false);
+        if (s.objectManager.bodies.getCount() == 0) return;
+        s.wakeHeldBodies();
+        s.setDataViewers();
+
+        s.integrateAndApplyConstraints(dt);
+        const IndexRange dynamicRange = s.objectManager.bodies.range(BodyGroup::Dynamic);
+        wrapBodyRotations(s.objectManager.bodies, dynamicRange);
+        Integrator::computeRotationCosSin(s.objectManager.bodies, dynamicRange);
+        dumpBodies(h, "int.");
+
+        const bool wasDirty = s.objectManager.spatialDirty;
+        if (s.objectManager.spatialDirty) s.rebuildSpatialData();
+        else s.updateDynamicSpatialData();
+        uint32_t dirtyFlag = wasDirty ? 1u : 0u;
+        h->put("sp.spatialDirty", &dirtyFlag, 1);
+        dumpColliders(h, "sp.");
+        dumpTree(h, "dyn.", BroadPhaseInternal::BvhTreeType::Dynamic);
+        dumpTree(h, "static.", BroadPhaseInternal::BvhTreeType::Static);
+        dumpTree(h, "sleep.", BroadPhaseInternal::BvhTreeType::Sleeping);
+
+        s.islandBodyCollisionEdges = {};
+        std::span<const ObjectPair> broad{};
+        std::span<BodyCollisionData> narrow{};
+        if (s.objectManager.colliders.getCount() > 1)
+        {
+            broad = s.broadPhaseCollisionDetector.findCollisions(ExecutionPolicy::ForceSingleThreaded);
+            h->put("bp.pairs", reinterpret_cast<const uint32_t*>(broad.data()), 2 * broad.size());
+            if (broad.empty())
+            {
+                s.narrowPhaseCollisionDetector.resetCollisionData();
+            }
+            else
+            {
+                narrow = s.narrowPhaseCollisionDetector.findCollisions(broad);
+                dumpManifolds(h, "np.", narrow);
+                if (narrow.empty())
+                {
+                    s.narrowPhaseCollisionDetector.rebuildContactCache();
+                }
+                else
+                {
+                    s.objectManager.wakeIslandsOfContacts(narrow);
+                    s.wakeSleepingContactData();
+                    narrow = s.narrowPhaseCollisionDetector.getBodyCollisionData();
+                    s.islandBodyCollisionEdges = s.bodyCollisionSolver.fillCollidingBodyPairs(narrow);
+                    dumpBodies(h, "svin.");
+                    dumpColliders(h, "svin.");
+                    dumpManifolds(h, "svin.man.", narrow);
+                    s.bodyCollisionSolver.solveCollisions(
+                        narrow,
+                        s.simulationSettings.collisionVelocitySolvingIterations,
+                        s.simulationSettings.collisionPositionSolvingIterations);
+                    dumpBodies(h, "sv.");
+                    dumpManifolds(h, "sv.man.", narrow);
+                    s.narrowPhaseCollisionDetector.rebuildContactCache();
+                    s.dispatchCollisionEvents();
+                }
+            }
+        }
+        else
+        {
+            s.narrowPhaseCollisionDetector.resetCollisionData();
+        }
+
+        s.islandManager.reset(s.objectManager.bodies);
+        s.islandManager.step(s.islandBodyCollisionEdges);
+        for (auto* cs : s.constraintSystems) s.islandManager.step(cs->getActiveEdges());
+        s.islandManager.finalize(s.objectManager.bodies);
+        h->putv("is.islandId", s.objectManager.bodies.islandId);
+
+        s.flushCommands();
+        s.updateSleeping(float(dt));
+        s.sleepContactData();
+        s.postUpdate();
+
+        dumpBodies(h, "post.");
+        dumpColliders(h, "post.");
+        dumpManifolds(h, "post.man.", s.getBodyCollisionData());
+    }
+
+    uint64_t agref_blob_size(void* hp, const char* name)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        auto it = h->blobs.find(name);
+        return it == h->blobs.end() ? ~0ull : uint64_t(it->second.size());
+    }
+
+    int32_t agref_blob_copy(void* hp, const char* name, void* dst)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        auto it = h->blobs.find(name);
+        if (it == h->blobs.end()) return -1;
+        if (!it->second.empty()) std::memcpy(dst, it->second.data(), it->second.size());
+        return 0;
+    }
+
+    // Newline-separated blob names (for discovery); returns the byte length needed including the terminator.
+    uint64_t agref_blob_names(void* hp, char* dst, uint64_t cap)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        std::string all;
+        for (auto& kv : h->blobs) { all += kv.first; all += '\n'; }
+        if (dst && cap > all.size()) std::memcpy(dst, all.c_str(), all.size() + 1);
+        return uint64_t(all.size() + 1);
+    }
+
+    void agref_clear_blobs(void* hp) { static_cast<Harness*>(hp)->blobs.clear(); }
+
+    // The reference's batched rotation cos/sin over an array (FastCosSin.cpp:26-109), SIMD body and scalar tail.
+    void agref_fastcossin(const float* in, float* outCos, float* outSin, uint64_t n)
+    {
+        FastCosSin::order5Array(in, outCos, outSin, size_t(n));
+    }
+}

@@ -1,0 +1,174 @@
+"""ctypes wrapper over oracle/_ref/libagony_ref.so, the reference engine (PS_AGONY2D) built on the CPU.
+
+TEST INFRASTRUCTURE ONLY: used by tests/golden/make_golden.py, by the oracle self-checks in tests/ and by the
+reference (CPU baseline) arm of bench.py. The product path never imports it.
+
+Scenes come from ag2d.scenes (the same generator feeds this library), so both sides start from identical inputs.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libagony_ref.so")
+
+
+class _Settings(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_float), ("velocity_iterations", ctypes.c_uint32),
+                ("position_iterations", ctypes.c_uint32), ("gravity_x", ctypes.c_float),
+                ("gravity_y", ctypes.c_float), ("ccd", ctypes.c_int32), ("sleep_speed", ctypes.c_float),
+                ("sleep_time", ctypes.c_float), ("threads", ctypes.c_int32)]
+
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"{LIB_PATH} is missing: run oracle/ref_build.sh")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, f, u32, i32, i64 = ctypes.c_void_p, ctypes.c_float, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int64
+        L.agref_create.restype = vp
+        L.agref_create.argtypes = [ctypes.POINTER(_Settings)]
+        L.agref_destroy.argtypes = [vp]
+        L.agref_material.restype = u32
+        L.agref_material.argtypes = [vp, f, f, f]
+        L.agref_add_polygon.restype = i64
+        L.agref_add_polygon.argtypes = [vp, vp, u32, f, f, f, f, f, f, f, u32]
+        L.agref_add_box.restype = i64
+        L.agref_add_box.argtypes = [vp, f, f, f, f, f, f, f, f, f, u32]
+        L.agref_add_circle.restype = i64
+        L.agref_add_circle.argtypes = [vp, f, f, f, f, f, f, f, f, u32]
+        L.agref_update.argtypes = [vp, i32]
+        L.agref_timed_update.restype = ctypes.c_double
+        L.agref_timed_update.argtypes = [vp, i32]
+        L.agref_body_count.restype = u32
+        L.agref_body_count.argtypes = [vp]
+        L.agref_collider_count.restype = u32
+        L.agref_collider_count.argtypes = [vp]
+        L.agref_manifold_count.restype = u32
+        L.agref_manifold_count.argtypes = [vp]
+        L.agref_dump_state.argtypes = [vp, ctypes.c_char_p]
+        L.agref_set_body_field.restype = i32
+        L.agref_set_body_field.argtypes = [vp, ctypes.c_char_p, vp]
+        L.agref_phase_step.argtypes = [vp]
+        L.agref_blob_size.restype = ctypes.c_uint64
+        L.agref_blob_size.argtypes = [vp, ctypes.c_char_p]
+        L.agref_blob_copy.restype = i32
+        L.agref_blob_copy.argtypes = [vp, ctypes.c_char_p, vp]
+        L.agref_blob_names.restype = ctypes.c_uint64
+        L.agref_blob_names.argtypes = [vp, ctypes.c_char_p, ctypes.c_uint64]
+        L.agref_clear_blobs.argtypes = [vp]
+        L.agref_fastcossin.argtypes = [vp, vp, vp, ctypes.c_uint64]
+        _lib = L
+    return _lib
+
+
+_U32_SUFFIXES = ("bodyIndex", "materialIndex", "shapeType", "shapeIndex", "groupStarts", "handleSlot", "handleGen",
+                 "islandId", "sleepIslandId", "colliderIndices", "counts", "colA", "colB", "slotA", "slotB", "count",
+                 "ids", "sorted", "morton", "pairs", "spatialDirty")
+
+
+def _dtype_for(name: str):
+    last = name.rsplit(".", 1)[-1]
+    return np.uint32 if last in _U32_SUFFIXES else np.float32
+
+
+class RefSim:
+    """One reference Simulation (Simulation.h:36-255) configured like a Scene and loaded with its bodies."""
+
+    def __init__(self, scene, threads: int = 0, ccd: bool = False, sleep_speed: float = 0.1,
+                 sleep_time: float = 0.5):
+        L = lib()
+        s = _Settings(scene.dt, scene.velocity_iterations, scene.position_iterations, scene.gravity[0],
+                      scene.gravity[1], 1 if ccd else 0, sleep_speed, sleep_time, threads)
+        self.h = L.agref_create(ctypes.byref(s))
+        self.scene = scene
+        mats = [L.agref_material(self.h, *m) for m in scene.materials]
+        self.body_slots = []
+        for i in range(scene.n):
+            mat = mats[int(scene.material[i]) - 1] if int(scene.material[i]) >= 1 else 0
+            args = (float(scene.px[i]), float(scene.py[i]), float(scene.rot[i]), float(scene.vx[i]),
+                    float(scene.vy[i]), float(scene.w[i]), float(scene.mass[i]), mat)
+            k = int(scene.kind[i])
+            if k == 2:
+                v = np.ascontiguousarray(scene.polygon_vertices(i), dtype=np.float32)
+                slot = L.agref_add_polygon(self.h, v.ctypes.data, v.shape[0], *args)
+            elif k == 1:
+                slot = L.agref_add_box(self.h, float(scene.width[i]), float(scene.height[i]), *args)
+            else:
+                slot = L.agref_add_circle(self.h, float(scene.radius[i]), *args)
+            if slot < 0:
+                raise ValueError(f"reference rejected body {i}")
+            self.body_slots.append(slot)
+
+    def close(self):
+        if self.h:
+            lib().agref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def update(self, steps: int = 1):
+        lib().agref_update(self.h, steps)
+
+    def timed_update(self, steps: int) -> float:
+        return float(lib().agref_timed_update(self.h, steps))
+
+    def phase_step(self):
+        lib().agref_clear_blobs(self.h)
+        lib().agref_phase_step(self.h)
+
+    def dump_state(self, prefix: str = "state."):
+        lib().agref_dump_state(self.h, prefix.encode())
+
+    def set_body_field(self, field: str, values: np.ndarray):
+        v = np.ascontiguousarray(values, dtype=np.float32)
+        if lib().agref_set_body_field(self.h, field.encode(), v.ctypes.data) != 0:
+            raise KeyError(field)
+
+    def blob_names(self):
+        L = lib()
+        n = L.agref_blob_names(self.h, None, 0)
+        buf = ctypes.create_string_buffer(int(n))
+        L.agref_blob_names(self.h, buf, n)
+        return [s for s in buf.value.decode().split("\n") if s]
+
+    def blob(self, name: str) -> np.ndarray:
+        L = lib()
+        size = L.agref_blob_size(self.h, name.encode())
+        if size == 2**64 - 1:
+            raise KeyError(name)
+        dt = _dtype_for(name)
+        out = np.empty(int(size) // np.dtype(dt).itemsize, dtype=dt)
+        if size:
+            L.agref_blob_copy(self.h, name.encode(), out.ctypes.data)
+        return out
+
+    def blobs(self, prefix: str = "") -> dict:
+        return {k: self.blob(k) for k in self.blob_names() if k.startswith(prefix)}
+
+    @property
+    def manifold_count(self) -> int:
+        return int(lib().agref_manifold_count(self.h))
+
+
+def fastcossin(angles: np.ndarray):
+    a = np.ascontiguousarray(angles, dtype=np.float32)
+    c = np.empty_like(a)
+    s = np.empty_like(a)
+    lib().agref_fastcossin(a.ctypes.data, c.ctypes.data, s.ctypes.data, a.size)
+    return c, s
