@@ -102,8 +102,15 @@ class OraWorld:
     COL_U = {"bodyIndex": "bodyIndex", "shapeType": "shapeType", "shapeIndex": "shapeIndex",
              "material": "materialIndex"}
 
-    def __init__(self, state: dict, prefix: str = "", materials=None):
-        g = lambda k: np.array(state[prefix + k])
+    def __init__(self, state: dict, prefix: str = "", materials=None, body_prefix=None):
+        bp = prefix if body_prefix is None else body_prefix
+
+        def g(k):
+            # Bodies come from body_prefix; shapes never change within a step, so they may come from "pre.".
+            for p in ((bp,) if k.startswith("body.") else (prefix, "pre.")):
+                if p + k in state:
+                    return np.array(state[p + k])
+            raise KeyError(prefix + k)
         self.a = {}
         for cname, rname in self.BODY_F.items():
             self.a[cname] = np.ascontiguousarray(g("body." + rname), dtype=np.float32)

@@ -1,0 +1,145 @@
+"""Generates the golden vectors in tests/golden/ from the reference engine itself.
+
+The reference (PS_AGONY2D) ships no tests, fixtures or known-answer vectors, so its behaviour is pinned by running
+it: oracle/ref_build.sh compiles the reference's own sources on the CPU (oracle/_ref/libagony_ref.so) and this
+script drives them through oracle/refapi.py on seeded synthetic scenes (ag2d.scenes), saving per-phase taps.
+
+Run from the repository root (needs the reference checkout, so only in the build container):
+    oracle/ref_build.sh && python tests/golden/make_golden.py
+
+Fixtures:
+    c1_n256_s0_step300.npz  polygons on a ground box, phase taps of step 301 (contacts, warm start, solver)
+    c2_n2000_s1_step240.npz circles/boxes/polygons in a U container, phase taps of step 241
+    c3_n1500_s0_step0.npz   circles and 4-6-gons, no gravity, the first step (full spatial rebuild)
+    cossin_edge.npz         FastCosSin over edge angles (quadrant boundaries, values just below 2 pi)
+    wrap_edge.npz           body rotations around wrap boundaries (SIMD body and scalar tail)
+    traj_c1_n256.npz        600-step trajectory statistics of a 256-polygon scene
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "physicssimulation-agony_b200"))
+
+from ag2d import scenes  # noqa: E402
+from oracle import refapi  # noqa: E402
+
+PHASE_PREFIXES = ("pre.", "int.body.", "sp.col.", "sp.spatialDirty", "dyn.", "bp.pairs", "np.", "svin.", "sv.",
+                  "is.islandId", "post.body.", "post.man.")
+DROP_SUFFIXES = (".localOffsetX", ".localOffsetY", ".mass", ".inertia", ".localCenterOfMassX",
+                 ".localCenterOfMassY", ".minExtent", ".maxExtent")
+
+
+def phase_fixture(scene, steps, path):
+    r = refapi.RefSim(scene)
+    r.update(steps)
+    r.phase_step()
+    blobs = {k: v for k, v in r.blobs().items()
+             if k.startswith(PHASE_PREFIXES) and not k.endswith(DROP_SUFFIXES)}
+    blobs["meta.dt"] = np.array([scene.dt], np.float32)
+    blobs["meta.gravity"] = np.array(scene.gravity, np.float32)
+    blobs["meta.iters"] = np.array([scene.velocity_iterations, scene.position_iterations], np.uint32)
+    blobs["meta.materials"] = np.array([(1.0, 0.0, 0.0)] + list(scene.materials), np.float32)
+    np.savez_compressed(path, **blobs)
+    r.close()
+    print(f"{os.path.basename(path)}: {len(blobs)} arrays, pairs {blobs['bp.pairs'].size // 2}, "
+          f"manifolds {blobs.get('np.count', np.zeros(0)).size}")
+
+
+def cossin_fixture(path):
+    two_pi = np.float32(2.0 * np.pi)
+    half_pi = np.float32(0.5 * np.pi)
+    edges = []
+    for base in (np.float32(0.0), half_pi, np.float32(np.pi), np.float32(1.5 * np.pi), two_pi):
+        b = np.float32(base)
+        v = b
+        for _ in range(6):
+            v = np.nextafter(v, np.float32(-1.0), dtype=np.float32)
+            edges.append(v)
+        v = b
+        for _ in range(6):
+            edges.append(v)
+            v = np.nextafter(v, np.float32(10.0), dtype=np.float32)
+    rng = np.random.default_rng(7)
+    angles = np.concatenate([np.asarray(edges, np.float32), rng.uniform(0, 2 * np.pi, 971).astype(np.float32)])
+    angles = angles[(angles >= 0) & (angles <= two_pi)]
+    c, s = refapi.fastcossin(angles)
+    np.savez_compressed(path, angles=angles, cos=c, sin=s)
+    print(f"{os.path.basename(path)}: {angles.size} angles")
+
+
+def wrap_fixture(path):
+    """21 bodies (ground + 20 dynamic): the dynamic range splits into a SIMD body of 16 and a scalar tail of 4."""
+    scene = scenes.make_c1(20, 3)
+    r = refapi.RefSim(scene)
+    n = refapi.lib().agref_body_count(r.h)
+    rng = np.random.default_rng(11)
+    two_pi = np.float32(2.0 * np.pi)
+    special = np.array([-1e-7, -two_pi, two_pi, np.nextafter(two_pi, np.float32(0), dtype=np.float32),
+                        np.nextafter(two_pi, np.float32(10), dtype=np.float32), 100.0, -100.0, 1e4, -1e4,
+                        3 * two_pi, -3 * two_pi], np.float32)
+    rot = rng.uniform(-50, 50, n).astype(np.float32)
+    rot[1:1 + special.size] = special
+    rot[n - 4:] = special[-4:]
+    r.set_body_field("rotation", rot)
+    r.set_body_field("angularVelocity", rng.uniform(-30, 30, n).astype(np.float32))
+    r.phase_step()
+    keep = {k: v for k, v in r.blobs().items() if k.startswith(("pre.", "int.body.", "sp.col."))
+            and not k.endswith(DROP_SUFFIXES)}
+    keep["meta.dt"] = np.array([scene.dt], np.float32)
+    keep["meta.gravity"] = np.array(scene.gravity, np.float32)
+    np.savez_compressed(path, **keep)
+    r.close()
+    print(f"{os.path.basename(path)}: {n} bodies")
+
+
+def trajectory_stats(sim, steps):
+    """Per-step: momentum (sum m v), kinetic energy, max manifold depth, manifold count, sleeping bodies."""
+    out = {k: [] for k in ("px", "py", "ke", "max_depth", "manifolds", "sleeping")}
+    for _ in range(steps):
+        sim.update(1)
+        sim.dump_state("t.")
+        m = sim.blob("t.body.mass")
+        vx, vy, w = sim.blob("t.body.velocityX"), sim.blob("t.body.velocityY"), sim.blob("t.body.angularVelocity")
+        inertia = sim.blob("t.body.inertia")
+        dyn = m > 0
+        out["px"].append(float(np.sum((m * vx)[dyn], dtype=np.float64)))
+        out["py"].append(float(np.sum((m * vy)[dyn], dtype=np.float64)))
+        out["ke"].append(float(0.5 * np.sum((m * (vx * vx + vy * vy) + inertia * w * w)[dyn], dtype=np.float64)))
+        depth = sim.blob("t.man.depth")
+        out["max_depth"].append(float(depth.max()) if depth.size else 0.0)
+        out["manifolds"].append(int(depth.size))
+        gs = sim.blob("t.body.groupStarts")
+        out["sleeping"].append(int(gs[2] - gs[1]))
+    return {k: np.asarray(v) for k, v in out.items()}
+
+
+def trajectory_fixture(path, n=256, steps=600):
+    scene = scenes.make_c1(n, 0)
+    r = refapi.RefSim(scene)
+    stats = trajectory_stats(r, steps)
+    np.savez_compressed(path, **stats)
+    r.close()
+    print(f"{os.path.basename(path)}: {steps} steps, final KE {stats['ke'][-1]:.3f}, "
+          f"sleeping {stats['sleeping'][-1]}")
+
+
+def main():
+    if not refapi.available():
+        sys.exit("oracle/_ref/libagony_ref.so missing: run oracle/ref_build.sh first")
+    phase_fixture(scenes.make_c1(256, 0), 300, os.path.join(HERE, "c1_n256_s0_step300.npz"))
+    phase_fixture(scenes.make_c2(2000, 1, columns=50), 240, os.path.join(HERE, "c2_n2000_s1_step240.npz"))
+    phase_fixture(scenes.make_c3(1500, 0, extent=70.0), 0, os.path.join(HERE, "c3_n1500_s0_step0.npz"))
+    cossin_fixture(os.path.join(HERE, "cossin_edge.npz"))
+    wrap_fixture(os.path.join(HERE, "wrap_edge.npz"))
+    trajectory_fixture(os.path.join(HERE, "traj_c1_n256.npz"))
+
+
+if __name__ == "__main__":
+    main()

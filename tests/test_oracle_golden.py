@@ -1,0 +1,152 @@
+"""The oracle (CPU restatement in oracle/) against golden vectors produced by the reference engine itself.
+
+These pin the oracle before it is trusted as the checker of the CUDA path: every phase must reproduce the
+reference's output bit for bit on the same inputs.
+"""
+import numpy as np
+import pytest
+
+import parity
+from oracle import oraapi
+
+
+def _fixture(name):
+    d = parity.load(name)
+    mats = [tuple(r) for r in d["meta.materials"]]
+    return d, mats
+
+
+@pytest.mark.parametrize("name", parity.PHASE_FIXTURES)
+def test_integration_wrap_cossin(oracle_lib, name):
+    d, mats = _fixture(name)
+    w = oraapi.OraWorld(d, "pre.", mats)
+    g = d["meta.gravity"]
+    w.integrate(float(d["meta.dt"][0]), float(g[0]), float(g[1]))
+    for ours, theirs in [("comX", "comX"), ("comY", "comY"), ("velX", "velocityX"), ("velY", "velocityY"),
+                         ("rot", "rotation"), ("angVel", "angularVelocity"), ("rotCos", "rotationCos"),
+                         ("rotSin", "rotationSin"), ("wrapCount", "renderRotationWrapCount")]:
+        assert parity.mismatches(w.a[ours], d["int.body." + theirs]) == 0, theirs
+
+
+@pytest.mark.parametrize("name", parity.PHASE_FIXTURES)
+def test_poses_aabbs_morton_sort(oracle_lib, name):
+    d, mats = _fixture(name)
+    w = oraapi.OraWorld(d, "pre.", mats)
+    g = d["meta.gravity"]
+    w.integrate(float(d["meta.dt"][0]), float(g[0]), float(g[1]))
+    w.spatial(bool(d["sp.spatialDirty"][0]))
+    for ours, theirs in oraapi.OraWorld.COL_F.items():
+        assert parity.mismatches(w.a[ours], d["sp.col." + theirs]) == 0, theirs
+    codes, sorted_c, sorted_k, _ = w.morton(2)
+    assert parity.mismatches(sorted_c, d["dyn.sorted"]) == 0
+    assert parity.mismatches(sorted_k, d["dyn.morton"]) == 0
+
+
+@pytest.mark.parametrize("name", parity.PHASE_FIXTURES)
+def test_broad_pair_set(oracle_lib, name):
+    d, mats = _fixture(name)
+    w = oraapi.OraWorld(d, "sp.", mats, body_prefix="int.")
+    ours = w.broad_pairs()
+    dyn_begin = int(d["sp.col.groupStarts"][2])
+    ref = parity.canonical_pairs(d["bp.pairs"], dyn_begin)
+    assert ours.shape == ref.shape
+    assert parity.mismatches(ours, ref) == 0
+
+
+@pytest.mark.parametrize("name", parity.PHASE_FIXTURES)
+def test_narrow_and_warm_start(oracle_lib, name):
+    d, mats = _fixture(name)
+    w = oraapi.OraWorld(d, "sp.", mats, body_prefix="int.")
+    pairs = d["bp.pairs"].reshape(-1, 2)
+    m = w.narrow(pairs)
+    prev = oraapi.manifolds_from_dump(d, "pre.man.")
+    prev_slots = np.stack([d["pre.man.slotA"], d["pre.man.slotB"]], 1)
+    slot = d["sp.col.handleSlot"]
+    m = oraapi.warm_start(prev, prev_slots, m, np.stack([slot[m["a"]], slot[m["b"]]], 1))
+    ref = parity.sort_manifolds(oraapi.manifolds_from_dump(d, "np."))
+    m = parity.sort_manifolds(m)
+    assert m.shape == ref.shape
+    for f in ("a", "b", "nx", "ny", "depth", "count", "jn", "jt"):
+        assert parity.mismatches(m[f], ref[f]) == 0, f
+    for f in ("px", "py", "id"):
+        assert parity.mismatches(parity.active_points(m, f), parity.active_points(ref, f)) == 0, f
+
+
+@pytest.mark.parametrize("name", parity.PHASE_FIXTURES)
+def test_solver_reference_order_fp32(oracle_lib, name):
+    """The FP32 restatement, run in the reference's own constraint order, matches it bit for bit."""
+    d, mats = _fixture(name)
+    if "svin.man.count" not in d:
+        pytest.skip("no manifolds at this step")
+    iters = d["meta.iters"]
+    w = oraapi.OraWorld(d, "svin.", mats)
+    m = oraapi.manifolds_from_dump(d, "svin.man.")
+    out = w.solve(m, None, int(iters[0]), int(iters[1]))
+    ref = oraapi.manifolds_from_dump(d, "sv.man.")
+    assert parity.mismatches(out["jn"], ref["jn"]) == 0
+    assert parity.mismatches(out["jt"], ref["jt"]) == 0
+    for ours, theirs in [("velX", "velocityX"), ("velY", "velocityY"), ("angVel", "angularVelocity"),
+                         ("comX", "comX"), ("comY", "comY")]:
+        assert parity.mismatches(w.a[ours], d["sv.body." + theirs]) == 0, theirs
+
+
+@pytest.mark.parametrize("name", parity.PHASE_FIXTURES)
+def test_solver_fp64_replay_close_to_fp32(oracle_lib, name):
+    """The FP64 replay tracks the FP32 restatement on the same order (it is the tolerance reference for the
+    coloured GPU order)."""
+    d, mats = _fixture(name)
+    if "svin.man.count" not in d:
+        pytest.skip("no manifolds at this step")
+    iters = d["meta.iters"]
+    w32 = oraapi.OraWorld(d, "svin.", mats)
+    w64 = oraapi.OraWorld(d, "svin.", mats)
+    m = oraapi.manifolds_from_dump(d, "svin.man.")
+    out = w32.solve(m, None, int(iters[0]), int(iters[1]))
+    vel, pos, imp = w64.solve_f64(m, None, int(iters[0]), int(iters[1]))
+    ours = np.stack([out["jn"][:, 0], out["jt"][:, 0], out["jn"][:, 1], out["jt"][:, 1]], 1).astype(np.float64)
+    scale = np.maximum(np.abs(imp).max(), 1e-6)
+    assert np.max(np.abs(ours - imp)) <= 1e-3 * scale
+
+
+@pytest.mark.parametrize("name", parity.PHASE_FIXTURES)
+def test_islands_partition(oracle_lib, name):
+    d, mats = _fixture(name)
+    if "svin.man.count" not in d:
+        pytest.skip("no manifolds at this step")
+    w = oraapi.OraWorld(d, "svin.", mats)
+    m = oraapi.manifolds_from_dump(d, "svin.man.")
+    body = d["svin.col.bodyIndex"]
+    ids, _ = w.islands(np.stack([body[m["a"]], body[m["b"]]], 1))
+    assert np.array_equal(parity.partition_labels(ids), parity.partition_labels(d["is.islandId"]))
+
+
+def test_fastcossin_edges(oracle_lib):
+    d = parity.load("cossin_edge.npz")
+    c, s = oraapi.fastcossin(d["angles"])
+    assert parity.mismatches(c, d["cos"]) == 0
+    assert parity.mismatches(s, d["sin"]) == 0
+
+
+def test_wrap_edges_simd_body_and_tail(oracle_lib):
+    d = parity.load("wrap_edge.npz")
+    w = oraapi.OraWorld(d, "pre.")
+    g = d["meta.gravity"]
+    w.integrate(float(d["meta.dt"][0]), float(g[0]), float(g[1]))
+    for ours, theirs in [("rot", "rotation"), ("wrapCount", "renderRotationWrapCount"), ("rotCos", "rotationCos"),
+                         ("rotSin", "rotationSin")]:
+        assert parity.mismatches(w.a[ours], d["int.body." + theirs]) == 0, theirs
+    w.spatial(bool(True))
+    for ours, theirs in [("worldRot", "worldRotation"), ("worldCos", "worldRotationCos"),
+                         ("worldSin", "worldRotationSin"), ("minX", "aabbMinX"), ("maxY", "aabbMaxY")]:
+        assert parity.mismatches(w.a[ours], d["sp.col." + theirs]) == 0, theirs
+
+
+def test_oracle_detects_a_planted_fault(oracle_lib):
+    """A restatement with one operation changed must fail the same comparison (the check has teeth)."""
+    d, mats = _fixture("c1_n256_s0_step300.npz")
+    w = oraapi.OraWorld(d, "sp.", mats, body_prefix="int.")
+    m = w.narrow(d["bp.pairs"].reshape(-1, 2))
+    w.a["worldX"][int(m["a"][0])] += np.float32(1e-3)
+    m2 = w.narrow(d["bp.pairs"].reshape(-1, 2))
+    assert parity.mismatches(parity.sort_manifolds(m)["depth"], parity.sort_manifolds(m2)["depth"]) > 0 or \
+        m.shape != m2.shape
