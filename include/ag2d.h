@@ -1,0 +1,181 @@
+/* ag2d — B200-native collision and contact pipeline for the PS_AGONY2D world/body/shape/step API.
+ *
+ * C ABI of libag2d.so: opaque handles, plain pointers and sizes, int32 status codes. Every entry point below
+ * names the reference interface it replaces (paths relative to PhysicsSimulation-Agony/PS_AGONY2D/ in
+ * Shadow001111/PhysicsSimulation-Agony). The reference is statically linked C++ with no FFI of its own; these are
+ * the calls its Simulation / ObjectAPI boundary maps onto (see INTEGRATION.md for the C++ facade and ctypes
+ * binding).
+ *
+ * Threading: a world is driven by one host thread at a time (the reference's Simulation is single-caller too,
+ * Simulation.h:36). Distinct worlds and batches may be driven from distinct threads.
+ * Errors: functions return AG2D_OK or a negative AG2D_ERR_*; ag2d_last_error_string() describes the last failure
+ * on the calling thread. Nothing aborts the process (the reference aborts or returns std::nullopt).
+ */
+#ifndef AG2D_H
+#define AG2D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AG2D_OK 0
+#define AG2D_ERR_INVALID_ARG (-1)
+#define AG2D_ERR_OOM (-2)
+#define AG2D_ERR_CAPACITY (-3)   /* a buffer overflowed and could not be regrown */
+#define AG2D_ERR_TIMEOUT (-4)    /* a bounded device-side wait gave up (status word set, GPU left usable) */
+#define AG2D_ERR_CUDA (-5)
+#define AG2D_ERR_NO_DEVICE (-6)
+#define AG2D_ERR_UNSUPPORTED (-7)
+
+typedef struct ag2d_world ag2d_world;
+typedef struct ag2d_batch ag2d_batch;
+
+/* Mirrors Simulation::SimulationSettings (Simulation.h:50-76), FixedClock::Settings (SimulationImpl/FixedClock.h:
+ * 12-17) and Integrator::Settings (Integration/Integrator.h:14-19). */
+typedef struct ag2d_world_settings {
+    float dt;                        /* fixed step (clockSettings.updateInterval) */
+    uint32_t velocity_iterations;    /* collisionVelocitySolvingIterations */
+    uint32_t position_iterations;    /* collisionPositionSolvingIterations */
+    float gravity_x, gravity_y;      /* integratorSettings.gravity */
+    float angular_damping;           /* integratorSettings.angularVelocityDamping (1 = off) */
+    float sleep_speed;               /* sleepSpeedThreshold */
+    float sleep_time;                /* sleepTimeThreshold */
+    int32_t ccd;                     /* continuousCollisionEnabled */
+    int32_t device;                  /* CUDA device ordinal */
+} ag2d_world_settings;
+
+/* Mirrors BodyCreateParams (SimulationImpl/ObjectCreateParams.h:14-24). mass 0 makes a static body. */
+typedef struct ag2d_body_desc {
+    float x, y, rotation;
+    float vx, vy, angular_velocity;
+    float mass;
+    uint32_t material;
+} ag2d_body_desc;
+
+/* Per-step counters (debug data): SURVEY-style metrics the reference keeps in DebugData. */
+typedef struct ag2d_counters {
+    uint32_t status;        /* device status bits of the last step */
+    uint32_t pairs;         /* broad-phase candidate pairs */
+    uint32_t manifolds;     /* contact manifolds */
+    uint32_t colors;        /* solver colours */
+    uint32_t woke;          /* bodies woken */
+    uint32_t slept;         /* bodies put to sleep */
+    uint32_t warm_hits;     /* manifolds warm-started */
+    uint32_t sleeping;      /* bodies sleeping after the step */
+    uint64_t steps;         /* steps taken by this world */
+} ag2d_counters;
+
+/* Reference-layout world state for ag2d_world_load_state: every array in the reference's dense order, as its
+ * SoA viewers expose them (SoA/BodySoA.h:14-36, SoA/ColliderSoA.h:10-32, SoA/Shapes/*.h). Group starts are
+ * GroupRanges::starts (GroupRanges.h:130-157): static, sleeping, dynamic, end. */
+typedef struct ag2d_state_desc {
+    uint32_t n_bodies, n_colliders, n_circles, n_boxes, n_polygons, n_materials;
+    const uint32_t* body_group_starts;   /* [4] */
+    const float *com_x, *com_y, *vel_x, *vel_y, *rotation, *angular_velocity;
+    const float *inv_mass, *inv_inertia, *rot_cos, *rot_sin, *wrap_count, *bound_radius, *sleep_timer;
+    const uint32_t* sleep_island;        /* may be NULL */
+    const uint32_t *col_body, *col_shape_type, *col_shape_index, *col_material;
+    const float *col_com_offset_x, *col_com_offset_y, *col_local_rotation;
+    const float* circle_radius;          /* [n_circles] */
+    const float *box_half_width, *box_half_height;   /* [n_boxes] */
+    const uint32_t* poly_count;          /* [n_polygons] vertex counts */
+    const float* poly_vertices;          /* xy pairs, concatenated */
+    const float* poly_normals;           /* xy pairs, concatenated */
+    const float* materials;              /* [n_materials][3]: elasticity, static friction, dynamic friction */
+} ag2d_state_desc;
+
+/* Readable / writable world fields (ag2d_world_read / ag2d_world_write). Body and collider arrays are float32 or
+ * uint32 in dense order; pair arrays are uint32 pairs; manifolds are 64-byte records (ag2d_manifold). */
+enum ag2d_field {
+    AG2D_BODY_COM_X = 1, AG2D_BODY_COM_Y, AG2D_BODY_VEL_X, AG2D_BODY_VEL_Y, AG2D_BODY_ROTATION,
+    AG2D_BODY_ANGULAR_VELOCITY, AG2D_BODY_ROT_COS, AG2D_BODY_ROT_SIN, AG2D_BODY_WRAP_COUNT, AG2D_BODY_SLEEP_TIMER,
+    AG2D_BODY_STATE /* uint32: 0 static, 1 sleeping, 2 dynamic */, AG2D_BODY_SLEEP_ISLAND,
+    AG2D_COL_WORLD_X = 32, AG2D_COL_WORLD_Y, AG2D_COL_WORLD_ROTATION, AG2D_COL_WORLD_COS, AG2D_COL_WORLD_SIN,
+    AG2D_COL_AABB_MIN_X, AG2D_COL_AABB_MIN_Y, AG2D_COL_AABB_MAX_X, AG2D_COL_AABB_MAX_Y,
+    AG2D_DYN_SORTED = 64,   /* dynamic tree: collider indices in Morton order */
+    AG2D_DYN_MORTON,        /* dynamic tree: sorted Morton keys */
+    AG2D_PAIRS,             /* candidate pairs (uint32 a, b) */
+    AG2D_MANIFOLDS,         /* current manifolds */
+    AG2D_PREV_MANIFOLDS,    /* previous step's manifolds (warm-start source) */
+    AG2D_SOLVE_ORDER,       /* uint32 manifold index per solving slot (colour-major) */
+    AG2D_COLOR_STARTS,      /* uint32 [colors + 1] */
+};
+
+/* Manifold record (NarrowPhaseCollisionDetector.h:26-61 with dense collider indices instead of handles). */
+typedef struct ag2d_manifold {
+    uint32_t a, b;
+    float nx, ny, depth;
+    uint32_t count, id0, id1;
+    float px0, py0, px1, py1;
+    float jn0, jt0, jn1, jt1;
+} ag2d_manifold;
+
+/* Debug phases (ag2d_world_run_phase): one phase of the step on the current state, for parity checks. */
+enum ag2d_phase {
+    AG2D_PHASE_INTEGRATE = 1,      /* integrate + wrap + rotation cos/sin over dynamic bodies */
+    AG2D_PHASE_SPATIAL_FULL,       /* collider poses + AABBs over all colliders */
+    AG2D_PHASE_SPATIAL_DYNAMIC,    /* collider poses + AABBs over dynamic colliders */
+    AG2D_PHASE_BROAD,              /* bounds, Morton, sort, LBVH, pair query */
+    AG2D_PHASE_NARROW,             /* narrow phase on AG2D_PAIRS, warm start from AG2D_PREV_MANIFOLDS */
+    AG2D_PHASE_SOLVE,              /* colouring + solver on AG2D_MANIFOLDS */
+    AG2D_PHASE_ISLANDS,            /* islands + sleep flags from AG2D_MANIFOLDS */
+};
+
+/* ---- library ---- */
+const char* ag2d_last_error_string(void);
+int32_t ag2d_version(void);
+int32_t ag2d_device_count(int32_t* out_count);
+
+/* ---- world lifecycle: Simulation::Simulation / ~Simulation (Simulation.cpp:21-30) ---- */
+int32_t ag2d_world_create(const ag2d_world_settings* settings, ag2d_world** out_world);
+int32_t ag2d_world_destroy(ag2d_world* world);
+
+/* Simulation::createMaterial (Simulation.cpp:76-79; values clamped like MaterialManager::sanitize,
+ * SimulationImpl/MaterialManager.h:29-35). Index 0 is the default material (elasticity 1, no friction). */
+int32_t ag2d_world_add_material(ag2d_world* world, float elasticity, float static_friction, float dynamic_friction,
+                                uint32_t* out_index);
+
+/* ObjectAPI::createCircleH / createBoxH / createPolygonH (SimulationAPIs/ObjectAPI.h:61-65;
+ * ObjectManager::createCircle/createBox/createPolygon, SimulationImpl/ObjectManager.cpp:233-349). Mass, inertia,
+ * centre of mass and polygon recentring follow the reference's PhysicsGeometry. Polygons must be convex after
+ * outline cleaning (concave decomposition is not provided: AG2D_ERR_UNSUPPORTED). The handle is
+ * (generation << 32) | slot and stays valid across other creations. */
+int32_t ag2d_world_add_circle(ag2d_world* world, const ag2d_body_desc* body, float radius, uint64_t* out_handle);
+int32_t ag2d_world_add_box(ag2d_world* world, const ag2d_body_desc* body, float width, float height,
+                           uint64_t* out_handle);
+int32_t ag2d_world_add_polygon(ag2d_world* world, const ag2d_body_desc* body, const float* vertices_xy,
+                               uint32_t vertex_count, uint64_t* out_handle);
+/* Dense body index of a handle (ObjectAPI::getBodyIndex, ObjectAPI.h:53), or UINT32_MAX if stale. */
+uint32_t ag2d_world_body_index(ag2d_world* world, uint64_t handle);
+
+/* Replaces the world with a reference-layout state (parity harness: same inputs as the reference). */
+int32_t ag2d_world_load_state(ag2d_world* world, const ag2d_state_desc* state);
+
+/* Simulation::update with dt == the fixed interval, 'steps' times (Simulation.cpp:32-74 -> physicsStep :255-351).
+ * Synchronous: returns when the steps are done and the counters are on the host. */
+int32_t ag2d_world_step(ag2d_world* world, int32_t steps);
+
+int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out);
+int32_t ag2d_world_body_count(ag2d_world* world, uint32_t* out_bodies, uint32_t* out_colliders);
+
+/* Copies a field into caller memory (host). out_bytes receives the field size; pass dst = NULL to query it.
+ * Replaces the reference's SoA viewers (ObjectAPI::getBodies/getColliders, ObjectAPI.h:96-101) and
+ * Simulation::getBodyCollisionData (Simulation.h:186). */
+int32_t ag2d_world_read(ag2d_world* world, int32_t field, void* dst, uint64_t capacity_bytes, uint64_t* out_bytes);
+/* Overwrites a field from host memory (body state, pairs, manifolds) for phase-level parity runs. */
+int32_t ag2d_world_write(ag2d_world* world, int32_t field, const void* src, uint64_t bytes);
+/* Runs one phase (enum ag2d_phase) on the current device state. */
+int32_t ag2d_world_run_phase(ag2d_world* world, int32_t phase);
+
+/* ---- batched worlds: many independent worlds advanced by one launch sequence per step ---- */
+int32_t ag2d_batch_create(ag2d_world* const* worlds, uint32_t world_count, ag2d_batch** out_batch);
+int32_t ag2d_batch_step(ag2d_batch* batch, int32_t steps);
+int32_t ag2d_batch_destroy(ag2d_batch* batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,316 @@
+"""ag2d: B200-native collision and contact pipeline behind the PS_AGONY2D world/body/shape/step API.
+
+Python binding over the C ABI of libag2d.so (include/ag2d.h). The library is the CUDA implementation; there is no
+CPU fallback: importing this package on a machine without the built library raises, and creating a world without
+a CUDA device returns AG2D_ERR_NO_DEVICE.
+
+    from ag2d import World, scenes
+    w = World.from_scene(scenes.make_c1(2048))
+    w.step(600)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import scenes  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libag2d.so")
+
+OK = 0
+ERR_INVALID_ARG, ERR_OOM, ERR_CAPACITY, ERR_TIMEOUT, ERR_CUDA, ERR_NO_DEVICE, ERR_UNSUPPORTED = -1, -2, -3, -4, -5, -6, -7
+
+# enum ag2d_field
+BODY_COM_X, BODY_COM_Y, BODY_VEL_X, BODY_VEL_Y, BODY_ROTATION, BODY_ANGULAR_VELOCITY, BODY_ROT_COS, BODY_ROT_SIN, \
+    BODY_WRAP_COUNT, BODY_SLEEP_TIMER, BODY_STATE, BODY_SLEEP_ISLAND = range(1, 13)
+COL_WORLD_X, COL_WORLD_Y, COL_WORLD_ROTATION, COL_WORLD_COS, COL_WORLD_SIN, COL_AABB_MIN_X, COL_AABB_MIN_Y, \
+    COL_AABB_MAX_X, COL_AABB_MAX_Y = range(32, 41)
+DYN_SORTED, DYN_MORTON, PAIRS, MANIFOLDS, PREV_MANIFOLDS, SOLVE_ORDER, COLOR_STARTS = range(64, 71)
+# enum ag2d_phase
+PHASE_INTEGRATE, PHASE_SPATIAL_FULL, PHASE_SPATIAL_DYNAMIC, PHASE_BROAD, PHASE_NARROW, PHASE_SOLVE, \
+    PHASE_ISLANDS = range(1, 8)
+
+MANIFOLD_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("nx", "<f4"), ("ny", "<f4"), ("depth", "<f4"),
+                           ("count", "<u4"), ("id0", "<u4"), ("id1", "<u4"), ("px0", "<f4"), ("py0", "<f4"),
+                           ("px1", "<f4"), ("py1", "<f4"), ("jn0", "<f4"), ("jt0", "<f4"), ("jn1", "<f4"),
+                           ("jt1", "<f4")])
+assert MANIFOLD_DTYPE.itemsize == 64
+
+_U32_FIELDS = {BODY_STATE, BODY_SLEEP_ISLAND, DYN_SORTED, DYN_MORTON, SOLVE_ORDER, COLOR_STARTS}
+
+
+class Ag2dError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"ag2d error {code}: {message}")
+        self.code = code
+
+
+class WorldSettings(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_float), ("velocity_iterations", ctypes.c_uint32),
+                ("position_iterations", ctypes.c_uint32), ("gravity_x", ctypes.c_float),
+                ("gravity_y", ctypes.c_float), ("angular_damping", ctypes.c_float), ("sleep_speed", ctypes.c_float),
+                ("sleep_time", ctypes.c_float), ("ccd", ctypes.c_int32), ("device", ctypes.c_int32)]
+
+
+class BodyDesc(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_float), ("y", ctypes.c_float), ("rotation", ctypes.c_float), ("vx", ctypes.c_float),
+                ("vy", ctypes.c_float), ("angular_velocity", ctypes.c_float), ("mass", ctypes.c_float),
+                ("material", ctypes.c_uint32)]
+
+
+class Counters(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_uint32), ("pairs", ctypes.c_uint32), ("manifolds", ctypes.c_uint32),
+                ("colors", ctypes.c_uint32), ("woke", ctypes.c_uint32), ("slept", ctypes.c_uint32),
+                ("warm_hits", ctypes.c_uint32), ("sleeping", ctypes.c_uint32), ("steps", ctypes.c_uint64)]
+
+
+_P = ctypes.c_void_p
+
+
+class StateDesc(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("n_bodies", "n_colliders", "n_circles", "n_boxes", "n_polygons",
+                                               "n_materials")] + \
+               [(n, _P) for n in ("body_group_starts", "com_x", "com_y", "vel_x", "vel_y", "rotation",
+                                  "angular_velocity", "inv_mass", "inv_inertia", "rot_cos", "rot_sin", "wrap_count",
+                                  "bound_radius", "sleep_timer", "sleep_island", "col_body", "col_shape_type",
+                                  "col_shape_index", "col_material", "col_com_offset_x", "col_com_offset_y",
+                                  "col_local_rotation", "circle_radius", "box_half_width", "box_half_height",
+                                  "poly_count", "poly_vertices", "poly_normals", "materials")]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with physicssimulation-agony_b200/build.py "
+                          "(the CUDA library is required; there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    i32, u32, u64, vp = ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p
+    L.ag2d_last_error_string.restype = ctypes.c_char_p
+    L.ag2d_version.restype = i32
+    L.ag2d_device_count.argtypes = [ctypes.POINTER(i32)]
+    L.ag2d_world_create.argtypes = [ctypes.POINTER(WorldSettings), ctypes.POINTER(vp)]
+    L.ag2d_world_destroy.argtypes = [vp]
+    L.ag2d_world_add_material.argtypes = [vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.POINTER(u32)]
+    L.ag2d_world_add_circle.argtypes = [vp, ctypes.POINTER(BodyDesc), ctypes.c_float, ctypes.POINTER(u64)]
+    L.ag2d_world_add_box.argtypes = [vp, ctypes.POINTER(BodyDesc), ctypes.c_float, ctypes.c_float,
+                                     ctypes.POINTER(u64)]
+    L.ag2d_world_add_polygon.argtypes = [vp, ctypes.POINTER(BodyDesc), vp, u32, ctypes.POINTER(u64)]
+    L.ag2d_world_body_index.restype = u32
+    L.ag2d_world_body_index.argtypes = [vp, u64]
+    L.ag2d_world_load_state.argtypes = [vp, ctypes.POINTER(StateDesc)]
+    L.ag2d_world_step.argtypes = [vp, i32]
+    L.ag2d_world_counters.argtypes = [vp, ctypes.POINTER(Counters)]
+    L.ag2d_world_body_count.argtypes = [vp, ctypes.POINTER(u32), ctypes.POINTER(u32)]
+    L.ag2d_world_read.argtypes = [vp, i32, vp, u64, ctypes.POINTER(u64)]
+    L.ag2d_world_write.argtypes = [vp, i32, vp, u64]
+    L.ag2d_world_run_phase.argtypes = [vp, i32]
+    L.ag2d_batch_create.argtypes = [ctypes.POINTER(vp), u32, ctypes.POINTER(vp)]
+    L.ag2d_batch_step.argtypes = [vp, i32]
+    L.ag2d_batch_destroy.argtypes = [vp]
+    return L
+
+
+class _Lib:
+    """Loads libag2d.so on first use (so that ag2d.scenes imports without it) and raises if it is missing."""
+
+    _handle = None
+
+    def __getattr__(self, name):
+        if _Lib._handle is None:
+            _Lib._handle = _load()
+        return getattr(_Lib._handle, name)
+
+
+lib = _Lib()
+
+
+def _check(code: int):
+    if code != OK:
+        raise Ag2dError(code, lib.ag2d_last_error_string().decode(errors="replace"))
+
+
+def device_count() -> int:
+    n = ctypes.c_int32(0)
+    _check(lib.ag2d_device_count(ctypes.byref(n)))
+    return int(n.value)
+
+
+class World:
+    """One simulated world (the reference's Simulation, Simulation.h:36-255) resident on a GPU."""
+
+    def __init__(self, dt=1.0 / 60.0, velocity_iterations=8, position_iterations=3, gravity=(0.0, -9.81),
+                 angular_damping=1.0, sleep_speed=0.1, sleep_time=0.5, ccd=False, device=0):
+        s = WorldSettings(dt, velocity_iterations, position_iterations, gravity[0], gravity[1], angular_damping,
+                          sleep_speed, sleep_time, 1 if ccd else 0, device)
+        h = ctypes.c_void_p()
+        _check(lib.ag2d_world_create(ctypes.byref(s), ctypes.byref(h)))
+        self.h = h
+        self.settings = s
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.ag2d_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- creation (ObjectAPI) ---
+    def add_material(self, elasticity, static_friction, dynamic_friction) -> int:
+        idx = ctypes.c_uint32()
+        _check(lib.ag2d_world_add_material(self.h, elasticity, static_friction, dynamic_friction, ctypes.byref(idx)))
+        return int(idx.value)
+
+    @staticmethod
+    def _desc(x, y, rotation, vx, vy, w, mass, material):
+        return BodyDesc(x, y, rotation, vx, vy, w, mass, material)
+
+    def add_circle(self, radius, x, y, rotation=0.0, vx=0.0, vy=0.0, w=0.0, mass=1.0, material=0) -> int:
+        h = ctypes.c_uint64()
+        d = self._desc(x, y, rotation, vx, vy, w, mass, material)
+        _check(lib.ag2d_world_add_circle(self.h, ctypes.byref(d), radius, ctypes.byref(h)))
+        return int(h.value)
+
+    def add_box(self, width, height, x, y, rotation=0.0, vx=0.0, vy=0.0, w=0.0, mass=1.0, material=0) -> int:
+        h = ctypes.c_uint64()
+        d = self._desc(x, y, rotation, vx, vy, w, mass, material)
+        _check(lib.ag2d_world_add_box(self.h, ctypes.byref(d), width, height, ctypes.byref(h)))
+        return int(h.value)
+
+    def add_polygon(self, vertices, x, y, rotation=0.0, vx=0.0, vy=0.0, w=0.0, mass=1.0, material=0) -> int:
+        v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 2)
+        h = ctypes.c_uint64()
+        d = self._desc(x, y, rotation, vx, vy, w, mass, material)
+        _check(lib.ag2d_world_add_polygon(self.h, ctypes.byref(d), v.ctypes.data, v.shape[0], ctypes.byref(h)))
+        return int(h.value)
+
+    def body_index(self, handle: int) -> int:
+        return int(lib.ag2d_world_body_index(self.h, handle))
+
+    @classmethod
+    def from_scene(cls, scene, device=0, **kw):
+        w = cls(dt=scene.dt, velocity_iterations=scene.velocity_iterations,
+                position_iterations=scene.position_iterations, gravity=scene.gravity, device=device, **kw)
+        mats = [w.add_material(*m) for m in scene.materials]
+        for i in range(scene.n):
+            mat = mats[int(scene.material[i]) - 1] if int(scene.material[i]) >= 1 else 0
+            args = (float(scene.px[i]), float(scene.py[i]), float(scene.rot[i]), float(scene.vx[i]),
+                    float(scene.vy[i]), float(scene.w[i]), float(scene.mass[i]), mat)
+            k = int(scene.kind[i])
+            if k == scenes.POLYGON:
+                w.add_polygon(scene.polygon_vertices(i), *args)
+            elif k == scenes.BOX:
+                w.add_box(float(scene.width[i]), float(scene.height[i]), *args)
+            else:
+                w.add_circle(float(scene.radius[i]), *args)
+        return w
+
+    def load_state(self, state: dict, prefix: str = "", materials=None, body_prefix=None):
+        """Replaces the world by a reference-layout state dict ("body.comX", "col.bodyIndex", ...)."""
+        bp = prefix if body_prefix is None else body_prefix
+
+        def g(k, dt):
+            for p in ((bp,) if k.startswith("body.") else (prefix, "pre.")):
+                if p + k in state:
+                    return np.ascontiguousarray(np.asarray(state[p + k]), dtype=dt)
+            raise KeyError(prefix + k)
+
+        f, u = np.float32, np.uint32
+        arrays = {
+            "body_group_starts": g("body.groupStarts", u), "com_x": g("body.comX", f), "com_y": g("body.comY", f),
+            "vel_x": g("body.velocityX", f), "vel_y": g("body.velocityY", f), "rotation": g("body.rotation", f),
+            "angular_velocity": g("body.angularVelocity", f), "inv_mass": g("body.invMass", f),
+            "inv_inertia": g("body.invInertia", f), "rot_cos": g("body.rotationCos", f),
+            "rot_sin": g("body.rotationSin", f), "wrap_count": g("body.renderRotationWrapCount", f),
+            "bound_radius": g("body.boundRadius", f), "sleep_timer": g("body.sleepingTimer", f),
+            "sleep_island": g("body.sleepIslandId", u), "col_body": g("col.bodyIndex", u),
+            "col_shape_type": g("col.shapeType", u), "col_shape_index": g("col.shapeIndex", u),
+            "col_material": g("col.materialIndex", u), "col_com_offset_x": g("col.comOffsetX", f),
+            "col_com_offset_y": g("col.comOffsetY", f), "col_local_rotation": g("col.localRotation", f),
+            "circle_radius": g("circle.radius", f), "box_half_width": g("box.halfWidth", f),
+            "box_half_height": g("box.halfHeight", f), "poly_count": g("poly.counts", u),
+            "poly_vertices": g("poly.vertices", f), "poly_normals": g("poly.normals", f),
+        }
+        mats = np.ascontiguousarray(np.asarray(materials if materials is not None else [(1.0, 0.0, 0.0)],
+                                               dtype=np.float32).reshape(-1, 3))
+        arrays["materials"] = mats
+        d = StateDesc()
+        d.n_bodies = arrays["com_x"].size
+        d.n_colliders = arrays["col_body"].size
+        d.n_circles = arrays["circle_radius"].size
+        d.n_boxes = arrays["box_half_width"].size
+        d.n_polygons = arrays["poly_count"].size
+        d.n_materials = mats.shape[0]
+        for k, v in arrays.items():
+            setattr(d, k, v.ctypes.data if v.size else None)
+        self._keep = list(arrays.values())
+        _check(lib.ag2d_world_load_state(self.h, ctypes.byref(d)))
+
+    # --- stepping ---
+    def step(self, steps: int = 1):
+        _check(lib.ag2d_world_step(self.h, steps))
+
+    def run_phase(self, phase: int):
+        _check(lib.ag2d_world_run_phase(self.h, phase))
+
+    def counters(self) -> dict:
+        c = Counters()
+        _check(lib.ag2d_world_counters(self.h, ctypes.byref(c)))
+        return {n: int(getattr(c, n)) for n, _ in Counters._fields_}
+
+    def counts(self):
+        b, c = ctypes.c_uint32(), ctypes.c_uint32()
+        _check(lib.ag2d_world_body_count(self.h, ctypes.byref(b), ctypes.byref(c)))
+        return int(b.value), int(c.value)
+
+    # --- field access ---
+    def read(self, field: int) -> np.ndarray:
+        n = ctypes.c_uint64()
+        _check(lib.ag2d_world_read(self.h, field, None, 0, ctypes.byref(n)))
+        buf = np.empty(int(n.value), dtype=np.uint8)
+        _check(lib.ag2d_world_read(self.h, field, buf.ctypes.data if buf.size else None, buf.size, ctypes.byref(n)))
+        if field in (MANIFOLDS, PREV_MANIFOLDS):
+            return buf.view(MANIFOLD_DTYPE)
+        if field == PAIRS:
+            return buf.view(np.uint32).reshape(-1, 2)
+        return buf.view(np.uint32 if field in _U32_FIELDS else np.float32)
+
+    def write(self, field: int, data: np.ndarray):
+        if field in (MANIFOLDS, PREV_MANIFOLDS):
+            a = np.ascontiguousarray(data, dtype=MANIFOLD_DTYPE)
+        elif field == PAIRS:
+            a = np.ascontiguousarray(data, dtype=np.uint32).reshape(-1, 2)
+        else:
+            a = np.ascontiguousarray(data, dtype=np.float32)
+        _check(lib.ag2d_world_write(self.h, field, a.ctypes.data if a.size else None, a.nbytes))
+
+
+class Batch:
+    """Many independent worlds advanced together (one launch sequence per step for all of them)."""
+
+    def __init__(self, worlds):
+        self.worlds = list(worlds)
+        arr = (ctypes.c_void_p * len(self.worlds))(*[w.h for w in self.worlds])
+        h = ctypes.c_void_p()
+        _check(lib.ag2d_batch_create(arr, len(self.worlds), ctypes.byref(h)))
+        self.h = h
+
+    def step(self, steps: int = 1):
+        _check(lib.ag2d_batch_step(self.h, steps))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.ag2d_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

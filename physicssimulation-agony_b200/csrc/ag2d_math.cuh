@@ -1,0 +1,537 @@
+// Device-side fp32 arithmetic of the collision/contact pipeline, shared by every kernel.
+//
+// Each function reproduces one reference routine operation for operation (PS_AGONY2D, paths relative to
+// PhysicsSimulation-Agony/PS_AGONY2D/). The library is compiled with --fmad=false, so a*b+c stays two roundings as
+// in the reference's parity build; __fmaf_rn appears only where the reference's AVX2 path issues an FMA
+// instruction (Simd::negMulAdd in the rotation wrap). sqrtf and '/' are IEEE-rounded (-prec-sqrt/-prec-div on).
+//
+// Where the reference's SIMD body and scalar tail compute differently, a 'simd' flag selects the variant: the
+// reference processes a range [begin, end) in 8-lane AVX2 chunks, so element begin + k takes the SIMD path iff
+// k < ((end - begin) & ~7).
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+namespace ag2d {
+
+// Constants.h:7-14 — double constants rounded to float.
+constexpr double FULL_PI = 3.14159265358979323846;
+constexpr float HALF_PI_F = float(FULL_PI * 0.5);
+constexpr float INV_HALF_PI_F = float(1.0 / (FULL_PI * 0.5));
+constexpr float TWO_PI_F = float(FULL_PI * 2.0);
+constexpr float INV_TWO_PI_F = float(1.0 / (FULL_PI * 2.0));
+
+// FastCosSin.cpp:10-14.
+constexpr float COEF0 = float(9.9999999999953215e-01);
+constexpr float COEF1 = float(-1.6666666534403832e-01);
+constexpr float COEF2 = float(8.3332302391869520e-03);
+constexpr float COEF3 = float(-1.9818200679665358e-04);
+constexpr float COEF4 = float(2.6182346015248291e-06);
+
+// Narrow/Constants.h:7-37.
+constexpr float ZERO_DIVISION_BOUNDARY = 1e-4f;
+constexpr float ZERO_DIVISION_BOUNDARY_SQUARED = 1e-8f;
+constexpr float SAT_EPSILON = 1e-4f;
+constexpr uint32_t REFERENCE_BODY_TAG = 0x80000000u;
+
+enum ShapeType : uint32_t { SHAPE_CIRCLE = 0, SHAPE_BOX = 1, SHAPE_POLYGON = 2 };
+constexpr uint32_t MAX_POLYGON_VERTICES = 16;   // Limits.h:6
+
+// std::fmax / std::fmin as glibc implements them on x86-64 (the reference's build): the first argument if it
+// compares greater (resp. smaller) or the second is NaN, else the second. fmax(+0, -0) is -0.
+__host__ __device__ __forceinline__ float rfmaxf(float a, float b) { return (a > b || b != b) ? a : b; }
+__host__ __device__ __forceinline__ float rfminf(float a, float b) { return (a < b || b != b) ? a : b; }
+
+// glm::clamp for scalars: min(max(x, lo), hi) with max(x, y) = (x < y) ? y : x and min(x, y) = (y < x) ? y : x.
+__host__ __device__ __forceinline__ float glm_clamp(float x, float lo, float hi)
+{
+    const float t = (x < lo) ? lo : x;
+    return (hi < t) ? hi : t;
+}
+
+__device__ __forceinline__ float xor_sign(float v, uint32_t bit) { return __uint_as_float(__float_as_uint(v) ^ bit); }
+
+// FastCosSin::order5Array, one element (FastCosSin.cpp:26-109).
+__device__ __forceinline__ void fast_cos_sin(float x, bool simd, float& out_cos, float& out_sin)
+{
+    const int q = int(x * INV_HALF_PI_F);                       // truncation (cvttps / int cast)
+    const float u = x - float(q) * HALF_PI_F;
+    const float mirror = float(q & 1);
+    const float a = mirror * (HALF_PI_F - 2.0f * u) + u;
+    const float a2 = a * a;
+    float s = COEF4;
+    s = s * a2 + COEF3;
+    s = s * a2 + COEF2;
+    s = s * a2 + COEF1;
+    s = s * a2 + COEF0;
+    s = s * a;
+    s = (s < 1.0f) ? s : 1.0f;                                  // min(sinMag, 1)
+    const float c = sqrtf(1.0f - s * s);
+    if (simd) {
+        out_sin = xor_sign(s, uint32_t(q & 2) << 30);
+        out_cos = xor_sign(c, uint32_t((q + 1) & 2) << 30);
+    } else {
+        const float sinSign = 1.0f - 2.0f * float(q >> 1);
+        const float cosSign = 1.0f - 2.0f * float(((q + 1) >> 1) & 1);
+        out_sin = sinSign * s;
+        out_cos = cosSign * c;
+    }
+}
+
+// wrapBodyRotations / wrapColliderRotations, one element (SimulationImpl/LeftOutFunctions.cpp:13-102).
+// Returns the wrapped angle in [0, 2 pi]; 'wraps' receives the whole-turn count removed.
+__device__ __forceinline__ float wrap_angle(float rot, bool simd, float& wraps)
+{
+    float wc;
+    if (simd) {
+        wc = truncf(rot * (1.0f / TWO_PI_F));
+        rot = __fmaf_rn(-wc, TWO_PI_F, rot);                    // _mm256_fnmadd_ps
+        if (rot < 0.0f) { rot += TWO_PI_F; wc -= 1.0f; } else { rot += 0.0f; wc -= 0.0f; }
+    } else {
+        wc = truncf(rot * INV_TWO_PI_F);
+        rot -= wc * TWO_PI_F;
+        const float neg = float(rot < 0.0f);
+        rot += neg * TWO_PI_F;
+        wc -= neg;
+    }
+    wraps = wc;
+    return rot;
+}
+
+__device__ __forceinline__ uint32_t part1by1(uint32_t x)
+{
+    x &= 0x0000ffffu;
+    x = (x | (x << 8)) & 0x00FF00FFu;
+    x = (x | (x << 4)) & 0x0F0F0F0Fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    x = (x | (x << 1)) & 0x55555555u;
+    return x;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Narrow phase (CollisionDetection/Narrow/*). Vectors are (x, y) pairs of floats; glm::dot(a, b) = a.x*b.x + a.y*b.y.
+// ---------------------------------------------------------------------------------------------------------------
+
+struct V2 { float x, y; };
+__device__ __forceinline__ V2 v2(float x, float y) { return V2{x, y}; }
+__device__ __forceinline__ float dot(V2 a, V2 b) { return a.x * b.x + a.y * b.y; }
+__device__ __forceinline__ V2 operator-(V2 a, V2 b) { return V2{a.x - b.x, a.y - b.y}; }
+__device__ __forceinline__ V2 operator+(V2 a, V2 b) { return V2{a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ V2 operator*(V2 a, float s) { return V2{a.x * s, a.y * s}; }
+__device__ __forceinline__ V2 operator-(V2 a) { return V2{-a.x, -a.y}; }
+__device__ __forceinline__ uint32_t next_index(uint32_t i, uint32_t n) { return i + 1 == n ? 0u : i + 1; }
+
+// One collider as the narrow phase sees it: world pose and shape parameters.
+struct ColliderView {
+    V2 pos;
+    float c, s;            // world rotation cos/sin
+    uint32_t type;
+    float r;               // circle radius
+    float hw, hh;          // box half extents
+    const float2* verts;   // polygon, body-local (centred on the piece centroid)
+    const float2* normals;
+    uint32_t nv;
+};
+
+// Manifold as produced by a method (before warm start).
+struct Contact {
+    V2 n;
+    float depth;
+    uint32_t count;
+    V2 p[2];
+    uint32_t id[2];
+};
+
+// clipSegment (HelperMethods.h:36-52). True if both points are outside the plane.
+__device__ __forceinline__ bool clip_segment(V2& p1, V2& p2, V2 planePoint, V2 planeNormal)
+{
+    const float d1 = dot(p1 - planePoint, planeNormal);
+    const float d2 = dot(p2 - planePoint, planeNormal);
+    if (d1 >= 0.0f && d2 >= 0.0f) return false;
+    if (d1 < 0.0f && d2 < 0.0f) return true;
+    const float t = d1 / (d1 - d2);
+    const V2 dir = p2 - p1;
+    const V2 inter = p1 + dir * t;
+    if (d1 >= 0.0f) p2 = inter; else p1 = inter;
+    return false;
+}
+
+// flipSignIfNegative (HelperMethods.h:26-34).
+__device__ __forceinline__ V2 flip_if_negative(V2 v, float sign)
+{
+    const uint32_t bit = __float_as_uint(sign) & 0x80000000u;
+    return V2{xor_sign(v.x, bit), xor_sign(v.y, bit)};
+}
+
+__device__ __forceinline__ V2 ld2(const float2* p, uint32_t k)
+{
+    const float2 f = __ldg(p + k);
+    return V2{f.x, f.y};
+}
+
+// collisionCircleCircle (CircleCircle.cpp:14-179).
+__device__ __forceinline__ bool collide_circle_circle(const ColliderView& A, const ColliderView& B, Contact& out)
+{
+    const V2 d = B.pos - A.pos;
+    const float rs = A.r + B.r;
+    const float sq = dot(d, d);
+    if (!(sq < rs * rs)) return false;
+    const float dist = sqrtf(sq);
+    V2 n;
+    if (dist < ZERO_DIVISION_BOUNDARY) n = v2(1.0f, 0.0f);
+    else { const float inv = 1.0f / dist; n = d * inv; }
+    out.n = n; out.depth = rs - dist; out.count = 1;
+    out.p[0] = A.pos + n * A.r; out.id[0] = 0;
+    return true;
+}
+
+// collisionCircleBox (CircleBox.cpp:9-120). A circle, B box.
+__device__ __forceinline__ bool collide_circle_box(const ColliderView& A, const ColliderView& B, Contact& out)
+{
+    const float cB = B.c, sB = B.s, hw = B.hw, hh = B.hh, rA = A.r;
+    const V2 dg = A.pos - B.pos;
+    const V2 loc = v2(dg.x * cB + dg.y * sB, dg.x * -sB + dg.y * cB);
+    const V2 cl = v2(rfminf(rfmaxf(loc.x, -hw), hw), rfminf(rfmaxf(loc.y, -hh), hh));
+    const V2 dl = cl - loc;
+    const float sq = dot(dl, dl);
+    if (sq >= rA * rA) return false;
+    out.count = 1;
+    if (sq >= ZERO_DIVISION_BOUNDARY_SQUARED) {
+        const float dist = sqrtf(sq);
+        const float inv = 1.0f / dist;
+        const V2 wd = v2(cB * dl.x - sB * dl.y, sB * dl.x + cB * dl.y);
+        const V2 n = wd * inv;
+        uint32_t id = 0;
+        id |= uint32_t(loc.x > hw);
+        id |= uint32_t(loc.x < -hw) << 1;
+        id |= uint32_t(loc.y > hh) << 2;
+        id |= uint32_t(loc.y < -hh) << 3;
+        out.n = n; out.depth = rA - dist; out.p[0] = A.pos + n * rA; out.id[0] = id;
+        return true;
+    }
+    const float dx = hw - fabsf(loc.x);
+    const float dy = hh - fabsf(loc.y);
+    const bool useY = dy <= dx;
+    const float minPen = useY ? dy : dx;
+    const float sign = copysignf(1.0f, useY ? loc.y : loc.x);
+    const V2 nl = v2(useY ? 0.0f : sign, useY ? sign : 0.0f);
+    const uint32_t id = 1u << (uint32_t(sign <= 0.0f) + (uint32_t(useY) << 1));
+    const V2 n = -v2(cB * nl.x - sB * nl.y, sB * nl.x + cB * nl.y);
+    out.n = n; out.depth = rA + minPen; out.p[0] = A.pos + n * rA; out.id[0] = id;
+    return true;
+}
+
+// collisionCirclePolygon (CirclePolygon.cpp:10-103), findSupportEdge / closestPointOnSegment
+// (HelperMethods.h:73-109). A circle, B polygon.
+__device__ __forceinline__ bool collide_circle_polygon(const ColliderView& A, const ColliderView& B, Contact& out)
+{
+    const float cB = B.c, sB = B.s, rA = A.r;
+    const V2 dg = A.pos - B.pos;
+    const V2 loc = v2(dg.x * cB + dg.y * sB, dg.x * -sB + dg.y * cB);
+    float maxSep = -FLT_MAX;
+    uint32_t edge = 0;
+    for (uint32_t i = 0; i < B.nv; i++) {
+        const float sep = dot(ld2(B.normals, i), loc - ld2(B.verts, i));
+        if (sep > rA) return false;
+        if (sep > maxSep) { maxSep = sep; edge = i; }
+    }
+    V2 nl;
+    float separation;
+    if (maxSep >= ZERO_DIVISION_BOUNDARY) {
+        const V2 va = ld2(B.verts, edge), vb = ld2(B.verts, next_index(edge, B.nv));
+        const V2 ab = vb - va;
+        const float denom = dot(ab, ab);
+        V2 cp;
+        if (denom < ZERO_DIVISION_BOUNDARY_SQUARED) cp = va;
+        else {
+            const float t = dot(loc - va, ab) / denom;
+            cp = va + ab * rfminf(rfmaxf(t, 0.0f), 1.0f);
+        }
+        const V2 cpd = loc - cp;
+        const float d2 = dot(cpd, cpd);
+        if (d2 > rA * rA) return false;
+        if (d2 < ZERO_DIVISION_BOUNDARY_SQUARED) { separation = 0.0f; nl = ld2(B.normals, edge); }
+        else { separation = sqrtf(d2); nl = cpd * (1.0f / separation); }
+    } else {
+        nl = ld2(B.normals, edge);
+        separation = maxSep;
+    }
+    const V2 n = -v2(cB * nl.x - sB * nl.y, sB * nl.x + cB * nl.y);
+    out.n = n; out.depth = rA - separation; out.count = 1; out.p[0] = A.pos + n * rA; out.id[0] = edge;
+    return true;
+}
+
+// collisionBoxBox (BoxBox.cpp:13-227).
+__device__ __forceinline__ bool collide_box_box(const ColliderView& A, const ColliderView& B, Contact& out)
+{
+    const float cA = A.c, sA = A.s, cB = B.c, sB = B.s;
+    const float hwA = A.hw, hhA = A.hh, hwB = B.hw, hhB = B.hh;
+    const V2 rightA = v2(cA, sA), upA = v2(-sA, cA), rightB = v2(cB, sB), upB = v2(-sB, cB);
+    const float relCos = cA * cB + sA * sB;
+    const float relSin = cA * sB - sA * cB;
+    const float arc = fabsf(relCos), ars = fabsf(relSin);
+    const V2 cd = B.pos - A.pos;
+    const float hwL[4] = {hwB, hwB, hwA, hwA}, hhL[4] = {hhB, hhB, hhA, hhA}, hwhL[4] = {hwA, hhA, hwB, hhB};
+    const float cs1[4] = {arc, ars, arc, ars}, cs2[4] = {ars, arc, ars, arc};
+    const float axX[4] = {cA, -sA, cB, -sB}, axY[4] = {sA, cA, sB, cB};
+    float ov[4], cdoa[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float rsum = hwL[k] * cs1[k] + hhL[k] * cs2[k] + hwhL[k];
+        cdoa[k] = cd.x * axX[k] + cd.y * axY[k];
+        ov[k] = rsum - fabsf(cdoa[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) if (ov[k] < 0.0f) return false;
+    const float depth = rfminf(rfminf(ov[0], ov[1]), rfminf(ov[2], ov[3]));
+    const uint32_t n0 = ov[0] != depth;
+    const uint32_t n01 = n0 & uint32_t(ov[1] != depth);
+    const uint32_t n012 = n01 & uint32_t(ov[2] != depth);
+    const uint32_t best = n0 + n01 + n012;
+    float bestAxX, bestAxY, bestCdoa;
+    switch (best) {   // register-friendly indexing
+    case 0: bestAxX = axX[0]; bestAxY = axY[0]; bestCdoa = cdoa[0]; break;
+    case 1: bestAxX = axX[1]; bestAxY = axY[1]; bestCdoa = cdoa[1]; break;
+    case 2: bestAxX = axX[2]; bestAxY = axY[2]; bestCdoa = cdoa[2]; break;
+    default: bestAxX = axX[3]; bestAxY = axY[3]; bestCdoa = cdoa[3]; break;
+    }
+    const V2 normal = flip_if_negative(v2(bestAxX, bestAxY), bestCdoa);
+    const bool refIsA = best < 2;
+    const V2 posRef = refIsA ? A.pos : B.pos, posInc = refIsA ? B.pos : A.pos;
+    const float hwRef = refIsA ? hwA : hwB, hhRef = refIsA ? hhA : hhB;
+    const float hwInc = refIsA ? hwB : hwA, hhInc = refIsA ? hhB : hhA;
+    const V2 rightRef = refIsA ? rightA : rightB, upRef = refIsA ? upA : upB;
+    const V2 rightInc = refIsA ? rightB : rightA, upInc = refIsA ? upB : upA;
+    const V2 refNormal = refIsA ? normal : -normal;
+    const float sign = copysignf(1.0f, refIsA ? bestCdoa : -bestCdoa);
+    const bool useX = best == 0 || best == 2;
+    V2 rfc, sideDir;
+    if (useX) { rfc = posRef + rightRef * (sign * hwRef); sideDir = upRef; }
+    else { rfc = posRef + upRef * (sign * hhRef); sideDir = rightRef; }
+    const V2 eo = sideDir * (useX ? hhRef : hwRef);
+    const V2 refStart = rfc + eo, refEnd = rfc - eo;
+    V2 c0, c1;
+    {
+        const bool axisIsUp = (best & 1u) != 0;
+        const float sideTerm = (best == 0 || best == 3) ? -relSin : relSin;
+        const float dotX = sign * (axisIsUp ? sideTerm : relCos);
+        const float dotY = sign * (axisIsUp ? relCos : sideTerm);
+        const bool useXi = fabsf(dotX) > fabsf(dotY);
+        const float incSign = -copysignf(1.0f, useXi ? dotX : dotY);
+        V2 fc, off;
+        if (useXi) { fc = posInc + rightInc * (incSign * hwInc); off = upInc * hhInc; }
+        else { fc = posInc + upInc * (incSign * hhInc); off = rightInc * hwInc; }
+        c0 = fc + off; c1 = fc - off;
+    }
+    if (clip_segment(c0, c1, refStart, -sideDir)) return false;
+    if (clip_segment(c0, c1, refEnd, sideDir)) return false;
+    const float refPlaneDist = dot(rfc, refNormal);
+    const uint32_t idBase = best << 1;
+    uint32_t cnt = 0;
+    if (dot(c0, refNormal) <= refPlaneDist + SAT_EPSILON) { out.p[cnt] = c0; out.id[cnt] = idBase | 0u; cnt++; }
+    if (dot(c1, refNormal) <= refPlaneDist + SAT_EPSILON) { out.p[cnt] = c1; out.id[cnt] = idBase | 1u; cnt++; }
+    if (cnt == 0) return false;
+    out.n = normal; out.depth = depth; out.count = cnt;
+    return true;
+}
+
+// collisionBoxPolygon (BoxPolygon.cpp:14-319). A box, B polygon; works in the polygon's frame.
+__device__ __forceinline__ bool collide_box_polygon(const ColliderView& A, const ColliderView& B, Contact& out)
+{
+    const float cA = A.c, sA = A.s, cB = B.c, sB = B.s, hwA = A.hw, hhA = A.hh;
+    const uint32_t nv = B.nv;
+    const V2 rightB = v2(cB, sB), upB = v2(-sB, cB);
+    const float relCos = cA * cB + sA * sB;
+    const float relSin = cA * sB - sA * cB;
+    const V2 rA = v2(relCos, -relSin), uA = v2(relSin, relCos);
+    const V2 dBA = A.pos - B.pos;
+    const V2 bc = v2(dot(dBA, rightB), dot(dBA, upB));
+    V2 nl;
+    float depth, bestFacing, pcxd, pcyd;
+    int bestType;
+    uint32_t bestIndex = 0;
+    {
+        float mn = FLT_MAX, mx = -FLT_MAX;
+        for (uint32_t k = 0; k < nv; k++) { const float p = dot(ld2(B.verts, k), rA); mn = rfminf(mn, p); mx = rfmaxf(mx, p); }
+        const float bcp = dot(bc, rA);
+        mn -= bcp; mx -= bcp;
+        const float overlap = hwA + rfminf(-mn, mx);
+        if (overlap < 0.0f) return false;
+        pcxd = mn + mx;
+        depth = overlap; nl = flip_if_negative(rA, pcxd); bestType = 0; bestFacing = -fabsf(pcxd);
+    }
+    {
+        float mn = FLT_MAX, mx = -FLT_MAX;
+        for (uint32_t k = 0; k < nv; k++) { const float p = dot(ld2(B.verts, k), uA); mn = rfminf(mn, p); mx = rfmaxf(mx, p); }
+        const float bcp = dot(bc, uA);
+        mn -= bcp; mx -= bcp;
+        const float overlap = hhA + rfminf(-mn, mx);
+        if (overlap < 0.0f) return false;
+        pcyd = mn + mx;
+        const float facing = -fabsf(pcyd);
+        if (overlap < depth || (overlap == depth && facing < bestFacing)) {
+            depth = overlap; nl = flip_if_negative(uA, pcyd); bestType = 1; bestFacing = facing;
+        }
+    }
+    const V2 pcr = v2(pcxd * rA.x + pcyd * uA.x, pcxd * rA.y + pcyd * uA.y);
+    for (uint32_t i = 0; i < nv; i++) {
+        const V2 ax = ld2(B.normals, i);
+        const float boxRadius = hwA * fabsf(dot(ax, rA)) + hhA * fabsf(dot(ax, uA));
+        const float bcp = dot(bc, ax);
+        const float overlap = dot(ax, ld2(B.verts, i)) - (bcp - boxRadius);
+        if (overlap < 0.0f) return false;
+        const float facing = dot(ax, pcr);
+        if (overlap < depth || (overlap == depth && facing < bestFacing)) {
+            depth = overlap; nl = -ax; bestType = 2; bestIndex = i; bestFacing = facing;
+        }
+    }
+    const bool refIsBox = bestType != 2;
+    V2 rnl, rfc, sd, rs, re, c0, c1;
+    uint32_t ie, ie2;
+    if (refIsBox) {
+        rnl = nl;
+        const bool useX = bestType == 0;
+        const float sign = useX ? dot(rnl, rA) : dot(rnl, uA);
+        if (useX) { rfc = bc + rA * (sign * hwA); sd = uA; }
+        else { rfc = bc + uA * (sign * hhA); sd = rA; }
+        const V2 eo = sd * (useX ? hhA : hwA);
+        rs = rfc + eo; re = rfc - eo;
+        ie = 0;
+        float minDot = FLT_MAX;
+        for (uint32_t i = 0; i < nv; i++) {
+            const float d = dot(rnl, ld2(B.normals, i));
+            if (d < minDot) { minDot = d; ie = i; }
+        }
+        ie2 = next_index(ie, nv);
+        c0 = ld2(B.verts, ie); c1 = ld2(B.verts, ie2);
+    } else {
+        rnl = -nl;
+        const uint32_t i0 = bestIndex, i1 = next_index(i0, nv);
+        rs = ld2(B.verts, i0); re = ld2(B.verts, i1);
+        rfc = (rs + re) * 0.5f;
+        const V2 edge = re - rs;
+        const float len2 = dot(edge, edge);
+        sd = edge * (-1.0f / sqrtf(len2));
+        const float dotX = dot(rnl, rA), dotY = dot(rnl, uA);
+        const bool useX = fabsf(dotX) > fabsf(dotY);
+        const float sign = -copysignf(1.0f, useX ? dotX : dotY);
+        // BOX_INCIDENT_EDGE_IDS[useX][sign > 0] (Narrow/Constants.h:34-37): {{1,2},{0,3}}, {{3,2},{0,1}}.
+        const bool pos = sign > 0.0f;
+        ie = pos ? 0u : (useX ? 3u : 1u);
+        ie2 = pos ? (useX ? 1u : 3u) : 2u;
+        V2 fc, off;
+        if (useX) { fc = bc + rA * (sign * hwA); off = uA * hhA; }
+        else { fc = bc + uA * (sign * hhA); off = rA * hwA; }
+        c0 = fc + off; c1 = fc - off;
+    }
+    if (clip_segment(c0, c1, rs, -sd)) return false;
+    if (clip_segment(c0, c1, re, sd)) return false;
+    const uint32_t tag = refIsBox ? REFERENCE_BODY_TAG : 0u;
+    const float refPlaneDist = dot(rfc, rnl);
+    uint32_t cnt = 0;
+    if (dot(c0, rnl) <= refPlaneDist + SAT_EPSILON) {
+        out.p[cnt] = (B.pos + rightB * c0.x) + upB * c0.y; out.id[cnt] = tag | ie; cnt++;
+    }
+    if (dot(c1, rnl) <= refPlaneDist + SAT_EPSILON) {
+        out.p[cnt] = (B.pos + rightB * c1.x) + upB * c1.y; out.id[cnt] = tag | ie2; cnt++;
+    }
+    if (cnt == 0) return false;
+    out.n = rightB * nl.x + upB * nl.y; out.depth = depth; out.count = cnt;
+    return true;
+}
+
+// collisionPolygonPolygon (PolygonPolygon.cpp:18-235). B's vertices are brought into A's frame.
+__device__ __forceinline__ bool collide_polygon_polygon(const ColliderView& A, const ColliderView& B, Contact& out)
+{
+    V2 vB[MAX_POLYGON_VERTICES];
+    const float cA = A.c, sA = A.s, cB = B.c, sB = B.s;
+    const uint32_t nA = A.nv, nB = B.nv;
+    const V2 rightA = v2(cA, sA), upA = v2(-sA, cA);
+    const V2 cd = B.pos - A.pos;
+    const V2 bdl = v2(dot(cd, rightA), dot(cd, upA));
+    const float relCos = cA * cB + sA * sB;
+    const float relSin = cA * sB - sA * cB;
+    for (uint32_t i = 0; i < nB; i++) {
+        const V2 v = ld2(B.verts, i);
+        vB[i] = v2(bdl.x + relCos * v.x - relSin * v.y, bdl.y + relSin * v.x + relCos * v.y);
+    }
+    V2 nl = v2(0.0f, 0.0f);
+    float depth = FLT_MAX, bestFacing = FLT_MAX;
+    bool bestIsB = false;
+    uint32_t bestIndex = 0;
+    for (uint32_t i = 0; i < nA; i++) {
+        const V2 ax = ld2(A.normals, i);
+        float minB = FLT_MAX;
+        for (uint32_t j = 0; j < nB; j++) minB = rfminf(minB, dot(vB[j], ax));
+        const float overlap = dot(ld2(A.verts, i), ax) - minB;
+        if (overlap < 0.0f) return false;
+        const float facing = -dot(ax, bdl);
+        if (overlap > depth) continue;
+        if (overlap < depth || facing < bestFacing) { depth = overlap; nl = ax; bestIsB = false; bestIndex = i; bestFacing = facing; }
+    }
+    for (uint32_t i = 0; i < nB; i++) {
+        const V2 nb = ld2(B.normals, i);
+        const V2 ax = v2(relCos * nb.x - relSin * nb.y, relSin * nb.x + relCos * nb.y);
+        float minA = FLT_MAX;
+        for (uint32_t j = 0; j < nA; j++) minA = rfminf(minA, dot(ld2(A.verts, j), ax));
+        const float overlap = dot(vB[i], ax) - minA;
+        if (overlap < 0.0f) return false;
+        const float facing = dot(ax, bdl);
+        if (overlap > depth) continue;
+        if (overlap < depth || facing < bestFacing) { depth = overlap; nl = -ax; bestIsB = true; bestIndex = i; bestFacing = facing; }
+    }
+    const bool refIsA = !bestIsB;
+    const uint32_t refCount = refIsA ? nA : nB, incCount = refIsA ? nB : nA;
+    const V2 rnl = refIsA ? nl : -nl;
+    const uint32_t i0 = bestIndex, i1 = next_index(i0, refCount);
+    const V2 rs = refIsA ? ld2(A.verts, i0) : vB[i0];
+    const V2 re = refIsA ? ld2(A.verts, i1) : vB[i1];
+    const V2 rfc = (rs + re) * 0.5f;
+    const V2 edge = re - rs;
+    const float len2 = dot(edge, edge);
+    const V2 sideDir = edge * (1.0f / sqrtf(len2));
+    uint32_t ie = 0;
+    float minDot = FLT_MAX;
+    for (uint32_t i = 0; i < incCount; i++) {
+        V2 n;
+        if (refIsA) { const V2 nb = ld2(B.normals, i); n = v2(relCos * nb.x - relSin * nb.y, relSin * nb.x + relCos * nb.y); }
+        else n = ld2(A.normals, i);
+        const float d = dot(rnl, n);
+        if (d < minDot) { minDot = d; ie = i; }
+    }
+    const uint32_t ie2 = next_index(ie, incCount);
+    V2 c0 = refIsA ? vB[ie] : ld2(A.verts, ie);
+    V2 c1 = refIsA ? vB[ie2] : ld2(A.verts, ie2);
+    if (clip_segment(c0, c1, rs, sideDir)) return false;
+    if (clip_segment(c0, c1, re, -sideDir)) return false;
+    const float refPlaneDist = dot(rfc, rnl);
+    const uint32_t tag = refIsA ? REFERENCE_BODY_TAG : 0u;
+    uint32_t cnt = 0;
+    if (dot(c0, rnl) <= refPlaneDist + SAT_EPSILON) {
+        out.p[cnt] = (A.pos + rightA * c0.x) + upA * c0.y; out.id[cnt] = tag | ie; cnt++;
+    }
+    if (dot(c1, rnl) <= refPlaneDist + SAT_EPSILON) {
+        out.p[cnt] = (A.pos + rightA * c1.x) + upA * c1.y; out.id[cnt] = tag | ie2; cnt++;
+    }
+    if (cnt == 0) return false;
+    out.n = rightA * nl.x + upA * nl.y; out.depth = depth; out.count = cnt;
+    return true;
+}
+
+// Dispatch on the (ordered) shape-type pair: typeA <= typeB.
+__device__ __forceinline__ bool collide(const ColliderView& A, const ColliderView& B, Contact& out)
+{
+    if (A.type == SHAPE_CIRCLE) {
+        if (B.type == SHAPE_CIRCLE) return collide_circle_circle(A, B, out);
+        if (B.type == SHAPE_BOX) return collide_circle_box(A, B, out);
+        return collide_circle_polygon(A, B, out);
+    }
+    if (A.type == SHAPE_BOX) {
+        if (B.type == SHAPE_BOX) return collide_box_box(A, B, out);
+        return collide_box_polygon(A, B, out);
+    }
+    return collide_polygon_polygon(A, B, out);
+}
+
+}  // namespace ag2d

@@ -1,0 +1,148 @@
+// Device-resident world state (HBM layout) and small device utilities shared by the kernels.
+//
+// Layout: structure of arrays, with the fields the solver gathers per body packed into float4 so one 16-byte load
+// serves a contact end: bvel = (vx, vy, w, invMass), bpos = (x, y, rotation, invInertia). Colliders keep their
+// world pose in one float4 (x, y, cos, sin) and their AABB in another (minX, minY, maxX, maxY).
+//
+// Collider and body indices follow the reference's dense order (GroupRanges.h: static, sleeping, dynamic at
+// creation); sleeping is a per-body state flag here instead of a dense-range move, and the per-step work lists
+// (dynamic bodies, dynamic colliders, static+sleeping colliders) are compacted index lists rebuilt on state changes.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ag2d {
+
+enum BodyState : uint8_t { STATE_STATIC = 0, STATE_SLEEPING = 1, STATE_DYNAMIC = 2 };
+
+// Error bits of the per-step status word (a device-side failure never traps; the host reads this word).
+enum StatusBits : uint32_t {
+    STATUS_PAIR_OVERFLOW = 1u << 0,
+    STATUS_MANIFOLD_OVERFLOW = 1u << 1,
+    STATUS_BARRIER_TIMEOUT = 1u << 2,
+    STATUS_LOOKBACK_TIMEOUT = 1u << 3,
+    STATUS_COLOR_OVERFLOW = 1u << 4,
+    STATUS_HASH_FULL = 1u << 5,
+    STATUS_STACK_OVERFLOW = 1u << 6,
+};
+
+// Counters written by the kernels and read back by the host after each step (one 64-byte transfer).
+struct StepCounters {
+    uint32_t status;          // StatusBits
+    uint32_t pairs;           // broad-phase candidate pairs
+    uint32_t manifolds;       // narrow-phase manifolds (>= 1 contact)
+    uint32_t colors;          // solver colours used
+    uint32_t woke;            // bodies woken this step
+    uint32_t slept;           // bodies put to sleep this step
+    uint32_t topoDirty;       // a body changed state: rebuild work lists before the next step
+    uint32_t warmHits;        // manifolds that took warm-start impulses
+    uint32_t barrierRounds;   // colouring rounds
+    uint32_t pad[7];
+};
+
+// Manifold record (64 bytes), NarrowPhaseCollisionDetector.h:26-61 minus the handle union: colliders are stable
+// device indices. Collider a is the reference side of the normal (normal points from a to b).
+struct alignas(16) Manifold {
+    uint32_t a, b;
+    float nx, ny;
+    float depth;
+    uint32_t count;
+    uint32_t id0, id1;
+    float px0, py0, px1, py1;
+    float jn0, jt0, jn1, jt1;     // persistent impulse accumulators (warm start)
+};
+static_assert(sizeof(Manifold) == 64, "Manifold is 64 bytes");
+
+// Per-constraint solver record (128 bytes), built from a Manifold in solving (colour) order: the fields of
+// BodyCollisionSolver's VelocityHotData, PositionHotData, VelocityConstraintData and FrictionData.
+struct alignas(16) Constraint {
+    uint32_t bodyA, bodyB, count, manifold;
+    float nx, ny, imA, imB;
+    float iIA, iIB, sf, df;
+    float jn0, jt0, jn1, jt1;
+    float rAn0, rBn0, rAt0, rBt0;
+    float nm0, tm0, bias0, penBase;
+    float rAn1, rBn1, rAt1, rBt1;
+    float nm1, tm1, bias1, pad;
+};
+static_assert(sizeof(Constraint) == 128, "Constraint is 128 bytes");
+
+struct DeviceWorld {
+    uint32_t nBodies, nColliders, nMaterials;
+    // Bodies.
+    float4* bvel;          // vx, vy, w, invMass
+    float4* bpos;          // x, y, rotation, invInertia
+    float2* brot;          // rotation cos, sin
+    float* wrapCount;      // renderRotationWrapCount
+    float* boundRadius;
+    float* sleepTimer;
+    uint8_t* bstate;       // BodyState
+    uint32_t* sleepIsland; // island id while sleeping (the island's root body index)
+    // Colliders.
+    uint32_t* cbody;       // owner body
+    uint32_t* cshape;      // type << 30 | shape index
+    uint32_t* cmat;        // material index
+    float4* coff;          // comOffsetX, comOffsetY, localRotation, 0
+    float4* cpose;         // world x, y, cos, sin
+    float* cworldRot;      // wrapped world rotation
+    float4* caabb;         // minX, minY, maxX, maxY
+    // Shapes.
+    float* circleRadius;
+    float2* boxHalf;       // halfWidth, halfHeight
+    uint32_t* polyOffset;  // into polyVerts / polyNormals
+    uint32_t* polyCount;
+    float2* polyVerts;
+    float2* polyNormals;
+    // Materials: elasticity, static friction, dynamic friction.
+    float4* materials;
+};
+
+__host__ __device__ __forceinline__ uint32_t shape_type(uint32_t packed) { return packed >> 30; }
+__host__ __device__ __forceinline__ uint32_t shape_index(uint32_t packed) { return packed & 0x3FFFFFFFu; }
+
+// Order-preserving float <-> uint32 map for atomicMin/atomicMax on floats.
+__device__ __forceinline__ uint32_t float_to_ordered(float f)
+{
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ordered_to_float(uint32_t u)
+{
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+// Spin-wait budget for inter-CTA waits (decoupled look-back, grid barriers). A wait that exhausts it records a
+// status bit and gives up instead of hanging the GPU.
+constexpr uint32_t SPIN_LIMIT = 1u << 22;
+
+// Grid-wide barrier for cooperative launches (all CTAs co-resident). 'bar' is {arrive count, generation}, zeroed
+// before launch. Returns false (and sets STATUS_BARRIER_TIMEOUT) if the wait ran out.
+__device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t* status)
+{
+    __syncthreads();
+    __shared__ int ok;
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile uint32_t* gen = bar + 1;
+        const uint32_t g = *gen;
+        __threadfence();
+        const uint32_t arrived = atomicAdd(bar, 1u);
+        if (arrived == gridDim.x - 1) {
+            bar[0] = 0;
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            uint32_t spins = 0;
+            while (*gen == g) {
+                if (++spins > SPIN_LIMIT) { atomicOr(status, STATUS_BARRIER_TIMEOUT); ok = 0; break; }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0 && (*(volatile uint32_t*)status & STATUS_BARRIER_TIMEOUT) == 0;
+}
+
+}  // namespace ag2d

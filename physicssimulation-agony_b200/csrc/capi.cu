@@ -1,0 +1,1104 @@
+// C ABI of libag2d.so (include/ag2d.h): world lifecycle, object creation, the per-step launch sequence, field
+// access and phase-level taps. Host code; every kernel it launches is in k_spatial.cu / k_contact.cu.
+#include "ag2d.h"
+#include "ag2d_kernels.cuh"
+#include "host_objects.hpp"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using namespace ag2d;
+
+namespace {
+
+thread_local std::string g_error;
+
+struct ApiError : std::runtime_error {
+    int32_t code;
+    ApiError(int32_t c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(expr)                                                                                              \
+    do {                                                                                                      \
+        const cudaError_t e_ = (expr);                                                                        \
+        if (e_ != cudaSuccess)                                                                                \
+            throw ApiError(e_ == cudaErrorMemoryAllocation ? AG2D_ERR_OOM : AG2D_ERR_CUDA,                     \
+                           std::string(#expr) + ": " + cudaGetErrorString(e_));                               \
+    } while (0)
+
+template <class F>
+int32_t guarded(F&& f)
+{
+    try {
+        f();
+        return AG2D_OK;
+    } catch (const ApiError& e) {
+        g_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_error = "host allocation failed";
+        return AG2D_ERR_OOM;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return AG2D_ERR_INVALID_ARG;
+    }
+}
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    // Grows to at least 'count' elements; contents are not preserved.
+    void reserve(size_t count)
+    {
+        if (count <= n && p) return;
+        release();
+        const size_t c = std::max<size_t>(count, 1);
+        CK(cudaMalloc(reinterpret_cast<void**>(&p), c * sizeof(T)));
+        n = c;
+    }
+    void upload(const T* src, size_t count, cudaStream_t s)
+    {
+        reserve(count);
+        if (count) CK(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+};
+
+template <class T>
+void swap_bufs(DBuf<T>& a, DBuf<T>& b)
+{
+    std::swap(a.p, b.p);
+    std::swap(a.n, b.n);
+}
+
+inline uint32_t div_up(uint64_t a, uint64_t b) { return uint32_t((a + b - 1) / b); }
+
+// Exclusive scan with per-level block-sum scratch.
+struct Scanner {
+    std::vector<std::unique_ptr<DBuf<uint32_t>>> levels;
+    void reserve(uint32_t n)
+    {
+        uint32_t m = n, lvl = 0;
+        while (true) {
+            const uint32_t nb = div_up(std::max<uint32_t>(m, 1), SCAN_TILE);
+            if (nb <= 1) break;
+            if (levels.size() <= lvl) levels.emplace_back(new DBuf<uint32_t>());
+            levels[lvl]->reserve(nb);
+            m = nb;
+            lvl++;
+        }
+    }
+    void run(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* total, cudaStream_t s, uint32_t lvl = 0)
+    {
+        const uint32_t nb = std::max<uint32_t>(div_up(n, SCAN_TILE), 1);
+        uint32_t* sums = nb > 1 ? levels.at(lvl)->p : nullptr;
+        k_scan_blocks<<<nb, SCAN_THREADS, 0, s>>>(in, out, n, sums);
+        CK(cudaGetLastError());
+        if (nb > 1) {
+            run(sums, sums, nb, nullptr, s, lvl + 1);
+            k_scan_add<<<nb, SCAN_THREADS, 0, s>>>(out, n, sums);
+            CK(cudaGetLastError());
+        }
+        if (total) {
+            k_scan_total<<<1, 32, 0, s>>>(in, out, n, total);
+            CK(cudaGetLastError());
+        }
+    }
+};
+
+struct Tree {
+    DBuf<uint32_t> keys, vals, keys2, vals2;
+    DBuf<int2> child, range;
+    DBuf<int> parent, leafParent;
+    DBuf<float4> leafAabb, nodeAabb;
+    DBuf<uint32_t> visit, bounds, hist, tileState, tileCounter;
+    int n = 0;
+    void reserve(uint32_t cap)
+    {
+        keys.reserve(cap); vals.reserve(cap); keys2.reserve(cap); vals2.reserve(cap);
+        child.reserve(cap); range.reserve(cap); parent.reserve(cap); leafParent.reserve(cap);
+        leafAabb.reserve(cap); nodeAabb.reserve(cap); visit.reserve(cap);
+        bounds.reserve(4); hist.reserve(4 * 256); tileCounter.reserve(4);
+        tileState.reserve(size_t(div_up(std::max<uint32_t>(cap, 1), SORT_TILE)) * 256 * 4);
+    }
+    TreeView view() const { return TreeView{n, child.p, range.p, nodeAabb.p, leafAabb.p, vals.p}; }
+};
+
+struct DeviceInfo {
+    int sms = 0;
+    int coopColorBlocks = 0, coopSolveBlocks = 0;
+};
+
+}  // namespace
+
+struct ag2d_world {
+    ag2d_world_settings settings{};
+    cudaStream_t stream = nullptr;
+    DeviceInfo dev;
+    HostObjects objects;
+    bool hostDirty = true;          // host objects changed since the last upload
+    bool listsDirty = true;         // work lists need a rebuild (state changes)
+    bool fullPose = true;           // next pose pass covers every collider (first step after an upload)
+    bool otherDirty = true;         // static + sleeping tree must be rebuilt
+    uint64_t stepsTaken = 0;
+
+    uint32_t nBodies = 0, nColliders = 0, nDynBody = 0, nDynCol = 0, nOther = 0, nStatic = 0;
+    uint32_t pairCap = 0, manifoldCap = 0, hashCap = 0;
+    uint32_t lastManifolds = 0;
+
+    // Bodies.
+    DBuf<float4> bvel, bpos;
+    DBuf<float2> brot;
+    DBuf<float> wrapCount, boundRadius, sleepTimer;
+    DBuf<uint8_t> bstate;
+    DBuf<uint32_t> sleepIsland;
+    // Snapshot of the mutable body state (restored when a step overflows a buffer).
+    DBuf<float4> snapVel, snapPos;
+    DBuf<float2> snapRot;
+    DBuf<float> snapWrap, snapTimer;
+    DBuf<uint8_t> snapState;
+    DBuf<uint32_t> snapIsland;
+    // Colliders and shapes.
+    DBuf<uint32_t> cbody, cshape, cmat;
+    DBuf<float4> coff, cpose, caabb;
+    DBuf<float> cworldRot;
+    DBuf<float> circleRadius;
+    DBuf<float2> boxHalf, polyVerts, polyNormals;
+    DBuf<uint32_t> polyOffset, polyCount;
+    DBuf<float4> materials;
+    // Work lists.
+    DBuf<uint32_t> dynBody, dynCol, otherCol, flagA, flagB, flagC, offA, offB, offC, listCounts;
+    // Trees and pairs.
+    Tree dynTree, otherTree;
+    DBuf<uint32_t> qCounts, qOffsets;
+    DBuf<uint2> pairs;
+    // Manifolds.
+    DBuf<Manifold> slots, manifolds, prevManifolds;
+    DBuf<uint32_t> hit, hitOffsets, nManifolds, nPrev;
+    DBuf<unsigned long long> hashKeys;
+    DBuf<uint32_t> hashVals;
+    // Colouring and solver.
+    DBuf<uint32_t> color, colorCount, colorStart, order, bar;
+    DBuf<unsigned long long> bodyMax;
+    DBuf<Constraint> cons;
+    // Islands.
+    DBuf<uint32_t> ufParent, ufFlag, wakeIsland;
+    // Counters.
+    DBuf<StepCounters> dCounters;
+    StepCounters* hCounters = nullptr;
+    Scanner scanner;
+
+    DeviceWorld view() const
+    {
+        DeviceWorld w;
+        w.nBodies = nBodies; w.nColliders = nColliders; w.nMaterials = objects.materialCount();
+        w.bvel = bvel.p; w.bpos = bpos.p; w.brot = brot.p; w.wrapCount = wrapCount.p; w.boundRadius = boundRadius.p;
+        w.sleepTimer = sleepTimer.p; w.bstate = bstate.p; w.sleepIsland = sleepIsland.p;
+        w.cbody = cbody.p; w.cshape = cshape.p; w.cmat = cmat.p; w.coff = coff.p; w.cpose = cpose.p;
+        w.cworldRot = cworldRot.p; w.caabb = caabb.p;
+        w.circleRadius = circleRadius.p; w.boxHalf = boxHalf.p; w.polyOffset = polyOffset.p; w.polyCount = polyCount.p;
+        w.polyVerts = polyVerts.p; w.polyNormals = polyNormals.p; w.materials = materials.p;
+        return w;
+    }
+
+    ~ag2d_world()
+    {
+        if (hCounters) cudaFreeHost(hCounters);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    uint32_t gridFor(uint64_t n, uint32_t threads = 256) const
+    {
+        const uint64_t want = (n + threads - 1) / threads;
+        const uint64_t cap = uint64_t(std::max(dev.sms, 1)) * 8;
+        return uint32_t(std::max<uint64_t>(1, std::min(want, cap)));
+    }
+
+    void init(const ag2d_world_settings& s)
+    {
+        settings = s;
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) throw ApiError(AG2D_ERR_NO_DEVICE, "no CUDA device");
+        if (s.device < 0 || s.device >= count) throw ApiError(AG2D_ERR_INVALID_ARG, "device ordinal out of range");
+        CK(cudaSetDevice(s.device));
+        CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        CK(cudaDeviceGetAttribute(&dev.sms, cudaDevAttrMultiProcessorCount, s.device));
+        int perSm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color, 256, 0));
+        dev.coopColorBlocks = std::max(1, perSm) * dev.sms;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_solve, 256, 0));
+        dev.coopSolveBlocks = std::max(1, perSm) * dev.sms;
+        CK(cudaMallocHost(reinterpret_cast<void**>(&hCounters), sizeof(StepCounters)));
+        std::memset(hCounters, 0, sizeof(StepCounters));
+        dCounters.reserve(1);
+        bar.reserve(2);
+        nManifolds.reserve(1);
+        nPrev.reserve(1);
+        listCounts.reserve(3);
+        colorCount.reserve(MAX_COLORS + 1);
+        colorStart.reserve(MAX_COLORS + 1);
+        CK(cudaMemsetAsync(nPrev.p, 0, sizeof(uint32_t), stream));
+        CK(cudaMemsetAsync(nManifolds.p, 0, sizeof(uint32_t), stream));
+    }
+
+    void reserveCapacities(uint32_t pairCapNew, uint32_t manCapNew)
+    {
+        pairCap = pairCapNew;
+        manifoldCap = manCapNew;
+        pairs.reserve(pairCap);
+        slots.reserve(pairCap);
+        hit.reserve(pairCap);
+        hitOffsets.reserve(pairCap);
+        // Manifold arrays keep their contents (the previous step's manifolds are the warm-start source).
+        auto grow_keep = [&](DBuf<Manifold>& b, uint32_t cap) {
+            if (b.n >= cap && b.p) return;
+            DBuf<Manifold> nb;
+            nb.reserve(cap);
+            if (b.p) CK(cudaMemcpyAsync(nb.p, b.p, b.n * sizeof(Manifold), cudaMemcpyDeviceToDevice, stream));
+            CK(cudaStreamSynchronize(stream));
+            swap_bufs(b, nb);
+        };
+        grow_keep(manifolds, manifoldCap);
+        grow_keep(prevManifolds, manifoldCap);
+        color.reserve(manifoldCap);
+        order.reserve(manifoldCap);
+        cons.reserve(manifoldCap);
+        hashCap = 16;
+        while (hashCap < 2 * manifoldCap) hashCap <<= 1;
+        hashKeys.reserve(hashCap);
+        hashVals.reserve(hashCap);
+        scanner.reserve(std::max({pairCap, nColliders, nBodies}));
+    }
+
+    // Uploads the host objects (bodies, colliders, shapes, materials) as the device state.
+    void upload()
+    {
+        const HostObjects& o = objects;
+        nBodies = uint32_t(o.bodies.size());
+        nColliders = uint32_t(o.colliders.size());
+        std::vector<float4> vel(nBodies), pos(nBodies);
+        std::vector<float2> rot(nBodies);
+        std::vector<float> wc(nBodies), br(nBodies), st(nBodies);
+        std::vector<uint8_t> state(nBodies);
+        std::vector<uint32_t> isl(nBodies);
+        for (uint32_t i = 0; i < nBodies; i++) {
+            const HBody& b = o.bodies[i];
+            vel[i] = make_float4(b.vx, b.vy, b.w, b.invMass);
+            pos[i] = make_float4(b.comX, b.comY, b.rot, b.invInertia);
+            rot[i] = make_float2(b.cos, b.sin);
+            wc[i] = b.wrapCount; br[i] = b.boundRadius; st[i] = b.sleepTimer;
+            state[i] = uint8_t(o.bodyGroups.groupOf(i) == 0 ? STATE_STATIC :
+                               (o.bodyGroups.groupOf(i) == 1 ? STATE_SLEEPING : STATE_DYNAMIC));
+            isl[i] = b.sleepIsland;
+        }
+        std::vector<uint32_t> cb(nColliders), cs(nColliders), cm(nColliders);
+        std::vector<float4> co(nColliders);
+        for (uint32_t i = 0; i < nColliders; i++) {
+            const HCollider& c = o.colliders[i];
+            cb[i] = c.body; cs[i] = (c.type << 30) | c.shape; cm[i] = c.material;
+            co[i] = make_float4(c.comOffX, c.comOffY, c.localRot, 0.0f);
+        }
+        std::vector<float2> bh(o.boxHalfW.size());
+        for (size_t i = 0; i < bh.size(); i++) bh[i] = make_float2(o.boxHalfW[i], o.boxHalfH[i]);
+        std::vector<uint32_t> po, pc;
+        std::vector<float2> pv, pn;
+        for (const HPolygon& p : o.polygons) {
+            po.push_back(uint32_t(pv.size()));
+            pc.push_back(uint32_t(p.verts.size() / 2));
+            for (size_t k = 0; k < p.verts.size() / 2; k++) {
+                pv.push_back(make_float2(p.verts[2 * k], p.verts[2 * k + 1]));
+                pn.push_back(make_float2(p.normals[2 * k], p.normals[2 * k + 1]));
+            }
+        }
+        std::vector<float4> mats(o.materialCount());
+        for (size_t i = 0; i < mats.size(); i++)
+            mats[i] = make_float4(o.materials[3 * i], o.materials[3 * i + 1], o.materials[3 * i + 2], 0.0f);
+        uploadArrays(vel, pos, rot, wc, br, st, state, isl, cb, cs, cm, co, o.circleRadius, bh, po, pc, pv, pn, mats);
+    }
+
+    void uploadArrays(const std::vector<float4>& vel, const std::vector<float4>& pos, const std::vector<float2>& rot,
+                      const std::vector<float>& wc, const std::vector<float>& br, const std::vector<float>& st,
+                      const std::vector<uint8_t>& state, const std::vector<uint32_t>& isl,
+                      const std::vector<uint32_t>& cb, const std::vector<uint32_t>& cs,
+                      const std::vector<uint32_t>& cm, const std::vector<float4>& co, const std::vector<float>& cr,
+                      const std::vector<float2>& bh, const std::vector<uint32_t>& po,
+                      const std::vector<uint32_t>& pc, const std::vector<float2>& pv,
+                      const std::vector<float2>& pn, const std::vector<float4>& mats)
+    {
+        const cudaStream_t s = stream;
+        bvel.upload(vel.data(), nBodies, s); bpos.upload(pos.data(), nBodies, s); brot.upload(rot.data(), nBodies, s);
+        wrapCount.upload(wc.data(), nBodies, s); boundRadius.upload(br.data(), nBodies, s);
+        sleepTimer.upload(st.data(), nBodies, s); bstate.upload(state.data(), nBodies, s);
+        sleepIsland.upload(isl.data(), nBodies, s);
+        snapVel.reserve(nBodies); snapPos.reserve(nBodies); snapRot.reserve(nBodies); snapWrap.reserve(nBodies);
+        snapTimer.reserve(nBodies); snapState.reserve(nBodies); snapIsland.reserve(nBodies);
+        cbody.upload(cb.data(), nColliders, s); cshape.upload(cs.data(), nColliders, s);
+        cmat.upload(cm.data(), nColliders, s); coff.upload(co.data(), nColliders, s);
+        cpose.reserve(nColliders); caabb.reserve(nColliders); cworldRot.reserve(nColliders);
+        CK(cudaMemsetAsync(cpose.p, 0, sizeof(float4) * std::max<uint32_t>(nColliders, 1), s));
+        CK(cudaMemsetAsync(caabb.p, 0, sizeof(float4) * std::max<uint32_t>(nColliders, 1), s));
+        CK(cudaMemsetAsync(cworldRot.p, 0, sizeof(float) * std::max<uint32_t>(nColliders, 1), s));
+        circleRadius.upload(cr.data(), cr.size(), s); boxHalf.upload(bh.data(), bh.size(), s);
+        polyOffset.upload(po.data(), po.size(), s); polyCount.upload(pc.data(), pc.size(), s);
+        polyVerts.upload(pv.data(), pv.size(), s); polyNormals.upload(pn.data(), pn.size(), s);
+        materials.upload(mats.data(), mats.size(), s);
+        nStatic = uint32_t(std::count(state.begin(), state.end(), uint8_t(STATE_STATIC)));
+        const uint32_t nmax = std::max(nBodies, nColliders);
+        for (auto* b : {&dynBody, &dynCol, &otherCol, &flagA, &flagB, &flagC, &offA, &offB, &offC}) b->reserve(nmax);
+        dynTree.reserve(nColliders);
+        otherTree.reserve(nColliders);
+        qCounts.reserve(nColliders); qOffsets.reserve(nColliders);
+        bodyMax.reserve(nBodies);
+        ufParent.reserve(nBodies); ufFlag.reserve(nBodies); wakeIsland.reserve(nBodies);
+        const uint32_t cap = std::max<uint32_t>(4 * nColliders, 4096);
+        reserveCapacities(std::max(pairCap, cap), std::max(manifoldCap, cap));
+        CK(cudaMemsetAsync(nPrev.p, 0, sizeof(uint32_t), s));
+        CK(cudaMemsetAsync(nManifolds.p, 0, sizeof(uint32_t), s));
+        CK(cudaStreamSynchronize(s));
+        hostDirty = false;
+        listsDirty = true;
+        fullPose = true;
+        otherDirty = true;
+        lastManifolds = 0;
+    }
+
+    void ensureUploaded()
+    {
+        if (hostDirty) upload();
+    }
+
+    void rebuildLists()
+    {
+        const cudaStream_t s = stream;
+        const uint32_t nmax = std::max(nBodies, nColliders);
+        k_state_flags<<<gridFor(nmax), 256, 0, s>>>(bstate.p, cbody.p, nBodies, nColliders, flagA.p, flagB.p, flagC.p);
+        CK(cudaGetLastError());
+        scanner.run(flagA.p, offA.p, nBodies, listCounts.p + 0, s);
+        scanner.run(flagB.p, offB.p, nColliders, listCounts.p + 1, s);
+        scanner.run(flagC.p, offC.p, nColliders, listCounts.p + 2, s);
+        k_scatter_list<<<gridFor(nBodies), 256, 0, s>>>(flagA.p, offA.p, nBodies, dynBody.p);
+        k_scatter_list<<<gridFor(nColliders), 256, 0, s>>>(flagB.p, offB.p, nColliders, dynCol.p);
+        k_scatter_list<<<gridFor(nColliders), 256, 0, s>>>(flagC.p, offC.p, nColliders, otherCol.p);
+        CK(cudaGetLastError());
+        uint32_t counts[3] = {0, 0, 0};
+        CK(cudaMemcpyAsync(counts, listCounts.p, sizeof(counts), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        nDynBody = counts[0];
+        nDynCol = counts[1];
+        nOther = counts[2];
+        listsDirty = false;
+    }
+
+    void snapshot(bool restore)
+    {
+        const cudaStream_t s = stream;
+        auto cp = [&](void* dst, const void* src, size_t bytes) {
+            if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+        };
+        const size_t n = nBodies;
+        if (!restore) {
+            cp(snapVel.p, bvel.p, n * sizeof(float4)); cp(snapPos.p, bpos.p, n * sizeof(float4));
+            cp(snapRot.p, brot.p, n * sizeof(float2)); cp(snapWrap.p, wrapCount.p, n * sizeof(float));
+            cp(snapTimer.p, sleepTimer.p, n * sizeof(float)); cp(snapState.p, bstate.p, n);
+            cp(snapIsland.p, sleepIsland.p, n * sizeof(uint32_t));
+        } else {
+            cp(bvel.p, snapVel.p, n * sizeof(float4)); cp(bpos.p, snapPos.p, n * sizeof(float4));
+            cp(brot.p, snapRot.p, n * sizeof(float2)); cp(wrapCount.p, snapWrap.p, n * sizeof(float));
+            cp(sleepTimer.p, snapTimer.p, n * sizeof(float)); cp(bstate.p, snapState.p, n);
+            cp(sleepIsland.p, snapIsland.p, n * sizeof(uint32_t));
+        }
+    }
+
+    // ---- phases ----
+    void phaseIntegrate()
+    {
+        const float damp = settings.angular_damping;
+        const float dampHalf = (damp >= 0.0f && damp < 1.0f) ? std::pow(damp, settings.dt * 0.5f) : 2.0f;
+        if (nDynBody) {
+            k_integrate<<<gridFor(nDynBody), 256, 0, stream>>>(view(), dynBody.p, nDynBody, settings.dt,
+                                                              settings.gravity_x, settings.gravity_y, dampHalf);
+            CK(cudaGetLastError());
+        }
+    }
+
+    void phasePose(bool full)
+    {
+        if (full) {
+            if (nColliders) k_collider_pose<<<gridFor(nColliders), 256, 0, stream>>>(view(), nullptr, nColliders);
+        } else if (nDynCol) {
+            k_collider_pose<<<gridFor(nDynCol), 256, 0, stream>>>(view(), dynCol.p, nDynCol);
+        }
+        CK(cudaGetLastError());
+    }
+
+    void buildTree(Tree& t, const uint32_t* list, uint32_t n)
+    {
+        const cudaStream_t s = stream;
+        t.n = int(n);
+        if (n == 0) return;
+        k_bounds_init<<<1, 32, 0, s>>>(t.bounds.p);
+        k_bounds<<<gridFor(n), 256, 0, s>>>(caabb.p, list, n, t.bounds.p);
+        k_morton<<<gridFor(n), 256, 0, s>>>(caabb.p, list, n, t.bounds.p, t.keys.p, t.vals.p);
+        CK(cudaGetLastError());
+        // Onesweep sort, 4 digit passes; results end in keys/vals.
+        CK(cudaMemsetAsync(t.hist.p, 0, 4 * 256 * sizeof(uint32_t), s));
+        k_sort_histogram<<<gridFor(n), 256, 0, s>>>(t.keys.p, n, t.hist.p);
+        k_sort_digit_scan<<<4, 256, 0, s>>>(t.hist.p);
+        CK(cudaGetLastError());
+        const uint32_t tiles = div_up(n, SORT_TILE);
+        CK(cudaMemsetAsync(t.tileState.p, 0, size_t(tiles) * 256 * 4 * sizeof(uint32_t), s));
+        CK(cudaMemsetAsync(t.tileCounter.p, 0, 4 * sizeof(uint32_t), s));
+        uint32_t *ki = t.keys.p, *vi = t.vals.p, *ko = t.keys2.p, *vo = t.vals2.p;
+        for (uint32_t pass = 0; pass < 4; pass++) {
+            k_sort_pass<<<tiles, SORT_THREADS, 0, s>>>(ki, vi, ko, vo, n, pass * 8, t.hist.p + pass * 256,
+                                                        t.tileState.p + size_t(pass) * tiles * 256,
+                                                        t.tileCounter.p + pass, &dCounters.p->status);
+            CK(cudaGetLastError());
+            std::swap(ki, ko);
+            std::swap(vi, vo);
+        }
+        k_lbvh_build<<<gridFor(n), 256, 0, s>>>(t.keys.p, t.vals.p, int(n), caabb.p, t.child.p, t.range.p,
+                                                 t.parent.p, t.leafParent.p, t.leafAabb.p, t.visit.p);
+        CK(cudaGetLastError());
+        if (n > 1) {
+            k_lbvh_refit<<<gridFor(n), 256, 0, s>>>(int(n), t.child.p, t.parent.p, t.leafParent.p, t.leafAabb.p,
+                                                     t.nodeAabb.p, t.visit.p);
+            CK(cudaGetLastError());
+        }
+    }
+
+    void phaseBroad()
+    {
+        const cudaStream_t s = stream;
+        buildTree(dynTree, dynCol.p, nDynCol);
+        if (otherDirty) {
+            buildTree(otherTree, otherCol.p, nOther);
+            otherDirty = false;
+        }
+        otherTree.n = int(nOther);
+        uint32_t* total = &dCounters.p->pairs;
+        if (nDynCol == 0) {
+            CK(cudaMemsetAsync(total, 0, sizeof(uint32_t), s));
+            return;
+        }
+        k_query_count<<<gridFor(nDynCol, 128), 128, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qCounts.p,
+                                                            &dCounters.p->status);
+        CK(cudaGetLastError());
+        scanner.run(qCounts.p, qOffsets.p, nDynCol, total, s);
+        k_query_write<<<gridFor(nDynCol, 128), 128, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qOffsets.p,
+                                                            pairs.p, pairCap, &dCounters.p->status);
+        CK(cudaGetLastError());
+    }
+
+    void phaseNarrow()
+    {
+        const cudaStream_t s = stream;
+        const uint32_t* nPairs = &dCounters.p->pairs;
+        const uint32_t g = gridFor(pairCap);
+        k_narrow<<<g, 256, 0, s>>>(view(), pairs.p, nPairs, pairCap, slots.p, hit.p);
+        CK(cudaGetLastError());
+        // The scan length must be host-known: scan the whole capacity (hit flags beyond the count are stale but the
+        // compaction kernel ignores them).
+        scanner.run(hit.p, hitOffsets.p, pairCap, nullptr, s);
+        k_compact_manifolds<<<g, 256, 0, s>>>(slots.p, hit.p, hitOffsets.p, nPairs, pairCap, manifolds.p,
+                                               manifoldCap, nManifolds.p, dCounters.p);
+        CK(cudaGetLastError());
+        // Warm start from the previous step's manifolds.
+        CK(cudaMemsetAsync(hashKeys.p, 0xFF, size_t(hashCap) * sizeof(unsigned long long), s));
+        k_warm_insert<<<gridFor(manifoldCap), 256, 0, s>>>(prevManifolds.p, nPrev.p, hashKeys.p, hashVals.p, hashCap,
+                                                           &dCounters.p->status);
+        k_warm_lookup<<<gridFor(manifoldCap), 256, 0, s>>>(prevManifolds.p, manifolds.p, nManifolds.p, hashKeys.p,
+                                                           hashVals.p, hashCap, dCounters.p);
+        CK(cudaGetLastError());
+    }
+
+    void phaseWake()
+    {
+        const cudaStream_t s = stream;
+        CK(cudaMemsetAsync(wakeIsland.p, 0, sizeof(uint32_t) * std::max<uint32_t>(nBodies, 1), s));
+        k_wake<<<gridFor(manifoldCap), 256, 0, s>>>(view(), manifolds.p, nManifolds.p, wakeIsland.p, dCounters.p);
+        k_wake_apply<<<gridFor(nBodies), 256, 0, s>>>(view(), wakeIsland.p, dCounters.p);
+        CK(cudaGetLastError());
+    }
+
+    void phaseSolve()
+    {
+        const cudaStream_t s = stream;
+        CK(cudaMemsetAsync(bodyMax.p, 0, sizeof(unsigned long long) * std::max<uint32_t>(nBodies, 1), s));
+        CK(cudaMemsetAsync(bar.p, 0, 2 * sizeof(uint32_t), s));
+        const uint32_t est = std::min<uint32_t>(manifoldCap, lastManifolds + lastManifolds / 2 + 1024);
+        DeviceWorld w = view();
+        const Manifold* mc = manifolds.p;
+        const uint32_t* nm = nManifolds.p;
+        uint32_t* colorp = color.p;
+        unsigned long long* bmax = bodyMax.p;
+        uint32_t *ccount = colorCount.p, *cstart = colorStart.p, *ord = order.p, *barp = bar.p;
+        StepCounters* ctr = dCounters.p;
+        {
+            const int grid = std::max(1, std::min<int>(dev.coopColorBlocks, int(div_up(est, 256))));
+            void* args[] = {&w, &mc, &nm, &colorp, &bmax, &ccount, &cstart, &ord, &barp, &ctr};
+            CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_color), dim3(grid), dim3(256), args, 0, s));
+        }
+        CK(cudaMemsetAsync(bar.p, 0, 2 * sizeof(uint32_t), s));
+        {
+            Manifold* mm = manifolds.p;
+            Constraint* cp = cons.p;
+            uint32_t vi = settings.velocity_iterations, pi = settings.position_iterations;
+            const int grid = std::max(1, std::min<int>(dev.coopSolveBlocks, int(div_up(est, 256))));
+            void* args[] = {&w, &mm, &nm, &ord, &cstart, &cp, &vi, &pi, &barp, &ctr};
+            CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve), dim3(grid), dim3(256), args, 0, s));
+        }
+    }
+
+    void phaseIslands()
+    {
+        const cudaStream_t s = stream;
+        const DeviceWorld w = view();
+        k_island_init<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p);
+        k_island_union<<<gridFor(manifoldCap), 256, 0, s>>>(w, manifolds.p, nManifolds.p, ufParent.p);
+        k_island_quiet<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p, settings.dt, settings.sleep_speed,
+                                                        settings.sleep_time);
+        k_island_sleep<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p, dCounters.p);
+        CK(cudaGetLastError());
+    }
+
+    void readCounters()
+    {
+        CK(cudaMemcpyAsync(hCounters, dCounters.p, sizeof(StepCounters), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    // One fixed step (Simulation::physicsStep order, Simulation.cpp:255-351).
+    void stepOnce()
+    {
+        ensureUploaded();
+        for (int attempt = 0; attempt < 8; attempt++) {
+            if (listsDirty) rebuildLists();
+            const cudaStream_t s = stream;
+            CK(cudaMemsetAsync(dCounters.p, 0, sizeof(StepCounters), s));
+            snapshot(false);
+            const bool fullPoseThisStep = fullPose;
+            const bool otherDirtyThisStep = otherDirty;
+            CK(cudaMemsetAsync(wrapCount.p, 0, sizeof(float) * std::max<uint32_t>(nBodies, 1), s));   // preUpdate
+            phaseIntegrate();
+            phasePose(fullPose);
+            phaseBroad();
+            phaseNarrow();
+            phaseWake();
+            phaseSolve();
+            phaseIslands();
+            readCounters();
+            const uint32_t st = hCounters->status;
+            if (st & (STATUS_PAIR_OVERFLOW | STATUS_MANIFOLD_OVERFLOW)) {
+                snapshot(true);
+                fullPose = fullPoseThisStep;
+                otherDirty = true;
+                (void)otherDirtyThisStep;
+                const uint64_t needP = std::max<uint64_t>(hCounters->pairs, pairCap) * 2;
+                const uint64_t needM = std::max<uint64_t>(hCounters->manifolds, manifoldCap) * 2;
+                if (needP > (1ull << 30)) throw ApiError(AG2D_ERR_CAPACITY, "pair buffer would exceed 2^30 entries");
+                reserveCapacities(uint32_t(needP), uint32_t(std::min<uint64_t>(needM, needP)));
+                CK(cudaStreamSynchronize(s));
+                continue;
+            }
+            if (st & (STATUS_BARRIER_TIMEOUT | STATUS_LOOKBACK_TIMEOUT)) {
+                snapshot(true);
+                CK(cudaStreamSynchronize(s));
+                throw ApiError(AG2D_ERR_TIMEOUT, "a bounded device-side wait timed out (status " + std::to_string(st) + ")");
+            }
+            if (st & (STATUS_COLOR_OVERFLOW | STATUS_HASH_FULL | STATUS_STACK_OVERFLOW)) {
+                snapshot(true);
+                CK(cudaStreamSynchronize(s));
+                throw ApiError(AG2D_ERR_CAPACITY, "capacity limit (colours, hash or traversal stack), status " + std::to_string(st));
+            }
+            fullPose = false;
+            // The solved manifolds become the next step's warm-start source.
+            swap_bufs(manifolds, prevManifolds);
+            CK(cudaMemcpyAsync(nPrev.p, nManifolds.p, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+            lastManifolds = hCounters->manifolds;
+            if (hCounters->topoDirty) {
+                // Woken or slept bodies: refresh the poses of every collider at the post-step state (the reference
+                // rebuilds its spatial data in postUpdate, Simulation.cpp:640-647), then the work lists and the
+                // static + sleeping tree before the next step.
+                listsDirty = true;
+                otherDirty = true;
+                phasePose(true);
+                rebuildLists();
+            }
+            // Grow ahead of need.
+            if (hCounters->pairs > pairCap / 2 || hCounters->manifolds > manifoldCap / 2) {
+                reserveCapacities(std::max<uint32_t>(pairCap, hCounters->pairs * 2),
+                                  std::max<uint32_t>(manifoldCap, hCounters->manifolds * 2));
+            }
+            stepsTaken++;
+            return;
+        }
+        throw ApiError(AG2D_ERR_CAPACITY, "step kept overflowing its buffers");
+    }
+};
+
+// ---------------------------------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------------------------------
+extern "C" {
+
+const char* ag2d_last_error_string(void) { return g_error.c_str(); }
+
+int32_t ag2d_version(void) { return 1; }
+
+int32_t ag2d_device_count(int32_t* out_count)
+{
+    return guarded([&] {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+        if (out_count) *out_count = n;
+    });
+}
+
+int32_t ag2d_world_create(const ag2d_world_settings* settings, ag2d_world** out_world)
+{
+    return guarded([&] {
+        if (!settings || !out_world) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        if (!(settings->dt > 0.0f)) throw ApiError(AG2D_ERR_INVALID_ARG, "dt must be > 0");
+        if (settings->ccd) throw ApiError(AG2D_ERR_UNSUPPORTED, "continuous collision detection is not available");
+        std::unique_ptr<ag2d_world> w(new ag2d_world());
+        w->init(*settings);
+        *out_world = w.release();
+    });
+}
+
+int32_t ag2d_world_destroy(ag2d_world* world)
+{
+    return guarded([&] {
+        if (world) cudaSetDevice(world->settings.device);
+        delete world;
+    });
+}
+
+int32_t ag2d_world_add_material(ag2d_world* world, float e, float sf, float df, uint32_t* out_index)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        const uint32_t idx = world->objects.addMaterial(e, sf, df);
+        if (out_index) *out_index = idx;
+        world->hostDirty = true;
+    });
+}
+
+static void body_desc(const ag2d_body_desc* b, float* d)
+{
+    d[0] = b->x; d[1] = b->y; d[2] = b->rotation; d[3] = b->vx; d[4] = b->vy; d[5] = b->angular_velocity;
+    d[6] = b->mass;
+}
+
+// Creation after the first step pulls the live device state back so new bodies join the running world.
+static void pull_state(ag2d_world* w);
+
+int32_t ag2d_world_add_circle(ag2d_world* world, const ag2d_body_desc* body, float radius, uint64_t* out_handle)
+{
+    return guarded([&] {
+        if (!world || !body) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        pull_state(world);
+        float d[7];
+        body_desc(body, d);
+        uint64_t h = 0;
+        std::string err;
+        if (!world->objects.addCircle(d, body->material, radius, h, err)) throw ApiError(AG2D_ERR_INVALID_ARG, err);
+        world->hostDirty = true;
+        if (out_handle) *out_handle = h;
+    });
+}
+
+int32_t ag2d_world_add_box(ag2d_world* world, const ag2d_body_desc* body, float width, float height,
+                           uint64_t* out_handle)
+{
+    return guarded([&] {
+        if (!world || !body) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        pull_state(world);
+        float d[7];
+        body_desc(body, d);
+        uint64_t h = 0;
+        std::string err;
+        if (!world->objects.addBox(d, body->material, width, height, h, err)) throw ApiError(AG2D_ERR_INVALID_ARG, err);
+        world->hostDirty = true;
+        if (out_handle) *out_handle = h;
+    });
+}
+
+int32_t ag2d_world_add_polygon(ag2d_world* world, const ag2d_body_desc* body, const float* xy, uint32_t n,
+                               uint64_t* out_handle)
+{
+    return guarded([&] {
+        if (!world || !body) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        pull_state(world);
+        float d[7];
+        body_desc(body, d);
+        uint64_t h = 0;
+        std::string err;
+        if (!world->objects.addPolygon(d, body->material, xy, n, h, err)) {
+            throw ApiError(err.find("not convex") != std::string::npos || err.find("16") != std::string::npos
+                               ? AG2D_ERR_UNSUPPORTED : AG2D_ERR_INVALID_ARG, err);
+        }
+        world->hostDirty = true;
+        if (out_handle) *out_handle = h;
+    });
+}
+
+uint32_t ag2d_world_body_index(ag2d_world* world, uint64_t handle)
+{
+    return world ? world->objects.indexOf(handle) : 0xFFFFFFFFu;
+}
+
+int32_t ag2d_world_load_state(ag2d_world* world, const ag2d_state_desc* st)
+{
+    return guarded([&] {
+        if (!world || !st) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        ag2d_world& w = *world;
+        const uint32_t nb = st->n_bodies, nc = st->n_colliders;
+        w.nBodies = nb;
+        w.nColliders = nc;
+        std::vector<float4> vel(nb), pos(nb);
+        std::vector<float2> rot(nb);
+        std::vector<float> wc(nb), br(nb), tm(nb);
+        std::vector<uint8_t> state(nb);
+        std::vector<uint32_t> isl(nb);
+        for (uint32_t i = 0; i < nb; i++) {
+            vel[i] = make_float4(st->vel_x[i], st->vel_y[i], st->angular_velocity[i], st->inv_mass[i]);
+            pos[i] = make_float4(st->com_x[i], st->com_y[i], st->rotation[i], st->inv_inertia[i]);
+            rot[i] = make_float2(st->rot_cos[i], st->rot_sin[i]);
+            wc[i] = st->wrap_count ? st->wrap_count[i] : 0.0f;
+            br[i] = st->bound_radius ? st->bound_radius[i] : 0.0f;
+            tm[i] = st->sleep_timer ? st->sleep_timer[i] : 0.0f;
+            const uint32_t* g = st->body_group_starts;
+            state[i] = uint8_t(i < g[1] ? STATE_STATIC : (i < g[2] ? STATE_SLEEPING : STATE_DYNAMIC));
+            isl[i] = st->sleep_island ? st->sleep_island[i] : 0xFFFFFFFFu;
+        }
+        // Sleeping islands are identified by their smallest member body index on the device (the union-find root
+        // convention); the reference numbers them from 2 (FIRST_SLEEP_ISLAND_ID, SoA/BodySoA.h:45).
+        {
+            std::vector<std::pair<uint32_t, uint32_t>> ids;   // (reference id, first member)
+            for (uint32_t i = 0; i < nb; i++) {
+                if (state[i] != STATE_SLEEPING) { isl[i] = 0xFFFFFFFFu; continue; }
+                auto it = std::find_if(ids.begin(), ids.end(), [&](const auto& p) { return p.first == isl[i]; });
+                if (it == ids.end()) { ids.emplace_back(isl[i], i); isl[i] = i; }
+                else isl[i] = it->second;
+            }
+        }
+        std::vector<uint32_t> cb(nc), cs(nc), cm(nc);
+        std::vector<float4> co(nc);
+        for (uint32_t i = 0; i < nc; i++) {
+            cb[i] = st->col_body[i];
+            cs[i] = (st->col_shape_type[i] << 30) | st->col_shape_index[i];
+            cm[i] = st->col_material[i];
+            co[i] = make_float4(st->col_com_offset_x[i], st->col_com_offset_y[i], st->col_local_rotation[i], 0.0f);
+        }
+        std::vector<float> cr(st->circle_radius, st->circle_radius + st->n_circles);
+        std::vector<float2> bh(st->n_boxes);
+        for (uint32_t i = 0; i < st->n_boxes; i++) bh[i] = make_float2(st->box_half_width[i], st->box_half_height[i]);
+        std::vector<uint32_t> po(st->n_polygons), pc(st->n_polygons);
+        uint32_t total = 0;
+        for (uint32_t i = 0; i < st->n_polygons; i++) { po[i] = total; pc[i] = st->poly_count[i]; total += pc[i]; }
+        std::vector<float2> pv(total), pn(total);
+        for (uint32_t k = 0; k < total; k++) {
+            pv[k] = make_float2(st->poly_vertices[2 * k], st->poly_vertices[2 * k + 1]);
+            pn[k] = make_float2(st->poly_normals[2 * k], st->poly_normals[2 * k + 1]);
+        }
+        std::vector<float4> mats(st->n_materials);
+        w.objects.materials.assign(st->materials, st->materials + 3 * st->n_materials);
+        for (uint32_t i = 0; i < st->n_materials; i++)
+            mats[i] = make_float4(st->materials[3 * i], st->materials[3 * i + 1], st->materials[3 * i + 2], 0.0f);
+        w.uploadArrays(vel, pos, rot, wc, br, tm, state, isl, cb, cs, cm, co, cr, bh, po, pc, pv, pn, mats);
+        // The loaded state replaces any host-created objects.
+        w.objects.bodies.clear();
+        w.objects.colliders.clear();
+        w.hostDirty = false;
+    });
+}
+
+int32_t ag2d_world_step(ag2d_world* world, int32_t steps)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        if (steps < 0) throw ApiError(AG2D_ERR_INVALID_ARG, "steps must be >= 0");
+        CK(cudaSetDevice(world->settings.device));
+        for (int32_t i = 0; i < steps; i++) world->stepOnce();
+    });
+}
+
+int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out)
+{
+    return guarded([&] {
+        if (!world || !out) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        const StepCounters& c = *world->hCounters;
+        out->status = c.status; out->pairs = c.pairs; out->manifolds = c.manifolds; out->colors = c.colors;
+        out->woke = c.woke; out->slept = c.slept; out->warm_hits = c.warmHits;
+        out->sleeping = world->nBodies - world->nDynBody - world->nStatic;
+        out->steps = world->stepsTaken;
+    });
+}
+
+int32_t ag2d_world_body_count(ag2d_world* world, uint32_t* out_bodies, uint32_t* out_colliders)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        const bool host = world->hostDirty;
+        if (out_bodies) *out_bodies = host ? uint32_t(world->objects.bodies.size()) : world->nBodies;
+        if (out_colliders) *out_colliders = host ? uint32_t(world->objects.colliders.size()) : world->nColliders;
+    });
+}
+
+}  // extern "C"
+
+// Field access ---------------------------------------------------------------------------------------------------
+
+template <class T>
+static std::vector<T> download(const T* p, size_t n, cudaStream_t s)
+{
+    std::vector<T> v(n);
+    if (n) CK(cudaMemcpyAsync(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return v;
+}
+
+static std::vector<uint8_t> read_field(ag2d_world& w, int32_t field)
+{
+    const cudaStream_t s = w.stream;
+    auto pack = [](const auto& v) {
+        std::vector<uint8_t> out(v.size() * sizeof(v[0]));
+        if (!v.empty()) std::memcpy(out.data(), v.data(), out.size());
+        return out;
+    };
+    auto comp4 = [&](const DBuf<float4>& b, uint32_t n, int c) {
+        const auto v = download(b.p, n, s);
+        std::vector<float> o(n);
+        for (uint32_t i = 0; i < n; i++) o[i] = c == 0 ? v[i].x : c == 1 ? v[i].y : c == 2 ? v[i].z : v[i].w;
+        return pack(o);
+    };
+    auto comp2 = [&](const DBuf<float2>& b, uint32_t n, int c) {
+        const auto v = download(b.p, n, s);
+        std::vector<float> o(n);
+        for (uint32_t i = 0; i < n; i++) o[i] = c == 0 ? v[i].x : v[i].y;
+        return pack(o);
+    };
+    const uint32_t nb = w.nBodies, nc = w.nColliders;
+    switch (field) {
+    case AG2D_BODY_COM_X: return comp4(w.bpos, nb, 0);
+    case AG2D_BODY_COM_Y: return comp4(w.bpos, nb, 1);
+    case AG2D_BODY_ROTATION: return comp4(w.bpos, nb, 2);
+    case AG2D_BODY_VEL_X: return comp4(w.bvel, nb, 0);
+    case AG2D_BODY_VEL_Y: return comp4(w.bvel, nb, 1);
+    case AG2D_BODY_ANGULAR_VELOCITY: return comp4(w.bvel, nb, 2);
+    case AG2D_BODY_ROT_COS: return comp2(w.brot, nb, 0);
+    case AG2D_BODY_ROT_SIN: return comp2(w.brot, nb, 1);
+    case AG2D_BODY_WRAP_COUNT: return pack(download(w.wrapCount.p, nb, s));
+    case AG2D_BODY_SLEEP_TIMER: return pack(download(w.sleepTimer.p, nb, s));
+    case AG2D_BODY_STATE: {
+        const auto v = download(w.bstate.p, nb, s);
+        std::vector<uint32_t> o(v.begin(), v.end());
+        return pack(o);
+    }
+    case AG2D_BODY_SLEEP_ISLAND: return pack(download(w.sleepIsland.p, nb, s));
+    case AG2D_COL_WORLD_X: return comp4(w.cpose, nc, 0);
+    case AG2D_COL_WORLD_Y: return comp4(w.cpose, nc, 1);
+    case AG2D_COL_WORLD_COS: return comp4(w.cpose, nc, 2);
+    case AG2D_COL_WORLD_SIN: return comp4(w.cpose, nc, 3);
+    case AG2D_COL_WORLD_ROTATION: return pack(download(w.cworldRot.p, nc, s));
+    case AG2D_COL_AABB_MIN_X: return comp4(w.caabb, nc, 0);
+    case AG2D_COL_AABB_MIN_Y: return comp4(w.caabb, nc, 1);
+    case AG2D_COL_AABB_MAX_X: return comp4(w.caabb, nc, 2);
+    case AG2D_COL_AABB_MAX_Y: return comp4(w.caabb, nc, 3);
+    case AG2D_DYN_SORTED: return pack(download(w.dynTree.vals.p, uint32_t(w.dynTree.n), s));
+    case AG2D_DYN_MORTON: return pack(download(w.dynTree.keys.p, uint32_t(w.dynTree.n), s));
+    case AG2D_PAIRS: {
+        uint32_t n = 0;
+        CK(cudaMemcpyAsync(&n, &w.dCounters.p->pairs, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return pack(download(w.pairs.p, std::min(n, w.pairCap), s));
+    }
+    case AG2D_MANIFOLDS:
+    case AG2D_PREV_MANIFOLDS: {
+        const bool prev = field == AG2D_PREV_MANIFOLDS;
+        uint32_t n = 0;
+        CK(cudaMemcpyAsync(&n, prev ? w.nPrev.p : w.nManifolds.p, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return pack(download(prev ? w.prevManifolds.p : w.manifolds.p, n, s));
+    }
+    case AG2D_SOLVE_ORDER: {
+        uint32_t n = 0;
+        CK(cudaMemcpyAsync(&n, w.nManifolds.p, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return pack(download(w.order.p, n, s));
+    }
+    case AG2D_COLOR_STARTS: {
+        StepCounters c;
+        CK(cudaMemcpyAsync(&c, w.dCounters.p, sizeof(c), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return pack(download(w.colorStart.p, c.colors + 1, s));
+    }
+    default: throw ApiError(AG2D_ERR_INVALID_ARG, "unknown field " + std::to_string(field));
+    }
+}
+
+extern "C" {
+
+int32_t ag2d_world_read(ag2d_world* world, int32_t field, void* dst, uint64_t cap, uint64_t* out_bytes)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        CK(cudaSetDevice(world->settings.device));
+        world->ensureUploaded();
+        const auto bytes = read_field(*world, field);
+        if (out_bytes) *out_bytes = bytes.size();
+        if (dst) {
+            if (cap < bytes.size()) throw ApiError(AG2D_ERR_INVALID_ARG, "destination too small");
+            if (!bytes.empty()) std::memcpy(dst, bytes.data(), bytes.size());
+        }
+    });
+}
+
+int32_t ag2d_world_write(ag2d_world* world, int32_t field, const void* src, uint64_t bytes)
+{
+    return guarded([&] {
+        if (!world || (!src && bytes)) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        ag2d_world& w = *world;
+        CK(cudaSetDevice(w.settings.device));
+        w.ensureUploaded();
+        const cudaStream_t s = w.stream;
+        auto set4 = [&](DBuf<float4>& b, int c) {
+            if (bytes != uint64_t(w.nBodies) * 4) throw ApiError(AG2D_ERR_INVALID_ARG, "size mismatch");
+            auto v = download(b.p, w.nBodies, s);
+            const float* f = static_cast<const float*>(src);
+            for (uint32_t i = 0; i < w.nBodies; i++) (c == 0 ? v[i].x : c == 1 ? v[i].y : c == 2 ? v[i].z : v[i].w) = f[i];
+            b.upload(v.data(), v.size(), s);
+        };
+        switch (field) {
+        case AG2D_BODY_COM_X: set4(w.bpos, 0); break;
+        case AG2D_BODY_COM_Y: set4(w.bpos, 1); break;
+        case AG2D_BODY_ROTATION: set4(w.bpos, 2); break;
+        case AG2D_BODY_VEL_X: set4(w.bvel, 0); break;
+        case AG2D_BODY_VEL_Y: set4(w.bvel, 1); break;
+        case AG2D_BODY_ANGULAR_VELOCITY: set4(w.bvel, 2); break;
+        case AG2D_PAIRS: {
+            const uint32_t n = uint32_t(bytes / sizeof(uint2));
+            if (n > w.pairCap) w.reserveCapacities(std::max(n, w.pairCap), std::max(n, w.manifoldCap));
+            w.pairs.reserve(std::max(n, w.pairCap));
+            if (n) CK(cudaMemcpyAsync(w.pairs.p, src, bytes, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(&w.dCounters.p->pairs, &n, 4, cudaMemcpyHostToDevice, s));
+            break;
+        }
+        case AG2D_MANIFOLDS:
+        case AG2D_PREV_MANIFOLDS: {
+            const uint32_t n = uint32_t(bytes / sizeof(Manifold));
+            if (n > w.manifoldCap) w.reserveCapacities(std::max(n, w.pairCap), n);
+            const bool prev = field == AG2D_PREV_MANIFOLDS;
+            if (n) CK(cudaMemcpyAsync(prev ? w.prevManifolds.p : w.manifolds.p, src, bytes, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(prev ? w.nPrev.p : w.nManifolds.p, &n, 4, cudaMemcpyHostToDevice, s));
+            break;
+        }
+        default: throw ApiError(AG2D_ERR_INVALID_ARG, "field is not writable");
+        }
+        CK(cudaStreamSynchronize(s));
+    });
+}
+
+int32_t ag2d_world_run_phase(ag2d_world* world, int32_t phase)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        ag2d_world& w = *world;
+        CK(cudaSetDevice(w.settings.device));
+        w.ensureUploaded();
+        if (w.listsDirty) w.rebuildLists();
+        switch (phase) {
+        case AG2D_PHASE_INTEGRATE:
+            CK(cudaMemsetAsync(w.wrapCount.p, 0, sizeof(float) * std::max<uint32_t>(w.nBodies, 1), w.stream));
+            w.phaseIntegrate();
+            break;
+        case AG2D_PHASE_SPATIAL_FULL: w.phasePose(true); break;
+        case AG2D_PHASE_SPATIAL_DYNAMIC: w.phasePose(false); break;
+        case AG2D_PHASE_BROAD:
+            CK(cudaMemsetAsync(w.dCounters.p, 0, sizeof(StepCounters), w.stream));
+            w.otherDirty = true;
+            w.phaseBroad();
+            break;
+        case AG2D_PHASE_NARROW: w.phaseNarrow(); break;
+        case AG2D_PHASE_SOLVE: w.phaseSolve(); break;
+        case AG2D_PHASE_ISLANDS: w.phaseIslands(); break;
+        default: throw ApiError(AG2D_ERR_INVALID_ARG, "unknown phase");
+        }
+        w.readCounters();
+        if (w.hCounters->status & (STATUS_BARRIER_TIMEOUT | STATUS_LOOKBACK_TIMEOUT))
+            throw ApiError(AG2D_ERR_TIMEOUT, "a bounded device-side wait timed out");
+        if (w.hCounters->status) throw ApiError(AG2D_ERR_CAPACITY, "phase status " + std::to_string(w.hCounters->status));
+    });
+}
+
+}  // extern "C"
+
+// Batches: the worlds step one after another here; the fused per-world-CTA path replaces this.
+struct ag2d_batch {
+    std::vector<ag2d_world*> worlds;
+};
+
+extern "C" {
+
+int32_t ag2d_batch_create(ag2d_world* const* worlds, uint32_t count, ag2d_batch** out)
+{
+    return guarded([&] {
+        if (!out || (!worlds && count)) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        std::unique_ptr<ag2d_batch> b(new ag2d_batch());
+        b->worlds.assign(worlds, worlds + count);
+        *out = b.release();
+    });
+}
+
+int32_t ag2d_batch_step(ag2d_batch* batch, int32_t steps)
+{
+    return guarded([&] {
+        if (!batch) throw ApiError(AG2D_ERR_INVALID_ARG, "null batch");
+        for (int32_t i = 0; i < steps; i++)
+            for (ag2d_world* w : batch->worlds) {
+                CK(cudaSetDevice(w->settings.device));
+                w->stepOnce();
+            }
+    });
+}
+
+int32_t ag2d_batch_destroy(ag2d_batch* batch)
+{
+    return guarded([&] { delete batch; });
+}
+
+}  // extern "C"
+
+static void pull_state(ag2d_world* w)
+{
+    // Bodies created after the world has run: bring the simulated state back into the host objects first.
+    if (w->hostDirty || w->objects.bodies.empty() || w->nBodies != w->objects.bodies.size()) return;
+    const cudaStream_t s = w->stream;
+    const auto vel = download(w->bvel.p, w->nBodies, s);
+    const auto pos = download(w->bpos.p, w->nBodies, s);
+    const auto rot = download(w->brot.p, w->nBodies, s);
+    const auto tm = download(w->sleepTimer.p, w->nBodies, s);
+    for (uint32_t i = 0; i < w->nBodies; i++) {
+        HBody& b = w->objects.bodies[i];
+        b.vx = vel[i].x; b.vy = vel[i].y; b.w = vel[i].z;
+        b.comX = pos[i].x; b.comY = pos[i].y; b.rot = pos[i].z;
+        b.cos = rot[i].x; b.sin = rot[i].y; b.sleepTimer = tm[i];
+    }
+}

@@ -1,0 +1,109 @@
+// Host-side object bookkeeping: body/collider/shape creation with the reference's geometry and dense ordering.
+//
+// Creation is host work in the reference too (ObjectManager, PhysicsGeometry). What matters for parity is
+// reproduced exactly: mass/inertia/centre-of-mass arithmetic (SimulationImpl/PhysicsGeometry.cpp:116-187),
+// polygon outline cleaning for convex input (:275-347) and recentring (ObjectManager.cpp:286-349, 535-562), the
+// bound radius (ObjectManager.cpp:24-43, 1103-1108), and the dense order that group moves produce
+// (moveBodyToGroup, ObjectManager.cpp:1232-1267): a new static body takes the first slot after the static group
+// and pushes the first body of each later group to that group's end. Paths are relative to
+// PhysicsSimulation-Agony/PS_AGONY2D/.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace ag2d {
+
+struct HBody {
+    float comX = 0, comY = 0, vx = 0, vy = 0, rot = 0, w = 0;
+    float mass = 0, invMass = 0, inertia = 0, invInertia = 0;
+    float lcomX = 0, lcomY = 0;
+    float cos = 1, sin = 0;
+    float boundRadius = 0;
+    float wrapCount = 0, sleepTimer = 0;
+    uint32_t sleepIsland = 0xFFFFFFFFu;
+    uint32_t handleSlot = 0;
+    std::vector<uint32_t> colliders;
+};
+
+struct HCollider {
+    uint32_t body = 0;
+    float locX = 0, locY = 0, comOffX = 0, comOffY = 0, localRot = 0;
+    uint32_t material = 0;
+    uint32_t type = 0, shape = 0;
+    float minExtent = 0, maxExtent = 0;
+};
+
+struct HPolygon {
+    std::vector<float> verts;     // xy pairs, collider-local, centred on the piece centroid
+    std::vector<float> normals;   // xy pairs, outward unit edge normals (0 for degenerate edges)
+};
+
+// Group ranges: [starts[g], starts[g + 1]) for static (0), sleeping (1), dynamic (2); starts[3] = live count.
+struct Groups {
+    uint32_t starts[4] = {0, 0, 0, 0};
+    uint32_t groupOf(uint32_t i) const
+    {
+        for (uint32_t g = 0; g < 3; g++) if (i < starts[g + 1]) return g;
+        return 3;
+    }
+};
+
+class HostObjects {
+public:
+    std::vector<HBody> bodies;
+    std::vector<HCollider> colliders;
+    std::vector<float> circleRadius;
+    std::vector<float> boxHalfW, boxHalfH;
+    std::vector<HPolygon> polygons;
+    std::vector<float> materials;   // 3 per material
+    Groups bodyGroups, colGroups;
+    // Handle table: slot -> dense index (generation kept beside it).
+    std::vector<uint32_t> slotIndex, slotGeneration;
+
+    HostObjects() { materials = {1.0f, 0.0f, 0.0f}; }   // MaterialManager: material 0 = default
+
+    uint32_t addMaterial(float e, float sf, float df)
+    {
+        // MaterialManager::sanitize (SimulationImpl/MaterialManager.h:29-35).
+        e = std::fmin(std::fmax(e, 0.0f), 1.0f);
+        sf = std::fmax(sf, 0.0f);
+        df = std::fmax(df, 0.0f);
+        materials.push_back(e); materials.push_back(sf); materials.push_back(df);
+        return uint32_t(materials.size() / 3 - 1);
+    }
+    uint32_t materialCount() const { return uint32_t(materials.size() / 3); }
+
+    // Returns the handle ((generation << 32) | slot) or sets err.
+    bool addCircle(const float* desc /* x,y,rot,vx,vy,w,mass */, uint32_t material, float radius, uint64_t& handle,
+                   std::string& err);
+    bool addBox(const float* desc, uint32_t material, float width, float height, uint64_t& handle, std::string& err);
+    bool addPolygon(const float* desc, uint32_t material, const float* xy, uint32_t n, uint64_t& handle,
+                    std::string& err);
+
+    uint32_t indexOf(uint64_t handle) const
+    {
+        const uint32_t slot = uint32_t(handle & 0xFFFFFFFFu), gen = uint32_t(handle >> 32);
+        if (slot >= slotIndex.size() || slotGeneration[slot] != gen) return 0xFFFFFFFFu;
+        return slotIndex[slot];
+    }
+
+private:
+    uint32_t appendBody(float px, float py, float vx, float vy, float rot, float w, float mass, float invMass,
+                        float inertia, float invInertia, float lcomX, float lcomY);
+    uint32_t appendCollider(uint32_t body, float locX, float locY, float localRot, uint32_t material, uint32_t type,
+                            uint32_t shape, float minExt, float maxExt);
+    void swapBodies(uint32_t a, uint32_t b);
+    void swapColliders(uint32_t a, uint32_t b);
+    uint32_t moveBodyDown(uint32_t index, uint32_t target);
+    uint32_t moveColliderDown(uint32_t index, uint32_t target);
+};
+
+// PhysicsGeometry::calculatePolygonInertia (PhysicsGeometry.cpp:130-187) without a requested pivot.
+// Returns false for a degenerate (or clockwise) outline.
+bool polygon_inertia(float mass, const std::vector<float>& xy, float& inertia, float& cx, float& cy);
+
+}  // namespace ag2d

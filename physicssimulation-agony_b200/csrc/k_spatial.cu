@@ -1,0 +1,562 @@
+// Spatial phase kernels: integration, collider poses + AABBs, Morton keys, onesweep radix sort, Karras LBVH build
+// and refit, and the candidate-pair query. Reference routines cited per kernel (paths relative to
+// PhysicsSimulation-Agony/PS_AGONY2D/).
+#include "ag2d_kernels.cuh"
+
+namespace ag2d {
+
+// ---------------------------------------------------------------------------------------------------------------
+// Integration: Integrator::integratePhase1/2_VelocityVerlet + dampAngularVelocities (Integration/Integrator.cpp:
+// 140-299, call order Simulation.cpp:392-407), wrapBodyRotations (LeftOutFunctions.cpp:13-60) and
+// computeRotationCosSin (Integrator.cpp:301-311), fused per dynamic body. Elementwise: HBM-bound at 40 B/body.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_integrate(DeviceWorld w, const uint32_t* __restrict__ dynBody, uint32_t nDyn, float dt, float gx,
+                            float gy, float dampHalf /* damping^(dt/2), or >= 1 when damping is off */)
+{
+    const uint32_t simdEnd = nDyn & ~7u;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nDyn; k += gridDim.x * blockDim.x) {
+        const uint32_t b = dynBody[k];
+        const bool simd = k < simdEnd;
+        float4 v = w.bvel[b];
+        float4 p = w.bpos[b];
+        const float halfDT = dt * 0.5f;
+        const float gdx = gx * halfDT, gdy = gy * halfDT;
+        const bool movable = v.w != 0.0f;
+        const bool angMovable = p.w != 0.0f;
+        if (simd) { v.x += movable ? gdx : 0.0f; v.y += movable ? gdy : 0.0f; }
+        else { v.x += gdx * float(movable); v.y += gdy * float(movable); }
+        if (dampHalf < 1.0f) {
+            const float nv = v.z * dampHalf;
+            if (simd) v.z = angMovable ? nv : v.z;
+            else { const float m = float(angMovable); v.z = m * nv + (1.0f - m) * v.z; }
+        }
+        p.x = v.x * dt + p.x;
+        p.y = v.y * dt + p.y;
+        p.z = v.z * dt + p.z;
+        if (simd) { v.x += movable ? gdx : 0.0f; v.y += movable ? gdy : 0.0f; }
+        else { v.x += gdx * float(movable); v.y += gdy * float(movable); }
+        if (dampHalf < 1.0f) {
+            const float nv = v.z * dampHalf;
+            if (simd) v.z = angMovable ? nv : v.z;
+            else { const float m = float(angMovable); v.z = m * nv + (1.0f - m) * v.z; }
+        }
+        float wraps;
+        p.z = wrap_angle(p.z, simd, wraps);
+        w.wrapCount[b] = w.wrapCount[b] + wraps;
+        float c, s;
+        fast_cos_sin(p.z, simd, c, s);
+        w.bvel[b] = v;
+        w.bpos[b] = p;
+        w.brot[b] = make_float2(c, s);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Collider world pose and AABB: computeColliderWorldPositions/Rotations (Simulation.cpp:673-736) and the shape
+// AABB builders (SimulationImpl/ColliderAABBBuilder.cpp:8-136). 'list' selects the colliders (null = all, in index
+// order); the k-th collider of the pass takes the reference's SIMD path iff k < (n & ~7).
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ float4 collider_aabb(const DeviceWorld& w, uint32_t c, float x, float y, float cs, float sn)
+{
+    const uint32_t packed = w.cshape[c];
+    const uint32_t si = shape_index(packed);
+    switch (shape_type(packed)) {
+    case SHAPE_CIRCLE: {
+        const float r = w.circleRadius[si];
+        return make_float4(x - r, y - r, x + r, y + r);
+    }
+    case SHAPE_BOX: {
+        const float2 h = w.boxHalf[si];
+        const float ac = fabsf(cs), as = fabsf(sn);
+        const float ex = ac * h.x + as * h.y;
+        const float ey = as * h.x + ac * h.y;
+        return make_float4(x - ex, y - ey, x + ex, y + ey);
+    }
+    default: {
+        const uint32_t off = w.polyOffset[si], nv = w.polyCount[si];
+        float mnx = FLT_MAX, mny = FLT_MAX, mxx = -FLT_MAX, mxy = -FLT_MAX;
+        for (uint32_t k = 0; k < nv; k++) {
+            const float2 v = w.polyVerts[off + k];
+            const float wx = cs * v.x - sn * v.y;
+            const float wy = sn * v.x + cs * v.y;
+            mnx = rfminf(mnx, wx); mxx = rfmaxf(mxx, wx);
+            mny = rfminf(mny, wy); mxy = rfmaxf(mxy, wy);
+        }
+        return make_float4(x + mnx, y + mny, x + mxx, y + mxy);
+    }
+    }
+}
+
+__global__ void k_collider_pose(DeviceWorld w, const uint32_t* __restrict__ list, uint32_t n)
+{
+    const uint32_t simdEnd = n & ~7u;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t c = list ? list[k] : k;
+        const bool simd = k < simdEnd;
+        const uint32_t b = w.cbody[c];
+        const float4 off = w.coff[c];
+        const float4 bp = w.bpos[b];
+        const float2 br = w.brot[b];
+        const float x = bp.x + (off.x * br.x - off.y * br.y);
+        const float y = bp.y + (off.x * br.y + off.y * br.x);
+        float wraps;
+        const float rot = wrap_angle(bp.z + off.z, simd, wraps);
+        float cs, sn;
+        fast_cos_sin(rot, simd, cs, sn);
+        w.cpose[c] = make_float4(x, y, cs, sn);
+        w.cworldRot[c] = rot;
+        w.caabb[c] = collider_aabb(w, c, x, y, cs, sn);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Tree bounds: the union of the AABBs of one tree's colliders (BvhTree::gatherCentroids, BvhTree.cpp:148-188).
+// min/max are order-independent, so a block reduction plus ordered-integer atomics gives the sequential result
+// (up to the sign of a zero bound).
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_bounds(const float4* __restrict__ aabb, const uint32_t* __restrict__ list, uint32_t n,
+                         uint32_t* __restrict__ bounds /* ordered: minX, minY, maxX, maxY */)
+{
+    float mnx = FLT_MAX, mny = FLT_MAX, mxx = -FLT_MAX, mxy = -FLT_MAX;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 a = aabb[list ? list[k] : k];
+        mnx = fminf(mnx, a.x); mny = fminf(mny, a.y); mxx = fmaxf(mxx, a.z); mxy = fmaxf(mxy, a.w);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+        mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+        mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+        mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(bounds + 0, float_to_ordered(mnx));
+        atomicMin(bounds + 1, float_to_ordered(mny));
+        atomicMax(bounds + 2, float_to_ordered(mxx));
+        atomicMax(bounds + 3, float_to_ordered(mxy));
+    }
+}
+
+__global__ void k_bounds_init(uint32_t* bounds)
+{
+    if (threadIdx.x == 0) {
+        bounds[0] = float_to_ordered(FLT_MAX);
+        bounds[1] = float_to_ordered(FLT_MAX);
+        bounds[2] = float_to_ordered(-FLT_MAX);
+        bounds[3] = float_to_ordered(-FLT_MAX);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Morton keys: transformCentroids + computeMortonCodes (BvhTree.cpp:191-280). 2 x centroid scaled into [0, 65535]
+// per axis by the tree bounds, truncated, bits interleaved (y in the odd bits): a 32-bit key.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_morton(const float4* __restrict__ aabb, const uint32_t* __restrict__ list, uint32_t n,
+                         const uint32_t* __restrict__ bounds, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals)
+{
+    const float bminX = ordered_to_float(bounds[0]), bminY = ordered_to_float(bounds[1]);
+    const float bmaxX = ordered_to_float(bounds[2]), bmaxY = ordered_to_float(bounds[3]);
+    const float kEps = 1e-5f;
+    const float maxX = rfmaxf(bmaxX, bminX + kEps);
+    const float maxY = rfmaxf(bmaxY, bminY + kEps);
+    const float clampMax = 65535.0f;
+    const float scaleX = clampMax / (maxX - bminX);
+    const float scaleY = clampMax / (maxY - bminY);
+    const float negScaledMinX = -bminX * scaleX;
+    const float negScaledMinY = -bminY * scaleY;
+    const float halfScaleX = scaleX * 0.5f;
+    const float halfScaleY = scaleY * 0.5f;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t c = list ? list[k] : k;
+        const float4 a = aabb[c];
+        const float cx = a.x + a.z;
+        const float cy = a.y + a.w;
+        float tx = cx * halfScaleX + negScaledMinX;
+        float ty = cy * halfScaleY + negScaledMinY;
+        tx = tx < 0.0f ? 0.0f : (tx > clampMax ? clampMax : tx);
+        ty = ty < 0.0f ? 0.0f : (ty > clampMax ? clampMax : ty);
+        keys[k] = (part1by1(uint32_t(ty)) << 1) | part1by1(uint32_t(tx));
+        vals[k] = c;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Onesweep LSD radix sort of (key, value) pairs, 8-bit digits, stable: the same permutation as
+// BvhTree::sortByMortonCodes (BvhTree.cpp:282-354). One histogram pass for all four digits, then per digit one
+// kernel that ranks a 4096-key tile (warp match-any ranking, striped so ranks follow input order), resolves the
+// tile's global digit offsets by decoupled look-back over the preceding tiles, reorders the tile in shared
+// memory and writes each digit's run contiguously.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_sort_histogram(const uint32_t* __restrict__ keys, uint32_t n, uint32_t* __restrict__ hist)
+{
+    __shared__ uint32_t sh[4 * 256];
+    for (uint32_t i = threadIdx.x; i < 4 * 256; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k = keys[i];
+        atomicAdd(&sh[0 * 256 + (k & 0xFF)], 1u);
+        atomicAdd(&sh[1 * 256 + ((k >> 8) & 0xFF)], 1u);
+        atomicAdd(&sh[2 * 256 + ((k >> 16) & 0xFF)], 1u);
+        atomicAdd(&sh[3 * 256 + (k >> 24)], 1u);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < 4 * 256; i += blockDim.x)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+// In-place exclusive scan of each 256-bin digit histogram; launched with 4 blocks of 256 threads.
+__global__ void k_sort_digit_scan(uint32_t* hist)
+{
+    __shared__ uint32_t s[256];
+    uint32_t* h = hist + blockIdx.x * 256;
+    const uint32_t t = threadIdx.x;
+    s[t] = h[t];
+    __syncthreads();
+    for (uint32_t o = 1; o < 256; o <<= 1) {
+        const uint32_t v = t >= o ? s[t - o] : 0u;
+        __syncthreads();
+        s[t] += v;
+        __syncthreads();
+    }
+    h[t] = s[t] - h[t];
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_pass(
+    const uint32_t* __restrict__ keysIn, const uint32_t* __restrict__ valsIn, uint32_t* __restrict__ keysOut,
+    uint32_t* __restrict__ valsOut, uint32_t n, uint32_t shift, const uint32_t* __restrict__ digitBase,
+    uint32_t* __restrict__ tileState, uint32_t* __restrict__ tileCounter, uint32_t* __restrict__ status)
+{
+    constexpr uint32_t WARPS = SORT_THREADS / 32;
+    __shared__ uint32_t warpHist[WARPS][256];
+    __shared__ uint32_t digitStart[256];     // exclusive scan of the tile's digit counts
+    __shared__ uint32_t globalBase[256];     // global output position of the tile's first key of each digit
+    __shared__ uint32_t smKey[SORT_TILE];
+    __shared__ uint32_t smVal[SORT_TILE];
+    __shared__ uint32_t tileSlot;
+
+    if (threadIdx.x == 0) tileSlot = atomicAdd(tileCounter, 1u);   // tiles start in order: look-back progresses
+    for (uint32_t i = threadIdx.x; i < WARPS * 256; i += SORT_THREADS) (&warpHist[0][0])[i] = 0;
+    __syncthreads();
+    const uint32_t tile = tileSlot;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t segBase = tile * SORT_TILE + warp * (SORT_ITEMS * 32);
+    const uint32_t ltMask = (1u << lane) - 1u;
+
+    uint32_t key[SORT_ITEMS], val[SORT_ITEMS], rank[SORT_ITEMS];
+#pragma unroll
+    for (uint32_t k = 0; k < SORT_ITEMS; k++) {
+        const uint32_t idx = segBase + k * 32 + lane;
+        const bool valid = idx < n;
+        key[k] = valid ? keysIn[idx] : 0u;
+        val[k] = valid ? valsIn[idx] : 0u;
+        const uint32_t d = valid ? ((key[k] >> shift) & 0xFFu) : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t before = __popc(peers & ltMask);
+        uint32_t base = 0;
+        if (valid) base = warpHist[warp][d];
+        __syncwarp();
+        if (valid && before == 0) warpHist[warp][d] = base + __popc(peers);
+        __syncwarp();
+        rank[k] = base + before;
+    }
+    __syncthreads();
+
+    // Per digit (one thread each): warp offsets within the tile, the tile aggregate, look-back.
+    {
+        const uint32_t d = threadIdx.x;
+        uint32_t running = 0;
+#pragma unroll
+        for (uint32_t wi = 0; wi < WARPS; wi++) {
+            const uint32_t c = warpHist[wi][d];
+            warpHist[wi][d] = running;
+            running += c;
+        }
+        volatile uint32_t* state = tileState;
+        if (tile == 0) {
+            state[d] = (2u << 30) | running;
+            globalBase[d] = digitBase[d];
+        } else {
+            state[tile * 256 + d] = (1u << 30) | running;
+            uint32_t prefix = 0;
+            int32_t t = int32_t(tile) - 1;
+            uint32_t spins = 0;
+            while (t >= 0) {
+                const uint32_t s = state[t * 256 + d];
+                const uint32_t flag = s >> 30;
+                if (flag == 0) {
+                    if (++spins > SPIN_LIMIT) { atomicOr(status, STATUS_LOOKBACK_TIMEOUT); break; }
+                    continue;
+                }
+                prefix += s & 0x3FFFFFFFu;
+                if (flag == 2) break;
+                t--;
+            }
+            __threadfence();
+            state[tile * 256 + d] = (2u << 30) | (prefix + running);
+            globalBase[d] = digitBase[d] + prefix;
+        }
+        digitStart[d] = running;   // scanned below
+    }
+    __syncthreads();
+    // Exclusive scan of the 256 digit counts (digitStart holds counts).
+    if (threadIdx.x < 32) {
+        uint32_t local[8];
+        uint32_t sum = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < 8; j++) { local[j] = digitStart[lane * 8 + j]; sum += local[j]; }
+        uint32_t incl = sum;
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        uint32_t excl = incl - sum;
+#pragma unroll
+        for (uint32_t j = 0; j < 8; j++) { digitStart[lane * 8 + j] = excl; excl += local[j]; }
+    }
+    __syncthreads();
+#pragma unroll
+    for (uint32_t k = 0; k < SORT_ITEMS; k++) {
+        const uint32_t idx = segBase + k * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = (key[k] >> shift) & 0xFFu;
+            const uint32_t pos = digitStart[d] + warpHist[warp][d] + rank[k];
+            smKey[pos] = key[k];
+            smVal[pos] = val[k];
+        }
+    }
+    __syncthreads();
+    const uint32_t tileBase = tile * SORT_TILE;
+    const uint32_t tileN = n - tileBase < SORT_TILE ? n - tileBase : SORT_TILE;
+    for (uint32_t i = threadIdx.x; i < tileN; i += SORT_THREADS) {
+        const uint32_t k = smKey[i];
+        const uint32_t d = (k >> shift) & 0xFFu;
+        const uint32_t dst = globalBase[d] + (i - digitStart[d]);
+        keysOut[dst] = k;
+        valsOut[dst] = smVal[i];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Karras LBVH over sorted keys (leaf = one collider). Internal node i spans [first, last] of the sorted order and
+// splits at the highest differing bit; equal keys are ordered by index (key ++ index), as the reference's stable
+// sort orders them. Children: >= 0 internal node, < 0 leaf ~rank.
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ int lbvh_delta(const uint32_t* keys, int n, int i, int j)
+{
+    if (j < 0 || j >= n) return -1;
+    const uint32_t a = keys[i], b = keys[j];
+    if (a != b) return __clz(a ^ b);
+    return 32 + __clz(uint32_t(i) ^ uint32_t(j));
+}
+
+__global__ void k_lbvh_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int n,
+                             const float4* __restrict__ caabb, int2* __restrict__ child, int2* __restrict__ range,
+                             int* __restrict__ parent, int* __restrict__ leafParent, float4* __restrict__ leafAabb,
+                             uint32_t* __restrict__ visit)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        leafAabb[i] = caabb[vals[i]];
+        if (n == 1) leafParent[0] = -1;
+        if (i >= n - 1) continue;
+        visit[i] = 0;
+        const int d = (lbvh_delta(keys, n, i, i + 1) - lbvh_delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+        const int dmin = lbvh_delta(keys, n, i, i - d);
+        int lmax = 2;
+        while (lbvh_delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+        int l = 0;
+        for (int t = lmax >> 1; t >= 1; t >>= 1)
+            if (lbvh_delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+        const int j = i + l * d;
+        const int dnode = lbvh_delta(keys, n, i, j);
+        int s = 0, t = l;
+        do {
+            t = (t + 1) >> 1;
+            if (lbvh_delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+        } while (t > 1);
+        const int gamma = i + s * d + (d < 0 ? -1 : 0);
+        const int first = i < j ? i : j, last = i < j ? j : i;
+        const int left = (first == gamma) ? ~gamma : gamma;
+        const int right = (last == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+        child[i] = make_int2(left, right);
+        range[i] = make_int2(first, last);
+        if (left < 0) leafParent[~left] = i; else parent[left] = i;
+        if (right < 0) leafParent[~right] = i; else parent[right] = i;
+        if (i == 0) parent[0] = -1;
+    }
+}
+
+// Bottom-up AABB refit: the second thread to reach a node merges its children (BvhTree::fitNodes equivalent).
+__global__ void k_lbvh_refit(int n, const int2* __restrict__ child, const int* __restrict__ parent,
+                             const int* __restrict__ leafParent, const float4* __restrict__ leafAabb,
+                             float4* __restrict__ nodeAabb, uint32_t* __restrict__ visit)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int node = n > 1 ? leafParent[i] : -1;
+        while (node >= 0) {
+            __threadfence();
+            if (atomicAdd(&visit[node], 1u) == 0) break;
+            __threadfence();
+            const int2 c = child[node];
+            const float4 a = c.x < 0 ? leafAabb[~c.x] : __ldcg(nodeAabb + c.x);
+            const float4 b = c.y < 0 ? leafAabb[~c.y] : __ldcg(nodeAabb + c.y);
+            const float4 u = make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w));
+            __stcg(nodeAabb + node, u);
+            node = parent[node];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Pair query. For dynamic collider of sorted rank i: every dynamic collider of rank > i whose AABB strictly
+// overlaps (BvhNode::overlaps, BvhNode.h:33-38) and has another owner body (LeafPairTesting.h:71-134), then every
+// static/sleeping collider that overlaps (cross pairs, ordered (dynamic, other)). Count pass then write pass at
+// scanned offsets: a deterministic pair list ordered by query rank and traversal order.
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool strict_overlap(const float4& a, const float4& b)
+{
+    return a.x < b.z && a.z > b.x && a.y < b.w && a.w > b.y;
+}
+
+template <bool WRITE>
+__device__ __forceinline__ void query_impl(const TreeView& dyn, const TreeView& other,
+                                           const uint32_t* __restrict__ cbody, uint32_t* __restrict__ counts,
+                                           const uint32_t* __restrict__ offsets, uint2* __restrict__ pairs,
+                                           uint32_t pairCap, uint32_t* __restrict__ status)
+{
+    const int n = dyn.n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 q = dyn.leafAabb[i];
+        const uint32_t me = dyn.vals[i];
+        const uint32_t myBody = cbody[me];
+        uint32_t count = 0;
+        uint32_t out = WRITE ? offsets[i] : 0u;
+        int stack[QUERY_STACK];
+        // Self pairs within the dynamic tree.
+        if (n > 1) {
+            int sp = 0;
+            stack[sp++] = 0;
+            while (sp > 0) {
+                const int node = stack[--sp];
+                const int2 c = dyn.child[node];
+#pragma unroll
+                for (int side = 0; side < 2; side++) {
+                    const int ch = side == 0 ? c.x : c.y;
+                    if (ch < 0) {
+                        const int j = ~ch;
+                        if (j > i && strict_overlap(q, dyn.leafAabb[j])) {
+                            const uint32_t other_c = dyn.vals[j];
+                            if (cbody[other_c] != myBody) {
+                                if (WRITE && out < pairCap) pairs[out] = make_uint2(me, other_c);
+                                out++;
+                                count++;
+                            }
+                        }
+                    } else if (dyn.range[ch].y > i && strict_overlap(q, dyn.nodeAabb[ch])) {
+                        if (sp < QUERY_STACK) stack[sp++] = ch;
+                        else atomicOr(status, STATUS_STACK_OVERFLOW);
+                    }
+                }
+            }
+        }
+        // Cross pairs against the static + sleeping tree.
+        if (other.n == 1) {
+            if (strict_overlap(q, other.leafAabb[0])) {
+                if (WRITE && out < pairCap) pairs[out] = make_uint2(me, other.vals[0]);
+                out++;
+                count++;
+            }
+        } else if (other.n > 1 && strict_overlap(q, other.nodeAabb[0])) {
+            int sp = 0;
+            stack[sp++] = 0;
+            while (sp > 0) {
+                const int node = stack[--sp];
+                const int2 c = other.child[node];
+#pragma unroll
+                for (int side = 0; side < 2; side++) {
+                    const int ch = side == 0 ? c.x : c.y;
+                    if (ch < 0) {
+                        if (strict_overlap(q, other.leafAabb[~ch])) {
+                            if (WRITE && out < pairCap) pairs[out] = make_uint2(me, other.vals[~ch]);
+                            out++;
+                            count++;
+                        }
+                    } else if (strict_overlap(q, other.nodeAabb[ch])) {
+                        if (sp < QUERY_STACK) stack[sp++] = ch;
+                        else atomicOr(status, STATUS_STACK_OVERFLOW);
+                    }
+                }
+            }
+        }
+        if (!WRITE) counts[i] = count;
+        else if (out > pairCap) atomicOr(status, STATUS_PAIR_OVERFLOW);
+    }
+}
+
+__global__ void k_query_count(TreeView dyn, TreeView other, const uint32_t* __restrict__ cbody,
+                              uint32_t* __restrict__ counts, uint32_t* __restrict__ status)
+{
+    query_impl<false>(dyn, other, cbody, counts, nullptr, nullptr, 0, status);
+}
+
+__global__ void k_query_write(TreeView dyn, TreeView other, const uint32_t* __restrict__ cbody,
+                              const uint32_t* __restrict__ offsets, uint2* __restrict__ pairs, uint32_t pairCap,
+                              uint32_t* __restrict__ status)
+{
+    query_impl<true>(dyn, other, cbody, nullptr, offsets, pairs, pairCap, status);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Exclusive scan of uint32 (reduce-then-scan, 2048 elements per block); used for pair offsets, compaction and
+// work lists.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_scan_blocks(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t n,
+                              uint32_t* __restrict__ blockSums)
+{
+    __shared__ uint32_t warpSums[SCAN_THREADS / 32];
+    const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    uint32_t v[SCAN_ITEMS];
+    uint32_t sum = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < SCAN_ITEMS; j++) { v[j] = base + j < n ? in[base + j] : 0u; sum += v[j]; }
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = sum;
+    for (uint32_t o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warpSums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t ws = lane < SCAN_THREADS / 32 ? warpSums[lane] : 0u;
+        uint32_t wi = ws;
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        if (lane < SCAN_THREADS / 32) warpSums[lane] = wi - ws;
+        if (lane == SCAN_THREADS / 32 - 1 && blockSums) blockSums[blockIdx.x] = wi;
+    }
+    __syncthreads();
+    uint32_t run = warpSums[warp] + incl - sum;
+#pragma unroll
+    for (uint32_t j = 0; j < SCAN_ITEMS; j++) {
+        if (base + j < n) out[base + j] = run;
+        run += v[j];
+    }
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_t* __restrict__ blockOffsets)
+{
+    const uint32_t add = blockOffsets[blockIdx.x];
+    const uint32_t base = blockIdx.x * SCAN_TILE;
+    for (uint32_t j = threadIdx.x; j < SCAN_TILE; j += blockDim.x)
+        if (base + j < n) out[base + j] += add;
+}
+
+// total = offsets[n-1] + in[n-1] (0 for n == 0).
+__global__ void k_scan_total(const uint32_t* __restrict__ in, const uint32_t* __restrict__ out, uint32_t n,
+                             uint32_t* __restrict__ total)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) *total = n ? out[n - 1] + in[n - 1] : 0u;
+}
+
+}  // namespace ag2d
