@@ -66,7 +66,15 @@ typedef struct ag2d_counters {
     uint32_t warm_hits;     /* manifolds warm-started */
     uint32_t sleeping;      /* bodies sleeping after the step */
     uint64_t steps;         /* steps taken by this world */
+    uint64_t launches;      /* kernel launches issued by this world so far */
 } ag2d_counters;
+
+/* Phases timed by ag2d_world_phase_times (index into the returned array). */
+enum ag2d_timed_phase {
+    AG2D_T_INTEGRATE = 0, AG2D_T_POSE, AG2D_T_TREE_DYNAMIC, AG2D_T_TREE_OTHER, AG2D_T_QUERY, AG2D_T_NARROW,
+    AG2D_T_COMPACT, AG2D_T_WARM, AG2D_T_WAKE, AG2D_T_COLOR, AG2D_T_SOLVE, AG2D_T_ISLANDS, AG2D_T_SORT,
+    AG2D_T_LBVH, AG2D_T_COUNT
+};
 
 /* Reference-layout world state for ag2d_world_load_state: every array in the reference's dense order, as its
  * SoA viewers expose them (SoA/BodySoA.h:14-36, SoA/ColliderSoA.h:10-32, SoA/Shapes/*.h). Group starts are
@@ -93,6 +101,7 @@ enum ag2d_field {
     AG2D_BODY_COM_X = 1, AG2D_BODY_COM_Y, AG2D_BODY_VEL_X, AG2D_BODY_VEL_Y, AG2D_BODY_ROTATION,
     AG2D_BODY_ANGULAR_VELOCITY, AG2D_BODY_ROT_COS, AG2D_BODY_ROT_SIN, AG2D_BODY_WRAP_COUNT, AG2D_BODY_SLEEP_TIMER,
     AG2D_BODY_STATE /* uint32: 0 static, 1 sleeping, 2 dynamic */, AG2D_BODY_SLEEP_ISLAND,
+    AG2D_BODY_POSE /* float32 x, y, rotation per body: one read of the pose array (a renderer's frame) */,
     AG2D_COL_WORLD_X = 32, AG2D_COL_WORLD_Y, AG2D_COL_WORLD_ROTATION, AG2D_COL_WORLD_COS, AG2D_COL_WORLD_SIN,
     AG2D_COL_AABB_MIN_X, AG2D_COL_AABB_MIN_Y, AG2D_COL_AABB_MAX_X, AG2D_COL_AABB_MAX_Y,
     AG2D_DYN_SORTED = 64,   /* dynamic tree: collider indices in Morton order */
@@ -159,6 +168,14 @@ int32_t ag2d_world_load_state(ag2d_world* world, const ag2d_state_desc* state);
 int32_t ag2d_world_step(ag2d_world* world, int32_t steps);
 
 int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out);
+
+/* Device timing of the step phases (the reference's Tracy zones, Profiling/TracyProfiler.h:66-72, become CUDA
+ * events on the world's stream). Enabling resets the totals. out_ms receives cumulative milliseconds per
+ * enum ag2d_timed_phase, out_calls the number of timed occurrences. */
+int32_t ag2d_world_set_profiling(ag2d_world* world, int32_t enable);
+int32_t ag2d_world_phase_times(ag2d_world* world, double* out_ms, uint64_t* out_calls, int32_t capacity);
+/* The CUDA stream the world's kernels run on (cudaStream_t), for callers that order their own work with it. */
+int32_t ag2d_world_stream(ag2d_world* world, void** out_stream);
 int32_t ag2d_world_body_count(ag2d_world* world, uint32_t* out_bodies, uint32_t* out_colliders);
 
 /* Copies a field into caller memory (host). out_bytes receives the field size; pass dst = NULL to query it.

@@ -25,7 +25,7 @@ ERR_INVALID_ARG, ERR_OOM, ERR_CAPACITY, ERR_TIMEOUT, ERR_CUDA, ERR_NO_DEVICE, ER
 
 # enum ag2d_field
 BODY_COM_X, BODY_COM_Y, BODY_VEL_X, BODY_VEL_Y, BODY_ROTATION, BODY_ANGULAR_VELOCITY, BODY_ROT_COS, BODY_ROT_SIN, \
-    BODY_WRAP_COUNT, BODY_SLEEP_TIMER, BODY_STATE, BODY_SLEEP_ISLAND = range(1, 13)
+    BODY_WRAP_COUNT, BODY_SLEEP_TIMER, BODY_STATE, BODY_SLEEP_ISLAND, BODY_POSE = range(1, 14)
 COL_WORLD_X, COL_WORLD_Y, COL_WORLD_ROTATION, COL_WORLD_COS, COL_WORLD_SIN, COL_AABB_MIN_X, COL_AABB_MIN_Y, \
     COL_AABB_MAX_X, COL_AABB_MAX_Y = range(32, 41)
 DYN_SORTED, DYN_MORTON, PAIRS, MANIFOLDS, PREV_MANIFOLDS, SOLVE_ORDER, COLOR_STARTS = range(64, 71)
@@ -64,7 +64,12 @@ class BodyDesc(ctypes.Structure):
 class Counters(ctypes.Structure):
     _fields_ = [("status", ctypes.c_uint32), ("pairs", ctypes.c_uint32), ("manifolds", ctypes.c_uint32),
                 ("colors", ctypes.c_uint32), ("woke", ctypes.c_uint32), ("slept", ctypes.c_uint32),
-                ("warm_hits", ctypes.c_uint32), ("sleeping", ctypes.c_uint32), ("steps", ctypes.c_uint64)]
+                ("warm_hits", ctypes.c_uint32), ("sleeping", ctypes.c_uint32), ("steps", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64)]
+
+
+TIMED_PHASES = ("integrate", "pose", "tree_dynamic", "tree_other", "query", "narrow", "compact", "warm", "wake",
+                "color", "solve", "islands", "sort", "lbvh")
 
 
 _P = ctypes.c_void_p
@@ -106,6 +111,9 @@ def _load():
     L.ag2d_world_read.argtypes = [vp, i32, vp, u64, ctypes.POINTER(u64)]
     L.ag2d_world_write.argtypes = [vp, i32, vp, u64]
     L.ag2d_world_run_phase.argtypes = [vp, i32]
+    L.ag2d_world_set_profiling.argtypes = [vp, i32]
+    L.ag2d_world_phase_times.argtypes = [vp, vp, vp, i32]
+    L.ag2d_world_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.ag2d_batch_create.argtypes = [ctypes.POINTER(vp), u32, ctypes.POINTER(vp)]
     L.ag2d_batch_step.argtypes = [vp, i32]
     L.ag2d_batch_destroy.argtypes = [vp]
@@ -263,6 +271,22 @@ class World:
         c = Counters()
         _check(lib.ag2d_world_counters(self.h, ctypes.byref(c)))
         return {n: int(getattr(c, n)) for n, _ in Counters._fields_}
+
+    def set_profiling(self, enable: bool = True):
+        _check(lib.ag2d_world_set_profiling(self.h, 1 if enable else 0))
+
+    def phase_times(self) -> dict:
+        """Cumulative device milliseconds and call counts per timed phase (profiling must be on)."""
+        ms = np.zeros(len(TIMED_PHASES), np.float64)
+        calls = np.zeros(len(TIMED_PHASES), np.uint64)
+        _check(lib.ag2d_world_phase_times(self.h, ms.ctypes.data, calls.ctypes.data, len(TIMED_PHASES)))
+        return {name: (float(ms[i]), int(calls[i])) for i, name in enumerate(TIMED_PHASES)}
+
+    def stream(self) -> int:
+        """cudaStream_t of the world's kernels (an integer handle)."""
+        s = ctypes.c_void_p()
+        _check(lib.ag2d_world_stream(self.h, ctypes.byref(s)))
+        return int(s.value or 0)
 
     def counts(self):
         b, c = ctypes.c_uint32(), ctypes.c_uint32()

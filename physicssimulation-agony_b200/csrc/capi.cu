@@ -203,6 +203,39 @@ struct ag2d_world {
     StepCounters* hCounters = nullptr;
     Scanner scanner;
 
+    // Per-phase device timers (CUDA events on the world's stream) and the count of kernel launches.
+    static constexpr int NPHASE = 14;
+    bool profiling = false;
+    cudaEvent_t ev[NPHASE][2] = {};
+    bool evPending[NPHASE] = {};
+    double phaseMs[NPHASE] = {};
+    uint64_t phaseCalls[NPHASE] = {};
+    uint64_t launches = 0;
+
+    void pbegin(int p)
+    {
+        if (!profiling) return;
+        if (!ev[p][0]) { CK(cudaEventCreate(&ev[p][0])); CK(cudaEventCreate(&ev[p][1])); }
+        CK(cudaEventRecord(ev[p][0], stream));
+    }
+    void pend(int p)
+    {
+        if (!profiling) return;
+        CK(cudaEventRecord(ev[p][1], stream));
+        evPending[p] = true;
+    }
+    void pcollect()
+    {
+        for (int p = 0; p < NPHASE; p++) {
+            if (!evPending[p]) continue;
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, ev[p][0], ev[p][1]));
+            phaseMs[p] += ms;
+            phaseCalls[p]++;
+            evPending[p] = false;
+        }
+    }
+
     DeviceWorld view() const
     {
         DeviceWorld w;
@@ -218,6 +251,10 @@ struct ag2d_world {
 
     ~ag2d_world()
     {
+        for (auto& e : ev) {
+            if (e[0]) cudaEventDestroy(e[0]);
+            if (e[1]) cudaEventDestroy(e[1]);
+        }
         if (hCounters) cudaFreeHost(hCounters);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -430,20 +467,24 @@ struct ag2d_world {
         const float damp = settings.angular_damping;
         const float dampHalf = (damp >= 0.0f && damp < 1.0f) ? std::pow(damp, settings.dt * 0.5f) : 2.0f;
         if (nDynBody) {
+            pbegin(0);
             k_integrate<<<gridFor(nDynBody), 256, 0, stream>>>(view(), dynBody.p, nDynBody, settings.dt,
                                                               settings.gravity_x, settings.gravity_y, dampHalf);
             CK(cudaGetLastError());
+            pend(0);
+            launches++;
         }
     }
 
     void phasePose(bool full)
     {
-        if (full) {
-            if (nColliders) k_collider_pose<<<gridFor(nColliders), 256, 0, stream>>>(view(), nullptr, nColliders);
-        } else if (nDynCol) {
-            k_collider_pose<<<gridFor(nDynCol), 256, 0, stream>>>(view(), dynCol.p, nDynCol);
-        }
+        const uint32_t n = full ? nColliders : nDynCol;
+        if (n == 0) return;
+        pbegin(1);
+        k_collider_pose<<<gridFor(n), 256, 0, stream>>>(view(), full ? nullptr : dynCol.p, n);
         CK(cudaGetLastError());
+        pend(1);
+        launches++;
     }
 
     void buildTree(Tree& t, const uint32_t* list, uint32_t n)
@@ -451,6 +492,7 @@ struct ag2d_world {
         const cudaStream_t s = stream;
         t.n = int(n);
         if (n == 0) return;
+        launches += 11 + (n > 1 ? 1 : 0);
         k_bounds_init<<<1, 32, 0, s>>>(t.bounds.p);
         k_bounds<<<gridFor(n), 256, 0, s>>>(caabb.p, list, n, t.bounds.p);
         k_morton<<<gridFor(n), 256, 0, s>>>(caabb.p, list, n, t.bounds.p, t.keys.p, t.vals.p);
@@ -461,6 +503,8 @@ struct ag2d_world {
         k_sort_digit_scan<<<4, 256, 0, s>>>(t.hist.p);
         CK(cudaGetLastError());
         const uint32_t tiles = div_up(n, SORT_TILE);
+        const bool isDyn = &t == &dynTree;
+        if (isDyn) pbegin(12);
         CK(cudaMemsetAsync(t.tileState.p, 0, size_t(tiles) * 256 * 4 * sizeof(uint32_t), s));
         CK(cudaMemsetAsync(t.tileCounter.p, 0, 4 * sizeof(uint32_t), s));
         uint32_t *ki = t.keys.p, *vi = t.vals.p, *ko = t.keys2.p, *vo = t.vals2.p;
@@ -472,6 +516,8 @@ struct ag2d_world {
             std::swap(ki, ko);
             std::swap(vi, vo);
         }
+        if (isDyn) pend(12);
+        if (isDyn) pbegin(13);
         k_lbvh_build<<<gridFor(n), 256, 0, s>>>(t.keys.p, t.vals.p, int(n), caabb.p, t.child.p, t.range.p,
                                                  t.parent.p, t.leafParent.p, t.leafAabb.p, t.visit.p);
         CK(cudaGetLastError());
@@ -480,14 +526,19 @@ struct ag2d_world {
                                                      t.nodeAabb.p, t.visit.p);
             CK(cudaGetLastError());
         }
+        if (isDyn) pend(13);
     }
 
     void phaseBroad()
     {
         const cudaStream_t s = stream;
+        pbegin(2);
         buildTree(dynTree, dynCol.p, nDynCol);
+        pend(2);
         if (otherDirty) {
+            pbegin(3);
             buildTree(otherTree, otherCol.p, nOther);
+            pend(3);
             otherDirty = false;
         }
         otherTree.n = int(nOther);
@@ -496,6 +547,8 @@ struct ag2d_world {
             CK(cudaMemsetAsync(total, 0, sizeof(uint32_t), s));
             return;
         }
+        pbegin(4);
+        launches += 2 + scanLaunches(nDynCol) + 1;
         k_query_count<<<gridFor(nDynCol, 128), 128, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qCounts.p,
                                                             &dCounters.p->status);
         CK(cudaGetLastError());
@@ -503,6 +556,7 @@ struct ag2d_world {
         k_query_write<<<gridFor(nDynCol, 128), 128, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qOffsets.p,
                                                             pairs.p, pairCap, &dCounters.p->status);
         CK(cudaGetLastError());
+        pend(4);
     }
 
     void phaseNarrow()
@@ -510,14 +564,20 @@ struct ag2d_world {
         const cudaStream_t s = stream;
         const uint32_t* nPairs = &dCounters.p->pairs;
         const uint32_t g = gridFor(pairCap);
+        pbegin(5);
         k_narrow<<<g, 256, 0, s>>>(view(), pairs.p, nPairs, pairCap, slots.p, hit.p);
         CK(cudaGetLastError());
+        pend(5);
+        pbegin(6);
+        launches += 1 + scanLaunches(pairCap) + 1 + 2;
         // The scan length must be host-known: scan the whole capacity (hit flags beyond the count are stale but the
         // compaction kernel ignores them).
         scanner.run(hit.p, hitOffsets.p, pairCap, nullptr, s);
         k_compact_manifolds<<<g, 256, 0, s>>>(slots.p, hit.p, hitOffsets.p, nPairs, pairCap, manifolds.p,
                                                manifoldCap, nManifolds.p, dCounters.p);
         CK(cudaGetLastError());
+        pend(6);
+        pbegin(7);
         // Warm start from the previous step's manifolds.
         CK(cudaMemsetAsync(hashKeys.p, 0xFF, size_t(hashCap) * sizeof(unsigned long long), s));
         k_warm_insert<<<gridFor(manifoldCap), 256, 0, s>>>(prevManifolds.p, nPrev.p, hashKeys.p, hashVals.p, hashCap,
@@ -525,15 +585,19 @@ struct ag2d_world {
         k_warm_lookup<<<gridFor(manifoldCap), 256, 0, s>>>(prevManifolds.p, manifolds.p, nManifolds.p, hashKeys.p,
                                                            hashVals.p, hashCap, dCounters.p);
         CK(cudaGetLastError());
+        pend(7);
     }
 
     void phaseWake()
     {
         const cudaStream_t s = stream;
+        pbegin(8);
+        launches += 2;
         CK(cudaMemsetAsync(wakeIsland.p, 0, sizeof(uint32_t) * std::max<uint32_t>(nBodies, 1), s));
         k_wake<<<gridFor(manifoldCap), 256, 0, s>>>(view(), manifolds.p, nManifolds.p, wakeIsland.p, dCounters.p);
         k_wake_apply<<<gridFor(nBodies), 256, 0, s>>>(view(), wakeIsland.p, dCounters.p);
         CK(cudaGetLastError());
+        pend(8);
     }
 
     void phaseSolve()
@@ -552,7 +616,10 @@ struct ag2d_world {
         {
             const int grid = std::max(1, std::min<int>(dev.coopColorBlocks, int(div_up(est, 256))));
             void* args[] = {&w, &mc, &nm, &colorp, &bmax, &ccount, &cstart, &ord, &barp, &ctr};
+            pbegin(9);
             CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_color), dim3(grid), dim3(256), args, 0, s));
+            pend(9);
+            launches++;
         }
         CK(cudaMemsetAsync(bar.p, 0, 2 * sizeof(uint32_t), s));
         {
@@ -561,7 +628,10 @@ struct ag2d_world {
             uint32_t vi = settings.velocity_iterations, pi = settings.position_iterations;
             const int grid = std::max(1, std::min<int>(dev.coopSolveBlocks, int(div_up(est, 256))));
             void* args[] = {&w, &mm, &nm, &ord, &cstart, &cp, &vi, &pi, &barp, &ctr};
+            pbegin(10);
             CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve), dim3(grid), dim3(256), args, 0, s));
+            pend(10);
+            launches++;
         }
     }
 
@@ -569,18 +639,34 @@ struct ag2d_world {
     {
         const cudaStream_t s = stream;
         const DeviceWorld w = view();
+        pbegin(11);
+        launches += 4;
         k_island_init<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p);
         k_island_union<<<gridFor(manifoldCap), 256, 0, s>>>(w, manifolds.p, nManifolds.p, ufParent.p);
         k_island_quiet<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p, settings.dt, settings.sleep_speed,
                                                         settings.sleep_time);
         k_island_sleep<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p, dCounters.p);
         CK(cudaGetLastError());
+        pend(11);
     }
 
     void readCounters()
     {
         CK(cudaMemcpyAsync(hCounters, dCounters.p, sizeof(StepCounters), cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
+        pcollect();
+    }
+
+    static uint32_t scanLaunches(uint32_t n)
+    {
+        uint32_t k = 0;
+        while (true) {
+            const uint32_t nb = std::max<uint32_t>(div_up(n, SCAN_TILE), 1);
+            k += nb > 1 ? 2 : 1;
+            if (nb <= 1) break;
+            n = nb;
+        }
+        return k;
     }
 
     // One fixed step (Simulation::physicsStep order, Simulation.cpp:255-351).
@@ -849,6 +935,39 @@ int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out)
         out->woke = c.woke; out->slept = c.slept; out->warm_hits = c.warmHits;
         out->sleeping = world->nBodies - world->nDynBody - world->nStatic;
         out->steps = world->stepsTaken;
+        out->launches = world->launches;
+    });
+}
+
+int32_t ag2d_world_set_profiling(ag2d_world* world, int32_t enable)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        world->profiling = enable != 0;
+        for (int p = 0; p < ag2d_world::NPHASE; p++) {
+            world->phaseMs[p] = 0.0;
+            world->phaseCalls[p] = 0;
+            world->evPending[p] = false;
+        }
+    });
+}
+
+int32_t ag2d_world_phase_times(ag2d_world* world, double* out_ms, uint64_t* out_calls, int32_t capacity)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        for (int p = 0; p < std::min<int>(capacity, ag2d_world::NPHASE); p++) {
+            if (out_ms) out_ms[p] = world->phaseMs[p];
+            if (out_calls) out_calls[p] = world->phaseCalls[p];
+        }
+    });
+}
+
+int32_t ag2d_world_stream(ag2d_world* world, void** out_stream)
+{
+    return guarded([&] {
+        if (!world || !out_stream) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        *out_stream = world->stream;
     });
 }
 
@@ -913,6 +1032,12 @@ static std::vector<uint8_t> read_field(ag2d_world& w, int32_t field)
         return pack(o);
     }
     case AG2D_BODY_SLEEP_ISLAND: return pack(download(w.sleepIsland.p, nb, s));
+    case AG2D_BODY_POSE: {
+        const auto v = download(w.bpos.p, nb, s);
+        std::vector<float> o(size_t(nb) * 3);
+        for (uint32_t i = 0; i < nb; i++) { o[3 * i] = v[i].x; o[3 * i + 1] = v[i].y; o[3 * i + 2] = v[i].z; }
+        return pack(o);
+    }
     case AG2D_COL_WORLD_X: return comp4(w.cpose, nc, 0);
     case AG2D_COL_WORLD_Y: return comp4(w.cpose, nc, 1);
     case AG2D_COL_WORLD_COS: return comp4(w.cpose, nc, 2);
