@@ -214,7 +214,7 @@ def run_ours(args):
     sampler = ClockSampler(local)
     sampler.start()
     per_step = []
-    pairs_sum = manifolds_sum = 0
+    pairs_sum = manifolds_sum = colors_sum = 0
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
@@ -227,6 +227,7 @@ def run_ours(args):
         c = w.counters()
         pairs_sum += c["pairs"]
         manifolds_sum += c["manifolds"]
+        colors_sum += c["colors"]
     torch.cuda.synchronize()
     if world_size > 1:
         dist.barrier()
@@ -310,6 +311,12 @@ def run_ours(args):
             "gpu_launches": int(c1["launches"] - c0["launches"]),
             "clocks": clocks,
             "phase_ms_per_step": {k: round(v[0] / max(K, 1), 4) for k, v in phases.items()},
+            "diagnostics": {"mean_colors": colors_sum / K,
+                            "list_rebuilds": c1["list_rebuilds"] - c0["list_rebuilds"],
+                            "retries": c1["retries"] - c0["retries"], "regrows": c1["regrows"] - c0["regrows"],
+                            "host_ms_per_step": (c1["host_ms"] - c0["host_ms"]) / K,
+                            "sync_wait_ms_per_step": (c1["sync_ms"] - c0["sync_ms"]) / K,
+                            "max_step_ms": max(per_step), "median_step_ms": statistics.median(per_step)},
         }
         print(json.dumps(line))
     if world_size > 1:

@@ -67,6 +67,11 @@ typedef struct ag2d_counters {
     uint32_t sleeping;      /* bodies sleeping after the step */
     uint64_t steps;         /* steps taken by this world */
     uint64_t launches;      /* kernel launches issued by this world so far */
+    uint64_t list_rebuilds; /* work-list rebuilds after sleep/wake changes */
+    uint64_t retries;       /* steps re-run after a buffer overflow (state restored, buffers grown) */
+    uint64_t regrows;       /* capacity growths */
+    double host_ms;         /* host wall time spent inside ag2d_world_step so far */
+    double sync_ms;         /* of which waiting for the device at the end of steps */
 } ag2d_counters;
 
 /* Phases timed by ag2d_world_phase_times (index into the returned array). */

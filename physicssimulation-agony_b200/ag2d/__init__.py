@@ -65,7 +65,8 @@ class Counters(ctypes.Structure):
     _fields_ = [("status", ctypes.c_uint32), ("pairs", ctypes.c_uint32), ("manifolds", ctypes.c_uint32),
                 ("colors", ctypes.c_uint32), ("woke", ctypes.c_uint32), ("slept", ctypes.c_uint32),
                 ("warm_hits", ctypes.c_uint32), ("sleeping", ctypes.c_uint32), ("steps", ctypes.c_uint64),
-                ("launches", ctypes.c_uint64)]
+                ("launches", ctypes.c_uint64), ("list_rebuilds", ctypes.c_uint64), ("retries", ctypes.c_uint64),
+                ("regrows", ctypes.c_uint64), ("host_ms", ctypes.c_double), ("sync_ms", ctypes.c_double)]
 
 
 TIMED_PHASES = ("integrate", "pose", "tree_dynamic", "tree_other", "query", "narrow", "compact", "warm", "wake",
@@ -270,7 +271,7 @@ class World:
     def counters(self) -> dict:
         c = Counters()
         _check(lib.ag2d_world_counters(self.h, ctypes.byref(c)))
-        return {n: int(getattr(c, n)) for n, _ in Counters._fields_}
+        return {n: (float(getattr(c, n)) if t is ctypes.c_double else int(getattr(c, n))) for n, t in Counters._fields_}
 
     def set_profiling(self, enable: bool = True):
         _check(lib.ag2d_world_set_profiling(self.h, 1 if enable else 0))

@@ -65,12 +65,6 @@ __global__ void k_warm_lookup(const Manifold* prev, Manifold* cur, const uint32_
 __global__ void k_wake(DeviceWorld w, const Manifold* m, const uint32_t* nM, uint32_t* wakeIsland,
                        StepCounters* counters);
 __global__ void k_wake_apply(DeviceWorld w, const uint32_t* wakeIsland, StepCounters* counters);
-__global__ void k_color(DeviceWorld w, const Manifold* m, const uint32_t* nM, uint32_t* color,
-                        unsigned long long* bodyMax, uint32_t* colorCount, uint32_t* colorStart, uint32_t* order,
-                        uint32_t* bar, StepCounters* counters);
-__global__ void k_solve(DeviceWorld w, Manifold* m, const uint32_t* nM, const uint32_t* order,
-                        const uint32_t* colorStart, Constraint* cons, uint32_t velIters, uint32_t posIters,
-                        uint32_t* bar, StepCounters* counters);
 __global__ void k_island_init(DeviceWorld w, uint32_t* parent, uint32_t* flag);
 __global__ void k_island_union(DeviceWorld w, const Manifold* m, const uint32_t* nM, uint32_t* parent);
 __global__ void k_island_quiet(DeviceWorld w, uint32_t* parent, uint32_t* flag, float dt, float speedThreshold,

@@ -1,0 +1,339 @@
+// Graph colouring + sequential-impulse solver as one device routine over a "team" of threads that share a barrier:
+// a thread-block cluster (hardware barrier.cluster, large single worlds), one CTA (batched small worlds) or a
+// cooperative grid (very large worlds). The per-constraint arithmetic (prep/warm/velocity/position) below is shared
+// by every variant.
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "ag2d_kernels.cuh"
+
+namespace ag2d {
+
+namespace cg = cooperative_groups;
+
+// ---------------------------------------------------------------------------------------------------------------
+// Sequential-impulse solver (Solving/BodyCollisionSolver.cpp): computeConstraintData (:229-390), applyWarmStarting
+// (:416-490), solveVelocityConstraints (:492-928; one-contact path, two-contact 2x2 block LCP with iterative
+// fallback, iterative friction), solvePositionConstraints (:930-980), scatterImpulses (:392-414). A team runs every
+// pass colour by colour with its barrier between colours.
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void prep_constraint(const DeviceWorld& w, const Manifold& m, uint32_t mi, Constraint& k)
+{
+    const uint32_t bA = w.cbody[m.a], bB = w.cbody[m.b];
+    const float4 vA = w.bvel[bA], vB = w.bvel[bB], pA = w.bpos[bA], pB = w.bpos[bB];
+    k.bodyA = bA; k.bodyB = bB; k.count = m.count; k.manifold = mi;
+    k.nx = m.nx; k.ny = m.ny;
+    k.imA = vA.w; k.imB = vB.w; k.iIA = pA.w; k.iIB = pB.w;
+    k.jn0 = m.jn0; k.jt0 = m.jt0; k.jn1 = m.jn1; k.jt1 = m.jt1;
+    k.penBase = m.depth + ((pB.x - pA.x) * m.nx + (pB.y - pA.y) * m.ny) - 0.001f;
+    const float4 matA = w.materials[w.cmat[m.a]], matB = w.materials[w.cmat[m.b]];
+    const float e = (matA.x + matB.x) * 0.5f;
+    k.sf = sqrtf(rfmaxf(0.0f, matA.y * matB.y));
+    k.df = sqrtf(rfmaxf(0.0f, matA.z * matB.z));
+    const float effMass = k.imA + k.imB;
+    const float tx = -m.ny, ty = m.nx;
+    float rAn[2] = {0, 0}, rBn[2] = {0, 0}, rAt[2] = {0, 0}, rBt[2] = {0, 0}, nm[2] = {0, 0}, tm[2] = {0, 0}, bias[2] = {0, 0};
+#pragma unroll
+    for (uint32_t i = 0; i < 2; i++) {
+        if (i >= m.count) break;
+        const float px = i == 0 ? m.px0 : m.px1, py = i == 0 ? m.py0 : m.py1;
+        const float rAx = px - pA.x, rAy = py - pA.y, rBx = px - pB.x, rBy = py - pB.y;
+        rAn[i] = (-rAy) * m.nx + rAx * m.ny;
+        rBn[i] = (-rBy) * m.nx + rBx * m.ny;
+        rAt[i] = (-rAy) * tx + rAx * ty;
+        rBt[i] = (-rBy) * tx + rBx * ty;
+        const float nd = effMass + rAn[i] * rAn[i] * k.iIA + rBn[i] * rBn[i] * k.iIB;
+        nm[i] = nd > 0.0f ? 1.0f / nd : 0.0f;
+        const float td = effMass + rAt[i] * rAt[i] * k.iIA + rBt[i] * rBt[i] * k.iIB;
+        tm[i] = td > 0.0f ? 1.0f / td : 0.0f;
+        const float negVn = -(((vB.x - vA.x) * m.nx + (vB.y - vA.y) * m.ny) + rBn[i] * vB.z - rAn[i] * vA.z);
+        bias[i] = (negVn > 0.0f) ? e * negVn : 0.0f;
+    }
+    k.rAn0 = rAn[0]; k.rBn0 = rBn[0]; k.rAt0 = rAt[0]; k.rBt0 = rBt[0]; k.nm0 = nm[0]; k.tm0 = tm[0]; k.bias0 = bias[0];
+    k.rAn1 = rAn[1]; k.rBn1 = rBn[1]; k.rAt1 = rAt[1]; k.rBt1 = rBt[1]; k.nm1 = nm[1]; k.tm1 = tm[1]; k.bias1 = bias[1];
+    k.pad = 0.0f;
+}
+
+__device__ __forceinline__ void warm_constraint(const DeviceWorld& w, const Constraint& k)
+{
+    float4 vA = w.bvel[k.bodyA], vB = w.bvel[k.bodyB];
+    const float tx = -k.ny, ty = k.nx;
+    const float jn0 = k.count > 0 ? k.jn0 : 0.0f, jt0 = k.count > 0 ? k.jt0 : 0.0f;
+    const float jn1 = k.count > 1 ? k.jn1 : 0.0f, jt1 = k.count > 1 ? k.jt1 : 0.0f;
+    const float sn = jn0 + jn1, st = jt0 + jt1;
+    const float ix = sn * k.nx + st * tx, iy = sn * k.ny + st * ty;
+    vA.x = vA.x - ix * k.imA; vA.y = vA.y - iy * k.imA;
+    vB.x = vB.x + ix * k.imB; vB.y = vB.y + iy * k.imB;
+    vA.z = vA.z - (jn0 * k.rAn0 + jt0 * k.rAt0 + jn1 * k.rAn1 + jt1 * k.rAt1) * k.iIA;
+    vB.z = vB.z + (jn0 * k.rBn0 + jt0 * k.rBt0 + jn1 * k.rBn1 + jt1 * k.rBt1) * k.iIB;
+    if (k.imA > 0.0f) w.bvel[k.bodyA] = vA;
+    if (k.imB > 0.0f) w.bvel[k.bodyB] = vB;
+}
+
+__device__ __forceinline__ void velocity_constraint(const DeviceWorld& w, Constraint& k)
+{
+    float4 vA = w.bvel[k.bodyA], vB = w.bvel[k.bodyB];
+    const float imA = k.imA, imB = k.imB, iIA = k.iIA, iIB = k.iIB;
+    const float nx = k.nx, ny = k.ny, tx = -ny, ty = nx;
+    if (k.count == 1) {
+        float jnSingle = 0.0f;
+        {
+            const float vn = ((vB.x - vA.x) * nx + (vB.y - vA.y) * ny) + k.rBn0 * vB.z - k.rAn0 * vA.z;
+            if (!(vn > 0.0f && k.jn0 == 0.0f)) {
+                const float jn = (k.bias0 - vn) * k.nm0;
+                const float old = k.jn0;
+                k.jn0 = rfmaxf(0.0f, old + jn);
+                const float dj = k.jn0 - old;
+                jnSingle = k.jn0;
+                const float ix = dj * nx, iy = dj * ny;
+                vA.x = vA.x - ix * imA; vA.y = vA.y - iy * imA;
+                vA.z = vA.z - dj * k.rAn0 * iIA;
+                vB.x = vB.x + ix * imB; vB.y = vB.y + iy * imB;
+                vB.z = vB.z + dj * k.rBn0 * iIB;
+            }
+        }
+        {
+            const float slip = ((vB.x - vA.x) * tx + (vB.y - vA.y) * ty) + k.rBt0 * vB.z - k.rAt0 * vA.z;
+            const float jt = -slip * k.tm0;
+            const float old = k.jt0;
+            const float target = old + jt;
+            if (fabsf(target) <= jnSingle * k.sf) k.jt0 = target;
+            else { const float maxD = jnSingle * k.df; k.jt0 = glm_clamp(target, -maxD, maxD); }
+            const float dj = k.jt0 - old;
+            const float ix = dj * tx, iy = dj * ty;
+            vA.x = vA.x - ix * imA; vA.y = vA.y - iy * imA;
+            vA.z = vA.z - dj * k.rAt0 * iIA;
+            vB.x = vB.x + ix * imB; vB.y = vB.y + iy * imB;
+            vB.z = vB.z + dj * k.rBt0 * iIB;
+        }
+    } else {
+        const float effMass = imA + imB;
+        float jnArr0 = 0.0f, jnArr1 = 0.0f;
+        bool ok = false;
+        {
+            const float dvn = (vB.x - vA.x) * nx + (vB.y - vA.y) * ny;
+            const float vn0 = dvn + k.rBn0 * vB.z - k.rAn0 * vA.z;
+            const float vn1 = dvn + k.rBn1 * vB.z - k.rAn1 * vA.z;
+            const float a0 = k.jn0, a1 = k.jn1;
+            const float K00 = effMass + k.rAn0 * k.rAn0 * iIA + k.rBn0 * k.rBn0 * iIB;
+            const float K11 = effMass + k.rAn1 * k.rAn1 * iIA + k.rBn1 * k.rBn1 * iIB;
+            const float K01 = effMass + k.rAn0 * k.rAn1 * iIA + k.rBn0 * k.rBn1 * iIB;
+            const float b0 = k.bias0 - vn0 + K00 * a0 + K01 * a1;
+            const float b1 = k.bias1 - vn1 + K01 * a0 + K11 * a1;
+            const float EPS = 1e-6f;
+            float x0 = 0.0f, x1 = 0.0f;
+            const float det = K00 * K11 - K01 * K01;
+            const float maxK = rfmaxf(K00, K11);
+            if (maxK * maxK < 1000.0f * det) {
+                const float invDet = 1.0f / det;
+                const float s0 = (K11 * b0 - K01 * b1) * invDet;
+                const float s1 = (K00 * b1 - K01 * b0) * invDet;
+                if (s0 >= -EPS && s1 >= -EPS) { x0 = rfmaxf(s0, 0.0f); x1 = rfmaxf(s1, 0.0f); ok = true; }
+            }
+            if (!ok && K11 > 0.0f) {
+                const float s1 = b1 / K11;
+                if (s1 >= -EPS && (K01 * s1 - b0) >= -EPS) { x0 = 0.0f; x1 = rfmaxf(s1, 0.0f); ok = true; }
+            }
+            if (!ok && K00 > 0.0f) {
+                const float s0 = b0 / K00;
+                if (s0 >= -EPS && (K01 * s0 - b1) >= -EPS) { x0 = rfmaxf(s0, 0.0f); x1 = 0.0f; ok = true; }
+            }
+            if (!ok && b0 <= EPS && b1 <= EPS) { x0 = 0.0f; x1 = 0.0f; ok = true; }
+            if (ok) {
+                const float d0 = x0 - a0, d1 = x1 - a1;
+                k.jn0 = x0; k.jn1 = x1;
+                jnArr0 = x0; jnArr1 = x1;
+                const float sum = d0 + d1;
+                const float sA = sum * imA, sB = sum * imB;
+                vA.x = vA.x - nx * sA; vA.y = vA.y - ny * sA;
+                vB.x = vB.x + nx * sB; vB.y = vB.y + ny * sB;
+                vA.z = vA.z - (d0 * k.rAn0 + d1 * k.rAn1) * iIA;
+                vB.z = vB.z + (d0 * k.rBn0 + d1 * k.rBn1) * iIB;
+            }
+        }
+        if (!ok) {
+#pragma unroll
+            for (uint32_t i = 0; i < 2; i++) {
+                const float rAn = i == 0 ? k.rAn0 : k.rAn1, rBn = i == 0 ? k.rBn0 : k.rBn1;
+                const float bias = i == 0 ? k.bias0 : k.bias1, nmass = i == 0 ? k.nm0 : k.nm1;
+                const float vn = ((vB.x - vA.x) * nx + (vB.y - vA.y) * ny) + rBn * vB.z - rAn * vA.z;
+                const float jn = (bias - vn) * nmass;
+                const float old = i == 0 ? k.jn0 : k.jn1;
+                const float acc = rfmaxf(0.0f, old + jn);
+                if (i == 0) { k.jn0 = acc; jnArr0 = acc; } else { k.jn1 = acc; jnArr1 = acc; }
+                const float dj = acc - old;
+                const float ix = dj * nx, iy = dj * ny;
+                vA.x = vA.x - ix * imA; vA.y = vA.y - iy * imA;
+                vA.z = vA.z - dj * rAn * iIA;
+                vB.x = vB.x + ix * imB; vB.y = vB.y + iy * imB;
+                vB.z = vB.z + dj * rBn * iIB;
+            }
+        }
+#pragma unroll
+        for (uint32_t i = 0; i < 2; i++) {
+            const float rAt = i == 0 ? k.rAt0 : k.rAt1, rBt = i == 0 ? k.rBt0 : k.rBt1;
+            const float tmass = i == 0 ? k.tm0 : k.tm1;
+            const float slip = ((vB.x - vA.x) * tx + (vB.y - vA.y) * ty) + rBt * vB.z - rAt * vA.z;
+            const float jt = -slip * tmass;
+            const float old = i == 0 ? k.jt0 : k.jt1;
+            const float target = old + jt;
+            const float jn = i == 0 ? jnArr0 : jnArr1;
+            float acc;
+            if (fabsf(target) <= jn * k.sf) acc = target;
+            else { const float maxD = jn * k.df; acc = glm_clamp(target, -maxD, maxD); }
+            if (i == 0) k.jt0 = acc; else k.jt1 = acc;
+            const float dj = acc - old;
+            const float ix = dj * tx, iy = dj * ty;
+            vA.x = vA.x - ix * imA; vA.y = vA.y - iy * imA;
+            vA.z = vA.z - dj * rAt * iIA;
+            vB.x = vB.x + ix * imB; vB.y = vB.y + iy * imB;
+            vB.z = vB.z + dj * rBt * iIB;
+        }
+    }
+    if (imA > 0.0f) w.bvel[k.bodyA] = vA;
+    if (imB > 0.0f) w.bvel[k.bodyB] = vB;
+}
+
+__device__ __forceinline__ void position_constraint(const DeviceWorld& w, const Constraint& k)
+{
+    float4 pA = w.bpos[k.bodyA], pB = w.bpos[k.bodyB];
+    const float pen = k.penBase - ((pB.x - pA.x) * k.nx + (pB.y - pA.y) * k.ny);
+    if (pen <= 0.0f) return;
+    const float imA = w.bvel[k.bodyA].w, imB = w.bvel[k.bodyB].w;
+    const float total = pen / (imA + imB) * 0.5f;
+    const float cA = imA * total, cB = imB * total;
+    const float cAx = k.nx * cA, cAy = k.ny * cA, cBx = k.nx * cB, cBy = k.ny * cB;
+    if (imA > 0.0f) { pA.x = pA.x - cAx; pA.y = pA.y - cAy; w.bpos[k.bodyA] = pA; }
+    if (imB > 0.0f) { pB.x = pB.x + cBx; pB.y = pB.y + cBy; w.bpos[k.bodyB] = pB; }
+}
+
+
+__device__ __forceinline__ uint32_t priority_hash(uint32_t x)
+{
+    x ^= x >> 16; x *= 0x85ebca6bu; x ^= x >> 13; x *= 0xc2b2ae35u; x ^= x >> 16;   // murmur3 finalizer (bijective)
+    return x;
+}
+
+// Scratch of one world's colouring and solve.
+struct SolveScratch {
+    uint32_t* color;                  // [manifolds]
+    uint32_t* order;                  // [manifolds] colour-major solving order
+    unsigned long long* bodyMax;      // [bodies], zeroed before the call
+    uint32_t* colorCount;             // [MAX_COLORS + 1], zeroed by the routine
+    uint32_t* colorStart;             // [MAX_COLORS + 1]
+    Constraint* cons;                 // [manifolds]
+};
+
+struct ClusterSync {
+    __device__ __forceinline__ bool operator()() const { cg::this_cluster().sync(); return true; }
+};
+struct BlockSync {
+    __device__ __forceinline__ bool operator()() const { __syncthreads(); return true; }
+};
+struct GridSync {
+    uint32_t* bar;
+    uint32_t* status;
+    __device__ __forceinline__ bool operator()() const { return grid_barrier(bar, status); }
+};
+
+// Colouring (Luby / Jones-Plassmann rounds: colour r goes to every uncoloured manifold whose priority is the largest
+// on each of its dynamic bodies) followed by the colour-major solve. rank/size: this thread's index in the team.
+// Returns false if the colouring needed more than MAX_COLORS colours or a barrier gave up.
+template <class Sync>
+__device__ bool color_and_solve(const DeviceWorld& w, Manifold* __restrict__ m, uint32_t n, const SolveScratch& s,
+                                uint32_t velIters, uint32_t posIters, uint32_t rank, uint32_t size, Sync sync,
+                                uint32_t* __restrict__ outColors, uint32_t* __restrict__ status)
+{
+    for (uint32_t i = rank; i < n; i += size) s.color[i] = NO_COLOR;
+    for (uint32_t c = rank; c <= MAX_COLORS; c += size) s.colorCount[c] = 0;
+    if (!sync()) return false;
+    uint32_t rounds = 0;
+    bool done = n == 0;
+    for (uint32_t r = 0; r < MAX_COLORS && !done; r++) {
+        rounds = r + 1;
+        const unsigned long long tag = static_cast<unsigned long long>(r + 1) << 32;
+        for (uint32_t i = rank; i < n; i += size) {
+            if (s.color[i] != NO_COLOR) continue;
+            const unsigned long long key = tag | priority_hash(i);
+            const uint32_t bA = w.cbody[m[i].a], bB = w.cbody[m[i].b];
+            if (__ldcg(&w.bvel[bA].w) > 0.0f) atomicMax(s.bodyMax + bA, key);
+            if (__ldcg(&w.bvel[bB].w) > 0.0f) atomicMax(s.bodyMax + bB, key);
+        }
+        if (!sync()) return false;
+        uint32_t got = 0;
+        for (uint32_t i = rank; i < n; i += size) {
+            if (s.color[i] != NO_COLOR) continue;
+            const unsigned long long key = tag | priority_hash(i);
+            const uint32_t bA = w.cbody[m[i].a], bB = w.cbody[m[i].b];
+            const bool okA = !(__ldcg(&w.bvel[bA].w) > 0.0f) || __ldcg(s.bodyMax + bA) == key;
+            const bool okB = !(__ldcg(&w.bvel[bB].w) > 0.0f) || __ldcg(s.bodyMax + bB) == key;
+            if (okA && okB) { s.color[i] = r; got++; }
+        }
+        for (int o = 16; o > 0; o >>= 1) got += __shfl_xor_sync(0xffffffffu, got, o);
+        if ((threadIdx.x & 31) == 0 && got) { atomicAdd(s.colorCount + r, got); atomicAdd(s.colorCount + MAX_COLORS, got); }
+        if (!sync()) return false;
+        done = __ldcg(s.colorCount + MAX_COLORS) >= n;
+    }
+    if (!done) { if (rank == 0) atomicOr(status, STATUS_COLOR_OVERFLOW); return false; }
+    if (rank == 0) {
+        uint32_t run = 0;
+        for (uint32_t c = 0; c < rounds; c++) { s.colorStart[c] = run; run += s.colorCount[c]; s.colorCount[c] = 0; }
+        s.colorStart[rounds] = run;
+        *outColors = rounds;
+    }
+    if (!sync()) return false;
+    for (uint32_t i = rank; i < n; i += size) {
+        const uint32_t c = s.color[i];
+        s.order[__ldcg(s.colorStart + c) + atomicAdd(s.colorCount + c, 1u)] = i;
+    }
+    if (!sync()) return false;
+    // Constraint build for every manifold before any velocity changes (computeConstraintData).
+    for (uint32_t c = rank; c < n; c += size) {
+        const uint32_t mi = __ldcg(s.order + c);
+        Constraint k;
+        prep_constraint(w, m[mi], mi, k);
+        s.cons[c] = k;
+    }
+    if (!sync()) return false;
+    for (uint32_t col = 0; col < rounds; col++) {
+        const uint32_t end = __ldcg(s.colorStart + col + 1);
+        for (uint32_t c = __ldcg(s.colorStart + col) + rank; c < end; c += size) warm_constraint(w, s.cons[c]);
+        if (!sync()) return false;
+    }
+    for (uint32_t it = 0; it < velIters; it++) {
+        for (uint32_t col = 0; col < rounds; col++) {
+            const uint32_t end = __ldcg(s.colorStart + col + 1);
+            for (uint32_t c = __ldcg(s.colorStart + col) + rank; c < end; c += size) {
+                Constraint k = s.cons[c];
+                velocity_constraint(w, k);
+                float4* imp = reinterpret_cast<float4*>(&s.cons[c].jn0);
+                *imp = make_float4(k.jn0, k.jt0, k.jn1, k.jt1);
+            }
+            if (!sync()) return false;
+        }
+    }
+    for (uint32_t it = 0; it < posIters; it++) {
+        for (uint32_t col = 0; col < rounds; col++) {
+            const uint32_t end = __ldcg(s.colorStart + col + 1);
+            for (uint32_t c = __ldcg(s.colorStart + col) + rank; c < end; c += size) position_constraint(w, s.cons[c]);
+            if (!sync()) return false;
+        }
+    }
+    for (uint32_t c = rank; c < n; c += size) {
+        const Constraint& k = s.cons[c];
+        Manifold& d = m[k.manifold];
+        d.jn0 = k.jn0; d.jt0 = k.jt0; d.jn1 = k.jn1; d.jt1 = k.jt1;
+    }
+    return true;
+}
+
+constexpr uint32_t SOLVE_CLUSTER_THREADS = 512;
+
+__global__ void __launch_bounds__(SOLVE_CLUSTER_THREADS, 1)
+k_color_solve_cluster(DeviceWorld w, Manifold* m, const uint32_t* nM, SolveScratch s, uint32_t velIters,
+                      uint32_t posIters, StepCounters* counters);
+__global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* nM, SolveScratch s, uint32_t velIters,
+                                   uint32_t posIters, uint32_t* bar, StepCounters* counters);
+
+}  // namespace ag2d

@@ -1,11 +1,14 @@
 // C ABI of libag2d.so (include/ag2d.h): world lifecycle, object creation, the per-step launch sequence, field
 // access and phase-level taps. Host code; every kernel it launches is in k_spatial.cu / k_contact.cu.
 #include "ag2d.h"
-#include "ag2d_kernels.cuh"
+#include "ag2d_solver.cuh"
 #include "host_objects.hpp"
 
 #include <algorithm>
+#include <chrono>
+#include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -141,8 +144,12 @@ struct Tree {
 
 struct DeviceInfo {
     int sms = 0;
-    int coopColorBlocks = 0, coopSolveBlocks = 0;
+    int coopSolveBlocks = 0;   // co-resident CTAs of the grid solver
+    int solveCluster = 0;      // CTAs per cluster of the cluster solver (16 when the device allows it)
 };
+
+// Manifold count above which the solver runs on the whole grid instead of one cluster.
+constexpr uint32_t GRID_SOLVE_THRESHOLD = 600000;
 
 }  // namespace
 
@@ -211,6 +218,8 @@ struct ag2d_world {
     double phaseMs[NPHASE] = {};
     uint64_t phaseCalls[NPHASE] = {};
     uint64_t launches = 0;
+    uint64_t listRebuilds = 0, retries = 0, regrows = 0;
+    double hostMs = 0.0, syncMs = 0.0;
 
     void pbegin(int p)
     {
@@ -276,10 +285,36 @@ struct ag2d_world {
         CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         CK(cudaDeviceGetAttribute(&dev.sms, cudaDevAttrMultiProcessorCount, s.device));
         int perSm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color, 256, 0));
-        dev.coopColorBlocks = std::max(1, perSm) * dev.sms;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_solve, 256, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color_solve_grid, 256, 0));
         dev.coopSolveBlocks = std::max(1, perSm) * dev.sms;
+        // Largest cluster (16 non-portable, else 8) that can be resident.
+        dev.solveCluster = 1;
+        if (cudaFuncSetAttribute(k_color_solve_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+            cudaSuccess) {
+            for (int cl : {16, 8, 4, 2}) {
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3(cl);
+                cfg.blockDim = dim3(SOLVE_CLUSTER_THREADS);
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = cl;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                int clusters = 0;
+                if (cudaOccupancyMaxActiveClusters(&clusters, k_color_solve_cluster, &cfg) == cudaSuccess &&
+                    clusters >= 1) {
+                    dev.solveCluster = cl;
+                    break;
+                }
+            }
+        }
+        cudaGetLastError();
+        // AG2D_SOLVER=grid forces the whole-grid solver (test hook for that variant).
+        if (const char* v = std::getenv("AG2D_SOLVER")) {
+            if (std::string(v) == "grid") dev.solveCluster = 1;
+        }
         CK(cudaMallocHost(reinterpret_cast<void**>(&hCounters), sizeof(StepCounters)));
         std::memset(hCounters, 0, sizeof(StepCounters));
         dCounters.reserve(1);
@@ -295,6 +330,7 @@ struct ag2d_world {
 
     void reserveCapacities(uint32_t pairCapNew, uint32_t manCapNew)
     {
+        regrows++;
         pairCap = pairCapNew;
         manifoldCap = manCapNew;
         pairs.reserve(pairCap);
@@ -421,6 +457,7 @@ struct ag2d_world {
 
     void rebuildLists()
     {
+        listRebuilds++;
         const cudaStream_t s = stream;
         const uint32_t nmax = std::max(nBodies, nColliders);
         k_state_flags<<<gridFor(nmax), 256, 0, s>>>(bstate.p, cbody.p, nBodies, nColliders, flagA.p, flagB.p, flagC.p);
@@ -605,34 +642,38 @@ struct ag2d_world {
         const cudaStream_t s = stream;
         CK(cudaMemsetAsync(bodyMax.p, 0, sizeof(unsigned long long) * std::max<uint32_t>(nBodies, 1), s));
         CK(cudaMemsetAsync(bar.p, 0, 2 * sizeof(uint32_t), s));
-        const uint32_t est = std::min<uint32_t>(manifoldCap, lastManifolds + lastManifolds / 2 + 1024);
         DeviceWorld w = view();
-        const Manifold* mc = manifolds.p;
+        Manifold* mm = manifolds.p;
         const uint32_t* nm = nManifolds.p;
-        uint32_t* colorp = color.p;
-        unsigned long long* bmax = bodyMax.p;
-        uint32_t *ccount = colorCount.p, *cstart = colorStart.p, *ord = order.p, *barp = bar.p;
+        SolveScratch scratch{color.p, order.p, bodyMax.p, colorCount.p, colorStart.p, cons.p};
+        uint32_t vi = settings.velocity_iterations, pi = settings.position_iterations;
         StepCounters* ctr = dCounters.p;
-        {
-            const int grid = std::max(1, std::min<int>(dev.coopColorBlocks, int(div_up(est, 256))));
-            void* args[] = {&w, &mc, &nm, &colorp, &bmax, &ccount, &cstart, &ord, &barp, &ctr};
-            pbegin(9);
-            CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_color), dim3(grid), dim3(256), args, 0, s));
-            pend(9);
-            launches++;
-        }
-        CK(cudaMemsetAsync(bar.p, 0, 2 * sizeof(uint32_t), s));
-        {
-            Manifold* mm = manifolds.p;
-            Constraint* cp = cons.p;
-            uint32_t vi = settings.velocity_iterations, pi = settings.position_iterations;
+        pbegin(10);
+        if (lastManifolds <= GRID_SOLVE_THRESHOLD && dev.solveCluster > 1) {
+            // One thread-block cluster, hardware barriers between colours.
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(dev.solveCluster);
+            cfg.blockDim = dim3(SOLVE_CLUSTER_THREADS);
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = dev.solveCluster;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            CK(cudaLaunchKernelEx(&cfg, k_color_solve_cluster, w, mm, nm, scratch, vi, pi, ctr));
+        } else {
+            // Whole-grid cooperative launch with the bounded software barrier.
+            uint32_t* barp = bar.p;
+            const uint32_t est = std::min<uint32_t>(manifoldCap, lastManifolds + lastManifolds / 2 + 1024);
             const int grid = std::max(1, std::min<int>(dev.coopSolveBlocks, int(div_up(est, 256))));
-            void* args[] = {&w, &mm, &nm, &ord, &cstart, &cp, &vi, &pi, &barp, &ctr};
-            pbegin(10);
-            CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_solve), dim3(grid), dim3(256), args, 0, s));
-            pend(10);
-            launches++;
+            void* args[] = {&w, &mm, &nm, &scratch, &vi, &pi, &barp, &ctr};
+            CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_color_solve_grid), dim3(grid), dim3(256), args,
+                                           0, s));
         }
+        pend(10);
+        launches++;
     }
 
     void phaseIslands()
@@ -653,7 +694,9 @@ struct ag2d_world {
     void readCounters()
     {
         CK(cudaMemcpyAsync(hCounters, dCounters.p, sizeof(StepCounters), cudaMemcpyDeviceToHost, stream));
+        const auto t0 = std::chrono::steady_clock::now();
         CK(cudaStreamSynchronize(stream));
+        syncMs += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         pcollect();
     }
 
@@ -672,8 +715,15 @@ struct ag2d_world {
     // One fixed step (Simulation::physicsStep order, Simulation.cpp:255-351).
     void stepOnce()
     {
+        const auto tStart = std::chrono::steady_clock::now();
+        struct HostTimer {
+            double& acc;
+            std::chrono::steady_clock::time_point t0;
+            ~HostTimer() { acc += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); }
+        } hostTimer{hostMs, tStart};
         ensureUploaded();
         for (int attempt = 0; attempt < 8; attempt++) {
+            if (attempt > 0) retries++;
             if (listsDirty) rebuildLists();
             const cudaStream_t s = stream;
             CK(cudaMemsetAsync(dCounters.p, 0, sizeof(StepCounters), s));
@@ -936,6 +986,11 @@ int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out)
         out->sleeping = world->nBodies - world->nDynBody - world->nStatic;
         out->steps = world->stepsTaken;
         out->launches = world->launches;
+        out->list_rebuilds = world->listRebuilds;
+        out->retries = world->retries;
+        out->regrows = world->regrows;
+        out->host_ms = world->hostMs;
+        out->sync_ms = world->syncMs;
     });
 }
 
