@@ -192,9 +192,20 @@ int32_t ag2d_world_write(ag2d_world* world, int32_t field, const void* src, uint
 /* Runs one phase (enum ag2d_phase) on the current device state. */
 int32_t ag2d_world_run_phase(ag2d_world* world, int32_t phase);
 
-/* ---- batched worlds: many independent worlds advanced by one launch sequence per step ---- */
+/* ---- batched worlds: many independent worlds advanced by one launch sequence per step ----
+ * The reference runs one Simulation per world (Simulation.h:36); a batch packs the current state of several
+ * worlds (same step settings) into one world-segmented device state: per-world Morton bounds, per-world trees,
+ * per-world colouring and solve. Each world's result equals what it gets when stepped alone. The source worlds
+ * are copied, not moved, and are not advanced by the batch. */
 int32_t ag2d_batch_create(ag2d_world* const* worlds, uint32_t world_count, ag2d_batch** out_batch);
 int32_t ag2d_batch_step(ag2d_batch* batch, int32_t steps);
+int32_t ag2d_batch_world_count(ag2d_batch* batch, uint32_t* out_count);
+/* The engine instance of the batch, for ag2d_world_counters / _stream / _set_profiling / _phase_times and
+ * whole-batch reads. Owned by the batch: do not destroy it or add bodies through it. */
+int32_t ag2d_batch_engine(ag2d_batch* batch, ag2d_world** out_world);
+/* Reads a body field, a collider field or the manifolds of one world of the batch, in that world's own indices. */
+int32_t ag2d_batch_read(ag2d_batch* batch, uint32_t world, int32_t field, void* dst, uint64_t capacity_bytes,
+                        uint64_t* out_bytes);
 int32_t ag2d_batch_destroy(ag2d_batch* batch);
 
 #ifdef __cplusplus

@@ -117,6 +117,9 @@ def _load():
     L.ag2d_world_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.ag2d_batch_create.argtypes = [ctypes.POINTER(vp), u32, ctypes.POINTER(vp)]
     L.ag2d_batch_step.argtypes = [vp, i32]
+    L.ag2d_batch_engine.argtypes = [vp, ctypes.POINTER(vp)]
+    L.ag2d_batch_world_count.argtypes = [vp, ctypes.POINTER(u32)]
+    L.ag2d_batch_read.argtypes = [vp, u32, i32, vp, u64, ctypes.POINTER(u64)]
     L.ag2d_batch_destroy.argtypes = [vp]
     return L
 
@@ -159,9 +162,20 @@ class World:
         self.settings = s
         self._keep = []
 
+    @classmethod
+    def _borrowed(cls, handle, owner):
+        """A non-owning view of an engine instance owned by 'owner' (a Batch)."""
+        w = cls.__new__(cls)
+        w.h = handle
+        w.settings = None
+        w._keep = []
+        w._owner = owner
+        return w
+
     def close(self):
         if getattr(self, "h", None):
-            lib.ag2d_world_destroy(self.h)
+            if getattr(self, "_owner", None) is None:
+                lib.ag2d_world_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -317,20 +331,41 @@ class World:
 
 
 class Batch:
-    """Many independent worlds advanced together (one launch sequence per step for all of them)."""
+    """Many independent worlds advanced together: their current states are packed into one world-segmented
+    engine instance stepped by one launch sequence per step. The source worlds are copied, not advanced."""
 
     def __init__(self, worlds):
-        self.worlds = list(worlds)
-        arr = (ctypes.c_void_p * len(self.worlds))(*[w.h for w in self.worlds])
+        worlds = list(worlds)
+        arr = (ctypes.c_void_p * len(worlds))(*[w.h for w in worlds])
         h = ctypes.c_void_p()
-        _check(lib.ag2d_batch_create(arr, len(self.worlds), ctypes.byref(h)))
+        _check(lib.ag2d_batch_create(arr, len(worlds), ctypes.byref(h)))
         self.h = h
+        self.n_worlds = len(worlds)
+        e = ctypes.c_void_p()
+        _check(lib.ag2d_batch_engine(self.h, ctypes.byref(e)))
+        self.engine = World._borrowed(e, self)
 
     def step(self, steps: int = 1):
         _check(lib.ag2d_batch_step(self.h, steps))
 
+    def read(self, world: int, field: int) -> np.ndarray:
+        """A body field, collider field or the manifolds of one world, in that world's own indices."""
+        n = ctypes.c_uint64()
+        _check(lib.ag2d_batch_read(self.h, world, field, None, 0, ctypes.byref(n)))
+        buf = np.empty(int(n.value), dtype=np.uint8)
+        _check(lib.ag2d_batch_read(self.h, world, field, buf.ctypes.data if buf.size else None, buf.size,
+                                   ctypes.byref(n)))
+        if field in (MANIFOLDS, PREV_MANIFOLDS):
+            return buf.view(MANIFOLD_DTYPE)
+        return buf.view(np.uint32 if field in _U32_FIELDS else np.float32)
+
+    def counters(self) -> dict:
+        return self.engine.counters()
+
     def close(self):
         if getattr(self, "h", None):
+            if getattr(self, "engine", None) is not None:
+                self.engine.h = None
             lib.ag2d_batch_destroy(self.h)
             self.h = None
 

@@ -25,7 +25,7 @@ CUDA_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-prec-div=true"
               "-Xcompiler", "-fPIC,-ffp-contract=off", f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
 CU_SOURCES = ["k_spatial.cu", "k_contact.cu", "k_batch.cu", "capi.cu"]
 CPP_SOURCES = ["host_objects.cpp"]
-HEADERS = ["ag2d_math.cuh", "ag2d_world.cuh", "ag2d_kernels.cuh", "host_objects.hpp"]
+HEADERS = ["ag2d_math.cuh", "ag2d_world.cuh", "ag2d_kernels.cuh", "ag2d_solver.cuh", "host_objects.hpp"]
 
 
 def _newer(src_paths, dst):

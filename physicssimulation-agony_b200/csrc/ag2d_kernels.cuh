@@ -16,31 +16,47 @@ constexpr int QUERY_STACK = 64;
 constexpr uint32_t MAX_COLORS = 256;
 constexpr uint32_t NO_COLOR = 0xFFFFFFFFu;
 
-// Read-only view of one LBVH (n leaves; n - 1 internal nodes, root 0).
+// Read-only view of one LBVH over n leaves in sorted order. A single tree has n - 1 internal nodes and root 0; a
+// world-segmented tree (sortedWorld non-null) holds one tree per world segment [segStart[w], segStart[w + 1]),
+// rooted at internal node segStart[w].
 struct TreeView {
     int n;
     const int2* child;
     const int2* range;
     const float4* nodeAabb;
-    const float4* leafAabb;   // AABBs in sorted (leaf) order
-    const uint32_t* vals;     // collider index of each leaf
+    const float4* leafAabb;       // AABBs in sorted (leaf) order
+    const uint32_t* vals;         // collider index of each leaf
+    const uint32_t* sortedWorld;  // world of each leaf, or null (one world)
+    const uint32_t* segStart;     // [worlds + 1] segment starts, or null (one world)
 };
 
 // Spatial kernels (k_spatial.cu).
-__global__ void k_integrate(DeviceWorld w, const uint32_t* dynBody, uint32_t nDyn, float dt, float gx, float gy,
-                            float dampHalf);
-__global__ void k_collider_pose(DeviceWorld w, const uint32_t* list, uint32_t n);
-__global__ void k_bounds_init(uint32_t* bounds);
-__global__ void k_bounds(const float4* aabb, const uint32_t* list, uint32_t n, uint32_t* bounds);
-__global__ void k_morton(const float4* aabb, const uint32_t* list, uint32_t n, const uint32_t* bounds,
-                         uint32_t* keys, uint32_t* vals);
+__global__ void k_integrate(DeviceWorld w, const uint32_t* dynBody, const uint8_t* dynSimd, uint32_t nDyn, float dt,
+                            float gx, float gy, float dampHalf);
+__global__ void k_collider_pose(DeviceWorld w, const uint32_t* list, const uint8_t* listSimd, uint32_t n,
+                                const uint32_t* worldMask);
+__global__ void k_bounds_init(uint32_t* bounds, uint32_t worlds);
+__global__ void k_bounds(const float4* aabb, const uint32_t* list, uint32_t n, const uint32_t* colWorld,
+                         uint32_t* bounds);
+__global__ void k_count_world(const uint32_t* list, uint32_t n, const uint32_t* elemWorld, uint32_t* counts);
+__global__ void k_simd_flags(const uint32_t* list, uint32_t n, const uint32_t* offsets, uint32_t nElems,
+                             const uint32_t* elemWorld, const uint32_t* worldStart, uint32_t worlds, uint8_t* simd);
+__global__ void k_morton(const float4* aabb, const uint32_t* list, uint32_t n, const uint32_t* colWorld,
+                         const uint32_t* bounds, uint32_t* keys, uint32_t* vals, uint32_t* keyOf);
+__global__ void k_world_keys(const uint32_t* vals, uint32_t n, const uint32_t* colWorld, uint32_t* keys);
+__global__ void k_seg_starts(const uint32_t* offsets, const uint32_t* worldStart, uint32_t worlds, uint32_t nElems,
+                             const uint32_t* total, uint32_t* segStart);
+__global__ void k_manifold_segments(const Manifold* m, const uint32_t* nM, const uint32_t* cbody,
+                                    const uint32_t* bodyWorld, uint32_t worlds, uint32_t* segStart);
+__global__ void k_tree_gather(const uint32_t* vals, uint32_t n, const uint32_t* keyOf, const uint32_t* colWorld,
+                              const float4* caabb, uint32_t* sortedKey, uint32_t* sortedWorld, float4* leafAabb);
 __global__ void k_sort_histogram(const uint32_t* keys, uint32_t n, uint32_t* hist);
 __global__ void k_sort_digit_scan(uint32_t* hist);
 __global__ void k_sort_pass(const uint32_t* keysIn, const uint32_t* valsIn, uint32_t* keysOut, uint32_t* valsOut,
                             uint32_t n, uint32_t shift, const uint32_t* digitBase, uint32_t* tileState,
                             uint32_t* tileCounter, uint32_t* status);
-__global__ void k_lbvh_build(const uint32_t* keys, const uint32_t* vals, int n, const float4* caabb, int2* child,
-                             int2* range, int* parent, int* leafParent, float4* leafAabb, uint32_t* visit);
+__global__ void k_lbvh_build(const uint32_t* keys, const uint32_t* sortedWorld, const uint32_t* segStart, int n,
+                             int2* child, int2* range, int* parent, int* leafParent, uint32_t* visit);
 __global__ void k_lbvh_refit(int n, const int2* child, const int* parent, const int* leafParent,
                              const float4* leafAabb, float4* nodeAabb, uint32_t* visit);
 __global__ void k_query_count(TreeView dyn, TreeView other, const uint32_t* cbody, uint32_t* counts,

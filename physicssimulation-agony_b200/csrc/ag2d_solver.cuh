@@ -225,16 +225,21 @@ struct SolveScratch {
     Constraint* cons;                 // [manifolds]
 };
 
+// Team barriers. ld() reads a colour counter written by other team members before the last barrier: global memory
+// through L2 for the multi-CTA teams, shared memory for one CTA.
 struct ClusterSync {
     __device__ __forceinline__ bool operator()() const { cg::this_cluster().sync(); return true; }
+    static __device__ __forceinline__ uint32_t ld(const uint32_t* p) { return __ldcg(p); }
 };
 struct BlockSync {
     __device__ __forceinline__ bool operator()() const { __syncthreads(); return true; }
+    static __device__ __forceinline__ uint32_t ld(const uint32_t* p) { return *static_cast<const volatile uint32_t*>(p); }
 };
 struct GridSync {
     uint32_t* bar;
     uint32_t* status;
     __device__ __forceinline__ bool operator()() const { return grid_barrier(bar, status); }
+    static __device__ __forceinline__ uint32_t ld(const uint32_t* p) { return __ldcg(p); }
 };
 
 // Colouring (Luby / Jones-Plassmann rounds: colour r goes to every uncoloured manifold whose priority is the largest
@@ -273,19 +278,19 @@ __device__ bool color_and_solve(const DeviceWorld& w, Manifold* __restrict__ m, 
         for (int o = 16; o > 0; o >>= 1) got += __shfl_xor_sync(0xffffffffu, got, o);
         if ((threadIdx.x & 31) == 0 && got) { atomicAdd(s.colorCount + r, got); atomicAdd(s.colorCount + MAX_COLORS, got); }
         if (!sync()) return false;
-        done = __ldcg(s.colorCount + MAX_COLORS) >= n;
+        done = Sync::ld(s.colorCount + MAX_COLORS) >= n;
     }
     if (!done) { if (rank == 0) atomicOr(status, STATUS_COLOR_OVERFLOW); return false; }
     if (rank == 0) {
         uint32_t run = 0;
         for (uint32_t c = 0; c < rounds; c++) { s.colorStart[c] = run; run += s.colorCount[c]; s.colorCount[c] = 0; }
         s.colorStart[rounds] = run;
-        *outColors = rounds;
+        atomicMax(outColors, rounds);
     }
     if (!sync()) return false;
     for (uint32_t i = rank; i < n; i += size) {
         const uint32_t c = s.color[i];
-        s.order[__ldcg(s.colorStart + c) + atomicAdd(s.colorCount + c, 1u)] = i;
+        s.order[Sync::ld(s.colorStart + c) + atomicAdd(s.colorCount + c, 1u)] = i;
     }
     if (!sync()) return false;
     // Constraint build for every manifold before any velocity changes (computeConstraintData).
@@ -297,14 +302,14 @@ __device__ bool color_and_solve(const DeviceWorld& w, Manifold* __restrict__ m, 
     }
     if (!sync()) return false;
     for (uint32_t col = 0; col < rounds; col++) {
-        const uint32_t end = __ldcg(s.colorStart + col + 1);
-        for (uint32_t c = __ldcg(s.colorStart + col) + rank; c < end; c += size) warm_constraint(w, s.cons[c]);
+        const uint32_t end = Sync::ld(s.colorStart + col + 1);
+        for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) warm_constraint(w, s.cons[c]);
         if (!sync()) return false;
     }
     for (uint32_t it = 0; it < velIters; it++) {
         for (uint32_t col = 0; col < rounds; col++) {
-            const uint32_t end = __ldcg(s.colorStart + col + 1);
-            for (uint32_t c = __ldcg(s.colorStart + col) + rank; c < end; c += size) {
+            const uint32_t end = Sync::ld(s.colorStart + col + 1);
+            for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) {
                 Constraint k = s.cons[c];
                 velocity_constraint(w, k);
                 float4* imp = reinterpret_cast<float4*>(&s.cons[c].jn0);
@@ -315,8 +320,8 @@ __device__ bool color_and_solve(const DeviceWorld& w, Manifold* __restrict__ m, 
     }
     for (uint32_t it = 0; it < posIters; it++) {
         for (uint32_t col = 0; col < rounds; col++) {
-            const uint32_t end = __ldcg(s.colorStart + col + 1);
-            for (uint32_t c = __ldcg(s.colorStart + col) + rank; c < end; c += size) position_constraint(w, s.cons[c]);
+            const uint32_t end = Sync::ld(s.colorStart + col + 1);
+            for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) position_constraint(w, s.cons[c]);
             if (!sync()) return false;
         }
     }
@@ -335,5 +340,13 @@ k_color_solve_cluster(DeviceWorld w, Manifold* m, const uint32_t* nM, SolveScrat
                       uint32_t posIters, StepCounters* counters);
 __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* nM, SolveScratch s, uint32_t velIters,
                                    uint32_t posIters, uint32_t* bar, StepCounters* counters);
+
+// Batched worlds: one CTA per world (taken from a work counter in 'worldOrder' order, largest worlds first), the
+// colour counters in shared memory and __syncthreads between colours.
+constexpr uint32_t SOLVE_WORLD_THREADS = 256;
+__global__ void __launch_bounds__(SOLVE_WORLD_THREADS)
+k_color_solve_worlds(DeviceWorld w, Manifold* m, const uint32_t* segStart, const uint32_t* worldOrder,
+                     uint32_t worlds, SolveScratch s, uint32_t velIters, uint32_t posIters, uint32_t* nextWorld,
+                     StepCounters* counters);
 
 }  // namespace ag2d

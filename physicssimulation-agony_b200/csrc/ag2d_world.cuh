@@ -96,6 +96,14 @@ struct DeviceWorld {
     float2* polyNormals;
     // Materials: elasticity, static friction, dynamic friction.
     float4* materials;
+    // World partition of a batch (null for a single world): world of each body / collider and the first body /
+    // collider of each world ([nWorlds + 1]).
+    uint32_t nWorlds;
+    uint32_t* bodyWorld;
+    uint32_t* colWorld;
+    uint32_t* worldBodyStart;
+    uint32_t* worldColStart;
+    uint32_t* worldDirty;   // set when a body of the world woke or fell asleep this step
 };
 
 __host__ __device__ __forceinline__ uint32_t shape_type(uint32_t packed) { return packed >> 30; }

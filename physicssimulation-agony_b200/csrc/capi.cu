@@ -130,22 +130,68 @@ struct Tree {
     DBuf<int> parent, leafParent;
     DBuf<float4> leafAabb, nodeAabb;
     DBuf<uint32_t> visit, bounds, hist, tileState, tileCounter;
+    // World-segmented trees: Morton key per collider, sorted keys / worlds, segment starts (filled with the lists).
+    DBuf<uint32_t> keyOf, sortedKey, sortedWorld, segStart;
+    uint32_t worlds = 1;
     int n = 0;
-    void reserve(uint32_t cap)
+    void reserve(uint32_t cap, uint32_t nWorlds)
     {
+        worlds = nWorlds;
         keys.reserve(cap); vals.reserve(cap); keys2.reserve(cap); vals2.reserve(cap);
         child.reserve(cap); range.reserve(cap); parent.reserve(cap); leafParent.reserve(cap);
         leafAabb.reserve(cap); nodeAabb.reserve(cap); visit.reserve(cap);
-        bounds.reserve(4); hist.reserve(4 * 256); tileCounter.reserve(4);
+        bounds.reserve(4 * size_t(nWorlds)); hist.reserve(4 * 256); tileCounter.reserve(4);
         tileState.reserve(size_t(div_up(std::max<uint32_t>(cap, 1), SORT_TILE)) * 256 * 4);
+        if (nWorlds > 1) {
+            keyOf.reserve(cap); sortedKey.reserve(cap); sortedWorld.reserve(cap); segStart.reserve(nWorlds + 1);
+        }
     }
-    TreeView view() const { return TreeView{n, child.p, range.p, nodeAabb.p, leafAabb.p, vals.p}; }
+    TreeView view() const
+    {
+        const bool seg = worlds > 1;
+        return TreeView{n, child.p, range.p, nodeAabb.p, leafAabb.p, vals.p, seg ? sortedWorld.p : nullptr,
+                        seg ? segStart.p : nullptr};
+    }
 };
 
 struct DeviceInfo {
     int sms = 0;
     int coopSolveBlocks = 0;   // co-resident CTAs of the grid solver
     int solveCluster = 0;      // CTAs per cluster of the cluster solver (16 when the device allows it)
+    int worldSolveBlocks = 0;  // co-resident CTAs of the per-world solver
+};
+
+// One world's state in the upload format (host arrays), and the warm-start manifolds.
+struct PackedArrays {
+    std::vector<float4> vel, pos, co, mats;
+    std::vector<float2> rot, bh, pv, pn;
+    std::vector<float> wc, br, st, cr;
+    std::vector<uint8_t> state;
+    std::vector<uint32_t> isl, cb, cs, cm, po, pc;
+    std::vector<Manifold> prev;
+
+    // Appends another world, shifting its body, collider, shape, vertex and material indices past this one's.
+    void append(const PackedArrays& o)
+    {
+        const uint32_t bo = uint32_t(vel.size()), cof = uint32_t(cb.size()), circ = uint32_t(cr.size());
+        const uint32_t box = uint32_t(bh.size()), poly = uint32_t(po.size()), vert = uint32_t(pv.size());
+        const uint32_t mat = uint32_t(mats.size());
+        auto cat = [](auto& d, const auto& s) { d.insert(d.end(), s.begin(), s.end()); };
+        cat(vel, o.vel); cat(pos, o.pos); cat(rot, o.rot); cat(wc, o.wc); cat(br, o.br); cat(st, o.st);
+        cat(state, o.state);
+        for (uint32_t v : o.isl) isl.push_back(v == 0xFFFFFFFFu ? v : v + bo);
+        for (uint32_t v : o.cb) cb.push_back(v + bo);
+        for (uint32_t v : o.cs) {
+            const uint32_t type = shape_type(v), idx = shape_index(v);
+            const uint32_t base = type == SHAPE_CIRCLE ? circ : (type == SHAPE_BOX ? box : poly);
+            cs.push_back((type << 30) | (idx + base));
+        }
+        for (uint32_t v : o.cm) cm.push_back(v + mat);
+        cat(co, o.co); cat(cr, o.cr); cat(bh, o.bh);
+        for (uint32_t v : o.po) po.push_back(v + vert);
+        cat(pc, o.pc); cat(pv, o.pv); cat(pn, o.pn); cat(mats, o.mats);
+        for (Manifold m : o.prev) { m.a += cof; m.b += cof; prev.push_back(m); }
+    }
 };
 
 // Manifold count above which the solver runs on the whole grid instead of one cluster.
@@ -205,6 +251,13 @@ struct ag2d_world {
     DBuf<Constraint> cons;
     // Islands.
     DBuf<uint32_t> ufParent, ufFlag, wakeIsland;
+    // World partition of a batch (nWorlds == 1: a single world, none of these is used).
+    uint32_t nWorlds = 1;
+    std::vector<uint32_t> hBodyStart, hColStart;     // [nWorlds + 1]
+    DBuf<uint32_t> bodyWorld, colWorld, worldBodyStart, worldColStart, worldOrder, manSeg, nextWorld, worldDirty;
+    DBuf<uint8_t> dynSimd, dynColSimd;               // SIMD-path flag of each work-list entry
+    // Shape table sizes of the last upload.
+    uint32_t nCircles = 0, nBoxes = 0, nPolygons = 0, nPolyVerts = 0, nMaterialRows = 0;
     // Counters.
     DBuf<StepCounters> dCounters;
     StepCounters* hCounters = nullptr;
@@ -255,7 +308,51 @@ struct ag2d_world {
         w.cworldRot = cworldRot.p; w.caabb = caabb.p;
         w.circleRadius = circleRadius.p; w.boxHalf = boxHalf.p; w.polyOffset = polyOffset.p; w.polyCount = polyCount.p;
         w.polyVerts = polyVerts.p; w.polyNormals = polyNormals.p; w.materials = materials.p;
+        const bool seg = nWorlds > 1;
+        w.nWorlds = nWorlds;
+        w.bodyWorld = seg ? bodyWorld.p : nullptr;
+        w.colWorld = seg ? colWorld.p : nullptr;
+        w.worldBodyStart = seg ? worldBodyStart.p : nullptr;
+        w.worldColStart = seg ? worldColStart.p : nullptr;
+        w.worldDirty = seg ? worldDirty.p : nullptr;
         return w;
+    }
+
+    // Installs the world partition of a batch: world k owns bodies [bodyStart[k], bodyStart[k + 1]) and colliders
+    // [colStart[k], colStart[k + 1]). Called after the arrays are uploaded.
+    void setPartition(const std::vector<uint32_t>& bodyStart, const std::vector<uint32_t>& colStart)
+    {
+        const cudaStream_t s = stream;
+        nWorlds = uint32_t(bodyStart.size() - 1);
+        hBodyStart = bodyStart;
+        hColStart = colStart;
+        std::vector<uint32_t> bw(nBodies), cw(nColliders), order(nWorlds);
+        for (uint32_t k = 0; k < nWorlds; k++) {
+            for (uint32_t i = bodyStart[k]; i < bodyStart[k + 1]; i++) bw[i] = k;
+            for (uint32_t i = colStart[k]; i < colStart[k + 1]; i++) cw[i] = k;
+            order[k] = k;
+        }
+        // Largest worlds first: the per-world solver takes worlds in this order, which balances its CTAs.
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+            return colStart[a + 1] - colStart[a] > colStart[b + 1] - colStart[b];
+        });
+        bodyWorld.upload(bw.data(), bw.size(), s);
+        colWorld.upload(cw.data(), cw.size(), s);
+        worldBodyStart.upload(bodyStart.data(), bodyStart.size(), s);
+        worldColStart.upload(colStart.data(), colStart.size(), s);
+        worldOrder.upload(order.data(), order.size(), s);
+        manSeg.reserve(nWorlds + 1);
+        nextWorld.reserve(1);
+        worldDirty.reserve(nWorlds);
+        CK(cudaMemsetAsync(worldDirty.p, 0, sizeof(uint32_t) * nWorlds, s));
+        dynSimd.reserve(std::max(nBodies, nColliders));
+        dynColSimd.reserve(std::max(nBodies, nColliders));
+        dynTree.reserve(nColliders, nWorlds);
+        otherTree.reserve(nColliders, nWorlds);
+        CK(cudaStreamSynchronize(s));
+        listsDirty = true;
+        otherDirty = true;
+        fullPose = true;
     }
 
     ~ag2d_world()
@@ -287,6 +384,8 @@ struct ag2d_world {
         int perSm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color_solve_grid, 256, 0));
         dev.coopSolveBlocks = std::max(1, perSm) * dev.sms;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color_solve_worlds, SOLVE_WORLD_THREADS, 0));
+        dev.worldSolveBlocks = std::max(1, perSm) * dev.sms;
         // Largest cluster (16 non-portable, else 8) that can be resident.
         dev.solveCluster = 1;
         if (cudaFuncSetAttribute(k_color_solve_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
@@ -433,8 +532,10 @@ struct ag2d_world {
         nStatic = uint32_t(std::count(state.begin(), state.end(), uint8_t(STATE_STATIC)));
         const uint32_t nmax = std::max(nBodies, nColliders);
         for (auto* b : {&dynBody, &dynCol, &otherCol, &flagA, &flagB, &flagC, &offA, &offB, &offC}) b->reserve(nmax);
-        dynTree.reserve(nColliders);
-        otherTree.reserve(nColliders);
+        dynTree.reserve(nColliders, nWorlds);
+        otherTree.reserve(nColliders, nWorlds);
+        nCircles = uint32_t(cr.size()); nBoxes = uint32_t(bh.size()); nPolygons = uint32_t(po.size());
+        nPolyVerts = uint32_t(pv.size()); nMaterialRows = uint32_t(mats.size());
         qCounts.reserve(nColliders); qOffsets.reserve(nColliders);
         bodyMax.reserve(nBodies);
         ufParent.reserve(nBodies); ufFlag.reserve(nBodies); wakeIsland.reserve(nBodies);
@@ -455,6 +556,31 @@ struct ag2d_world {
         if (hostDirty) upload();
     }
 
+    // The device state as upload-format host arrays plus the warm-start manifolds (for packing into a batch).
+    void exportArrays(PackedArrays& a)
+    {
+        ensureUploaded();
+        const cudaStream_t s = stream;
+        auto get = [&](auto& v, const auto* p, size_t n) {
+            v.resize(n);
+            if (n) CK(cudaMemcpyAsync(v.data(), p, n * sizeof(v[0]), cudaMemcpyDeviceToHost, s));
+        };
+        get(a.vel, bvel.p, nBodies); get(a.pos, bpos.p, nBodies); get(a.rot, brot.p, nBodies);
+        get(a.wc, wrapCount.p, nBodies); get(a.br, boundRadius.p, nBodies); get(a.st, sleepTimer.p, nBodies);
+        get(a.state, bstate.p, nBodies); get(a.isl, sleepIsland.p, nBodies);
+        get(a.cb, cbody.p, nColliders); get(a.cs, cshape.p, nColliders); get(a.cm, cmat.p, nColliders);
+        get(a.co, coff.p, nColliders);
+        get(a.cr, circleRadius.p, nCircles); get(a.bh, boxHalf.p, nBoxes);
+        get(a.po, polyOffset.p, nPolygons); get(a.pc, polyCount.p, nPolygons);
+        get(a.pv, polyVerts.p, nPolyVerts); get(a.pn, polyNormals.p, nPolyVerts);
+        get(a.mats, materials.p, nMaterialRows);
+        uint32_t np = 0;
+        CK(cudaMemcpyAsync(&np, nPrev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        get(a.prev, prevManifolds.p, np);
+        CK(cudaStreamSynchronize(s));
+    }
+
     void rebuildLists()
     {
         listRebuilds++;
@@ -469,12 +595,34 @@ struct ag2d_world {
         k_scatter_list<<<gridFor(nColliders), 256, 0, s>>>(flagB.p, offB.p, nColliders, dynCol.p);
         k_scatter_list<<<gridFor(nColliders), 256, 0, s>>>(flagC.p, offC.p, nColliders, otherCol.p);
         CK(cudaGetLastError());
+        if (nWorlds > 1) {
+            // World segments of both trees (the lists are world-grouped).
+            const uint32_t W = nWorlds;
+            k_seg_starts<<<gridFor(W + 1), 256, 0, s>>>(offB.p, worldColStart.p, W, nColliders, listCounts.p + 1,
+                                                        dynTree.segStart.p);
+            k_seg_starts<<<gridFor(W + 1), 256, 0, s>>>(offC.p, worldColStart.p, W, nColliders, listCounts.p + 2,
+                                                        otherTree.segStart.p);
+            CK(cudaGetLastError());
+            launches += 2;
+        }
         uint32_t counts[3] = {0, 0, 0};
         CK(cudaMemcpyAsync(counts, listCounts.p, sizeof(counts), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         nDynBody = counts[0];
         nDynCol = counts[1];
         nOther = counts[2];
+        if (nWorlds > 1) {
+            // SIMD-path flag of each entry: its rank within its world's part of the list against (count & ~7).
+            const uint32_t W = nWorlds;
+            if (nDynBody)
+                k_simd_flags<<<gridFor(nDynBody), 256, 0, s>>>(dynBody.p, nDynBody, offA.p, nBodies, bodyWorld.p,
+                                                               worldBodyStart.p, W, dynSimd.p);
+            if (nDynCol)
+                k_simd_flags<<<gridFor(nDynCol), 256, 0, s>>>(dynCol.p, nDynCol, offB.p, nColliders, colWorld.p,
+                                                              worldColStart.p, W, dynColSimd.p);
+            CK(cudaGetLastError());
+            launches += 2;
+        }
         listsDirty = false;
     }
 
@@ -505,47 +653,43 @@ struct ag2d_world {
         const float dampHalf = (damp >= 0.0f && damp < 1.0f) ? std::pow(damp, settings.dt * 0.5f) : 2.0f;
         if (nDynBody) {
             pbegin(0);
-            k_integrate<<<gridFor(nDynBody), 256, 0, stream>>>(view(), dynBody.p, nDynBody, settings.dt,
-                                                              settings.gravity_x, settings.gravity_y, dampHalf);
+            k_integrate<<<gridFor(nDynBody), 256, 0, stream>>>(view(), dynBody.p, nWorlds > 1 ? dynSimd.p : nullptr,
+                                                              nDynBody, settings.dt, settings.gravity_x,
+                                                              settings.gravity_y, dampHalf);
             CK(cudaGetLastError());
             pend(0);
             launches++;
         }
     }
 
-    void phasePose(bool full)
+    // full: every collider (or, with 'changedWorlds', those of the worlds whose bodies changed state this step).
+    void phasePose(bool full, bool changedWorlds = false)
     {
         const uint32_t n = full ? nColliders : nDynCol;
         if (n == 0) return;
         pbegin(1);
-        k_collider_pose<<<gridFor(n), 256, 0, stream>>>(view(), full ? nullptr : dynCol.p, n);
+        const uint32_t* mask = (full && changedWorlds && nWorlds > 1) ? worldDirty.p : nullptr;
+        k_collider_pose<<<gridFor(n), 256, 0, stream>>>(view(), full ? nullptr : dynCol.p,
+                                                         (full || nWorlds == 1) ? nullptr : dynColSimd.p, n, mask);
         CK(cudaGetLastError());
         pend(1);
         launches++;
     }
 
-    void buildTree(Tree& t, const uint32_t* list, uint32_t n)
+    // Radix passes over (keys, vals) for the digits [0, passes) with one histogram pass; the result ends in
+    // t.keys / t.vals (buffers swap after an odd number of passes).
+    void sortPasses(Tree& t, uint32_t n, uint32_t passes)
     {
         const cudaStream_t s = stream;
-        t.n = int(n);
-        if (n == 0) return;
-        launches += 11 + (n > 1 ? 1 : 0);
-        k_bounds_init<<<1, 32, 0, s>>>(t.bounds.p);
-        k_bounds<<<gridFor(n), 256, 0, s>>>(caabb.p, list, n, t.bounds.p);
-        k_morton<<<gridFor(n), 256, 0, s>>>(caabb.p, list, n, t.bounds.p, t.keys.p, t.vals.p);
-        CK(cudaGetLastError());
-        // Onesweep sort, 4 digit passes; results end in keys/vals.
         CK(cudaMemsetAsync(t.hist.p, 0, 4 * 256 * sizeof(uint32_t), s));
         k_sort_histogram<<<gridFor(n), 256, 0, s>>>(t.keys.p, n, t.hist.p);
         k_sort_digit_scan<<<4, 256, 0, s>>>(t.hist.p);
         CK(cudaGetLastError());
         const uint32_t tiles = div_up(n, SORT_TILE);
-        const bool isDyn = &t == &dynTree;
-        if (isDyn) pbegin(12);
-        CK(cudaMemsetAsync(t.tileState.p, 0, size_t(tiles) * 256 * 4 * sizeof(uint32_t), s));
+        CK(cudaMemsetAsync(t.tileState.p, 0, size_t(tiles) * 256 * passes * sizeof(uint32_t), s));
         CK(cudaMemsetAsync(t.tileCounter.p, 0, 4 * sizeof(uint32_t), s));
         uint32_t *ki = t.keys.p, *vi = t.vals.p, *ko = t.keys2.p, *vo = t.vals2.p;
-        for (uint32_t pass = 0; pass < 4; pass++) {
+        for (uint32_t pass = 0; pass < passes; pass++) {
             k_sort_pass<<<tiles, SORT_THREADS, 0, s>>>(ki, vi, ko, vo, n, pass * 8, t.hist.p + pass * 256,
                                                         t.tileState.p + size_t(pass) * tiles * 256,
                                                         t.tileCounter.p + pass, &dCounters.p->status);
@@ -553,10 +697,49 @@ struct ag2d_world {
             std::swap(ki, ko);
             std::swap(vi, vo);
         }
+        if (passes & 1) {
+            swap_bufs(t.keys, t.keys2);
+            swap_bufs(t.vals, t.vals2);
+        }
+        launches += 2 + passes;
+    }
+
+    // Tree over the colliders of 'list' (Morton keys from the world's bounds, sorted, Karras build, refit). With
+    // several worlds the order is (world, Morton key) and every world gets its own tree over its segment.
+    void buildTree(Tree& t, const uint32_t* list, uint32_t n)
+    {
+        const cudaStream_t s = stream;
+        t.n = int(n);
+        if (n == 0) return;
+        const uint32_t W = nWorlds;
+        const bool seg = W > 1;
+        const uint32_t* cw = seg ? colWorld.p : nullptr;
+        launches += 5 + (n > 1 ? 1 : 0);
+        k_bounds_init<<<gridFor(W), 256, 0, s>>>(t.bounds.p, W);
+        k_bounds<<<gridFor(n), 256, 0, s>>>(caabb.p, list, n, cw, t.bounds.p);
+        k_morton<<<gridFor(n), 256, 0, s>>>(caabb.p, list, n, cw, t.bounds.p, t.keys.p, t.vals.p,
+                                             seg ? t.keyOf.p : nullptr);
+        CK(cudaGetLastError());
+        const bool isDyn = &t == &dynTree;
+        if (isDyn) pbegin(12);
+        sortPasses(t, n, 4);
+        if (seg) {
+            // Stable passes on the world id: order (world, Morton key, collider).
+            uint32_t passes = 1;
+            while (passes < 4 && (W - 1) >> (8 * passes)) passes++;
+            k_world_keys<<<gridFor(n), 256, 0, s>>>(t.vals.p, n, colWorld.p, t.keys.p);
+            CK(cudaGetLastError());
+            launches++;
+            sortPasses(t, n, passes);
+        }
         if (isDyn) pend(12);
         if (isDyn) pbegin(13);
-        k_lbvh_build<<<gridFor(n), 256, 0, s>>>(t.keys.p, t.vals.p, int(n), caabb.p, t.child.p, t.range.p,
-                                                 t.parent.p, t.leafParent.p, t.leafAabb.p, t.visit.p);
+        k_tree_gather<<<gridFor(n), 256, 0, s>>>(t.vals.p, n, seg ? t.keyOf.p : nullptr, cw, caabb.p,
+                                                  seg ? t.sortedKey.p : nullptr, seg ? t.sortedWorld.p : nullptr,
+                                                  t.leafAabb.p);
+        k_lbvh_build<<<gridFor(n), 256, 0, s>>>(seg ? t.sortedKey.p : t.keys.p, seg ? t.sortedWorld.p : nullptr,
+                                                 seg ? t.segStart.p : nullptr, int(n), t.child.p, t.range.p,
+                                                 t.parent.p, t.leafParent.p, t.visit.p);
         CK(cudaGetLastError());
         if (n > 1) {
             k_lbvh_refit<<<gridFor(n), 256, 0, s>>>(int(n), t.child.p, t.parent.p, t.leafParent.p, t.leafAabb.p,
@@ -649,7 +832,17 @@ struct ag2d_world {
         uint32_t vi = settings.velocity_iterations, pi = settings.position_iterations;
         StepCounters* ctr = dCounters.p;
         pbegin(10);
-        if (lastManifolds <= GRID_SOLVE_THRESHOLD && dev.solveCluster > 1) {
+        if (nWorlds > 1) {
+            // One CTA per world over the world-grouped manifold list.
+            CK(cudaMemsetAsync(nextWorld.p, 0, sizeof(uint32_t), s));
+            k_manifold_segments<<<gridFor(manifoldCap), 256, 0, s>>>(mm, nm, cbody.p, bodyWorld.p, nWorlds,
+                                                                      manSeg.p);
+            const uint32_t grid = std::min<uint32_t>(nWorlds, uint32_t(dev.worldSolveBlocks));
+            k_color_solve_worlds<<<grid, SOLVE_WORLD_THREADS, 0, s>>>(w, mm, manSeg.p, worldOrder.p, nWorlds, scratch,
+                                                                      vi, pi, nextWorld.p, ctr);
+            CK(cudaGetLastError());
+            launches++;
+        } else if (lastManifolds <= GRID_SOLVE_THRESHOLD && dev.solveCluster > 1) {
             // One thread-block cluster, hardware barriers between colours.
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(dev.solveCluster);
@@ -742,6 +935,7 @@ struct ag2d_world {
             const uint32_t st = hCounters->status;
             if (st & (STATUS_PAIR_OVERFLOW | STATUS_MANIFOLD_OVERFLOW)) {
                 snapshot(true);
+                if (nWorlds > 1) CK(cudaMemsetAsync(worldDirty.p, 0, sizeof(uint32_t) * nWorlds, s));
                 fullPose = fullPoseThisStep;
                 otherDirty = true;
                 (void)otherDirtyThisStep;
@@ -773,13 +967,17 @@ struct ag2d_world {
                 // static + sleeping tree before the next step.
                 listsDirty = true;
                 otherDirty = true;
-                phasePose(true);
+                phasePose(true, true);
+                if (nWorlds > 1) CK(cudaMemsetAsync(worldDirty.p, 0, sizeof(uint32_t) * nWorlds, s));
                 rebuildLists();
             }
-            // Grow ahead of need.
+            // Grow ahead of need, geometrically (a reallocation synchronises the device).
             if (hCounters->pairs > pairCap / 2 || hCounters->manifolds > manifoldCap / 2) {
-                reserveCapacities(std::max<uint32_t>(pairCap, hCounters->pairs * 2),
-                                  std::max<uint32_t>(manifoldCap, hCounters->manifolds * 2));
+                const uint64_t p = hCounters->pairs > pairCap / 2 ? std::max<uint64_t>(2ull * pairCap, 2ull * hCounters->pairs) : pairCap;
+                const uint64_t m = hCounters->manifolds > manifoldCap / 2
+                                       ? std::max<uint64_t>(2ull * manifoldCap, 2ull * hCounters->manifolds)
+                                       : manifoldCap;
+                reserveCapacities(uint32_t(std::min<uint64_t>(p, 1ull << 30)), uint32_t(std::min<uint64_t>(m, 1ull << 30)));
             }
             stepsTaken++;
             return;
@@ -1103,7 +1301,8 @@ static std::vector<uint8_t> read_field(ag2d_world& w, int32_t field)
     case AG2D_COL_AABB_MAX_X: return comp4(w.caabb, nc, 2);
     case AG2D_COL_AABB_MAX_Y: return comp4(w.caabb, nc, 3);
     case AG2D_DYN_SORTED: return pack(download(w.dynTree.vals.p, uint32_t(w.dynTree.n), s));
-    case AG2D_DYN_MORTON: return pack(download(w.dynTree.keys.p, uint32_t(w.dynTree.n), s));
+    case AG2D_DYN_MORTON:
+        return pack(download(w.nWorlds > 1 ? w.dynTree.sortedKey.p : w.dynTree.keys.p, uint32_t(w.dynTree.n), s));
     case AG2D_PAIRS: {
         uint32_t n = 0;
         CK(cudaMemcpyAsync(&n, &w.dCounters.p->pairs, 4, cudaMemcpyDeviceToHost, s));
@@ -1230,19 +1429,66 @@ int32_t ag2d_world_run_phase(ag2d_world* world, int32_t phase)
 
 }  // extern "C"
 
-// Batches: the worlds step one after another here; the fused per-world-CTA path replaces this.
+// Batches: several worlds packed into one engine instance (world-segmented arrays, trees and solver), stepped by
+// one launch sequence per step. The source worlds are left as they were.
 struct ag2d_batch {
-    std::vector<ag2d_world*> worlds;
+    std::unique_ptr<ag2d_world> engine;
+    uint32_t worlds = 0;
 };
+
+static bool same_settings(const ag2d_world_settings& a, const ag2d_world_settings& b)
+{
+    return a.dt == b.dt && a.velocity_iterations == b.velocity_iterations &&
+           a.position_iterations == b.position_iterations && a.gravity_x == b.gravity_x &&
+           a.gravity_y == b.gravity_y && a.angular_damping == b.angular_damping && a.sleep_speed == b.sleep_speed &&
+           a.sleep_time == b.sleep_time && a.ccd == b.ccd && a.device == b.device;
+}
 
 extern "C" {
 
 int32_t ag2d_batch_create(ag2d_world* const* worlds, uint32_t count, ag2d_batch** out)
 {
     return guarded([&] {
-        if (!out || (!worlds && count)) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        if (!out || !worlds || count == 0) throw ApiError(AG2D_ERR_INVALID_ARG, "a batch needs at least one world");
+        for (uint32_t k = 0; k < count; k++) {
+            if (!worlds[k]) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+            if (!same_settings(worlds[k]->settings, worlds[0]->settings))
+                throw ApiError(AG2D_ERR_INVALID_ARG, "worlds of a batch must share their step settings");
+        }
+        CK(cudaSetDevice(worlds[0]->settings.device));
+        PackedArrays all;
+        std::vector<uint32_t> bodyStart{0}, colStart{0};
+        for (uint32_t k = 0; k < count; k++) {
+            PackedArrays one;
+            CK(cudaSetDevice(worlds[k]->settings.device));
+            worlds[k]->exportArrays(one);
+            all.append(one);
+            bodyStart.push_back(uint32_t(all.vel.size()));
+            colStart.push_back(uint32_t(all.cb.size()));
+        }
         std::unique_ptr<ag2d_batch> b(new ag2d_batch());
-        b->worlds.assign(worlds, worlds + count);
+        b->worlds = count;
+        b->engine.reset(new ag2d_world());
+        ag2d_world& e = *b->engine;
+        e.init(worlds[0]->settings);
+        e.nBodies = uint32_t(all.vel.size());
+        e.nColliders = uint32_t(all.cb.size());
+        e.nWorlds = count;
+        e.uploadArrays(all.vel, all.pos, all.rot, all.wc, all.br, all.st, all.state, all.isl, all.cb, all.cs, all.cm,
+                       all.co, all.cr, all.bh, all.po, all.pc, all.pv, all.pn, all.mats);
+        e.objects.materials.resize(size_t(all.mats.size()) * 3);   // material count for the device view
+        for (size_t i = 0; i < all.mats.size(); i++) {
+            e.objects.materials[3 * i] = all.mats[i].x;
+            e.objects.materials[3 * i + 1] = all.mats[i].y;
+            e.objects.materials[3 * i + 2] = all.mats[i].z;
+        }
+        e.setPartition(bodyStart, colStart);
+        const uint32_t np = uint32_t(all.prev.size());
+        if (np > e.manifoldCap) e.reserveCapacities(std::max(np, e.pairCap), np);
+        if (np) CK(cudaMemcpyAsync(e.prevManifolds.p, all.prev.data(), np * sizeof(Manifold), cudaMemcpyHostToDevice,
+                                   e.stream));
+        CK(cudaMemcpyAsync(e.nPrev.p, &np, sizeof(uint32_t), cudaMemcpyHostToDevice, e.stream));
+        CK(cudaStreamSynchronize(e.stream));
         *out = b.release();
     });
 }
@@ -1251,17 +1497,83 @@ int32_t ag2d_batch_step(ag2d_batch* batch, int32_t steps)
 {
     return guarded([&] {
         if (!batch) throw ApiError(AG2D_ERR_INVALID_ARG, "null batch");
-        for (int32_t i = 0; i < steps; i++)
-            for (ag2d_world* w : batch->worlds) {
-                CK(cudaSetDevice(w->settings.device));
-                w->stepOnce();
+        if (steps < 0) throw ApiError(AG2D_ERR_INVALID_ARG, "steps must be >= 0");
+        CK(cudaSetDevice(batch->engine->settings.device));
+        for (int32_t i = 0; i < steps; i++) batch->engine->stepOnce();
+    });
+}
+
+int32_t ag2d_batch_engine(ag2d_batch* batch, ag2d_world** out_world)
+{
+    return guarded([&] {
+        if (!batch || !out_world) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        *out_world = batch->engine.get();
+    });
+}
+
+int32_t ag2d_batch_world_count(ag2d_batch* batch, uint32_t* out_count)
+{
+    return guarded([&] {
+        if (!batch || !out_count) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        *out_count = batch->worlds;
+    });
+}
+
+int32_t ag2d_batch_read(ag2d_batch* batch, uint32_t world, int32_t field, void* dst, uint64_t cap,
+                        uint64_t* out_bytes)
+{
+    return guarded([&] {
+        if (!batch) throw ApiError(AG2D_ERR_INVALID_ARG, "null batch");
+        if (world >= batch->worlds) throw ApiError(AG2D_ERR_INVALID_ARG, "world index out of range");
+        ag2d_world& e = *batch->engine;
+        CK(cudaSetDevice(e.settings.device));
+        const uint32_t b0 = e.hBodyStart[world], b1 = e.hBodyStart[world + 1];
+        const uint32_t c0 = e.hColStart[world], c1 = e.hColStart[world + 1];
+        const std::vector<uint8_t> all = read_field(e, field);
+        std::vector<uint8_t> out;
+        auto slice = [&](size_t elemBytes, uint32_t lo, uint32_t hi) {
+            out.assign(all.begin() + size_t(lo) * elemBytes, all.begin() + size_t(hi) * elemBytes);
+        };
+        if (field == AG2D_BODY_POSE) {
+            slice(12, b0, b1);
+        } else if (field == AG2D_BODY_SLEEP_ISLAND) {
+            slice(4, b0, b1);
+            uint32_t* v = reinterpret_cast<uint32_t*>(out.data());
+            for (uint32_t i = 0; i < b1 - b0; i++) if (v[i] != 0xFFFFFFFFu) v[i] -= b0;
+        } else if (field >= AG2D_BODY_COM_X && field < AG2D_BODY_POSE) {
+            slice(4, b0, b1);
+        } else if (field >= AG2D_COL_WORLD_X && field < AG2D_DYN_SORTED) {
+            slice(4, c0, c1);
+        } else if (field == AG2D_MANIFOLDS || field == AG2D_PREV_MANIFOLDS) {
+            const Manifold* m = reinterpret_cast<const Manifold*>(all.data());
+            const size_t n = all.size() / sizeof(Manifold);
+            std::vector<Manifold> mine;
+            for (size_t i = 0; i < n; i++) {
+                if (m[i].a < c0 || m[i].a >= c1) continue;
+                Manifold x = m[i];
+                x.a -= c0;
+                x.b -= c0;
+                mine.push_back(x);
             }
+            out.resize(mine.size() * sizeof(Manifold));
+            if (!mine.empty()) std::memcpy(out.data(), mine.data(), out.size());
+        } else {
+            throw ApiError(AG2D_ERR_UNSUPPORTED, "field is not readable per world of a batch");
+        }
+        if (out_bytes) *out_bytes = out.size();
+        if (dst) {
+            if (cap < out.size()) throw ApiError(AG2D_ERR_INVALID_ARG, "destination too small");
+            if (!out.empty()) std::memcpy(dst, out.data(), out.size());
+        }
     });
 }
 
 int32_t ag2d_batch_destroy(ag2d_batch* batch)
 {
-    return guarded([&] { delete batch; });
+    return guarded([&] {
+        if (batch && batch->engine) cudaSetDevice(batch->engine->settings.device);
+        delete batch;
+    });
 }
 
 }  // extern "C"

@@ -171,6 +171,7 @@ __global__ void k_wake_apply(DeviceWorld w, const uint32_t* __restrict__ wakeIsl
         if (w.bstate[b] == STATE_SLEEPING && w.sleepIsland[b] < w.nBodies && wakeIsland[w.sleepIsland[b]]) {
             w.bstate[b] = STATE_DYNAMIC;
             w.sleepTimer[b] = 0.0f;
+            if (w.worldDirty) w.worldDirty[w.bodyWorld[b]] = 1u;
             woke++;
         }
     }
@@ -208,6 +209,33 @@ __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* n
     const uint32_t size = gridDim.x * blockDim.x;
     color_and_solve(w, m, *nM, s, velIters, posIters, rank, size, GridSync{bar, &counters->status},
                     &counters->colors, &counters->status);
+}
+
+// Batched worlds: each CTA takes the next world from the work counter and colours + solves that world's manifold
+// segment alone. Segment-relative manifold indices give every world the colouring and solving order it has when
+// stepped on its own, so a world's result does not depend on the batch it is in.
+__global__ void __launch_bounds__(SOLVE_WORLD_THREADS)
+k_color_solve_worlds(DeviceWorld w, Manifold* m, const uint32_t* __restrict__ segStart,
+                     const uint32_t* __restrict__ worldOrder, uint32_t worlds, SolveScratch s, uint32_t velIters,
+                     uint32_t posIters, uint32_t* nextWorld, StepCounters* counters)
+{
+    __shared__ uint32_t colorCount[MAX_COLORS + 1];
+    __shared__ uint32_t colorStart[MAX_COLORS + 1];
+    __shared__ uint32_t item;
+    while (true) {
+        if (threadIdx.x == 0) item = atomicAdd(nextWorld, 1u);
+        __syncthreads();
+        const uint32_t k = item;
+        __syncthreads();
+        if (k >= worlds) return;
+        const uint32_t wd = worldOrder ? worldOrder[k] : k;
+        const uint32_t lo = segStart[wd], hi = segStart[wd + 1];
+        if (hi <= lo) continue;
+        const SolveScratch ls{s.color + lo, s.order + lo, s.bodyMax, colorCount, colorStart, s.cons + lo};
+        color_and_solve(w, m + lo, hi - lo, ls, velIters, posIters, threadIdx.x, blockDim.x, BlockSync{},
+                        &counters->colors, &counters->status);
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -278,6 +306,7 @@ __global__ void k_island_sleep(DeviceWorld w, uint32_t* __restrict__ parent, con
             w.bstate[b] = STATE_SLEEPING;
             w.sleepIsland[b] = root;
             w.sleepTimer[b] = 0.0f;
+            if (w.worldDirty) w.worldDirty[w.bodyWorld[b]] = 1u;
             slept++;
         }
     }

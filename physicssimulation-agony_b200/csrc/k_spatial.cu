@@ -10,13 +10,13 @@ namespace ag2d {
 // 140-299, call order Simulation.cpp:392-407), wrapBodyRotations (LeftOutFunctions.cpp:13-60) and
 // computeRotationCosSin (Integrator.cpp:301-311), fused per dynamic body. Elementwise: HBM-bound at 40 B/body.
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void k_integrate(DeviceWorld w, const uint32_t* __restrict__ dynBody, uint32_t nDyn, float dt, float gx,
-                            float gy, float dampHalf /* damping^(dt/2), or >= 1 when damping is off */)
+__global__ void k_integrate(DeviceWorld w, const uint32_t* __restrict__ dynBody, const uint8_t* __restrict__ dynSimd,
+                            uint32_t nDyn, float dt, float gx, float gy,
+                            float dampHalf /* damping^(dt/2), or >= 1 when damping is off */)
 {
-    const uint32_t simdEnd = nDyn & ~7u;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nDyn; k += gridDim.x * blockDim.x) {
         const uint32_t b = dynBody[k];
-        const bool simd = k < simdEnd;
+        const bool simd = dynSimd ? dynSimd[k] != 0 : k < (nDyn & ~7u);
         float4 v = w.bvel[b];
         float4 p = w.bpos[b];
         const float halfDT = dt * 0.5f;
@@ -53,8 +53,10 @@ __global__ void k_integrate(DeviceWorld w, const uint32_t* __restrict__ dynBody,
 
 // ---------------------------------------------------------------------------------------------------------------
 // Collider world pose and AABB: computeColliderWorldPositions/Rotations (Simulation.cpp:673-736) and the shape
-// AABB builders (SimulationImpl/ColliderAABBBuilder.cpp:8-136). 'list' selects the colliders (null = all, in index
-// order); the k-th collider of the pass takes the reference's SIMD path iff k < (n & ~7).
+// AABB builders (SimulationImpl/ColliderAABBBuilder.cpp:8-136). 'list' selects the colliders with their SIMD-path
+// flags (the k-th collider of its world's pass takes the reference's SIMD path iff k < (count & ~7)); null = every
+// collider, classified by its index within its world's collider range (the reference's live-range pass), or only
+// those of the worlds set in 'worldMask'.
 // ---------------------------------------------------------------------------------------------------------------
 __device__ __forceinline__ float4 collider_aabb(const DeviceWorld& w, uint32_t c, float x, float y, float cs, float sn)
 {
@@ -87,12 +89,22 @@ __device__ __forceinline__ float4 collider_aabb(const DeviceWorld& w, uint32_t c
     }
 }
 
-__global__ void k_collider_pose(DeviceWorld w, const uint32_t* __restrict__ list, uint32_t n)
+__global__ void k_collider_pose(DeviceWorld w, const uint32_t* __restrict__ list, const uint8_t* __restrict__ listSimd,
+                                uint32_t n, const uint32_t* __restrict__ worldMask)
 {
-    const uint32_t simdEnd = n & ~7u;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t c = list ? list[k] : k;
-        const bool simd = k < simdEnd;
+        if (worldMask && !worldMask[w.colWorld[c]]) continue;
+        bool simd;
+        if (list) {
+            simd = listSimd ? listSimd[k] != 0 : k < (n & ~7u);
+        } else if (w.colWorld) {
+            const uint32_t wd = w.colWorld[c];
+            const uint32_t lo = w.worldColStart[wd], hi = w.worldColStart[wd + 1];
+            simd = (c - lo) < ((hi - lo) & ~7u);
+        } else {
+            simd = k < (n & ~7u);
+        }
         const uint32_t b = w.cbody[c];
         const float4 off = w.coff[c];
         const float4 bp = w.bpos[b];
@@ -114,35 +126,79 @@ __global__ void k_collider_pose(DeviceWorld w, const uint32_t* __restrict__ list
 // min/max are order-independent, so a block reduction plus ordered-integer atomics gives the sequential result
 // (up to the sign of a zero bound).
 // ---------------------------------------------------------------------------------------------------------------
+// Per world (4 ordered words each). A warp whose lanes all belong to one world reduces first and issues one atomic
+// per word; a warp that straddles worlds issues per-lane atomics.
 __global__ void k_bounds(const float4* __restrict__ aabb, const uint32_t* __restrict__ list, uint32_t n,
-                         uint32_t* __restrict__ bounds /* ordered: minX, minY, maxX, maxY */)
+                         const uint32_t* __restrict__ colWorld, uint32_t* __restrict__ bounds)
 {
-    float mnx = FLT_MAX, mny = FLT_MAX, mxx = -FLT_MAX, mxy = -FLT_MAX;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const float4 a = aabb[list ? list[k] : k];
-        mnx = fminf(mnx, a.x); mny = fminf(mny, a.y); mxx = fmaxf(mxx, a.z); mxy = fmaxf(mxy, a.w);
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
-        mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
-        mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
-        mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicMin(bounds + 0, float_to_ordered(mnx));
-        atomicMin(bounds + 1, float_to_ordered(mny));
-        atomicMax(bounds + 2, float_to_ordered(mxx));
-        atomicMax(bounds + 3, float_to_ordered(mxy));
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t base0 = blockIdx.x * blockDim.x;
+    for (uint32_t base = base0; base < n; base += stride) {
+        const uint32_t k = base + threadIdx.x;
+        const bool valid = k < n;
+        const uint32_t c = valid ? (list ? list[k] : k) : 0u;
+        const float4 a = valid ? aabb[c] : make_float4(FLT_MAX, FLT_MAX, -FLT_MAX, -FLT_MAX);
+        const uint32_t wd = valid ? (colWorld ? colWorld[c] : 0u) : 0xFFFFFFFFu;
+        const uint32_t active = __ballot_sync(0xffffffffu, valid);
+        const uint32_t firstLane = __ffs(active) - 1;
+        const uint32_t w0 = __shfl_sync(0xffffffffu, wd, firstLane);
+        const bool uniform = __all_sync(0xffffffffu, !valid || wd == w0);
+        if (uniform) {
+            float mnx = a.x, mny = a.y, mxx = a.z, mxy = a.w;
+            for (int o = 16; o > 0; o >>= 1) {
+                mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+                mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+                mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+                mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+            }
+            if ((threadIdx.x & 31) == firstLane && active) {
+                uint32_t* b = bounds + 4 * w0;
+                atomicMin(b + 0, float_to_ordered(mnx));
+                atomicMin(b + 1, float_to_ordered(mny));
+                atomicMax(b + 2, float_to_ordered(mxx));
+                atomicMax(b + 3, float_to_ordered(mxy));
+            }
+        } else if (valid) {
+            uint32_t* b = bounds + 4 * wd;
+            atomicMin(b + 0, float_to_ordered(a.x));
+            atomicMin(b + 1, float_to_ordered(a.y));
+            atomicMax(b + 2, float_to_ordered(a.z));
+            atomicMax(b + 3, float_to_ordered(a.w));
+        }
     }
 }
 
-__global__ void k_bounds_init(uint32_t* bounds)
+__global__ void k_bounds_init(uint32_t* bounds, uint32_t worlds)
 {
-    if (threadIdx.x == 0) {
-        bounds[0] = float_to_ordered(FLT_MAX);
-        bounds[1] = float_to_ordered(FLT_MAX);
-        bounds[2] = float_to_ordered(-FLT_MAX);
-        bounds[3] = float_to_ordered(-FLT_MAX);
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < worlds; w += gridDim.x * blockDim.x) {
+        bounds[4 * w + 0] = float_to_ordered(FLT_MAX);
+        bounds[4 * w + 1] = float_to_ordered(FLT_MAX);
+        bounds[4 * w + 2] = float_to_ordered(-FLT_MAX);
+        bounds[4 * w + 3] = float_to_ordered(-FLT_MAX);
+    }
+}
+
+// Elements per world of a work list (for the per-world segment offsets of a tree or a manifold list).
+__global__ void k_count_world(const uint32_t* __restrict__ list, uint32_t n, const uint32_t* __restrict__ elemWorld,
+                              uint32_t* __restrict__ counts)
+{
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        atomicAdd(counts + elemWorld[list ? list[k] : k], 1u);
+}
+
+// SIMD-path flag of each work-list entry: the rank of its element among its world's listed elements, against that
+// world's (count & ~7). 'offsets' is the exclusive scan of the list flags over all elements, 'worldStart' the
+// first element index of each world.
+__global__ void k_simd_flags(const uint32_t* __restrict__ list, uint32_t n, const uint32_t* __restrict__ offsets,
+                             uint32_t nElems, const uint32_t* __restrict__ elemWorld,
+                             const uint32_t* __restrict__ worldStart, uint32_t worlds, uint8_t* __restrict__ simd)
+{
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t w = elemWorld[list[k]];
+        const uint32_t firstElem = worldStart[w], endElem = worldStart[w + 1];
+        const uint32_t lo = offsets[firstElem];
+        const uint32_t hi = endElem < nElems ? offsets[endElem] : n;
+        simd[k] = (k - lo) < ((hi - lo) & ~7u) ? 1u : 0u;
     }
 }
 
@@ -151,22 +207,24 @@ __global__ void k_bounds_init(uint32_t* bounds)
 // per axis by the tree bounds, truncated, bits interleaved (y in the odd bits): a 32-bit key.
 // ---------------------------------------------------------------------------------------------------------------
 __global__ void k_morton(const float4* __restrict__ aabb, const uint32_t* __restrict__ list, uint32_t n,
-                         const uint32_t* __restrict__ bounds, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals)
+                         const uint32_t* __restrict__ colWorld, const uint32_t* __restrict__ bounds,
+                         uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t* __restrict__ keyOf)
 {
-    const float bminX = ordered_to_float(bounds[0]), bminY = ordered_to_float(bounds[1]);
-    const float bmaxX = ordered_to_float(bounds[2]), bmaxY = ordered_to_float(bounds[3]);
-    const float kEps = 1e-5f;
-    const float maxX = rfmaxf(bmaxX, bminX + kEps);
-    const float maxY = rfmaxf(bmaxY, bminY + kEps);
-    const float clampMax = 65535.0f;
-    const float scaleX = clampMax / (maxX - bminX);
-    const float scaleY = clampMax / (maxY - bminY);
-    const float negScaledMinX = -bminX * scaleX;
-    const float negScaledMinY = -bminY * scaleY;
-    const float halfScaleX = scaleX * 0.5f;
-    const float halfScaleY = scaleY * 0.5f;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const uint32_t c = list ? list[k] : k;
+        const uint32_t* b = bounds + 4 * (colWorld ? colWorld[c] : 0u);
+        const float bminX = ordered_to_float(b[0]), bminY = ordered_to_float(b[1]);
+        const float bmaxX = ordered_to_float(b[2]), bmaxY = ordered_to_float(b[3]);
+        const float kEps = 1e-5f;
+        const float maxX = rfmaxf(bmaxX, bminX + kEps);
+        const float maxY = rfmaxf(bmaxY, bminY + kEps);
+        const float clampMax = 65535.0f;
+        const float scaleX = clampMax / (maxX - bminX);
+        const float scaleY = clampMax / (maxY - bminY);
+        const float negScaledMinX = -bminX * scaleX;
+        const float negScaledMinY = -bminY * scaleY;
+        const float halfScaleX = scaleX * 0.5f;
+        const float halfScaleY = scaleY * 0.5f;
         const float4 a = aabb[c];
         const float cx = a.x + a.z;
         const float cy = a.y + a.w;
@@ -174,8 +232,59 @@ __global__ void k_morton(const float4* __restrict__ aabb, const uint32_t* __rest
         float ty = cy * halfScaleY + negScaledMinY;
         tx = tx < 0.0f ? 0.0f : (tx > clampMax ? clampMax : tx);
         ty = ty < 0.0f ? 0.0f : (ty > clampMax ? clampMax : ty);
-        keys[k] = (part1by1(uint32_t(ty)) << 1) | part1by1(uint32_t(tx));
+        const uint32_t key = (part1by1(uint32_t(ty)) << 1) | part1by1(uint32_t(tx));
+        keys[k] = key;
         vals[k] = c;
+        if (keyOf) keyOf[c] = key;
+    }
+}
+
+// After the Morton passes: the world id of each sorted element becomes the key of the next (stable) passes, so the
+// final order is by (world, Morton key) with ties in collider order.
+__global__ void k_world_keys(const uint32_t* __restrict__ vals, uint32_t n, const uint32_t* __restrict__ colWorld,
+                             uint32_t* __restrict__ keys)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        keys[i] = colWorld[vals[i]];
+}
+
+// First index of every world's segment of a world-grouped list: segStart[w] = offsets[worldStart[w]] (the exclusive
+// scan of the list flags over the elements), segStart[worlds] = the list length.
+__global__ void k_seg_starts(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ worldStart,
+                             uint32_t worlds, uint32_t nElems, const uint32_t* __restrict__ total,
+                             uint32_t* __restrict__ segStart)
+{
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w <= worlds; w += gridDim.x * blockDim.x) {
+        const uint32_t e = worldStart[w];
+        segStart[w] = (w == worlds || e >= nElems) ? *total : offsets[e];
+    }
+}
+
+// Segment starts of the world-grouped manifold list (world of body a, non-decreasing): the thread at each world
+// change fills the starts of every world in the gap, so worlds without manifolds get empty segments.
+__global__ void k_manifold_segments(const Manifold* __restrict__ m, const uint32_t* __restrict__ nM,
+                                    const uint32_t* __restrict__ cbody, const uint32_t* __restrict__ bodyWorld,
+                                    uint32_t worlds, uint32_t* __restrict__ segStart)
+{
+    const uint32_t n = *nM;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x) {
+        const int prev = i == 0 ? -1 : int(bodyWorld[cbody[m[i - 1].a]]);
+        const int cur = i == n ? int(worlds) : int(bodyWorld[cbody[m[i].a]]);
+        for (int w = prev + 1; w <= cur; w++) segStart[w] = i;
+    }
+}
+
+// Sorted-order gathers for the tree: Morton key (after the world passes), world id and AABB of every leaf.
+__global__ void k_tree_gather(const uint32_t* __restrict__ vals, uint32_t n, const uint32_t* __restrict__ keyOf,
+                              const uint32_t* __restrict__ colWorld, const float4* __restrict__ caabb,
+                              uint32_t* __restrict__ sortedKey, uint32_t* __restrict__ sortedWorld,
+                              float4* __restrict__ leafAabb)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t c = vals[i];
+        if (keyOf) sortedKey[i] = keyOf[c];
+        if (colWorld) sortedWorld[i] = colWorld[c];
+        leafAabb[i] = caabb[c];
     }
 }
 
@@ -338,39 +447,49 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_pass(
 // ---------------------------------------------------------------------------------------------------------------
 // Karras LBVH over sorted keys (leaf = one collider). Internal node i spans [first, last] of the sorted order and
 // splits at the highest differing bit; equal keys are ordered by index (key ++ index), as the reference's stable
-// sort orders them. Children: >= 0 internal node, < 0 leaf ~rank.
+// sort orders them. Children: >= 0 internal node, < 0 leaf ~rank. Worlds are independent segments [lo, hi) of the
+// sorted order (sorted by world first): keys outside the segment count as unrelated (delta -1), so one build makes
+// every world's tree, rooted at internal node lo.
 // ---------------------------------------------------------------------------------------------------------------
-__device__ __forceinline__ int lbvh_delta(const uint32_t* keys, int n, int i, int j)
+__device__ __forceinline__ int lbvh_delta(const uint32_t* keys, int lo, int hi, int i, int j)
 {
-    if (j < 0 || j >= n) return -1;
+    if (j < lo || j >= hi) return -1;
     const uint32_t a = keys[i], b = keys[j];
     if (a != b) return __clz(a ^ b);
-    return 32 + __clz(uint32_t(i) ^ uint32_t(j));
+    // Index tie-break on segment-relative positions: a world's tree does not depend on where its segment starts.
+    return 32 + __clz(uint32_t(i - lo) ^ uint32_t(j - lo));
 }
 
-__global__ void k_lbvh_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ vals, int n,
-                             const float4* __restrict__ caabb, int2* __restrict__ child, int2* __restrict__ range,
-                             int* __restrict__ parent, int* __restrict__ leafParent, float4* __restrict__ leafAabb,
+// sortedWorld/segStart null: one segment [0, n).
+__global__ void k_lbvh_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ sortedWorld,
+                             const uint32_t* __restrict__ segStart, int n, int2* __restrict__ child,
+                             int2* __restrict__ range, int* __restrict__ parent, int* __restrict__ leafParent,
                              uint32_t* __restrict__ visit)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        leafAabb[i] = caabb[vals[i]];
-        if (n == 1) leafParent[0] = -1;
-        if (i >= n - 1) continue;
+        int lo = 0, hi = n;
+        if (sortedWorld) {
+            const uint32_t wd = sortedWorld[i];
+            lo = int(segStart[wd]);
+            hi = int(segStart[wd + 1]);
+        }
+        if (hi - lo == 1) leafParent[i] = -1;
+        if (i >= hi - 1) continue;
         visit[i] = 0;
-        const int d = (lbvh_delta(keys, n, i, i + 1) - lbvh_delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
-        const int dmin = lbvh_delta(keys, n, i, i - d);
+        if (i == lo) parent[i] = -1;
+        const int d = (lbvh_delta(keys, lo, hi, i, i + 1) - lbvh_delta(keys, lo, hi, i, i - 1)) >= 0 ? 1 : -1;
+        const int dmin = lbvh_delta(keys, lo, hi, i, i - d);
         int lmax = 2;
-        while (lbvh_delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+        while (lbvh_delta(keys, lo, hi, i, i + lmax * d) > dmin) lmax <<= 1;
         int l = 0;
         for (int t = lmax >> 1; t >= 1; t >>= 1)
-            if (lbvh_delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+            if (lbvh_delta(keys, lo, hi, i, i + (l + t) * d) > dmin) l += t;
         const int j = i + l * d;
-        const int dnode = lbvh_delta(keys, n, i, j);
+        const int dnode = lbvh_delta(keys, lo, hi, i, j);
         int s = 0, t = l;
         do {
             t = (t + 1) >> 1;
-            if (lbvh_delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+            if (lbvh_delta(keys, lo, hi, i, i + (s + t) * d) > dnode) s += t;
         } while (t > 1);
         const int gamma = i + s * d + (d < 0 ? -1 : 0);
         const int first = i < j ? i : j, last = i < j ? j : i;
@@ -380,7 +499,6 @@ __global__ void k_lbvh_build(const uint32_t* __restrict__ keys, const uint32_t* 
         range[i] = make_int2(first, last);
         if (left < 0) leafParent[~left] = i; else parent[left] = i;
         if (right < 0) leafParent[~right] = i; else parent[right] = i;
-        if (i == 0) parent[0] = -1;
     }
 }
 
@@ -390,7 +508,7 @@ __global__ void k_lbvh_refit(int n, const int2* __restrict__ child, const int* _
                              float4* __restrict__ nodeAabb, uint32_t* __restrict__ visit)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int node = n > 1 ? leafParent[i] : -1;
+        int node = leafParent[i];   // -1 for the leaf of a one-collider segment
         while (node >= 0) {
             __threadfence();
             if (atomicAdd(&visit[node], 1u) == 0) break;
@@ -427,13 +545,26 @@ __device__ __forceinline__ void query_impl(const TreeView& dyn, const TreeView& 
         const float4 q = dyn.leafAabb[i];
         const uint32_t me = dyn.vals[i];
         const uint32_t myBody = cbody[me];
+        // This collider's world: the segments of both trees it is tested against.
+        int dlo = 0, dhi = n, olo = 0, ohi = other.n;
+        if (dyn.sortedWorld) {
+            const uint32_t wd = dyn.sortedWorld[i];
+            dlo = int(dyn.segStart[wd]);
+            dhi = int(dyn.segStart[wd + 1]);
+            if (other.n > 0) {
+                olo = int(other.segStart[wd]);
+                ohi = int(other.segStart[wd + 1]);
+            } else {
+                ohi = 0;
+            }
+        }
         uint32_t count = 0;
         uint32_t out = WRITE ? offsets[i] : 0u;
         int stack[QUERY_STACK];
         // Self pairs within the dynamic tree.
-        if (n > 1) {
+        if (dhi - dlo > 1) {
             int sp = 0;
-            stack[sp++] = 0;
+            stack[sp++] = dlo;
             while (sp > 0) {
                 const int node = stack[--sp];
                 const int2 c = dyn.child[node];
@@ -458,15 +589,15 @@ __device__ __forceinline__ void query_impl(const TreeView& dyn, const TreeView& 
             }
         }
         // Cross pairs against the static + sleeping tree.
-        if (other.n == 1) {
-            if (strict_overlap(q, other.leafAabb[0])) {
-                if (WRITE && out < pairCap) pairs[out] = make_uint2(me, other.vals[0]);
+        if (ohi - olo == 1) {
+            if (strict_overlap(q, other.leafAabb[olo])) {
+                if (WRITE && out < pairCap) pairs[out] = make_uint2(me, other.vals[olo]);
                 out++;
                 count++;
             }
-        } else if (other.n > 1 && strict_overlap(q, other.nodeAabb[0])) {
+        } else if (ohi - olo > 1 && strict_overlap(q, other.nodeAabb[olo])) {
             int sp = 0;
-            stack[sp++] = 0;
+            stack[sp++] = olo;
             while (sp > 0) {
                 const int node = stack[--sp];
                 const int2 c = other.child[node];
