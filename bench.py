@@ -1,31 +1,41 @@
 #!/usr/bin/env python
-"""Throughput of the collision/contact pipeline on B200: body-steps/s of the single large world (100,000 mixed
-bodies, U container, dt 1/60, 8 velocity + 3 position iterations), stepped from the drop.
+"""Throughput of the collision/contact pipeline on B200, in body-steps/s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--bodies n]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c4|c2|c3]
 
-One process per GPU (torchrun for N > 1): a single world does not shard without a halo exchange, so every rank
-steps its own replica of the world (replicas only, no collective on the step path) and the whole-job value is
-N x bodies x K / (the slowest rank's device time). Rank 0 prints one JSON line.
+Workloads (seeded synthetic scenes, ag2d.scenes):
+  c4 (default)  4,096 independent worlds, body counts log-uniform in [16, 2048] (c1 mix: 3-8-gons on a ground box),
+                packed into one batch and advanced by one launch sequence per step; the same worlds stepped one
+                world per launch sequence are timed beside it ("per_world_launch").
+  c2            one world of 100,000 mixed bodies dropped into a static U container.
+  c3            1,000,000 circles and 4-6-gons: collision detection alone (poses, AABBs, Morton, sort, LBVH,
+                query, SAT), reported as broad+narrow GB/s against the HBM roofline, with the exact pair count
+                checked against the oracle's sweep.
 
-Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events on the world's stream, with a 256 MiB
-write between steps (L2 flushed; the timed region excludes it); barrier + synchronize around the timed region; the
-max over ranks. SM clocks are sampled with nvidia-smi during the timed region. The end-to-end number goes through
-the C ABI with host buffers: the scene uploaded from host memory, then per step one ag2d_world_step and one
-readback of every body's pose into host memory.
+One process per GPU (torchrun for N > 1). Worlds exchange nothing on the step path, so each rank advances its own
+batch (rank r's worlds are seeded r * worlds + k): weak scaling with no collective in the step; the whole-job value
+is the sum of all ranks' body-steps over the slowest rank's device time.
+
+Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events on the engine's stream, with a 256 MiB
+write between steps outside the events (L2 flushed); barrier + synchronize around the timed region; the max over
+ranks. SM clocks are sampled with nvidia-smi during the timed region. The end-to-end number ("e2e") goes through the
+C ABI with host buffers: the bodies created on the host and uploaded inside the timed region, then per step one
+step call and one readback of every body's pose into host memory.
 
 --impl reference times the reference engine itself (oracle/_ref/libagony_ref.so, its own C++ on the host cores,
-all threads) on the same workload and prints the same line with "impl": "reference".
+all threads) on a bounded sample of the same workload and prints the same line with "impl": "reference".
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import queue
 import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -35,35 +45,88 @@ for _p in (ROOT, PKG):
         sys.path.insert(0, _p)
 
 METRIC = "body-steps/s"
-WORKLOAD = "c2: single large world, 100k mixed bodies (60% boxes, 25% circles, 15% 3-8-gons) in a static U, " \
-           "dt 1/60, 8 velocity + 3 position iterations, stepped from the drop"
+WORKLOADS = {
+    "c4": "c4: 4096 independent worlds, body counts log-uniform [16, 2048] (3-8-gons r U[0.5,2] +-15% jitter on a "
+          "static 220 m ground box each), dt 1/60, 8 velocity + 3 position iterations, batched",
+    "c2": "c2: single large world, 100k mixed bodies (60% boxes, 25% circles, 15% 3-8-gons) in a static U, "
+          "dt 1/60, 8 velocity + 3 position iterations, stepped from the drop",
+    "c3": "c3: 1M bodies (50% circles, 50% 4-6-gons, size log-uniform 0.1-2 m) uniform in 4000 x 4000 m, "
+          "v ~ N(0, 5 m/s); collision detection alone (poses, AABBs, Morton, sort, LBVH, query, SAT)",
+}
+DEFAULT_STEPS = {"c4": 600, "c2": 1000, "c3": 20}
+BODY_UPLOAD_BYTES = 16 + 16 + 8 + 4 + 4 + 4 + 1 + 4 + 4 + 4 + 4 + 16   # body + collider records as uploaded
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--bodies", type=int, default=100_000)
+    ap.add_argument("--workload", default="c4", choices=sorted(WORKLOADS))
+    ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--bodies", type=int, default=None, help="c2 / c3 body count")
+    ap.add_argument("--per-world-sample", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.steps is None:
+        a.steps = DEFAULT_STEPS[a.workload]
+    if a.bodies is None:
+        a.bodies = 1_000_000 if a.workload == "c3" else 100_000
+    return a
 
 
 def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def make_scene(n):
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# Scenes
+# ---------------------------------------------------------------------------------------------------------------
+def c4_scenes(worlds, seed):
+    from ag2d import scenes
+    return scenes.make_c4_worlds(worlds=worlds, seed=seed, processes=max(1, min(32, host_threads())))
+
+
+def c2_scene(n):
     from ag2d import scenes
     cols = 500 if n >= 100_000 else max(10, int(round((n / 200.0) ** 0.5 * 10)))
     return scenes.make_c2(n, 0, columns=cols)
 
 
+def c3_scene(n):
+    from ag2d import scenes
+    return scenes.make_c3(n, 0, extent=4000.0 * (n / 1e6) ** 0.5)
+
+
+def mean_shape_bytes(scene_list):
+    import numpy as np
+    from ag2d import roofline, scenes
+    total, count = 0.0, 0
+    for sc in scene_list:
+        k = sc.kind.astype(np.int64)
+        total += float(np.where(k == scenes.POLYGON, 8.0 + 16.0 * sc.poly_count,
+                                np.where(k == scenes.BOX, roofline.SHAPE_BYTES[1], roofline.SHAPE_BYTES[0])).sum())
+        count += sc.n
+    return total / max(count, 1)
+
+
+def upload_bytes(scene_list):
+    return sum(sc.n * BODY_UPLOAD_BYTES + int(sc.poly_count.sum()) * 16 for sc in scene_list)
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# Measurement helpers
+# ---------------------------------------------------------------------------------------------------------------
 class ClockSampler:
     """nvidia-smi sampled every 200 ms while running (the clocks line of the timing rules)."""
 
@@ -127,22 +190,142 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def mean_shape_bytes(scene):
-    from ag2d import roofline, scenes
-    total = 0.0
-    for k in range(scene.n):
-        kind = int(scene.kind[k])
-        total += roofline.polygon_bytes(int(scene.poly_count[k])) if kind == scenes.POLYGON else \
-            roofline.SHAPE_BYTES[kind]
-    return total / max(scene.n, 1)
+def dram_traffic(kernel):
+    """Per-launch DRAM bytes of a kernel (for the bench's workload) from the committed ncu summary, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
+            return json.load(f).get(kernel)
+    except (OSError, ValueError):
+        return None
 
 
-def cpu_baseline(scene, seconds):
-    """The reference engine (its own C++, all host threads) on the first steps of the same workload."""
+class Timer:
+    """Per-step device time on one stream: CUDA events around each step, an L2 flush between steps."""
+
+    def __init__(self, torch, stream, dev):
+        self.torch = torch
+        self.stream = stream
+        self.flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MiB > 126 MB L2
+        self.ms = []
+
+    def run(self, fn, steps, on_step=None):
+        torch = self.torch
+        for _ in range(steps):
+            with torch.cuda.stream(self.stream):
+                self.flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(self.stream)
+            fn()
+            e1.record(self.stream)
+            e1.synchronize()
+            self.ms.append(e0.elapsed_time(e1))
+            if on_step:
+                on_step()
+        return float(sum(self.ms))
+
+
+def roofline_line(phases, bytes_by_phase, kernel_of, workload):
+    dominant = max(bytes_by_phase, key=lambda p: phases[p][0])
+    peak, peak_kind = measured_peaks()
+    dom_ms, dom_calls = phases[dominant]
+    achieved = bytes_by_phase[dominant] / max(dom_ms / 1e3, 1e-12) / 1e9
+    calls = max(dom_calls, 1)
+    return {"bound": "hbm", "kernel": kernel_of[dominant], "phase": dominant, "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "traffic": dram_traffic(f"{workload}:{kernel_of[dominant]}"),
+            "algorithmic_bytes_per_launch": bytes_by_phase[dominant] / calls, "launch_ms": dom_ms / calls}
+
+
+def step_bytes(msb, pairs_sum, manifolds_sum, dyn_bodies, steps, vi=8, pi=3):
+    from ag2d import roofline
+    K = steps
+    return {
+        "solve": roofline.solve_bytes(manifolds_sum, vi, pi),
+        "narrow": roofline.narrow_bytes(pairs_sum, msb, manifolds_sum),
+        "integrate": roofline.integrate_bytes(dyn_bodies * K),
+        "pose": roofline.pose_bytes(dyn_bodies * K, msb),
+        "sort": roofline.sort_bytes(dyn_bodies * K),
+        "query": roofline.query_bytes(dyn_bodies * K, pairs_sum),
+    }
+
+
+def diagnostics(c0, c1, per_step, colors_sum, K):
+    return {"mean_colors": colors_sum / K, "list_rebuilds": c1["list_rebuilds"] - c0["list_rebuilds"],
+            "retries": c1["retries"] - c0["retries"], "regrows": c1["regrows"] - c0["regrows"],
+            "host_ms_per_step": (c1["host_ms"] - c0["host_ms"]) / K,
+            "sync_wait_ms_per_step": (c1["sync_ms"] - c0["sync_ms"]) / K,
+            "max_step_ms": max(per_step), "median_step_ms": statistics.median(per_step)}
+
+
+def reduce_max(torch, dist, world_size, dev, value):
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    if world_size > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(torch, dist, world_size, dev, value):
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    if world_size > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# CPU baselines: the reference engine (oracle/_ref) on the host cores
+# ---------------------------------------------------------------------------------------------------------------
+def cpu_worlds_rate(scene_list, seconds, threads):
+    """Reference Simulation objects, one world per task, over a pool of host threads (ctypes releases the GIL).
+    Each task creates its world and steps it in chunks of 10 until 600 steps or the time budget; body-steps/s."""
+    from oracle import refapi
+    work = queue.Queue()
+    for sc in scene_list:
+        work.put(sc)
+    done = [0.0]
+    lock = threading.Lock()
+    deadline = time.perf_counter() + seconds
+
+    def worker():
+        while time.perf_counter() < deadline:
+            try:
+                sc = work.get_nowait()
+            except queue.Empty:
+                return
+            sim = refapi.RefSim(sc, threads=0)
+            steps = 0
+            while time.perf_counter() < deadline and steps < 600:
+                sim.update(10)
+                steps += 10
+            sim.close()
+            with lock:
+                done[0] += sc.n * steps
+    t0 = time.perf_counter()
+    pool = [threading.Thread(target=worker) for _ in range(threads)]
+    for t in pool:
+        t.start()
+    for t in pool:
+        t.join()
+    return done[0] / (time.perf_counter() - t0)
+
+
+def cpu_c4(scene_list, seconds):
     from oracle import refapi
     if not refapi.available():
         return None
-    threads = max(0, (os.cpu_count() or 1) - 1)
+    threads = host_threads()
+    stride = max(1, len(scene_list) // 256)
+    value = cpu_worlds_rate(scene_list[::stride], seconds, threads)
+    return {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
+            "sample": f"reference engine (oracle/_ref, -O2 -mavx2 -mfma), one single-threaded Simulation per world, "
+                      f"{threads} worlds at a time, every {stride}-th world of the batch stepped from rest in chunks "
+                      f"of 10 steps for {seconds:.0f} s"}
+
+
+def cpu_c2(scene, seconds):
+    from oracle import refapi
+    if not refapi.available():
+        return None
+    threads = max(0, host_threads() - 1)
     sim = refapi.RefSim(scene, threads=threads)
     steps, elapsed = 0, 0.0
     while elapsed < seconds and steps < 100000:
@@ -154,170 +337,362 @@ def cpu_baseline(scene, seconds):
                       f"{scene.n}-body world from the drop, {threads + 1} threads, {elapsed:.1f} s wall"}
 
 
+def cpu_c3(scene, reps):
+    from oracle import refapi
+    if not refapi.available():
+        return None
+    threads = max(0, host_threads() - 1)
+    sim = refapi.RefSim(scene, threads=threads)
+    sim.timed_collide()
+    times, pairs, mans = [], 0, 0
+    for _ in range(reps):
+        t, pairs, mans = sim.timed_collide()
+        times.append(t)
+    sim.close()
+    return {"seconds": statistics.median(times), "pairs": pairs, "manifolds": mans, "threads": threads + 1}
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# Reference arm
+# ---------------------------------------------------------------------------------------------------------------
 def run_reference(args):
-    rank, world, _ = dist_env()
+    rank, _, _ = dist_env()
     if rank != 0:
         return
     from oracle import refapi
     if not refapi.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libagony_ref.so was not built"}))
         return
-    scene = make_scene(args.bodies)
-    threads = max(0, (os.cpu_count() or 1) - 1)
-    sim = refapi.RefSim(scene, threads=threads)
-    sim.update(args.warmup)
     budget = 150.0
-    steps, elapsed = 0, 0.0
-    while steps < args.steps and elapsed < budget:
-        elapsed += sim.timed_update(1)
-        steps += 1
-    sim.close()
-    value = scene.n * steps / elapsed
-    sample = f"steps {args.warmup}..{args.warmup + steps} of the {scene.n}-body world ({threads + 1} threads)"
-    if steps < args.steps:
-        sample += f"; stopped after {budget:.0f} s of {args.steps} requested steps"
-    print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 0, "steps": steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / max(steps, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "bodies": scene.n},
-        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads + 1, "kind": "reference",
-                         "sample": sample},
-        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }))
+    base = {"impl": "reference", "metric": METRIC, "unit": METRIC, "n_gpus": 0, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic (seeded scene generator, ag2d.scenes)"}
+    if args.workload == "c4":
+        scene_list = c4_scenes(args.worlds, 0)
+        threads = host_threads()
+        stride = max(1, len(scene_list) // 256)
+        seconds = min(budget, 10.0 * max(args.steps, 1) / 60.0 + 20.0)
+        value = cpu_worlds_rate(scene_list[::stride], seconds, threads)
+        sample = (f"every {stride}-th world, one single-threaded Simulation per world, {threads} at a time, "
+                  f"{seconds:.0f} s of stepping from rest")
+        bodies = int(sum(s.n for s in scene_list))
+        line = dict(base, value=value, steps=args.steps, ms_per_step=1e3 * bodies / value,
+                    config={"workload": WORKLOADS["c4"], "worlds": args.worlds, "bodies": bodies,
+                            "ms_per_step": "equivalent time of one step of the whole batch at this rate"})
+    elif args.workload == "c2":
+        scene = c2_scene(args.bodies)
+        threads = max(0, host_threads() - 1)
+        sim = refapi.RefSim(scene, threads=threads)
+        sim.update(args.warmup)
+        steps, elapsed = 0, 0.0
+        while steps < args.steps and elapsed < budget:
+            elapsed += sim.timed_update(1)
+            steps += 1
+        sim.close()
+        value = scene.n * steps / elapsed
+        threads += 1
+        sample = f"steps {args.warmup}..{args.warmup + steps} of the {scene.n}-body world ({threads} threads)"
+        if steps < args.steps:
+            sample += f"; stopped after {budget:.0f} s of {args.steps} requested steps"
+        line = dict(base, value=value, steps=steps, ms_per_step=1e3 * elapsed / max(steps, 1),
+                    config={"workload": WORKLOADS["c2"], "bodies": scene.n})
+    else:
+        scene = c3_scene(args.bodies)
+        r = cpu_c3(scene, max(1, min(args.steps, 5)))
+        threads = r["threads"]
+        value = scene.n / r["seconds"]
+        sample = f"median of collision-detection passes over the {scene.n}-body world ({threads} threads)"
+        line = dict(base, value=value, steps=1, ms_per_step=1e3 * r["seconds"],
+                    config={"workload": WORKLOADS["c3"], "bodies": scene.n, "pairs": r["pairs"]})
+    line["cpu_baseline"] = {"value": value, "unit": METRIC, "cores": threads, "kind": "reference", "sample": sample}
+    line["e2e"] = {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    print(json.dumps(line))
 
 
-def run_ours(args):
-    import torch
-    import torch.distributed as dist
-
+# ---------------------------------------------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------------------------------------------
+def run_c4(args, torch, dist, rank, world_size, local, dev):
     import ag2d
-    from ag2d import roofline
-
-    rank, world_size, local = dist_env()
+    scene_list = c4_scenes(args.worlds, rank * args.worlds)
+    n_bodies = int(sum(s.n for s in scene_list))
+    settings = dict(dt=scene_list[0].dt, velocity_iterations=8, position_iterations=3, gravity=scene_list[0].gravity,
+                    device=local)
+    worlds = []
+    for sc in scene_list:   # host objects only: a world touches the device on its first step
+        w = ag2d.World(**settings)
+        w.add_scene(sc)
+        worlds.append(w)
+    batch = ag2d.Batch(worlds)
+    e = batch.engine
+    stream = torch.cuda.ExternalStream(e.stream(), device=dev)
+    batch.step(args.warmup)
+    e.set_profiling(True)
+    c0 = e.counters()
     if world_size > 1:
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
-    torch.cuda.set_device(local)
-    dev = torch.device(f"cuda:{local}")
+        dist.barrier()
+    torch.cuda.synchronize()
+    sums = {"pairs": 0, "manifolds": 0, "colors": 0}
 
-    scene = make_scene(args.bodies)
+    def acc():
+        c = e.counters()
+        for k in sums:
+            sums[k] += c[k]
+    timer = Timer(torch, stream, dev)
+    sampler = ClockSampler(local)
+    sampler.start()
+    total_ms = timer.run(lambda: batch.step(1), args.steps, acc)
+    torch.cuda.synchronize()
+    if world_size > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    c1 = e.counters()
+    K = args.steps
+    max_ms = reduce_max(torch, dist, world_size, dev, total_ms)
+    job_bodies = reduce_sum(torch, dist, world_size, dev, float(n_bodies))
+    value = job_bodies * K / (max_ms / 1e3)
+    phases = e.phase_times()
+    msb = mean_shape_bytes(scene_list)
+    bytes_by_phase = step_bytes(msb, sums["pairs"], sums["manifolds"], n_bodies - len(scene_list), K)
+    kernel_of = {"solve": "k_color_solve_worlds", "narrow": "k_narrow", "integrate": "k_integrate",
+                 "pose": "k_collider_pose", "sort": "k_sort_pass", "query": "k_query_count + k_query_write"}
+    roof = roofline_line(phases, bytes_by_phase, kernel_of, "c4")
+    del batch, e
+
+    # End to end through the C ABI: a batch packed from the host-created worlds and uploaded inside the timed
+    # region, then per step one ag2d_batch_step and a readback of every body's pose (x, y, rotation).
+    e2e_steps = min(K, 200)
+    if world_size > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b2 = ag2d.Batch(worlds)
+    for _ in range(e2e_steps):
+        b2.step(1)
+        pose = b2.engine.read(ag2d.BODY_POSE)
+    torch.cuda.synchronize()
+    e2e_s = reduce_max(torch, dist, world_size, dev, time.perf_counter() - t0)
+    e2e = {"value": job_bodies * e2e_steps / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": upload_bytes(scene_list) / e2e_steps, "d2h_bytes_per_step": int(pose.nbytes),
+           "steps": e2e_steps}
+    del b2, pose
+
+    # The same worlds, one launch sequence per world per step (a Simulation per world): every k-th world.
+    stride = max(1, len(worlds) // max(1, args.per_world_sample))
+    sample = worlds[::stride]
+    for w in sample:
+        w.step(args.warmup)
+    torch.cuda.synchronize()
+    pw_steps = 5
+    t0 = time.perf_counter()
+    for _ in range(pw_steps):
+        for w in sample:
+            w.step(1)
+    torch.cuda.synchronize()
+    pw_s = time.perf_counter() - t0
+    pw_bodies = sum(scene_list[k].n for k in range(0, len(worlds), stride))
+    per_world = reduce_sum(torch, dist, world_size, dev, pw_bodies * pw_steps / pw_s)
+    per_world_line = {"value": per_world, "unit": METRIC,
+                      "sample": f"every {stride}-th world ({len(sample)} worlds), {pw_steps} steps each after "
+                                f"{args.warmup} warm-up steps, each world its own ag2d_world_step launch sequence, "
+                                f"wall clock (host launch bound)",
+                      "batched_over_per_world": value / per_world}
+    del sample
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        cpu = cpu_c4(scene_list, args.cpu_seconds)
+    return {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world_size, "steps": K, "warmup": args.warmup,
+        "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32", "data": "synthetic (seeded scene generator, ag2d.scenes.make_c4_worlds)",
+        "config": {"workload": WORKLOADS["c4"], "worlds_per_gpu": len(scene_list), "bodies_per_gpu": n_bodies,
+                   "parallelism": f"independent worlds x{world_size} GPUs (no step-path collective)",
+                   "l2": "flushed between timed steps (256 MiB write outside the events)",
+                   "mean_pairs_per_step": sums["pairs"] / K, "mean_manifolds_per_step": sums["manifolds"] / K},
+        "per_world_launch": per_world_line,
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": int(c1["launches"] - c0["launches"]), "clocks": clocks,
+        "phase_ms_per_step": {k: round(v[0] / max(K, 1), 4) for k, v in phases.items()},
+        "diagnostics": diagnostics(c0, c1, timer.ms, sums["colors"], K),
+    }
+
+
+def run_c2(args, torch, dist, rank, world_size, local, dev):
+    import ag2d
+    scene = c2_scene(args.bodies)
     w = ag2d.World.from_scene(scene, device=local)
     stream = torch.cuda.ExternalStream(w.stream(), device=dev)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MiB > 126 MB L2
-
     w.step(args.warmup)
     w.set_profiling(True)
     c0 = w.counters()
     if world_size > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    sums = {"pairs": 0, "manifolds": 0, "colors": 0}
+
+    def acc():
+        c = w.counters()
+        for k in sums:
+            sums[k] += c[k]
+    timer = Timer(torch, stream, dev)
     sampler = ClockSampler(local)
     sampler.start()
-    per_step = []
-    pairs_sum = manifolds_sum = colors_sum = 0
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        w.step(1)
-        e1.record(stream)
-        e1.synchronize()
-        per_step.append(e0.elapsed_time(e1))
-        c = w.counters()
-        pairs_sum += c["pairs"]
-        manifolds_sum += c["manifolds"]
-        colors_sum += c["colors"]
+    total_ms = timer.run(lambda: w.step(1), args.steps, acc)
     torch.cuda.synchronize()
     if world_size > 1:
         dist.barrier()
     clocks = sampler.stop()
     c1 = w.counters()
-    total_ms = float(sum(per_step))
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world_size > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world_size * scene.n * args.steps / (max_ms / 1e3)
-    phases = w.phase_times()
-
-    # Dominant single-kernel phase and its roofline (algorithmic bytes / measured kernel time).
     K = args.steps
-    msb = mean_shape_bytes(scene)
+    max_ms = reduce_max(torch, dist, world_size, dev, total_ms)
+    value = world_size * scene.n * K / (max_ms / 1e3)
+    phases = w.phase_times()
+    msb = mean_shape_bytes([scene])
     nb, nc = w.counts()
-    dyn_bodies = nb - int((scene.mass == 0).sum())
-    bytes_by_phase = {
-        "solve": roofline.solve_bytes(manifolds_sum, 8, 3),
-        "narrow": roofline.narrow_bytes(pairs_sum, msb, manifolds_sum),
-        "integrate": roofline.integrate_bytes(dyn_bodies * K),
-        "pose": roofline.pose_bytes(dyn_bodies * K, msb),
-        "sort": roofline.sort_bytes(dyn_bodies * K),
-        "query": roofline.query_bytes(dyn_bodies * K, pairs_sum),
-    }
-    kernel_of = {"solve": "k_solve", "narrow": "k_narrow", "integrate": "k_integrate", "pose": "k_collider_pose",
-                 "sort": "k_sort_pass", "query": "k_query_count + k_query_write"}
-    dominant = max(bytes_by_phase, key=lambda p: phases[p][0])
-    peak, peak_kind = measured_peaks()
-    dom_ms, dom_calls = phases[dominant]
-    achieved = bytes_by_phase[dominant] / max(dom_ms / 1e3, 1e-12) / 1e9
-    traffic = None
-    prof_path = os.path.join(ROOT, "profiles", "dram_traffic.json")
-    if os.path.exists(prof_path):
-        try:
-            traffic = json.load(open(prof_path)).get(kernel_of[dominant])
-        except (OSError, ValueError):
-            traffic = None
+    bytes_by_phase = step_bytes(msb, sums["pairs"], sums["manifolds"], nb - int((scene.mass == 0).sum()), K)
+    kernel_of = {"solve": "k_color_solve_cluster", "narrow": "k_narrow", "integrate": "k_integrate",
+                 "pose": "k_collider_pose", "sort": "k_sort_pass", "query": "k_query_count + k_query_write"}
+    roof = roofline_line(phases, bytes_by_phase, kernel_of, "c2")
 
-    # End to end through the C ABI: scene upload from host memory, then per step a step + a pose readback.
-    w2 = ag2d.World.from_scene(scene, device=local)
     e2e_steps = min(K, 300)
-    h2d = scene.n * (4 * 4 + 4 * 4 + 8 + 12) + int(scene.poly_count.sum()) * 16
     if world_size > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    w2.step(1)          # first step uploads the host scene
-    pose = w2.read(ag2d.BODY_POSE)
-    for _ in range(e2e_steps - 1):
+    w2 = ag2d.World.from_scene(scene, device=local)
+    for _ in range(e2e_steps):
         w2.step(1)
         pose = w2.read(ag2d.BODY_POSE)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world_size > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world_size * scene.n * e2e_steps / float(te.item())
+    e2e_s = reduce_max(torch, dist, world_size, dev, time.perf_counter() - t0)
+    e2e = {"value": world_size * scene.n * e2e_steps / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": upload_bytes([scene]) / e2e_steps, "d2h_bytes_per_step": int(pose.nbytes),
+           "steps": e2e_steps}
     del pose, w2
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(scene, args.cpu_seconds)
+        cpu = cpu_c2(scene, args.cpu_seconds)
+    return {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world_size, "steps": K, "warmup": args.warmup,
+        "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32", "data": "synthetic (seeded scene generator, ag2d.scenes.make_c2)",
+        "config": {"workload": WORKLOADS["c2"], "bodies": scene.n, "colliders": nc,
+                   "parallelism": f"replicas x{world_size} (one world per GPU, no step-path collective)",
+                   "l2": "flushed between timed steps (256 MiB write outside the events)",
+                   "mean_pairs_per_step": sums["pairs"] / K, "mean_manifolds_per_step": sums["manifolds"] / K},
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": int(c1["launches"] - c0["launches"]), "clocks": clocks,
+        "phase_ms_per_step": {k: round(v[0] / max(K, 1), 4) for k, v in phases.items()},
+        "diagnostics": diagnostics(c0, c1, timer.ms, sums["colors"], K),
+    }
 
+
+def run_c3(args, torch, dist, rank, world_size, local, dev):
+    import numpy as np
+    import ag2d
+    from ag2d import roofline
+    scene = c3_scene(args.bodies)
+    w = ag2d.World.from_scene(scene, device=local)
+    stream = torch.cuda.ExternalStream(w.stream(), device=dev)
+    w.run_phase(ag2d.PHASE_SPATIAL_FULL)
+    for _ in range(args.warmup):
+        w.run_phase(ag2d.PHASE_COLLIDE)
+    w.set_profiling(True)
+    c0 = w.counters()
+    if world_size > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    timer = Timer(torch, stream, dev)
+    sampler = ClockSampler(local)
+    sampler.start()
+    total_ms = timer.run(lambda: w.run_phase(ag2d.PHASE_COLLIDE), args.steps)
+    torch.cuda.synchronize()
+    if world_size > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    c1 = w.counters()
+    K = args.steps
+    max_ms = reduce_max(torch, dist, world_size, dev, total_ms)
+    ms_step = max_ms / K
+    value = world_size * scene.n * K / (max_ms / 1e3)
+    pairs, mans = c1["pairs"], c1["manifolds"]
+    msb = mean_shape_bytes([scene])
+    step_b = roofline.broad_narrow_bytes_per_step(scene.n, msb, pairs, mans)
+    peak, peak_kind = measured_peaks()
+    achieved = step_b / (ms_step / 1e3) / 1e9
+    phases = w.phase_times()
+    # Exact pair set against the oracle's sweep over the same AABBs.
+    aabb = [w.read(f) for f in (ag2d.COL_AABB_MIN_X, ag2d.COL_AABB_MIN_Y, ag2d.COL_AABB_MAX_X, ag2d.COL_AABB_MAX_Y)]
+    ours = w.read(ag2d.PAIRS)
+    overlap_frac = float(np.unique(ours.reshape(-1)).size) / scene.n if ours.size else 0.0
+    try:
+        from oracle import oraapi
+        ref = oraapi.broad_pairs_from_aabbs(*aabb, np.arange(scene.n, dtype=np.uint32))
+        canon = np.sort(ours, axis=1)
+        canon = canon[np.lexsort((canon[:, 1], canon[:, 0]))]
+        pair_check = {"oracle_pairs": int(ref.shape[0]),
+                      "identical_pair_set": bool(ref.shape == canon.shape and np.array_equal(ref, canon))}
+    except Exception as exc:  # the oracle library is test infrastructure and may be absent
+        pair_check = {"oracle_pairs": None, "identical_pair_set": None, "note": f"oracle unavailable: {exc}"}
+
+    e2e_reps = min(K, 10)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    w2 = ag2d.World.from_scene(scene, device=local)
+    w2.run_phase(ag2d.PHASE_SPATIAL_FULL)
+    for _ in range(e2e_reps):
+        w2.run_phase(ag2d.PHASE_COLLIDE)
+        man = w2.read(ag2d.MANIFOLDS)
+    torch.cuda.synchronize()
+    e2e_s = reduce_max(torch, dist, world_size, dev, time.perf_counter() - t0)
+    e2e = {"value": world_size * scene.n * e2e_reps / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": upload_bytes([scene]) / e2e_reps, "d2h_bytes_per_step": int(man.nbytes),
+           "steps": e2e_reps}
+    del w2, man
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        r = cpu_c3(scene, 3)
+        if r:
+            cpu = {"value": scene.n / r["seconds"], "unit": METRIC, "cores": r["threads"], "kind": "reference",
+                   "sample": f"reference engine collision detection (spatial data, broad, narrow; "
+                             f"agref_timed_collide) on the same {scene.n}-body world, median of 3 passes, "
+                             f"{r['seconds'] * 1e3:.1f} ms; its pair count {r['pairs']}",
+                   "gbs_equivalent": step_b / r["seconds"] / 1e9}
+    return {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world_size, "steps": K, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic (seeded scene generator, ag2d.scenes.make_c3)",
+        "config": {"workload": WORKLOADS["c3"], "bodies": scene.n, "pairs": pairs, "manifolds": mans,
+                   "fraction_of_bodies_with_overlap": overlap_frac, "pair_check": pair_check,
+                   "l2": "flushed between timed passes (256 MiB write outside the events)"},
+        "broadphase_gbs": achieved,
+        "roofline": {"bound": "hbm", "kernel": "collision detection pass (pose, bounds, Morton, sort, LBVH, query, "
+                                                "narrow, compaction)", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)", "traffic": None,
+                     "algorithmic_bytes_per_launch": step_b},
+        "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": int(c1["launches"] - c0["launches"]), "clocks": clocks,
+        "phase_ms_per_step": {k: round(v[0] / max(K, 1), 4) for k, v in phases.items()},
+    }
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, world_size, local = dist_env()
+    if world_size > 1:
+        import datetime
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device(f"cuda:{local}")
+    fn = {"c4": run_c4, "c2": run_c2, "c3": run_c3}[args.workload]
+    line = fn(args, torch, dist, rank, world_size, local, dev)
     if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world_size, "steps": K,
-            "warmup": args.warmup, "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded scene generator, ag2d.scenes.make_c2)",
-            "config": {"workload": WORKLOAD, "bodies": scene.n, "colliders": nc,
-                       "parallelism": f"replicas x{world_size} (one world per GPU, no step-path collective)",
-                       "l2": "flushed between timed steps (256 MiB write outside the events)",
-                       "mean_pairs_per_step": pairs_sum / K, "mean_manifolds_per_step": manifolds_sum / K},
-            "roofline": {"bound": "hbm", "kernel": kernel_of[dominant], "phase": dominant, "achieved": achieved,
-                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                         "traffic": traffic, "launch_ms": dom_ms / max(dom_calls, 1)},
-            "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d / e2e_steps,
-                    "d2h_bytes_per_step": scene.n * 16, "steps": e2e_steps},
-            "gpu_launches": int(c1["launches"] - c0["launches"]),
-            "clocks": clocks,
-            "phase_ms_per_step": {k: round(v[0] / max(K, 1), 4) for k, v in phases.items()},
-            "diagnostics": {"mean_colors": colors_sum / K,
-                            "list_rebuilds": c1["list_rebuilds"] - c0["list_rebuilds"],
-                            "retries": c1["retries"] - c0["retries"], "regrows": c1["regrows"] - c0["regrows"],
-                            "host_ms_per_step": (c1["host_ms"] - c0["host_ms"]) / K,
-                            "sync_wait_ms_per_step": (c1["sync_ms"] - c0["sync_ms"]) / K,
-                            "max_step_ms": max(per_step), "median_step_ms": statistics.median(per_step)},
-        }
         print(json.dumps(line))
     if world_size > 1:
         dist.barrier()

@@ -3,8 +3,7 @@
  * C ABI of libag2d.so: opaque handles, plain pointers and sizes, int32 status codes. Every entry point below
  * names the reference interface it replaces (paths relative to PhysicsSimulation-Agony/PS_AGONY2D/ in
  * Shadow001111/PhysicsSimulation-Agony). The reference is statically linked C++ with no FFI of its own; these are
- * the calls its Simulation / ObjectAPI boundary maps onto (see INTEGRATION.md for the C++ facade and ctypes
- * binding).
+ * the calls its Simulation / ObjectAPI boundary maps onto.
  *
  * Threading: a world is driven by one host thread at a time (the reference's Simulation is single-caller too,
  * Simulation.h:36). Distinct worlds and batches may be driven from distinct threads.
@@ -55,7 +54,7 @@ typedef struct ag2d_body_desc {
     uint32_t material;
 } ag2d_body_desc;
 
-/* Per-step counters (debug data): SURVEY-style metrics the reference keeps in DebugData. */
+/* Per-step counters (the step statistics the reference keeps in its DebugData). */
 typedef struct ag2d_counters {
     uint32_t status;        /* device status bits of the last step */
     uint32_t pairs;         /* broad-phase candidate pairs */
@@ -136,6 +135,7 @@ enum ag2d_phase {
     AG2D_PHASE_NARROW,             /* narrow phase on AG2D_PAIRS, warm start from AG2D_PREV_MANIFOLDS */
     AG2D_PHASE_SOLVE,              /* colouring + solver on AG2D_MANIFOLDS */
     AG2D_PHASE_ISLANDS,            /* islands + sleep flags from AG2D_MANIFOLDS */
+    AG2D_PHASE_COLLIDE,            /* collision detection alone: dynamic poses + AABBs, broad, narrow (no warm start) */
 };
 
 /* ---- library ---- */
@@ -162,6 +162,14 @@ int32_t ag2d_world_add_box(ag2d_world* world, const ag2d_body_desc* body, float 
                            uint64_t* out_handle);
 int32_t ag2d_world_add_polygon(ag2d_world* world, const ag2d_body_desc* body, const float* vertices_xy,
                                uint32_t vertex_count, uint64_t* out_handle);
+/* Creates 'count' bodies in one call: the same bodies, in the same order, as the matching add_circle / add_box /
+ * add_polygon calls (a scene loader's loop over ObjectAPI::create*, ObjectAPI.h:20-45, without a call per body).
+ * kinds[i]: 0 circle (params[2i] = radius), 1 box (params[2i], params[2i+1] = width, height), 2 polygon
+ * (poly_counts[i] vertex pairs at poly_xy + 2 * poly_offsets[i]). out_handles may be NULL. Stops at the first body
+ * that cannot be created (its index is in the error string); the bodies before it stay created. */
+int32_t ag2d_world_add_bodies(ag2d_world* world, uint32_t count, const ag2d_body_desc* bodies,
+                              const uint32_t* kinds, const float* params, const uint32_t* poly_offsets,
+                              const uint32_t* poly_counts, const float* poly_xy, uint64_t* out_handles);
 /* Dense body index of a handle (ObjectAPI::getBodyIndex, ObjectAPI.h:53), or UINT32_MAX if stale. */
 uint32_t ag2d_world_body_index(ag2d_world* world, uint64_t handle);
 

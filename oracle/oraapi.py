@@ -242,6 +242,29 @@ def warm_start(prev: np.ndarray, prev_slots: np.ndarray, cur: np.ndarray, cur_sl
     return c
 
 
+def broad_pairs_from_aabbs(minx, miny, maxx, maxy, body) -> np.ndarray:
+    """Candidate pairs of a world whose colliders are all dynamic, from their AABBs and owner bodies (the oracle's
+    x-sweep, ora_broad_pairs): (min, max) collider pairs that overlap strictly and belong to different bodies."""
+    n = int(np.asarray(minx).size)
+    c = OraWorldC()
+    c.n_bodies = int(np.max(body)) + 1 if n else 0
+    c.n_colliders = n
+    for k, v in enumerate((0, 0, 0, n)):
+        c.col_starts[k] = v
+    keep = []
+    for name, arr in (("minX", minx), ("minY", miny), ("maxX", maxx), ("maxY", maxy), ("bodyIndex", body)):
+        a = np.ascontiguousarray(arr, dtype=np.uint32 if name == "bodyIndex" else np.float32)
+        keep.append(a)
+        setattr(c, name, a.ctypes.data_as(_U if a.dtype == np.uint32 else _F))
+    cap = max(16 * n, 1024)
+    while True:
+        out = np.zeros((cap, 2), np.uint32)
+        got = lib().ora_broad_pairs(ctypes.byref(c), out.ctypes.data, cap)
+        if got >= 0:
+            return out[:got]
+        cap = int(-got)   # the buffer was too small: the count comes back negated
+
+
 def fastcossin(angles: np.ndarray):
     a = np.ascontiguousarray(angles, dtype=np.float32)
     c = np.empty_like(a)

@@ -382,6 +382,31 @@ extern "C"
         return std::chrono::duration<double>(t1 - t0).count();
     }
 
+    // Wall-clock seconds of the collision detection part of one step on the current state, as collisionStep runs
+    // it (Simulation.cpp:410-421): spatial data (poses, AABBs, trees), broad phase, narrow phase. Nothing is
+    // integrated or solved. Reports the pair and manifold counts.
+    double agref_timed_collide(void* hp, uint64_t* out_pairs, uint64_t* out_manifolds)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        useBackend(h);
+        Simulation& s = h->sim;
+        s.flushCommands();
+        s.setDataViewers();
+        const auto t0 = std::chrono::steady_clock::now();
+        if (s.objectManager.spatialDirty) s.rebuildSpatialData();
+        else s.updateDynamicSpatialData();
+        std::span<const ObjectPair> broad{};
+        std::span<BodyCollisionData> narrow{};
+        if (s.objectManager.colliders.getCount() > 1) {
+            broad = s.broadPhaseCollisionDetector.findCollisions(ExecutionPolicy::ForceSingleThreaded);
+            if (!broad.empty()) narrow = s.narrowPhaseCollisionDetector.findCollisions(broad);
+        }
+        const auto t1 = std::chrono::steady_clock::now();
+        if (out_pairs) *out_pairs = broad.size();
+        if (out_manifolds) *out_manifolds = narrow.size();
+        return std::chrono::duration<double>(t1 - t0).count();
+    }
+
     uint32_t agref_body_count(void* hp) { return uint32_t(static_cast<Harness*>(hp)->sim.objectManager.bodies.getCount()); }
     uint32_t agref_collider_count(void* hp) { return uint32_t(static_cast<Harness*>(hp)->sim.objectManager.colliders.getCount()); }
     uint32_t agref_manifold_count(void* hp) { return uint32_t(static_cast<Harness*>(hp)->sim.getBodyCollisionData().size()); }

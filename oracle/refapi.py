@@ -51,6 +51,8 @@ def lib():
         L.agref_update.argtypes = [vp, i32]
         L.agref_timed_update.restype = ctypes.c_double
         L.agref_timed_update.argtypes = [vp, i32]
+        L.agref_timed_collide.restype = ctypes.c_double
+        L.agref_timed_collide.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
         L.agref_body_count.restype = u32
         L.agref_body_count.argtypes = [vp]
         L.agref_collider_count.restype = u32
@@ -124,6 +126,12 @@ class RefSim:
 
     def update(self, steps: int = 1):
         lib().agref_update(self.h, steps)
+
+    def timed_collide(self):
+        """(seconds, pairs, manifolds) of one collision detection pass (spatial data, broad, narrow)."""
+        p, m = ctypes.c_uint64(), ctypes.c_uint64()
+        t = lib().agref_timed_collide(self.h, ctypes.byref(p), ctypes.byref(m))
+        return float(t), int(p.value), int(m.value)
 
     def timed_update(self, steps: int) -> float:
         return float(lib().agref_timed_update(self.h, steps))

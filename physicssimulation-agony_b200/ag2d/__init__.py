@@ -1,8 +1,8 @@
 """ag2d: B200-native collision and contact pipeline behind the PS_AGONY2D world/body/shape/step API.
 
 Python binding over the C ABI of libag2d.so (include/ag2d.h). The library is the CUDA implementation; there is no
-CPU fallback: importing this package on a machine without the built library raises, and creating a world without
-a CUDA device returns AG2D_ERR_NO_DEVICE.
+CPU fallback: the first call into the library raises ImportError when the built library is missing (the scene
+generators import without it), and creating a world without a CUDA device returns AG2D_ERR_NO_DEVICE.
 
     from ag2d import World, scenes
     w = World.from_scene(scenes.make_c1(2048))
@@ -31,7 +31,7 @@ COL_WORLD_X, COL_WORLD_Y, COL_WORLD_ROTATION, COL_WORLD_COS, COL_WORLD_SIN, COL_
 DYN_SORTED, DYN_MORTON, PAIRS, MANIFOLDS, PREV_MANIFOLDS, SOLVE_ORDER, COLOR_STARTS = range(64, 71)
 # enum ag2d_phase
 PHASE_INTEGRATE, PHASE_SPATIAL_FULL, PHASE_SPATIAL_DYNAMIC, PHASE_BROAD, PHASE_NARROW, PHASE_SOLVE, \
-    PHASE_ISLANDS = range(1, 8)
+    PHASE_ISLANDS, PHASE_COLLIDE = range(1, 9)
 
 MANIFOLD_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("nx", "<f4"), ("ny", "<f4"), ("depth", "<f4"),
                            ("count", "<u4"), ("id0", "<u4"), ("id1", "<u4"), ("px0", "<f4"), ("py0", "<f4"),
@@ -59,6 +59,11 @@ class BodyDesc(ctypes.Structure):
     _fields_ = [("x", ctypes.c_float), ("y", ctypes.c_float), ("rotation", ctypes.c_float), ("vx", ctypes.c_float),
                 ("vy", ctypes.c_float), ("angular_velocity", ctypes.c_float), ("mass", ctypes.c_float),
                 ("material", ctypes.c_uint32)]
+
+
+_BODY_DESC_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("rotation", "<f4"), ("vx", "<f4"), ("vy", "<f4"),
+                             ("w", "<f4"), ("mass", "<f4"), ("material", "<u4")])
+assert _BODY_DESC_DTYPE.itemsize == ctypes.sizeof(BodyDesc)
 
 
 class Counters(ctypes.Structure):
@@ -104,6 +109,7 @@ def _load():
                                      ctypes.POINTER(u64)]
     L.ag2d_world_add_polygon.argtypes = [vp, ctypes.POINTER(BodyDesc), vp, u32, ctypes.POINTER(u64)]
     L.ag2d_world_body_index.restype = u32
+    L.ag2d_world_add_bodies.argtypes = [vp, u32, ctypes.POINTER(BodyDesc), vp, vp, vp, vp, vp, vp]
     L.ag2d_world_body_index.argtypes = [vp, u64]
     L.ag2d_world_load_state.argtypes = [vp, ctypes.POINTER(StateDesc)]
     L.ag2d_world_step.argtypes = [vp, i32]
@@ -220,19 +226,33 @@ class World:
     def from_scene(cls, scene, device=0, **kw):
         w = cls(dt=scene.dt, velocity_iterations=scene.velocity_iterations,
                 position_iterations=scene.position_iterations, gravity=scene.gravity, device=device, **kw)
-        mats = [w.add_material(*m) for m in scene.materials]
-        for i in range(scene.n):
-            mat = mats[int(scene.material[i]) - 1] if int(scene.material[i]) >= 1 else 0
-            args = (float(scene.px[i]), float(scene.py[i]), float(scene.rot[i]), float(scene.vx[i]),
-                    float(scene.vy[i]), float(scene.w[i]), float(scene.mass[i]), mat)
-            k = int(scene.kind[i])
-            if k == scenes.POLYGON:
-                w.add_polygon(scene.polygon_vertices(i), *args)
-            elif k == scenes.BOX:
-                w.add_box(float(scene.width[i]), float(scene.height[i]), *args)
-            else:
-                w.add_circle(float(scene.radius[i]), *args)
+        w.add_scene(scene)
         return w
+
+    def add_scene(self, scene) -> np.ndarray:
+        """Adds every body of a scene (ag2d.scenes.Scene) with one ag2d_world_add_bodies call; returns handles."""
+        mats = np.asarray([self.add_material(*m) for m in scene.materials] or [0], dtype=np.uint32)
+        n = scene.n
+        descs = (BodyDesc * max(n, 1))()
+        d = np.ctypeslib.as_array(ctypes.cast(descs, ctypes.POINTER(ctypes.c_uint8)),
+                                  shape=(max(n, 1) * ctypes.sizeof(BodyDesc),)).view(_BODY_DESC_DTYPE)[:n]
+        d["x"], d["y"], d["rotation"] = scene.px, scene.py, scene.rot
+        d["vx"], d["vy"], d["w"], d["mass"] = scene.vx, scene.vy, scene.w, scene.mass
+        m = scene.material.astype(np.int64)
+        d["material"] = np.where(m >= 1, mats[np.clip(m - 1, 0, len(mats) - 1)], 0)
+        kinds = np.ascontiguousarray(scene.kind, dtype=np.uint32)
+        params = np.zeros((max(n, 1), 2), np.float32)
+        circ, box = kinds == scenes.CIRCLE, kinds == scenes.BOX
+        params[:n, 0] = np.where(circ, scene.radius, np.where(box, scene.width, 0.0))
+        params[:n, 1] = np.where(box, scene.height, 0.0)
+        offs = np.ascontiguousarray(scene.poly_offset, dtype=np.uint32)
+        cnts = np.ascontiguousarray(scene.poly_count, dtype=np.uint32)
+        xy = np.ascontiguousarray(scene.poly_xy, dtype=np.float32).reshape(-1)
+        handles = np.zeros(max(n, 1), np.uint64)
+        _check(lib.ag2d_world_add_bodies(self.h, n, descs, kinds.ctypes.data, params.ctypes.data, offs.ctypes.data,
+                                         cnts.ctypes.data, xy.ctypes.data if xy.size else None,
+                                         handles.ctypes.data))
+        return handles[:n]
 
     def load_state(self, state: dict, prefix: str = "", materials=None, body_prefix=None):
         """Replaces the world by a reference-layout state dict ("body.comX", "col.bodyIndex", ...)."""

@@ -177,16 +177,24 @@ def log_uniform_counts(rng: np.random.Generator, count: int, lo: int, hi: int) -
     return np.floor(np.exp(rng.uniform(math.log(lo), math.log(hi + 1), count))).astype(np.int64).clip(lo, hi)
 
 
-def make_c4_worlds(worlds: int = 4096, seed: int = 0, lo: int = 16, hi: int = 2048) -> list:
+def _c4_world(args):
+    count, world_seed = args
+    scale = math.sqrt(count / 2048.0)
+    return make_c1(int(count), world_seed, width=max(20.0, 200.0 * scale), height=max(10.0, 100.0 * scale))
+
+
+def make_c4_worlds(worlds: int = 4096, seed: int = 0, lo: int = 16, hi: int = 2048, processes: int = 1) -> list:
     """Batched worlds: body counts log-uniform in [lo, hi]; world k is make_c1(count_k, seed + k) (c1 shape mix,
-    own ground box), with the region scaled so the body density matches c1 (2048 bodies in 200 x 100 m)."""
+    own ground box), with the region scaled so the body density matches c1 (2048 bodies in 200 x 100 m).
+    processes > 1 generates the worlds in a spawned process pool (same worlds: each has its own seed)."""
     rng = np.random.default_rng(seed)
     counts = log_uniform_counts(rng, worlds, lo, hi)
-    out = []
-    for k in range(worlds):
-        scale = math.sqrt(counts[k] / 2048.0)
-        out.append(make_c1(int(counts[k]), seed + k, width=max(20.0, 200.0 * scale), height=max(10.0, 100.0 * scale)))
-    return out
+    jobs = [(int(counts[k]), seed + k) for k in range(worlds)]
+    if processes > 1 and worlds > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(processes) as pool:
+            return pool.map(_c4_world, jobs, chunksize=max(1, worlds // (4 * processes)))
+    return [_c4_world(j) for j in jobs]
 
 
 def make_c5_request(rng: np.random.Generator, request_id: int, lo: int = 32, hi: int = 8192) -> Scene:

@@ -10,7 +10,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -199,6 +201,53 @@ constexpr uint32_t GRID_SOLVE_THRESHOLD = 600000;
 
 }  // namespace
 
+// Launch limits of the solver kernels on a device (queried once per device and process).
+static DeviceInfo probe_device(int device)
+{
+    static std::mutex mu;
+    static std::map<int, DeviceInfo> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(device);
+    if (it != cache.end()) return it->second;
+    DeviceInfo dev;
+    CK(cudaDeviceGetAttribute(&dev.sms, cudaDevAttrMultiProcessorCount, device));
+    int perSm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color_solve_grid, 256, 0));
+    dev.coopSolveBlocks = std::max(1, perSm) * dev.sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color_solve_worlds, SOLVE_WORLD_THREADS, 0));
+    dev.worldSolveBlocks = std::max(1, perSm) * dev.sms;
+    // Largest cluster (16 non-portable, else 8, 4, 2) that can be resident.
+    dev.solveCluster = 1;
+    if (cudaFuncSetAttribute(k_color_solve_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+        cudaSuccess) {
+        for (int cl : {16, 8, 4, 2}) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(cl);
+            cfg.blockDim = dim3(SOLVE_CLUSTER_THREADS);
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = cl;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, k_color_solve_cluster, &cfg) == cudaSuccess &&
+                clusters >= 1) {
+                dev.solveCluster = cl;
+                break;
+            }
+        }
+    }
+    cudaGetLastError();
+    // AG2D_SOLVER=grid forces the whole-grid solver (test hook for that variant).
+    if (const char* v = std::getenv("AG2D_SOLVER")) {
+        if (std::string(v) == "grid") dev.solveCluster = 1;
+    }
+    cache[device] = dev;
+    return dev;
+}
+
 struct ag2d_world {
     ag2d_world_settings settings{};
     cudaStream_t stream = nullptr;
@@ -372,48 +421,24 @@ struct ag2d_world {
         return uint32_t(std::max<uint64_t>(1, std::min(want, cap)));
     }
 
+    // Settings only: device resources are created on first device use (creating many worlds on the host, e.g. to
+    // pack them into a batch, costs no CUDA calls per world).
     void init(const ag2d_world_settings& s)
     {
         settings = s;
         int count = 0;
         if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) throw ApiError(AG2D_ERR_NO_DEVICE, "no CUDA device");
         if (s.device < 0 || s.device >= count) throw ApiError(AG2D_ERR_INVALID_ARG, "device ordinal out of range");
-        CK(cudaSetDevice(s.device));
+    }
+
+    bool deviceReady() const { return stream != nullptr; }
+
+    void ensureDevice()
+    {
+        if (deviceReady()) return;
+        CK(cudaSetDevice(settings.device));
+        dev = probe_device(settings.device);
         CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-        CK(cudaDeviceGetAttribute(&dev.sms, cudaDevAttrMultiProcessorCount, s.device));
-        int perSm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color_solve_grid, 256, 0));
-        dev.coopSolveBlocks = std::max(1, perSm) * dev.sms;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color_solve_worlds, SOLVE_WORLD_THREADS, 0));
-        dev.worldSolveBlocks = std::max(1, perSm) * dev.sms;
-        // Largest cluster (16 non-portable, else 8) that can be resident.
-        dev.solveCluster = 1;
-        if (cudaFuncSetAttribute(k_color_solve_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
-            cudaSuccess) {
-            for (int cl : {16, 8, 4, 2}) {
-                cudaLaunchConfig_t cfg = {};
-                cfg.gridDim = dim3(cl);
-                cfg.blockDim = dim3(SOLVE_CLUSTER_THREADS);
-                cudaLaunchAttribute attr[1];
-                attr[0].id = cudaLaunchAttributeClusterDimension;
-                attr[0].val.clusterDim.x = cl;
-                attr[0].val.clusterDim.y = 1;
-                attr[0].val.clusterDim.z = 1;
-                cfg.attrs = attr;
-                cfg.numAttrs = 1;
-                int clusters = 0;
-                if (cudaOccupancyMaxActiveClusters(&clusters, k_color_solve_cluster, &cfg) == cudaSuccess &&
-                    clusters >= 1) {
-                    dev.solveCluster = cl;
-                    break;
-                }
-            }
-        }
-        cudaGetLastError();
-        // AG2D_SOLVER=grid forces the whole-grid solver (test hook for that variant).
-        if (const char* v = std::getenv("AG2D_SOLVER")) {
-            if (std::string(v) == "grid") dev.solveCluster = 1;
-        }
         CK(cudaMallocHost(reinterpret_cast<void**>(&hCounters), sizeof(StepCounters)));
         std::memset(hCounters, 0, sizeof(StepCounters));
         dCounters.reserve(1);
@@ -457,50 +482,56 @@ struct ag2d_world {
         scanner.reserve(std::max({pairCap, nColliders, nBodies}));
     }
 
-    // Uploads the host objects (bodies, colliders, shapes, materials) as the device state.
-    void upload()
+    // The host objects (bodies, colliders, shapes, materials) in the upload format.
+    void hostArrays(PackedArrays& a) const
     {
         const HostObjects& o = objects;
-        nBodies = uint32_t(o.bodies.size());
-        nColliders = uint32_t(o.colliders.size());
-        std::vector<float4> vel(nBodies), pos(nBodies);
-        std::vector<float2> rot(nBodies);
-        std::vector<float> wc(nBodies), br(nBodies), st(nBodies);
-        std::vector<uint8_t> state(nBodies);
-        std::vector<uint32_t> isl(nBodies);
-        for (uint32_t i = 0; i < nBodies; i++) {
+        const uint32_t nb = uint32_t(o.bodies.size()), nc = uint32_t(o.colliders.size());
+        a.vel.resize(nb); a.pos.resize(nb); a.rot.resize(nb); a.wc.resize(nb); a.br.resize(nb); a.st.resize(nb);
+        a.state.resize(nb); a.isl.resize(nb);
+        for (uint32_t i = 0; i < nb; i++) {
             const HBody& b = o.bodies[i];
-            vel[i] = make_float4(b.vx, b.vy, b.w, b.invMass);
-            pos[i] = make_float4(b.comX, b.comY, b.rot, b.invInertia);
-            rot[i] = make_float2(b.cos, b.sin);
-            wc[i] = b.wrapCount; br[i] = b.boundRadius; st[i] = b.sleepTimer;
-            state[i] = uint8_t(o.bodyGroups.groupOf(i) == 0 ? STATE_STATIC :
-                               (o.bodyGroups.groupOf(i) == 1 ? STATE_SLEEPING : STATE_DYNAMIC));
-            isl[i] = b.sleepIsland;
+            a.vel[i] = make_float4(b.vx, b.vy, b.w, b.invMass);
+            a.pos[i] = make_float4(b.comX, b.comY, b.rot, b.invInertia);
+            a.rot[i] = make_float2(b.cos, b.sin);
+            a.wc[i] = b.wrapCount; a.br[i] = b.boundRadius; a.st[i] = b.sleepTimer;
+            a.state[i] = uint8_t(o.bodyGroups.groupOf(i) == 0 ? STATE_STATIC :
+                                 (o.bodyGroups.groupOf(i) == 1 ? STATE_SLEEPING : STATE_DYNAMIC));
+            a.isl[i] = b.sleepIsland;
         }
-        std::vector<uint32_t> cb(nColliders), cs(nColliders), cm(nColliders);
-        std::vector<float4> co(nColliders);
-        for (uint32_t i = 0; i < nColliders; i++) {
+        a.cb.resize(nc); a.cs.resize(nc); a.cm.resize(nc); a.co.resize(nc);
+        for (uint32_t i = 0; i < nc; i++) {
             const HCollider& c = o.colliders[i];
-            cb[i] = c.body; cs[i] = (c.type << 30) | c.shape; cm[i] = c.material;
-            co[i] = make_float4(c.comOffX, c.comOffY, c.localRot, 0.0f);
+            a.cb[i] = c.body; a.cs[i] = (c.type << 30) | c.shape; a.cm[i] = c.material;
+            a.co[i] = make_float4(c.comOffX, c.comOffY, c.localRot, 0.0f);
         }
-        std::vector<float2> bh(o.boxHalfW.size());
-        for (size_t i = 0; i < bh.size(); i++) bh[i] = make_float2(o.boxHalfW[i], o.boxHalfH[i]);
-        std::vector<uint32_t> po, pc;
-        std::vector<float2> pv, pn;
+        a.cr = o.circleRadius;
+        a.bh.resize(o.boxHalfW.size());
+        for (size_t i = 0; i < a.bh.size(); i++) a.bh[i] = make_float2(o.boxHalfW[i], o.boxHalfH[i]);
+        a.po.clear(); a.pc.clear(); a.pv.clear(); a.pn.clear();
         for (const HPolygon& p : o.polygons) {
-            po.push_back(uint32_t(pv.size()));
-            pc.push_back(uint32_t(p.verts.size() / 2));
+            a.po.push_back(uint32_t(a.pv.size()));
+            a.pc.push_back(uint32_t(p.verts.size() / 2));
             for (size_t k = 0; k < p.verts.size() / 2; k++) {
-                pv.push_back(make_float2(p.verts[2 * k], p.verts[2 * k + 1]));
-                pn.push_back(make_float2(p.normals[2 * k], p.normals[2 * k + 1]));
+                a.pv.push_back(make_float2(p.verts[2 * k], p.verts[2 * k + 1]));
+                a.pn.push_back(make_float2(p.normals[2 * k], p.normals[2 * k + 1]));
             }
         }
-        std::vector<float4> mats(o.materialCount());
-        for (size_t i = 0; i < mats.size(); i++)
-            mats[i] = make_float4(o.materials[3 * i], o.materials[3 * i + 1], o.materials[3 * i + 2], 0.0f);
-        uploadArrays(vel, pos, rot, wc, br, st, state, isl, cb, cs, cm, co, o.circleRadius, bh, po, pc, pv, pn, mats);
+        a.mats.resize(o.materialCount());
+        for (size_t i = 0; i < a.mats.size(); i++)
+            a.mats[i] = make_float4(o.materials[3 * i], o.materials[3 * i + 1], o.materials[3 * i + 2], 0.0f);
+        a.prev.clear();
+    }
+
+    // Uploads the host objects as the device state.
+    void upload()
+    {
+        PackedArrays a;
+        hostArrays(a);
+        nBodies = uint32_t(a.vel.size());
+        nColliders = uint32_t(a.cb.size());
+        uploadArrays(a.vel, a.pos, a.rot, a.wc, a.br, a.st, a.state, a.isl, a.cb, a.cs, a.cm, a.co, a.cr, a.bh, a.po,
+                     a.pc, a.pv, a.pn, a.mats);
     }
 
     void uploadArrays(const std::vector<float4>& vel, const std::vector<float4>& pos, const std::vector<float2>& rot,
@@ -512,6 +543,7 @@ struct ag2d_world {
                       const std::vector<uint32_t>& pc, const std::vector<float2>& pv,
                       const std::vector<float2>& pn, const std::vector<float4>& mats)
     {
+        ensureDevice();
         const cudaStream_t s = stream;
         bvel.upload(vel.data(), nBodies, s); bpos.upload(pos.data(), nBodies, s); brot.upload(rot.data(), nBodies, s);
         wrapCount.upload(wc.data(), nBodies, s); boundRadius.upload(br.data(), nBodies, s);
@@ -553,12 +585,17 @@ struct ag2d_world {
 
     void ensureUploaded()
     {
+        ensureDevice();
         if (hostDirty) upload();
     }
 
     // The device state as upload-format host arrays plus the warm-start manifolds (for packing into a batch).
     void exportArrays(PackedArrays& a)
     {
+        if (hostDirty) {   // never uploaded (or changed on the host since): no device round trip
+            hostArrays(a);
+            return;
+        }
         ensureUploaded();
         const cudaStream_t s = stream;
         auto get = [&](auto& v, const auto* p, size_t n) {
@@ -779,7 +816,7 @@ struct ag2d_world {
         pend(4);
     }
 
-    void phaseNarrow()
+    void phaseNarrow(bool warm = true)
     {
         const cudaStream_t s = stream;
         const uint32_t* nPairs = &dCounters.p->pairs;
@@ -797,6 +834,7 @@ struct ag2d_world {
                                                manifoldCap, nManifolds.p, dCounters.p);
         CK(cudaGetLastError());
         pend(6);
+        if (!warm) return;
         pbegin(7);
         // Warm start from the previous step's manifolds.
         CK(cudaMemsetAsync(hashKeys.p, 0xFF, size_t(hashCap) * sizeof(unsigned long long), s));
@@ -1093,6 +1131,42 @@ int32_t ag2d_world_add_polygon(ag2d_world* world, const ag2d_body_desc* body, co
     });
 }
 
+int32_t ag2d_world_add_bodies(ag2d_world* world, uint32_t count, const ag2d_body_desc* bodies,
+                              const uint32_t* kinds, const float* params, const uint32_t* poly_offsets,
+                              const uint32_t* poly_counts, const float* poly_xy, uint64_t* out_handles)
+{
+    return guarded([&] {
+        if (!world || (count && (!bodies || !kinds || !params)))
+            throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        pull_state(world);
+        for (uint32_t i = 0; i < count; i++) {
+            float d[7];
+            body_desc(bodies + i, d);
+            uint64_t h = 0;
+            std::string err;
+            bool ok = false;
+            int32_t code = AG2D_ERR_INVALID_ARG;
+            switch (kinds[i]) {
+            case SHAPE_CIRCLE: ok = world->objects.addCircle(d, bodies[i].material, params[2 * i], h, err); break;
+            case SHAPE_BOX:
+                ok = world->objects.addBox(d, bodies[i].material, params[2 * i], params[2 * i + 1], h, err);
+                break;
+            case SHAPE_POLYGON:
+                if (!poly_offsets || !poly_counts || !poly_xy) { err = "polygon without vertex arrays"; break; }
+                ok = world->objects.addPolygon(d, bodies[i].material, poly_xy + 2 * size_t(poly_offsets[i]),
+                                               poly_counts[i], h, err);
+                if (!ok && (err.find("not convex") != std::string::npos || err.find("16") != std::string::npos))
+                    code = AG2D_ERR_UNSUPPORTED;
+                break;
+            default: err = "unknown shape kind"; break;
+            }
+            if (!ok) throw ApiError(code, "body " + std::to_string(i) + ": " + err);
+            world->hostDirty = true;
+            if (out_handles) out_handles[i] = h;
+        }
+    });
+}
+
 uint32_t ag2d_world_body_index(ag2d_world* world, uint64_t handle)
 {
     return world ? world->objects.indexOf(handle) : 0xFFFFFFFFu;
@@ -1178,7 +1252,8 @@ int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out)
 {
     return guarded([&] {
         if (!world || !out) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
-        const StepCounters& c = *world->hCounters;
+        static const StepCounters none{};
+        const StepCounters& c = world->hCounters ? *world->hCounters : none;
         out->status = c.status; out->pairs = c.pairs; out->manifolds = c.manifolds; out->colors = c.colors;
         out->woke = c.woke; out->slept = c.slept; out->warm_hits = c.warmHits;
         out->sleeping = world->nBodies - world->nDynBody - world->nStatic;
@@ -1220,6 +1295,7 @@ int32_t ag2d_world_stream(ag2d_world* world, void** out_stream)
 {
     return guarded([&] {
         if (!world || !out_stream) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        world->ensureDevice();
         *out_stream = world->stream;
     });
 }
@@ -1416,6 +1492,12 @@ int32_t ag2d_world_run_phase(ag2d_world* world, int32_t phase)
             w.phaseBroad();
             break;
         case AG2D_PHASE_NARROW: w.phaseNarrow(); break;
+        case AG2D_PHASE_COLLIDE:
+            CK(cudaMemsetAsync(w.dCounters.p, 0, sizeof(StepCounters), w.stream));
+            w.phasePose(false);
+            w.phaseBroad();
+            w.phaseNarrow(false);
+            break;
         case AG2D_PHASE_SOLVE: w.phaseSolve(); break;
         case AG2D_PHASE_ISLANDS: w.phaseIslands(); break;
         default: throw ApiError(AG2D_ERR_INVALID_ARG, "unknown phase");
