@@ -80,6 +80,14 @@ enum ag2d_timed_phase {
     AG2D_T_LBVH, AG2D_T_COUNT
 };
 
+/* Launch shapes chosen by ag2d_world_autotune. */
+typedef struct ag2d_tuning {
+    uint32_t team_colliders;   /* batched solver: consecutive worlds per CTA team (0 for a single world) */
+    uint32_t query_threads;    /* pair-query block size */
+    uint32_t narrow_threads;   /* narrow-phase block size */
+    float solve_ms, query_ms, narrow_ms;   /* device time per step of each phase at the chosen setting */
+} ag2d_tuning;
+
 /* Reference-layout world state for ag2d_world_load_state: every array in the reference's dense order, as its
  * SoA viewers expose them (SoA/BodySoA.h:14-36, SoA/ColliderSoA.h:10-32, SoA/Shapes/*.h). Group starts are
  * GroupRanges::starts (GroupRanges.h:130-157): static, sleeping, dynamic, end. */
@@ -182,6 +190,12 @@ int32_t ag2d_world_step(ag2d_world* world, int32_t steps);
 
 int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out);
 
+/* Launch-shape autotuner (no reference counterpart: the reference runs on CPU threads). Times real steps under each
+ * candidate solver team size (batches), pair-query and narrow-phase block size and keeps the fastest. A step's
+ * results do not depend on these settings, so tuning only advances the world: by 1 + candidates x
+ * (steps_per_candidate + 1) steps, with 10 candidates for a batch and 6 for a single world. Works on a batch
+ * through ag2d_batch_engine. */
+int32_t ag2d_world_autotune(ag2d_world* world, int32_t steps_per_candidate, ag2d_tuning* out);
 /* Device timing of the step phases (the reference's Tracy zones, Profiling/TracyProfiler.h:66-72, become CUDA
  * events on the world's stream). Enabling resets the totals. out_ms receives cumulative milliseconds per
  * enum ag2d_timed_phase, out_calls the number of timed occurrences. */

@@ -74,6 +74,12 @@ class Counters(ctypes.Structure):
                 ("regrows", ctypes.c_uint64), ("host_ms", ctypes.c_double), ("sync_ms", ctypes.c_double)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("team_colliders", ctypes.c_uint32), ("query_threads", ctypes.c_uint32),
+                ("narrow_threads", ctypes.c_uint32), ("solve_ms", ctypes.c_float), ("query_ms", ctypes.c_float),
+                ("narrow_ms", ctypes.c_float)]
+
+
 TIMED_PHASES = ("integrate", "pose", "tree_dynamic", "tree_other", "query", "narrow", "compact", "warm", "wake",
                 "color", "solve", "islands", "sort", "lbvh")
 
@@ -119,6 +125,7 @@ def _load():
     L.ag2d_world_write.argtypes = [vp, i32, vp, u64]
     L.ag2d_world_run_phase.argtypes = [vp, i32]
     L.ag2d_world_set_profiling.argtypes = [vp, i32]
+    L.ag2d_world_autotune.argtypes = [vp, i32, ctypes.POINTER(Tuning)]
     L.ag2d_world_phase_times.argtypes = [vp, vp, vp, i32]
     L.ag2d_world_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.ag2d_batch_create.argtypes = [ctypes.POINTER(vp), u32, ctypes.POINTER(vp)]
@@ -306,6 +313,12 @@ class World:
         c = Counters()
         _check(lib.ag2d_world_counters(self.h, ctypes.byref(c)))
         return {n: (float(getattr(c, n)) if t is ctypes.c_double else int(getattr(c, n))) for n, t in Counters._fields_}
+
+    def autotune(self, steps_per_candidate: int = 3) -> dict:
+        """Launch-shape autotuner (solver team size, query and narrow block sizes); advances the world."""
+        t = Tuning()
+        _check(lib.ag2d_world_autotune(self.h, steps_per_candidate, ctypes.byref(t)))
+        return {n: (float(getattr(t, n)) if k is ctypes.c_float else int(getattr(t, n))) for n, k in Tuning._fields_}
 
     def set_profiling(self, enable: bool = True):
         _check(lib.ag2d_world_set_profiling(self.h, 1 if enable else 0))

@@ -18,10 +18,33 @@ namespace cg = cooperative_groups;
 // fallback, iterative friction), solvePositionConstraints (:930-980), scatterImpulses (:392-414). A team runs every
 // pass colour by colour with its barrier between colours.
 // ---------------------------------------------------------------------------------------------------------------
-__device__ __forceinline__ void prep_constraint(const DeviceWorld& w, const Manifold& m, uint32_t mi, Constraint& k)
+// Body state seen by the solver: global memory, or a team's contiguous body range staged in shared memory.
+struct GlobalBodies {
+    float4* vel;
+    float4* pos;
+    __device__ __forceinline__ float4 v(uint32_t b) const { return vel[b]; }
+    __device__ __forceinline__ float4 p(uint32_t b) const { return pos[b]; }
+    __device__ __forceinline__ void setV(uint32_t b, const float4& x) const { vel[b] = x; }
+    __device__ __forceinline__ void setP(uint32_t b, const float4& x) const { pos[b] = x; }
+    __device__ __forceinline__ float invMass(uint32_t b) const { return __ldcg(&vel[b].w); }
+};
+struct SharedBodies {
+    float4* vel;     // shared: bodies [base, base + count)
+    float4* pos;
+    uint32_t base;
+    __device__ __forceinline__ float4 v(uint32_t b) const { return vel[b - base]; }
+    __device__ __forceinline__ float4 p(uint32_t b) const { return pos[b - base]; }
+    __device__ __forceinline__ void setV(uint32_t b, const float4& x) const { vel[b - base] = x; }
+    __device__ __forceinline__ void setP(uint32_t b, const float4& x) const { pos[b - base] = x; }
+    __device__ __forceinline__ float invMass(uint32_t b) const { return vel[b - base].w; }
+};
+
+template <class Bodies>
+__device__ __forceinline__ void prep_constraint(const DeviceWorld& w, const Bodies& B, const Manifold& m, uint32_t mi,
+                                                Constraint& k)
 {
     const uint32_t bA = w.cbody[m.a], bB = w.cbody[m.b];
-    const float4 vA = w.bvel[bA], vB = w.bvel[bB], pA = w.bpos[bA], pB = w.bpos[bB];
+    const float4 vA = B.v(bA), vB = B.v(bB), pA = B.p(bA), pB = B.p(bB);
     k.bodyA = bA; k.bodyB = bB; k.count = m.count; k.manifold = mi;
     k.nx = m.nx; k.ny = m.ny;
     k.imA = vA.w; k.imB = vB.w; k.iIA = pA.w; k.iIB = pB.w;
@@ -55,9 +78,10 @@ __device__ __forceinline__ void prep_constraint(const DeviceWorld& w, const Mani
     k.pad = 0.0f;
 }
 
-__device__ __forceinline__ void warm_constraint(const DeviceWorld& w, const Constraint& k)
+template <class Bodies>
+__device__ __forceinline__ void warm_constraint(const Bodies& B, const Constraint& k)
 {
-    float4 vA = w.bvel[k.bodyA], vB = w.bvel[k.bodyB];
+    float4 vA = B.v(k.bodyA), vB = B.v(k.bodyB);
     const float tx = -k.ny, ty = k.nx;
     const float jn0 = k.count > 0 ? k.jn0 : 0.0f, jt0 = k.count > 0 ? k.jt0 : 0.0f;
     const float jn1 = k.count > 1 ? k.jn1 : 0.0f, jt1 = k.count > 1 ? k.jt1 : 0.0f;
@@ -67,13 +91,14 @@ __device__ __forceinline__ void warm_constraint(const DeviceWorld& w, const Cons
     vB.x = vB.x + ix * k.imB; vB.y = vB.y + iy * k.imB;
     vA.z = vA.z - (jn0 * k.rAn0 + jt0 * k.rAt0 + jn1 * k.rAn1 + jt1 * k.rAt1) * k.iIA;
     vB.z = vB.z + (jn0 * k.rBn0 + jt0 * k.rBt0 + jn1 * k.rBn1 + jt1 * k.rBt1) * k.iIB;
-    if (k.imA > 0.0f) w.bvel[k.bodyA] = vA;
-    if (k.imB > 0.0f) w.bvel[k.bodyB] = vB;
+    if (k.imA > 0.0f) B.setV(k.bodyA, vA);
+    if (k.imB > 0.0f) B.setV(k.bodyB, vB);
 }
 
-__device__ __forceinline__ void velocity_constraint(const DeviceWorld& w, Constraint& k)
+template <class Bodies>
+__device__ __forceinline__ void velocity_constraint(const Bodies& B, Constraint& k)
 {
-    float4 vA = w.bvel[k.bodyA], vB = w.bvel[k.bodyB];
+    float4 vA = B.v(k.bodyA), vB = B.v(k.bodyB);
     const float imA = k.imA, imB = k.imB, iIA = k.iIA, iIB = k.iIB;
     const float nx = k.nx, ny = k.ny, tx = -ny, ty = nx;
     if (k.count == 1) {
@@ -191,21 +216,22 @@ __device__ __forceinline__ void velocity_constraint(const DeviceWorld& w, Constr
             vB.z = vB.z + dj * rBt * iIB;
         }
     }
-    if (imA > 0.0f) w.bvel[k.bodyA] = vA;
-    if (imB > 0.0f) w.bvel[k.bodyB] = vB;
+    if (imA > 0.0f) B.setV(k.bodyA, vA);
+    if (imB > 0.0f) B.setV(k.bodyB, vB);
 }
 
-__device__ __forceinline__ void position_constraint(const DeviceWorld& w, const Constraint& k)
+template <class Bodies>
+__device__ __forceinline__ void position_constraint(const Bodies& B, const Constraint& k)
 {
-    float4 pA = w.bpos[k.bodyA], pB = w.bpos[k.bodyB];
+    float4 pA = B.p(k.bodyA), pB = B.p(k.bodyB);
     const float pen = k.penBase - ((pB.x - pA.x) * k.nx + (pB.y - pA.y) * k.ny);
     if (pen <= 0.0f) return;
-    const float imA = w.bvel[k.bodyA].w, imB = w.bvel[k.bodyB].w;
+    const float imA = B.v(k.bodyA).w, imB = B.v(k.bodyB).w;
     const float total = pen / (imA + imB) * 0.5f;
     const float cA = imA * total, cB = imB * total;
     const float cAx = k.nx * cA, cAy = k.ny * cA, cBx = k.nx * cB, cBy = k.ny * cB;
-    if (imA > 0.0f) { pA.x = pA.x - cAx; pA.y = pA.y - cAy; w.bpos[k.bodyA] = pA; }
-    if (imB > 0.0f) { pB.x = pB.x + cBx; pB.y = pB.y + cBy; w.bpos[k.bodyB] = pB; }
+    if (imA > 0.0f) { pA.x = pA.x - cAx; pA.y = pA.y - cAy; B.setP(k.bodyA, pA); }
+    if (imB > 0.0f) { pB.x = pB.x + cBx; pB.y = pB.y + cBy; B.setP(k.bodyB, pB); }
 }
 
 
@@ -215,14 +241,24 @@ __device__ __forceinline__ uint32_t priority_hash(uint32_t x)
     return x;
 }
 
-// Scratch of one world's colouring and solve.
+// Colour counters: one per colour, then the lengths of the two uncoloured lists, then the colour count.
+constexpr uint32_t COLOR_SLOTS = MAX_COLORS + 4;
+// Colours 0..63 are chosen first-fit from a body's 64-bit mask of neighbouring colours; a manifold whose bodies see
+// all 64 taken gets colour 64 + its round (unique to the round, so still conflict-free).
+constexpr uint32_t MAX_ROUNDS = MAX_COLORS - 64;
+
+// Scratch of one world's (or one team of worlds') colouring and solve.
 struct SolveScratch {
     uint32_t* color;                  // [manifolds]
     uint32_t* order;                  // [manifolds] colour-major solving order
     unsigned long long* bodyMax;      // [bodies], zeroed before the call
-    uint32_t* colorCount;             // [MAX_COLORS + 1], zeroed by the routine
+    unsigned long long* bodyMask;     // [bodies] colours taken around each body, zeroed before the call
+    uint32_t* colorCount;             // [COLOR_SLOTS], zeroed by the routine
     uint32_t* colorStart;             // [MAX_COLORS + 1]
     Constraint* cons;                 // [manifolds]
+    const uint32_t* prio;             // [manifolds] colouring priorities, or null: priority_hash(index)
+    uint32_t* listA;                  // [manifolds] uncoloured manifolds, ping
+    uint32_t* listB;                  // [manifolds] uncoloured manifolds, pong
 };
 
 // Team barriers. ld() reads a colour counter written by other team members before the last barrier: global memory
@@ -242,50 +278,86 @@ struct GridSync {
     static __device__ __forceinline__ uint32_t ld(const uint32_t* p) { return __ldcg(p); }
 };
 
-// Colouring (Luby / Jones-Plassmann rounds: colour r goes to every uncoloured manifold whose priority is the largest
-// on each of its dynamic bodies) followed by the colour-major solve. rank/size: this thread's index in the team.
-// Returns false if the colouring needed more than MAX_COLORS colours or a barrier gave up.
-template <class Sync>
-__device__ bool color_and_solve(const DeviceWorld& w, Manifold* __restrict__ m, uint32_t n, const SolveScratch& s,
-                                uint32_t velIters, uint32_t posIters, uint32_t rank, uint32_t size, Sync sync,
-                                uint32_t* __restrict__ outColors, uint32_t* __restrict__ status)
+// Pulls the 128-byte constraint of slot c into L1 ahead of the pass that reads it.
+__device__ __forceinline__ void prefetch_l1(const void* p)
 {
-    for (uint32_t i = rank; i < n; i += size) s.color[i] = NO_COLOR;
-    for (uint32_t c = rank; c <= MAX_COLORS; c += size) s.colorCount[c] = 0;
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+// The constraint slot this thread handles first in colour 'col' (or nothing), prefetched before the barrier that
+// precedes that colour's pass.
+template <class Sync>
+__device__ __forceinline__ void prefetch_colour(const SolveScratch& s, uint32_t col, uint32_t ncol, uint32_t rank)
+{
+    if (col >= ncol) return;
+    const uint32_t c = Sync::ld(s.colorStart + col) + rank;
+    if (c < Sync::ld(s.colorStart + col + 1)) prefetch_l1(s.cons + c);
+}
+
+// Colouring followed by the colour-major solve. Colouring runs Jones-Plassmann rounds: in round r every uncoloured
+// manifold whose priority is the largest on each of its dynamic bodies takes the smallest colour not yet taken
+// around its dynamic bodies (first fit); winners of one round share no dynamic body, so the colours stay
+// conflict-free and depend only on the manifold list and priorities. Each round visits only the manifolds still
+// uncoloured (compacted into a list whose order does not affect the result). rank/size: this thread's index in the
+// team. Returns false if the colouring ran out of colours or a barrier gave up.
+template <class Sync, class Bodies>
+__device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold* __restrict__ m, uint32_t n,
+                                const SolveScratch& s, uint32_t velIters, uint32_t posIters, uint32_t rank,
+                                uint32_t size, Sync sync, uint32_t* __restrict__ outColors, uint32_t* __restrict__ status)
+{
+    for (uint32_t c = rank; c < COLOR_SLOTS; c += size) s.colorCount[c] = 0;
     if (!sync()) return false;
-    uint32_t rounds = 0;
-    bool done = n == 0;
-    for (uint32_t r = 0; r < MAX_COLORS && !done; r++) {
-        rounds = r + 1;
+    uint32_t* const nColors = s.colorCount + MAX_COLORS + 3;
+    uint32_t len = n;
+    const uint32_t* in = nullptr;   // round 0 visits every manifold
+    for (uint32_t r = 0; r < MAX_ROUNDS && len > 0; r++) {
+        uint32_t* out = (r & 1) ? s.listB : s.listA;
+        uint32_t* outLen = s.colorCount + MAX_COLORS + 1 + (r & 1);
+        // This counter was last read before the barrier that ended the previous round.
+        if (rank == 0) *outLen = 0;
         const unsigned long long tag = static_cast<unsigned long long>(r + 1) << 32;
-        for (uint32_t i = rank; i < n; i += size) {
-            if (s.color[i] != NO_COLOR) continue;
-            const unsigned long long key = tag | priority_hash(i);
+        for (uint32_t j = rank; j < len; j += size) {
+            const uint32_t i = in ? in[j] : j;
+            const unsigned long long key = tag | (s.prio ? s.prio[i] : priority_hash(i));
             const uint32_t bA = w.cbody[m[i].a], bB = w.cbody[m[i].b];
-            if (__ldcg(&w.bvel[bA].w) > 0.0f) atomicMax(s.bodyMax + bA, key);
-            if (__ldcg(&w.bvel[bB].w) > 0.0f) atomicMax(s.bodyMax + bB, key);
+            if (B.invMass(bA) > 0.0f) atomicMax(s.bodyMax + bA, key);
+            if (B.invMass(bB) > 0.0f) atomicMax(s.bodyMax + bB, key);
         }
         if (!sync()) return false;
-        uint32_t got = 0;
-        for (uint32_t i = rank; i < n; i += size) {
-            if (s.color[i] != NO_COLOR) continue;
-            const unsigned long long key = tag | priority_hash(i);
+        uint32_t top = 0;
+        for (uint32_t j = rank; j < len; j += size) {
+            const uint32_t i = in ? in[j] : j;
+            const unsigned long long key = tag | (s.prio ? s.prio[i] : priority_hash(i));
             const uint32_t bA = w.cbody[m[i].a], bB = w.cbody[m[i].b];
-            const bool okA = !(__ldcg(&w.bvel[bA].w) > 0.0f) || __ldcg(s.bodyMax + bA) == key;
-            const bool okB = !(__ldcg(&w.bvel[bB].w) > 0.0f) || __ldcg(s.bodyMax + bB) == key;
-            if (okA && okB) { s.color[i] = r; got++; }
+            const bool dA = B.invMass(bA) > 0.0f, dB = B.invMass(bB) > 0.0f;
+            if ((!dA || __ldcg(s.bodyMax + bA) == key) && (!dB || __ldcg(s.bodyMax + bB) == key)) {
+                const unsigned long long used = (dA ? __ldcg(s.bodyMask + bA) : 0ull) |
+                                                (dB ? __ldcg(s.bodyMask + bB) : 0ull);
+                const uint32_t c = used == ~0ull ? 64u + r : uint32_t(__ffsll(static_cast<long long>(~used)) - 1);
+                s.color[i] = c;
+                atomicAdd(s.colorCount + c, 1u);
+                top = max(top, c + 1);
+                if (c < 64) {
+                    if (dA) atomicOr(s.bodyMask + bA, 1ull << c);
+                    if (dB) atomicOr(s.bodyMask + bB, 1ull << c);
+                }
+            } else {
+                out[atomicAdd(outLen, 1u)] = i;
+            }
         }
-        for (int o = 16; o > 0; o >>= 1) got += __shfl_xor_sync(0xffffffffu, got, o);
-        if ((threadIdx.x & 31) == 0 && got) { atomicAdd(s.colorCount + r, got); atomicAdd(s.colorCount + MAX_COLORS, got); }
+        for (int o = 16; o > 0; o >>= 1) top = max(top, __shfl_xor_sync(0xffffffffu, top, o));
+        if ((threadIdx.x & 31) == 0 && top) atomicMax(nColors, top);
         if (!sync()) return false;
-        done = Sync::ld(s.colorCount + MAX_COLORS) >= n;
+        len = Sync::ld(outLen);
+        in = out;
     }
-    if (!done) { if (rank == 0) atomicOr(status, STATUS_COLOR_OVERFLOW); return false; }
+    if (len > 0) { if (rank == 0) atomicOr(status, STATUS_COLOR_OVERFLOW); return false; }
+    const uint32_t ncol = Sync::ld(nColors);
     if (rank == 0) {
         uint32_t run = 0;
-        for (uint32_t c = 0; c < rounds; c++) { s.colorStart[c] = run; run += s.colorCount[c]; s.colorCount[c] = 0; }
-        s.colorStart[rounds] = run;
-        atomicMax(outColors, rounds);
+        for (uint32_t c = 0; c < ncol; c++) { s.colorStart[c] = run; run += s.colorCount[c]; s.colorCount[c] = 0; }
+        s.colorStart[ncol] = run;
+        atomicMax(outColors, ncol);
     }
     if (!sync()) return false;
     for (uint32_t i = rank; i < n; i += size) {
@@ -297,31 +369,34 @@ __device__ bool color_and_solve(const DeviceWorld& w, Manifold* __restrict__ m, 
     for (uint32_t c = rank; c < n; c += size) {
         const uint32_t mi = __ldcg(s.order + c);
         Constraint k;
-        prep_constraint(w, m[mi], mi, k);
+        prep_constraint(w, B, m[mi], mi, k);
         s.cons[c] = k;
     }
     if (!sync()) return false;
-    for (uint32_t col = 0; col < rounds; col++) {
+    for (uint32_t col = 0; col < ncol; col++) {
         const uint32_t end = Sync::ld(s.colorStart + col + 1);
-        for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) warm_constraint(w, s.cons[c]);
+        for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) warm_constraint(B, s.cons[c]);
         if (!sync()) return false;
     }
     for (uint32_t it = 0; it < velIters; it++) {
-        for (uint32_t col = 0; col < rounds; col++) {
+        for (uint32_t col = 0; col < ncol; col++) {
             const uint32_t end = Sync::ld(s.colorStart + col + 1);
             for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) {
                 Constraint k = s.cons[c];
-                velocity_constraint(w, k);
+                velocity_constraint(B, k);
                 float4* imp = reinterpret_cast<float4*>(&s.cons[c].jn0);
                 *imp = make_float4(k.jn0, k.jt0, k.jn1, k.jt1);
             }
+            // The next pass's constraint: from the next colour, or colour 0 of the next iteration.
+            prefetch_colour<Sync>(s, col + 1 < ncol ? col + 1 : 0, ncol, rank);
             if (!sync()) return false;
         }
     }
     for (uint32_t it = 0; it < posIters; it++) {
-        for (uint32_t col = 0; col < rounds; col++) {
+        for (uint32_t col = 0; col < ncol; col++) {
             const uint32_t end = Sync::ld(s.colorStart + col + 1);
-            for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) position_constraint(w, s.cons[c]);
+            for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) position_constraint(B, s.cons[c]);
+            prefetch_colour<Sync>(s, col + 1 < ncol ? col + 1 : 0, ncol, rank);
             if (!sync()) return false;
         }
     }
@@ -341,12 +416,14 @@ k_color_solve_cluster(DeviceWorld w, Manifold* m, const uint32_t* nM, SolveScrat
 __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* nM, SolveScratch s, uint32_t velIters,
                                    uint32_t posIters, uint32_t* bar, StepCounters* counters);
 
-// Batched worlds: one CTA per world (taken from a work counter in 'worldOrder' order, largest worlds first), the
-// colour counters in shared memory and __syncthreads between colours.
-constexpr uint32_t SOLVE_WORLD_THREADS = 256;
-__global__ void __launch_bounds__(SOLVE_WORLD_THREADS)
-k_color_solve_worlds(DeviceWorld w, Manifold* m, const uint32_t* segStart, const uint32_t* worldOrder,
-                     uint32_t worlds, SolveScratch s, uint32_t velIters, uint32_t posIters, uint32_t* nextWorld,
-                     StepCounters* counters);
+// Batched worlds: teams of consecutive worlds (team k owns worlds [teamWorld[k], teamWorld[k + 1])), each coloured
+// and solved by one CTA with __syncthreads between colours. Teams are taken from the work counter *nextTeam (zeroed
+// before the launch) in 'teamOrder' order, largest first. Colouring priorities are world-local manifold indices, so
+// the colours of a world do not depend on its team.
+constexpr uint32_t SOLVE_TEAM_THREADS = 256;
+__global__ void __launch_bounds__(SOLVE_TEAM_THREADS)
+k_color_solve_teams(DeviceWorld w, Manifold* m, const uint32_t* manSeg, const uint32_t* teamWorld,
+                    const uint32_t* teamOrder, uint32_t teams, uint32_t bodyCap, SolveScratch s, uint32_t velIters,
+                    uint32_t posIters, uint32_t* nextTeam, StepCounters* counters);
 
 }  // namespace ag2d

@@ -160,7 +160,6 @@ struct DeviceInfo {
     int sms = 0;
     int coopSolveBlocks = 0;   // co-resident CTAs of the grid solver
     int solveCluster = 0;      // CTAs per cluster of the cluster solver (16 when the device allows it)
-    int worldSolveBlocks = 0;  // co-resident CTAs of the per-world solver
 };
 
 // One world's state in the upload format (host arrays), and the warm-start manifolds.
@@ -196,6 +195,9 @@ struct PackedArrays {
     }
 };
 
+// Largest body range a solver team stages in shared memory (32 bytes per body).
+constexpr uint32_t MAX_TEAM_BODY_CAP = 4096;
+
 // Manifold count above which the solver runs on the whole grid instead of one cluster.
 constexpr uint32_t GRID_SOLVE_THRESHOLD = 600000;
 
@@ -214,8 +216,8 @@ static DeviceInfo probe_device(int device)
     int perSm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color_solve_grid, 256, 0));
     dev.coopSolveBlocks = std::max(1, perSm) * dev.sms;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color_solve_worlds, SOLVE_WORLD_THREADS, 0));
-    dev.worldSolveBlocks = std::max(1, perSm) * dev.sms;
+    CK(cudaFuncSetAttribute(k_color_solve_teams, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            int(MAX_TEAM_BODY_CAP * 2 * sizeof(float4))));
     // Largest cluster (16 non-portable, else 8, 4, 2) that can be resident.
     dev.solveCluster = 1;
     if (cudaFuncSetAttribute(k_color_solve_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
@@ -295,15 +297,22 @@ struct ag2d_world {
     DBuf<unsigned long long> hashKeys;
     DBuf<uint32_t> hashVals;
     // Colouring and solver.
-    DBuf<uint32_t> color, colorCount, colorStart, order, bar;
-    DBuf<unsigned long long> bodyMax;
+    DBuf<uint32_t> color, colorCount, colorStart, order, bar, prio, listA, listB;
+    DBuf<unsigned long long> bodyMax, bodyMask;
     DBuf<Constraint> cons;
     // Islands.
     DBuf<uint32_t> ufParent, ufFlag, wakeIsland;
     // World partition of a batch (nWorlds == 1: a single world, none of these is used).
     uint32_t nWorlds = 1;
+    uint32_t teamColliders = 2048;         // solver team size: consecutive worlds packed up to this many colliders
+    uint32_t teamBodyCap = 2048;           // bodies of a team staged in shared memory (larger teams use global)
+    uint32_t nTeams = 0;
+    uint32_t teamBlocks = 1;               // co-resident CTAs of the team solver at this shared-memory size
+    uint32_t queryThreads = 128;           // block sizes of the pair query and the narrow phase (tunable)
+    uint32_t narrowThreads = 256;
     std::vector<uint32_t> hBodyStart, hColStart;     // [nWorlds + 1]
-    DBuf<uint32_t> bodyWorld, colWorld, worldBodyStart, worldColStart, worldOrder, manSeg, nextWorld, worldDirty;
+    DBuf<uint32_t> bodyWorld, colWorld, worldBodyStart, worldColStart, manSeg, nextWorld, worldDirty;
+    DBuf<uint32_t> teamWorld, teamOrder;     // solver teams: first world of each team [nTeams + 1]; largest first
     DBuf<uint8_t> dynSimd, dynColSimd;               // SIMD-path flag of each work-list entry
     // Shape table sizes of the last upload.
     uint32_t nCircles = 0, nBoxes = 0, nPolygons = 0, nPolyVerts = 0, nMaterialRows = 0;
@@ -367,6 +376,37 @@ struct ag2d_world {
         return w;
     }
 
+    // Solver teams: consecutive worlds packed while the team stays within 'colliders' colliders (a larger world is
+    // a team of its own), scheduled largest first.
+    void setTeams(uint32_t colliders)
+    {
+        teamColliders = colliders;
+        teamBodyCap = std::min<uint32_t>(MAX_TEAM_BODY_CAP, colliders);
+        int perSm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color_solve_teams, SOLVE_TEAM_THREADS,
+                                                         teamBodyCap * 2 * sizeof(float4)));
+        teamBlocks = uint32_t(std::max(1, perSm) * dev.sms);
+        std::vector<uint32_t> start{0};
+        uint32_t acc = 0;
+        for (uint32_t k = 0; k < nWorlds; k++) {
+            const uint32_t c = hColStart[k + 1] - hColStart[k];
+            if (acc > 0 && acc + c > colliders) {
+                start.push_back(k);
+                acc = 0;
+            }
+            acc += c;
+        }
+        start.push_back(nWorlds);
+        nTeams = uint32_t(start.size() - 1);
+        std::vector<uint32_t> ord(nTeams);
+        for (uint32_t t = 0; t < nTeams; t++) ord[t] = t;
+        auto size = [&](uint32_t t) { return hColStart[start[t + 1]] - hColStart[start[t]]; };
+        std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return size(a) > size(b); });
+        teamWorld.upload(start.data(), start.size(), stream);
+        teamOrder.upload(ord.data(), ord.size(), stream);
+        CK(cudaStreamSynchronize(stream));
+    }
+
     // Installs the world partition of a batch: world k owns bodies [bodyStart[k], bodyStart[k + 1]) and colliders
     // [colStart[k], colStart[k + 1]). Called after the arrays are uploaded.
     void setPartition(const std::vector<uint32_t>& bodyStart, const std::vector<uint32_t>& colStart)
@@ -375,23 +415,18 @@ struct ag2d_world {
         nWorlds = uint32_t(bodyStart.size() - 1);
         hBodyStart = bodyStart;
         hColStart = colStart;
-        std::vector<uint32_t> bw(nBodies), cw(nColliders), order(nWorlds);
+        std::vector<uint32_t> bw(nBodies), cw(nColliders);
         for (uint32_t k = 0; k < nWorlds; k++) {
             for (uint32_t i = bodyStart[k]; i < bodyStart[k + 1]; i++) bw[i] = k;
             for (uint32_t i = colStart[k]; i < colStart[k + 1]; i++) cw[i] = k;
-            order[k] = k;
         }
-        // Largest worlds first: the per-world solver takes worlds in this order, which balances its CTAs.
-        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-            return colStart[a + 1] - colStart[a] > colStart[b + 1] - colStart[b];
-        });
         bodyWorld.upload(bw.data(), bw.size(), s);
         colWorld.upload(cw.data(), cw.size(), s);
         worldBodyStart.upload(bodyStart.data(), bodyStart.size(), s);
         worldColStart.upload(colStart.data(), colStart.size(), s);
-        worldOrder.upload(order.data(), order.size(), s);
         manSeg.reserve(nWorlds + 1);
         nextWorld.reserve(1);
+        setTeams(teamColliders);
         worldDirty.reserve(nWorlds);
         CK(cudaMemsetAsync(worldDirty.p, 0, sizeof(uint32_t) * nWorlds, s));
         dynSimd.reserve(std::max(nBodies, nColliders));
@@ -417,7 +452,7 @@ struct ag2d_world {
     uint32_t gridFor(uint64_t n, uint32_t threads = 256) const
     {
         const uint64_t want = (n + threads - 1) / threads;
-        const uint64_t cap = uint64_t(std::max(dev.sms, 1)) * 8;
+        const uint64_t cap = uint64_t(std::max(dev.sms, 1)) * std::max<uint32_t>(1, 2048 / threads);   // one full SM each
         return uint32_t(std::max<uint64_t>(1, std::min(want, cap)));
     }
 
@@ -446,7 +481,7 @@ struct ag2d_world {
         nManifolds.reserve(1);
         nPrev.reserve(1);
         listCounts.reserve(3);
-        colorCount.reserve(MAX_COLORS + 1);
+        colorCount.reserve(COLOR_SLOTS);
         colorStart.reserve(MAX_COLORS + 1);
         CK(cudaMemsetAsync(nPrev.p, 0, sizeof(uint32_t), stream));
         CK(cudaMemsetAsync(nManifolds.p, 0, sizeof(uint32_t), stream));
@@ -474,6 +509,9 @@ struct ag2d_world {
         grow_keep(prevManifolds, manifoldCap);
         color.reserve(manifoldCap);
         order.reserve(manifoldCap);
+        prio.reserve(manifoldCap);
+        listA.reserve(manifoldCap);
+        listB.reserve(manifoldCap);
         cons.reserve(manifoldCap);
         hashCap = 16;
         while (hashCap < 2 * manifoldCap) hashCap <<= 1;
@@ -570,6 +608,7 @@ struct ag2d_world {
         nPolyVerts = uint32_t(pv.size()); nMaterialRows = uint32_t(mats.size());
         qCounts.reserve(nColliders); qOffsets.reserve(nColliders);
         bodyMax.reserve(nBodies);
+        bodyMask.reserve(nBodies);
         ufParent.reserve(nBodies); ufFlag.reserve(nBodies); wakeIsland.reserve(nBodies);
         const uint32_t cap = std::max<uint32_t>(4 * nColliders, 4096);
         reserveCapacities(std::max(pairCap, cap), std::max(manifoldCap, cap));
@@ -806,11 +845,11 @@ struct ag2d_world {
         }
         pbegin(4);
         launches += 2 + scanLaunches(nDynCol) + 1;
-        k_query_count<<<gridFor(nDynCol, 128), 128, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qCounts.p,
+        k_query_count<<<gridFor(nDynCol, queryThreads), queryThreads, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qCounts.p,
                                                             &dCounters.p->status);
         CK(cudaGetLastError());
         scanner.run(qCounts.p, qOffsets.p, nDynCol, total, s);
-        k_query_write<<<gridFor(nDynCol, 128), 128, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qOffsets.p,
+        k_query_write<<<gridFor(nDynCol, queryThreads), queryThreads, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qOffsets.p,
                                                             pairs.p, pairCap, &dCounters.p->status);
         CK(cudaGetLastError());
         pend(4);
@@ -821,8 +860,9 @@ struct ag2d_world {
         const cudaStream_t s = stream;
         const uint32_t* nPairs = &dCounters.p->pairs;
         const uint32_t g = gridFor(pairCap);
+        const uint32_t gn = gridFor(pairCap, narrowThreads);
         pbegin(5);
-        k_narrow<<<g, 256, 0, s>>>(view(), pairs.p, nPairs, pairCap, slots.p, hit.p);
+        k_narrow<<<gn, narrowThreads, 0, s>>>(view(), pairs.p, nPairs, pairCap, slots.p, hit.p);
         CK(cudaGetLastError());
         pend(5);
         pbegin(6);
@@ -862,11 +902,13 @@ struct ag2d_world {
     {
         const cudaStream_t s = stream;
         CK(cudaMemsetAsync(bodyMax.p, 0, sizeof(unsigned long long) * std::max<uint32_t>(nBodies, 1), s));
+        CK(cudaMemsetAsync(bodyMask.p, 0, sizeof(unsigned long long) * std::max<uint32_t>(nBodies, 1), s));
         CK(cudaMemsetAsync(bar.p, 0, 2 * sizeof(uint32_t), s));
         DeviceWorld w = view();
         Manifold* mm = manifolds.p;
         const uint32_t* nm = nManifolds.p;
-        SolveScratch scratch{color.p, order.p, bodyMax.p, colorCount.p, colorStart.p, cons.p};
+        SolveScratch scratch{color.p, order.p, bodyMax.p, bodyMask.p, colorCount.p, colorStart.p, cons.p, nullptr,
+                             listA.p, listB.p};
         uint32_t vi = settings.velocity_iterations, pi = settings.position_iterations;
         StepCounters* ctr = dCounters.p;
         pbegin(10);
@@ -875,9 +917,10 @@ struct ag2d_world {
             CK(cudaMemsetAsync(nextWorld.p, 0, sizeof(uint32_t), s));
             k_manifold_segments<<<gridFor(manifoldCap), 256, 0, s>>>(mm, nm, cbody.p, bodyWorld.p, nWorlds,
                                                                       manSeg.p);
-            const uint32_t grid = std::min<uint32_t>(nWorlds, uint32_t(dev.worldSolveBlocks));
-            k_color_solve_worlds<<<grid, SOLVE_WORLD_THREADS, 0, s>>>(w, mm, manSeg.p, worldOrder.p, nWorlds, scratch,
-                                                                      vi, pi, nextWorld.p, ctr);
+            scratch.prio = prio.p;
+            const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(nTeams, teamBlocks));
+            k_color_solve_teams<<<grid, SOLVE_TEAM_THREADS, teamBodyCap * 2 * sizeof(float4), s>>>(
+                w, mm, manSeg.p, teamWorld.p, teamOrder.p, nTeams, teamBodyCap, scratch, vi, pi, nextWorld.p, ctr);
             CK(cudaGetLastError());
             launches++;
         } else if (lastManifolds <= GRID_SOLVE_THRESHOLD && dev.solveCluster > 1) {
@@ -941,6 +984,53 @@ struct ag2d_world {
             n = nb;
         }
         return k;
+    }
+
+    // Device milliseconds per step of one timed phase over 'steps' real steps.
+    double timePhase(int phase, uint32_t steps)
+    {
+        phaseMs[phase] = 0.0;
+        phaseCalls[phase] = 0;
+        for (uint32_t i = 0; i < steps; i++) stepOnce();
+        return phaseCalls[phase] ? phaseMs[phase] / double(phaseCalls[phase]) : 0.0;
+    }
+
+    // Launch-shape autotuner: times real steps under each candidate and keeps the fastest, one setting at a time
+    // (solver team size for batches, then the pair-query and narrow-phase block sizes). The results of a step do not
+    // depend on these settings, so tuning on the live world only advances it: one step, then per candidate one
+    // settling step and stepsPer timed steps.
+    void autotune(uint32_t stepsPer, ag2d_tuning& out)
+    {
+        const bool wasProfiling = profiling;
+        profiling = true;
+        stepOnce();   // first step: uploads, list build, buffer growth
+        auto pick = [&](int phase, const std::vector<uint32_t>& cands, auto apply) {
+            double best = 1e300;
+            uint32_t arg = cands.front();
+            for (uint32_t c : cands) {
+                apply(c);
+                stepOnce();
+                const double ms = timePhase(phase, stepsPer);
+                if (ms < best) { best = ms; arg = c; }
+            }
+            apply(arg);
+            return std::make_pair(arg, best);
+        };
+        out.team_colliders = 0;
+        out.solve_ms = 0.0f;
+        if (nWorlds > 1) {
+            const auto r = pick(10, {512, 1024, 2048, 4096}, [&](uint32_t t) { setTeams(t); });
+            out.team_colliders = r.first;
+            out.solve_ms = float(r.second);
+        }
+        const auto q = pick(4, {64, 128, 256}, [&](uint32_t t) { queryThreads = t; });
+        out.query_threads = q.first;
+        out.query_ms = float(q.second);
+        const auto nr = pick(5, {128, 256, 512}, [&](uint32_t t) { narrowThreads = t; });
+        out.narrow_threads = nr.first;
+        out.narrow_ms = float(nr.second);
+        profiling = wasProfiling;
+        for (int p = 0; p < NPHASE; p++) { phaseMs[p] = 0.0; phaseCalls[p] = 0; evPending[p] = false; }
     }
 
     // One fixed step (Simulation::physicsStep order, Simulation.cpp:255-351).
@@ -1264,6 +1354,19 @@ int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out)
         out->regrows = world->regrows;
         out->host_ms = world->hostMs;
         out->sync_ms = world->syncMs;
+    });
+}
+
+int32_t ag2d_world_autotune(ag2d_world* world, int32_t steps_per_candidate, ag2d_tuning* out)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        if (steps_per_candidate < 1) throw ApiError(AG2D_ERR_INVALID_ARG, "steps_per_candidate must be >= 1");
+        CK(cudaSetDevice(world->settings.device));
+        world->ensureUploaded();
+        ag2d_tuning t{};
+        world->autotune(uint32_t(steps_per_candidate), t);
+        if (out) *out = t;
     });
 }
 

@@ -197,7 +197,8 @@ k_color_solve_cluster(DeviceWorld w, Manifold* m, const uint32_t* nM, SolveScrat
     const cg::cluster_group cluster = cg::this_cluster();
     const uint32_t rank = cluster.block_rank() * blockDim.x + threadIdx.x;
     const uint32_t size = cluster.num_blocks() * blockDim.x;
-    color_and_solve(w, m, *nM, s, velIters, posIters, rank, size, ClusterSync{}, &counters->colors,
+    color_and_solve(w, GlobalBodies{w.bvel, w.bpos}, m, *nM, s, velIters, posIters, rank, size, ClusterSync{},
+                    &counters->colors,
                     &counters->status);
 }
 
@@ -207,33 +208,62 @@ __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* n
 {
     const uint32_t rank = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t size = gridDim.x * blockDim.x;
-    color_and_solve(w, m, *nM, s, velIters, posIters, rank, size, GridSync{bar, &counters->status},
+    color_and_solve(w, GlobalBodies{w.bvel, w.bpos}, m, *nM, s, velIters, posIters, rank, size,
+                    GridSync{bar, &counters->status},
                     &counters->colors, &counters->status);
 }
 
-// Batched worlds: each CTA takes the next world from the work counter and colours + solves that world's manifold
-// segment alone. Segment-relative manifold indices give every world the colouring and solving order it has when
-// stepped on its own, so a world's result does not depend on the batch it is in.
-__global__ void __launch_bounds__(SOLVE_WORLD_THREADS)
-k_color_solve_worlds(DeviceWorld w, Manifold* m, const uint32_t* __restrict__ segStart,
-                     const uint32_t* __restrict__ worldOrder, uint32_t worlds, SolveScratch s, uint32_t velIters,
-                     uint32_t posIters, uint32_t* nextWorld, StepCounters* counters)
+// Batched worlds: each CTA takes the next team of consecutive worlds, whose manifolds are one contiguous range of
+// the world-grouped list, and colours + solves that range as one problem (the worlds share no body, so their
+// colour classes simply merge). Priorities are world-local indices: every world gets the colouring, hence the
+// solving order, it has when stepped on its own, whichever team it is in. A team whose bodies fit the dynamic
+// shared memory (bodyCap bodies) solves on a shared-memory copy of their velocities and poses.
+__global__ void __launch_bounds__(SOLVE_TEAM_THREADS)
+k_color_solve_teams(DeviceWorld w, Manifold* m, const uint32_t* __restrict__ manSeg,
+                    const uint32_t* __restrict__ teamWorld, const uint32_t* __restrict__ teamOrder, uint32_t teams,
+                    uint32_t bodyCap, SolveScratch s, uint32_t velIters, uint32_t posIters, uint32_t* nextTeam,
+                    StepCounters* counters)
 {
-    __shared__ uint32_t colorCount[MAX_COLORS + 1];
+    extern __shared__ float4 bodyCache[];   // [bodyCap] velocities, then [bodyCap] poses
+    __shared__ uint32_t colorCount[COLOR_SLOTS];
     __shared__ uint32_t colorStart[MAX_COLORS + 1];
     __shared__ uint32_t item;
+    uint32_t* prio = const_cast<uint32_t*>(s.prio);
     while (true) {
-        if (threadIdx.x == 0) item = atomicAdd(nextWorld, 1u);
+        if (threadIdx.x == 0) item = atomicAdd(nextTeam, 1u);
         __syncthreads();
         const uint32_t k = item;
         __syncthreads();
-        if (k >= worlds) return;
-        const uint32_t wd = worldOrder ? worldOrder[k] : k;
-        const uint32_t lo = segStart[wd], hi = segStart[wd + 1];
+        if (k >= teams) return;
+        const uint32_t t = teamOrder[k];
+        const uint32_t w0 = teamWorld[t], w1 = teamWorld[t + 1];
+        const uint32_t lo = manSeg[w0], hi = manSeg[w1];
         if (hi <= lo) continue;
-        const SolveScratch ls{s.color + lo, s.order + lo, s.bodyMax, colorCount, colorStart, s.cons + lo};
-        color_and_solve(w, m + lo, hi - lo, ls, velIters, posIters, threadIdx.x, blockDim.x, BlockSync{},
-                        &counters->colors, &counters->status);
+        for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
+            prio[i] = priority_hash(i - manSeg[w.bodyWorld[w.cbody[m[i].a]]]);
+        const SolveScratch ls{s.color + lo, s.order + lo, s.bodyMax, s.bodyMask, colorCount, colorStart,
+                              s.cons + lo, prio + lo, s.listA + lo, s.listB + lo};
+        const uint32_t b0 = w.worldBodyStart[w0], nb = w.worldBodyStart[w1] - b0;
+        if (nb <= bodyCap) {
+            float4* vel = bodyCache;
+            float4* pos = bodyCache + bodyCap;
+            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+                vel[i] = w.bvel[b0 + i];
+                pos[i] = w.bpos[b0 + i];
+            }
+            __syncthreads();
+            color_and_solve(w, SharedBodies{vel, pos, b0}, m + lo, hi - lo, ls, velIters, posIters, threadIdx.x,
+                            blockDim.x, BlockSync{}, &counters->colors, &counters->status);
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+                w.bvel[b0 + i] = vel[i];
+                w.bpos[b0 + i] = pos[i];
+            }
+        } else {
+            __syncthreads();
+            color_and_solve(w, GlobalBodies{w.bvel, w.bpos}, m + lo, hi - lo, ls, velIters, posIters, threadIdx.x,
+                            blockDim.x, BlockSync{}, &counters->colors, &counters->status);
+        }
         __syncthreads();
     }
 }

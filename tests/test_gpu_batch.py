@@ -98,3 +98,17 @@ def test_batch_errors():
         batch.read(1, ag2d.BODY_COM_X)
     with pytest.raises(ag2d.Ag2dError):
         batch.read(0, ag2d.PAIRS)
+
+
+def test_autotune_does_not_change_results():
+    """The autotuner times real steps under different launch shapes; the world must come out as if stepped plainly."""
+    sc = _scene_list(seed=17)
+    tuned = ag2d.Batch([ag2d.World.from_scene(s) for s in sc])
+    plain = ag2d.Batch([ag2d.World.from_scene(s) for s in sc])
+    t = tuned.engine.autotune(1)
+    assert t["team_colliders"] in (512, 1024, 2048, 4096)
+    assert t["query_threads"] in (64, 128, 256) and t["narrow_threads"] in (128, 256, 512)
+    plain.step(1 + 10 * 2)
+    for k in range(len(sc)):
+        for f in BODY_FIELDS:
+            assert np.array_equal(_bits(tuned.read(k, f)), _bits(plain.read(k, f))), (k, f)
