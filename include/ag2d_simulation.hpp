@@ -1,0 +1,249 @@
+// C++ facade over the C ABI of libag2d.so with the names and call shapes of PS_AGONY2D's public API, so scene code
+// written against the reference's Simulation / ObjectAPI compiles against this library with a namespace change.
+//
+//   reference                                   here
+//   PS_AGONY2D::Simulation (Simulation.h:36)    ag2d::Simulation      update, createMaterial, objects,
+//                                                                     getBodyCollisionData, getSimulationSettings
+//   PS_AGONY2D::ObjectAPI (ObjectAPI.h:14)      ag2d::ObjectAPI       createCircle/Box/Polygon (+ H variants),
+//                                                                     getBodyIndex, getBodies
+//   SimulationSettings (Simulation.h:50-76)     ag2d::SimulationSettings
+//   FixedClock (SimulationImpl/FixedClock.h)    the same accumulator semantics inside Simulation::update
+//   Body/Circle/Box/PolygonCreateParams         same fields (SimulationImpl/ObjectCreateParams.h:14-95)
+//
+// Creation failures return std::nullopt like the reference (ObjectManager.cpp:92-97); device and capacity errors
+// throw std::runtime_error carrying ag2d_last_error_string(). Header-only; link with -lag2d.
+#pragma once
+
+#include "ag2d.h"
+
+#include <cmath>
+#include <cstdint>
+#include <memory>
+#include <optional>
+#include <span>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace ag2d {
+
+using Real = float;
+using ObjectDenseIndex = uint32_t;
+using MaterialIndex = uint32_t;
+
+struct Vec2 {
+    Real x = 0, y = 0;
+};
+
+// A body handle as the C ABI returns it (slot and generation packed in 64 bits).
+struct Handle {
+    uint64_t value = 0;
+};
+
+struct Material {
+    Real elasticity = 1;
+    Real staticFriction = 0;
+    Real dynamicFriction = 0;
+};
+
+struct BodyCreateParams {
+    Vec2 position{};
+    Vec2 velocity{};
+    Real rotation = 0;
+    Real angularVelocity = 0;
+    Real mass = 0;          // 0: a static body
+    Real inertia = 0;       // 0: from the shape (the only form the C ABI takes)
+    MaterialIndex materialIndex = 0;
+};
+struct CircleCreateParams {
+    BodyCreateParams base;
+    Real radius = 0;
+};
+struct BoxCreateParams {
+    BodyCreateParams base;
+    Vec2 size{};
+};
+struct PolygonCreateParams {
+    BodyCreateParams base;
+    std::span<Vec2> localVertices;
+};
+
+struct FixedClockSettings {
+    Real updateInterval = Real(1) / Real(300);
+    Real maxDeltaTimePerUpdateCall = Real(1) / Real(20);
+    Real timeScale = Real(1);
+};
+struct IntegratorSettings {
+    Vec2 gravity{0, Real(-9.81)};
+    Real angularVelocityDamping = 1;   // 1: off
+};
+struct SimulationSettings {
+    FixedClockSettings clockSettings;
+    uint32_t collisionVelocitySolvingIterations = 6;
+    uint32_t collisionPositionSolvingIterations = 3;
+    IntegratorSettings integratorSettings;
+    bool continuousCollisionEnabled = false;   // the reference defaults to true; this library has no CCD yet
+    Real sleepSpeedThreshold = Real(0.1);
+    Real sleepTimeThreshold = Real(0.5);
+    int device = 0;                            // CUDA device ordinal
+};
+
+// Host copy of the body arrays in dense order (the reference's BodySoAViewer fields used by scene code).
+struct BodyView {
+    std::vector<Real> comX, comY, rotation, velocityX, velocityY, angularVelocity;
+    uint32_t getCount() const { return uint32_t(comX.size()); }
+};
+
+namespace detail {
+inline void check(int32_t code)
+{
+    if (code != AG2D_OK) throw std::runtime_error(std::string("ag2d: ") + ag2d_last_error_string());
+}
+inline ag2d_body_desc desc(const BodyCreateParams& b)
+{
+    ag2d_body_desc d{};
+    d.x = b.position.x; d.y = b.position.y; d.rotation = b.rotation;
+    d.vx = b.velocity.x; d.vy = b.velocity.y; d.angular_velocity = b.angularVelocity;
+    d.mass = b.mass; d.material = b.materialIndex;
+    return d;
+}
+inline std::vector<float> read_floats(ag2d_world* w, int32_t field)
+{
+    uint64_t bytes = 0;
+    check(ag2d_world_read(w, field, nullptr, 0, &bytes));
+    std::vector<float> v(bytes / sizeof(float));
+    check(ag2d_world_read(w, field, v.data(), bytes, &bytes));
+    return v;
+}
+}  // namespace detail
+
+class ObjectAPI {
+public:
+    explicit ObjectAPI(ag2d_world* w) : world(w) {}
+    ObjectAPI(const ObjectAPI&) = delete;
+    ObjectAPI& operator=(const ObjectAPI&) = delete;
+
+    std::optional<ObjectDenseIndex> createCircle(const CircleCreateParams& p) { return index(createCircleH(p)); }
+    std::optional<ObjectDenseIndex> createBox(const BoxCreateParams& p) { return index(createBoxH(p)); }
+    std::optional<ObjectDenseIndex> createPolygon(const PolygonCreateParams& p) { return index(createPolygonH(p)); }
+
+    std::optional<Handle> createCircleH(const CircleCreateParams& p)
+    {
+        if (p.base.inertia != 0) return std::nullopt;
+        const ag2d_body_desc d = detail::desc(p.base);
+        uint64_t h = 0;
+        return created(ag2d_world_add_circle(world, &d, p.radius, &h), h);
+    }
+    std::optional<Handle> createBoxH(const BoxCreateParams& p)
+    {
+        if (p.base.inertia != 0) return std::nullopt;
+        const ag2d_body_desc d = detail::desc(p.base);
+        uint64_t h = 0;
+        return created(ag2d_world_add_box(world, &d, p.size.x, p.size.y, &h), h);
+    }
+    std::optional<Handle> createPolygonH(const PolygonCreateParams& p)
+    {
+        if (p.base.inertia != 0) return std::nullopt;
+        const ag2d_body_desc d = detail::desc(p.base);
+        std::vector<float> xy;
+        xy.reserve(p.localVertices.size() * 2);
+        for (const Vec2& v : p.localVertices) { xy.push_back(v.x); xy.push_back(v.y); }
+        uint64_t h = 0;
+        return created(ag2d_world_add_polygon(world, &d, xy.data(), uint32_t(p.localVertices.size()), &h), h);
+    }
+
+    // Dense index of a handle; UINT32_MAX when the handle is stale (ObjectAPI::getBodyIndex, ObjectAPI.h:53).
+    ObjectDenseIndex getBodyIndex(Handle h) const noexcept { return ag2d_world_body_index(world, h.value); }
+
+    BodyView getBodies() const
+    {
+        BodyView v;
+        v.comX = detail::read_floats(world, AG2D_BODY_COM_X);
+        v.comY = detail::read_floats(world, AG2D_BODY_COM_Y);
+        v.rotation = detail::read_floats(world, AG2D_BODY_ROTATION);
+        v.velocityX = detail::read_floats(world, AG2D_BODY_VEL_X);
+        v.velocityY = detail::read_floats(world, AG2D_BODY_VEL_Y);
+        v.angularVelocity = detail::read_floats(world, AG2D_BODY_ANGULAR_VELOCITY);
+        return v;
+    }
+
+private:
+    // Invalid shapes (the reference's nullopt cases) return nullopt; anything else is an error.
+    static std::optional<Handle> created(int32_t code, uint64_t h)
+    {
+        if (code == AG2D_ERR_INVALID_ARG || code == AG2D_ERR_UNSUPPORTED) return std::nullopt;
+        detail::check(code);
+        return Handle{h};
+    }
+    std::optional<ObjectDenseIndex> index(std::optional<Handle> h) const
+    {
+        if (!h) return std::nullopt;
+        return getBodyIndex(*h);
+    }
+    ag2d_world* world;
+};
+
+class Simulation {
+public:
+    explicit Simulation(const SimulationSettings& s = {}) : settings(s)
+    {
+        ag2d_world_settings w{};
+        w.dt = s.clockSettings.updateInterval * s.clockSettings.timeScale;
+        w.velocity_iterations = s.collisionVelocitySolvingIterations;
+        w.position_iterations = s.collisionPositionSolvingIterations;
+        w.gravity_x = s.integratorSettings.gravity.x;
+        w.gravity_y = s.integratorSettings.gravity.y;
+        w.angular_damping = s.integratorSettings.angularVelocityDamping;
+        w.sleep_speed = s.sleepSpeedThreshold;
+        w.sleep_time = s.sleepTimeThreshold;
+        w.ccd = s.continuousCollisionEnabled ? 1 : 0;
+        w.device = s.device;
+        detail::check(ag2d_world_create(&w, &world));
+        api = std::make_unique<ObjectAPI>(world);
+    }
+    ~Simulation() { ag2d_world_destroy(world); }
+    Simulation(const Simulation&) = delete;
+    Simulation& operator=(const Simulation&) = delete;
+
+    // Simulation::update (Simulation.cpp:32-74) with FixedClock::advance (FixedClock.h:35-63): the call's time,
+    // capped at maxDeltaTimePerUpdateCall, accumulates; every whole updateInterval in the accumulator is one step.
+    void update(Real deltaTime)
+    {
+        if (!(deltaTime > 0)) return;
+        accumulator += std::fmin(deltaTime, settings.clockSettings.maxDeltaTimePerUpdateCall);
+        const uint32_t steps = uint32_t(std::floor(accumulator / settings.clockSettings.updateInterval));
+        accumulator -= Real(steps) * settings.clockSettings.updateInterval;
+        if (steps) detail::check(ag2d_world_step(world, int32_t(steps)));
+    }
+
+    MaterialIndex createMaterial(const Material& m)
+    {
+        uint32_t idx = 0;
+        detail::check(ag2d_world_add_material(world, m.elasticity, m.staticFriction, m.dynamicFriction, &idx));
+        return idx;
+    }
+
+    ObjectAPI& objects() noexcept { return *api; }
+    const ObjectAPI& objects() const noexcept { return *api; }
+
+    // The manifolds of the last step (Simulation::getBodyCollisionData, Simulation.h:186), as host copies.
+    std::vector<ag2d_manifold> getBodyCollisionData() const
+    {
+        uint64_t bytes = 0;
+        detail::check(ag2d_world_read(world, AG2D_PREV_MANIFOLDS, nullptr, 0, &bytes));
+        std::vector<ag2d_manifold> m(bytes / sizeof(ag2d_manifold));
+        detail::check(ag2d_world_read(world, AG2D_PREV_MANIFOLDS, m.data(), bytes, &bytes));
+        return m;
+    }
+
+    const SimulationSettings& getSimulationSettings() const noexcept { return settings; }
+    ag2d_world* handle() noexcept { return world; }
+
+private:
+    SimulationSettings settings;
+    ag2d_world* world = nullptr;
+    std::unique_ptr<ObjectAPI> api;
+    Real accumulator = 0;
+};
+
+}  // namespace ag2d

@@ -11,6 +11,7 @@ for p in (ROOT, PKG, os.path.join(ROOT, "tests")):
         sys.path.insert(0, p)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+LIB_DIR = os.path.join(PKG, "ag2d")
 
 
 def pytest_configure(config):

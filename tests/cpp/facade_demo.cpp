@@ -1,0 +1,53 @@
+// Scene code in the reference's style (App/Scenes.cpp: create a material, a static ground box and a pile of
+// bodies through ObjectAPI, then Simulation::update) compiled against the C++ facade of libag2d.so.
+// Prints "no-device" and exits 0 when the machine has no CUDA device; otherwise steps the scene and prints
+// "ok <bodies> <manifolds> <mean y>".
+#include "ag2d_simulation.hpp"
+
+#include <cstdio>
+#include <cstring>
+
+int main()
+{
+    ag2d::SimulationSettings settings;
+    settings.clockSettings.updateInterval = 1.0f / 60.0f;
+    settings.collisionVelocitySolvingIterations = 8;
+    std::optional<ag2d::Simulation> sim;
+    try {
+        sim.emplace(settings);
+    } catch (const std::runtime_error& e) {
+        if (std::strstr(e.what(), "no CUDA device")) { std::printf("no-device\n"); return 0; }
+        std::printf("error %s\n", e.what());
+        return 1;
+    }
+    const ag2d::MaterialIndex mat = sim->createMaterial({0.0f, 0.4f, 0.4f});
+    ag2d::BoxCreateParams ground;
+    ground.base.position = {0.0f, -1.0f};
+    ground.base.materialIndex = mat;
+    ground.size = {40.0f, 2.0f};
+    if (!sim->objects().createBox(ground)) return 2;
+    ag2d::Vec2 tri[3] = {{-0.5f, -0.4f}, {0.5f, -0.4f}, {0.0f, 0.6f}};
+    int created = 1;
+    for (int i = 0; i < 60; i++) {
+        ag2d::BodyCreateParams b;
+        b.position = {-12.0f + float(i % 12) * 2.0f, 1.0f + float(i / 12) * 1.5f};
+        b.mass = 1.0f;
+        b.materialIndex = mat;
+        bool ok;
+        if (i % 3 == 0) ok = sim->objects().createCircle({b, 0.45f}).has_value();
+        else if (i % 3 == 1) ok = sim->objects().createBox({b, {0.8f, 0.8f}}).has_value();
+        else ok = sim->objects().createPolygon({b, std::span<ag2d::Vec2>(tri, 3)}).has_value();
+        created += ok ? 1 : 0;
+    }
+    ag2d::BoxCreateParams bad;
+    bad.base.mass = 1.0f;
+    bad.size = {-1.0f, 1.0f};
+    if (sim->objects().createBox(bad)) return 3;     // invalid shape: nullopt, as in the reference
+    for (int frame = 0; frame < 120; frame++) sim->update(1.0f / 60.0f);
+    const ag2d::BodyView bodies = sim->objects().getBodies();
+    double meanY = 0.0;
+    for (uint32_t i = 0; i < bodies.getCount(); i++) meanY += bodies.comY[i];
+    std::printf("ok %u %zu %.3f\n", bodies.getCount(), sim->getBodyCollisionData().size(),
+                meanY / double(bodies.getCount()));
+    return bodies.getCount() == uint32_t(created) ? 0 : 4;
+}
