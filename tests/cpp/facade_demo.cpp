@@ -1,9 +1,10 @@
 // Scene code in the reference's style (App/Scenes.cpp: create a material, a static ground box and a pile of
 // bodies through ObjectAPI, then Simulation::update) compiled against the C++ facade of libag2d.so.
 // Prints "no-device" and exits 0 when the machine has no CUDA device; otherwise steps the scene and prints
-// "ok <bodies> <manifolds> <mean y>".
+// "ok <bodies> <most manifolds in one step> <mean y>".
 #include "ag2d_simulation.hpp"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 
@@ -43,11 +44,14 @@ int main()
     bad.base.mass = 1.0f;
     bad.size = {-1.0f, 1.0f};
     if (sim->objects().createBox(bad)) return 3;     // invalid shape: nullopt, as in the reference
-    for (int frame = 0; frame < 120; frame++) sim->update(1.0f / 60.0f);
+    size_t maxManifolds = 0;   // the pile settles and falls asleep, so track the most contacts seen
+    for (int frame = 0; frame < 120; frame++) {
+        sim->update(1.0f / 60.0f);
+        maxManifolds = std::max(maxManifolds, sim->getBodyCollisionData().size());
+    }
     const ag2d::BodyView bodies = sim->objects().getBodies();
     double meanY = 0.0;
     for (uint32_t i = 0; i < bodies.getCount(); i++) meanY += bodies.comY[i];
-    std::printf("ok %u %zu %.3f\n", bodies.getCount(), sim->getBodyCollisionData().size(),
-                meanY / double(bodies.getCount()));
+    std::printf("ok %u %zu %.3f\n", bodies.getCount(), maxManifolds, meanY / double(bodies.getCount()));
     return bodies.getCount() == uint32_t(created) ? 0 : 4;
 }
