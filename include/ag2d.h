@@ -230,6 +230,40 @@ int32_t ag2d_batch_read(ag2d_batch* batch, uint32_t world, int32_t field, void* 
                         uint64_t* out_bytes);
 int32_t ag2d_batch_destroy(ag2d_batch* batch);
 
+/* ---- allocation-free solve: no counterpart in the reference (its solver allocates freely on the host) ----
+ * Colours and solves n_manifolds manifolds in place on caller-owned device arrays: body velocities and poses are
+ * updated and the manifolds' impulses written back, as AG2D_PHASE_SOLVE does for a world. The call makes no device
+ * allocation and no allocating library call. It is for callers that cannot allocate at this point: a host loop
+ * that has handed all free device memory to its own pool and runs inside that budget, or code that must not stall
+ * a busy device on the implicit synchronisation that cudaMalloc / cudaFree can bring. Its scratch is one fixed
+ * static device array of about 2.6 MiB per device, so:
+ *  - at most AG2D_SOLVE_NOALLOC_MAX_MANIFOLDS manifolds and AG2D_SOLVE_NOALLOC_MAX_BODIES bodies per call; larger
+ *    sizes return AG2D_ERR_CAPACITY with the limit in the error string, before any launch;
+ *  - the first call with a device current looks the array's address up (cudaGetSymbolAddress) and so performs
+ *    set-up; make it before any stream capture on that device;
+ *  - the kernel clears what it needs at the start of every call: nothing has to start at zero;
+ *  - calls that overlap on one device share the array and race: serialise them (one stream, or events).
+ * The call is asynchronous on 'stream' (a cudaStream_t, NULL for the default stream) on the current device.
+ * Layout: body_velocity [n_bodies][4] = vx, vy, angular velocity, inverse mass; body_pose [n_bodies][4] =
+ * x, y, rotation, inverse inertia; materials [n_materials][4] = elasticity, static friction, dynamic friction,
+ * unused; collider_body / collider_material index those arrays and must be in range. Float4 arrays and the
+ * manifolds must be 16-byte aligned. device_status (device memory, may be NULL) receives {status bits, colours}. */
+#define AG2D_SOLVE_NOALLOC_MAX_MANIFOLDS 16384u
+#define AG2D_SOLVE_NOALLOC_MAX_BODIES 16384u
+typedef struct ag2d_solve_view {
+    uint32_t n_bodies;
+    float* body_velocity;
+    float* body_pose;
+    uint32_t n_colliders;
+    const uint32_t* collider_body;
+    const uint32_t* collider_material;
+    uint32_t n_materials;
+    const float* materials;
+} ag2d_solve_view;
+int32_t ag2d_solve_noalloc(const ag2d_solve_view* view, ag2d_manifold* manifolds, uint32_t n_manifolds,
+                           uint32_t velocity_iterations, uint32_t position_iterations, void* stream,
+                           uint32_t* device_status);
+
 #ifdef __cplusplus
 }
 #endif

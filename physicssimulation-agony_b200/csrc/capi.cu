@@ -36,6 +36,15 @@ struct ApiError : std::runtime_error {
                            std::string(#expr) + ": " + cudaGetErrorString(e_));                               \
     } while (0)
 
+}  // namespace
+
+namespace ag2d {
+// Sets the calling thread's ag2d_last_error_string (for entry points defined in other translation units).
+void set_last_error(const std::string& message) { g_error = message; }
+}  // namespace ag2d
+
+namespace {
+
 template <class F>
 int32_t guarded(F&& f)
 {
