@@ -456,7 +456,7 @@ def run_c4(args, torch, dist, rank, world_size, local, dev):
     msb = mean_shape_bytes(scene_list)
     bytes_by_phase = step_bytes(msb, sums["pairs"], sums["manifolds"], n_bodies - len(scene_list), K)
     kernel_of = {"solve": "k_color_solve_teams", "narrow": "k_narrow", "integrate": "k_integrate",
-                 "pose": "k_collider_pose", "sort": "k_sort_pass", "query": "k_query_count + k_query_write"}
+                 "pose": "k_collider_pose", "sort": "k_sort_pass", "query": "k_query_stash + k_query_emit"}
     roof = roofline_line(phases, bytes_by_phase, kernel_of, "c4")
     del batch, e
 
@@ -509,7 +509,7 @@ def run_c4(args, torch, dist, rank, world_size, local, dev):
         "dtype": "fp32", "data": "synthetic (seeded scene generator, ag2d.scenes.make_c4_worlds)",
         "config": {"workload": WORKLOADS["c4"], "worlds_per_gpu": len(scene_list), "bodies_per_gpu": n_bodies,
                    "parallelism": f"independent worlds x{world_size} GPUs (no step-path collective)",
-                   "autotuned": tuning, "steps_before_timing": f"{1 + 10 * 3} autotune steps + {args.warmup} warm-up",
+                   "autotuned": tuning, "steps_before_timing": f"{1 + 13 * 3} autotune steps + {args.warmup} warm-up",
                    "l2": "flushed between timed steps (256 MiB write outside the events)",
                    "mean_pairs_per_step": sums["pairs"] / K, "mean_manifolds_per_step": sums["manifolds"] / K},
         "per_world_launch": per_world_line,
@@ -554,7 +554,7 @@ def run_c2(args, torch, dist, rank, world_size, local, dev):
     nb, nc = w.counts()
     bytes_by_phase = step_bytes(msb, sums["pairs"], sums["manifolds"], nb - int((scene.mass == 0).sum()), K)
     kernel_of = {"solve": "k_color_solve_cluster", "narrow": "k_narrow", "integrate": "k_integrate",
-                 "pose": "k_collider_pose", "sort": "k_sort_pass", "query": "k_query_count + k_query_write"}
+                 "pose": "k_collider_pose", "sort": "k_sort_pass", "query": "k_query_stash + k_query_emit"}
     roof = roofline_line(phases, bytes_by_phase, kernel_of, "c2")
 
     e2e_steps = min(K, 300)

@@ -82,7 +82,8 @@ enum ag2d_timed_phase {
 
 /* Launch shapes chosen by ag2d_world_autotune. */
 typedef struct ag2d_tuning {
-    uint32_t team_colliders;   /* batched solver: consecutive worlds per CTA team (0 for a single world) */
+    uint32_t team_colliders;   /* batched solver: colliders per CTA team of consecutive worlds (0: single world) */
+    uint32_t team_threads;     /* batched solver: threads per team CTA (0: single world) */
     uint32_t query_threads;    /* pair-query block size */
     uint32_t narrow_threads;   /* narrow-phase block size */
     float solve_ms, query_ms, narrow_ms;   /* device time per step of each phase at the chosen setting */
@@ -193,7 +194,7 @@ int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out);
 /* Launch-shape autotuner (no reference counterpart: the reference runs on CPU threads). Times real steps under each
  * candidate solver team size (batches), pair-query and narrow-phase block size and keeps the fastest. A step's
  * results do not depend on these settings, so tuning only advances the world: by 1 + candidates x
- * (steps_per_candidate + 1) steps, with 10 candidates for a batch and 6 for a single world. Works on a batch
+ * (steps_per_candidate + 1) steps, with 13 candidates for a batch and 6 for a single world. Works on a batch
  * through ag2d_batch_engine. */
 int32_t ag2d_world_autotune(ag2d_world* world, int32_t steps_per_candidate, ag2d_tuning* out);
 /* Device timing of the step phases (the reference's Tracy zones, Profiling/TracyProfiler.h:66-72, become CUDA
@@ -236,7 +237,7 @@ int32_t ag2d_batch_destroy(ag2d_batch* batch);
  * allocation and no allocating library call. It is for callers that cannot allocate at this point: a host loop
  * that has handed all free device memory to its own pool and runs inside that budget, or code that must not stall
  * a busy device on the implicit synchronisation that cudaMalloc / cudaFree can bring. Its scratch is one fixed
- * static device array of about 2.6 MiB per device, so:
+ * static device array of about 3.1 MiB per device, so:
  *  - at most AG2D_SOLVE_NOALLOC_MAX_MANIFOLDS manifolds and AG2D_SOLVE_NOALLOC_MAX_BODIES bodies per call; larger
  *    sizes return AG2D_ERR_CAPACITY with the limit in the error string, before any launch;
  *  - the first call with a device current looks the array's address up (cudaGetSymbolAddress) and so performs

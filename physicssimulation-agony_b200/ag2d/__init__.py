@@ -75,7 +75,7 @@ class Counters(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("team_colliders", ctypes.c_uint32), ("query_threads", ctypes.c_uint32),
+    _fields_ = [("team_colliders", ctypes.c_uint32), ("team_threads", ctypes.c_uint32), ("query_threads", ctypes.c_uint32),
                 ("narrow_threads", ctypes.c_uint32), ("solve_ms", ctypes.c_float), ("query_ms", ctypes.c_float),
                 ("narrow_ms", ctypes.c_float)]
 

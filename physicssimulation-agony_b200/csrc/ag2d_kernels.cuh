@@ -13,6 +13,7 @@ constexpr uint32_t SCAN_THREADS = 256;
 constexpr uint32_t SCAN_ITEMS = 8;
 constexpr uint32_t SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
 constexpr int QUERY_STACK = 64;
+constexpr uint32_t QUERY_STASH = 8;   // pairs a query keeps from its counting traversal
 constexpr uint32_t MAX_COLORS = 256;
 constexpr uint32_t NO_COLOR = 0xFFFFFFFFu;
 
@@ -59,15 +60,17 @@ __global__ void k_lbvh_build(const uint32_t* keys, const uint32_t* sortedWorld, 
                              int2* child, int2* range, int* parent, int* leafParent, uint32_t* visit);
 __global__ void k_lbvh_refit(int n, const int2* child, const int* parent, const int* leafParent,
                              const float4* leafAabb, float4* nodeAabb, uint32_t* visit);
-__global__ void k_query_count(TreeView dyn, TreeView other, const uint32_t* cbody, uint32_t* counts,
+__global__ void k_query_stash(TreeView dyn, TreeView other, const uint32_t* cbody, uint32_t* counts, uint2* stash,
                               uint32_t* status);
-__global__ void k_query_write(TreeView dyn, TreeView other, const uint32_t* cbody, const uint32_t* offsets,
-                              uint2* pairs, uint32_t pairCap, uint32_t* status);
+__global__ void k_query_emit(TreeView dyn, TreeView other, const uint32_t* cbody, const uint32_t* counts,
+                             const uint32_t* offsets, const uint2* stash, uint2* pairs, uint32_t pairCap,
+                             uint32_t* status);
 __global__ void k_scan_blocks(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* blockSums);
 __global__ void k_scan_add(uint32_t* out, uint32_t n, const uint32_t* blockOffsets);
 __global__ void k_scan_total(const uint32_t* in, const uint32_t* out, uint32_t n, uint32_t* total);
 
 // Contact kernels (k_contact.cu).
+constexpr uint32_t NARROW_SMEM_PER_THREAD = 2 * MAX_POLYGON_VERTICES * sizeof(V2) / NARROW_GROUP;
 __global__ void k_narrow(DeviceWorld w, const uint2* pairs, const uint32_t* nPairs, uint32_t pairCap,
                          Manifold* slots, uint32_t* hit);
 __global__ void k_compact_manifolds(const Manifold* slots, const uint32_t* hit, const uint32_t* offsets,

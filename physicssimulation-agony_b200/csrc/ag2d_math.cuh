@@ -519,6 +519,130 @@ __device__ __forceinline__ bool collide_polygon_polygon(const ColliderView& A, c
     return true;
 }
 
+// collisionPolygonPolygon for one pair on a group of NARROW_GROUP lanes (lane = this lane's index in the group,
+// mask = the group's lanes in the warp). Lanes share the two polygons' vertices (A local, B in A's frame) through
+// the group's shared-memory tiles sA / sB, each lane projects its own axes, and group shuffles pick the separating
+// axis and the incident edge. The sequential choice keeps the axis with the smallest (overlap, facing), the first
+// one on ties (A's axes before B's), and the incident edge with the smallest dot, the first on ties: exactly the
+// lexicographic minima the reductions below take, so the result equals collide_polygon_polygon bit for bit. Every
+// lane returns the hit flag; the contact is valid on lane 0 of the group.
+constexpr uint32_t NARROW_GROUP = 8;
+
+__device__ __forceinline__ bool sat_better(float ov, float fac, uint32_t ord, float bov, float bfac, uint32_t bord)
+{
+    if (ov != bov) return ov < bov;
+    if (fac != bfac) return fac < bfac;
+    return ord < bord;
+}
+
+__device__ __forceinline__ bool collide_polygon_polygon_group(const ColliderView& A, const ColliderView& B,
+                                                              Contact& out, uint32_t lane, uint32_t mask,
+                                                              V2* sA, V2* sB)
+{
+    const float cA = A.c, sAn = A.s, cB = B.c, sBn = B.s;
+    const uint32_t nA = A.nv, nB = B.nv;
+    const V2 rightA = v2(cA, sAn), upA = v2(-sAn, cA);
+    const V2 cd = B.pos - A.pos;
+    const V2 bdl = v2(dot(cd, rightA), dot(cd, upA));
+    const float relCos = cA * cB + sAn * sBn;
+    const float relSin = cA * sBn - sAn * cB;
+    for (uint32_t k = lane; k < nB; k += NARROW_GROUP) {
+        const V2 v = ld2(B.verts, k);
+        sB[k] = v2(bdl.x + relCos * v.x - relSin * v.y, bdl.y + relSin * v.x + relCos * v.y);
+    }
+    for (uint32_t k = lane; k < nA; k += NARROW_GROUP) sA[k] = ld2(A.verts, k);
+    __syncwarp(mask);
+    bool separated = false;
+    float bov = FLT_MAX, bfac = FLT_MAX;
+    uint32_t bord = 0xFFFFFFFFu;
+    for (uint32_t i = lane; i < nA; i += NARROW_GROUP) {
+        const V2 ax = ld2(A.normals, i);
+        float minB = FLT_MAX;
+        for (uint32_t j = 0; j < nB; j++) minB = rfminf(minB, dot(sB[j], ax));
+        const float overlap = dot(sA[i], ax) - minB;
+        if (overlap < 0.0f) separated = true;
+        const float facing = -dot(ax, bdl);
+        if (sat_better(overlap, facing, i, bov, bfac, bord)) { bov = overlap; bfac = facing; bord = i; }
+    }
+    for (uint32_t i = lane; i < nB; i += NARROW_GROUP) {
+        const V2 nb = ld2(B.normals, i);
+        const V2 ax = v2(relCos * nb.x - relSin * nb.y, relSin * nb.x + relCos * nb.y);
+        float minA = FLT_MAX;
+        for (uint32_t j = 0; j < nA; j++) minA = rfminf(minA, dot(sA[j], ax));
+        const float overlap = dot(sB[i], ax) - minA;
+        if (overlap < 0.0f) separated = true;
+        const float facing = dot(ax, bdl);
+        const uint32_t ord = MAX_POLYGON_VERTICES + i;
+        if (sat_better(overlap, facing, ord, bov, bfac, bord)) { bov = overlap; bfac = facing; bord = ord; }
+    }
+    if (__any_sync(mask, separated)) return false;
+#pragma unroll
+    for (uint32_t o = NARROW_GROUP / 2; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(mask, bov, o), fac = __shfl_xor_sync(mask, bfac, o);
+        const uint32_t ord = __shfl_xor_sync(mask, bord, o);
+        if (sat_better(ov, fac, ord, bov, bfac, bord)) { bov = ov; bfac = fac; bord = ord; }
+    }
+    const bool refIsA = bord < MAX_POLYGON_VERTICES;
+    const uint32_t bestIndex = refIsA ? bord : bord - MAX_POLYGON_VERTICES;
+    V2 nl;
+    if (refIsA) {
+        nl = ld2(A.normals, bestIndex);
+    } else {
+        const V2 nb = ld2(B.normals, bestIndex);
+        nl = -v2(relCos * nb.x - relSin * nb.y, relSin * nb.x + relCos * nb.y);
+    }
+    const float depth = bov;
+    const uint32_t refCount = refIsA ? nA : nB, incCount = refIsA ? nB : nA;
+    const V2 rnl = refIsA ? nl : -nl;
+    float bd = FLT_MAX;
+    uint32_t bi = 0xFFFFFFFFu;
+    for (uint32_t i = lane; i < incCount; i += NARROW_GROUP) {
+        V2 n;
+        if (refIsA) { const V2 nb = ld2(B.normals, i); n = v2(relCos * nb.x - relSin * nb.y, relSin * nb.x + relCos * nb.y); }
+        else n = ld2(A.normals, i);
+        const float d = dot(rnl, n);
+        if (d < bd || (d == bd && i < bi && d < FLT_MAX)) { bd = d; bi = i; }
+    }
+#pragma unroll
+    for (uint32_t o = NARROW_GROUP / 2; o > 0; o >>= 1) {
+        const float d = __shfl_xor_sync(mask, bd, o);
+        const uint32_t i = __shfl_xor_sync(mask, bi, o);
+        if (d < bd || (d == bd && i < bi && d < FLT_MAX)) { bd = d; bi = i; }
+    }
+    // The sequential search starts at edge 0 with minDot = FLT_MAX and takes strictly smaller dots only, so with no
+    // dot below FLT_MAX it keeps edge 0.
+    const uint32_t ie = bi == 0xFFFFFFFFu ? 0u : bi;
+    bool hit = false;
+    if (lane == 0) {
+        const uint32_t i0 = bestIndex, i1 = next_index(i0, refCount);
+        const V2 rs = refIsA ? sA[i0] : sB[i0];
+        const V2 re = refIsA ? sA[i1] : sB[i1];
+        const V2 rfc = (rs + re) * 0.5f;
+        const V2 edge = re - rs;
+        const float len2 = dot(edge, edge);
+        const V2 sideDir = edge * (1.0f / sqrtf(len2));
+        const uint32_t ie2 = next_index(ie, incCount);
+        V2 c0 = refIsA ? sB[ie] : sA[ie];
+        V2 c1 = refIsA ? sB[ie2] : sA[ie2];
+        if (!clip_segment(c0, c1, rs, sideDir) && !clip_segment(c0, c1, re, -sideDir)) {
+            const float refPlaneDist = dot(rfc, rnl);
+            const uint32_t tag = refIsA ? REFERENCE_BODY_TAG : 0u;
+            uint32_t cnt = 0;
+            if (dot(c0, rnl) <= refPlaneDist + SAT_EPSILON) {
+                out.p[cnt] = (A.pos + rightA * c0.x) + upA * c0.y; out.id[cnt] = tag | ie; cnt++;
+            }
+            if (dot(c1, rnl) <= refPlaneDist + SAT_EPSILON) {
+                out.p[cnt] = (A.pos + rightA * c1.x) + upA * c1.y; out.id[cnt] = tag | ie2; cnt++;
+            }
+            if (cnt > 0) {
+                out.n = rightA * nl.x + upA * nl.y; out.depth = depth; out.count = cnt;
+                hit = true;
+            }
+        }
+    }
+    return __shfl_sync(mask, hit ? 1u : 0u, __ffs(mask) - 1) != 0;
+}
+
 // Dispatch on the (ordered) shape-type pair: typeA <= typeB.
 __device__ __forceinline__ bool collide(const ColliderView& A, const ColliderView& B, Contact& out)
 {

@@ -18,25 +18,40 @@ namespace cg = cooperative_groups;
 // fallback, iterative friction), solvePositionConstraints (:930-980), scatterImpulses (:392-414). A team runs every
 // pass colour by colour with its barrier between colours.
 // ---------------------------------------------------------------------------------------------------------------
-// Body state seen by the solver: global memory, or a team's contiguous body range staged in shared memory.
+// Body state seen by the solver, with the colouring words of each body (the round's highest priority and the mask of
+// colours taken around the body): global memory indexed by body, or a team's contiguous body range staged in shared
+// memory.
 struct GlobalBodies {
     float4* vel;
     float4* pos;
+    unsigned long long* maxW;    // [bodies], zeroed before the call
+    unsigned long long* maskW;   // [bodies], zeroed before the call
     __device__ __forceinline__ float4 v(uint32_t b) const { return vel[b]; }
     __device__ __forceinline__ float4 p(uint32_t b) const { return pos[b]; }
     __device__ __forceinline__ void setV(uint32_t b, const float4& x) const { vel[b] = x; }
     __device__ __forceinline__ void setP(uint32_t b, const float4& x) const { pos[b] = x; }
     __device__ __forceinline__ float invMass(uint32_t b) const { return __ldcg(&vel[b].w); }
+    __device__ __forceinline__ unsigned long long* maxWord(uint32_t b) const { return maxW + b; }
+    __device__ __forceinline__ unsigned long long* maskWord(uint32_t b) const { return maskW + b; }
+    static __device__ __forceinline__ unsigned long long ldWord(const unsigned long long* p) { return __ldcg(p); }
 };
 struct SharedBodies {
-    float4* vel;     // shared: bodies [base, base + count)
+    float4* vel;                 // shared: bodies [base, base + count)
     float4* pos;
+    unsigned long long* maxW;    // shared, zeroed by the team before colouring
+    unsigned long long* maskW;
     uint32_t base;
     __device__ __forceinline__ float4 v(uint32_t b) const { return vel[b - base]; }
     __device__ __forceinline__ float4 p(uint32_t b) const { return pos[b - base]; }
     __device__ __forceinline__ void setV(uint32_t b, const float4& x) const { vel[b - base] = x; }
     __device__ __forceinline__ void setP(uint32_t b, const float4& x) const { pos[b - base] = x; }
     __device__ __forceinline__ float invMass(uint32_t b) const { return vel[b - base].w; }
+    __device__ __forceinline__ unsigned long long* maxWord(uint32_t b) const { return maxW + (b - base); }
+    __device__ __forceinline__ unsigned long long* maskWord(uint32_t b) const { return maskW + (b - base); }
+    static __device__ __forceinline__ unsigned long long ldWord(const unsigned long long* p)
+    {
+        return *static_cast<const volatile unsigned long long*>(p);
+    }
 };
 
 template <class Bodies>
@@ -95,10 +110,9 @@ __device__ __forceinline__ void warm_constraint(const Bodies& B, const Constrain
     if (k.imB > 0.0f) B.setV(k.bodyB, vB);
 }
 
-template <class Bodies>
-__device__ __forceinline__ void velocity_constraint(const Bodies& B, Constraint& k)
+// One velocity iteration of one constraint on its two bodies' velocities held in registers.
+__device__ __forceinline__ void velocity_solve(Constraint& k, float4& vA, float4& vB)
 {
-    float4 vA = B.v(k.bodyA), vB = B.v(k.bodyB);
     const float imA = k.imA, imB = k.imB, iIA = k.iIA, iIB = k.iIB;
     const float nx = k.nx, ny = k.ny, tx = -ny, ty = nx;
     if (k.count == 1) {
@@ -216,8 +230,29 @@ __device__ __forceinline__ void velocity_constraint(const Bodies& B, Constraint&
             vB.z = vB.z + dj * rBt * iIB;
         }
     }
-    if (imA > 0.0f) B.setV(k.bodyA, vA);
-    if (imB > 0.0f) B.setV(k.bodyB, vB);
+}
+
+template <class Bodies>
+__device__ __forceinline__ void velocity_constraint(const Bodies& B, Constraint& k)
+{
+    float4 vA = B.v(k.bodyA), vB = B.v(k.bodyB);
+    velocity_solve(k, vA, vB);
+    if (k.imA > 0.0f) B.setV(k.bodyA, vA);
+    if (k.imB > 0.0f) B.setV(k.bodyB, vB);
+}
+
+// Two constraints of one colour (no shared dynamic body) at once: loads first, then both solves, then the stores,
+// so the two dependency chains overlap. Static bodies are never written, so a body the two share is only read.
+template <class Bodies>
+__device__ __forceinline__ void velocity_constraint2(const Bodies& B, Constraint& k0, Constraint& k1)
+{
+    float4 vA0 = B.v(k0.bodyA), vB0 = B.v(k0.bodyB), vA1 = B.v(k1.bodyA), vB1 = B.v(k1.bodyB);
+    velocity_solve(k0, vA0, vB0);
+    velocity_solve(k1, vA1, vB1);
+    if (k0.imA > 0.0f) B.setV(k0.bodyA, vA0);
+    if (k0.imB > 0.0f) B.setV(k0.bodyB, vB0);
+    if (k1.imA > 0.0f) B.setV(k1.bodyA, vA1);
+    if (k1.imB > 0.0f) B.setV(k1.bodyB, vB1);
 }
 
 template <class Bodies>
@@ -251,14 +286,15 @@ constexpr uint32_t MAX_ROUNDS = MAX_COLORS - 64;
 struct SolveScratch {
     uint32_t* color;                  // [manifolds]
     uint32_t* order;                  // [manifolds] colour-major solving order
-    unsigned long long* bodyMax;      // [bodies], zeroed before the call
+    unsigned long long* bodyMax;      // [bodies] global colouring words (GlobalBodies), zeroed before the call
     unsigned long long* bodyMask;     // [bodies] colours taken around each body, zeroed before the call
     uint32_t* colorCount;             // [COLOR_SLOTS], zeroed by the routine
     uint32_t* colorStart;             // [MAX_COLORS + 1]
     Constraint* cons;                 // [manifolds]
     const uint32_t* prio;             // [manifolds] colouring priorities, or null: priority_hash(index)
-    uint32_t* listA;                  // [manifolds] uncoloured manifolds, ping
-    uint32_t* listB;                  // [manifolds] uncoloured manifolds, pong
+    uint4* listA;                     // [manifolds] uncoloured manifold records, ping
+    uint4* listB;                     // [manifolds] uncoloured manifold records, pong
+    uint2* pairBodies;                // [manifolds] the two bodies, bit 31 set when the body is dynamic
 };
 
 // Team barriers. ld() reads a colour counter written by other team members before the last barrier: global memory
@@ -306,43 +342,68 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
                                 uint32_t size, Sync sync, uint32_t* __restrict__ outColors, uint32_t* __restrict__ status)
 {
     for (uint32_t c = rank; c < COLOR_SLOTS; c += size) s.colorCount[c] = 0;
+    // Each manifold's two bodies and whether they are dynamic, looked up once for all colouring rounds.
+    constexpr uint32_t DYN = 0x80000000u;
+    for (uint32_t i = rank; i < n; i += size) {
+        const uint32_t bA = w.cbody[m[i].a], bB = w.cbody[m[i].b];
+        s.pairBodies[i] = make_uint2(bA | (B.invMass(bA) > 0.0f ? DYN : 0u), bB | (B.invMass(bB) > 0.0f ? DYN : 0u));
+    }
     if (!sync()) return false;
     uint32_t* const nColors = s.colorCount + MAX_COLORS + 3;
     uint32_t len = n;
-    const uint32_t* in = nullptr;   // round 0 visits every manifold
+    const uint4* in = nullptr;   // round 0 visits every manifold; later rounds the uncoloured records
+    // Record j of this round: {manifold, priority, body A | dynamic bit, body B | dynamic bit}.
+    auto rec = [&](uint32_t j) -> uint4 {
+        if (in) return in[j];
+        const uint2 pb = s.pairBodies[j];
+        return make_uint4(j, s.prio ? s.prio[j] : priority_hash(j), pb.x, pb.y);
+    };
+    constexpr uint32_t BATCH = 4;   // records loaded together per thread (independent loads in flight)
     for (uint32_t r = 0; r < MAX_ROUNDS && len > 0; r++) {
-        uint32_t* out = (r & 1) ? s.listB : s.listA;
+        uint4* out = (r & 1) ? s.listB : s.listA;
         uint32_t* outLen = s.colorCount + MAX_COLORS + 1 + (r & 1);
         // This counter was last read before the barrier that ended the previous round.
         if (rank == 0) *outLen = 0;
         const unsigned long long tag = static_cast<unsigned long long>(r + 1) << 32;
-        for (uint32_t j = rank; j < len; j += size) {
-            const uint32_t i = in ? in[j] : j;
-            const unsigned long long key = tag | (s.prio ? s.prio[i] : priority_hash(i));
-            const uint32_t bA = w.cbody[m[i].a], bB = w.cbody[m[i].b];
-            if (B.invMass(bA) > 0.0f) atomicMax(s.bodyMax + bA, key);
-            if (B.invMass(bB) > 0.0f) atomicMax(s.bodyMax + bB, key);
+        for (uint32_t j0 = rank; j0 < len; j0 += BATCH * size) {
+            uint4 e[BATCH];
+#pragma unroll
+            for (uint32_t u = 0; u < BATCH; u++) e[u] = j0 + u * size < len ? rec(j0 + u * size) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+            for (uint32_t u = 0; u < BATCH; u++) {
+                if (j0 + u * size >= len) break;
+                const unsigned long long key = tag | e[u].y;
+                if (e[u].z & DYN) atomicMax(B.maxWord(e[u].z & ~DYN), key);
+                if (e[u].w & DYN) atomicMax(B.maxWord(e[u].w & ~DYN), key);
+            }
         }
         if (!sync()) return false;
         uint32_t top = 0;
-        for (uint32_t j = rank; j < len; j += size) {
-            const uint32_t i = in ? in[j] : j;
-            const unsigned long long key = tag | (s.prio ? s.prio[i] : priority_hash(i));
-            const uint32_t bA = w.cbody[m[i].a], bB = w.cbody[m[i].b];
-            const bool dA = B.invMass(bA) > 0.0f, dB = B.invMass(bB) > 0.0f;
-            if ((!dA || __ldcg(s.bodyMax + bA) == key) && (!dB || __ldcg(s.bodyMax + bB) == key)) {
-                const unsigned long long used = (dA ? __ldcg(s.bodyMask + bA) : 0ull) |
-                                                (dB ? __ldcg(s.bodyMask + bB) : 0ull);
-                const uint32_t c = used == ~0ull ? 64u + r : uint32_t(__ffsll(static_cast<long long>(~used)) - 1);
-                s.color[i] = c;
-                atomicAdd(s.colorCount + c, 1u);
-                top = max(top, c + 1);
-                if (c < 64) {
-                    if (dA) atomicOr(s.bodyMask + bA, 1ull << c);
-                    if (dB) atomicOr(s.bodyMask + bB, 1ull << c);
+        for (uint32_t j0 = rank; j0 < len; j0 += BATCH * size) {
+            uint4 e[BATCH];
+#pragma unroll
+            for (uint32_t u = 0; u < BATCH; u++) e[u] = j0 + u * size < len ? rec(j0 + u * size) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+            for (uint32_t u = 0; u < BATCH; u++) {
+                if (j0 + u * size >= len) break;
+                const uint32_t i = e[u].x;
+                const unsigned long long key = tag | e[u].y;
+                const uint32_t bA = e[u].z & ~DYN, bB = e[u].w & ~DYN;
+                const bool dA = (e[u].z & DYN) != 0, dB = (e[u].w & DYN) != 0;
+                if ((!dA || B.ldWord(B.maxWord(bA)) == key) && (!dB || B.ldWord(B.maxWord(bB)) == key)) {
+                    const unsigned long long used = (dA ? B.ldWord(B.maskWord(bA)) : 0ull) |
+                                                    (dB ? B.ldWord(B.maskWord(bB)) : 0ull);
+                    const uint32_t c = used == ~0ull ? 64u + r : uint32_t(__ffsll(static_cast<long long>(~used)) - 1);
+                    s.color[i] = c;
+                    atomicAdd(s.colorCount + c, 1u);
+                    top = max(top, c + 1);
+                    if (c < 64) {
+                        if (dA) atomicOr(B.maskWord(bA), 1ull << c);
+                        if (dB) atomicOr(B.maskWord(bB), 1ull << c);
+                    }
+                } else {
+                    out[atomicAdd(outLen, 1u)] = e[u];
                 }
-            } else {
-                out[atomicAdd(outLen, 1u)] = i;
             }
         }
         for (int o = 16; o > 0; o >>= 1) top = max(top, __shfl_xor_sync(0xffffffffu, top, o));
@@ -366,7 +427,17 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
     }
     if (!sync()) return false;
     // Constraint build for every manifold before any velocity changes (computeConstraintData).
-    for (uint32_t c = rank; c < n; c += size) {
+    uint32_t c = rank;
+    for (; c + size < n; c += 2 * size) {   // two at a time: independent loads and arithmetic overlap
+        const uint32_t mi0 = __ldcg(s.order + c), mi1 = __ldcg(s.order + c + size);
+        const Manifold m0 = m[mi0], m1 = m[mi1];
+        Constraint k0, k1;
+        prep_constraint(w, B, m0, mi0, k0);
+        prep_constraint(w, B, m1, mi1, k1);
+        s.cons[c] = k0;
+        s.cons[c + size] = k1;
+    }
+    if (c < n) {
         const uint32_t mi = __ldcg(s.order + c);
         Constraint k;
         prep_constraint(w, B, m[mi], mi, k);
@@ -381,11 +452,17 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
     for (uint32_t it = 0; it < velIters; it++) {
         for (uint32_t col = 0; col < ncol; col++) {
             const uint32_t end = Sync::ld(s.colorStart + col + 1);
-            for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) {
+            uint32_t c = Sync::ld(s.colorStart + col) + rank;
+            for (; c + size < end; c += 2 * size) {
+                Constraint k0 = s.cons[c], k1 = s.cons[c + size];
+                velocity_constraint2(B, k0, k1);
+                *reinterpret_cast<float4*>(&s.cons[c].jn0) = make_float4(k0.jn0, k0.jt0, k0.jn1, k0.jt1);
+                *reinterpret_cast<float4*>(&s.cons[c + size].jn0) = make_float4(k1.jn0, k1.jt0, k1.jn1, k1.jt1);
+            }
+            if (c < end) {
                 Constraint k = s.cons[c];
                 velocity_constraint(B, k);
-                float4* imp = reinterpret_cast<float4*>(&s.cons[c].jn0);
-                *imp = make_float4(k.jn0, k.jt0, k.jn1, k.jt1);
+                *reinterpret_cast<float4*>(&s.cons[c].jn0) = make_float4(k.jn0, k.jt0, k.jn1, k.jt1);
             }
             // The next pass's constraint: from the next colour, or colour 0 of the next iteration.
             prefetch_colour<Sync>(s, col + 1 < ncol ? col + 1 : 0, ncol, rank);
@@ -419,11 +496,29 @@ __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* n
 // Batched worlds: teams of consecutive worlds (team k owns worlds [teamWorld[k], teamWorld[k + 1])), each coloured
 // and solved by one CTA with __syncthreads between colours. Teams are taken from the work counter *nextTeam (zeroed
 // before the launch) in 'teamOrder' order, largest first. Colouring priorities are world-local manifold indices, so
-// the colours of a world do not depend on its team.
-constexpr uint32_t SOLVE_TEAM_THREADS = 256;
-__global__ void __launch_bounds__(SOLVE_TEAM_THREADS)
-k_color_solve_teams(DeviceWorld w, Manifold* m, const uint32_t* manSeg, const uint32_t* teamWorld,
-                    const uint32_t* teamOrder, uint32_t teams, uint32_t bodyCap, SolveScratch s, uint32_t velIters,
-                    uint32_t posIters, uint32_t* nextTeam, StepCounters* counters);
+// the colours of a world do not depend on its team. The CTA size (64 to 512 threads) is a launch parameter;
+// a team whose bodies fit 'bodyCap' keeps their state and colouring words in dynamic shared memory
+// (TEAM_SMEM_PER_BODY bytes per body).
+constexpr uint32_t TEAM_SMEM_PER_BODY = 2 * sizeof(float4) + 2 * sizeof(unsigned long long);
+constexpr uint32_t MAX_TEAM_BODY_CAP = 4096;   // largest body range a team stages in shared memory
+struct TeamLaunch {
+    DeviceWorld w;
+    Manifold* m;
+    const uint32_t* manSeg;
+    const uint32_t* teamWorld;
+    const uint32_t* teamOrder;
+    uint32_t teams;
+    uint32_t bodyCap;
+    SolveScratch s;
+    uint32_t velIters, posIters;
+    uint32_t* nextTeam;
+    StepCounters* counters;
+};
+// Host side: launches the team solver with 'threads' per CTA; returns the launch error.
+cudaError_t launch_color_solve_teams(uint32_t threads, uint32_t grid, cudaStream_t stream, const TeamLaunch& a);
+// Host side: co-resident CTAs per SM of the team solver at this CTA size and body capacity. Also raises the kernel's
+// dynamic shared-memory limit to what MAX_TEAM_BODY_CAP needs (the limit is per kernel, shared by every engine in the
+// process, so it is never lowered).
+cudaError_t team_solver_blocks_per_sm(uint32_t threads, uint32_t bodyCap, int* out);
 
 }  // namespace ag2d

@@ -204,9 +204,6 @@ struct PackedArrays {
     }
 };
 
-// Largest body range a solver team stages in shared memory (32 bytes per body).
-constexpr uint32_t MAX_TEAM_BODY_CAP = 4096;
-
 // Manifold count above which the solver runs on the whole grid instead of one cluster.
 constexpr uint32_t GRID_SOLVE_THRESHOLD = 600000;
 
@@ -225,8 +222,6 @@ static DeviceInfo probe_device(int device)
     int perSm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color_solve_grid, 256, 0));
     dev.coopSolveBlocks = std::max(1, perSm) * dev.sms;
-    CK(cudaFuncSetAttribute(k_color_solve_teams, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            int(MAX_TEAM_BODY_CAP * 2 * sizeof(float4))));
     // Largest cluster (16 non-portable, else 8, 4, 2) that can be resident.
     dev.solveCluster = 1;
     if (cudaFuncSetAttribute(k_color_solve_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
@@ -273,6 +268,7 @@ struct ag2d_world {
     uint32_t nBodies = 0, nColliders = 0, nDynBody = 0, nDynCol = 0, nOther = 0, nStatic = 0;
     uint32_t pairCap = 0, manifoldCap = 0, hashCap = 0;
     uint32_t lastManifolds = 0;
+    uint32_t prevCount = 0;   // manifolds in prevManifolds (the warm-start source), as the host knows them
 
     // Bodies.
     DBuf<float4> bvel, bpos;
@@ -299,6 +295,7 @@ struct ag2d_world {
     // Trees and pairs.
     Tree dynTree, otherTree;
     DBuf<uint32_t> qCounts, qOffsets;
+    DBuf<uint2> qStash;   // QUERY_STASH pairs per dynamic collider
     DBuf<uint2> pairs;
     // Manifolds.
     DBuf<Manifold> slots, manifolds, prevManifolds;
@@ -306,14 +303,17 @@ struct ag2d_world {
     DBuf<unsigned long long> hashKeys;
     DBuf<uint32_t> hashVals;
     // Colouring and solver.
-    DBuf<uint32_t> color, colorCount, colorStart, order, bar, prio, listA, listB;
+    DBuf<uint32_t> color, colorCount, colorStart, order, bar, prio;
+    DBuf<uint4> listA, listB;
     DBuf<unsigned long long> bodyMax, bodyMask;
     DBuf<Constraint> cons;
+    DBuf<uint2> pairBodies;
     // Islands.
     DBuf<uint32_t> ufParent, ufFlag, wakeIsland;
     // World partition of a batch (nWorlds == 1: a single world, none of these is used).
     uint32_t nWorlds = 1;
-    uint32_t teamColliders = 2048;         // solver team size: consecutive worlds packed up to this many colliders
+    uint32_t teamColliders = 1024;         // solver team size: consecutive worlds packed up to this many colliders
+    uint32_t teamThreads = 128;            // CTA size of the team solver
     uint32_t teamBodyCap = 2048;           // bodies of a team staged in shared memory (larger teams use global)
     uint32_t nTeams = 0;
     uint32_t teamBlocks = 1;               // co-resident CTAs of the team solver at this shared-memory size
@@ -386,14 +386,14 @@ struct ag2d_world {
     }
 
     // Solver teams: consecutive worlds packed while the team stays within 'colliders' colliders (a larger world is
-    // a team of its own), scheduled largest first.
-    void setTeams(uint32_t colliders)
+    // a team of its own), scheduled largest first, each solved by one CTA of 'threads' threads.
+    void setTeams(uint32_t colliders, uint32_t threads)
     {
         teamColliders = colliders;
+        teamThreads = threads;
         teamBodyCap = std::min<uint32_t>(MAX_TEAM_BODY_CAP, colliders);
         int perSm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_color_solve_teams, SOLVE_TEAM_THREADS,
-                                                         teamBodyCap * 2 * sizeof(float4)));
+        CK(team_solver_blocks_per_sm(teamThreads, teamBodyCap, &perSm));
         teamBlocks = uint32_t(std::max(1, perSm) * dev.sms);
         std::vector<uint32_t> start{0};
         uint32_t acc = 0;
@@ -435,7 +435,7 @@ struct ag2d_world {
         worldColStart.upload(colStart.data(), colStart.size(), s);
         manSeg.reserve(nWorlds + 1);
         nextWorld.reserve(1);
-        setTeams(teamColliders);
+        setTeams(teamColliders, teamThreads);
         worldDirty.reserve(nWorlds);
         CK(cudaMemsetAsync(worldDirty.p, 0, sizeof(uint32_t) * nWorlds, s));
         dynSimd.reserve(std::max(nBodies, nColliders));
@@ -521,6 +521,7 @@ struct ag2d_world {
         prio.reserve(manifoldCap);
         listA.reserve(manifoldCap);
         listB.reserve(manifoldCap);
+        pairBodies.reserve(manifoldCap);
         cons.reserve(manifoldCap);
         hashCap = 16;
         while (hashCap < 2 * manifoldCap) hashCap <<= 1;
@@ -616,6 +617,7 @@ struct ag2d_world {
         nCircles = uint32_t(cr.size()); nBoxes = uint32_t(bh.size()); nPolygons = uint32_t(po.size());
         nPolyVerts = uint32_t(pv.size()); nMaterialRows = uint32_t(mats.size());
         qCounts.reserve(nColliders); qOffsets.reserve(nColliders);
+        qStash.reserve(size_t(std::max<uint32_t>(nColliders, 1)) * QUERY_STASH);
         bodyMax.reserve(nBodies);
         bodyMask.reserve(nBodies);
         ufParent.reserve(nBodies); ufFlag.reserve(nBodies); wakeIsland.reserve(nBodies);
@@ -629,6 +631,7 @@ struct ag2d_world {
         fullPose = true;
         otherDirty = true;
         lastManifolds = 0;
+        prevCount = 0;
     }
 
     void ensureUploaded()
@@ -854,12 +857,13 @@ struct ag2d_world {
         }
         pbegin(4);
         launches += 2 + scanLaunches(nDynCol) + 1;
-        k_query_count<<<gridFor(nDynCol, queryThreads), queryThreads, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qCounts.p,
-                                                            &dCounters.p->status);
+        const uint32_t gq = gridFor(nDynCol, queryThreads);
+        k_query_stash<<<gq, queryThreads, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qCounts.p, qStash.p,
+                                                  &dCounters.p->status);
         CK(cudaGetLastError());
         scanner.run(qCounts.p, qOffsets.p, nDynCol, total, s);
-        k_query_write<<<gridFor(nDynCol, queryThreads), queryThreads, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qOffsets.p,
-                                                            pairs.p, pairCap, &dCounters.p->status);
+        k_query_emit<<<gq, queryThreads, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qCounts.p, qOffsets.p,
+                                                 qStash.p, pairs.p, pairCap, &dCounters.p->status);
         CK(cudaGetLastError());
         pend(4);
     }
@@ -871,7 +875,8 @@ struct ag2d_world {
         const uint32_t g = gridFor(pairCap);
         const uint32_t gn = gridFor(pairCap, narrowThreads);
         pbegin(5);
-        k_narrow<<<gn, narrowThreads, 0, s>>>(view(), pairs.p, nPairs, pairCap, slots.p, hit.p);
+        k_narrow<<<gn, narrowThreads, narrowThreads * NARROW_SMEM_PER_THREAD, s>>>(view(), pairs.p, nPairs, pairCap,
+                                                                                slots.p, hit.p);
         CK(cudaGetLastError());
         pend(5);
         pbegin(6);
@@ -886,11 +891,16 @@ struct ag2d_world {
         if (!warm) return;
         pbegin(7);
         // Warm start from the previous step's manifolds.
-        CK(cudaMemsetAsync(hashKeys.p, 0xFF, size_t(hashCap) * sizeof(unsigned long long), s));
-        k_warm_insert<<<gridFor(manifoldCap), 256, 0, s>>>(prevManifolds.p, nPrev.p, hashKeys.p, hashVals.p, hashCap,
+        // Table sized for the manifolds actually stored (load <= 1/2), not the buffer capacity: a smaller table is
+        // cheaper to clear and stays in L2.
+        uint32_t slotsUsed = 1024;
+        while (slotsUsed < 2 * prevCount && slotsUsed < hashCap) slotsUsed <<= 1;
+        slotsUsed = std::min(slotsUsed, hashCap);
+        CK(cudaMemsetAsync(hashKeys.p, 0xFF, size_t(slotsUsed) * sizeof(unsigned long long), s));
+        k_warm_insert<<<gridFor(manifoldCap), 256, 0, s>>>(prevManifolds.p, nPrev.p, hashKeys.p, hashVals.p, slotsUsed,
                                                            &dCounters.p->status);
         k_warm_lookup<<<gridFor(manifoldCap), 256, 0, s>>>(prevManifolds.p, manifolds.p, nManifolds.p, hashKeys.p,
-                                                           hashVals.p, hashCap, dCounters.p);
+                                                           hashVals.p, slotsUsed, dCounters.p);
         CK(cudaGetLastError());
         pend(7);
     }
@@ -917,7 +927,7 @@ struct ag2d_world {
         Manifold* mm = manifolds.p;
         const uint32_t* nm = nManifolds.p;
         SolveScratch scratch{color.p, order.p, bodyMax.p, bodyMask.p, colorCount.p, colorStart.p, cons.p, nullptr,
-                             listA.p, listB.p};
+                             listA.p, listB.p, pairBodies.p};
         uint32_t vi = settings.velocity_iterations, pi = settings.position_iterations;
         StepCounters* ctr = dCounters.p;
         pbegin(10);
@@ -928,9 +938,9 @@ struct ag2d_world {
                                                                       manSeg.p);
             scratch.prio = prio.p;
             const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(nTeams, teamBlocks));
-            k_color_solve_teams<<<grid, SOLVE_TEAM_THREADS, teamBodyCap * 2 * sizeof(float4), s>>>(
-                w, mm, manSeg.p, teamWorld.p, teamOrder.p, nTeams, teamBodyCap, scratch, vi, pi, nextWorld.p, ctr);
-            CK(cudaGetLastError());
+            const TeamLaunch args{w, mm, manSeg.p, teamWorld.p, teamOrder.p, nTeams, teamBodyCap, scratch, vi, pi,
+                                  nextWorld.p, ctr};
+            CK(launch_color_solve_teams(teamThreads, grid, s, args));
             launches++;
         } else if (lastManifolds <= GRID_SOLVE_THRESHOLD && dev.solveCluster > 1) {
             // One thread-block cluster, hardware barriers between colours.
@@ -1013,23 +1023,40 @@ struct ag2d_world {
         const bool wasProfiling = profiling;
         profiling = true;
         stepOnce();   // first step: uploads, list build, buffer growth
+        // Candidates are timed in interleaved rounds, so that all of them see the same stretch of the simulation
+        // (the load changes from step to step); each first runs one untimed step (first launches load code).
         auto pick = [&](int phase, const std::vector<uint32_t>& cands, auto apply) {
-            double best = 1e300;
-            uint32_t arg = cands.front();
+            std::vector<double> total(cands.size(), 0.0);
+            const bool log = std::getenv("AG2D_TUNE_LOG") != nullptr;   // per-candidate times on stderr
             for (uint32_t c : cands) {
+                if (log) std::fprintf(stderr, "ag2d autotune phase %d trying %u\n", phase, c);
                 apply(c);
                 stepOnce();
-                const double ms = timePhase(phase, stepsPer);
-                if (ms < best) { best = ms; arg = c; }
             }
-            apply(arg);
-            return std::make_pair(arg, best);
+            for (uint32_t r = 0; r < stepsPer; r++)
+                for (size_t k = 0; k < cands.size(); k++) {
+                    apply(cands[k]);
+                    total[k] += timePhase(phase, 1);
+                }
+            size_t best = 0;
+            for (size_t k = 0; k < cands.size(); k++) {
+                if (log) std::fprintf(stderr, "ag2d autotune phase %d candidate %u: %.4f ms\n", phase, cands[k],
+                                      total[k] / stepsPer);
+                if (total[k] < total[best]) best = k;
+            }
+            apply(cands[best]);
+            return std::make_pair(cands[best], total[best] / stepsPer);
         };
         out.team_colliders = 0;
+        out.team_threads = 0;
         out.solve_ms = 0.0f;
         if (nWorlds > 1) {
-            const auto r = pick(10, {512, 1024, 2048, 4096}, [&](uint32_t t) { setTeams(t); });
-            out.team_colliders = r.first;
+            // (colliders per team, threads per CTA), packed as colliders << 16 | threads.
+            const auto r = pick(10, {512u << 16 | 128, 1024u << 16 | 128, 1024u << 16 | 256, 2048u << 16 | 256,
+                                     2048u << 16 | 512, 4096u << 16 | 256, 4096u << 16 | 512},
+                                [&](uint32_t t) { setTeams(t >> 16, t & 0xFFFF); });
+            out.team_colliders = r.first >> 16;
+            out.team_threads = r.first & 0xFFFF;
             out.solve_ms = float(r.second);
         }
         const auto q = pick(4, {64, 128, 256}, [&](uint32_t t) { queryThreads = t; });
@@ -1098,6 +1125,7 @@ struct ag2d_world {
             swap_bufs(manifolds, prevManifolds);
             CK(cudaMemcpyAsync(nPrev.p, nManifolds.p, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
             lastManifolds = hCounters->manifolds;
+            prevCount = std::min(lastManifolds, manifoldCap);
             if (hCounters->topoDirty) {
                 // Woken or slept bodies: refresh the poses of every collider at the post-step state (the reference
                 // rebuilds its spatial data in postUpdate, Simulation.cpp:640-647), then the work lists and the
@@ -1575,6 +1603,7 @@ int32_t ag2d_world_write(ag2d_world* world, int32_t field, const void* src, uint
             const bool prev = field == AG2D_PREV_MANIFOLDS;
             if (n) CK(cudaMemcpyAsync(prev ? w.prevManifolds.p : w.manifolds.p, src, bytes, cudaMemcpyHostToDevice, s));
             CK(cudaMemcpyAsync(prev ? w.nPrev.p : w.nManifolds.p, &n, 4, cudaMemcpyHostToDevice, s));
+            if (prev) w.prevCount = n;
             break;
         }
         default: throw ApiError(AG2D_ERR_INVALID_ARG, "field is not writable");
@@ -1682,6 +1711,7 @@ int32_t ag2d_batch_create(ag2d_world* const* worlds, uint32_t count, ag2d_batch*
         if (np) CK(cudaMemcpyAsync(e.prevManifolds.p, all.prev.data(), np * sizeof(Manifold), cudaMemcpyHostToDevice,
                                    e.stream));
         CK(cudaMemcpyAsync(e.nPrev.p, &np, sizeof(uint32_t), cudaMemcpyHostToDevice, e.stream));
+        e.prevCount = np;
         CK(cudaStreamSynchronize(e.stream));
         *out = b.release();
     });

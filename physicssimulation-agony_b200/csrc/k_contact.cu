@@ -35,26 +35,70 @@ __device__ __forceinline__ ColliderView collider_view(const DeviceWorld& w, uint
 // lower shape type first, equal types put the higher collider index first) and the shape-pair method. One thread
 // per candidate pair writes the pair's manifold slot and a hit flag; a scan then compacts hits in pair order.
 // ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void write_slot(const Contact& ct, uint32_t a, uint32_t b, Manifold* slot)
+{
+    Manifold m;
+    m.a = a; m.b = b; m.nx = ct.n.x; m.ny = ct.n.y; m.depth = ct.depth; m.count = ct.count;
+    m.id0 = ct.id[0]; m.px0 = ct.p[0].x; m.py0 = ct.p[0].y;
+    if (ct.count > 1) { m.id1 = ct.id[1]; m.px1 = ct.p[1].x; m.py1 = ct.p[1].y; }
+    else { m.id1 = 0; m.px1 = 0.0f; m.py1 = 0.0f; }
+    m.jn0 = 0.0f; m.jt0 = 0.0f; m.jn1 = 0.0f; m.jt1 = 0.0f;
+    *slot = m;
+}
+
+// Each warp takes 32 consecutive pairs. Pairs of other shape types run one per lane; then the warp's
+// polygon-polygon pairs run four at a time, one per group of NARROW_GROUP lanes (collide_polygon_polygon_group).
+// Launched with a multiple of 32 threads per block and NARROW_SMEM_PER_THREAD bytes of dynamic shared memory per
+// thread (each group's vertex tiles).
 __global__ void k_narrow(DeviceWorld w, const uint2* __restrict__ pairs, const uint32_t* __restrict__ nPairs,
                          uint32_t pairCap, Manifold* __restrict__ slots, uint32_t* __restrict__ hit)
 {
+    extern __shared__ V2 tiles[];   // per group: A's vertices, then B's (in A's frame)
     const uint32_t n = min(*nPairs, pairCap);
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-        uint32_t a = pairs[p].x, b = pairs[p].y;
-        uint32_t ta = shape_type(w.cshape[a]), tb = shape_type(w.cshape[b]);
-        if (ta > tb || (ta == tb && b > a)) { const uint32_t t = a; a = b; b = t; }
-        const ColliderView A = collider_view(w, a), B = collider_view(w, b);
-        Contact ct;
-        const bool h = collide(A, B, ct);
-        hit[p] = h ? 1u : 0u;
-        if (h) {
-            Manifold m;
-            m.a = a; m.b = b; m.nx = ct.n.x; m.ny = ct.n.y; m.depth = ct.depth; m.count = ct.count;
-            m.id0 = ct.id[0]; m.px0 = ct.p[0].x; m.py0 = ct.p[0].y;
-            if (ct.count > 1) { m.id1 = ct.id[1]; m.px1 = ct.p[1].x; m.py1 = ct.p[1].y; }
-            else { m.id1 = 0; m.px1 = 0.0f; m.py1 = 0.0f; }
-            m.jn0 = 0.0f; m.jt0 = 0.0f; m.jn1 = 0.0f; m.jt1 = 0.0f;
-            slots[p] = m;
+    const uint32_t lane = threadIdx.x & 31, group = lane / NARROW_GROUP, gl = lane % NARROW_GROUP;
+    const uint32_t gmask = ((1u << NARROW_GROUP) - 1u) << (group * NARROW_GROUP);
+    V2* sA = tiles + (threadIdx.x / NARROW_GROUP) * 2 * MAX_POLYGON_VERTICES;
+    V2* sB = sA + MAX_POLYGON_VERTICES;
+    const uint32_t warps = gridDim.x * (blockDim.x / 32);
+    for (uint32_t tile = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; tile * 32u < n; tile += warps) {
+        const uint32_t p = tile * 32u + lane;
+        const bool valid = p < n;
+        uint32_t a = 0, b = 0;
+        bool pp = false;
+        if (valid) {
+            a = pairs[p].x;
+            b = pairs[p].y;
+            const uint32_t ta = shape_type(w.cshape[a]), tb = shape_type(w.cshape[b]);
+            if (ta > tb || (ta == tb && b > a)) { const uint32_t t = a; a = b; b = t; }
+            pp = ta == SHAPE_POLYGON && tb == SHAPE_POLYGON;
+            if (!pp) {
+                const ColliderView A = collider_view(w, a), B = collider_view(w, b);
+                Contact ct;
+                const bool h = collide(A, B, ct);
+                hit[p] = h ? 1u : 0u;
+                if (h) write_slot(ct, a, b, slots + p);
+            }
+        }
+        uint32_t todo = __ballot_sync(0xffffffffu, pp);
+        while (todo) {
+            // Group g takes the g-th remaining polygon-polygon lane.
+            uint32_t pick = todo;
+            for (uint32_t k = 0; k < group && pick; k++) pick &= pick - 1;
+            const bool has = pick != 0;
+            const uint32_t src = has ? uint32_t(__ffs(pick) - 1) : 0u;
+            const uint32_t ga = __shfl_sync(0xffffffffu, a, src), gb = __shfl_sync(0xffffffffu, b, src);
+            const uint32_t gp = tile * 32u + src;
+            for (uint32_t k = 0; k < 32 / NARROW_GROUP && todo; k++) todo &= todo - 1;
+            if (has) {
+                const ColliderView A = collider_view(w, ga), B = collider_view(w, gb);
+                Contact ct;
+                const bool h = collide_polygon_polygon_group(A, B, ct, gl, gmask, sA, sB);
+                if (gl == 0) {
+                    hit[gp] = h ? 1u : 0u;
+                    if (h) write_slot(ct, ga, gb, slots + gp);
+                }
+                __syncwarp(gmask);   // the group's tiles are reused by its next pair
+            }
         }
     }
 }
@@ -197,7 +241,8 @@ k_color_solve_cluster(DeviceWorld w, Manifold* m, const uint32_t* nM, SolveScrat
     const cg::cluster_group cluster = cg::this_cluster();
     const uint32_t rank = cluster.block_rank() * blockDim.x + threadIdx.x;
     const uint32_t size = cluster.num_blocks() * blockDim.x;
-    color_and_solve(w, GlobalBodies{w.bvel, w.bpos}, m, *nM, s, velIters, posIters, rank, size, ClusterSync{},
+    color_and_solve(w, GlobalBodies{w.bvel, w.bpos, s.bodyMax, s.bodyMask}, m, *nM, s, velIters, posIters, rank, size,
+                    ClusterSync{},
                     &counters->colors,
                     &counters->status);
 }
@@ -208,8 +253,8 @@ __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* n
 {
     const uint32_t rank = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t size = gridDim.x * blockDim.x;
-    color_and_solve(w, GlobalBodies{w.bvel, w.bpos}, m, *nM, s, velIters, posIters, rank, size,
-                    GridSync{bar, &counters->status},
+    color_and_solve(w, GlobalBodies{w.bvel, w.bpos, s.bodyMax, s.bodyMask}, m, *nM, s, velIters, posIters, rank,
+                    size, GridSync{bar, &counters->status},
                     &counters->colors, &counters->status);
 }
 
@@ -217,55 +262,93 @@ __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* n
 // the world-grouped list, and colours + solves that range as one problem (the worlds share no body, so their
 // colour classes simply merge). Priorities are world-local indices: every world gets the colouring, hence the
 // solving order, it has when stepped on its own, whichever team it is in. A team whose bodies fit the dynamic
-// shared memory (bodyCap bodies) solves on a shared-memory copy of their velocities and poses.
-__global__ void __launch_bounds__(SOLVE_TEAM_THREADS)
-k_color_solve_teams(DeviceWorld w, Manifold* m, const uint32_t* __restrict__ manSeg,
-                    const uint32_t* __restrict__ teamWorld, const uint32_t* __restrict__ teamOrder, uint32_t teams,
-                    uint32_t bodyCap, SolveScratch s, uint32_t velIters, uint32_t posIters, uint32_t* nextTeam,
-                    StepCounters* counters)
+// shared memory (bodyCap bodies) keeps their velocities, poses and colouring words there.
+template <uint32_t THREADS>
+__global__ void __launch_bounds__(THREADS) k_color_solve_teams(TeamLaunch a)
 {
-    extern __shared__ float4 bodyCache[];   // [bodyCap] velocities, then [bodyCap] poses
+    extern __shared__ float4 teamCache[];   // [bodyCap] velocities, [bodyCap] poses, then 2 x [bodyCap] u64 words
     __shared__ uint32_t colorCount[COLOR_SLOTS];
     __shared__ uint32_t colorStart[MAX_COLORS + 1];
     __shared__ uint32_t item;
-    uint32_t* prio = const_cast<uint32_t*>(s.prio);
+    const DeviceWorld& w = a.w;
+    Manifold* m = a.m;
+    uint32_t* prio = const_cast<uint32_t*>(a.s.prio);
     while (true) {
-        if (threadIdx.x == 0) item = atomicAdd(nextTeam, 1u);
+        if (threadIdx.x == 0) item = atomicAdd(a.nextTeam, 1u);
         __syncthreads();
         const uint32_t k = item;
         __syncthreads();
-        if (k >= teams) return;
-        const uint32_t t = teamOrder[k];
-        const uint32_t w0 = teamWorld[t], w1 = teamWorld[t + 1];
-        const uint32_t lo = manSeg[w0], hi = manSeg[w1];
+        if (k >= a.teams) return;
+        const uint32_t t = a.teamOrder[k];
+        const uint32_t w0 = a.teamWorld[t], w1 = a.teamWorld[t + 1];
+        const uint32_t lo = a.manSeg[w0], hi = a.manSeg[w1];
         if (hi <= lo) continue;
-        for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
-            prio[i] = priority_hash(i - manSeg[w.bodyWorld[w.cbody[m[i].a]]]);
-        const SolveScratch ls{s.color + lo, s.order + lo, s.bodyMax, s.bodyMask, colorCount, colorStart,
-                              s.cons + lo, prio + lo, s.listA + lo, s.listB + lo};
+        for (uint32_t i = lo + threadIdx.x; i < hi; i += THREADS)
+            prio[i] = priority_hash(i - a.manSeg[w.bodyWorld[w.cbody[m[i].a]]]);
+        const SolveScratch ls{a.s.color + lo, a.s.order + lo, a.s.bodyMax, a.s.bodyMask, colorCount, colorStart,
+                              a.s.cons + lo, prio + lo, a.s.listA + lo, a.s.listB + lo, a.s.pairBodies + lo};
         const uint32_t b0 = w.worldBodyStart[w0], nb = w.worldBodyStart[w1] - b0;
-        if (nb <= bodyCap) {
-            float4* vel = bodyCache;
-            float4* pos = bodyCache + bodyCap;
-            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+        if (nb <= a.bodyCap) {
+            float4* vel = teamCache;
+            float4* pos = teamCache + a.bodyCap;
+            auto* maxW = reinterpret_cast<unsigned long long*>(teamCache + 2 * a.bodyCap);
+            unsigned long long* maskW = maxW + a.bodyCap;
+            for (uint32_t i = threadIdx.x; i < nb; i += THREADS) {
                 vel[i] = w.bvel[b0 + i];
                 pos[i] = w.bpos[b0 + i];
+                maxW[i] = 0ull;
+                maskW[i] = 0ull;
             }
             __syncthreads();
-            color_and_solve(w, SharedBodies{vel, pos, b0}, m + lo, hi - lo, ls, velIters, posIters, threadIdx.x,
-                            blockDim.x, BlockSync{}, &counters->colors, &counters->status);
+            color_and_solve(w, SharedBodies{vel, pos, maxW, maskW, b0}, m + lo, hi - lo, ls, a.velIters, a.posIters,
+                            threadIdx.x, THREADS, BlockSync{}, &a.counters->colors, &a.counters->status);
             __syncthreads();
-            for (uint32_t i = threadIdx.x; i < nb; i += blockDim.x) {
+            for (uint32_t i = threadIdx.x; i < nb; i += THREADS) {
                 w.bvel[b0 + i] = vel[i];
                 w.bpos[b0 + i] = pos[i];
             }
         } else {
             __syncthreads();
-            color_and_solve(w, GlobalBodies{w.bvel, w.bpos}, m + lo, hi - lo, ls, velIters, posIters, threadIdx.x,
-                            blockDim.x, BlockSync{}, &counters->colors, &counters->status);
+            color_and_solve(w, GlobalBodies{w.bvel, w.bpos, a.s.bodyMax, a.s.bodyMask}, m + lo, hi - lo, ls,
+                            a.velIters, a.posIters, threadIdx.x, THREADS, BlockSync{}, &a.counters->colors,
+                            &a.counters->status);
         }
         __syncthreads();
     }
+}
+
+template <uint32_t THREADS>
+static cudaError_t team_occupancy(uint32_t bodyCap, int* out)
+{
+    cudaError_t e = cudaFuncSetAttribute(k_color_solve_teams<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(size_t(MAX_TEAM_BODY_CAP) * TEAM_SMEM_PER_BODY));
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, k_color_solve_teams<THREADS>, THREADS,
+                                                         size_t(bodyCap) * TEAM_SMEM_PER_BODY);
+}
+
+cudaError_t team_solver_blocks_per_sm(uint32_t threads, uint32_t bodyCap, int* out)
+{
+    switch (threads) {
+    case 64: return team_occupancy<64>(bodyCap, out);
+    case 128: return team_occupancy<128>(bodyCap, out);
+    case 256: return team_occupancy<256>(bodyCap, out);
+    case 512: return team_occupancy<512>(bodyCap, out);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_color_solve_teams(uint32_t threads, uint32_t grid, cudaStream_t stream, const TeamLaunch& a)
+{
+    const size_t smem = size_t(a.bodyCap) * TEAM_SMEM_PER_BODY;
+    switch (threads) {
+    case 64: k_color_solve_teams<64><<<grid, 64, smem, stream>>>(a); break;
+    case 128: k_color_solve_teams<128><<<grid, 128, smem, stream>>>(a); break;
+    case 256: k_color_solve_teams<256><<<grid, 256, smem, stream>>>(a); break;
+    case 512: k_color_solve_teams<512><<<grid, 512, smem, stream>>>(a); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------------------------------------------

@@ -510,9 +510,10 @@ __global__ void k_lbvh_refit(int n, const int2* __restrict__ child, const int* _
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int node = leafParent[i];   // -1 for the leaf of a one-collider segment
         while (node >= 0) {
-            __threadfence();
+            // Release this thread's node write before the arrival count; the second arrival acquires both children.
+            asm volatile("fence.acq_rel.gpu;" ::: "memory");
             if (atomicAdd(&visit[node], 1u) == 0) break;
-            __threadfence();
+            asm volatile("fence.acq_rel.gpu;" ::: "memory");
             const int2 c = child[node];
             const float4 a = c.x < 0 ? leafAabb[~c.x] : __ldcg(nodeAabb + c.x);
             const float4 b = c.y < 0 ? leafAabb[~c.y] : __ldcg(nodeAabb + c.y);
@@ -526,113 +527,118 @@ __global__ void k_lbvh_refit(int n, const int2* __restrict__ child, const int* _
 // ---------------------------------------------------------------------------------------------------------------
 // Pair query. For dynamic collider of sorted rank i: every dynamic collider of rank > i whose AABB strictly
 // overlaps (BvhNode::overlaps, BvhNode.h:33-38) and has another owner body (LeafPairTesting.h:71-134), then every
-// static/sleeping collider that overlaps (cross pairs, ordered (dynamic, other)). Count pass then write pass at
-// scanned offsets: a deterministic pair list ordered by query rank and traversal order.
+// static/sleeping collider that overlaps (cross pairs, ordered (dynamic, other)). One traversal counts each query's
+// pairs and keeps the first few; after a scan of the counts they land at their offsets: a deterministic pair list
+// ordered by query rank and traversal order.
 // ---------------------------------------------------------------------------------------------------------------
 __device__ __forceinline__ bool strict_overlap(const float4& a, const float4& b)
 {
     return a.x < b.z && a.z > b.x && a.y < b.w && a.w > b.y;
 }
 
-template <bool WRITE>
-__device__ __forceinline__ void query_impl(const TreeView& dyn, const TreeView& other,
-                                           const uint32_t* __restrict__ cbody, uint32_t* __restrict__ counts,
-                                           const uint32_t* __restrict__ offsets, uint2* __restrict__ pairs,
-                                           uint32_t pairCap, uint32_t* __restrict__ status)
+// All pairs of dynamic collider rank i, in traversal order; emit(k, pair) receives the k-th. Returns the count.
+template <class Emit>
+__device__ __forceinline__ uint32_t query_one(const TreeView& dyn, const TreeView& other,
+                                              const uint32_t* __restrict__ cbody, int i, Emit emit,
+                                              uint32_t* __restrict__ status)
 {
     const int n = dyn.n;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 q = dyn.leafAabb[i];
-        const uint32_t me = dyn.vals[i];
-        const uint32_t myBody = cbody[me];
-        // This collider's world: the segments of both trees it is tested against.
-        int dlo = 0, dhi = n, olo = 0, ohi = other.n;
-        if (dyn.sortedWorld) {
-            const uint32_t wd = dyn.sortedWorld[i];
-            dlo = int(dyn.segStart[wd]);
-            dhi = int(dyn.segStart[wd + 1]);
-            if (other.n > 0) {
-                olo = int(other.segStart[wd]);
-                ohi = int(other.segStart[wd + 1]);
-            } else {
-                ohi = 0;
-            }
+    const float4 q = dyn.leafAabb[i];
+    const uint32_t me = dyn.vals[i];
+    const uint32_t myBody = cbody[me];
+    // This collider's world: the segments of both trees it is tested against.
+    int dlo = 0, dhi = n, olo = 0, ohi = other.n;
+    if (dyn.sortedWorld) {
+        const uint32_t wd = dyn.sortedWorld[i];
+        dlo = int(dyn.segStart[wd]);
+        dhi = int(dyn.segStart[wd + 1]);
+        if (other.n > 0) {
+            olo = int(other.segStart[wd]);
+            ohi = int(other.segStart[wd + 1]);
+        } else {
+            ohi = 0;
         }
-        uint32_t count = 0;
-        uint32_t out = WRITE ? offsets[i] : 0u;
-        int stack[QUERY_STACK];
-        // Self pairs within the dynamic tree.
-        if (dhi - dlo > 1) {
-            int sp = 0;
-            stack[sp++] = dlo;
-            while (sp > 0) {
-                const int node = stack[--sp];
-                const int2 c = dyn.child[node];
+    }
+    uint32_t count = 0;
+    int stack[QUERY_STACK];
+    // Self pairs within the dynamic tree.
+    if (dhi - dlo > 1) {
+        int sp = 0;
+        stack[sp++] = dlo;
+        while (sp > 0) {
+            const int node = stack[--sp];
+            const int2 c = dyn.child[node];
 #pragma unroll
-                for (int side = 0; side < 2; side++) {
-                    const int ch = side == 0 ? c.x : c.y;
-                    if (ch < 0) {
-                        const int j = ~ch;
-                        if (j > i && strict_overlap(q, dyn.leafAabb[j])) {
-                            const uint32_t other_c = dyn.vals[j];
-                            if (cbody[other_c] != myBody) {
-                                if (WRITE && out < pairCap) pairs[out] = make_uint2(me, other_c);
-                                out++;
-                                count++;
-                            }
-                        }
-                    } else if (dyn.range[ch].y > i && strict_overlap(q, dyn.nodeAabb[ch])) {
-                        if (sp < QUERY_STACK) stack[sp++] = ch;
-                        else atomicOr(status, STATUS_STACK_OVERFLOW);
+            for (int side = 0; side < 2; side++) {
+                const int ch = side == 0 ? c.x : c.y;
+                if (ch < 0) {
+                    const int j = ~ch;
+                    if (j > i && strict_overlap(q, dyn.leafAabb[j])) {
+                        const uint32_t other_c = dyn.vals[j];
+                        if (cbody[other_c] != myBody) emit(count++, make_uint2(me, other_c));
                     }
+                } else if (dyn.range[ch].y > i && strict_overlap(q, dyn.nodeAabb[ch])) {
+                    if (sp < QUERY_STACK) stack[sp++] = ch;
+                    else atomicOr(status, STATUS_STACK_OVERFLOW);
                 }
             }
         }
-        // Cross pairs against the static + sleeping tree.
-        if (ohi - olo == 1) {
-            if (strict_overlap(q, other.leafAabb[olo])) {
-                if (WRITE && out < pairCap) pairs[out] = make_uint2(me, other.vals[olo]);
-                out++;
-                count++;
-            }
-        } else if (ohi - olo > 1 && strict_overlap(q, other.nodeAabb[olo])) {
-            int sp = 0;
-            stack[sp++] = olo;
-            while (sp > 0) {
-                const int node = stack[--sp];
-                const int2 c = other.child[node];
+    }
+    // Cross pairs against the static + sleeping tree.
+    if (ohi - olo == 1) {
+        if (strict_overlap(q, other.leafAabb[olo])) emit(count++, make_uint2(me, other.vals[olo]));
+    } else if (ohi - olo > 1 && strict_overlap(q, other.nodeAabb[olo])) {
+        int sp = 0;
+        stack[sp++] = olo;
+        while (sp > 0) {
+            const int node = stack[--sp];
+            const int2 c = other.child[node];
 #pragma unroll
-                for (int side = 0; side < 2; side++) {
-                    const int ch = side == 0 ? c.x : c.y;
-                    if (ch < 0) {
-                        if (strict_overlap(q, other.leafAabb[~ch])) {
-                            if (WRITE && out < pairCap) pairs[out] = make_uint2(me, other.vals[~ch]);
-                            out++;
-                            count++;
-                        }
-                    } else if (strict_overlap(q, other.nodeAabb[ch])) {
-                        if (sp < QUERY_STACK) stack[sp++] = ch;
-                        else atomicOr(status, STATUS_STACK_OVERFLOW);
-                    }
+            for (int side = 0; side < 2; side++) {
+                const int ch = side == 0 ? c.x : c.y;
+                if (ch < 0) {
+                    if (strict_overlap(q, other.leafAabb[~ch])) emit(count++, make_uint2(me, other.vals[~ch]));
+                } else if (strict_overlap(q, other.nodeAabb[ch])) {
+                    if (sp < QUERY_STACK) stack[sp++] = ch;
+                    else atomicOr(status, STATUS_STACK_OVERFLOW);
                 }
             }
         }
-        if (!WRITE) counts[i] = count;
-        else if (out > pairCap) atomicOr(status, STATUS_PAIR_OVERFLOW);
+    }
+    return count;
+}
+
+// One traversal per query: the count, and the first QUERY_STASH pairs kept in the query's stash slots.
+__global__ void k_query_stash(TreeView dyn, TreeView other, const uint32_t* __restrict__ cbody,
+                              uint32_t* __restrict__ counts, uint2* __restrict__ stash, uint32_t* __restrict__ status)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < dyn.n; i += gridDim.x * blockDim.x) {
+        uint2* mine = stash + size_t(i) * QUERY_STASH;
+        counts[i] = query_one(dyn, other, cbody, i, [&](uint32_t k, uint2 p) { if (k < QUERY_STASH) mine[k] = p; },
+                              status);
     }
 }
 
-__global__ void k_query_count(TreeView dyn, TreeView other, const uint32_t* __restrict__ cbody,
-                              uint32_t* __restrict__ counts, uint32_t* __restrict__ status)
+// Pairs to their scanned offsets: copied from the stash, or, for a query with more pairs than the stash holds,
+// written by a second traversal (the same order).
+__global__ void k_query_emit(TreeView dyn, TreeView other, const uint32_t* __restrict__ cbody,
+                             const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
+                             const uint2* __restrict__ stash, uint2* __restrict__ pairs, uint32_t pairCap,
+                             uint32_t* __restrict__ status)
 {
-    query_impl<false>(dyn, other, cbody, counts, nullptr, nullptr, 0, status);
-}
-
-__global__ void k_query_write(TreeView dyn, TreeView other, const uint32_t* __restrict__ cbody,
-                              const uint32_t* __restrict__ offsets, uint2* __restrict__ pairs, uint32_t pairCap,
-                              uint32_t* __restrict__ status)
-{
-    query_impl<true>(dyn, other, cbody, nullptr, offsets, pairs, pairCap, status);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < dyn.n; i += gridDim.x * blockDim.x) {
+        const uint32_t c = counts[i], out = offsets[i];
+        if (c == 0) continue;
+        if (out + c > pairCap) atomicOr(status, STATUS_PAIR_OVERFLOW);
+        if (c <= QUERY_STASH) {
+            const uint2* mine = stash + size_t(i) * QUERY_STASH;
+            for (uint32_t k = 0; k < c; k++)
+                if (out + k < pairCap) pairs[out + k] = mine[k];
+        } else {
+            query_one(dyn, other, cbody, i, [&](uint32_t k, uint2 p) { if (out + k < pairCap) pairs[out + k] = p; },
+                      status);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------------------------------------

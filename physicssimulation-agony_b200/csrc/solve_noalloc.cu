@@ -23,12 +23,14 @@ constexpr uint32_t NOALLOC_THREADS = 512;
 constexpr size_t NA_CONS = 0;                                                         // Constraint[M]
 constexpr size_t NA_COLOR = NA_CONS + size_t(NOALLOC_MAX_MANIFOLDS) * sizeof(Constraint);   // u32[M]
 constexpr size_t NA_ORDER = NA_COLOR + size_t(NOALLOC_MAX_MANIFOLDS) * 4;            // u32[M]
-constexpr size_t NA_LIST_A = NA_ORDER + size_t(NOALLOC_MAX_MANIFOLDS) * 4;           // u32[M]
-constexpr size_t NA_LIST_B = NA_LIST_A + size_t(NOALLOC_MAX_MANIFOLDS) * 4;          // u32[M]
-constexpr size_t NA_BODY_MAX = NA_LIST_B + size_t(NOALLOC_MAX_MANIFOLDS) * 4;        // u64[B]
+constexpr size_t NA_LIST_A = NA_ORDER + size_t(NOALLOC_MAX_MANIFOLDS) * 4;           // uint4[M]
+constexpr size_t NA_LIST_B = NA_LIST_A + size_t(NOALLOC_MAX_MANIFOLDS) * 16;         // uint4[M]
+constexpr size_t NA_BODY_MAX = NA_LIST_B + size_t(NOALLOC_MAX_MANIFOLDS) * 16;       // u64[B]
 constexpr size_t NA_BODY_MASK = NA_BODY_MAX + size_t(NOALLOC_MAX_BODIES) * 8;        // u64[B]
-constexpr size_t NA_BYTES = NA_BODY_MASK + size_t(NOALLOC_MAX_BODIES) * 8;           // 2.6 MiB
-static_assert(NA_COLOR % 256 == 0 && NA_BODY_MAX % 256 == 0 && NA_BODY_MASK % 256 == 0, "256-byte parts");
+constexpr size_t NA_PAIRS = NA_BODY_MASK + size_t(NOALLOC_MAX_BODIES) * 8;           // uint2[M]
+constexpr size_t NA_BYTES = NA_PAIRS + size_t(NOALLOC_MAX_MANIFOLDS) * 8;             // 3.1 MiB
+static_assert(NA_COLOR % 256 == 0 && NA_BODY_MAX % 256 == 0 && NA_BODY_MASK % 256 == 0 && NA_PAIRS % 256 == 0,
+              "256-byte parts");
 static_assert(sizeof(ag2d_manifold) == sizeof(Manifold), "ag2d_manifold is the device Manifold record");
 
 static __device__ __align__(256) unsigned char g_solveScratch[NA_BYTES];
@@ -55,10 +57,10 @@ k_color_solve_static(DeviceWorld w, Manifold* m, uint32_t n, unsigned char* scra
     __syncthreads();
     const SolveScratch s{reinterpret_cast<uint32_t*>(scratch + NA_COLOR), reinterpret_cast<uint32_t*>(scratch + NA_ORDER),
                          bodyMax, bodyMask, colorCount, colorStart, reinterpret_cast<Constraint*>(scratch + NA_CONS),
-                         nullptr, reinterpret_cast<uint32_t*>(scratch + NA_LIST_A),
-                         reinterpret_cast<uint32_t*>(scratch + NA_LIST_B)};
-    color_and_solve(w, GlobalBodies{w.bvel, w.bpos}, m, n, s, velIters, posIters, threadIdx.x, blockDim.x,
-                    BlockSync{}, &colors, &status);
+                         nullptr, reinterpret_cast<uint4*>(scratch + NA_LIST_A),
+                         reinterpret_cast<uint4*>(scratch + NA_LIST_B), reinterpret_cast<uint2*>(scratch + NA_PAIRS)};
+    color_and_solve(w, GlobalBodies{w.bvel, w.bpos, bodyMax, bodyMask}, m, n, s, velIters, posIters, threadIdx.x,
+                    blockDim.x, BlockSync{}, &colors, &status);
     __syncthreads();
     if (threadIdx.x == 0 && statusOut) {
         statusOut[0] = status;
