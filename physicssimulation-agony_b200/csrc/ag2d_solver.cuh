@@ -241,20 +241,6 @@ __device__ __forceinline__ void velocity_constraint(const Bodies& B, Constraint&
     if (k.imB > 0.0f) B.setV(k.bodyB, vB);
 }
 
-// Two constraints of one colour (no shared dynamic body) at once: loads first, then both solves, then the stores,
-// so the two dependency chains overlap. Static bodies are never written, so a body the two share is only read.
-template <class Bodies>
-__device__ __forceinline__ void velocity_constraint2(const Bodies& B, Constraint& k0, Constraint& k1)
-{
-    float4 vA0 = B.v(k0.bodyA), vB0 = B.v(k0.bodyB), vA1 = B.v(k1.bodyA), vB1 = B.v(k1.bodyB);
-    velocity_solve(k0, vA0, vB0);
-    velocity_solve(k1, vA1, vB1);
-    if (k0.imA > 0.0f) B.setV(k0.bodyA, vA0);
-    if (k0.imB > 0.0f) B.setV(k0.bodyB, vB0);
-    if (k1.imA > 0.0f) B.setV(k1.bodyA, vA1);
-    if (k1.imB > 0.0f) B.setV(k1.bodyB, vB1);
-}
-
 template <class Bodies>
 __device__ __forceinline__ void position_constraint(const Bodies& B, const Constraint& k)
 {
@@ -427,17 +413,7 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
     }
     if (!sync()) return false;
     // Constraint build for every manifold before any velocity changes (computeConstraintData).
-    uint32_t c = rank;
-    for (; c + size < n; c += 2 * size) {   // two at a time: independent loads and arithmetic overlap
-        const uint32_t mi0 = __ldcg(s.order + c), mi1 = __ldcg(s.order + c + size);
-        const Manifold m0 = m[mi0], m1 = m[mi1];
-        Constraint k0, k1;
-        prep_constraint(w, B, m0, mi0, k0);
-        prep_constraint(w, B, m1, mi1, k1);
-        s.cons[c] = k0;
-        s.cons[c + size] = k1;
-    }
-    if (c < n) {
+    for (uint32_t c = rank; c < n; c += size) {
         const uint32_t mi = __ldcg(s.order + c);
         Constraint k;
         prep_constraint(w, B, m[mi], mi, k);
@@ -452,14 +428,7 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
     for (uint32_t it = 0; it < velIters; it++) {
         for (uint32_t col = 0; col < ncol; col++) {
             const uint32_t end = Sync::ld(s.colorStart + col + 1);
-            uint32_t c = Sync::ld(s.colorStart + col) + rank;
-            for (; c + size < end; c += 2 * size) {
-                Constraint k0 = s.cons[c], k1 = s.cons[c + size];
-                velocity_constraint2(B, k0, k1);
-                *reinterpret_cast<float4*>(&s.cons[c].jn0) = make_float4(k0.jn0, k0.jt0, k0.jn1, k0.jt1);
-                *reinterpret_cast<float4*>(&s.cons[c + size].jn0) = make_float4(k1.jn0, k1.jt0, k1.jn1, k1.jt1);
-            }
-            if (c < end) {
+            for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) {
                 Constraint k = s.cons[c];
                 velocity_constraint(B, k);
                 *reinterpret_cast<float4*>(&s.cons[c].jn0) = make_float4(k.jn0, k.jt0, k.jn1, k.jt1);
@@ -501,6 +470,7 @@ __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* n
 // (TEAM_SMEM_PER_BODY bytes per body).
 constexpr uint32_t TEAM_SMEM_PER_BODY = 2 * sizeof(float4) + 2 * sizeof(unsigned long long);
 constexpr uint32_t MAX_TEAM_BODY_CAP = 4096;   // largest body range a team stages in shared memory
+constexpr uint32_t BIG_TEAM_THREADS = 512;     // CTA size for a world larger than the team size
 struct TeamLaunch {
     DeviceWorld w;
     Manifold* m;

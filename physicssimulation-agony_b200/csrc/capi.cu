@@ -317,11 +317,14 @@ struct ag2d_world {
     uint32_t teamBodyCap = 2048;           // bodies of a team staged in shared memory (larger teams use global)
     uint32_t nTeams = 0;
     uint32_t teamBlocks = 1;               // co-resident CTAs of the team solver at this shared-memory size
+    uint32_t nBigTeams = 0, bigBodyCap = 0, bigBlocks = 1;   // worlds larger than a team, one CTA each
+    cudaStream_t sideStream = nullptr;     // the big-world solver runs here, beside the small-team solver
+    cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
     uint32_t queryThreads = 128;           // block sizes of the pair query and the narrow phase (tunable)
     uint32_t narrowThreads = 256;
     std::vector<uint32_t> hBodyStart, hColStart;     // [nWorlds + 1]
     DBuf<uint32_t> bodyWorld, colWorld, worldBodyStart, worldColStart, manSeg, nextWorld, worldDirty;
-    DBuf<uint32_t> teamWorld, teamOrder;     // solver teams: first world of each team [nTeams + 1]; largest first
+    DBuf<uint32_t> teamWorld, teamOrder;     // solver teams: first world of each team; small then big, largest first
     DBuf<uint8_t> dynSimd, dynColSimd;               // SIMD-path flag of each work-list entry
     // Shape table sizes of the last upload.
     uint32_t nCircles = 0, nBoxes = 0, nPolygons = 0, nPolyVerts = 0, nMaterialRows = 0;
@@ -395,24 +398,44 @@ struct ag2d_world {
         int perSm = 0;
         CK(team_solver_blocks_per_sm(teamThreads, teamBodyCap, &perSm));
         teamBlocks = uint32_t(std::max(1, perSm) * dev.sms);
+        // Worlds above the team size are teams of their own ("big", solved by BIG_TEAM_THREADS-thread CTAs);
+        // the others are packed, in order, into teams of up to 'colliders' colliders.
         std::vector<uint32_t> start{0};
-        uint32_t acc = 0;
+        std::vector<uint32_t> big, small;
+        uint32_t acc = 0, bigMax = 0;
+        auto close = [&](uint32_t k) {
+            if (k > start.back()) { small.push_back(uint32_t(start.size() - 1)); start.push_back(k); }
+            acc = 0;
+        };
         for (uint32_t k = 0; k < nWorlds; k++) {
             const uint32_t c = hColStart[k + 1] - hColStart[k];
-            if (acc > 0 && acc + c > colliders) {
-                start.push_back(k);
-                acc = 0;
+            if (c > colliders) {
+                close(k);
+                big.push_back(uint32_t(start.size() - 1));
+                start.push_back(k + 1);
+                bigMax = std::max(bigMax, c);
+                continue;
             }
+            if (acc > 0 && acc + c > colliders) close(k);
             acc += c;
         }
-        start.push_back(nWorlds);
-        nTeams = uint32_t(start.size() - 1);
-        std::vector<uint32_t> ord(nTeams);
-        for (uint32_t t = 0; t < nTeams; t++) ord[t] = t;
+        close(nWorlds);
         auto size = [&](uint32_t t) { return hColStart[start[t + 1]] - hColStart[start[t]]; };
-        std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return size(a) > size(b); });
+        auto bySize = [&](uint32_t x, uint32_t y) { return size(x) > size(y); };
+        std::stable_sort(big.begin(), big.end(), bySize);
+        std::stable_sort(small.begin(), small.end(), bySize);
+        nTeams = uint32_t(small.size());
+        nBigTeams = uint32_t(big.size());
+        bigBodyCap = std::min<uint32_t>(MAX_TEAM_BODY_CAP, bigMax);
+        bigBlocks = 1;
+        if (nBigTeams) {
+            CK(team_solver_blocks_per_sm(BIG_TEAM_THREADS, bigBodyCap, &perSm));
+            bigBlocks = uint32_t(std::max(1, perSm) * dev.sms);
+        }
+        std::vector<uint32_t> order(small);
+        order.insert(order.end(), big.begin(), big.end());   // small teams, then big teams
         teamWorld.upload(start.data(), start.size(), stream);
-        teamOrder.upload(ord.data(), ord.size(), stream);
+        teamOrder.upload(order.data(), std::max<size_t>(order.size(), 1), stream);
         CK(cudaStreamSynchronize(stream));
     }
 
@@ -434,7 +457,7 @@ struct ag2d_world {
         worldBodyStart.upload(bodyStart.data(), bodyStart.size(), s);
         worldColStart.upload(colStart.data(), colStart.size(), s);
         manSeg.reserve(nWorlds + 1);
-        nextWorld.reserve(1);
+        nextWorld.reserve(2);
         setTeams(teamColliders, teamThreads);
         worldDirty.reserve(nWorlds);
         CK(cudaMemsetAsync(worldDirty.p, 0, sizeof(uint32_t) * nWorlds, s));
@@ -455,6 +478,9 @@ struct ag2d_world {
             if (e[1]) cudaEventDestroy(e[1]);
         }
         if (hCounters) cudaFreeHost(hCounters);
+        if (forkEvent) cudaEventDestroy(forkEvent);
+        if (joinEvent) cudaEventDestroy(joinEvent);
+        if (sideStream) cudaStreamDestroy(sideStream);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -483,6 +509,9 @@ struct ag2d_world {
         CK(cudaSetDevice(settings.device));
         dev = probe_device(settings.device);
         CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&sideStream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&forkEvent, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&joinEvent, cudaEventDisableTiming));
         CK(cudaMallocHost(reinterpret_cast<void**>(&hCounters), sizeof(StepCounters)));
         std::memset(hCounters, 0, sizeof(StepCounters));
         dCounters.reserve(1);
@@ -933,14 +962,29 @@ struct ag2d_world {
         pbegin(10);
         if (nWorlds > 1) {
             // One CTA per world over the world-grouped manifold list.
-            CK(cudaMemsetAsync(nextWorld.p, 0, sizeof(uint32_t), s));
+            CK(cudaMemsetAsync(nextWorld.p, 0, 2 * sizeof(uint32_t), s));
             k_manifold_segments<<<gridFor(manifoldCap), 256, 0, s>>>(mm, nm, cbody.p, bodyWorld.p, nWorlds,
                                                                       manSeg.p);
             scratch.prio = prio.p;
-            const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(nTeams, teamBlocks));
-            const TeamLaunch args{w, mm, manSeg.p, teamWorld.p, teamOrder.p, nTeams, teamBodyCap, scratch, vi, pi,
-                                  nextWorld.p, ctr};
-            CK(launch_color_solve_teams(teamThreads, grid, s, args));
+            if (nBigTeams) {
+                // Worlds larger than a team: their own wide CTAs on the side stream, overlapping the small teams.
+                CK(cudaEventRecord(forkEvent, s));
+                CK(cudaStreamWaitEvent(sideStream, forkEvent, 0));
+                const TeamLaunch big{w, mm, manSeg.p, teamWorld.p, teamOrder.p + nTeams, nBigTeams, bigBodyCap,
+                                     scratch, vi, pi, nextWorld.p + 1, ctr};
+                CK(launch_color_solve_teams(BIG_TEAM_THREADS, std::min(nBigTeams, bigBlocks), sideStream, big));
+                launches++;
+            }
+            if (nTeams) {
+                const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(nTeams, teamBlocks));
+                const TeamLaunch args{w, mm, manSeg.p, teamWorld.p, teamOrder.p, nTeams, teamBodyCap, scratch, vi,
+                                      pi, nextWorld.p, ctr};
+                CK(launch_color_solve_teams(teamThreads, grid, s, args));
+            }
+            if (nBigTeams) {
+                CK(cudaEventRecord(joinEvent, sideStream));
+                CK(cudaStreamWaitEvent(s, joinEvent, 0));
+            }
             launches++;
         } else if (lastManifolds <= GRID_SOLVE_THRESHOLD && dev.solveCluster > 1) {
             // One thread-block cluster, hardware barriers between colours.
@@ -1052,8 +1096,8 @@ struct ag2d_world {
         out.solve_ms = 0.0f;
         if (nWorlds > 1) {
             // (colliders per team, threads per CTA), packed as colliders << 16 | threads.
-            const auto r = pick(10, {512u << 16 | 128, 1024u << 16 | 128, 1024u << 16 | 256, 2048u << 16 | 256,
-                                     2048u << 16 | 512, 4096u << 16 | 256, 4096u << 16 | 512},
+            const auto r = pick(10, {256u << 16 | 64, 512u << 16 | 64, 512u << 16 | 128, 1024u << 16 | 128,
+                                     1024u << 16 | 256, 2048u << 16 | 256, 2048u << 16 | 512},
                                 [&](uint32_t t) { setTeams(t >> 16, t & 0xFFFF); });
             out.team_colliders = r.first >> 16;
             out.team_threads = r.first & 0xFFFF;
