@@ -115,6 +115,7 @@ enum ag2d_field {
     AG2D_BODY_ANGULAR_VELOCITY, AG2D_BODY_ROT_COS, AG2D_BODY_ROT_SIN, AG2D_BODY_WRAP_COUNT, AG2D_BODY_SLEEP_TIMER,
     AG2D_BODY_STATE /* uint32: 0 static, 1 sleeping, 2 dynamic */, AG2D_BODY_SLEEP_ISLAND,
     AG2D_BODY_POSE /* float32 x, y, rotation per body: one read of the pose array (a renderer's frame) */,
+    AG2D_BODY_INV_MASS, AG2D_BODY_INV_INERTIA,
     AG2D_COL_WORLD_X = 32, AG2D_COL_WORLD_Y, AG2D_COL_WORLD_ROTATION, AG2D_COL_WORLD_COS, AG2D_COL_WORLD_SIN,
     AG2D_COL_AABB_MIN_X, AG2D_COL_AABB_MIN_Y, AG2D_COL_AABB_MAX_X, AG2D_COL_AABB_MAX_Y,
     AG2D_DYN_SORTED = 64,   /* dynamic tree: collider indices in Morton order */

@@ -25,7 +25,8 @@ ERR_INVALID_ARG, ERR_OOM, ERR_CAPACITY, ERR_TIMEOUT, ERR_CUDA, ERR_NO_DEVICE, ER
 
 # enum ag2d_field
 BODY_COM_X, BODY_COM_Y, BODY_VEL_X, BODY_VEL_Y, BODY_ROTATION, BODY_ANGULAR_VELOCITY, BODY_ROT_COS, BODY_ROT_SIN, \
-    BODY_WRAP_COUNT, BODY_SLEEP_TIMER, BODY_STATE, BODY_SLEEP_ISLAND, BODY_POSE = range(1, 14)
+    BODY_WRAP_COUNT, BODY_SLEEP_TIMER, BODY_STATE, BODY_SLEEP_ISLAND, BODY_POSE, BODY_INV_MASS, \
+    BODY_INV_INERTIA = range(1, 16)
 COL_WORLD_X, COL_WORLD_Y, COL_WORLD_ROTATION, COL_WORLD_COS, COL_WORLD_SIN, COL_AABB_MIN_X, COL_AABB_MIN_Y, \
     COL_AABB_MAX_X, COL_AABB_MAX_Y = range(32, 41)
 DYN_SORTED, DYN_MORTON, PAIRS, MANIFOLDS, PREV_MANIFOLDS, SOLVE_ORDER, COLOR_STARTS = range(64, 71)

@@ -1545,6 +1545,8 @@ static std::vector<uint8_t> read_field(ag2d_world& w, int32_t field)
         return pack(o);
     }
     case AG2D_BODY_SLEEP_ISLAND: return pack(download(w.sleepIsland.p, nb, s));
+    case AG2D_BODY_INV_MASS: return comp4(w.bvel, nb, 3);
+    case AG2D_BODY_INV_INERTIA: return comp4(w.bpos, nb, 3);
     case AG2D_BODY_POSE: {
         const auto v = download(w.bpos.p, nb, s);
         std::vector<float> o(size_t(nb) * 3);
@@ -1808,7 +1810,8 @@ int32_t ag2d_batch_read(ag2d_batch* batch, uint32_t world, int32_t field, void* 
             slice(4, b0, b1);
             uint32_t* v = reinterpret_cast<uint32_t*>(out.data());
             for (uint32_t i = 0; i < b1 - b0; i++) if (v[i] != 0xFFFFFFFFu) v[i] -= b0;
-        } else if (field >= AG2D_BODY_COM_X && field < AG2D_BODY_POSE) {
+        } else if ((field >= AG2D_BODY_COM_X && field < AG2D_BODY_POSE) || field == AG2D_BODY_INV_MASS ||
+                   field == AG2D_BODY_INV_INERTIA) {
             slice(4, b0, b1);
         } else if (field >= AG2D_COL_WORLD_X && field < AG2D_DYN_SORTED) {
             slice(4, c0, c1);
