@@ -64,6 +64,8 @@ typedef struct ag2d_counters {
     uint32_t slept;         /* bodies put to sleep */
     uint32_t warm_hits;     /* manifolds warm-started */
     uint32_t sleeping;      /* bodies sleeping after the step */
+    uint32_t ccd_hits;      /* bodies moved back by continuous collision detection in the last step */
+    uint32_t reserved;
     uint64_t steps;         /* steps taken by this world */
     uint64_t launches;      /* kernel launches issued by this world so far */
     uint64_t list_rebuilds; /* work-list rebuilds after sleep/wake changes */
@@ -77,7 +79,7 @@ typedef struct ag2d_counters {
 enum ag2d_timed_phase {
     AG2D_T_INTEGRATE = 0, AG2D_T_POSE, AG2D_T_TREE_DYNAMIC, AG2D_T_TREE_OTHER, AG2D_T_QUERY, AG2D_T_NARROW,
     AG2D_T_COMPACT, AG2D_T_WARM, AG2D_T_WAKE, AG2D_T_COLOR, AG2D_T_SOLVE, AG2D_T_ISLANDS, AG2D_T_SORT,
-    AG2D_T_LBVH, AG2D_T_COUNT
+    AG2D_T_LBVH, AG2D_T_CCD, AG2D_T_COUNT
 };
 
 /* Launch shapes chosen by ag2d_world_autotune. */
@@ -106,6 +108,10 @@ typedef struct ag2d_state_desc {
     const float* poly_vertices;          /* xy pairs, concatenated */
     const float* poly_normals;           /* xy pairs, concatenated */
     const float* materials;              /* [n_materials][3]: elasticity, static friction, dynamic friction */
+    /* Optional (NULL: computed by the next spatial pass): each collider's world pose and AABB as the state holds
+     * them (ColliderSoA worldPos / worldRotationCos / Sin, aabbMin / Max). */
+    const float *col_world_x, *col_world_y, *col_world_cos, *col_world_sin;
+    const float *col_aabb_min_x, *col_aabb_min_y, *col_aabb_max_x, *col_aabb_max_y;
 } ag2d_state_desc;
 
 /* Readable / writable world fields (ag2d_world_read / ag2d_world_write). Body and collider arrays are float32 or
@@ -146,6 +152,8 @@ enum ag2d_phase {
     AG2D_PHASE_SOLVE,              /* colouring + solver on AG2D_MANIFOLDS */
     AG2D_PHASE_ISLANDS,            /* islands + sleep flags from AG2D_MANIFOLDS */
     AG2D_PHASE_COLLIDE,            /* collision detection alone: dynamic poses + AABBs, broad, narrow (no warm start) */
+    AG2D_PHASE_CCD,                /* continuous collision: sweep fast dynamic colliders against static ones, move
+                                      hit bodies back (uses the poses AG2D_PHASE_INTEGRATE recorded) */
 };
 
 /* ---- library ---- */

@@ -82,7 +82,7 @@ struct SimulationSettings {
     uint32_t collisionVelocitySolvingIterations = 6;
     uint32_t collisionPositionSolvingIterations = 3;
     IntegratorSettings integratorSettings;
-    bool continuousCollisionEnabled = false;   // the reference defaults to true; this library has no CCD yet
+    bool continuousCollisionEnabled = true;
     Real sleepSpeedThreshold = Real(0.1);
     Real sleepTimeThreshold = Real(0.5);
     int device = 0;                            // CUDA device ordinal

@@ -467,6 +467,11 @@ extern "C"
         s.wakeHeldBodies();
         s.setDataViewers();
 
+        const bool ccd = s.simulationSettings.continuousCollisionEnabled;
+        if (ccd) {
+            s.continuousCollisionDetector.settings = s.simulationSettings.ccdSettings;
+            s.continuousCollisionDetector.snapshotPoses(s.objectManager.bodies, s.objectManager.colliders);
+        }
         s.integrateAndApplyConstraints(dt);
         const IndexRange dynamicRange = s.objectManager.bodies.range(BodyGroup::Dynamic);
         wrapBodyRotations(s.objectManager.bodies, dynamicRange);
@@ -479,6 +484,24 @@ extern "C"
         uint32_t dirtyFlag = wasDirty ? 1u : 0u;
         h->put("sp.spatialDirty", &dirtyFlag, 1);
         dumpColliders(h, "sp.");
+        // Continuous collision as physicsStep runs it (Simulation.cpp:299-316): tap "ccd." after the move-back.
+        if (ccd) {
+            const auto* staticTreePtr = s.broadPhaseCollisionDetector.getTree(BroadPhaseInternal::BvhTreeType::Static);
+            uint32_t hit = 0;
+            if (staticTreePtr) {
+                hit = s.continuousCollisionDetector.resolve(s.objectManager.bodies, s.objectManager.colliders,
+                                                            s.objectManager.circles, s.objectManager.boxes,
+                                                            s.objectManager.polygons, s.objectManager.capsules,
+                                                            *staticTreePtr) ? 1u : 0u;
+                if (hit) {
+                    s.buildColliderAABBs(false);
+                    s.broadPhaseCollisionDetector.refitTrees(BroadPhaseInternal::BvhTreeTypeFlag::Dynamic);
+                }
+            }
+            h->put("ccd.hit", &hit, 1);
+            dumpBodies(h, "ccd.");
+            dumpColliders(h, "ccd.");
+        }
         dumpTree(h, "dyn.", BroadPhaseInternal::BvhTreeType::Dynamic);
         dumpTree(h, "static.", BroadPhaseInternal::BvhTreeType::Static);
         dumpTree(h, "sleep.", BroadPhaseInternal::BvhTreeType::Sleeping);

@@ -32,7 +32,7 @@ COL_WORLD_X, COL_WORLD_Y, COL_WORLD_ROTATION, COL_WORLD_COS, COL_WORLD_SIN, COL_
 DYN_SORTED, DYN_MORTON, PAIRS, MANIFOLDS, PREV_MANIFOLDS, SOLVE_ORDER, COLOR_STARTS = range(64, 71)
 # enum ag2d_phase
 PHASE_INTEGRATE, PHASE_SPATIAL_FULL, PHASE_SPATIAL_DYNAMIC, PHASE_BROAD, PHASE_NARROW, PHASE_SOLVE, \
-    PHASE_ISLANDS, PHASE_COLLIDE = range(1, 9)
+    PHASE_ISLANDS, PHASE_COLLIDE, PHASE_CCD = range(1, 10)
 
 MANIFOLD_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("nx", "<f4"), ("ny", "<f4"), ("depth", "<f4"),
                            ("count", "<u4"), ("id0", "<u4"), ("id1", "<u4"), ("px0", "<f4"), ("py0", "<f4"),
@@ -70,7 +70,8 @@ assert _BODY_DESC_DTYPE.itemsize == ctypes.sizeof(BodyDesc)
 class Counters(ctypes.Structure):
     _fields_ = [("status", ctypes.c_uint32), ("pairs", ctypes.c_uint32), ("manifolds", ctypes.c_uint32),
                 ("colors", ctypes.c_uint32), ("woke", ctypes.c_uint32), ("slept", ctypes.c_uint32),
-                ("warm_hits", ctypes.c_uint32), ("sleeping", ctypes.c_uint32), ("steps", ctypes.c_uint64),
+                ("warm_hits", ctypes.c_uint32), ("sleeping", ctypes.c_uint32), ("ccd_hits", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("steps", ctypes.c_uint64),
                 ("launches", ctypes.c_uint64), ("list_rebuilds", ctypes.c_uint64), ("retries", ctypes.c_uint64),
                 ("regrows", ctypes.c_uint64), ("host_ms", ctypes.c_double), ("sync_ms", ctypes.c_double)]
 
@@ -82,7 +83,7 @@ class Tuning(ctypes.Structure):
 
 
 TIMED_PHASES = ("integrate", "pose", "tree_dynamic", "tree_other", "query", "narrow", "compact", "warm", "wake",
-                "color", "solve", "islands", "sort", "lbvh")
+                "color", "solve", "islands", "sort", "lbvh", "ccd")
 
 
 _P = ctypes.c_void_p
@@ -96,7 +97,9 @@ class StateDesc(ctypes.Structure):
                                   "bound_radius", "sleep_timer", "sleep_island", "col_body", "col_shape_type",
                                   "col_shape_index", "col_material", "col_com_offset_x", "col_com_offset_y",
                                   "col_local_rotation", "circle_radius", "box_half_width", "box_half_height",
-                                  "poly_count", "poly_vertices", "poly_normals", "materials")]
+                                  "poly_count", "poly_vertices", "poly_normals", "materials", "col_world_x",
+                                  "col_world_y", "col_world_cos", "col_world_sin", "col_aabb_min_x",
+                                  "col_aabb_min_y", "col_aabb_max_x", "col_aabb_max_y")]
 
 
 def _load():
@@ -262,7 +265,7 @@ class World:
                                          handles.ctypes.data))
         return handles[:n]
 
-    def load_state(self, state: dict, prefix: str = "", materials=None, body_prefix=None):
+    def load_state(self, state: dict, prefix: str = "", materials=None, body_prefix=None, with_poses=False):
         """Replaces the world by a reference-layout state dict ("body.comX", "col.bodyIndex", ...)."""
         bp = prefix if body_prefix is None else body_prefix
 
@@ -291,6 +294,14 @@ class World:
         mats = np.ascontiguousarray(np.asarray(materials if materials is not None else [(1.0, 0.0, 0.0)],
                                                dtype=np.float32).reshape(-1, 3))
         arrays["materials"] = mats
+        # Collider poses and AABBs as the state holds them, when it does (all four of a kind or none).
+        for keys, names in ((("col.worldPosX", "col.worldPosY", "col.worldRotationCos", "col.worldRotationSin"),
+                             ("col_world_x", "col_world_y", "col_world_cos", "col_world_sin")),
+                            (("col.aabbMinX", "col.aabbMinY", "col.aabbMaxX", "col.aabbMaxY"),
+                             ("col_aabb_min_x", "col_aabb_min_y", "col_aabb_max_x", "col_aabb_max_y"))):
+            if with_poses and all(prefix + k in state for k in keys):
+                for k, name in zip(keys, names):
+                    arrays[name] = np.ascontiguousarray(np.asarray(state[prefix + k]), dtype=f)
         d = StateDesc()
         d.n_bodies = arrays["com_x"].size
         d.n_colliders = arrays["col_body"].size

@@ -65,6 +65,12 @@ __global__ void k_query_stash(TreeView dyn, TreeView other, const uint32_t* cbod
 __global__ void k_query_emit(TreeView dyn, TreeView other, const uint32_t* cbody, const uint32_t* counts,
                              const uint32_t* offsets, const uint2* stash, uint2* pairs, uint32_t pairCap,
                              uint32_t* status);
+__global__ void k_ccd_sweep(DeviceWorld w, const uint32_t* dynCol, uint32_t n, TreeView other, const float4* prevPos,
+                            const float4* prevPose, const float* minExtent, uint32_t* hitTime, uint32_t* status);
+__global__ void k_ccd_shift_colliders(DeviceWorld w, const uint32_t* dynCol, uint32_t n, const float4* prevPos,
+                                      const uint32_t* hitTime);
+__global__ void k_ccd_shift_bodies(DeviceWorld w, const uint32_t* dynBody, uint32_t n, const float4* prevPos,
+                                   uint32_t* hitTime, StepCounters* counters);
 __global__ void k_scan_blocks(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* blockSums);
 __global__ void k_scan_add(uint32_t* out, uint32_t n, const uint32_t* blockOffsets);
 __global__ void k_scan_total(const uint32_t* in, const uint32_t* out, uint32_t n, uint32_t* total);

@@ -38,7 +38,8 @@ struct StepCounters {
     uint32_t topoDirty;       // a body changed state: rebuild work lists before the next step
     uint32_t warmHits;        // manifolds that took warm-start impulses
     uint32_t barrierRounds;   // colouring rounds
-    uint32_t pad[7];
+    uint32_t ccdHits;         // bodies moved back by continuous collision detection
+    uint32_t pad[6];
 };
 
 // Manifold record (64 bytes), NarrowPhaseCollisionDetector.h:26-61 minus the handle union: colliders are stable

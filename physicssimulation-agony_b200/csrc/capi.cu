@@ -171,6 +171,12 @@ struct DeviceInfo {
     int solveCluster = 0;      // CTAs per cluster of the cluster solver (16 when the device allows it)
 };
 
+// glibc fmin / fmax (the reference's std::fmin / std::fmax on x86-64): the first argument unless the comparison
+// fails or the second is NaN.
+inline float host_fmin(float a, float b) { return (a < b || b != b) ? a : b; }
+inline float host_fmax(float a, float b) { return (a > b || b != b) ? a : b; }
+constexpr uint32_t ORDERED_ONE = 0xBF800000u;   // 1.0f in the order-preserving map of float_to_ordered
+
 // One world's state in the upload format (host arrays), and the warm-start manifolds.
 struct PackedArrays {
     std::vector<float4> vel, pos, co, mats;
@@ -286,6 +292,9 @@ struct ag2d_world {
     DBuf<uint32_t> cbody, cshape, cmat;
     DBuf<float4> coff, cpose, caabb;
     DBuf<float> cworldRot;
+    DBuf<float> minExtent;      // continuous collision: min extent per collider
+    DBuf<float4> prevPose;      // continuous collision: collider world poses before integration
+    DBuf<uint32_t> ccdHit;      // continuous collision: earliest time of impact per body (ordered float, 1 = none)
     DBuf<float> circleRadius;
     DBuf<float2> boxHalf, polyVerts, polyNormals;
     DBuf<uint32_t> polyOffset, polyCount;
@@ -334,7 +343,7 @@ struct ag2d_world {
     Scanner scanner;
 
     // Per-phase device timers (CUDA events on the world's stream) and the count of kernel launches.
-    static constexpr int NPHASE = 14;
+    static constexpr int NPHASE = 15;
     bool profiling = false;
     cudaEvent_t ev[NPHASE][2] = {};
     bool evPending[NPHASE] = {};
@@ -638,6 +647,31 @@ struct ag2d_world {
         polyOffset.upload(po.data(), po.size(), s); polyCount.upload(pc.data(), pc.size(), s);
         polyVerts.upload(pv.data(), pv.size(), s); polyNormals.upload(pn.data(), pn.size(), s);
         materials.upload(mats.data(), mats.size(), s);
+        // Min extent of each collider about its origin (ObjectManager.cpp setColliderExtents calls: circle radius,
+        // min box half extent, polygon in-radius PhysicsGeometry::calculatePolygonInnerRadius), for continuous
+        // collision detection.
+        {
+            std::vector<float> me(nColliders);
+            for (uint32_t i = 0; i < nColliders; i++) {
+                const uint32_t type = cs[i] >> 30, si = cs[i] & 0x3FFFFFFFu;
+                if (type == SHAPE_CIRCLE) {
+                    me[i] = cr[si];
+                } else if (type == SHAPE_BOX) {
+                    me[i] = host_fmin(bh[si].x, bh[si].y);
+                } else {
+                    float r = FLT_MAX;
+                    for (uint32_t k = 0; k < pc[si]; k++) {
+                        const float2 n = pn[po[si] + k], v = pv[po[si] + k];
+                        r = host_fmin(r, n.x * v.x + n.y * v.y);
+                    }
+                    me[i] = host_fmax(r, 0.0f);
+                }
+            }
+            minExtent.upload(me.data(), me.size(), s);
+            const std::vector<uint32_t> ones(std::max<uint32_t>(nBodies, 1), ORDERED_ONE);
+            ccdHit.upload(ones.data(), ones.size(), s);
+            prevPose.reserve(nColliders);
+        }
         nStatic = uint32_t(std::count(state.begin(), state.end(), uint8_t(STATE_STATIC)));
         const uint32_t nmax = std::max(nBodies, nColliders);
         for (auto* b : {&dynBody, &dynCol, &otherCol, &flagA, &flagB, &flagC, &offA, &offB, &offC}) b->reserve(nmax);
@@ -864,6 +898,32 @@ struct ag2d_world {
             CK(cudaGetLastError());
         }
         if (isDyn) pend(13);
+    }
+
+    // Continuous collision detection after the dynamic poses (Simulation.cpp:299-316): sweep fast dynamic colliders
+    // against the static colliders of their world, move hit bodies and their colliders back to the time of impact.
+    void phaseCcd()
+    {
+        const cudaStream_t s = stream;
+        if (nDynCol == 0 || nDynBody == 0) return;
+        if (otherDirty) {
+            pbegin(3);
+            buildTree(otherTree, otherCol.p, nOther);
+            pend(3);
+            otherDirty = false;
+        }
+        otherTree.n = int(nOther);
+        if (nOther == 0) return;
+        pbegin(14);
+        const DeviceWorld w = view();
+        k_ccd_sweep<<<gridFor(nDynCol), 256, 0, s>>>(w, dynCol.p, nDynCol, otherTree.view(), snapPos.p, prevPose.p,
+                                                     minExtent.p, ccdHit.p, &dCounters.p->status);
+        k_ccd_shift_colliders<<<gridFor(nDynCol), 256, 0, s>>>(w, dynCol.p, nDynCol, snapPos.p, ccdHit.p);
+        k_ccd_shift_bodies<<<gridFor(nDynBody), 256, 0, s>>>(w, dynBody.p, nDynBody, snapPos.p, ccdHit.p,
+                                                             dCounters.p);
+        CK(cudaGetLastError());
+        pend(14);
+        launches += 3;
     }
 
     void phaseBroad()
@@ -1129,11 +1189,14 @@ struct ag2d_world {
             const cudaStream_t s = stream;
             CK(cudaMemsetAsync(dCounters.p, 0, sizeof(StepCounters), s));
             snapshot(false);
+            if (settings.ccd && nColliders)
+                CK(cudaMemcpyAsync(prevPose.p, cpose.p, sizeof(float4) * nColliders, cudaMemcpyDeviceToDevice, s));
             const bool fullPoseThisStep = fullPose;
             const bool otherDirtyThisStep = otherDirty;
             CK(cudaMemsetAsync(wrapCount.p, 0, sizeof(float) * std::max<uint32_t>(nBodies, 1), s));   // preUpdate
             phaseIntegrate();
             phasePose(fullPose);
+            if (settings.ccd) phaseCcd();
             phaseBroad();
             phaseNarrow();
             phaseWake();
@@ -1218,7 +1281,6 @@ int32_t ag2d_world_create(const ag2d_world_settings* settings, ag2d_world** out_
     return guarded([&] {
         if (!settings || !out_world) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
         if (!(settings->dt > 0.0f)) throw ApiError(AG2D_ERR_INVALID_ARG, "dt must be > 0");
-        if (settings->ccd) throw ApiError(AG2D_ERR_UNSUPPORTED, "continuous collision detection is not available");
         std::unique_ptr<ag2d_world> w(new ag2d_world());
         w->init(*settings);
         *out_world = w.release();
@@ -1402,6 +1464,21 @@ int32_t ag2d_world_load_state(ag2d_world* world, const ag2d_state_desc* st)
         for (uint32_t i = 0; i < st->n_materials; i++)
             mats[i] = make_float4(st->materials[3 * i], st->materials[3 * i + 1], st->materials[3 * i + 2], 0.0f);
         w.uploadArrays(vel, pos, rot, wc, br, tm, state, isl, cb, cs, cm, co, cr, bh, po, pc, pv, pn, mats);
+        if (st->col_world_x && st->col_world_y && st->col_world_cos && st->col_world_sin) {
+            std::vector<float4> pose(nc);
+            for (uint32_t i = 0; i < nc; i++)
+                pose[i] = make_float4(st->col_world_x[i], st->col_world_y[i], st->col_world_cos[i], st->col_world_sin[i]);
+            if (nc) CK(cudaMemcpyAsync(w.cpose.p, pose.data(), nc * sizeof(float4), cudaMemcpyHostToDevice, w.stream));
+            CK(cudaStreamSynchronize(w.stream));
+        }
+        if (st->col_aabb_min_x && st->col_aabb_min_y && st->col_aabb_max_x && st->col_aabb_max_y) {
+            std::vector<float4> box(nc);
+            for (uint32_t i = 0; i < nc; i++)
+                box[i] = make_float4(st->col_aabb_min_x[i], st->col_aabb_min_y[i], st->col_aabb_max_x[i],
+                                     st->col_aabb_max_y[i]);
+            if (nc) CK(cudaMemcpyAsync(w.caabb.p, box.data(), nc * sizeof(float4), cudaMemcpyHostToDevice, w.stream));
+            CK(cudaStreamSynchronize(w.stream));
+        }
         // The loaded state replaces any host-created objects.
         w.objects.bodies.clear();
         w.objects.colliders.clear();
@@ -1428,6 +1505,8 @@ int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out)
         out->status = c.status; out->pairs = c.pairs; out->manifolds = c.manifolds; out->colors = c.colors;
         out->woke = c.woke; out->slept = c.slept; out->warm_hits = c.warmHits;
         out->sleeping = world->nBodies - world->nDynBody - world->nStatic;
+        out->ccd_hits = c.ccdHits;
+        out->reserved = 0;
         out->steps = world->stepsTaken;
         out->launches = world->launches;
         out->list_rebuilds = world->listRebuilds;
@@ -1669,7 +1748,15 @@ int32_t ag2d_world_run_phase(ag2d_world* world, int32_t phase)
         switch (phase) {
         case AG2D_PHASE_INTEGRATE:
             CK(cudaMemsetAsync(w.wrapCount.p, 0, sizeof(float) * std::max<uint32_t>(w.nBodies, 1), w.stream));
+            w.snapshot(false);   // the pre-integration poses continuous collision sweeps from
+            if (w.nColliders)
+                CK(cudaMemcpyAsync(w.prevPose.p, w.cpose.p, sizeof(float4) * w.nColliders, cudaMemcpyDeviceToDevice,
+                                   w.stream));
             w.phaseIntegrate();
+            break;
+        case AG2D_PHASE_CCD:
+            CK(cudaMemsetAsync(w.dCounters.p, 0, sizeof(StepCounters), w.stream));
+            w.phaseCcd();
             break;
         case AG2D_PHASE_SPATIAL_FULL: w.phasePose(true); break;
         case AG2D_PHASE_SPATIAL_DYNAMIC: w.phasePose(false); break;

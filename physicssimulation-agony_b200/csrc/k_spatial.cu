@@ -1,6 +1,7 @@
 // Spatial phase kernels: integration, collider poses + AABBs, Morton keys, onesweep radix sort, Karras LBVH build
 // and refit, and the candidate-pair query. Reference routines cited per kernel (paths relative to
 // PhysicsSimulation-Agony/PS_AGONY2D/).
+#include "ag2d_ccd.cuh"
 #include "ag2d_kernels.cuh"
 
 namespace ag2d {
@@ -639,6 +640,145 @@ __global__ void k_query_emit(TreeView dyn, TreeView other, const uint32_t* __res
                       status);
         }
     }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Continuous collision (ContinuousCollisionDetector::processShapeRange / resolve, ContinuousCollisionDetector.cpp:
+// 303-531). Per dynamic collider: skip unless both the body and the collider moved more than fastFactor x min
+// extent this step; sweep the core circle's AABB through the static colliders of its world's static + sleeping
+// tree (sleeping ones are skipped: the reference sweeps the static tree only); keep the earliest time of impact per
+// body. 'prevPos' holds each body's (x, y) and 'prevPose' each collider's world pose from before integration.
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ float ccd_cast_core(const DeviceWorld& w, uint32_t c, V2 start, V2 d, float dd,
+                                               float coreRadius, float best)
+{
+    const float4 pose = w.cpose[c];
+    const float cs = pose.z, sn = pose.w;
+    const float rx = start.x - pose.x, ry = start.y - pose.y;
+    const V2 q0 = v2(cs * rx + sn * ry, cs * ry - sn * rx);
+    const V2 dl = v2(cs * d.x + sn * d.y, cs * d.y - sn * d.x);
+    const uint32_t packed = w.cshape[c];
+    const uint32_t si = shape_index(packed);
+    switch (shape_type(packed)) {
+    case SHAPE_CIRCLE: return ccd_cast_circle(q0.x, q0.y, dl.x, dl.y, dd, w.circleRadius[si] + coreRadius, best);
+    case SHAPE_BOX: {
+        const float2 h = w.boxHalf[si];
+        return ccd_cast_box(q0, dl, dd, h.x, h.y, coreRadius, best);
+    }
+    default: {
+        const uint32_t off = w.polyOffset[si];
+        return ccd_cast_polygon(q0, dl, dd, w.polyVerts + off, w.polyNormals + off, w.polyCount[si], coreRadius, best);
+    }
+    }
+}
+
+__global__ void k_ccd_sweep(DeviceWorld w, const uint32_t* __restrict__ dynCol, uint32_t n, TreeView other,
+                            const float4* __restrict__ prevPos, const float4* __restrict__ prevPose,
+                            const float* __restrict__ minExtent, uint32_t* __restrict__ hitTime,
+                            uint32_t* __restrict__ status)
+{
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t c = dynCol[k];
+        const uint32_t body = w.cbody[c];
+        const float4 com = w.bpos[body], pcom = prevPos[body];
+        const float bodyDx = com.x - pcom.x, bodyDy = com.y - pcom.y;
+        const float bodyDeltaSq = bodyDx * bodyDx + bodyDy * bodyDy;
+        if (bodyDeltaSq <= CCD_MIN_DISPLACEMENT_SQ) continue;
+        const float me = minExtent[c];
+        if (me <= 0.0f) continue;
+        const float threshold = CCD_FAST_FACTOR * me;
+        const float thresholdSq = threshold * threshold;
+        if (bodyDeltaSq <= thresholdSq) continue;
+        const float4 pp = prevPose[c], cp = w.cpose[c];
+        const V2 start = v2(pp.x, pp.y), end = v2(cp.x, cp.y);
+        const V2 d = end - start;
+        const float dd = dot(d, d);
+        if (dd <= thresholdSq) continue;
+        const float coreRadius = CCD_CORE_FRACTION * me;
+        const float4 sweep = make_float4(rfminf(start.x, end.x) - coreRadius, rfminf(start.y, end.y) - coreRadius,
+                                         rfmaxf(start.x, end.x) + coreRadius, rfmaxf(start.y, end.y) + coreRadius);
+        // This collider's world segment of the static + sleeping tree.
+        int lo = 0, hi = other.n;
+        if (other.segStart) {
+            const uint32_t wd = w.colWorld[c];
+            lo = int(other.segStart[wd]);
+            hi = int(other.segStart[wd + 1]);
+        }
+        float best = 1.0f;
+        auto leaf = [&](int j) {
+            const float4 b = other.leafAabb[j];
+            if (!(sweep.x < b.z && sweep.z > b.x && sweep.y < b.w && sweep.w > b.y)) return;
+            const uint32_t sc = other.vals[j];
+            if (w.bstate[w.cbody[sc]] != STATE_STATIC) return;
+            best = rfminf(best, ccd_cast_core(w, sc, start, d, dd, coreRadius, best));
+        };
+        if (hi - lo == 1) {
+            leaf(lo);
+        } else if (hi - lo > 1) {
+            int stack[QUERY_STACK];
+            int sp = 0;
+            stack[sp++] = lo;
+            while (sp > 0) {
+                const int node = stack[--sp];
+                const float4 nb = other.nodeAabb[node];
+                if (nb.z < sweep.x || nb.x > sweep.z || nb.w < sweep.y || nb.y > sweep.w) continue;
+                const int2 ch = other.child[node];
+#pragma unroll
+                for (int side = 0; side < 2; side++) {
+                    const int x = side == 0 ? ch.x : ch.y;
+                    if (x < 0) leaf(~x);
+                    else if (sp < QUERY_STACK) stack[sp++] = x;
+                    else atomicOr(status, STATUS_STACK_OVERFLOW);
+                }
+            }
+        }
+        if (best < 1.0f) atomicMin(hitTime + body, float_to_ordered(best));
+    }
+}
+
+// Colliders of hit bodies move back with their body (worldPos += shift) and get their AABB rebuilt from the moved
+// pose (resolve, ContinuousCollisionDetector.cpp:495-512, then buildColliderAABBs). Runs before the bodies move.
+__global__ void k_ccd_shift_colliders(DeviceWorld w, const uint32_t* __restrict__ dynCol, uint32_t n,
+                                      const float4* __restrict__ prevPos, const uint32_t* __restrict__ hitTime)
+{
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t c = dynCol[k];
+        const uint32_t body = w.cbody[c];
+        const float t = ordered_to_float(hitTime[body]);
+        if (!(t < 1.0f)) continue;
+        const float back = t - 1.0f;
+        const float4 com = w.bpos[body], pcom = prevPos[body];
+        const float shiftX = (com.x - pcom.x) * back, shiftY = (com.y - pcom.y) * back;
+        float4 p = w.cpose[c];
+        p.x += shiftX;
+        p.y += shiftY;
+        w.cpose[c] = p;
+        w.caabb[c] = collider_aabb(w, c, p.x, p.y, p.z, p.w);
+    }
+}
+
+// Hit bodies move back along their displacement to the time of impact; the hit time returns to 1.
+__global__ void k_ccd_shift_bodies(DeviceWorld w, const uint32_t* __restrict__ dynBody, uint32_t n,
+                                   const float4* __restrict__ prevPos, uint32_t* __restrict__ hitTime,
+                                   StepCounters* counters)
+{
+    uint32_t moved = 0;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t body = dynBody[k];
+        const float t = ordered_to_float(hitTime[body]);
+        if (!(t < 1.0f)) continue;
+        const float back = t - 1.0f;
+        float4 com = w.bpos[body];
+        const float4 pcom = prevPos[body];
+        const float shiftX = (com.x - pcom.x) * back, shiftY = (com.y - pcom.y) * back;
+        com.x += shiftX;
+        com.y += shiftY;
+        w.bpos[body] = com;
+        hitTime[body] = float_to_ordered(1.0f);
+        moved++;
+    }
+    for (int o = 16; o > 0; o >>= 1) moved += __shfl_xor_sync(0xffffffffu, moved, o);
+    if ((threadIdx.x & 31) == 0 && moved) atomicAdd(&counters->ccdHits, moved);
 }
 
 // ---------------------------------------------------------------------------------------------------------------

@@ -14,6 +14,7 @@ Fixtures:
     cossin_edge.npz         FastCosSin over edge angles (quadrant boundaries, values just below 2 pi)
     wrap_edge.npz           body rotations around wrap boundaries (SIMD body and scalar tail)
     traj_c1_n256.npz        600-step trajectory statistics of a 256-polygon scene
+    c5_ccd_hit.npz          the first continuous-collision hit of a serving-style request (fast circles)
 """
 from __future__ import annotations
 
@@ -130,6 +131,29 @@ def trajectory_fixture(path, n=256, steps=600):
           f"sleeping {stats['sleeping'][-1]}")
 
 
+def ccd_fixture(path, max_steps=80):
+    """First step with a continuous-collision hit in a serving-style request (c1 mix + 5% fast circles at 200 m/s,
+    continuous collision on): the state entering the step, the spatial tap and the state after the move-back."""
+    scene = scenes.make_c5_request(np.random.default_rng(3), 0, lo=200, hi=300)
+    r = refapi.RefSim(scene, ccd=True)
+    for step in range(max_steps):
+        r.phase_step()
+        if int(r.blob("ccd.hit").view(np.uint32)[0]):
+            break
+    else:
+        raise RuntimeError("no continuous-collision hit")
+    keep = {k: v for k, v in r.blobs().items() if k.startswith(("pre.", "sp.", "ccd."))
+            and not k.endswith(tuple(x for x in DROP_SUFFIXES if x != ".minExtent"))}
+    keep["meta.dt"] = np.array([scene.dt], np.float32)
+    keep["meta.gravity"] = np.array(scene.gravity, np.float32)
+    keep["meta.iters"] = np.array([scene.velocity_iterations, scene.position_iterations], np.uint32)
+    keep["meta.materials"] = np.array([(1.0, 0.0, 0.0)] + list(scene.materials), np.float32)
+    keep["meta.step"] = np.array([step], np.uint32)
+    np.savez_compressed(path, **keep)
+    r.close()
+    print(f"{os.path.basename(path)}: step {step}, {scene.n} bodies")
+
+
 def main():
     if not refapi.available():
         sys.exit("oracle/_ref/libagony_ref.so missing: run oracle/ref_build.sh first")
@@ -139,6 +163,7 @@ def main():
     cossin_fixture(os.path.join(HERE, "cossin_edge.npz"))
     wrap_fixture(os.path.join(HERE, "wrap_edge.npz"))
     trajectory_fixture(os.path.join(HERE, "traj_c1_n256.npz"))
+    ccd_fixture(os.path.join(HERE, "c5_ccd_hit.npz"))
 
 
 if __name__ == "__main__":
