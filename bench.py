@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Throughput of the collision/contact pipeline on B200, in body-steps/s.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c4|c2|c3]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c4|c2|c3|c5]
 
 Workloads (seeded synthetic scenes, ag2d.scenes):
   c4 (default)  4,096 independent worlds, body counts log-uniform in [16, 2048] (c1 mix: 3-8-gons on a ground box),
@@ -11,6 +11,10 @@ Workloads (seeded synthetic scenes, ag2d.scenes):
   c3            1,000,000 circles and 4-6-gons: collision detection alone (poses, AABBs, Morton, sort, LBVH,
                 query, SAT), reported as broad+narrow GB/s against the HBM roofline, with the exact pair count
                 checked against the oracle's sweep.
+  c5            serving: requests arrive as a Poisson stream (lambda 2,000/s), each a world of log-uniform
+                [32, 8192] bodies (c1 mix, 5% small fast circles, continuous collision detection on) asking for 120
+                steps, admitted against a 120 GB budget into one resident batch (ag2d.Server); a fixed-length run of
+                --requests arrivals, reporting aggregate body-steps/s and p50 / p99 completion latency.
 
 One process per GPU (torchrun for N > 1). Worlds exchange nothing on the step path, so each rank advances its own
 batch (rank r's worlds are seeded r * worlds + k): weak scaling with no collective in the step; the whole-job value
@@ -52,8 +56,10 @@ WORKLOADS = {
           "dt 1/60, 8 velocity + 3 position iterations, stepped from the drop",
     "c3": "c3: 1M bodies (50% circles, 50% 4-6-gons, size log-uniform 0.1-2 m) uniform in 4000 x 4000 m, "
           "v ~ N(0, 5 m/s); collision detection alone (poses, AABBs, Morton, sort, LBVH, query, SAT)",
+    "c5": "c5: serving, Poisson arrivals at 2000 req/s, each a world of log-uniform [32, 8192] bodies (c1 mix, 5% "
+          "circles r 0.05 m at 200 m/s, CCD on) for 120 steps, 120 GB admission budget, continuous batching",
 }
-DEFAULT_STEPS = {"c4": 600, "c2": 1000, "c3": 20}
+DEFAULT_STEPS = {"c4": 600, "c2": 1000, "c3": 20, "c5": 120}
 BODY_UPLOAD_BYTES = 16 + 16 + 8 + 4 + 4 + 4 + 1 + 4 + 4 + 4 + 4 + 16   # body + collider records as uploaded
 
 
@@ -69,6 +75,12 @@ def parse():
     ap.add_argument("--per-world-sample", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--requests", type=int, default=4000, help="c5 arrivals in the timed run")
+    ap.add_argument("--rate", type=float, default=2000.0, help="c5 Poisson arrival rate, requests/s")
+    ap.add_argument("--budget-gb", type=float, default=120.0, help="c5 admission budget")
+    ap.add_argument("--round-steps", type=int, default=8, help="c5 steps between admission rounds")
+    ap.add_argument("--reserve-bodies", type=int, default=4_000_000,
+                    help="c5 resident bodies the server sizes its batch for at start-up")
     a = ap.parse_args()
     if a.steps is None:
         a.steps = DEFAULT_STEPS[a.workload]
@@ -95,6 +107,16 @@ def host_threads():
 def c4_scenes(worlds, seed):
     from ag2d import scenes
     return scenes.make_c4_worlds(worlds=worlds, seed=seed, processes=max(1, min(32, host_threads())))
+
+
+def c5_requests(count, seed):
+    from ag2d import scenes
+    return scenes.make_c5_requests(count, seed=seed, processes=max(1, min(32, host_threads())))
+
+
+def poisson_arrivals(count, rate, seed):
+    import numpy as np
+    return np.cumsum(np.random.default_rng(seed ^ 0xA221).exponential(1.0 / rate, count))
 
 
 def c2_scene(n):
@@ -274,9 +296,9 @@ def reduce_sum(torch, dist, world_size, dev, value):
 # ---------------------------------------------------------------------------------------------------------------
 # CPU baselines: the reference engine (oracle/_ref) on the host cores
 # ---------------------------------------------------------------------------------------------------------------
-def cpu_worlds_rate(scene_list, seconds, threads):
+def cpu_worlds_rate(scene_list, seconds, threads, max_steps=600, ccd=False):
     """Reference Simulation objects, one world per task, over a pool of host threads (ctypes releases the GIL).
-    Each task creates its world and steps it in chunks of 10 until 600 steps or the time budget; body-steps/s."""
+    Each task creates its world and steps it in chunks of 10 until max_steps or the time budget; body-steps/s."""
     from oracle import refapi
     work = queue.Queue()
     for sc in scene_list:
@@ -291,9 +313,9 @@ def cpu_worlds_rate(scene_list, seconds, threads):
                 sc = work.get_nowait()
             except queue.Empty:
                 return
-            sim = refapi.RefSim(sc, threads=0)
+            sim = refapi.RefSim(sc, threads=0, ccd=ccd)
             steps = 0
-            while time.perf_counter() < deadline and steps < 600:
+            while time.perf_counter() < deadline and steps < max_steps:
                 sim.update(10)
                 steps += 10
             sim.close()
@@ -396,6 +418,18 @@ def run_reference(args):
             sample += f"; stopped after {budget:.0f} s of {args.steps} requested steps"
         line = dict(base, value=value, steps=steps, ms_per_step=1e3 * elapsed / max(steps, 1),
                     config={"workload": WORKLOADS["c2"], "bodies": scene.n})
+    elif args.workload == "c5":
+        # The reference serves a request by stepping its own Simulation: requests are served by a pool of host
+        # threads, one single-threaded Simulation each, 120 steps, over a bounded sample of the stream.
+        scene_list = c5_requests(min(args.requests, 512), 0)
+        threads = host_threads()
+        seconds = min(budget, 30.0)
+        value = cpu_worlds_rate(scene_list, seconds, threads, max_steps=args.steps, ccd=True)
+        sample = (f"the first {len(scene_list)} requests of the stream, one single-threaded Simulation each (CCD "
+                  f"on), {threads} at a time, {args.steps} steps each, {seconds:.0f} s of serving")
+        line = dict(base, value=value, steps=args.steps, ms_per_step=None,
+                    config={"workload": WORKLOADS["c5"], "requests": len(scene_list),
+                            "note": "throughput of the host pool; arrivals are not replayed on the host"})
     else:
         scene = c3_scene(args.bodies)
         r = cpu_c3(scene, max(1, min(args.steps, 5)))
@@ -682,6 +716,109 @@ def run_c3(args, torch, dist, rank, world_size, local, dev):
     }
 
 
+def run_c5(args, torch, dist, rank, world_size, local, dev):
+    """Serving: arrivals replayed on a wall clock by a submitter thread; the server admits, steps and retires the
+    requests on its own host thread. Worlds are built on the host before the run (request construction is the
+    client's work); each submit copies the world's arrays into the request. Every rank serves its own stream."""
+    import ag2d
+    import numpy as np
+    n_req = args.requests
+    scene_list = c5_requests(n_req, rank * 1_000_003)
+    warm_list = c5_requests(32, rank * 1_000_003 + 777)
+    arrivals = poisson_arrivals(n_req, args.rate, rank)
+    settings = dict(dt=scene_list[0].dt, velocity_iterations=8, position_iterations=3,
+                    gravity=scene_list[0].gravity, ccd=True, device=local)
+
+    def build(lst):
+        out = []
+        for sc in lst:
+            w = ag2d.World(**settings)
+            w.add_scene(sc)
+            out.append(w)
+        return out
+    worlds, warm = build(scene_list), build(warm_list)
+    server = ag2d.Server(memory_budget_bytes=int(args.budget_gb * (1 << 30)), steps_per_round=args.round_steps,
+                         reserve_bodies=args.reserve_bodies, **settings)
+    # Warm-up: a burst of requests through the same server (allocations, first launches).
+    for w in warm:
+        server.submit(w, args.steps)
+    server.wait_all(600_000)
+    s0 = server.stats()
+    if world_size > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ids = [0] * n_req
+    lag = [0.0]
+
+    def submitter():
+        t_start = time.perf_counter()
+        for k in range(n_req):
+            delay = arrivals[k] - (time.perf_counter() - t_start)
+            if delay > 0:
+                time.sleep(delay)
+            else:
+                lag[0] = max(lag[0], -delay)
+            ids[k] = server.submit(worlds[k], args.steps)
+    t0 = time.perf_counter()
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    server.wait_all(1_800_000)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    s1 = server.stats()
+    lat = np.array([server.poll(i)[1] for i in ids])
+    bodies = int(sum(sc.n for sc in scene_list))
+    body_steps = bodies * args.steps
+    max_wall = reduce_max(torch, dist, world_size, dev, wall)
+    job = reduce_sum(torch, dist, world_size, dev, float(body_steps))
+    value = job / max_wall
+    p50, p99 = float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+    served_rate = n_req / wall
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
+        from oracle import refapi
+        if refapi.available():
+            sample = scene_list[:512]
+            threads = host_threads()
+            v = cpu_worlds_rate(sample, args.cpu_seconds, threads, max_steps=args.steps, ccd=True)
+            cpu = {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
+                   "sample": f"reference engine (oracle/_ref), the first {len(sample)} requests, one single-threaded "
+                             f"Simulation each with CCD, {threads} at a time, {args.steps} steps each, "
+                             f"{args.cpu_seconds:.0f} s of serving"}
+    req_bytes = upload_bytes(scene_list) / n_req
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world_size, "steps": args.steps,
+        "warmup": len(warm), "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32", "data": "synthetic (seeded request generator, ag2d.scenes.make_c5_requests)",
+        "config": {"workload": WORKLOADS["c5"], "requests_per_gpu": n_req, "bodies_per_gpu": bodies,
+                   "rate_per_s": args.rate, "budget_gb": args.budget_gb, "round_steps": args.round_steps,
+                   "reserve_bodies": args.reserve_bodies,
+                   "parallelism": f"one server per GPU x{world_size} (no collective)",
+                   "timing": "wall clock from the first arrival to the last completion (arrivals follow a wall "
+                             "clock); warm-up: a burst of 32 requests through the same server",
+                   "l2": "inputs larger than L2 (the resident batch)"},
+        "latency_ms": {"p50": p50, "p99": p99, "max": float(lat.max()), "mean": float(lat.mean())},
+        "serving": {"offered_body_steps_per_s": args.rate * bodies * args.steps / n_req,
+                    "served_requests_per_s": served_rate, "rounds": s1["rounds"] - s0["rounds"],
+                    "peak_resident": s1["peak_resident"], "server_busy_ms": s1["busy_ms"] - s0["busy_ms"],
+                    "server_step_ms": s1["step_ms"] - s0["step_ms"], "server_repack_ms": s1["repack_ms"] - s0["repack_ms"],
+                    "submit_lag_ms": 1e3 * lag[0]},
+        "roofline": None,
+        "roofline_note": "per-kernel roofline is reported on the c4 and c3 lines; this line measures serving",
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_request": req_bytes,
+                "d2h_bytes_per_request": 36.0 * bodies / n_req,
+                "note": "the serving run is end to end: host worlds in, host results out"},
+        "clocks": clocks,
+    }
+    server.close()
+    return line
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -692,7 +829,7 @@ def run_ours(args):
         dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
     dev = torch.device(f"cuda:{local}")
-    fn = {"c4": run_c4, "c2": run_c2, "c3": run_c3}[args.workload]
+    fn = {"c4": run_c4, "c2": run_c2, "c3": run_c3, "c5": run_c5}[args.workload]
     line = fn(args, torch, dist, rank, world_size, local, dev)
     if rank == 0:
         print(json.dumps(line))

@@ -240,6 +240,45 @@ int32_t ag2d_batch_read(ag2d_batch* batch, uint32_t world, int32_t field, void* 
                         uint64_t* out_bytes);
 int32_t ag2d_batch_destroy(ag2d_batch* batch);
 
+/* ---- request server: world rollouts served from one resident, continuously repacked batch ----
+ * No counterpart in the reference (it steps one Simulation per caller). A server owns one device batch and a host
+ * thread. Submitted requests (a world built with the ag2d_world_add_* calls, and a step count) wait in arrival
+ * order until the resident set has room under the device-memory budget (an estimate per request) and the world
+ * limit; between rounds of steps, finished requests leave and waiting ones join, the batch being rebuilt on the
+ * device. Each resident world advances exactly its requested number of steps, and its result is the one it gets
+ * stepped alone. Latency is measured from submission to the moment the result is stored. */
+typedef struct ag2d_server ag2d_server;
+typedef struct ag2d_server_settings {
+    ag2d_world_settings world;      /* step settings every request must share */
+    uint64_t memory_budget_bytes;   /* device memory the resident requests may take (estimated per request) */
+    uint32_t steps_per_round;       /* steps between admission / retirement rounds (at most; 0: 8) */
+    uint32_t max_worlds;            /* resident requests at most (0: no limit) */
+    uint32_t reserve_bodies;        /* size the device batch for this many resident bodies at creation (0: grow) */
+    uint32_t reserved;
+} ag2d_server_settings;
+typedef struct ag2d_server_stats {
+    uint64_t submitted, completed, waiting, resident;
+    uint64_t peak_resident;          /* most requests resident at once */
+    uint64_t rounds, body_steps;     /* rounds run, sum of bodies x steps of completed requests */
+    double busy_ms;                  /* host time the loop spent on rounds with resident worlds */
+    double step_ms, repack_ms;       /* of which: stepping, and retiring + repacking the batch */
+    double p50_ms, p99_ms, max_ms;   /* completion latency of the completed requests */
+} ag2d_server_stats;
+enum ag2d_request_state { AG2D_REQUEST_WAITING = 0, AG2D_REQUEST_RUNNING = 1, AG2D_REQUEST_DONE = 2 };
+
+int32_t ag2d_server_create(const ag2d_server_settings* settings, ag2d_server** out_server);
+/* Copies the world's bodies into a new request; the world itself is not modified or kept. */
+int32_t ag2d_server_submit(ag2d_server* server, ag2d_world* world, uint32_t steps, uint64_t* out_request);
+int32_t ag2d_server_poll(ag2d_server* server, uint64_t request, int32_t* out_state, double* out_latency_ms);
+/* Blocks until every submitted request is done (or the loop failed); timeout_ms < 0 waits without limit. */
+int32_t ag2d_server_wait_all(ag2d_server* server, double timeout_ms);
+/* A body field of a finished request (AG2D_BODY_COM_X/Y, ROTATION, VEL_X/Y, ANGULAR_VELOCITY, POSE, STATE). */
+int32_t ag2d_server_read(ag2d_server* server, uint64_t request, int32_t field, void* dst, uint64_t capacity_bytes,
+                         uint64_t* out_bytes);
+int32_t ag2d_server_release(ag2d_server* server, uint64_t request);
+int32_t ag2d_server_stats_get(ag2d_server* server, ag2d_server_stats* out_stats);
+int32_t ag2d_server_destroy(ag2d_server* server);
+
 /* ---- allocation-free solve: no counterpart in the reference (its solver allocates freely on the host) ----
  * Colours and solves n_manifolds manifolds in place on caller-owned device arrays: body velocities and poses are
  * updated and the manifolds' impulses written back, as AG2D_PHASE_SOLVE does for a world. The call makes no device

@@ -86,6 +86,20 @@ TIMED_PHASES = ("integrate", "pose", "tree_dynamic", "tree_other", "query", "nar
                 "color", "solve", "islands", "sort", "lbvh", "ccd")
 
 
+class ServerSettings(ctypes.Structure):
+    _fields_ = [("world", WorldSettings), ("memory_budget_bytes", ctypes.c_uint64),
+                ("steps_per_round", ctypes.c_uint32), ("max_worlds", ctypes.c_uint32),
+                ("reserve_bodies", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("submitted", "completed", "waiting", "resident",
+                                               "peak_resident", "rounds", "body_steps")] + \
+               [(n, ctypes.c_double) for n in ("busy_ms", "step_ms", "repack_ms", "p50_ms", "p99_ms", "max_ms")]
+
+
+REQUEST_WAITING, REQUEST_RUNNING, REQUEST_DONE = 0, 1, 2
+
 _P = ctypes.c_void_p
 
 
@@ -138,6 +152,14 @@ def _load():
     L.ag2d_batch_world_count.argtypes = [vp, ctypes.POINTER(u32)]
     L.ag2d_batch_read.argtypes = [vp, u32, i32, vp, u64, ctypes.POINTER(u64)]
     L.ag2d_batch_destroy.argtypes = [vp]
+    L.ag2d_server_create.argtypes = [ctypes.POINTER(ServerSettings), ctypes.POINTER(vp)]
+    L.ag2d_server_submit.argtypes = [vp, vp, u32, ctypes.POINTER(u64)]
+    L.ag2d_server_poll.argtypes = [vp, u64, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)]
+    L.ag2d_server_wait_all.argtypes = [vp, ctypes.c_double]
+    L.ag2d_server_read.argtypes = [vp, u64, i32, vp, u64, ctypes.POINTER(u64)]
+    L.ag2d_server_release.argtypes = [vp, u64]
+    L.ag2d_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats)]
+    L.ag2d_server_destroy.argtypes = [vp]
     return L
 
 
@@ -412,6 +434,66 @@ class Batch:
             if getattr(self, "engine", None) is not None:
                 self.engine.h = None
             lib.ag2d_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching request server: submitted worlds wait in arrival order, join the resident batch while
+    their estimated device memory fits the budget, advance together in rounds of up to `steps_per_round` steps and
+    leave with their final body state once their requested steps are done. Every request's result equals the same
+    world stepped alone."""
+
+    def __init__(self, memory_budget_bytes=8 << 30, steps_per_round=8, max_worlds=0, reserve_bodies=0, dt=1.0 / 60.0,
+                 velocity_iterations=8, position_iterations=3, gravity=(0.0, -9.81), angular_damping=1.0,
+                 sleep_speed=0.1, sleep_time=0.5, ccd=False, device=0):
+        w = WorldSettings(dt, velocity_iterations, position_iterations, gravity[0], gravity[1], angular_damping,
+                          sleep_speed, sleep_time, 1 if ccd else 0, device)
+        s = ServerSettings(w, memory_budget_bytes, steps_per_round, max_worlds, reserve_bodies, 0)
+        h = ctypes.c_void_p()
+        _check(lib.ag2d_server_create(ctypes.byref(s), ctypes.byref(h)))
+        self.h = h
+
+    def submit(self, world: World, steps: int) -> int:
+        """Queues a copy of the world's current state for `steps` steps; returns the request id."""
+        r = ctypes.c_uint64()
+        _check(lib.ag2d_server_submit(self.h, world.h, steps, ctypes.byref(r)))
+        return int(r.value)
+
+    def poll(self, request: int):
+        """(state, latency_ms): REQUEST_WAITING / RUNNING / DONE; the latency once done, else -1."""
+        st, lat = ctypes.c_int32(), ctypes.c_double()
+        _check(lib.ag2d_server_poll(self.h, request, ctypes.byref(st), ctypes.byref(lat)))
+        return int(st.value), float(lat.value)
+
+    def wait_all(self, timeout_ms: float = -1.0):
+        _check(lib.ag2d_server_wait_all(self.h, timeout_ms))
+
+    def read(self, request: int, field: int) -> np.ndarray:
+        """A body field of a finished request (positions, rotation, velocities, pose or state)."""
+        n = ctypes.c_uint64()
+        _check(lib.ag2d_server_read(self.h, request, field, None, 0, ctypes.byref(n)))
+        buf = np.empty(int(n.value), dtype=np.uint8)
+        _check(lib.ag2d_server_read(self.h, request, field, buf.ctypes.data if buf.size else None, buf.size,
+                                    ctypes.byref(n)))
+        return buf.view(np.uint32 if field in _U32_FIELDS else np.float32)
+
+    def release(self, request: int):
+        _check(lib.ag2d_server_release(self.h, request))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib.ag2d_server_stats_get(self.h, ctypes.byref(st)))
+        return {n: getattr(st, n) for n, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.ag2d_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -197,11 +197,8 @@ def make_c4_worlds(worlds: int = 4096, seed: int = 0, lo: int = 16, hi: int = 20
     return [_c4_world(j) for j in jobs]
 
 
-def make_c5_request(rng: np.random.Generator, request_id: int, lo: int = 32, hi: int = 8192) -> Scene:
-    """Serving request: a world of log-uniform [lo, hi] bodies in the c1 mix, of which 5% are small fast
-    circles (r = 0.05 m) moving at 200 m/s towards the ground (continuous collision detection exercise)."""
-    count = int(log_uniform_counts(rng, 1, lo, hi)[0])
-    seed = int(rng.integers(0, 2**31 - 1))
+def _c5_world(args):
+    request_id, count, seed = args
     scale = math.sqrt(count / 2048.0)
     base = make_c1(count, seed, width=max(20.0, 200.0 * scale), height=max(10.0, 100.0 * scale))
     r2 = np.random.default_rng(seed ^ 0x5EED)
@@ -217,3 +214,26 @@ def make_c5_request(rng: np.random.Generator, request_id: int, lo: int = 32, hi:
         base.poly_count[i] = 0
     base.name = f"c5_req{request_id}_n{count}"
     return base
+
+
+def make_c5_request(rng: np.random.Generator, request_id: int, lo: int = 32, hi: int = 8192) -> Scene:
+    """Serving request: a world of log-uniform [lo, hi] bodies in the c1 mix, of which 5% are small fast
+    circles (r = 0.05 m) moving at 200 m/s towards the ground (continuous collision detection exercise)."""
+    count = int(log_uniform_counts(rng, 1, lo, hi)[0])
+    seed = int(rng.integers(0, 2**31 - 1))
+    return _c5_world((request_id, count, seed))
+
+
+def make_c5_requests(requests: int, seed: int = 0, lo: int = 32, hi: int = 8192, processes: int = 1) -> list:
+    """The first `requests` worlds of the serving stream with this seed (make_c5_request in order); processes > 1
+    builds them in a spawned process pool (the same worlds)."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for k in range(requests):
+        count = int(log_uniform_counts(rng, 1, lo, hi)[0])
+        jobs.append((k, count, int(rng.integers(0, 2**31 - 1))))
+    if processes > 1 and requests > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(processes) as pool:
+            return pool.map(_c5_world, jobs, chunksize=max(1, requests // (4 * processes)))
+    return [_c5_world(j) for j in jobs]

@@ -99,4 +99,22 @@ __global__ void k_state_flags(const uint8_t* bstate, const uint32_t* cbody, uint
                               uint32_t* bodyDyn, uint32_t* colDyn, uint32_t* colOther);
 __global__ void k_scatter_list(const uint32_t* flag, const uint32_t* offset, uint32_t n, uint32_t* list);
 
+// Batch repacking (k_repack.cu). A segment copies 'count' elements from [src, ...) of the current array (fromNew
+// 0), or from the staged section of joining world 'src' (fromNew 1), to [dst, ...) of the new array; the deltas
+// shift the indices stored in the elements (new start - source start of that kind of element in the segment's
+// world; a staged world's indices start at 0).
+struct GatherSeg {
+    uint32_t dst, src, count, fromNew;
+    int32_t dBody, dCol, dCircle, dBox, dPoly, dVert, dMat, pad;
+};
+enum GatherMode : uint32_t {
+    GATHER_PLAIN = 0, GATHER_ISLAND, GATHER_BODY, GATHER_SHAPE, GATHER_MATERIAL, GATHER_VERTEX
+};
+template <class T>
+cudaError_t launch_gather(T* dst, const T* srcOld, const T* srcNew, const GatherSeg* segs, uint32_t nsegs,
+                          uint32_t total, uint32_t mode, uint32_t grid, cudaStream_t stream,
+                          const unsigned long long* sections, uint32_t nsec, uint32_t section);
+__global__ void k_world_of(const uint32_t* starts, uint32_t worlds, uint32_t n, uint32_t* out);
+__global__ void k_fill_u32(uint32_t* out, uint32_t n, uint32_t value);
+
 }  // namespace ag2d

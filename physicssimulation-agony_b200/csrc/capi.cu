@@ -11,8 +11,11 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <condition_variable>
+#include <deque>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -77,12 +80,14 @@ struct DBuf {
         p = nullptr;
         n = 0;
     }
-    // Grows to at least 'count' elements; contents are not preserved.
+    // Grows to at least 'count' elements; contents are not preserved. A buffer that grows again takes half as much
+    // again on top, so a steadily growing size (a server batch filling up) reallocates a logarithmic number of
+    // times: fresh device memory is slow to map.
     void reserve(size_t count)
     {
         if (count <= n && p) return;
+        const size_t c = std::max<size_t>(p ? std::max(count, n + n / 2) : count, 1);
         release();
-        const size_t c = std::max<size_t>(count, 1);
         CK(cudaMalloc(reinterpret_cast<void**>(&p), c * sizeof(T)));
         n = c;
     }
@@ -177,6 +182,51 @@ inline float host_fmin(float a, float b) { return (a < b || b != b) ? a : b; }
 inline float host_fmax(float a, float b) { return (a > b || b != b) ? a : b; }
 constexpr uint32_t ORDERED_ONE = 0xBF800000u;   // 1.0f in the order-preserving map of float_to_ordered
 
+// Min extent of every collider about its origin (ObjectManager.cpp setColliderExtents calls: circle radius, min box
+// half extent, polygon in-radius PhysicsGeometry::calculatePolygonInnerRadius), for continuous collision detection.
+inline std::vector<float> min_extents(const std::vector<uint32_t>& cs, const std::vector<float>& cr,
+                                      const std::vector<float2>& bh, const std::vector<uint32_t>& po,
+                                      const std::vector<uint32_t>& pc, const std::vector<float2>& pv,
+                                      const std::vector<float2>& pn)
+{
+    std::vector<float> me(cs.size());
+    for (size_t i = 0; i < cs.size(); i++) {
+        const uint32_t type = cs[i] >> 30, si = cs[i] & 0x3FFFFFFFu;
+        if (type == SHAPE_CIRCLE) {
+            me[i] = cr[si];
+        } else if (type == SHAPE_BOX) {
+            me[i] = host_fmin(bh[si].x, bh[si].y);
+        } else {
+            float r = FLT_MAX;
+            for (uint32_t k = 0; k < pc[si]; k++) {
+                const float2 n = pn[po[si] + k], v = pv[po[si] + k];
+                r = host_fmin(r, n.x * v.x + n.y * v.y);
+            }
+            me[i] = host_fmax(r, 0.0f);
+        }
+    }
+    return me;
+}
+
+// Element counts of one resident world, per kind of array (a server engine's worlds are consecutive ranges).
+struct WorldExtent {
+    uint32_t body = 0, col = 0, circle = 0, box = 0, poly = 0, vert = 0, mat = 0, man = 0, statics = 0;
+};
+
+// A world waiting to join a server batch: all its arrays in one host blob (sections at 64-byte aligned offsets,
+// indices local to the world), copied to the device with one transfer and gathered into place there.
+enum StagedSection : uint32_t {
+    SEC_VEL, SEC_POS, SEC_ROT, SEC_WRAP, SEC_BOUND, SEC_TIMER, SEC_STATE, SEC_ISLAND,
+    SEC_CBODY, SEC_CSHAPE, SEC_CMAT, SEC_COFF, SEC_CPOSE, SEC_CAABB, SEC_CROT, SEC_MINEXT,
+    SEC_CIRCLE, SEC_BOXHALF, SEC_POLYOFF, SEC_POLYCOUNT, SEC_POLYVERTS, SEC_POLYNORMALS, SEC_MATS, SEC_PREV,
+    NSEC
+};
+struct StagedWorld {
+    WorldExtent ext;
+    std::vector<uint8_t> blob;
+    uint64_t sec[NSEC] = {};
+};
+
 // One world's state in the upload format (host arrays), and the warm-start manifolds.
 struct PackedArrays {
     std::vector<float4> vel, pos, co, mats;
@@ -185,6 +235,7 @@ struct PackedArrays {
     std::vector<uint8_t> state;
     std::vector<uint32_t> isl, cb, cs, cm, po, pc;
     std::vector<Manifold> prev;
+    std::vector<float4> cp;   // collider world poses at the end of the last step (empty: never stepped, zeros)
 
     // Appends another world, shifting its body, collider, shape, vertex and material indices past this one's.
     void append(const PackedArrays& o)
@@ -207,8 +258,62 @@ struct PackedArrays {
         for (uint32_t v : o.po) po.push_back(v + vert);
         cat(pc, o.pc); cat(pv, o.pv); cat(pn, o.pn); cat(mats, o.mats);
         for (Manifold m : o.prev) { m.a += cof; m.b += cof; prev.push_back(m); }
+        if (!o.cp.empty() || !cp.empty()) {
+            cp.resize(cof, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+            if (o.cp.empty()) cp.resize(cof + o.cb.size(), make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+            else cat(cp, o.cp);
+        }
     }
 };
+
+// Packs one world's arrays into its staging blob. Collider poses come from the world's last step (zeros for a
+// never-stepped world, as when uploaded alone); AABBs and wrapped rotations are recomputed by the joining world's
+// first full pose pass.
+StagedWorld stage_world(const PackedArrays& a)
+{
+    StagedWorld w;
+    WorldExtent& e = w.ext;
+    e.body = uint32_t(a.vel.size());
+    e.col = uint32_t(a.cb.size());
+    e.circle = uint32_t(a.cr.size());
+    e.box = uint32_t(a.bh.size());
+    e.poly = uint32_t(a.po.size());
+    e.vert = uint32_t(a.pv.size());
+    e.mat = uint32_t(a.mats.size());
+    e.man = uint32_t(a.prev.size());
+    e.statics = uint32_t(std::count(a.state.begin(), a.state.end(), uint8_t(STATE_STATIC)));
+    const std::vector<float> me = min_extents(a.cs, a.cr, a.bh, a.po, a.pc, a.pv, a.pn);
+    const size_t sizes[NSEC] = {
+        e.body * sizeof(float4), e.body * sizeof(float4), e.body * sizeof(float2), e.body * 4, e.body * 4,
+        e.body * 4, e.body, e.body * 4,
+        e.col * 4, e.col * 4, e.col * 4, e.col * sizeof(float4), e.col * sizeof(float4), e.col * sizeof(float4),
+        e.col * 4, e.col * 4,
+        e.circle * 4, e.box * sizeof(float2), e.poly * 4, e.poly * 4, e.vert * sizeof(float2), e.vert * sizeof(float2),
+        e.mat * sizeof(float4), e.man * sizeof(Manifold)};
+    uint64_t off = 0;
+    for (uint32_t k = 0; k < NSEC; k++) {
+        w.sec[k] = off;
+        off += (sizes[k] + 63) & ~uint64_t(63);
+    }
+    w.blob.assign(off, 0);   // zero sections: collider AABBs and wrapped rotations, poses of a never-stepped world
+    auto put = [&](uint32_t k, const void* src) {
+        if (sizes[k]) std::memcpy(w.blob.data() + w.sec[k], src, sizes[k]);
+    };
+    put(SEC_VEL, a.vel.data()); put(SEC_POS, a.pos.data()); put(SEC_ROT, a.rot.data()); put(SEC_WRAP, a.wc.data());
+    put(SEC_BOUND, a.br.data()); put(SEC_TIMER, a.st.data()); put(SEC_STATE, a.state.data());
+    put(SEC_ISLAND, a.isl.data());
+    put(SEC_CBODY, a.cb.data()); put(SEC_CSHAPE, a.cs.data()); put(SEC_CMAT, a.cm.data()); put(SEC_COFF, a.co.data());
+    if (a.cp.size() == e.col) put(SEC_CPOSE, a.cp.data());
+    put(SEC_MINEXT, me.data());
+    put(SEC_CIRCLE, a.cr.data()); put(SEC_BOXHALF, a.bh.data()); put(SEC_POLYOFF, a.po.data());
+    put(SEC_POLYCOUNT, a.pc.data()); put(SEC_POLYVERTS, a.pv.data()); put(SEC_POLYNORMALS, a.pn.data());
+    put(SEC_MATS, a.mats.data()); put(SEC_PREV, a.prev.data());
+    return w;
+}
+
+// Candidate pairs (and manifolds) reserved per collider up front. A settled pile of convex bodies has about two
+// candidate pairs per collider; growing later synchronises the device and can take long on first touch of memory.
+constexpr uint32_t INITIAL_PAIRS_PER_COLLIDER = 8;
 
 // Manifold count above which the solver runs on the whole grid instead of one cluster.
 constexpr uint32_t GRID_SOLVE_THRESHOLD = 600000;
@@ -335,6 +440,19 @@ struct ag2d_world {
     DBuf<uint32_t> bodyWorld, colWorld, worldBodyStart, worldColStart, manSeg, nextWorld, worldDirty;
     DBuf<uint32_t> teamWorld, teamOrder;     // solver teams: first world of each team; small then big, largest first
     DBuf<uint8_t> dynSimd, dynColSimd;               // SIMD-path flag of each work-list entry
+    // Request-server engines: extents of the resident worlds, back buffers the repack gathers into, and the
+    // staging upload of joining worlds.
+    std::vector<WorldExtent> worldExt;
+    bool manSegFresh = false;   // manSeg describes prevManifolds (a batched step ran since the last repack)
+    DBuf<float4> bk_bvel, bk_bpos, bk_coff, bk_cpose, bk_caabb, bk_mats, out_vel, out_pos;
+    DBuf<float2> bk_brot, bk_boxHalf, bk_polyVerts, bk_polyNormals;
+    DBuf<float> bk_wrap, bk_bound, bk_timer, bk_cworldRot, bk_minExt, bk_circle;
+    DBuf<uint8_t> bk_bstate, staging, out_state;
+    DBuf<uint32_t> bk_island, bk_cbody, bk_cshape, bk_cmat, bk_polyOff, bk_polyCount, newWorldMask;
+    DBuf<Manifold> bk_prev;
+    DBuf<unsigned long long> stagedSections;   // [joining world][section] byte offsets into 'staging'
+    DBuf<GatherSeg> gatherSegs;
+    bool newWorldsPending = false;   // joined worlds take a full pose pass in their first step
     // Shape table sizes of the last upload.
     uint32_t nCircles = 0, nBoxes = 0, nPolygons = 0, nPolyVerts = 0, nMaterialRows = 0;
     // Counters.
@@ -395,6 +513,269 @@ struct ag2d_world {
         w.worldColStart = seg ? worldColStart.p : nullptr;
         w.worldDirty = seg ? worldDirty.p : nullptr;
         return w;
+    }
+
+    // Per-body and per-collider work buffers for the current sizes (grow only).
+    void sizeFor()
+    {
+        snapVel.reserve(nBodies); snapPos.reserve(nBodies); snapRot.reserve(nBodies); snapWrap.reserve(nBodies);
+        snapTimer.reserve(nBodies); snapState.reserve(nBodies); snapIsland.reserve(nBodies);
+        prevPose.reserve(nColliders);
+        ccdHit.reserve(nBodies);
+        const uint32_t nmax = std::max(nBodies, nColliders);
+        for (auto* b : {&dynBody, &dynCol, &otherCol, &flagA, &flagB, &flagC, &offA, &offB, &offC}) b->reserve(nmax);
+        dynSimd.reserve(nmax);
+        dynColSimd.reserve(nmax);
+        dynTree.reserve(nColliders, nWorlds);
+        otherTree.reserve(nColliders, nWorlds);
+        qCounts.reserve(nColliders); qOffsets.reserve(nColliders);
+        qStash.reserve(size_t(std::max<uint32_t>(nColliders, 1)) * QUERY_STASH);
+        bodyMax.reserve(nBodies);
+        bodyMask.reserve(nBodies);
+        ufParent.reserve(nBodies); ufFlag.reserve(nBodies); wakeIsland.reserve(nBodies);
+        const uint32_t cap = std::max<uint32_t>(INITIAL_PAIRS_PER_COLLIDER * nColliders, 4096);
+        if (cap > pairCap || cap > manifoldCap)
+            reserveCapacities(std::max(pairCap + pairCap / 2, cap), std::max(manifoldCap + manifoldCap / 2, cap));
+        scanner.reserve(std::max({pairCap, nColliders, nBodies}));
+    }
+
+    // Rebuilds the resident batch on the device: the worlds 'keep' (indices into worldExt, in order) followed by the
+    // joining worlds 'add' (host blobs, indices local to each world). Every world's state is carried over element
+    // for element, so the worlds step on exactly as they would alone; joining worlds get their first-step full
+    // pose pass. One transfer per joining world; the gathers shift the stored indices. Returns synchronised.
+    void repack(const std::vector<uint32_t>& keep, const std::vector<const StagedWorld*>& add)
+    {
+        ensureDevice();
+        const cudaStream_t s = stream;
+        // AG2D_SERVER_LOG: per-part times of each repack on stderr (synchronising between the parts).
+        const bool log = std::getenv("AG2D_SERVER_LOG") != nullptr;
+        auto tPrev = std::chrono::steady_clock::now();
+        std::string parts;
+        auto mark = [&](const char* name) {
+            if (!log) return;
+            CK(cudaStreamSynchronize(s));
+            const auto now = std::chrono::steady_clock::now();
+            parts += std::string(" ") + name + "=" +
+                     std::to_string(std::chrono::duration<double, std::milli>(now - tPrev).count());
+            tPrev = now;
+        };
+        const uint32_t W0 = uint32_t(worldExt.size());
+        // Current extents of the warm-start manifolds.
+        if (W0 == 1) {
+            worldExt[0].man = prevCount;
+        } else if (W0 > 1 && manSegFresh) {
+            std::vector<uint32_t> seg(W0 + 1);
+            CK(cudaMemcpyAsync(seg.data(), manSeg.p, (W0 + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            for (uint32_t k = 0; k < W0; k++) worldExt[k].man = seg[k + 1] - seg[k];
+        }
+        auto prefix = [](const std::vector<WorldExtent>& ex, uint32_t WorldExtent::*f) {
+            std::vector<uint32_t> st(ex.size() + 1, 0);
+            for (size_t i = 0; i < ex.size(); i++) st[i + 1] = st[i] + ex[i].*f;
+            return st;
+        };
+        static constexpr uint32_t WorldExtent::*kinds[8] = {&WorldExtent::body, &WorldExtent::col,
+                                                            &WorldExtent::circle, &WorldExtent::box,
+                                                            &WorldExtent::poly, &WorldExtent::vert,
+                                                            &WorldExtent::mat, &WorldExtent::man};
+        std::vector<uint32_t> oldStart[8], newStart[8];
+        std::vector<WorldExtent> next;
+        for (uint32_t k : keep) next.push_back(worldExt[k]);
+        for (const StagedWorld* w : add) next.push_back(w->ext);
+        for (int c = 0; c < 8; c++) {
+            oldStart[c] = prefix(worldExt, kinds[c]);
+            newStart[c] = prefix(next, kinds[c]);
+        }
+        // Segments per kind (empty ones left out). A kept world's segment reads the current arrays from its old
+        // start; a joining world's reads its staged sections (src = its index among the joining worlds). The
+        // deltas shift the indices stored inside the elements to the new starts.
+        std::vector<GatherSeg> segs[8];
+        for (size_t j = 0; j < next.size(); j++) {
+            const bool fresh = j >= keep.size();
+            GatherSeg g{};
+            g.fromNew = fresh ? 1u : 0u;
+            int32_t d[8];
+            for (int c = 0; c < 8; c++)
+                d[c] = int32_t(newStart[c][j]) - (fresh ? 0 : int32_t(oldStart[c][keep[j]]));
+            g.dBody = d[0]; g.dCol = d[1]; g.dCircle = d[2]; g.dBox = d[3]; g.dPoly = d[4]; g.dVert = d[5];
+            g.dMat = d[6];
+            for (int c = 0; c < 8; c++) {
+                g.dst = newStart[c][j];
+                g.src = fresh ? uint32_t(j - keep.size()) : oldStart[c][keep[j]];
+                g.count = next[j].*kinds[c];
+                if (g.count) segs[c].push_back(g);
+            }
+        }
+        std::vector<GatherSeg> allSegs;
+        uint32_t segOff[9] = {0};
+        for (int c = 0; c < 8; c++) {
+            segOff[c] = uint32_t(allSegs.size());
+            allSegs.insert(allSegs.end(), segs[c].begin(), segs[c].end());
+        }
+        segOff[8] = uint32_t(allSegs.size());
+        mark("plan");
+        gatherSegs.upload(allSegs.data(), allSegs.size(), s);   // empty when every world leaves
+        // Staging: each joining world's blob at a 256-byte aligned offset, one transfer each.
+        std::vector<unsigned long long> secOff(std::max<size_t>(add.size(), 1) * NSEC, 0);
+        uint64_t stagedBytes = 0;
+        for (size_t f = 0; f < add.size(); f++) {
+            for (uint32_t k = 0; k < NSEC; k++) secOff[f * NSEC + k] = stagedBytes + add[f]->sec[k];
+            stagedBytes += (add[f]->blob.size() + 255) & ~uint64_t(255);
+        }
+        staging.reserve(std::max<uint64_t>(stagedBytes, 1));
+        uint64_t at = 0;
+        for (const StagedWorld* w : add) {
+            if (!w->blob.empty())
+                CK(cudaMemcpyAsync(staging.p + at, w->blob.data(), w->blob.size(), cudaMemcpyHostToDevice, s));
+            at += (w->blob.size() + 255) & ~uint64_t(255);
+        }
+        stagedSections.upload(secOff.data(), secOff.size(), s);
+        mark("stage");
+        // Gathers into the back buffers, then swap them in front.
+        const uint32_t grid = gridFor(std::max(newStart[0].back(), newStart[1].back()) + 1);
+        auto run = [&](auto& front, auto& back, uint32_t section, int kind, uint32_t mode) {
+            using T = std::remove_reference_t<decltype(*front.p)>;
+            const uint32_t total = newStart[kind].back();
+            // Warm-start manifolds trade places with the current-step buffer every step: keep the full capacity.
+            back.reserve(std::max<uint32_t>(kind == 7 ? std::max(total, manifoldCap) : total, 1));
+            CK(launch_gather(back.p, front.p, reinterpret_cast<const T*>(staging.p), gatherSegs.p + segOff[kind],
+                             segOff[kind + 1] - segOff[kind], total, mode, grid, s, stagedSections.p, NSEC, section));
+            swap_bufs(front, back);
+        };
+        run(bvel, bk_bvel, SEC_VEL, 0, GATHER_PLAIN);
+        run(bpos, bk_bpos, SEC_POS, 0, GATHER_PLAIN);
+        run(brot, bk_brot, SEC_ROT, 0, GATHER_PLAIN);
+        run(wrapCount, bk_wrap, SEC_WRAP, 0, GATHER_PLAIN);
+        run(boundRadius, bk_bound, SEC_BOUND, 0, GATHER_PLAIN);
+        run(sleepTimer, bk_timer, SEC_TIMER, 0, GATHER_PLAIN);
+        run(bstate, bk_bstate, SEC_STATE, 0, GATHER_PLAIN);
+        run(sleepIsland, bk_island, SEC_ISLAND, 0, GATHER_ISLAND);
+        run(cbody, bk_cbody, SEC_CBODY, 1, GATHER_BODY);
+        run(cshape, bk_cshape, SEC_CSHAPE, 1, GATHER_SHAPE);
+        run(cmat, bk_cmat, SEC_CMAT, 1, GATHER_MATERIAL);
+        run(coff, bk_coff, SEC_COFF, 1, GATHER_PLAIN);
+        run(cpose, bk_cpose, SEC_CPOSE, 1, GATHER_PLAIN);
+        run(caabb, bk_caabb, SEC_CAABB, 1, GATHER_PLAIN);
+        run(cworldRot, bk_cworldRot, SEC_CROT, 1, GATHER_PLAIN);
+        run(minExtent, bk_minExt, SEC_MINEXT, 1, GATHER_PLAIN);
+        run(circleRadius, bk_circle, SEC_CIRCLE, 2, GATHER_PLAIN);
+        run(boxHalf, bk_boxHalf, SEC_BOXHALF, 3, GATHER_PLAIN);
+        run(polyOffset, bk_polyOff, SEC_POLYOFF, 4, GATHER_VERTEX);
+        run(polyCount, bk_polyCount, SEC_POLYCOUNT, 4, GATHER_PLAIN);
+        run(polyVerts, bk_polyVerts, SEC_POLYVERTS, 5, GATHER_PLAIN);
+        run(polyNormals, bk_polyNormals, SEC_POLYNORMALS, 5, GATHER_PLAIN);
+        run(materials, bk_mats, SEC_MATS, 6, GATHER_PLAIN);
+        run(prevManifolds, bk_prev, SEC_PREV, 7, GATHER_PLAIN);
+        mark("gather");
+        // Sizes, partition and per-world state.
+        worldExt = next;
+        const uint32_t W = uint32_t(next.size());
+        nBodies = newStart[0].back();
+        nColliders = newStart[1].back();
+        nCircles = newStart[2].back(); nBoxes = newStart[3].back(); nPolygons = newStart[4].back();
+        nPolyVerts = newStart[5].back(); nMaterialRows = newStart[6].back();
+        objects.materials.assign(size_t(nMaterialRows) * 3, 0.0f);   // the material count the device view reads
+        nStatic = 0;
+        for (const WorldExtent& e : next) nStatic += e.statics;
+        prevCount = newStart[7].back();
+        CK(cudaMemcpyAsync(nPrev.p, &prevCount, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        nWorlds = std::max<uint32_t>(W, 1);
+        hBodyStart = newStart[0];
+        hColStart = newStart[1];
+        if (W == 0) { hBodyStart = {0, 0}; hColStart = {0, 0}; }
+        sizeFor();
+        mark("size");
+        const uint32_t ones = std::max<uint32_t>(nBodies, 1);
+        k_fill_u32<<<gridFor(ones), 256, 0, s>>>(ccdHit.p, ones, ORDERED_ONE);
+        if (nWorlds > 1) {
+            bodyWorld.reserve(std::max<uint32_t>(nBodies, 1));
+            colWorld.reserve(std::max<uint32_t>(nColliders, 1));
+            worldBodyStart.upload(hBodyStart.data(), hBodyStart.size(), s);
+            worldColStart.upload(hColStart.data(), hColStart.size(), s);
+            k_world_of<<<gridFor(nBodies), 256, 0, s>>>(worldBodyStart.p, nWorlds, nBodies, bodyWorld.p);
+            k_world_of<<<gridFor(nColliders), 256, 0, s>>>(worldColStart.p, nWorlds, nColliders, colWorld.p);
+            manSeg.reserve(nWorlds + 1);
+            nextWorld.reserve(2);
+            worldDirty.reserve(nWorlds);
+            CK(cudaMemsetAsync(worldDirty.p, 0, sizeof(uint32_t) * nWorlds, s));
+            setTeams(teamColliders, teamThreads);
+        }
+        // Joining worlds: a full pose pass in their first step (as a freshly uploaded world has).
+        newWorldMask.reserve(nWorlds);
+        std::vector<uint32_t> mask(nWorlds, 0u);
+        for (size_t j = keep.size(); j < next.size(); j++) mask[j] = 1u;
+        newWorldMask.upload(mask.data(), mask.size(), s);
+        newWorldsPending = next.size() > keep.size();
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s));
+        mark("partition");
+        if (log)
+            std::fprintf(stderr, "ag2d repack worlds=%zu joined=%zu bodies=%u colliders=%u ms:%s\n", next.size(),
+                         add.size(), nBodies, nColliders, parts.c_str());
+        hostDirty = false;
+        listsDirty = true;
+        otherDirty = true;
+        fullPose = false;
+        manSegFresh = false;
+        lastManifolds = prevCount;
+    }
+
+    // The final body state (velocity, pose, state) of the given resident worlds, concatenated in that order: one
+    // device gather and one transfer per field.
+    void exportBodies(const std::vector<uint32_t>& worlds, std::vector<float4>& vel, std::vector<float4>& pos,
+                      std::vector<uint8_t>& state)
+    {
+        const cudaStream_t s = stream;
+        std::vector<uint32_t> start(worldExt.size() + 1, 0);
+        for (size_t k = 0; k < worldExt.size(); k++) start[k + 1] = start[k] + worldExt[k].body;
+        std::vector<GatherSeg> segs;
+        uint32_t total = 0;
+        for (uint32_t k : worlds) {
+            GatherSeg g{};
+            g.dst = total;
+            g.src = start[k];
+            g.count = worldExt[k].body;
+            total += g.count;
+            if (g.count) segs.push_back(g);
+        }
+        vel.resize(total); pos.resize(total); state.resize(total);
+        if (!total) return;
+        gatherSegs.upload(segs.data(), segs.size(), s);
+        out_vel.reserve(total); out_pos.reserve(total); out_state.reserve(total);
+        const uint32_t grid = gridFor(total), n = uint32_t(segs.size());
+        CK(launch_gather<float4>(out_vel.p, bvel.p, nullptr, gatherSegs.p, n, total, GATHER_PLAIN, grid, s, nullptr, 0, 0));
+        CK(launch_gather<float4>(out_pos.p, bpos.p, nullptr, gatherSegs.p, n, total, GATHER_PLAIN, grid, s, nullptr, 0, 0));
+        CK(launch_gather<uint8_t>(out_state.p, bstate.p, nullptr, gatherSegs.p, n, total, GATHER_PLAIN, grid, s, nullptr,
+                                  0, 0));
+        CK(cudaMemcpyAsync(vel.data(), out_vel.p, total * sizeof(float4), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(pos.data(), out_pos.p, total * sizeof(float4), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(state.data(), out_state.p, total, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+
+    // Sizes every per-element buffer of a batch for 'bodies' resident bodies (one collider each) up front, so
+    // that a server filling up does not reallocate on the way. Only for an engine with no resident world.
+    void reserveResident(uint32_t bodies)
+    {
+        ensureDevice();
+        const uint32_t b = std::max<uint32_t>(bodies, 1), verts = 8 * b, worlds = std::max<uint32_t>(b / 16, 2);
+        auto both = [](auto& x, auto& y, size_t n) { x.reserve(n); y.reserve(n); };
+        both(bvel, bk_bvel, b); both(bpos, bk_bpos, b); both(brot, bk_brot, b); both(wrapCount, bk_wrap, b);
+        both(boundRadius, bk_bound, b); both(sleepTimer, bk_timer, b); both(bstate, bk_bstate, b);
+        both(sleepIsland, bk_island, b); both(cbody, bk_cbody, b); both(cshape, bk_cshape, b);
+        both(cmat, bk_cmat, b); both(coff, bk_coff, b); both(cpose, bk_cpose, b); both(caabb, bk_caabb, b);
+        both(cworldRot, bk_cworldRot, b); both(minExtent, bk_minExt, b); both(circleRadius, bk_circle, b);
+        both(boxHalf, bk_boxHalf, b); both(polyOffset, bk_polyOff, b); both(polyCount, bk_polyCount, b);
+        both(polyVerts, bk_polyVerts, verts); both(polyNormals, bk_polyNormals, verts); both(materials, bk_mats, worlds);
+        bodyWorld.reserve(b); colWorld.reserve(b); worldBodyStart.reserve(worlds + 1); worldColStart.reserve(worlds + 1);
+        manSeg.reserve(worlds + 1); worldDirty.reserve(worlds); newWorldMask.reserve(worlds);
+        staging.reserve(size_t(b) * 64);
+        const uint32_t saveB = nBodies, saveC = nColliders, saveW = nWorlds;
+        nBodies = b; nColliders = b; nWorlds = worlds;
+        sizeFor();
+        bk_prev.reserve(manifoldCap);
+        nBodies = saveB; nColliders = saveC; nWorlds = saveW;
+        CK(cudaStreamSynchronize(stream));
     }
 
     // Solver teams: consecutive worlds packed while the team stays within 'colliders' colliders (a larger world is
@@ -647,26 +1028,8 @@ struct ag2d_world {
         polyOffset.upload(po.data(), po.size(), s); polyCount.upload(pc.data(), pc.size(), s);
         polyVerts.upload(pv.data(), pv.size(), s); polyNormals.upload(pn.data(), pn.size(), s);
         materials.upload(mats.data(), mats.size(), s);
-        // Min extent of each collider about its origin (ObjectManager.cpp setColliderExtents calls: circle radius,
-        // min box half extent, polygon in-radius PhysicsGeometry::calculatePolygonInnerRadius), for continuous
-        // collision detection.
         {
-            std::vector<float> me(nColliders);
-            for (uint32_t i = 0; i < nColliders; i++) {
-                const uint32_t type = cs[i] >> 30, si = cs[i] & 0x3FFFFFFFu;
-                if (type == SHAPE_CIRCLE) {
-                    me[i] = cr[si];
-                } else if (type == SHAPE_BOX) {
-                    me[i] = host_fmin(bh[si].x, bh[si].y);
-                } else {
-                    float r = FLT_MAX;
-                    for (uint32_t k = 0; k < pc[si]; k++) {
-                        const float2 n = pn[po[si] + k], v = pv[po[si] + k];
-                        r = host_fmin(r, n.x * v.x + n.y * v.y);
-                    }
-                    me[i] = host_fmax(r, 0.0f);
-                }
-            }
+            const std::vector<float> me = min_extents(cs, cr, bh, po, pc, pv, pn);
             minExtent.upload(me.data(), me.size(), s);
             const std::vector<uint32_t> ones(std::max<uint32_t>(nBodies, 1), ORDERED_ONE);
             ccdHit.upload(ones.data(), ones.size(), s);
@@ -684,7 +1047,7 @@ struct ag2d_world {
         bodyMax.reserve(nBodies);
         bodyMask.reserve(nBodies);
         ufParent.reserve(nBodies); ufFlag.reserve(nBodies); wakeIsland.reserve(nBodies);
-        const uint32_t cap = std::max<uint32_t>(4 * nColliders, 4096);
+        const uint32_t cap = std::max<uint32_t>(INITIAL_PAIRS_PER_COLLIDER * nColliders, 4096);
         reserveCapacities(std::max(pairCap, cap), std::max(manifoldCap, cap));
         CK(cudaMemsetAsync(nPrev.p, 0, sizeof(uint32_t), s));
         CK(cudaMemsetAsync(nManifolds.p, 0, sizeof(uint32_t), s));
@@ -720,7 +1083,7 @@ struct ag2d_world {
         get(a.wc, wrapCount.p, nBodies); get(a.br, boundRadius.p, nBodies); get(a.st, sleepTimer.p, nBodies);
         get(a.state, bstate.p, nBodies); get(a.isl, sleepIsland.p, nBodies);
         get(a.cb, cbody.p, nColliders); get(a.cs, cshape.p, nColliders); get(a.cm, cmat.p, nColliders);
-        get(a.co, coff.p, nColliders);
+        get(a.co, coff.p, nColliders); get(a.cp, cpose.p, nColliders);
         get(a.cr, circleRadius.p, nCircles); get(a.bh, boxHalf.p, nBoxes);
         get(a.po, polyOffset.p, nPolygons); get(a.pc, polyCount.p, nPolygons);
         get(a.pv, polyVerts.p, nPolyVerts); get(a.pn, polyNormals.p, nPolyVerts);
@@ -1189,13 +1552,26 @@ struct ag2d_world {
             const cudaStream_t s = stream;
             CK(cudaMemsetAsync(dCounters.p, 0, sizeof(StepCounters), s));
             snapshot(false);
-            if (settings.ccd && nColliders)
-                CK(cudaMemcpyAsync(prevPose.p, cpose.p, sizeof(float4) * nColliders, cudaMemcpyDeviceToDevice, s));
+            if (settings.ccd && nColliders) {
+                // The poses continuous collision sweeps from; a retried step starts again from the same poses.
+                if (attempt == 0)
+                    CK(cudaMemcpyAsync(prevPose.p, cpose.p, sizeof(float4) * nColliders, cudaMemcpyDeviceToDevice, s));
+                else
+                    CK(cudaMemcpyAsync(cpose.p, prevPose.p, sizeof(float4) * nColliders, cudaMemcpyDeviceToDevice, s));
+            }
             const bool fullPoseThisStep = fullPose;
             const bool otherDirtyThisStep = otherDirty;
             CK(cudaMemsetAsync(wrapCount.p, 0, sizeof(float) * std::max<uint32_t>(nBodies, 1), s));   // preUpdate
             phaseIntegrate();
             phasePose(fullPose);
+            if (newWorldsPending && !fullPose) {
+                // Worlds that joined a server batch: their first step poses every collider, as alone.
+                const DeviceWorld wv = view();
+                k_collider_pose<<<gridFor(nColliders), 256, 0, s>>>(wv, nullptr, nullptr, nColliders,
+                                                                    nWorlds > 1 ? newWorldMask.p : nullptr);
+                CK(cudaGetLastError());
+                launches++;
+            }
             if (settings.ccd) phaseCcd();
             phaseBroad();
             phaseNarrow();
@@ -1230,6 +1606,8 @@ struct ag2d_world {
             fullPose = false;
             // The solved manifolds become the next step's warm-start source.
             swap_bufs(manifolds, prevManifolds);
+            newWorldsPending = false;
+            manSegFresh = nWorlds > 1;
             CK(cudaMemcpyAsync(nPrev.p, nManifolds.p, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
             lastManifolds = hCounters->manifolds;
             prevCount = std::min(lastManifolds, manifoldCap);
@@ -1839,6 +2217,9 @@ int32_t ag2d_batch_create(ag2d_world* const* worlds, uint32_t count, ag2d_batch*
             e.objects.materials[3 * i + 2] = all.mats[i].z;
         }
         e.setPartition(bodyStart, colStart);
+        if (!all.cp.empty())   // collider poses of stepped worlds (continuous collision detection sweeps from them)
+            CK(cudaMemcpyAsync(e.cpose.p, all.cp.data(), all.cp.size() * sizeof(float4), cudaMemcpyHostToDevice,
+                               e.stream));
         const uint32_t np = uint32_t(all.prev.size());
         if (np > e.manifoldCap) e.reserveCapacities(std::max(np, e.pairCap), np);
         if (np) CK(cudaMemcpyAsync(e.prevManifolds.p, all.prev.data(), np * sizeof(Manifold), cudaMemcpyHostToDevice,
@@ -1931,6 +2312,346 @@ int32_t ag2d_batch_destroy(ag2d_batch* batch)
     return guarded([&] {
         if (batch && batch->engine) cudaSetDevice(batch->engine->settings.device);
         delete batch;
+    });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------------------
+// Request server: one resident batch engine and a host thread that admits, steps and retires requests in rounds.
+// ---------------------------------------------------------------------------------------------------------------
+namespace {
+
+struct ServerRequest {
+    uint64_t id = 0;
+    StagedWorld staged;             // dropped once resident
+    WorldExtent ext;
+    uint64_t bytes = 0;             // device memory estimate
+    uint32_t steps = 0, done = 0;
+    int32_t state = AG2D_REQUEST_WAITING;
+    std::chrono::steady_clock::time_point submitted, finished;
+    std::vector<float4> vel, pos;   // final body state
+    std::vector<uint8_t> bstate;
+};
+
+// Device bytes a resident request may take: its arrays (front and back copies), per-step scratch and the pair /
+// manifold capacities reserved per collider (80 bytes a candidate pair, about 330 a manifold slot).
+uint64_t request_bytes(const WorldExtent& e)
+{
+    return uint64_t(e.body) * 200 + uint64_t(e.col) * (200 + INITIAL_PAIRS_PER_COLLIDER * 410) +
+           uint64_t(e.vert) * 32 + 4096;
+}
+
+}  // namespace
+
+struct ag2d_server {
+    ag2d_server_settings settings{};
+    std::unique_ptr<ag2d_world> engine;
+    std::mutex mu;
+    std::condition_variable cv, doneCv;
+    std::deque<std::shared_ptr<ServerRequest>> waiting;
+    std::vector<std::shared_ptr<ServerRequest>> resident;   // in engine world order
+    std::map<uint64_t, std::shared_ptr<ServerRequest>> requests;
+    std::thread worker;
+    bool stop = false;
+    int32_t failCode = AG2D_OK;
+    std::string failMessage;
+    uint64_t nextId = 1, submitted = 0, completed = 0, rounds = 0, bodySteps = 0, residentBytes = 0;
+    uint64_t peakResident = 0;
+    double busyMs = 0.0, stepMs = 0.0, repackMs = 0.0;
+    std::vector<double> latencies;
+
+    void loop()
+    {
+        try {
+            CK(cudaSetDevice(settings.world.device));
+            const uint32_t perRound = settings.steps_per_round ? settings.steps_per_round : 8u;
+            while (true) {
+                ag2d_world& e = *engine;
+                // Finished requests leave; their budget is free for this round's admissions.
+                std::vector<uint32_t> keep;
+                std::vector<std::shared_ptr<ServerRequest>> leaving;
+                uint64_t keptBytes = 0;
+                for (uint32_t k = 0; k < resident.size(); k++) {
+                    if (resident[k]->done >= resident[k]->steps) {
+                        leaving.push_back(resident[k]);
+                    } else {
+                        keep.push_back(k);
+                        keptBytes += resident[k]->bytes;
+                    }
+                }
+                std::vector<std::shared_ptr<ServerRequest>> join;
+                {
+                    std::unique_lock<std::mutex> lk(mu);
+                    if (stop) return;
+                    if (resident.empty() && waiting.empty()) {
+                        cv.wait_for(lk, std::chrono::milliseconds(20));
+                        continue;
+                    }
+                    // Admission in arrival order under the memory budget and the world limit (a request larger
+                    // than the whole budget still runs, alone).
+                    uint64_t bytes = keptBytes;
+                    size_t worlds = keep.size();
+                    while (!waiting.empty()) {
+                        const auto& r = waiting.front();
+                        const bool fits = bytes + r->bytes <= settings.memory_budget_bytes || worlds == 0;
+                        if (!fits || (settings.max_worlds && worlds >= settings.max_worlds)) break;
+                        bytes += r->bytes;
+                        worlds++;
+                        join.push_back(r);
+                        waiting.pop_front();
+                    }
+                }
+                const auto t0 = std::chrono::steady_clock::now();
+                if (!leaving.empty()) {
+                    // The leaving requests' final body state, in one gather and transfer per field.
+                    std::vector<uint32_t> idx;
+                    for (uint32_t k = 0; k < resident.size(); k++)
+                        if (resident[k]->done >= resident[k]->steps) idx.push_back(k);
+                    std::vector<float4> vel, pos;
+                    std::vector<uint8_t> st;
+                    e.exportBodies(idx, vel, pos, st);
+                    size_t at = 0;
+                    for (const auto& r : leaving) {
+                        const size_t nb = r->ext.body;
+                        r->vel.assign(vel.begin() + at, vel.begin() + at + nb);
+                        r->pos.assign(pos.begin() + at, pos.begin() + at + nb);
+                        r->bstate.assign(st.begin() + at, st.begin() + at + nb);
+                        at += nb;
+                    }
+                }
+                if (!leaving.empty() || !join.empty()) {
+                    std::vector<const StagedWorld*> add;
+                    for (const auto& r : join) add.push_back(&r->staged);
+                    e.repack(keep, add);
+                    std::vector<std::shared_ptr<ServerRequest>> next;
+                    for (uint32_t k : keep) next.push_back(resident[k]);
+                    for (const auto& r : join) next.push_back(r);
+                    std::lock_guard<std::mutex> lk(mu);
+                    const auto now = std::chrono::steady_clock::now();
+                    for (const auto& r : leaving) {
+                        r->state = AG2D_REQUEST_DONE;
+                        r->finished = now;
+                        completed++;
+                        bodySteps += uint64_t(r->ext.body) * r->steps;
+                        latencies.push_back(std::chrono::duration<double, std::milli>(now - r->submitted).count());
+                    }
+                    for (const auto& r : join) {
+                        r->state = AG2D_REQUEST_RUNNING;
+                        r->staged = StagedWorld();
+                    }
+                    resident = next;
+                    residentBytes = bytesOf(resident);
+                    peakResident = std::max<uint64_t>(peakResident, resident.size());
+                    doneCv.notify_all();
+                }
+                if (resident.empty()) continue;
+                // A round: as many steps as the closest request still needs, up to the round length.
+                uint32_t k = perRound;
+                for (const auto& r : resident) k = std::min(k, r->steps - r->done);
+                const auto t1 = std::chrono::steady_clock::now();
+                for (uint32_t i = 0; i < k; i++) e.stepOnce();
+                for (const auto& r : resident) r->done += k;
+                const auto t2 = std::chrono::steady_clock::now();
+                rounds++;
+                repackMs += std::chrono::duration<double, std::milli>(t1 - t0).count();
+                stepMs += std::chrono::duration<double, std::milli>(t2 - t1).count();
+                busyMs += std::chrono::duration<double, std::milli>(t2 - t0).count();
+            }
+        } catch (const ApiError& err) {
+            std::lock_guard<std::mutex> lk(mu);
+            failCode = err.code;
+            failMessage = err.what();
+        } catch (const std::exception& err) {
+            std::lock_guard<std::mutex> lk(mu);
+            failCode = AG2D_ERR_CUDA;
+            failMessage = err.what();
+        }
+        doneCv.notify_all();
+    }
+
+    static uint64_t bytesOf(const std::vector<std::shared_ptr<ServerRequest>>& v)
+    {
+        uint64_t b = 0;
+        for (const auto& r : v) b += r->bytes;
+        return b;
+    }
+
+    void checkFailed()
+    {
+        if (failCode != AG2D_OK) throw ApiError(failCode, "server loop stopped: " + failMessage);
+    }
+};
+
+extern "C" {
+
+int32_t ag2d_server_create(const ag2d_server_settings* settings, ag2d_server** out)
+{
+    return guarded([&] {
+        if (!settings || !out) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        if (!(settings->world.dt > 0.0f)) throw ApiError(AG2D_ERR_INVALID_ARG, "dt must be > 0");
+        std::unique_ptr<ag2d_server> sv(new ag2d_server());
+        sv->settings = *settings;
+        sv->engine.reset(new ag2d_world());
+        sv->engine->init(settings->world);
+        sv->engine->hostDirty = false;
+        sv->engine->ensureDevice();
+        if (settings->reserve_bodies) sv->engine->reserveResident(settings->reserve_bodies);
+        ag2d_server* p = sv.get();
+        sv->worker = std::thread([p] { p->loop(); });
+        *out = sv.release();
+    });
+}
+
+int32_t ag2d_server_submit(ag2d_server* server, ag2d_world* world, uint32_t steps, uint64_t* out_request)
+{
+    return guarded([&] {
+        if (!server || !world) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        if (!same_settings(world->settings, server->settings.world))
+            throw ApiError(AG2D_ERR_INVALID_ARG, "the request's world settings differ from the server's");
+        auto r = std::make_shared<ServerRequest>();
+        {
+            // Packed on the caller's thread: the server loop only copies the blob to the device.
+            PackedArrays a;
+            world->exportArrays(a);
+            r->staged = stage_world(a);
+        }
+        r->ext = r->staged.ext;
+        r->bytes = request_bytes(r->ext);
+        r->steps = steps;
+        r->submitted = std::chrono::steady_clock::now();
+        std::lock_guard<std::mutex> lk(server->mu);
+        server->checkFailed();
+        r->id = server->nextId++;
+        server->requests[r->id] = r;
+        server->waiting.push_back(r);
+        server->submitted++;
+        if (out_request) *out_request = r->id;
+        server->cv.notify_all();
+    });
+}
+
+int32_t ag2d_server_poll(ag2d_server* server, uint64_t request, int32_t* out_state, double* out_latency_ms)
+{
+    return guarded([&] {
+        if (!server) throw ApiError(AG2D_ERR_INVALID_ARG, "null server");
+        std::lock_guard<std::mutex> lk(server->mu);
+        server->checkFailed();
+        auto it = server->requests.find(request);
+        if (it == server->requests.end()) throw ApiError(AG2D_ERR_INVALID_ARG, "unknown request");
+        const ServerRequest& r = *it->second;
+        if (out_state) *out_state = r.state;
+        if (out_latency_ms)
+            *out_latency_ms = r.state == AG2D_REQUEST_DONE
+                                  ? std::chrono::duration<double, std::milli>(r.finished - r.submitted).count()
+                                  : -1.0;
+    });
+}
+
+int32_t ag2d_server_wait_all(ag2d_server* server, double timeout_ms)
+{
+    return guarded([&] {
+        if (!server) throw ApiError(AG2D_ERR_INVALID_ARG, "null server");
+        std::unique_lock<std::mutex> lk(server->mu);
+        auto done = [&] { return server->failCode != AG2D_OK || server->completed == server->submitted; };
+        if (timeout_ms < 0) server->doneCv.wait(lk, done);
+        else if (!server->doneCv.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), done))
+            throw ApiError(AG2D_ERR_TIMEOUT, "requests still running after the timeout");
+        server->checkFailed();
+    });
+}
+
+int32_t ag2d_server_read(ag2d_server* server, uint64_t request, int32_t field, void* dst, uint64_t cap,
+                         uint64_t* out_bytes)
+{
+    return guarded([&] {
+        if (!server) throw ApiError(AG2D_ERR_INVALID_ARG, "null server");
+        std::shared_ptr<ServerRequest> r;
+        {
+            std::lock_guard<std::mutex> lk(server->mu);
+            auto it = server->requests.find(request);
+            if (it == server->requests.end()) throw ApiError(AG2D_ERR_INVALID_ARG, "unknown request");
+            r = it->second;
+            if (r->state != AG2D_REQUEST_DONE) throw ApiError(AG2D_ERR_INVALID_ARG, "request not finished");
+        }
+        const size_t nb = r->vel.size();
+        std::vector<float> f;
+        std::vector<uint32_t> u;
+        auto comp = [&](const std::vector<float4>& v, int c) {
+            f.resize(nb);
+            for (size_t i = 0; i < nb; i++) f[i] = c == 0 ? v[i].x : c == 1 ? v[i].y : c == 2 ? v[i].z : v[i].w;
+        };
+        switch (field) {
+        case AG2D_BODY_COM_X: comp(r->pos, 0); break;
+        case AG2D_BODY_COM_Y: comp(r->pos, 1); break;
+        case AG2D_BODY_ROTATION: comp(r->pos, 2); break;
+        case AG2D_BODY_VEL_X: comp(r->vel, 0); break;
+        case AG2D_BODY_VEL_Y: comp(r->vel, 1); break;
+        case AG2D_BODY_ANGULAR_VELOCITY: comp(r->vel, 2); break;
+        case AG2D_BODY_POSE:
+            f.resize(nb * 3);
+            for (size_t i = 0; i < nb; i++) { f[3 * i] = r->pos[i].x; f[3 * i + 1] = r->pos[i].y; f[3 * i + 2] = r->pos[i].z; }
+            break;
+        case AG2D_BODY_STATE: u.assign(r->bstate.begin(), r->bstate.end()); break;
+        default: throw ApiError(AG2D_ERR_UNSUPPORTED, "field is not kept for finished requests");
+        }
+        const size_t bytes = field == AG2D_BODY_STATE ? u.size() * 4 : f.size() * 4;
+        if (out_bytes) *out_bytes = bytes;
+        if (dst) {
+            if (cap < bytes) throw ApiError(AG2D_ERR_INVALID_ARG, "destination too small");
+            if (bytes) std::memcpy(dst, field == AG2D_BODY_STATE ? static_cast<const void*>(u.data()) : f.data(), bytes);
+        }
+    });
+}
+
+int32_t ag2d_server_release(ag2d_server* server, uint64_t request)
+{
+    return guarded([&] {
+        if (!server) throw ApiError(AG2D_ERR_INVALID_ARG, "null server");
+        std::lock_guard<std::mutex> lk(server->mu);
+        auto it = server->requests.find(request);
+        if (it == server->requests.end()) throw ApiError(AG2D_ERR_INVALID_ARG, "unknown request");
+        if (it->second->state != AG2D_REQUEST_DONE) throw ApiError(AG2D_ERR_INVALID_ARG, "request not finished");
+        server->requests.erase(it);
+    });
+}
+
+int32_t ag2d_server_stats_get(ag2d_server* server, ag2d_server_stats* out)
+{
+    return guarded([&] {
+        if (!server || !out) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        std::lock_guard<std::mutex> lk(server->mu);
+        out->submitted = server->submitted;
+        out->completed = server->completed;
+        out->waiting = server->waiting.size();
+        out->resident = server->resident.size();
+        out->peak_resident = server->peakResident;
+        out->rounds = server->rounds;
+        out->body_steps = server->bodySteps;
+        out->busy_ms = server->busyMs;
+        out->step_ms = server->stepMs;
+        out->repack_ms = server->repackMs;
+        std::vector<double> l = server->latencies;
+        std::sort(l.begin(), l.end());
+        auto q = [&](double p) { return l.empty() ? 0.0 : l[std::min(l.size() - 1, size_t(p * double(l.size())))]; };
+        out->p50_ms = q(0.50);
+        out->p99_ms = q(0.99);
+        out->max_ms = l.empty() ? 0.0 : l.back();
+    });
+}
+
+int32_t ag2d_server_destroy(ag2d_server* server)
+{
+    return guarded([&] {
+        if (!server) return;
+        {
+            std::lock_guard<std::mutex> lk(server->mu);
+            server->stop = true;
+        }
+        server->cv.notify_all();
+        if (server->worker.joinable()) server->worker.join();
+        cudaSetDevice(server->settings.world.device);
+        delete server;
     });
 }
 
