@@ -134,6 +134,39 @@ __global__ void k_bounds(const float4* __restrict__ aabb, const uint32_t* __rest
 {
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t base0 = blockIdx.x * blockDim.x;
+    if (!colWorld) {
+        // One world: per-thread running bounds over the grid-stride loop, then one block reduction and four
+        // atomics per block (per-warp atomics on four addresses serialise at one L2 slice for large n).
+        float mnx = FLT_MAX, mny = FLT_MAX, mxx = -FLT_MAX, mxy = -FLT_MAX;
+        for (uint32_t k = base0 + threadIdx.x; k < n; k += stride) {
+            const float4 a = aabb[list ? list[k] : k];
+            mnx = fminf(mnx, a.x); mny = fminf(mny, a.y); mxx = fmaxf(mxx, a.z); mxy = fmaxf(mxy, a.w);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+            mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+            mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+            mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+        }
+        __shared__ float4 part[32];
+        const uint32_t warp = threadIdx.x >> 5, warps = (blockDim.x + 31) >> 5;
+        if ((threadIdx.x & 31) == 0) part[warp] = make_float4(mnx, mny, mxx, mxy);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float4 r = part[0];
+            for (uint32_t k = 1; k < warps; k++) {
+                const float4 q = part[k];
+                r = make_float4(fminf(r.x, q.x), fminf(r.y, q.y), fmaxf(r.z, q.z), fmaxf(r.w, q.w));
+            }
+            if (r.x <= r.z) {   // the block saw at least one collider
+                atomicMin(bounds + 0, float_to_ordered(r.x));
+                atomicMin(bounds + 1, float_to_ordered(r.y));
+                atomicMax(bounds + 2, float_to_ordered(r.z));
+                atomicMax(bounds + 3, float_to_ordered(r.w));
+            }
+        }
+        return;
+    }
     for (uint32_t base = base0; base < n; base += stride) {
         const uint32_t k = base + threadIdx.x;
         const bool valid = k < n;
@@ -510,17 +543,26 @@ __global__ void k_lbvh_refit(int n, const int2* __restrict__ child, const int* _
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int node = leafParent[i];   // -1 for the leaf of a one-collider segment
+        int self = ~i;              // child encoding of the subtree this thread carries up
+        float4 box = leafAabb[i];   // its bounds
         while (node >= 0) {
-            // Release this thread's node write before the arrival count; the second arrival acquires both children.
-            asm volatile("fence.acq_rel.gpu;" ::: "memory");
-            if (atomicAdd(&visit[node], 1u) == 0) break;
-            asm volatile("fence.acq_rel.gpu;" ::: "memory");
+            // The tree links do not depend on the arrival: fetch them before the atomic.
             const int2 c = child[node];
-            const float4 a = c.x < 0 ? leafAabb[~c.x] : __ldcg(nodeAabb + c.x);
-            const float4 b = c.y < 0 ? leafAabb[~c.y] : __ldcg(nodeAabb + c.y);
-            const float4 u = make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w));
-            __stcg(nodeAabb + node, u);
-            node = parent[node];
+            const int up = parent[node];
+            // One acq_rel arrival: releases this thread's last node write and, for the second arrival, acquires
+            // the sibling's. Only the sibling's bounds are loaded; this thread's own are in registers.
+            uint32_t arrived;
+            asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
+                         : "=r"(arrived) : "l"(visit + node) : "memory");
+            if (arrived == 0) break;
+            const int sib = c.x == self ? c.y : c.x;
+            const float4 o = sib < 0 ? leafAabb[~sib] : __ldcg(nodeAabb + sib);
+            const float4 a = c.x == self ? box : o;
+            const float4 b = c.x == self ? o : box;
+            box = make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w));
+            __stcg(nodeAabb + node, box);
+            self = node;
+            node = up;
         }
     }
 }
