@@ -89,6 +89,7 @@ typedef struct ag2d_tuning {
     uint32_t query_threads;    /* pair-query block size */
     uint32_t narrow_threads;   /* narrow-phase block size */
     float solve_ms, query_ms, narrow_ms;   /* device time per step of each phase at the chosen setting */
+    uint32_t team_cons_on_chip;  /* batched solver: a team's constraint records kept in shared memory (1) or not */
 } ag2d_tuning;
 
 /* Reference-layout world state for ag2d_world_load_state: every array in the reference's dense order, as its
@@ -203,9 +204,12 @@ int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out);
 /* Launch-shape autotuner (no reference counterpart: the reference runs on CPU threads). Times real steps under each
  * candidate solver team size (batches), pair-query and narrow-phase block size and keeps the fastest. A step's
  * results do not depend on these settings, so tuning only advances the world: by 1 + candidates x
- * (steps_per_candidate + 1) steps, with 13 candidates for a batch and 6 for a single world. Works on a batch
+ * (steps_per_candidate + 1) steps, with 19 candidates for a batch and 6 for a single world. Works on a batch
  * through ag2d_batch_engine. */
 int32_t ag2d_world_autotune(ag2d_world* world, int32_t steps_per_candidate, ag2d_tuning* out);
+/* Applies launch shapes (for instance those the autotuner chose on a copy of the batch stepped ahead to a settled
+ * state). Results do not depend on them. */
+int32_t ag2d_world_set_tuning(ag2d_world* world, const ag2d_tuning* tuning);
 /* Device timing of the step phases (the reference's Tracy zones, Profiling/TracyProfiler.h:66-72, become CUDA
  * events on the world's stream). Enabling resets the totals. out_ms receives cumulative milliseconds per
  * enum ag2d_timed_phase, out_calls the number of timed occurrences. */

@@ -79,7 +79,7 @@ class Counters(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("team_colliders", ctypes.c_uint32), ("team_threads", ctypes.c_uint32), ("query_threads", ctypes.c_uint32),
                 ("narrow_threads", ctypes.c_uint32), ("solve_ms", ctypes.c_float), ("query_ms", ctypes.c_float),
-                ("narrow_ms", ctypes.c_float)]
+                ("narrow_ms", ctypes.c_float), ("team_cons_on_chip", ctypes.c_uint32)]
 
 
 TIMED_PHASES = ("integrate", "pose", "tree_dynamic", "tree_other", "query", "narrow", "compact", "warm", "wake",
@@ -144,6 +144,7 @@ def _load():
     L.ag2d_world_run_phase.argtypes = [vp, i32]
     L.ag2d_world_set_profiling.argtypes = [vp, i32]
     L.ag2d_world_autotune.argtypes = [vp, i32, ctypes.POINTER(Tuning)]
+    L.ag2d_world_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
     L.ag2d_world_phase_times.argtypes = [vp, vp, vp, i32]
     L.ag2d_world_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.ag2d_batch_create.argtypes = [ctypes.POINTER(vp), u32, ctypes.POINTER(vp)]
@@ -353,6 +354,14 @@ class World:
         t = Tuning()
         _check(lib.ag2d_world_autotune(self.h, steps_per_candidate, ctypes.byref(t)))
         return {n: (float(getattr(t, n)) if k is ctypes.c_float else int(getattr(t, n))) for n, k in Tuning._fields_}
+
+    def set_tuning(self, tuning: dict):
+        """Applies launch shapes (a dict as autotune returns); results do not depend on them."""
+        t = Tuning()
+        for n, k in Tuning._fields_:
+            if n in tuning:
+                setattr(t, n, tuning[n])
+        _check(lib.ag2d_world_set_tuning(self.h, ctypes.byref(t)))
 
     def set_profiling(self, enable: bool = True):
         _check(lib.ag2d_world_set_profiling(self.h, 1 if enable else 0))

@@ -300,6 +300,55 @@ struct GridSync {
     static __device__ __forceinline__ uint32_t ld(const uint32_t* p) { return __ldcg(p); }
 };
 
+// Constraint records of a team kept in shared memory for the warm, velocity and position passes: seven float4
+// fields per constraint, structure of arrays (q[f * cap + c]), so a warp's 16-byte accesses are contiguous. Body
+// indices are stored relative to the team's first body (12 bits each, MAX_TEAM_BODY_CAP <= 4096). cap == 0: the
+// records stay in global memory (SolveScratch::cons). The arithmetic on a record is the same either way.
+struct ConsSmem {
+    float4* q = nullptr;
+    uint32_t cap = 0;
+    uint32_t base = 0;
+    static constexpr uint32_t FIELDS = 7;
+    __device__ __forceinline__ void store(uint32_t c, const Constraint& k) const
+    {
+        const uint32_t packed = (k.bodyA - base) | (k.bodyB - base) << 12 | k.count << 24;
+        q[c] = make_float4(__uint_as_float(packed), k.penBase, k.nx, k.ny);
+        q[cap + c] = make_float4(k.jn0, k.jt0, k.jn1, k.jt1);
+        q[2 * cap + c] = make_float4(k.rAn0, k.rBn0, k.rAt0, k.rBt0);
+        q[3 * cap + c] = make_float4(k.rAn1, k.rBn1, k.rAt1, k.rBt1);
+        q[4 * cap + c] = make_float4(k.nm0, k.tm0, k.bias0, k.nm1);
+        q[5 * cap + c] = make_float4(k.tm1, k.bias1, k.sf, k.df);
+        q[6 * cap + c] = make_float4(k.imA, k.imB, k.iIA, k.iIB);
+    }
+    __device__ __forceinline__ void loadHead(uint32_t c, Constraint& k) const
+    {
+        const float4 a = q[c];
+        const uint32_t packed = __float_as_uint(a.x);
+        k.bodyA = base + (packed & 0xFFFu);
+        k.bodyB = base + ((packed >> 12) & 0xFFFu);
+        k.count = packed >> 24;
+        k.penBase = a.y; k.nx = a.z; k.ny = a.w;
+    }
+    __device__ __forceinline__ void load(uint32_t c, Constraint& k) const
+    {
+        loadHead(c, k);
+        const float4 j = q[cap + c], r0 = q[2 * cap + c], r1 = q[3 * cap + c], m0 = q[4 * cap + c],
+                     m1 = q[5 * cap + c], ms = q[6 * cap + c];
+        k.jn0 = j.x; k.jt0 = j.y; k.jn1 = j.z; k.jt1 = j.w;
+        k.rAn0 = r0.x; k.rBn0 = r0.y; k.rAt0 = r0.z; k.rBt0 = r0.w;
+        k.rAn1 = r1.x; k.rBn1 = r1.y; k.rAt1 = r1.z; k.rBt1 = r1.w;
+        k.nm0 = m0.x; k.tm0 = m0.y; k.bias0 = m0.z; k.nm1 = m0.w;
+        k.tm1 = m1.x; k.bias1 = m1.y; k.sf = m1.z; k.df = m1.w;
+        k.imA = ms.x; k.imB = ms.y; k.iIA = ms.z; k.iIB = ms.w;
+    }
+    __device__ __forceinline__ void storeImpulses(uint32_t c, const Constraint& k) const
+    {
+        q[cap + c] = make_float4(k.jn0, k.jt0, k.jn1, k.jt1);
+    }
+    __device__ __forceinline__ float4 impulses(uint32_t c) const { return q[cap + c]; }
+};
+constexpr uint32_t CONS_SMEM_BYTES = ConsSmem::FIELDS * sizeof(float4);
+
 // Pulls the 128-byte constraint of slot c into L1 ahead of the pass that reads it.
 __device__ __forceinline__ void prefetch_l1(const void* p)
 {
@@ -325,7 +374,8 @@ __device__ __forceinline__ void prefetch_colour(const SolveScratch& s, uint32_t 
 template <class Sync, class Bodies>
 __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold* __restrict__ m, uint32_t n,
                                 const SolveScratch& s, uint32_t velIters, uint32_t posIters, uint32_t rank,
-                                uint32_t size, Sync sync, uint32_t* __restrict__ outColors, uint32_t* __restrict__ status)
+                                uint32_t size, Sync sync, uint32_t* __restrict__ outColors, uint32_t* __restrict__ status,
+                                ConsSmem cs = ConsSmem{})
 {
     for (uint32_t c = rank; c < COLOR_SLOTS; c += size) s.colorCount[c] = 0;
     // Each manifold's two bodies and whether they are dynamic, looked up once for all colouring rounds.
@@ -412,44 +462,72 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
         s.order[Sync::ld(s.colorStart + c) + atomicAdd(s.colorCount + c, 1u)] = i;
     }
     if (!sync()) return false;
-    // Constraint build for every manifold before any velocity changes (computeConstraintData).
+    // Constraint build for every manifold before any velocity changes (computeConstraintData). The records go to
+    // shared memory when the team's fit there (the colouring words they overwrite are no longer needed).
+    const bool onChip = cs.cap >= n && cs.q != nullptr;
     for (uint32_t c = rank; c < n; c += size) {
         const uint32_t mi = __ldcg(s.order + c);
         Constraint k;
         prep_constraint(w, B, m[mi], mi, k);
-        s.cons[c] = k;
+        if (onChip) cs.store(c, k);
+        else s.cons[c] = k;
     }
     if (!sync()) return false;
     for (uint32_t col = 0; col < ncol; col++) {
         const uint32_t end = Sync::ld(s.colorStart + col + 1);
-        for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) warm_constraint(B, s.cons[c]);
+        for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) {
+            if (onChip) {
+                Constraint k;
+                cs.load(c, k);
+                warm_constraint(B, k);
+            } else {
+                warm_constraint(B, s.cons[c]);
+            }
+        }
         if (!sync()) return false;
     }
     for (uint32_t it = 0; it < velIters; it++) {
         for (uint32_t col = 0; col < ncol; col++) {
             const uint32_t end = Sync::ld(s.colorStart + col + 1);
             for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) {
-                Constraint k = s.cons[c];
+                Constraint k;
+                if (onChip) cs.load(c, k);
+                else k = s.cons[c];
                 velocity_constraint(B, k);
-                *reinterpret_cast<float4*>(&s.cons[c].jn0) = make_float4(k.jn0, k.jt0, k.jn1, k.jt1);
+                if (onChip) cs.storeImpulses(c, k);
+                else *reinterpret_cast<float4*>(&s.cons[c].jn0) = make_float4(k.jn0, k.jt0, k.jn1, k.jt1);
             }
             // The next pass's constraint: from the next colour, or colour 0 of the next iteration.
-            prefetch_colour<Sync>(s, col + 1 < ncol ? col + 1 : 0, ncol, rank);
+            if (!onChip) prefetch_colour<Sync>(s, col + 1 < ncol ? col + 1 : 0, ncol, rank);
             if (!sync()) return false;
         }
     }
     for (uint32_t it = 0; it < posIters; it++) {
         for (uint32_t col = 0; col < ncol; col++) {
             const uint32_t end = Sync::ld(s.colorStart + col + 1);
-            for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) position_constraint(B, s.cons[c]);
-            prefetch_colour<Sync>(s, col + 1 < ncol ? col + 1 : 0, ncol, rank);
+            for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) {
+                if (onChip) {
+                    Constraint k;
+                    cs.loadHead(c, k);
+                    position_constraint(B, k);
+                } else {
+                    position_constraint(B, s.cons[c]);
+                }
+            }
+            if (!onChip) prefetch_colour<Sync>(s, col + 1 < ncol ? col + 1 : 0, ncol, rank);
             if (!sync()) return false;
         }
     }
     for (uint32_t c = rank; c < n; c += size) {
-        const Constraint& k = s.cons[c];
-        Manifold& d = m[k.manifold];
-        d.jn0 = k.jn0; d.jt0 = k.jt0; d.jn1 = k.jn1; d.jt1 = k.jt1;
+        if (onChip) {
+            const float4 j = cs.impulses(c);
+            Manifold& d = m[__ldcg(s.order + c)];
+            d.jn0 = j.x; d.jt0 = j.y; d.jn1 = j.z; d.jt1 = j.w;
+        } else {
+            const Constraint& k = s.cons[c];
+            Manifold& d = m[k.manifold];
+            d.jn0 = k.jn0; d.jt0 = k.jt0; d.jn1 = k.jn1; d.jt1 = k.jt1;
+        }
     }
     return true;
 }
@@ -466,10 +544,19 @@ __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* n
 // and solved by one CTA with __syncthreads between colours. Teams are taken from the work counter *nextTeam (zeroed
 // before the launch) in 'teamOrder' order, largest first. Colouring priorities are world-local manifold indices, so
 // the colours of a world do not depend on its team. The CTA size (64 to 512 threads) is a launch parameter;
-// a team whose bodies fit 'bodyCap' keeps their state and colouring words in dynamic shared memory
-// (TEAM_SMEM_PER_BODY bytes per body).
-constexpr uint32_t TEAM_SMEM_PER_BODY = 2 * sizeof(float4) + 2 * sizeof(unsigned long long);
+// a team whose bodies fit 'bodyCap' keeps their state and colouring words in dynamic shared memory, and, when its
+// manifolds fit 'consCap', its constraint records too (team_smem_bytes).
 constexpr uint32_t MAX_TEAM_BODY_CAP = 4096;   // largest body range a team stages in shared memory
+constexpr uint32_t TEAM_SMEM_MAX = 220 * 1024; // dynamic shared memory of a team CTA (sm_100 allows 227 KB in
+                                               // all, the kernel's static arrays included)
+// Dynamic shared memory of a team CTA: body velocities and poses, then one region holding first the colouring words
+// (16 B a body) and then the constraint records (CONS_SMEM_BYTES each, consCap of them).
+__host__ __device__ constexpr size_t team_smem_bytes(uint32_t bodyCap, uint32_t consCap)
+{
+    return size_t(bodyCap) * 2 * sizeof(float4) +
+           (size_t(bodyCap) * 16 > size_t(consCap) * CONS_SMEM_BYTES ? size_t(bodyCap) * 16
+                                                                       : size_t(consCap) * CONS_SMEM_BYTES);
+}
 constexpr uint32_t BIG_TEAM_THREADS = 512;     // CTA size for a world larger than the team size
 struct TeamLaunch {
     DeviceWorld w;
@@ -479,6 +566,7 @@ struct TeamLaunch {
     const uint32_t* teamOrder;
     uint32_t teams;
     uint32_t bodyCap;
+    uint32_t consCap;   // constraint records a team keeps in shared memory (0: global memory)
     SolveScratch s;
     uint32_t velIters, posIters;
     uint32_t* nextTeam;
@@ -486,9 +574,9 @@ struct TeamLaunch {
 };
 // Host side: launches the team solver with 'threads' per CTA; returns the launch error.
 cudaError_t launch_color_solve_teams(uint32_t threads, uint32_t grid, cudaStream_t stream, const TeamLaunch& a);
-// Host side: co-resident CTAs per SM of the team solver at this CTA size and body capacity. Also raises the kernel's
-// dynamic shared-memory limit to what MAX_TEAM_BODY_CAP needs (the limit is per kernel, shared by every engine in the
+// Host side: co-resident CTAs per SM of the team solver at this CTA size and shared-memory capacities. Also raises
+// the kernel's dynamic shared-memory limit to TEAM_SMEM_MAX (the limit is per kernel, shared by every engine in the
 // process, so it is never lowered).
-cudaError_t team_solver_blocks_per_sm(uint32_t threads, uint32_t bodyCap, int* out);
+cudaError_t team_solver_blocks_per_sm(uint32_t threads, uint32_t bodyCap, uint32_t consCap, int* out);
 
 }  // namespace ag2d

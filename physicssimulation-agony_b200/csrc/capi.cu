@@ -429,6 +429,9 @@ struct ag2d_world {
     uint32_t teamColliders = 1024;         // solver team size: consecutive worlds packed up to this many colliders
     uint32_t teamThreads = 128;            // CTA size of the team solver
     uint32_t teamBodyCap = 2048;           // bodies of a team staged in shared memory (larger teams use global)
+    uint32_t teamConsCap = 0;              // constraint records a team keeps in shared memory (more: global)
+    uint32_t bigConsCap = 0;
+    bool consOnChip = true;                // team constraint records in shared memory when they fit (tunable)
     uint32_t nTeams = 0;
     uint32_t teamBlocks = 1;               // co-resident CTAs of the team solver at this shared-memory size
     uint32_t nBigTeams = 0, bigBodyCap = 0, bigBlocks = 1;   // worlds larger than a team, one CTA each
@@ -785,8 +788,17 @@ struct ag2d_world {
         teamColliders = colliders;
         teamThreads = threads;
         teamBodyCap = std::min<uint32_t>(MAX_TEAM_BODY_CAP, colliders);
+        // Constraint records kept on chip: room for 3 manifolds per collider (a settled pile of convex bodies has
+        // about 1.5 on average, with denser worlds well above), within the CTA's shared-memory limit; a team with
+        // more solves from global memory.
+        auto consFit = [&](uint32_t bodyCap, uint32_t want) -> uint32_t {
+            if (!consOnChip) return 0;
+            const size_t room = (TEAM_SMEM_MAX - size_t(bodyCap) * 2 * sizeof(float4)) / CONS_SMEM_BYTES;
+            return uint32_t(std::min<size_t>(want, room));
+        };
+        teamConsCap = consFit(teamBodyCap, 3 * colliders);
         int perSm = 0;
-        CK(team_solver_blocks_per_sm(teamThreads, teamBodyCap, &perSm));
+        CK(team_solver_blocks_per_sm(teamThreads, teamBodyCap, teamConsCap, &perSm));
         teamBlocks = uint32_t(std::max(1, perSm) * dev.sms);
         // Worlds above the team size are teams of their own ("big", solved by BIG_TEAM_THREADS-thread CTAs);
         // the others are packed, in order, into teams of up to 'colliders' colliders.
@@ -817,9 +829,10 @@ struct ag2d_world {
         nTeams = uint32_t(small.size());
         nBigTeams = uint32_t(big.size());
         bigBodyCap = std::min<uint32_t>(MAX_TEAM_BODY_CAP, bigMax);
+        bigConsCap = consFit(bigBodyCap, 3 * bigMax);
         bigBlocks = 1;
         if (nBigTeams) {
-            CK(team_solver_blocks_per_sm(BIG_TEAM_THREADS, bigBodyCap, &perSm));
+            CK(team_solver_blocks_per_sm(BIG_TEAM_THREADS, bigBodyCap, bigConsCap, &perSm));
             bigBlocks = uint32_t(std::max(1, perSm) * dev.sms);
         }
         std::vector<uint32_t> order(small);
@@ -1394,14 +1407,14 @@ struct ag2d_world {
                 CK(cudaEventRecord(forkEvent, s));
                 CK(cudaStreamWaitEvent(sideStream, forkEvent, 0));
                 const TeamLaunch big{w, mm, manSeg.p, teamWorld.p, teamOrder.p + nTeams, nBigTeams, bigBodyCap,
-                                     scratch, vi, pi, nextWorld.p + 1, ctr};
+                                     bigConsCap, scratch, vi, pi, nextWorld.p + 1, ctr};
                 CK(launch_color_solve_teams(BIG_TEAM_THREADS, std::min(nBigTeams, bigBlocks), sideStream, big));
                 launches++;
             }
             if (nTeams) {
                 const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(nTeams, teamBlocks));
-                const TeamLaunch args{w, mm, manSeg.p, teamWorld.p, teamOrder.p, nTeams, teamBodyCap, scratch, vi,
-                                      pi, nextWorld.p, ctr};
+                const TeamLaunch args{w, mm, manSeg.p, teamWorld.p, teamOrder.p, nTeams, teamBodyCap, teamConsCap,
+                                      scratch, vi, pi, nextWorld.p, ctr};
                 CK(launch_color_solve_teams(teamThreads, grid, s, args));
             }
             if (nBigTeams) {
@@ -1516,14 +1529,26 @@ struct ag2d_world {
         };
         out.team_colliders = 0;
         out.team_threads = 0;
+        out.team_cons_on_chip = consOnChip ? 1 : 0;
         out.solve_ms = 0.0f;
         if (nWorlds > 1) {
-            // (colliders per team, threads per CTA), packed as colliders << 16 | threads.
-            const auto r = pick(10, {256u << 16 | 64, 512u << 16 | 64, 512u << 16 | 128, 1024u << 16 | 128,
-                                     1024u << 16 | 256, 2048u << 16 | 256, 2048u << 16 | 512},
-                                [&](uint32_t t) { setTeams(t >> 16, t & 0xFFFF); });
+            // (colliders per team, threads per CTA, constraint records on chip), packed as
+            // colliders << 16 | on-chip << 15 | threads.
+            std::vector<uint32_t> cands;
+            for (uint32_t t : {256u << 16 | 64, 512u << 16 | 64, 512u << 16 | 128, 1024u << 16 | 128,
+                               1024u << 16 | 256, 2048u << 16 | 256, 2048u << 16 | 512})
+                cands.push_back(t);
+            // On chip: smaller teams, so that their records fit and several CTAs share an SM.
+            for (uint32_t t : {128u << 16 | 64, 256u << 16 | 64, 256u << 16 | 128, 512u << 16 | 128,
+                               512u << 16 | 256, 1024u << 16 | 256})
+                cands.push_back(t | 1u << 15);
+            const auto r = pick(10, cands, [&](uint32_t t) {
+                consOnChip = (t >> 15) & 1;
+                setTeams(t >> 16, t & 0x7FFF);
+            });
             out.team_colliders = r.first >> 16;
-            out.team_threads = r.first & 0xFFFF;
+            out.team_threads = r.first & 0x7FFF;
+            out.team_cons_on_chip = (r.first >> 15) & 1;
             out.solve_ms = float(r.second);
         }
         const auto q = pick(4, {64, 128, 256}, [&](uint32_t t) { queryThreads = t; });
@@ -1905,6 +1930,32 @@ int32_t ag2d_world_autotune(ag2d_world* world, int32_t steps_per_candidate, ag2d
         ag2d_tuning t{};
         world->autotune(uint32_t(steps_per_candidate), t);
         if (out) *out = t;
+    });
+}
+
+int32_t ag2d_world_set_tuning(ag2d_world* world, const ag2d_tuning* tuning)
+{
+    return guarded([&] {
+        if (!world || !tuning) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        const ag2d_tuning& t = *tuning;
+        auto oneOf = [](uint32_t v, std::initializer_list<uint32_t> ok) {
+            return std::find(ok.begin(), ok.end(), v) != ok.end();
+        };
+        if (!oneOf(t.query_threads, {64, 128, 256}) || !oneOf(t.narrow_threads, {128, 256, 512}))
+            throw ApiError(AG2D_ERR_INVALID_ARG, "query / narrow block size out of range");
+        if (t.team_colliders && (!oneOf(t.team_threads, {64, 128, 256, 512}) || t.team_colliders < 64 ||
+                                 t.team_colliders > MAX_TEAM_BODY_CAP))
+            throw ApiError(AG2D_ERR_INVALID_ARG, "team size out of range");
+        CK(cudaSetDevice(world->settings.device));
+        world->ensureUploaded();
+        world->queryThreads = t.query_threads;
+        world->narrowThreads = t.narrow_threads;
+        world->consOnChip = t.team_cons_on_chip != 0;
+        if (t.team_colliders) {
+            world->teamColliders = t.team_colliders;
+            world->teamThreads = t.team_threads;
+            if (world->nWorlds > 1) world->setTeams(t.team_colliders, t.team_threads);
+        }
     });
 }
 

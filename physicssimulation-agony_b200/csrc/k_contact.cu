@@ -266,7 +266,9 @@ __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* n
 template <uint32_t THREADS>
 __global__ void __launch_bounds__(THREADS) k_color_solve_teams(TeamLaunch a)
 {
-    extern __shared__ float4 teamCache[];   // [bodyCap] velocities, [bodyCap] poses, then 2 x [bodyCap] u64 words
+    // [bodyCap] velocities, [bodyCap] poses, then 2 x [bodyCap] u64 colouring words, overwritten after colouring by
+    // the constraint records (team_smem_bytes).
+    extern __shared__ float4 teamCache[];
     __shared__ uint32_t colorCount[COLOR_SLOTS];
     __shared__ uint32_t colorStart[MAX_COLORS + 1];
     __shared__ uint32_t item;
@@ -300,8 +302,12 @@ __global__ void __launch_bounds__(THREADS) k_color_solve_teams(TeamLaunch a)
                 maskW[i] = 0ull;
             }
             __syncthreads();
+            ConsSmem cs;
+            cs.q = teamCache + 2 * a.bodyCap;
+            cs.cap = a.consCap;
+            cs.base = b0;
             color_and_solve(w, SharedBodies{vel, pos, maxW, maskW, b0}, m + lo, hi - lo, ls, a.velIters, a.posIters,
-                            threadIdx.x, THREADS, BlockSync{}, &a.counters->colors, &a.counters->status);
+                            threadIdx.x, THREADS, BlockSync{}, &a.counters->colors, &a.counters->status, cs);
             __syncthreads();
             for (uint32_t i = threadIdx.x; i < nb; i += THREADS) {
                 w.bvel[b0 + i] = vel[i];
@@ -318,29 +324,30 @@ __global__ void __launch_bounds__(THREADS) k_color_solve_teams(TeamLaunch a)
 }
 
 template <uint32_t THREADS>
-static cudaError_t team_occupancy(uint32_t bodyCap, int* out)
+static cudaError_t team_occupancy(uint32_t bodyCap, uint32_t consCap, int* out)
 {
     cudaError_t e = cudaFuncSetAttribute(k_color_solve_teams<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(size_t(MAX_TEAM_BODY_CAP) * TEAM_SMEM_PER_BODY));
+                                         int(TEAM_SMEM_MAX));
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, k_color_solve_teams<THREADS>, THREADS,
-                                                         size_t(bodyCap) * TEAM_SMEM_PER_BODY);
+                                                         team_smem_bytes(bodyCap, consCap));
 }
 
-cudaError_t team_solver_blocks_per_sm(uint32_t threads, uint32_t bodyCap, int* out)
+cudaError_t team_solver_blocks_per_sm(uint32_t threads, uint32_t bodyCap, uint32_t consCap, int* out)
 {
     switch (threads) {
-    case 64: return team_occupancy<64>(bodyCap, out);
-    case 128: return team_occupancy<128>(bodyCap, out);
-    case 256: return team_occupancy<256>(bodyCap, out);
-    case 512: return team_occupancy<512>(bodyCap, out);
+    case 64: return team_occupancy<64>(bodyCap, consCap, out);
+    case 128: return team_occupancy<128>(bodyCap, consCap, out);
+    case 256: return team_occupancy<256>(bodyCap, consCap, out);
+    case 512: return team_occupancy<512>(bodyCap, consCap, out);
     default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_color_solve_teams(uint32_t threads, uint32_t grid, cudaStream_t stream, const TeamLaunch& a)
 {
-    const size_t smem = size_t(a.bodyCap) * TEAM_SMEM_PER_BODY;
+    const size_t smem = team_smem_bytes(a.bodyCap, a.consCap);
+    if (smem > TEAM_SMEM_MAX) return cudaErrorInvalidValue;
     switch (threads) {
     case 64: k_color_solve_teams<64><<<grid, 64, smem, stream>>>(a); break;
     case 128: k_color_solve_teams<128><<<grid, 128, smem, stream>>>(a); break;

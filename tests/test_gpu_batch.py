@@ -106,9 +106,35 @@ def test_autotune_does_not_change_results():
     tuned = ag2d.Batch([ag2d.World.from_scene(s) for s in sc])
     plain = ag2d.Batch([ag2d.World.from_scene(s) for s in sc])
     t = tuned.engine.autotune(1)
-    assert t["team_colliders"] in (256, 512, 1024, 2048) and t["team_threads"] in (64, 128, 256, 512)
+    assert t["team_colliders"] in (128, 256, 512, 1024, 2048) and t["team_threads"] in (64, 128, 256, 512)
     assert t["query_threads"] in (64, 128, 256) and t["narrow_threads"] in (128, 256, 512)
-    plain.step(1 + 13 * 2)
+    assert t["team_cons_on_chip"] in (0, 1)
+    plain.step(1 + 19 * 2)
     for k in range(len(sc)):
         for f in BODY_FIELDS:
             assert np.array_equal(_bits(tuned.read(k, f)), _bits(plain.read(k, f))), (k, f)
+
+
+@pytest.mark.parametrize("on_chip,colliders,threads", [(0, 1024, 128), (1, 128, 64), (1, 512, 256), (1, 2048, 512)])
+def test_set_tuning_does_not_change_results(on_chip, colliders, threads):
+    """Team solver with its constraint records in global or shared memory (and teams too large for the shared-memory
+    records, which fall back to global memory): the same results as the default launch shapes."""
+    sc = _scene_list(seed=23)
+    tuned = ag2d.Batch([ag2d.World.from_scene(s) for s in sc])
+    plain = ag2d.Batch([ag2d.World.from_scene(s) for s in sc])
+    tuned.engine.set_tuning({"team_colliders": colliders, "team_threads": threads, "query_threads": 64,
+                             "narrow_threads": 512, "team_cons_on_chip": on_chip})
+    tuned.step(150)
+    plain.step(150)
+    for k in range(len(sc)):
+        _assert_world_equal(tuned, k, _Alone(plain, k))
+
+
+class _Alone:
+    """A world of a batch read through the single-world interface (for _assert_world_equal)."""
+
+    def __init__(self, batch, k):
+        self.batch, self.k = batch, k
+
+    def read(self, field):
+        return self.batch.read(self.k, field)
