@@ -17,6 +17,15 @@ constexpr uint32_t QUERY_STASH = 8;   // pairs a query keeps from its counting t
 constexpr uint32_t MAX_COLORS = 256;
 constexpr uint32_t NO_COLOR = 0xFFFFFFFFu;
 
+// Traversal record of an internal node: both children's AABBs, their child codes (internal node index, or ~leaf)
+// and the last leaf of each child's range, so that a traversal step is one 48-byte load.
+struct alignas(16) NodeRec {
+    float4 box[2];
+    int2 child;
+    int2 last;
+};
+static_assert(sizeof(NodeRec) == 48, "NodeRec is 48 bytes");
+
 // Read-only view of one LBVH over n leaves in sorted order. A single tree has n - 1 internal nodes and root 0; a
 // world-segmented tree (sortedWorld non-null) holds one tree per world segment [segStart[w], segStart[w + 1]),
 // rooted at internal node segStart[w].
@@ -29,6 +38,7 @@ struct TreeView {
     const uint32_t* vals;         // collider index of each leaf
     const uint32_t* sortedWorld;  // world of each leaf, or null (one world)
     const uint32_t* segStart;     // [worlds + 1] segment starts, or null (one world)
+    const NodeRec* rec;           // traversal records of the internal nodes
 };
 
 // Spatial kernels (k_spatial.cu).
@@ -57,9 +67,9 @@ __global__ void k_sort_pass(const uint32_t* keysIn, const uint32_t* valsIn, uint
                             uint32_t n, uint32_t shift, const uint32_t* digitBase, uint32_t* tileState,
                             uint32_t* tileCounter, uint32_t* status);
 __global__ void k_lbvh_build(const uint32_t* keys, const uint32_t* sortedWorld, const uint32_t* segStart, int n,
-                             int2* child, int2* range, int* parent, int* leafParent, uint32_t* visit);
+                             int2* child, int2* range, int* parent, int* leafParent, uint32_t* visit, NodeRec* rec);
 __global__ void k_lbvh_refit(int n, const int2* child, const int* parent, const int* leafParent,
-                             const float4* leafAabb, float4* nodeAabb, uint32_t* visit);
+                             const float4* leafAabb, float4* nodeAabb, uint32_t* visit, NodeRec* rec);
 __global__ void k_query_stash(TreeView dyn, TreeView other, const uint32_t* cbody, uint32_t* counts, uint2* stash,
                               uint32_t* status);
 __global__ void k_query_emit(TreeView dyn, TreeView other, const uint32_t* cbody, const uint32_t* counts,
@@ -71,8 +81,8 @@ __global__ void k_ccd_shift_colliders(DeviceWorld w, const uint32_t* dynCol, uin
                                       const uint32_t* hitTime);
 __global__ void k_ccd_shift_bodies(DeviceWorld w, const uint32_t* dynBody, uint32_t n, const float4* prevPos,
                                    uint32_t* hitTime, StepCounters* counters);
-__global__ void k_scan_blocks(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* blockSums);
-__global__ void k_scan_add(uint32_t* out, uint32_t n, const uint32_t* blockOffsets);
+__global__ void k_scan_blocks(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* blockSums, const uint32_t* nDev);
+__global__ void k_scan_add(uint32_t* out, uint32_t n, const uint32_t* blockOffsets, const uint32_t* nDev);
 __global__ void k_scan_total(const uint32_t* in, const uint32_t* out, uint32_t n, uint32_t* total);
 
 // Contact kernels (k_contact.cu).

@@ -122,15 +122,18 @@ struct Scanner {
             lvl++;
         }
     }
-    void run(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* total, cudaStream_t s, uint32_t lvl = 0)
+    // Exclusive scan of in[0, n) (n the capacity; nDev, if given, the device-side count within it: elements past it
+    // are neither read nor written).
+    void run(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* total, cudaStream_t s, uint32_t lvl = 0,
+             const uint32_t* nDev = nullptr)
     {
         const uint32_t nb = std::max<uint32_t>(div_up(n, SCAN_TILE), 1);
         uint32_t* sums = nb > 1 ? levels.at(lvl)->p : nullptr;
-        k_scan_blocks<<<nb, SCAN_THREADS, 0, s>>>(in, out, n, sums);
+        k_scan_blocks<<<nb, SCAN_THREADS, 0, s>>>(in, out, n, sums, nDev);
         CK(cudaGetLastError());
         if (nb > 1) {
             run(sums, sums, nb, nullptr, s, lvl + 1);
-            k_scan_add<<<nb, SCAN_THREADS, 0, s>>>(out, n, sums);
+            k_scan_add<<<nb, SCAN_THREADS, 0, s>>>(out, n, sums, nDev);
             CK(cudaGetLastError());
         }
         if (total) {
@@ -145,6 +148,7 @@ struct Tree {
     DBuf<int2> child, range;
     DBuf<int> parent, leafParent;
     DBuf<float4> leafAabb, nodeAabb;
+    DBuf<NodeRec> rec;
     DBuf<uint32_t> visit, bounds, hist, tileState, tileCounter;
     // World-segmented trees: Morton key per collider, sorted keys / worlds, segment starts (filled with the lists).
     DBuf<uint32_t> keyOf, sortedKey, sortedWorld, segStart;
@@ -155,7 +159,7 @@ struct Tree {
         worlds = nWorlds;
         keys.reserve(cap); vals.reserve(cap); keys2.reserve(cap); vals2.reserve(cap);
         child.reserve(cap); range.reserve(cap); parent.reserve(cap); leafParent.reserve(cap);
-        leafAabb.reserve(cap); nodeAabb.reserve(cap); visit.reserve(cap);
+        leafAabb.reserve(cap); nodeAabb.reserve(cap); visit.reserve(cap); rec.reserve(cap);
         bounds.reserve(4 * size_t(nWorlds)); hist.reserve(4 * 256); tileCounter.reserve(4);
         tileState.reserve(size_t(div_up(std::max<uint32_t>(cap, 1), SORT_TILE)) * 256 * 4);
         if (nWorlds > 1) {
@@ -166,7 +170,7 @@ struct Tree {
     {
         const bool seg = worlds > 1;
         return TreeView{n, child.p, range.p, nodeAabb.p, leafAabb.p, vals.p, seg ? sortedWorld.p : nullptr,
-                        seg ? segStart.p : nullptr};
+                        seg ? segStart.p : nullptr, rec.p};
     }
 };
 
@@ -1266,11 +1270,11 @@ struct ag2d_world {
                                                   t.leafAabb.p);
         k_lbvh_build<<<gridFor(n), 256, 0, s>>>(seg ? t.sortedKey.p : t.keys.p, seg ? t.sortedWorld.p : nullptr,
                                                  seg ? t.segStart.p : nullptr, int(n), t.child.p, t.range.p,
-                                                 t.parent.p, t.leafParent.p, t.visit.p);
+                                                 t.parent.p, t.leafParent.p, t.visit.p, t.rec.p);
         CK(cudaGetLastError());
         if (n > 1) {
             k_lbvh_refit<<<gridFor(n), 256, 0, s>>>(int(n), t.child.p, t.parent.p, t.leafParent.p, t.leafAabb.p,
-                                                     t.nodeAabb.p, t.visit.p);
+                                                     t.nodeAabb.p, t.visit.p, t.rec.p);
             CK(cudaGetLastError());
         }
         if (isDyn) pend(13);
@@ -1346,9 +1350,8 @@ struct ag2d_world {
         pend(5);
         pbegin(6);
         launches += 1 + scanLaunches(pairCap) + 1 + 2;
-        // The scan length must be host-known: scan the whole capacity (hit flags beyond the count are stale but the
-        // compaction kernel ignores them).
-        scanner.run(hit.p, hitOffsets.p, pairCap, nullptr, s);
+        // Grid sized for the capacity, work bounded by the device-side pair count.
+        scanner.run(hit.p, hitOffsets.p, pairCap, nullptr, s, 0, nPairs);
         k_compact_manifolds<<<g, 256, 0, s>>>(slots.p, hit.p, hitOffsets.p, nPairs, pairCap, manifolds.p,
                                                manifoldCap, nManifolds.p, dCounters.p);
         CK(cudaGetLastError());

@@ -498,7 +498,7 @@ __device__ __forceinline__ int lbvh_delta(const uint32_t* keys, int lo, int hi, 
 __global__ void k_lbvh_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ sortedWorld,
                              const uint32_t* __restrict__ segStart, int n, int2* __restrict__ child,
                              int2* __restrict__ range, int* __restrict__ parent, int* __restrict__ leafParent,
-                             uint32_t* __restrict__ visit)
+                             uint32_t* __restrict__ visit, NodeRec* __restrict__ rec)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int lo = 0, hi = n;
@@ -531,6 +531,8 @@ __global__ void k_lbvh_build(const uint32_t* __restrict__ keys, const uint32_t* 
         const int right = (last == gamma + 1) ? ~(gamma + 1) : gamma + 1;
         child[i] = make_int2(left, right);
         range[i] = make_int2(first, last);
+        rec[i].child = make_int2(left, right);
+        rec[i].last = make_int2(gamma, last);
         if (left < 0) leafParent[~left] = i; else parent[left] = i;
         if (right < 0) leafParent[~right] = i; else parent[right] = i;
     }
@@ -539,7 +541,7 @@ __global__ void k_lbvh_build(const uint32_t* __restrict__ keys, const uint32_t* 
 // Bottom-up AABB refit: the second thread to reach a node merges its children (BvhTree::fitNodes equivalent).
 __global__ void k_lbvh_refit(int n, const int2* __restrict__ child, const int* __restrict__ parent,
                              const int* __restrict__ leafParent, const float4* __restrict__ leafAabb,
-                             float4* __restrict__ nodeAabb, uint32_t* __restrict__ visit)
+                             float4* __restrict__ nodeAabb, uint32_t* __restrict__ visit, NodeRec* __restrict__ rec)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int node = leafParent[i];   // -1 for the leaf of a one-collider segment
@@ -549,16 +551,18 @@ __global__ void k_lbvh_refit(int n, const int2* __restrict__ child, const int* _
             // The tree links do not depend on the arrival: fetch them before the atomic.
             const int2 c = child[node];
             const int up = parent[node];
-            // One acq_rel arrival: releases this thread's last node write and, for the second arrival, acquires
-            // the sibling's. Only the sibling's bounds are loaded; this thread's own are in registers.
+            // This subtree's bounds go into the parent's traversal record before the arrival.
+            const int side = c.x == self ? 0 : 1;
+            __stcg(&rec[node].box[side], box);
+            // One acq_rel arrival: releases this thread's record write and, for the second arrival, acquires the
+            // sibling's. Only the sibling's bounds are loaded; this thread's own are in registers.
             uint32_t arrived;
             asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
                          : "=r"(arrived) : "l"(visit + node) : "memory");
             if (arrived == 0) break;
-            const int sib = c.x == self ? c.y : c.x;
-            const float4 o = sib < 0 ? leafAabb[~sib] : __ldcg(nodeAabb + sib);
-            const float4 a = c.x == self ? box : o;
-            const float4 b = c.x == self ? o : box;
+            const float4 o = __ldcg(&rec[node].box[side ^ 1]);
+            const float4 a = side == 0 ? box : o;
+            const float4 b = side == 0 ? o : box;
             box = make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w));
             __stcg(nodeAabb + node, box);
             self = node;
@@ -610,19 +614,19 @@ __device__ __forceinline__ uint32_t query_one(const TreeView& dyn, const TreeVie
         stack[sp++] = dlo;
         while (sp > 0) {
             const int node = stack[--sp];
-            const int2 c = dyn.child[node];
+            const NodeRec r = dyn.rec[node];
 #pragma unroll
             for (int side = 0; side < 2; side++) {
-                const int ch = side == 0 ? c.x : c.y;
+                const int ch = side == 0 ? r.child.x : r.child.y;
+                const int last = side == 0 ? r.last.x : r.last.y;
+                if (last <= i || !strict_overlap(q, r.box[side])) continue;   // every leaf below ranks <= i
                 if (ch < 0) {
-                    const int j = ~ch;
-                    if (j > i && strict_overlap(q, dyn.leafAabb[j])) {
-                        const uint32_t other_c = dyn.vals[j];
-                        if (cbody[other_c] != myBody) emit(count++, make_uint2(me, other_c));
-                    }
-                } else if (dyn.range[ch].y > i && strict_overlap(q, dyn.nodeAabb[ch])) {
-                    if (sp < QUERY_STACK) stack[sp++] = ch;
-                    else atomicOr(status, STATUS_STACK_OVERFLOW);
+                    const uint32_t other_c = dyn.vals[~ch];
+                    if (cbody[other_c] != myBody) emit(count++, make_uint2(me, other_c));
+                } else if (sp < QUERY_STACK) {
+                    stack[sp++] = ch;
+                } else {
+                    atomicOr(status, STATUS_STACK_OVERFLOW);
                 }
             }
         }
@@ -635,16 +639,14 @@ __device__ __forceinline__ uint32_t query_one(const TreeView& dyn, const TreeVie
         stack[sp++] = olo;
         while (sp > 0) {
             const int node = stack[--sp];
-            const int2 c = other.child[node];
+            const NodeRec r = other.rec[node];
 #pragma unroll
             for (int side = 0; side < 2; side++) {
-                const int ch = side == 0 ? c.x : c.y;
-                if (ch < 0) {
-                    if (strict_overlap(q, other.leafAabb[~ch])) emit(count++, make_uint2(me, other.vals[~ch]));
-                } else if (strict_overlap(q, other.nodeAabb[ch])) {
-                    if (sp < QUERY_STACK) stack[sp++] = ch;
-                    else atomicOr(status, STATUS_STACK_OVERFLOW);
-                }
+                const int ch = side == 0 ? r.child.x : r.child.y;
+                if (!strict_overlap(q, r.box[side])) continue;
+                if (ch < 0) emit(count++, make_uint2(me, other.vals[~ch]));
+                else if (sp < QUERY_STACK) stack[sp++] = ch;
+                else atomicOr(status, STATUS_STACK_OVERFLOW);
             }
         }
     }
@@ -828,8 +830,15 @@ __global__ void k_ccd_shift_bodies(DeviceWorld w, const uint32_t* __restrict__ d
 // work lists.
 // ---------------------------------------------------------------------------------------------------------------
 __global__ void k_scan_blocks(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t n,
-                              uint32_t* __restrict__ blockSums)
+                              uint32_t* __restrict__ blockSums, const uint32_t* __restrict__ nDev)
 {
+    // nDev: the element count on the device (at most n, the capacity the grid was sized for); blocks past it only
+    // contribute a zero block sum.
+    if (nDev) n = min(n, *nDev);
+    if (blockIdx.x * SCAN_TILE >= n && blockIdx.x > 0) {
+        if (threadIdx.x == 0 && blockSums) blockSums[blockIdx.x] = 0u;
+        return;
+    }
     __shared__ uint32_t warpSums[SCAN_THREADS / 32];
     const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
     uint32_t v[SCAN_ITEMS];
@@ -863,8 +872,11 @@ __global__ void k_scan_blocks(const uint32_t* __restrict__ in, uint32_t* __restr
     }
 }
 
-__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_t* __restrict__ blockOffsets)
+__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_t* __restrict__ blockOffsets,
+                           const uint32_t* __restrict__ nDev)
 {
+    if (nDev) n = min(n, *nDev);
+    if (blockIdx.x * SCAN_TILE >= n) return;
     const uint32_t add = blockOffsets[blockIdx.x];
     const uint32_t base = blockIdx.x * SCAN_TILE;
     for (uint32_t j = threadIdx.x; j < SCAN_TILE; j += blockDim.x)
