@@ -94,9 +94,10 @@ __global__ void k_compact_manifolds(const Manifold* slots, const uint32_t* hit, 
                                     uint32_t* nOut, StepCounters* counters);
 __global__ void k_warm_insert(const Manifold* prev, const uint32_t* nPrev, unsigned long long* keys,
                               uint32_t* vals, uint32_t capacity, uint32_t* status);
+constexpr uint32_t WARM_CACHED = 0x80000000u;   // contact-cache value flag: the manifold had a non-zero impulse
 __global__ void k_warm_lookup(const Manifold* prev, Manifold* cur, const uint32_t* nCur,
                               const unsigned long long* keys, const uint32_t* vals, uint32_t capacity,
-                              StepCounters* counters);
+                              StepCounters* counters, const uint32_t* prevColor, uint32_t* hint);
 __global__ void k_wake(DeviceWorld w, const Manifold* m, const uint32_t* nM, uint32_t* wakeIsland,
                        StepCounters* counters);
 __global__ void k_wake_apply(DeviceWorld w, const uint32_t* wakeIsland, StepCounters* counters);

@@ -262,6 +262,11 @@ __device__ __forceinline__ uint32_t priority_hash(uint32_t x)
     return x;
 }
 
+// Colour word of a manifold: colour in the low bits, steps it has kept that colour in the high byte.
+constexpr uint32_t COLOR_AGE_SHIFT = 24;
+constexpr uint32_t COLOR_MASK = (1u << COLOR_AGE_SHIFT) - 1u;
+constexpr uint32_t COLOR_KEEP_STEPS = 16;
+
 // Colour counters: one per colour, then the lengths of the two uncoloured lists, then the colour count.
 constexpr uint32_t COLOR_SLOTS = MAX_COLORS + 4;
 // Colours 0..63 are chosen first-fit from a body's 64-bit mask of neighbouring colours; a manifold whose bodies see
@@ -281,6 +286,7 @@ struct SolveScratch {
     uint4* listA;                     // [manifolds] uncoloured manifold records, ping
     uint4* listB;                     // [manifolds] uncoloured manifold records, pong
     uint2* pairBodies;                // [manifolds] the two bodies, bit 31 set when the body is dynamic
+    const uint32_t* hint;             // [manifolds] colour of the same contact pair last step (NO_COLOR: none), or null
 };
 
 // Team barriers. ld() reads a colour counter written by other team members before the last barrier: global memory
@@ -371,6 +377,12 @@ __device__ __forceinline__ void prefetch_colour(const SolveScratch& s, uint32_t 
 // conflict-free and depend only on the manifold list and priorities. Each round visits only the manifolds still
 // uncoloured (compacted into a list whose order does not affect the result). rank/size: this thread's index in the
 // team. Returns false if the colouring ran out of colours or a barrier gave up.
+// Colouring with carried colours: a manifold whose collider pair was solved last step (its hint) keeps that
+// step's colour when it was a first-fit one (< 64) and has been kept for fewer than COLOR_KEEP_STEPS steps in a
+// row (so each contact's place in the solving order is revisited regularly). Two kept manifolds of one colour
+// cannot share a dynamic body: their predecessors were coloured together last step, and a body's dynamic flag
+// (finite mass) does not change between steps. The other manifolds run the Jones-Plassmann rounds around the kept
+// colours. With no hints every manifold runs the rounds. s.color holds colour | age << COLOR_AGE_SHIFT.
 template <class Sync, class Bodies>
 __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold* __restrict__ m, uint32_t n,
                                 const SolveScratch& s, uint32_t velIters, uint32_t posIters, uint32_t rank,
@@ -378,17 +390,36 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
                                 ConsSmem cs = ConsSmem{})
 {
     for (uint32_t c = rank; c < COLOR_SLOTS; c += size) s.colorCount[c] = 0;
-    // Each manifold's two bodies and whether they are dynamic, looked up once for all colouring rounds.
-    constexpr uint32_t DYN = 0x80000000u;
+    uint32_t* const nColors = s.colorCount + MAX_COLORS + 3;
+    // Each manifold's two bodies and whether they are dynamic, looked up once for all colouring rounds; kept
+    // colours are counted and marked around their bodies here.
+    constexpr uint32_t DYN = 0x80000000u, KEPT = 0x40000000u;
+    if (s.hint && !sync()) return false;   // the counters are zeroed before kept colours are counted
+    uint32_t keptTop = 0;
     for (uint32_t i = rank; i < n; i += size) {
         const uint32_t bA = w.cbody[m[i].a], bB = w.cbody[m[i].b];
-        s.pairBodies[i] = make_uint2(bA | (B.invMass(bA) > 0.0f ? DYN : 0u), bB | (B.invMass(bB) > 0.0f ? DYN : 0u));
+        const bool dA = B.invMass(bA) > 0.0f, dB = B.invMass(bB) > 0.0f;
+        const uint32_t hw = s.hint ? s.hint[i] : NO_COLOR;
+        const uint32_t h = hw & COLOR_MASK, age = hw >> COLOR_AGE_SHIFT;
+        const bool kept = hw != NO_COLOR && h < 64 && age + 1 < COLOR_KEEP_STEPS;
+        if (kept) {
+            s.color[i] = h | (age + 1) << COLOR_AGE_SHIFT;
+            atomicAdd(s.colorCount + h, 1u);
+            keptTop = max(keptTop, h + 1);
+            if (dA) atomicOr(B.maskWord(bA), 1ull << h);
+            if (dB) atomicOr(B.maskWord(bB), 1ull << h);
+        }
+        s.pairBodies[i] = make_uint2(bA | (dA ? DYN : 0u) | (kept ? KEPT : 0u), bB | (dB ? DYN : 0u));
+    }
+    if (s.hint) {
+        for (int o = 16; o > 0; o >>= 1) keptTop = max(keptTop, __shfl_xor_sync(0xffffffffu, keptTop, o));
+        if ((threadIdx.x & 31) == 0 && keptTop) atomicMax(nColors, keptTop);
     }
     if (!sync()) return false;
-    uint32_t* const nColors = s.colorCount + MAX_COLORS + 3;
     uint32_t len = n;
     const uint4* in = nullptr;   // round 0 visits every manifold; later rounds the uncoloured records
-    // Record j of this round: {manifold, priority, body A | dynamic bit, body B | dynamic bit}.
+    // Record j of this round: {manifold, priority, body A | dynamic bit, body B | dynamic bit}. In round 0 a kept
+    // manifold's record carries the KEPT bit and takes no part.
     auto rec = [&](uint32_t j) -> uint4 {
         if (in) return in[j];
         const uint2 pb = s.pairBodies[j];
@@ -408,6 +439,7 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
 #pragma unroll
             for (uint32_t u = 0; u < BATCH; u++) {
                 if (j0 + u * size >= len) break;
+                if (e[u].z & KEPT) continue;
                 const unsigned long long key = tag | e[u].y;
                 if (e[u].z & DYN) atomicMax(B.maxWord(e[u].z & ~DYN), key);
                 if (e[u].w & DYN) atomicMax(B.maxWord(e[u].w & ~DYN), key);
@@ -422,6 +454,7 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
 #pragma unroll
             for (uint32_t u = 0; u < BATCH; u++) {
                 if (j0 + u * size >= len) break;
+                if (e[u].z & KEPT) continue;
                 const uint32_t i = e[u].x;
                 const unsigned long long key = tag | e[u].y;
                 const uint32_t bA = e[u].z & ~DYN, bB = e[u].w & ~DYN;
@@ -458,7 +491,7 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
     }
     if (!sync()) return false;
     for (uint32_t i = rank; i < n; i += size) {
-        const uint32_t c = s.color[i];
+        const uint32_t c = s.color[i] & COLOR_MASK;
         s.order[Sync::ld(s.colorStart + c) + atomicAdd(s.colorCount + c, 1u)] = i;
     }
     if (!sync()) return false;

@@ -223,7 +223,7 @@ enum StagedSection : uint32_t {
     SEC_VEL, SEC_POS, SEC_ROT, SEC_WRAP, SEC_BOUND, SEC_TIMER, SEC_STATE, SEC_ISLAND,
     SEC_CBODY, SEC_CSHAPE, SEC_CMAT, SEC_COFF, SEC_CPOSE, SEC_CAABB, SEC_CROT, SEC_MINEXT,
     SEC_CIRCLE, SEC_BOXHALF, SEC_POLYOFF, SEC_POLYCOUNT, SEC_POLYVERTS, SEC_POLYNORMALS, SEC_MATS, SEC_PREV,
-    NSEC
+    SEC_PREVCOLOR, NSEC
 };
 struct StagedWorld {
     WorldExtent ext;
@@ -239,6 +239,7 @@ struct PackedArrays {
     std::vector<uint8_t> state;
     std::vector<uint32_t> isl, cb, cs, cm, po, pc;
     std::vector<Manifold> prev;
+    std::vector<uint32_t> pcol;   // colour of each warm-start manifold (empty: none known)
     std::vector<float4> cp;   // collider world poses at the end of the last step (empty: never stepped, zeros)
 
     // Appends another world, shifting its body, collider, shape, vertex and material indices past this one's.
@@ -262,6 +263,8 @@ struct PackedArrays {
         for (uint32_t v : o.po) po.push_back(v + vert);
         cat(pc, o.pc); cat(pv, o.pv); cat(pn, o.pn); cat(mats, o.mats);
         for (Manifold m : o.prev) { m.a += cof; m.b += cof; prev.push_back(m); }
+        if (o.pcol.size() == o.prev.size()) cat(pcol, o.pcol);
+        else pcol.insert(pcol.end(), o.prev.size(), NO_COLOR);
         if (!o.cp.empty() || !cp.empty()) {
             cp.resize(cof, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
             if (o.cp.empty()) cp.resize(cof + o.cb.size(), make_float4(0.0f, 0.0f, 0.0f, 0.0f));
@@ -293,7 +296,7 @@ StagedWorld stage_world(const PackedArrays& a)
         e.col * 4, e.col * 4, e.col * 4, e.col * sizeof(float4), e.col * sizeof(float4), e.col * sizeof(float4),
         e.col * 4, e.col * 4,
         e.circle * 4, e.box * sizeof(float2), e.poly * 4, e.poly * 4, e.vert * sizeof(float2), e.vert * sizeof(float2),
-        e.mat * sizeof(float4), e.man * sizeof(Manifold)};
+        e.mat * sizeof(float4), e.man * sizeof(Manifold), e.man * 4};
     uint64_t off = 0;
     for (uint32_t k = 0; k < NSEC; k++) {
         w.sec[k] = off;
@@ -312,6 +315,8 @@ StagedWorld stage_world(const PackedArrays& a)
     put(SEC_CIRCLE, a.cr.data()); put(SEC_BOXHALF, a.bh.data()); put(SEC_POLYOFF, a.po.data());
     put(SEC_POLYCOUNT, a.pc.data()); put(SEC_POLYVERTS, a.pv.data()); put(SEC_POLYNORMALS, a.pn.data());
     put(SEC_MATS, a.mats.data()); put(SEC_PREV, a.prev.data());
+    if (a.pcol.size() == e.man) put(SEC_PREVCOLOR, a.pcol.data());
+    else if (e.man) std::memset(w.blob.data() + w.sec[SEC_PREVCOLOR], 0xFF, sizes[SEC_PREVCOLOR]);   // NO_COLOR
     return w;
 }
 
@@ -422,6 +427,10 @@ struct ag2d_world {
     DBuf<uint32_t> hashVals;
     // Colouring and solver.
     DBuf<uint32_t> color, colorCount, colorStart, order, bar, prio;
+    // Colour of each warm-start manifold (NO_COLOR: unknown), swapped with 'color' after each step; the warm-start
+    // lookup turns it into this step's colouring hints (written into 'color').
+    DBuf<uint32_t> prevColor;
+    bool hintsReady = false;   // this step's lookup wrote the hints
     DBuf<uint4> listA, listB;
     DBuf<unsigned long long> bodyMax, bodyMask;
     DBuf<Constraint> cons;
@@ -431,17 +440,17 @@ struct ag2d_world {
     // World partition of a batch (nWorlds == 1: a single world, none of these is used).
     uint32_t nWorlds = 1;
     uint32_t teamColliders = 1024;         // solver team size: consecutive worlds packed up to this many colliders
-    uint32_t teamThreads = 128;            // CTA size of the team solver
+    uint32_t teamThreads = 256;            // CTA size of the team solver
     uint32_t teamBodyCap = 2048;           // bodies of a team staged in shared memory (larger teams use global)
     uint32_t teamConsCap = 0;              // constraint records a team keeps in shared memory (more: global)
     uint32_t bigConsCap = 0;
-    bool consOnChip = true;                // team constraint records in shared memory when they fit (tunable)
+    bool consOnChip = false;               // team constraint records in shared memory when they fit (tunable)
     uint32_t nTeams = 0;
     uint32_t teamBlocks = 1;               // co-resident CTAs of the team solver at this shared-memory size
     uint32_t nBigTeams = 0, bigBodyCap = 0, bigBlocks = 1;   // worlds larger than a team, one CTA each
     cudaStream_t sideStream = nullptr;     // the big-world solver runs here, beside the small-team solver
     cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
-    uint32_t queryThreads = 128;           // block sizes of the pair query and the narrow phase (tunable)
+    uint32_t queryThreads = 256;           // block sizes of the pair query and the narrow phase (tunable)
     uint32_t narrowThreads = 256;
     std::vector<uint32_t> hBodyStart, hColStart;     // [nWorlds + 1]
     DBuf<uint32_t> bodyWorld, colWorld, worldBodyStart, worldColStart, manSeg, nextWorld, worldDirty;
@@ -457,6 +466,7 @@ struct ag2d_world {
     DBuf<uint8_t> bk_bstate, staging, out_state;
     DBuf<uint32_t> bk_island, bk_cbody, bk_cshape, bk_cmat, bk_polyOff, bk_polyCount, newWorldMask;
     DBuf<Manifold> bk_prev;
+    DBuf<uint32_t> bk_prevColor;
     DBuf<unsigned long long> stagedSections;   // [joining world][section] byte offsets into 'staging'
     DBuf<GatherSeg> gatherSegs;
     bool newWorldsPending = false;   // joined worlds take a full pose pass in their first step
@@ -673,6 +683,7 @@ struct ag2d_world {
         run(polyNormals, bk_polyNormals, SEC_POLYNORMALS, 5, GATHER_PLAIN);
         run(materials, bk_mats, SEC_MATS, 6, GATHER_PLAIN);
         run(prevManifolds, bk_prev, SEC_PREV, 7, GATHER_PLAIN);
+        run(prevColor, bk_prevColor, SEC_PREVCOLOR, 7, GATHER_PLAIN);
         mark("gather");
         // Sizes, partition and per-world state.
         worldExt = next;
@@ -781,6 +792,7 @@ struct ag2d_world {
         nBodies = b; nColliders = b; nWorlds = worlds;
         sizeFor();
         bk_prev.reserve(manifoldCap);
+        bk_prevColor.reserve(manifoldCap);
         nBodies = saveB; nColliders = saveC; nWorlds = saveW;
         CK(cudaStreamSynchronize(stream));
     }
@@ -952,6 +964,13 @@ struct ag2d_world {
         };
         grow_keep(manifolds, manifoldCap);
         grow_keep(prevManifolds, manifoldCap);
+        if (prevColor.n < manifoldCap || !prevColor.p) {   // colours of the warm-start manifolds are kept too
+            DBuf<uint32_t> nb;
+            nb.reserve(manifoldCap);
+            if (prevColor.p) CK(cudaMemcpyAsync(nb.p, prevColor.p, prevColor.n * 4, cudaMemcpyDeviceToDevice, stream));
+            CK(cudaStreamSynchronize(stream));
+            swap_bufs(prevColor, nb);
+        }
         color.reserve(manifoldCap);
         order.reserve(manifoldCap);
         prio.reserve(manifoldCap);
@@ -1109,6 +1128,7 @@ struct ag2d_world {
         CK(cudaMemcpyAsync(&np, nPrev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         get(a.prev, prevManifolds.p, np);
+        get(a.pcol, prevColor.p, np);
         CK(cudaStreamSynchronize(s));
     }
 
@@ -1368,7 +1388,8 @@ struct ag2d_world {
         k_warm_insert<<<gridFor(manifoldCap), 256, 0, s>>>(prevManifolds.p, nPrev.p, hashKeys.p, hashVals.p, slotsUsed,
                                                            &dCounters.p->status);
         k_warm_lookup<<<gridFor(manifoldCap), 256, 0, s>>>(prevManifolds.p, manifolds.p, nManifolds.p, hashKeys.p,
-                                                           hashVals.p, slotsUsed, dCounters.p);
+                                                           hashVals.p, slotsUsed, dCounters.p, prevColor.p, color.p);
+        hintsReady = true;
         CK(cudaGetLastError());
         pend(7);
     }
@@ -1395,7 +1416,8 @@ struct ag2d_world {
         Manifold* mm = manifolds.p;
         const uint32_t* nm = nManifolds.p;
         SolveScratch scratch{color.p, order.p, bodyMax.p, bodyMask.p, colorCount.p, colorStart.p, cons.p, nullptr,
-                             listA.p, listB.p, pairBodies.p};
+                             listA.p, listB.p, pairBodies.p, hintsReady ? color.p : nullptr};
+        hintsReady = false;
         uint32_t vi = settings.velocity_iterations, pi = settings.position_iterations;
         StepCounters* ctr = dCounters.p;
         pbegin(10);
@@ -1634,6 +1656,7 @@ struct ag2d_world {
             fullPose = false;
             // The solved manifolds become the next step's warm-start source.
             swap_bufs(manifolds, prevManifolds);
+            swap_bufs(color, prevColor);   // this step's colours: next step's hints
             newWorldsPending = false;
             manSegFresh = nWorlds > 1;
             CK(cudaMemcpyAsync(nPrev.p, nManifolds.p, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
@@ -2277,6 +2300,8 @@ int32_t ag2d_batch_create(ag2d_world* const* worlds, uint32_t count, ag2d_batch*
         const uint32_t np = uint32_t(all.prev.size());
         if (np > e.manifoldCap) e.reserveCapacities(std::max(np, e.pairCap), np);
         if (np) CK(cudaMemcpyAsync(e.prevManifolds.p, all.prev.data(), np * sizeof(Manifold), cudaMemcpyHostToDevice,
+                                   e.stream));
+        if (np) CK(cudaMemcpyAsync(e.prevColor.p, all.pcol.data(), np * sizeof(uint32_t), cudaMemcpyHostToDevice,
                                    e.stream));
         CK(cudaMemcpyAsync(e.nPrev.p, &np, sizeof(uint32_t), cudaMemcpyHostToDevice, e.stream));
         e.prevCount = np;

@@ -120,10 +120,11 @@ __global__ void k_compact_manifolds(const Manifold* __restrict__ slots, const ui
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// Warm start: the previous step's manifolds with a non-zero impulse on an active contact go into an
-// open-addressing table keyed by the unordered collider pair (rebuildContactCache, NarrowPhaseCollisionDetector.cpp:
-// 272-297; makePairKey .h:216-219); each new manifold of the same ordered pair takes the impulses of the previous
-// contacts with equal ids (finalizeResults, :749-766).
+// Warm start: the previous step's manifolds go into an open-addressing table keyed by the unordered collider pair,
+// those with a non-zero impulse on an active contact flagged (bit 31 of the value: the reference caches only these,
+// rebuildContactCache, NarrowPhaseCollisionDetector.cpp:272-297; makePairKey .h:216-219); each new manifold of the
+// same ordered pair takes the flagged manifold's impulses of the contacts with equal ids (finalizeResults,
+// :749-766). Every new manifold whose pair was there also takes that manifold's colour as its colouring hint.
 // ---------------------------------------------------------------------------------------------------------------
 __device__ __forceinline__ unsigned long long pair_key(uint32_t a, uint32_t b)
 {
@@ -146,13 +147,12 @@ __global__ void k_warm_insert(const Manifold* __restrict__ prev, const uint32_t*
         uint32_t mask = uint32_t(m.jn0 != 0.0f) | uint32_t(m.jt0 != 0.0f) << 1 | uint32_t(m.jn1 != 0.0f) << 2 |
                         uint32_t(m.jt1 != 0.0f) << 3;
         mask &= (1u << (2u * m.count)) - 1u;
-        if (!mask) continue;
         const unsigned long long key = pair_key(m.a, m.b);
         uint32_t s = slot_of(key, capacity);
         uint32_t probes = 0;
         for (;;) {
             const unsigned long long old = atomicCAS(keys + s, ~0ull, key);
-            if (old == ~0ull || old == key) { vals[s] = i; break; }
+            if (old == ~0ull || old == key) { vals[s] = i | (mask ? WARM_CACHED : 0u); break; }
             s = (s + 1) & (capacity - 1u);
             if (++probes >= capacity) { atomicOr(status, STATUS_HASH_FULL); break; }
         }
@@ -161,7 +161,8 @@ __global__ void k_warm_insert(const Manifold* __restrict__ prev, const uint32_t*
 
 __global__ void k_warm_lookup(const Manifold* __restrict__ prev, Manifold* __restrict__ cur,
                               const uint32_t* __restrict__ nCur, const unsigned long long* __restrict__ keys,
-                              const uint32_t* __restrict__ vals, uint32_t capacity, StepCounters* counters)
+                              const uint32_t* __restrict__ vals, uint32_t capacity, StepCounters* counters,
+                              const uint32_t* __restrict__ prevColor, uint32_t* __restrict__ hint)
 {
     const uint32_t n = *nCur;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -175,7 +176,9 @@ __global__ void k_warm_lookup(const Manifold* __restrict__ prev, Manifold* __res
             if (k == ~0ull) break;
             s = (s + 1) & (capacity - 1u);
         }
-        if (idx == NO_COLOR) continue;
+        if (hint) hint[i] = (idx != NO_COLOR && prevColor) ? prevColor[idx & ~WARM_CACHED] : NO_COLOR;
+        if (idx == NO_COLOR || !(idx & WARM_CACHED)) continue;
+        idx &= ~WARM_CACHED;
         const Manifold p = prev[idx];
         if (p.a != c.a || p.b != c.b) continue;
         bool any = false;
@@ -288,7 +291,8 @@ __global__ void __launch_bounds__(THREADS) k_color_solve_teams(TeamLaunch a)
         for (uint32_t i = lo + threadIdx.x; i < hi; i += THREADS)
             prio[i] = priority_hash(i - a.manSeg[w.bodyWorld[w.cbody[m[i].a]]]);
         const SolveScratch ls{a.s.color + lo, a.s.order + lo, a.s.bodyMax, a.s.bodyMask, colorCount, colorStart,
-                              a.s.cons + lo, prio + lo, a.s.listA + lo, a.s.listB + lo, a.s.pairBodies + lo};
+                              a.s.cons + lo, prio + lo, a.s.listA + lo, a.s.listB + lo, a.s.pairBodies + lo,
+                              a.s.hint ? a.s.hint + lo : nullptr};
         const uint32_t b0 = w.worldBodyStart[w0], nb = w.worldBodyStart[w1] - b0;
         if (nb <= a.bodyCap) {
             float4* vel = teamCache;
