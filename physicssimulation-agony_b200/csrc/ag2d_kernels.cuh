@@ -67,9 +67,11 @@ __global__ void k_sort_pass(const uint32_t* keysIn, const uint32_t* valsIn, uint
                             uint32_t n, uint32_t shift, const uint32_t* digitBase, uint32_t* tileState,
                             uint32_t* tileCounter, uint32_t* status);
 __global__ void k_lbvh_build(const uint32_t* keys, const uint32_t* sortedWorld, const uint32_t* segStart, int n,
-                             int2* child, int2* range, int* parent, int* leafParent, uint32_t* visit, NodeRec* rec);
+                             int2* child, int2* range, int* parent, int* leafParent, float4* meet, NodeRec* rec);
 __global__ void k_lbvh_refit(int n, const int2* child, const int* parent, const int* leafParent,
-                             const float4* leafAabb, float4* nodeAabb, uint32_t* visit, NodeRec* rec);
+                             const float4* leafAabb, float4* nodeAabb, float4* meet, NodeRec* rec);
+// Empty marker of a refit meeting slot (min x bits): a NaN no arithmetic produces.
+constexpr uint32_t MEET_EMPTY = 0xFFFFFFFFu;
 __global__ void k_query_stash(TreeView dyn, TreeView other, const uint32_t* cbody, uint32_t* counts, uint2* stash,
                               uint32_t* status);
 __global__ void k_query_emit(TreeView dyn, TreeView other, const uint32_t* cbody, const uint32_t* counts,

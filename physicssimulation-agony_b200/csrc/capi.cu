@@ -149,7 +149,8 @@ struct Tree {
     DBuf<int> parent, leafParent;
     DBuf<float4> leafAabb, nodeAabb;
     DBuf<NodeRec> rec;
-    DBuf<uint32_t> visit, bounds, hist, tileState, tileCounter;
+    DBuf<float4> meet;   // refit meeting slots, one per internal node
+    DBuf<uint32_t> bounds, hist, tileState, tileCounter;
     // World-segmented trees: Morton key per collider, sorted keys / worlds, segment starts (filled with the lists).
     DBuf<uint32_t> keyOf, sortedKey, sortedWorld, segStart;
     uint32_t worlds = 1;
@@ -159,7 +160,7 @@ struct Tree {
         worlds = nWorlds;
         keys.reserve(cap); vals.reserve(cap); keys2.reserve(cap); vals2.reserve(cap);
         child.reserve(cap); range.reserve(cap); parent.reserve(cap); leafParent.reserve(cap);
-        leafAabb.reserve(cap); nodeAabb.reserve(cap); visit.reserve(cap); rec.reserve(cap);
+        leafAabb.reserve(cap); nodeAabb.reserve(cap); meet.reserve(cap); rec.reserve(cap);
         bounds.reserve(4 * size_t(nWorlds)); hist.reserve(4 * 256); tileCounter.reserve(4);
         tileState.reserve(size_t(div_up(std::max<uint32_t>(cap, 1), SORT_TILE)) * 256 * 4);
         if (nWorlds > 1) {
@@ -1290,11 +1291,11 @@ struct ag2d_world {
                                                   t.leafAabb.p);
         k_lbvh_build<<<gridFor(n), 256, 0, s>>>(seg ? t.sortedKey.p : t.keys.p, seg ? t.sortedWorld.p : nullptr,
                                                  seg ? t.segStart.p : nullptr, int(n), t.child.p, t.range.p,
-                                                 t.parent.p, t.leafParent.p, t.visit.p, t.rec.p);
+                                                 t.parent.p, t.leafParent.p, t.meet.p, t.rec.p);
         CK(cudaGetLastError());
         if (n > 1) {
             k_lbvh_refit<<<gridFor(n), 256, 0, s>>>(int(n), t.child.p, t.parent.p, t.leafParent.p, t.leafAabb.p,
-                                                     t.nodeAabb.p, t.visit.p, t.rec.p);
+                                                     t.nodeAabb.p, t.meet.p, t.rec.p);
             CK(cudaGetLastError());
         }
         if (isDyn) pend(13);

@@ -498,7 +498,7 @@ __device__ __forceinline__ int lbvh_delta(const uint32_t* keys, int lo, int hi, 
 __global__ void k_lbvh_build(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ sortedWorld,
                              const uint32_t* __restrict__ segStart, int n, int2* __restrict__ child,
                              int2* __restrict__ range, int* __restrict__ parent, int* __restrict__ leafParent,
-                             uint32_t* __restrict__ visit, NodeRec* __restrict__ rec)
+                             float4* __restrict__ meet, NodeRec* __restrict__ rec)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int lo = 0, hi = n;
@@ -509,7 +509,7 @@ __global__ void k_lbvh_build(const uint32_t* __restrict__ keys, const uint32_t* 
         }
         if (hi - lo == 1) leafParent[i] = -1;
         if (i >= hi - 1) continue;
-        visit[i] = 0;
+        meet[i] = make_float4(__uint_as_float(MEET_EMPTY), 0.0f, 0.0f, 0.0f);
         if (i == lo) parent[i] = -1;
         const int d = (lbvh_delta(keys, lo, hi, i, i + 1) - lbvh_delta(keys, lo, hi, i, i - 1)) >= 0 ? 1 : -1;
         const int dmin = lbvh_delta(keys, lo, hi, i, i - d);
@@ -538,10 +538,26 @@ __global__ void k_lbvh_build(const uint32_t* __restrict__ keys, const uint32_t* 
     }
 }
 
-// Bottom-up AABB refit: the second thread to reach a node merges its children (BvhTree::fitNodes equivalent).
+// Swaps a box into a node's meeting slot with one 16-byte atomic and returns what was there.
+__device__ __forceinline__ float4 exchange_box(float4* slot, float4 v)
+{
+    const unsigned long long lo = uint64_t(__float_as_uint(v.x)) | uint64_t(__float_as_uint(v.y)) << 32;
+    const unsigned long long hi = uint64_t(__float_as_uint(v.z)) | uint64_t(__float_as_uint(v.w)) << 32;
+    unsigned long long rlo, rhi;
+    asm volatile("{\n\t.reg .b128 d, s;\n\tmov.b128 s, {%2, %3};\n\t"
+                 "atom.relaxed.gpu.global.exch.b128 d, [%4], s;\n\tmov.b128 {%0, %1}, d;\n\t}"
+                 : "=l"(rlo), "=l"(rhi) : "l"(lo), "l"(hi), "l"(slot) : "memory");
+    return make_float4(__uint_as_float(uint32_t(rlo)), __uint_as_float(uint32_t(rlo >> 32)),
+                       __uint_as_float(uint32_t(rhi)), __uint_as_float(uint32_t(rhi >> 32)));
+}
+
+// Bottom-up AABB refit (BvhTree::fitNodes equivalent). The two subtrees of a node meet in its slot: each swaps its
+// bounds in with one 16-byte atomic exchange; the first finds the empty marker and stops, the second receives its
+// sibling's bounds in the same operation (no flag, fence or second load on the chain), writes the node's record
+// and bounds and carries on upwards.
 __global__ void k_lbvh_refit(int n, const int2* __restrict__ child, const int* __restrict__ parent,
                              const int* __restrict__ leafParent, const float4* __restrict__ leafAabb,
-                             float4* __restrict__ nodeAabb, uint32_t* __restrict__ visit, NodeRec* __restrict__ rec)
+                             float4* __restrict__ nodeAabb, float4* __restrict__ meet, NodeRec* __restrict__ rec)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int node = leafParent[i];   // -1 for the leaf of a one-collider segment
@@ -551,18 +567,13 @@ __global__ void k_lbvh_refit(int n, const int2* __restrict__ child, const int* _
             // The tree links do not depend on the arrival: fetch them before the atomic.
             const int2 c = child[node];
             const int up = parent[node];
-            // This subtree's bounds go into the parent's traversal record before the arrival.
+            const float4 o = exchange_box(meet + node, box);
+            if (__float_as_uint(o.x) == MEET_EMPTY) break;   // first arrival: the sibling carries on
             const int side = c.x == self ? 0 : 1;
-            __stcg(&rec[node].box[side], box);
-            // One acq_rel arrival: releases this thread's record write and, for the second arrival, acquires the
-            // sibling's. Only the sibling's bounds are loaded; this thread's own are in registers.
-            uint32_t arrived;
-            asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
-                         : "=r"(arrived) : "l"(visit + node) : "memory");
-            if (arrived == 0) break;
-            const float4 o = __ldcg(&rec[node].box[side ^ 1]);
             const float4 a = side == 0 ? box : o;
             const float4 b = side == 0 ? o : box;
+            __stcg(&rec[node].box[0], a);
+            __stcg(&rec[node].box[1], b);
             box = make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fmaxf(a.z, b.z), fmaxf(a.w, b.w));
             __stcg(nodeAabb + node, box);
             self = node;
