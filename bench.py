@@ -295,6 +295,19 @@ def reduce_sum(torch, dist, world_size, dev, value):
     return float(t.item())
 
 
+def job_rate(torch, dist, world_size, dev, units, seconds):
+    """Whole-job rate: the units all ranks processed over the slowest rank's time. Returns (rate, slowest seconds,
+    total units)."""
+    slowest = reduce_max(torch, dist, world_size, dev, seconds)
+    total = reduce_sum(torch, dist, world_size, dev, float(units))
+    return total / slowest, slowest, total
+
+
+def rank_seed(rank, per_rank):
+    """First seed of a rank's worlds or requests: ranks draw disjoint seed ranges."""
+    return rank * per_rank
+
+
 # ---------------------------------------------------------------------------------------------------------------
 # CPU baselines: the reference engine (oracle/_ref) on the host cores
 # ---------------------------------------------------------------------------------------------------------------
@@ -450,7 +463,7 @@ def run_reference(args):
 # ---------------------------------------------------------------------------------------------------------------
 def run_c4(args, torch, dist, rank, world_size, local, dev):
     import ag2d
-    scene_list = c4_scenes(args.worlds, rank * args.worlds)
+    scene_list = c4_scenes(args.worlds, rank_seed(rank, args.worlds))
     n_bodies = int(sum(s.n for s in scene_list))
     settings = dict(dt=scene_list[0].dt, velocity_iterations=8, position_iterations=3, gravity=scene_list[0].gravity,
                     device=local)
@@ -492,9 +505,8 @@ def run_c4(args, torch, dist, rank, world_size, local, dev):
     clocks = sampler.stop()
     c1 = e.counters()
     K = args.steps
-    max_ms = reduce_max(torch, dist, world_size, dev, total_ms)
-    job_bodies = reduce_sum(torch, dist, world_size, dev, float(n_bodies))
-    value = job_bodies * K / (max_ms / 1e3)
+    value, max_s, job_steps = job_rate(torch, dist, world_size, dev, n_bodies * K, total_ms / 1e3)
+    max_ms, job_bodies = max_s * 1e3, job_steps / K
     phases = e.phase_times()
     msb = mean_shape_bytes(scene_list)
     bytes_by_phase = step_bytes(msb, sums["pairs"], sums["manifolds"], n_bodies - len(scene_list), K)
@@ -733,8 +745,8 @@ def run_c5(args, torch, dist, rank, world_size, local, dev):
     import ag2d
     import numpy as np
     n_req = args.requests
-    scene_list = c5_requests(n_req, rank * 1_000_003)
-    warm_list = c5_requests(32, rank * 1_000_003 + 777)
+    scene_list = c5_requests(n_req, rank_seed(rank, 1_000_003))
+    warm_list = c5_requests(32, rank_seed(rank, 1_000_003) + 777)
     arrivals = poisson_arrivals(n_req, args.rate, rank)
     settings = dict(dt=scene_list[0].dt, velocity_iterations=8, position_iterations=3,
                     gravity=scene_list[0].gravity, ccd=True, device=local)
@@ -783,9 +795,7 @@ def run_c5(args, torch, dist, rank, world_size, local, dev):
     lat = np.array([server.poll(i)[1] for i in ids])
     bodies = int(sum(sc.n for sc in scene_list))
     body_steps = bodies * args.steps
-    max_wall = reduce_max(torch, dist, world_size, dev, wall)
-    job = reduce_sum(torch, dist, world_size, dev, float(body_steps))
-    value = job / max_wall
+    value, max_wall, job = job_rate(torch, dist, world_size, dev, body_steps, wall)
     p50, p99 = float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
     served_rate = n_req / wall
     cpu = None
