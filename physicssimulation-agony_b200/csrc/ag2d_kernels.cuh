@@ -66,6 +66,11 @@ __global__ void k_sort_digit_scan(uint32_t* hist);
 __global__ void k_sort_pass(const uint32_t* keysIn, const uint32_t* valsIn, uint32_t* keysOut, uint32_t* valsOut,
                             uint32_t n, uint32_t shift, const uint32_t* digitBase, uint32_t* tileState,
                             uint32_t* tileCounter, uint32_t* status);
+// Segments up to SEGMENT_SORT_MAX keys are sorted in shared memory (k_segment_sort), in two size classes.
+constexpr uint32_t SEGMENT_SORT_SMALL = 2048;
+constexpr uint32_t SEGMENT_SORT_MAX = 16384;
+__global__ void k_segment_sort(const uint32_t* keysIn, const uint32_t* valsIn, uint32_t* keysOut, uint32_t* valsOut,
+                               const uint32_t* segStart, uint32_t worlds, uint32_t minSize, uint32_t maxSize);
 __global__ void k_lbvh_build(const uint32_t* keys, const uint32_t* sortedWorld, const uint32_t* segStart, int n,
                              int2* child, int2* range, int* parent, int* leafParent, float4* meet, NodeRec* rec);
 __global__ void k_lbvh_refit(int n, const int2* child, const int* parent, const int* leafParent,

@@ -444,6 +444,8 @@ struct ag2d_world {
     uint32_t teamThreads = 256;            // CTA size of the team solver
     uint32_t teamBodyCap = 2048;           // bodies of a team staged in shared memory (larger teams use global)
     uint32_t teamConsCap = 0;              // constraint records a team keeps in shared memory (more: global)
+    uint32_t maxWorldCols = 0;             // colliders of the largest world of a batch (segmented-sort class)
+    bool segSortReady = false;
     uint32_t bigConsCap = 0;
     bool consOnChip = false;               // team constraint records in shared memory when they fit (tunable)
     uint32_t nTeams = 0;
@@ -804,6 +806,8 @@ struct ag2d_world {
     {
         teamColliders = colliders;
         teamThreads = threads;
+        maxWorldCols = 0;
+        for (uint32_t k = 0; k < nWorlds; k++) maxWorldCols = std::max(maxWorldCols, hColStart[k + 1] - hColStart[k]);
         teamBodyCap = std::min<uint32_t>(MAX_TEAM_BODY_CAP, colliders);
         // Constraint records kept on chip: room for 3 manifolds per collider (a settled pile of convex bodies has
         // about 1.5 on average, with denser worlds well above), within the CTA's shared-memory limit; a team with
@@ -1274,8 +1278,30 @@ struct ag2d_world {
         CK(cudaGetLastError());
         const bool isDyn = &t == &dynTree;
         if (isDyn) pbegin(12);
-        sortPasses(t, n, 4);
-        if (seg) {
+        if (seg && maxWorldCols <= SEGMENT_SORT_MAX) {
+            // Every world's segment sorted in shared memory, small and large segments by separate launches.
+            if (!segSortReady) {
+                CK(cudaFuncSetAttribute(k_segment_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(SEGMENT_SORT_MAX * sizeof(unsigned long long))));
+                segSortReady = true;
+            }
+            const uint32_t grid = std::min<uint32_t>(W, uint32_t(dev.sms) * 8);
+            k_segment_sort<<<grid, 256, SEGMENT_SORT_SMALL * sizeof(unsigned long long), s>>>(
+                t.keys.p, t.vals.p, t.keys2.p, t.vals2.p, t.segStart.p, W, 0, SEGMENT_SORT_SMALL);
+            launches++;
+            if (maxWorldCols > SEGMENT_SORT_SMALL) {
+                k_segment_sort<<<std::min<uint32_t>(W, uint32_t(dev.sms)), 1024,
+                                 SEGMENT_SORT_MAX * sizeof(unsigned long long), s>>>(
+                    t.keys.p, t.vals.p, t.keys2.p, t.vals2.p, t.segStart.p, W, SEGMENT_SORT_SMALL, SEGMENT_SORT_MAX);
+                launches++;
+            }
+            CK(cudaGetLastError());
+            swap_bufs(t.keys, t.keys2);
+            swap_bufs(t.vals, t.vals2);
+        } else {
+            sortPasses(t, n, 4);
+        }
+        if (seg && maxWorldCols > SEGMENT_SORT_MAX) {
             // Stable passes on the world id: order (world, Morton key, collider).
             uint32_t passes = 1;
             while (passes < 4 && (W - 1) >> (8 * passes)) passes++;

@@ -551,6 +551,48 @@ __device__ __forceinline__ float4 exchange_box(float4* slot, float4 v)
                        __uint_as_float(uint32_t(rhi)), __uint_as_float(uint32_t(rhi >> 32)));
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// Segmented sort of a world-grouped tree list: every world segment [segStart[w], segStart[w + 1]) is sorted by its
+// Morton key in shared memory, one CTA per segment, by a bitonic network over (key << 32 | position) so that equal
+// keys keep their list order: the result equals the stable (world, key, position) order of the global radix passes.
+// A CTA takes only the segments of its size class (minSize, maxSize]; every segment of the list is written to the
+// output arrays by exactly one class.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_segment_sort(const uint32_t* __restrict__ keysIn, const uint32_t* __restrict__ valsIn,
+                               uint32_t* __restrict__ keysOut, uint32_t* __restrict__ valsOut,
+                               const uint32_t* __restrict__ segStart, uint32_t worlds, uint32_t minSize,
+                               uint32_t maxSize)
+{
+    extern __shared__ unsigned long long sortTile[];
+    for (uint32_t w = blockIdx.x; w < worlds; w += gridDim.x) {
+        const uint32_t lo = segStart[w], n = segStart[w + 1] - lo;
+        if (n <= minSize || n > maxSize) continue;
+        uint32_t m = 1;
+        while (m < n) m <<= 1;
+        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x)
+            sortTile[i] = i < n ? (static_cast<unsigned long long>(keysIn[lo + i]) << 32 | i) : ~0ull;
+        __syncthreads();
+        for (uint32_t k = 2; k <= m; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+                    const uint32_t p = i ^ j;
+                    if (p > i) {
+                        const unsigned long long a = sortTile[i], b = sortTile[p];
+                        if ((a > b) == ((i & k) == 0)) { sortTile[i] = b; sortTile[p] = a; }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const unsigned long long e = sortTile[i];
+            keysOut[lo + i] = uint32_t(e >> 32);
+            valsOut[lo + i] = valsIn[lo + uint32_t(e)];
+        }
+        __syncthreads();
+    }
+}
+
 // Bottom-up AABB refit (BvhTree::fitNodes equivalent). The two subtrees of a node meet in its slot: each swaps its
 // bounds in with one 16-byte atomic exchange; the first finds the empty marker and stops, the second receives its
 // sibling's bounds in the same operation (no flag, fence or second load on the chain), writes the node's record
