@@ -422,16 +422,28 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_pass(
             uint32_t prefix = 0;
             int32_t t = int32_t(tile) - 1;
             uint32_t spins = 0;
-            while (t >= 0) {
-                const uint32_t s = state[t * 256 + d];
-                const uint32_t flag = s >> 30;
-                if (flag == 0) {
-                    if (++spins > SPIN_LIMIT) { atomicOr(status, STATUS_LOOKBACK_TIMEOUT); break; }
-                    continue;
+            // Look back over a window of LOOKBACK predecessors per round trip: their states are loaded together,
+            // then summed newest first up to the first inclusive prefix; a tile not yet published restarts the
+            // window at that tile. Tile 0 always publishes an inclusive prefix, so the walk ends there at the latest.
+            // Only a window that makes no progress counts towards the spin limit.
+            constexpr int32_t LOOKBACK = 8;
+            bool done = false;
+            while (!done && t >= 0) {
+                uint32_t s[LOOKBACK];
+#pragma unroll
+                for (int32_t j = 0; j < LOOKBACK; j++) s[j] = t - j >= 0 ? state[(t - j) * 256 + d] : (2u << 30);
+#pragma unroll
+                for (int32_t j = 0; j < LOOKBACK; j++) {
+                    const uint32_t flag = s[j] >> 30;
+                    if (flag == 0) break;   // not published yet: reload from tile t
+                    prefix += s[j] & 0x3FFFFFFFu;
+                    t--;
+                    if (flag == 2) { done = true; break; }
                 }
-                prefix += s & 0x3FFFFFFFu;
-                if (flag == 2) break;
-                t--;
+                if (!done && t >= 0 && (s[0] >> 30) == 0 && ++spins > SPIN_LIMIT) {
+                    atomicOr(status, STATUS_LOOKBACK_TIMEOUT);
+                    break;
+                }
             }
             __threadfence();
             state[tile * 256 + d] = (2u << 30) | (prefix + running);
