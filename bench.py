@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--per-world-sample", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="c4: keep the engine's default launch shapes (shorter runs, e.g. under a profiler)")
     ap.add_argument("--tune-ahead", type=int, default=300,
                     help="c4: steps a copy of the batch runs before the autotuner times launch shapes on it")
     ap.add_argument("--requests", type=int, default=4000, help="c5 arrivals in the timed run")
@@ -477,12 +479,15 @@ def run_c4(args, torch, dist, rank, world_size, local, dev):
     stream = torch.cuda.ExternalStream(e.stream(), device=dev)
     # Launch shapes are tuned on a copy of the batch stepped ahead into the settled part of the run (the contact
     # count of the first steps is far below the later one's); results do not depend on them.
-    ahead = ag2d.Batch(worlds)
-    ahead.step(args.tune_ahead)
-    tuning = ahead.engine.autotune(2)
-    ahead.close()
-    del ahead
-    e.set_tuning(tuning)
+    if args.no_autotune:
+        tuning = None   # the engine's default launch shapes (the settled-state choice on this workload)
+    else:
+        ahead = ag2d.Batch(worlds)
+        ahead.step(args.tune_ahead)
+        tuning = ahead.engine.autotune(2)
+        ahead.close()
+        del ahead
+        e.set_tuning(tuning)
     batch.step(args.warmup)
     e.set_profiling(True)
     c0 = e.counters()

@@ -98,6 +98,27 @@ struct DBuf {
     }
 };
 
+// Page-locked host buffer (grow only): host<->device copies through it are one DMA each, without the driver's
+// staging of pageable memory. Freeing synchronises the device, so it only happens when the buffer grows.
+struct PinnedBuf {
+    uint8_t* p = nullptr;
+    size_t n = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+    ~PinnedBuf() { if (p) cudaFreeHost(p); }
+    void reserve(size_t bytes)
+    {
+        if (bytes <= n && p) return;
+        const size_t c = std::max<size_t>(p ? std::max(bytes, n + n / 2) : bytes, 4096);
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        CK(cudaHostAlloc(reinterpret_cast<void**>(&p), c, cudaHostAllocDefault));
+        n = c;
+    }
+};
+
 template <class T>
 void swap_bufs(DBuf<T>& a, DBuf<T>& b)
 {
@@ -471,6 +492,7 @@ struct ag2d_world {
     DBuf<Manifold> bk_prev;
     DBuf<uint32_t> bk_prevColor;
     DBuf<unsigned long long> stagedSections;   // [joining world][section] byte offsets into 'staging'
+    PinnedBuf hostStage, hostOut;              // page-locked copies of the staged blobs and the leaving bodies
     DBuf<GatherSeg> gatherSegs;
     bool newWorldsPending = false;   // joined worlds take a full pose pass in their first step
     // Shape table sizes of the last upload.
@@ -643,12 +665,14 @@ struct ag2d_world {
             stagedBytes += (add[f]->blob.size() + 255) & ~uint64_t(255);
         }
         staging.reserve(std::max<uint64_t>(stagedBytes, 1));
+        // The blobs are packed into a page-locked buffer and go over in one transfer.
+        hostStage.reserve(std::max<uint64_t>(stagedBytes, 1));
         uint64_t at = 0;
         for (const StagedWorld* w : add) {
-            if (!w->blob.empty())
-                CK(cudaMemcpyAsync(staging.p + at, w->blob.data(), w->blob.size(), cudaMemcpyHostToDevice, s));
+            if (!w->blob.empty()) std::memcpy(hostStage.p + at, w->blob.data(), w->blob.size());
             at += (w->blob.size() + 255) & ~uint64_t(255);
         }
+        if (stagedBytes) CK(cudaMemcpyAsync(staging.p, hostStage.p, stagedBytes, cudaMemcpyHostToDevice, s));
         stagedSections.upload(secOff.data(), secOff.size(), s);
         mark("stage");
         // Gathers into the back buffers, then swap them in front.
@@ -768,10 +792,16 @@ struct ag2d_world {
         CK(launch_gather<float4>(out_pos.p, bpos.p, nullptr, gatherSegs.p, n, total, GATHER_PLAIN, grid, s, nullptr, 0, 0));
         CK(launch_gather<uint8_t>(out_state.p, bstate.p, nullptr, gatherSegs.p, n, total, GATHER_PLAIN, grid, s, nullptr,
                                   0, 0));
-        CK(cudaMemcpyAsync(vel.data(), out_vel.p, total * sizeof(float4), cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(pos.data(), out_pos.p, total * sizeof(float4), cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(state.data(), out_state.p, total, cudaMemcpyDeviceToHost, s));
+        // Through a page-locked buffer: velocities, poses, states back to back.
+        const size_t bv = size_t(total) * sizeof(float4);
+        hostOut.reserve(2 * bv + total);
+        CK(cudaMemcpyAsync(hostOut.p, out_vel.p, bv, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(hostOut.p + bv, out_pos.p, bv, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(hostOut.p + 2 * bv, out_state.p, total, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
+        std::memcpy(vel.data(), hostOut.p, bv);
+        std::memcpy(pos.data(), hostOut.p + bv, bv);
+        std::memcpy(state.data(), hostOut.p + 2 * bv, total);
     }
 
     // Sizes every per-element buffer of a batch for 'bodies' resident bodies (one collider each) up front, so
@@ -791,6 +821,8 @@ struct ag2d_world {
         bodyWorld.reserve(b); colWorld.reserve(b); worldBodyStart.reserve(worlds + 1); worldColStart.reserve(worlds + 1);
         manSeg.reserve(worlds + 1); worldDirty.reserve(worlds); newWorldMask.reserve(worlds);
         staging.reserve(size_t(b) * 64);
+        hostStage.reserve(size_t(b) * 64);
+        hostOut.reserve(size_t(b) * 8);
         const uint32_t saveB = nBodies, saveC = nColliders, saveW = nWorlds;
         nBodies = b; nColliders = b; nWorlds = worlds;
         sizeFor();
