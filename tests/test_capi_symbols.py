@@ -48,3 +48,26 @@ def test_errors_without_a_device_are_reported_not_fatal(lib):
     assert lib.ag2d_world_create(None, None) == -1
     lib.ag2d_last_error_string.restype = ctypes.c_char_p
     assert lib.ag2d_last_error_string()
+
+
+def test_server_errors_are_reported_not_fatal(lib):
+    vp = ctypes.c_void_p
+    lib.ag2d_server_create.argtypes = [vp, vp]
+    assert lib.ag2d_server_create(None, None) == -1
+    for name, args in (("ag2d_server_wait_all", (None, ctypes.c_double(0.0))),
+                       ("ag2d_server_poll", (None, ctypes.c_uint64(1), None, None)),
+                       ("ag2d_server_release", (None, ctypes.c_uint64(1))),
+                       ("ag2d_server_stats_get", (None, None))):
+        assert getattr(lib, name)(*args) == -1, name
+    assert lib.ag2d_server_destroy(None) == 0   # destroying nothing is a no-op, as free(NULL)
+
+
+def test_server_without_a_device_fails_cleanly(lib):
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "physicssimulation-agony_b200"))
+    import ag2d
+    if ag2d.device_count() > 0:
+        pytest.skip("a device is present: the server starts")
+    with pytest.raises(ag2d.Ag2dError) as err:
+        ag2d.Server(memory_budget_bytes=1 << 20)
+    assert err.value.code == ag2d.ERR_NO_DEVICE
