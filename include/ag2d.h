@@ -219,6 +219,21 @@ int32_t ag2d_world_phase_times(ag2d_world* world, double* out_ms, uint64_t* out_
 int32_t ag2d_world_stream(ag2d_world* world, void** out_stream);
 int32_t ag2d_world_body_count(ag2d_world* world, uint32_t* out_bodies, uint32_t* out_colliders);
 
+/* Spatial query, replacing BroadPhaseCollisionDetector::queryCollidersInShape (BroadPhaseCollisionDetector.h:
+ * 189-203, BvhTree.h:110-192) with its AABBQuery and CircleQuery shapes (QueryShapes.h:8-86). Returns the indices,
+ * ascending, of the colliders whose AABB as of the last step's broad phase passes the shape's test (AABB: strict
+ * overlap; circle: closest-point squared distance <= radius^2, radius clamped at 0), among the trees selected by
+ * 'trees' (AG2D_TREE_* bits, by the owner body's state). params: AABB {min_x, min_y, max_x, max_y}; circle
+ * {x, y, radius}. Before the first step after creation or a host-side edit nothing is found (the reference's
+ * trees are empty then). The reference
+ * also adds every collider of a node its shape contains without the collider's own test; the sets differ only for
+ * a collider AABB of zero width or height lying on the query AABB's boundary. out_count receives the full count;
+ * at most 'capacity' indices are written. On a batch's engine the query covers every world of the batch. */
+enum ag2d_tree_flag { AG2D_TREE_DYNAMIC = 1, AG2D_TREE_STATIC = 2, AG2D_TREE_SLEEPING = 4, AG2D_TREE_ALL = 7 };
+enum ag2d_query_shape { AG2D_QUERY_AABB = 0, AG2D_QUERY_CIRCLE = 1 };
+int32_t ag2d_world_query_shape(ag2d_world* world, int32_t shape, const float* params, uint32_t trees,
+                               uint32_t* out_colliders, uint32_t capacity, uint32_t* out_count);
+
 /* Copies a field into caller memory (host). out_bytes receives the field size; pass dst = NULL to query it.
  * Replaces the reference's SoA viewers (ObjectAPI::getBodies/getColliders, ObjectAPI.h:96-101) and
  * Simulation::getBodyCollisionData (Simulation.h:186). */

@@ -99,6 +99,9 @@ class ServerStats(ctypes.Structure):
 
 
 REQUEST_WAITING, REQUEST_RUNNING, REQUEST_DONE = 0, 1, 2
+# enum ag2d_tree_flag / ag2d_query_shape
+TREE_DYNAMIC, TREE_STATIC, TREE_SLEEPING, TREE_ALL = 1, 2, 4, 7
+QUERY_AABB, QUERY_CIRCLE = 0, 1
 
 _P = ctypes.c_void_p
 
@@ -145,6 +148,7 @@ def _load():
     L.ag2d_world_set_profiling.argtypes = [vp, i32]
     L.ag2d_world_autotune.argtypes = [vp, i32, ctypes.POINTER(Tuning)]
     L.ag2d_world_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+    L.ag2d_world_query_shape.argtypes = [vp, i32, vp, u32, vp, u32, ctypes.POINTER(u32)]
     L.ag2d_world_phase_times.argtypes = [vp, vp, vp, i32]
     L.ag2d_world_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.ag2d_batch_create.argtypes = [ctypes.POINTER(vp), u32, ctypes.POINTER(vp)]
@@ -354,6 +358,24 @@ class World:
         t = Tuning()
         _check(lib.ag2d_world_autotune(self.h, steps_per_candidate, ctypes.byref(t)))
         return {n: (float(getattr(t, n)) if k is ctypes.c_float else int(getattr(t, n))) for n, k in Tuning._fields_}
+
+    def _query(self, shape, params, trees):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        n = ctypes.c_uint32()
+        _check(lib.ag2d_world_query_shape(self.h, shape, p.ctypes.data, trees, None, 0, ctypes.byref(n)))
+        out = np.empty(max(int(n.value), 1), np.uint32)
+        _check(lib.ag2d_world_query_shape(self.h, shape, p.ctypes.data, trees, out.ctypes.data, out.size,
+                                          ctypes.byref(n)))
+        return out[:int(n.value)]
+
+    def query_aabb(self, lo, hi, trees: int = TREE_ALL) -> np.ndarray:
+        """Colliders whose AABB strictly overlaps [lo, hi] (BroadPhaseCollisionDetector::queryCollidersInShape
+        with an AABBQuery), ascending indices."""
+        return self._query(QUERY_AABB, [lo[0], lo[1], hi[0], hi[1]], trees)
+
+    def query_circle(self, centre, radius: float, trees: int = TREE_ALL) -> np.ndarray:
+        """Colliders whose AABB is within 'radius' of 'centre' (a CircleQuery), ascending indices."""
+        return self._query(QUERY_CIRCLE, [centre[0], centre[1], radius], trees)
 
     def set_tuning(self, tuning: dict):
         """Applies launch shapes (a dict as autotune returns); results do not depend on them."""

@@ -116,6 +116,8 @@ __global__ void k_island_sleep(DeviceWorld w, uint32_t* parent, const uint32_t* 
 __global__ void k_state_flags(const uint8_t* bstate, const uint32_t* cbody, uint32_t nBodies, uint32_t nColliders,
                               uint32_t* bodyDyn, uint32_t* colDyn, uint32_t* colOther);
 __global__ void k_scatter_list(const uint32_t* flag, const uint32_t* offset, uint32_t n, uint32_t* list);
+__global__ void k_query_shape(const float4* caabb, const uint32_t* cbody, const uint8_t* bstate, uint32_t n,
+                              uint32_t shape, float4 q, uint32_t trees, uint32_t* flag);
 
 // Batch repacking (k_repack.cu). A segment copies 'count' elements from [src, ...) of the current array (fromNew
 // 0), or from the staged section of joining world 'src' (fromNew 1), to [dst, ...) of the new array; the deltas

@@ -493,6 +493,7 @@ struct ag2d_world {
     DBuf<uint32_t> bk_prevColor;
     DBuf<unsigned long long> stagedSections;   // [joining world][section] byte offsets into 'staging'
     PinnedBuf hostStage, hostOut;              // page-locked copies of the staged blobs and the leaving bodies
+    DBuf<uint32_t> queryFlag, queryOffset, queryList, queryCount;   // spatial query scratch
     DBuf<GatherSeg> gatherSegs;
     bool newWorldsPending = false;   // joined worlds take a full pose pass in their first step
     // Shape table sizes of the last upload.
@@ -2189,6 +2190,47 @@ static std::vector<uint8_t> read_field(ag2d_world& w, int32_t field)
 }
 
 extern "C" {
+
+int32_t ag2d_world_query_shape(ag2d_world* world, int32_t shape, const float* params, uint32_t trees,
+                               uint32_t* out_colliders, uint32_t capacity, uint32_t* out_count)
+{
+    return guarded([&] {
+        if (!world || !params || !out_count) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        if (shape != AG2D_QUERY_AABB && shape != AG2D_QUERY_CIRCLE)
+            throw ApiError(AG2D_ERR_INVALID_ARG, "unknown query shape");
+        if (capacity && !out_colliders) throw ApiError(AG2D_ERR_INVALID_ARG, "null output with a capacity");
+        CK(cudaSetDevice(world->settings.device));
+        ag2d_world& w = *world;
+        w.ensureUploaded();
+        *out_count = 0;
+        const uint32_t n = w.nColliders;
+        // fullPose: no step has computed the poses and AABBs of the uploaded state yet.
+        if (n == 0 || w.fullPose || (trees & AG2D_TREE_ALL) == 0) return;
+        const cudaStream_t s = w.stream;
+        w.queryFlag.reserve(n);
+        w.queryOffset.reserve(n);
+        w.queryList.reserve(n);
+        w.queryCount.reserve(1);
+        w.scanner.reserve(std::max({w.pairCap, w.nColliders, w.nBodies}));
+        const float4 q = shape == AG2D_QUERY_AABB ? make_float4(params[0], params[1], params[2], params[3])
+                                                   : make_float4(params[0], params[1], params[2], 0.0f);
+        k_query_shape<<<w.gridFor(n), 256, 0, s>>>(w.caabb.p, w.cbody.p, w.bstate.p, n, uint32_t(shape), q,
+                                                   trees & AG2D_TREE_ALL, w.queryFlag.p);
+        CK(cudaGetLastError());
+        w.scanner.run(w.queryFlag.p, w.queryOffset.p, n, w.queryCount.p, s);
+        k_scatter_list<<<w.gridFor(n), 256, 0, s>>>(w.queryFlag.p, w.queryOffset.p, n, w.queryList.p);
+        CK(cudaGetLastError());
+        uint32_t count = 0;
+        CK(cudaMemcpyAsync(&count, w.queryCount.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        const uint32_t m = std::min(count, capacity);
+        if (m) {
+            CK(cudaMemcpyAsync(out_colliders, w.queryList.p, size_t(m) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        }
+        *out_count = count;
+    });
+}
 
 int32_t ag2d_world_read(ag2d_world* world, int32_t field, void* dst, uint64_t cap, uint64_t* out_bytes)
 {

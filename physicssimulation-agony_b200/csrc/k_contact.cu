@@ -456,6 +456,37 @@ __global__ void k_state_flags(const uint8_t* __restrict__ bstate, const uint32_t
     }
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// Spatial query (BroadPhaseCollisionDetector::queryCollidersInShape, BroadPhaseCollisionDetector.h:189-203;
+// BvhTree::queryCollidersInShape, BvhTree.h:110-192): a collider is found when its body's tree (dynamic, static
+// or sleeping) is selected and its AABB passes the query shape's leaf test (QueryShapes.h): strict overlap for an
+// AABB (AABBQuery::simdOverlap), closest-point squared distance within the squared radius for a circle
+// (CircleQuery::simdOverlap, radius clamped at 0). One flag per collider, compacted afterwards in index order.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void k_query_shape(const float4* __restrict__ caabb, const uint32_t* __restrict__ cbody,
+                              const uint8_t* __restrict__ bstate, uint32_t n, uint32_t shape, float4 q,
+                              uint32_t trees, uint32_t* __restrict__ flag)
+{
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const uint8_t st = bstate[cbody[c]];
+        const uint32_t tree = st == STATE_DYNAMIC ? 1u : (st == STATE_STATIC ? 2u : 4u);
+        bool hit = false;
+        if (trees & tree) {
+            const float4 b = caabb[c];
+            if (shape == 0) {
+                hit = b.x < q.z && b.z > q.x && b.y < q.w && b.w > q.y;
+            } else {
+                const float r = rfmaxf(0.0f, q.z);
+                const float rr = r * r;
+                const float dx = rfmaxf(b.x - q.x, rfmaxf(0.0f, q.x - b.z));
+                const float dy = rfmaxf(b.y - q.y, rfmaxf(0.0f, q.y - b.w));
+                hit = (dx * dx + dy * dy) <= rr;
+            }
+        }
+        flag[c] = hit ? 1u : 0u;
+    }
+}
+
 __global__ void k_scatter_list(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ offset, uint32_t n,
                                uint32_t* __restrict__ list)
 {
