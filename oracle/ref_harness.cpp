@@ -594,6 +594,27 @@ extern "C"
 
     void agref_clear_blobs(void* hp) { static_cast<Harness*>(hp)->blobs.clear(); }
 
+    // Colliders a shape query finds through the reference's own trees (BroadPhaseCollisionDetector::
+    // queryCollidersInShape, BroadPhaseCollisionDetector.h:189-203, with AABBQuery / CircleQuery, QueryShapes.h):
+    // shape 0 = AABB {minX, minY, maxX, maxY}, 1 = circle {x, y, radius}; 'trees' the BvhTreeTypeFlag bits. Returns
+    // the count and writes at most 'cap' dense collider indices, in the reference's traversal order.
+    int64_t agref_query_shape(void* hp, int32_t shape, const float* p, uint32_t trees, uint32_t* out, uint64_t cap)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        std::vector<ObjectDenseIndex> found;
+        const BroadPhaseCollisionDetector& bp = h->sim.getBroadPhaseCollisionDetector();
+        const auto flags = static_cast<BroadPhaseInternal::BvhTreeTypeFlag>(trees);
+        if (shape == 0) {
+            AABB box;
+            box.minX = p[0]; box.minY = p[1]; box.maxX = p[2]; box.maxY = p[3];
+            bp.queryCollidersInShape(BroadPhaseInternal::AABBQuery(box), flags, found);
+        } else {
+            bp.queryCollidersInShape(BroadPhaseInternal::CircleQuery(Vec2{p[0], p[1]}, p[2]), flags, found);
+        }
+        for (size_t i = 0; i < found.size() && i < cap; i++) out[i] = uint32_t(found[i]);
+        return int64_t(found.size());
+    }
+
     // The reference's batched rotation cos/sin over an array (FastCosSin.cpp:26-109), SIMD body and scalar tail.
     void agref_fastcossin(const float* in, float* outCos, float* outSin, uint64_t n)
     {

@@ -70,6 +70,8 @@ def lib():
         L.agref_blob_names.restype = ctypes.c_uint64
         L.agref_blob_names.argtypes = [vp, ctypes.c_char_p, ctypes.c_uint64]
         L.agref_clear_blobs.argtypes = [vp]
+        L.agref_query_shape.argtypes = [vp, i32, vp, u32, vp, ctypes.c_uint64]
+        L.agref_query_shape.restype = ctypes.c_int64
         L.agref_fastcossin.argtypes = [vp, vp, vp, ctypes.c_uint64]
         _lib = L
     return _lib
@@ -168,6 +170,14 @@ class RefSim:
 
     def blobs(self, prefix: str = "") -> dict:
         return {k: self.blob(k) for k in self.blob_names() if k.startswith(prefix)}
+
+    def query_shape(self, shape: int, params, trees: int = 7) -> np.ndarray:
+        """Dense collider indices a shape query finds in the reference's trees (0 = AABB, 1 = circle)."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        n = lib().agref_query_shape(self.h, shape, p.ctypes.data, trees, None, 0)
+        out = np.empty(max(int(n), 1), np.uint32)
+        lib().agref_query_shape(self.h, shape, p.ctypes.data, trees, out.ctypes.data, out.size)
+        return out[:int(n)]
 
     @property
     def manifold_count(self) -> int:

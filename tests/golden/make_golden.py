@@ -154,6 +154,37 @@ def ccd_fixture(path, max_steps=80):
     print(f"{os.path.basename(path)}: step {step}, {scene.n} bodies")
 
 
+def query_fixture(path, n=600, steps=700, queries=24):
+    """Spatial queries through the reference's own trees (agref_query_shape: queryCollidersInShape with AABB and
+    circle shapes, every tree selection) on a settled pile with sleeping bodies, with the colliders' AABBs and
+    group ranges the queries ran on."""
+    scene = scenes.make_c1(n, seed=5, width=60.0, height=40.0)
+    r = refapi.RefSim(scene)
+    r.update(steps)
+    r.dump_state("q.")
+    b = r.blobs("q.col.")
+    rng = np.random.default_rng(9)
+    params, shapes, trees, found, offsets = [], [], [], [], [0]
+    for _ in range(queries):
+        cx, cy = rng.uniform(-35, 35), rng.uniform(-5, 30)
+        hw, hh, rad = rng.uniform(0.1, 15), rng.uniform(0.1, 15), rng.uniform(-1, 12)
+        for t in (7, 1, 2, 4, 5):
+            for shape, prm in ((0, (cx - hw, cy - hh, cx + hw, cy + hh, 0.0)), (1, (cx, cy, rad, 0.0, 0.0))):
+                got = r.query_shape(shape, prm[:4] if shape == 0 else prm[:3], t)
+                params.append(prm); shapes.append(shape); trees.append(t)
+                found.append(np.sort(got)); offsets.append(offsets[-1] + got.size)
+    keep = {k: b[k] for k in ("q.col.aabbMinX", "q.col.aabbMinY", "q.col.aabbMaxX", "q.col.aabbMaxY",
+                              "q.col.groupStarts")}
+    keep["params"] = np.asarray(params, np.float32)
+    keep["shape"] = np.asarray(shapes, np.uint32)
+    keep["trees"] = np.asarray(trees, np.uint32)
+    keep["found"] = np.concatenate(found).astype(np.uint32)
+    keep["offsets"] = np.asarray(offsets, np.uint32)
+    np.savez_compressed(path, **keep)
+    r.close()
+    print(f"{os.path.basename(path)}: {len(shapes)} queries, groups {keep['q.col.groupStarts'].tolist()}")
+
+
 def main():
     if not refapi.available():
         sys.exit("oracle/_ref/libagony_ref.so missing: run oracle/ref_build.sh first")
@@ -164,6 +195,7 @@ def main():
     wrap_fixture(os.path.join(HERE, "wrap_edge.npz"))
     trajectory_fixture(os.path.join(HERE, "traj_c1_n256.npz"))
     ccd_fixture(os.path.join(HERE, "c5_ccd_hit.npz"))
+    query_fixture(os.path.join(HERE, "query_c1_n600_step700.npz"))
 
 
 if __name__ == "__main__":

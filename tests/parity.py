@@ -49,3 +49,25 @@ def partition_labels(ids: np.ndarray) -> np.ndarray:
     _, inv = np.unique(np.asarray(ids), return_inverse=True)
     first = {}
     return np.array([first.setdefault(int(v), len(first)) for v in inv], dtype=np.int64)
+
+
+def query_leaf_test(mnx, mny, mxx, mxy, tree_bits, shape, params, trees):
+    """Colliders a shape query finds, restated from the reference's query shapes (CollisionDetection/Broad/
+    QueryShapes.h:8-86) in float32 without fused multiply-add: AABB (shape 0, params min_x, min_y, max_x, max_y) -
+    strict overlap on both axes (AABBQuery::simdOverlap); circle (shape 1, params x, y, r) - dx = fmax(min_x - x,
+    fmax(0, x - max_x)), dy alike, found when dx*dx + dy*dy <= fmax(0, r)^2 (CircleQuery::simdOverlap). tree_bits:
+    each collider's tree (1 dynamic, 2 static, 4 sleeping); trees: the selected bits. Returns ascending indices."""
+    f32 = np.float32
+    mnx, mny, mxx, mxy = (np.asarray(a, f32) for a in (mnx, mny, mxx, mxy))
+    sel = (np.asarray(tree_bits) & trees) != 0
+    if shape == 0:
+        qx0, qy0, qx1, qy1 = (f32(v) for v in params)
+        hit = (mnx < qx1) & (mxx > qx0) & (mny < qy1) & (mxy > qy0)
+    else:
+        x, y, r = (f32(v) for v in params)
+        r = np.fmax(f32(0), r)
+        rr = f32(r * r)
+        dx = np.fmax(mnx - x, np.fmax(f32(0), x - mxx)).astype(f32)
+        dy = np.fmax(mny - y, np.fmax(f32(0), y - mxy)).astype(f32)
+        hit = (dx * dx + dy * dy).astype(f32) <= rr
+    return np.nonzero(sel & hit)[0].astype(np.uint32)

@@ -1,14 +1,13 @@
 """Spatial queries (BroadPhaseCollisionDetector::queryCollidersInShape with the AABBQuery and CircleQuery shapes of
-CollisionDetection/Broad/QueryShapes.h:8-86) through the C ABI, against a float32 restatement of the shapes' leaf
-tests over the colliders' AABBs read back from the same world.
-
-The checker below restates the reference's tests with numpy float32 (no fused multiply-add, as the reference is
-built): AABB - strict overlap on both axes; circle - dx = fmax(min_x - x, fmax(0, x - max_x)) (and dy alike),
-found when dx*dx + dy*dy <= fmax(0, r)^2. A collider belongs to the dynamic, static or sleeping tree by its body's
-state. Found sets must be equal, index for index.
+CollisionDetection/Broad/QueryShapes.h:8-86) through the C ABI, against the restated leaf tests
+(parity.query_leaf_test) over the colliders' AABBs read back from the same world. The restatement is pinned to the
+reference's own trees by tests/test_oracle_golden.py::test_query_restatement_matches_the_reference. A collider
+belongs to the dynamic, static or sleeping tree by its body's state. Found sets must be equal, index for index.
 """
 import numpy as np
 import pytest
+
+import parity
 
 pytestmark = pytest.mark.gpu
 
@@ -17,24 +16,12 @@ from ag2d import scenes  # noqa: E402
 
 
 def _expected(w, shape, params, trees):
-    f32 = np.float32
-    mnx, mny = w.read(ag2d.COL_AABB_MIN_X), w.read(ag2d.COL_AABB_MIN_Y)
-    mxx, mxy = w.read(ag2d.COL_AABB_MAX_X), w.read(ag2d.COL_AABB_MAX_Y)
     state = w.read(ag2d.BODY_STATE)   # one collider per body, in body order, in these scenes
+    mnx = w.read(ag2d.COL_AABB_MIN_X)
     assert state.size == mnx.size
-    bit = np.where(state == 2, 1, np.where(state == 0, 2, 4))
-    sel = (bit & trees) != 0
-    if shape == ag2d.QUERY_AABB:
-        qx0, qy0, qx1, qy1 = (f32(v) for v in params)
-        hit = (mnx < qx1) & (mxx > qx0) & (mny < qy1) & (mxy > qy0)
-    else:
-        x, y, r = (f32(v) for v in params)
-        r = np.fmax(f32(0), r)
-        rr = f32(r * r)
-        dx = np.fmax(mnx - x, np.fmax(f32(0), x - mxx)).astype(f32)
-        dy = np.fmax(mny - y, np.fmax(f32(0), y - mxy)).astype(f32)
-        hit = (dx * dx + dy * dy).astype(f32) <= rr
-    return np.nonzero(sel & hit)[0].astype(np.uint32)
+    tree_bits = np.where(state == 2, 1, np.where(state == 0, 2, 4))
+    return parity.query_leaf_test(mnx, w.read(ag2d.COL_AABB_MIN_Y), w.read(ag2d.COL_AABB_MAX_X),
+                                  w.read(ag2d.COL_AABB_MAX_Y), tree_bits, shape, params, trees)
 
 
 @pytest.fixture(scope="module")

@@ -150,3 +150,25 @@ def test_oracle_detects_a_planted_fault(oracle_lib):
     m2 = w.narrow(d["bp.pairs"].reshape(-1, 2))
     assert parity.mismatches(parity.sort_manifolds(m)["depth"], parity.sort_manifolds(m2)["depth"]) > 0 or \
         m.shape != m2.shape
+
+
+def test_query_restatement_matches_the_reference():
+    """The restated query-shape leaf tests (parity.query_leaf_test, which the GPU query test checks the kernel
+    against) find exactly the colliders the reference's own trees return (queryCollidersInShape), for AABB and
+    circle shapes and every tree selection, on a settled pile with sleeping bodies."""
+    g = parity.load("query_c1_n600_step700.npz")
+    starts = g["q.col.groupStarts"]   # BodyGroup order: static, sleeping, dynamic
+    n = g["q.col.aabbMinX"].size
+    idx = np.arange(n)
+    tree_bits = np.where(idx < starts[1], 2, np.where(idx < starts[2], 4, 1))
+    assert (tree_bits == 4).any() and (tree_bits == 2).any()
+    nonempty = 0
+    for k in range(g["shape"].size):
+        shape, trees = int(g["shape"][k]), int(g["trees"][k])
+        params = g["params"][k][:4] if shape == 0 else g["params"][k][:3]
+        got = parity.query_leaf_test(g["q.col.aabbMinX"], g["q.col.aabbMinY"], g["q.col.aabbMaxX"],
+                                     g["q.col.aabbMaxY"], tree_bits, shape, params, trees)
+        want = g["found"][g["offsets"][k]:g["offsets"][k + 1]]
+        assert np.array_equal(got, want), (k, shape, trees)
+        nonempty += want.size > 0
+    assert nonempty > 20
