@@ -225,7 +225,7 @@ int32_t ag2d_world_body_count(ag2d_world* world, uint32_t* out_bodies, uint32_t*
  * overlap; circle: closest-point squared distance <= radius^2, radius clamped at 0), among the trees selected by
  * 'trees' (AG2D_TREE_* bits, by the owner body's state). params: AABB {min_x, min_y, max_x, max_y}; circle
  * {x, y, radius}. Before the first step after creation or a host-side edit nothing is found (the reference's
- * trees are empty then). The reference
+ * trees are empty then), unless ag2d_world_load_state brought the AABBs. The reference
  * also adds every collider of a node its shape contains without the collider's own test; the sets differ only for
  * a collider AABB of zero width or height lying on the query AABB's boundary. out_count receives the full count;
  * at most 'capacity' indices are written. On a batch's engine the query covers every world of the batch. */
@@ -233,6 +233,14 @@ enum ag2d_tree_flag { AG2D_TREE_DYNAMIC = 1, AG2D_TREE_STATIC = 2, AG2D_TREE_SLE
 enum ag2d_query_shape { AG2D_QUERY_AABB = 0, AG2D_QUERY_CIRCLE = 1 };
 int32_t ag2d_world_query_shape(ag2d_world* world, int32_t shape, const float* params, uint32_t trees,
                                uint32_t* out_colliders, uint32_t capacity, uint32_t* out_count);
+/* Colliders a circle touches, replacing NarrowPhaseCollisionDetector::findCollisionsInCircle (NarrowPhase
+ * CollisionDetector.cpp:153-270) applied to what a circle query finds (ag2d_world_query_shape with
+ * AG2D_QUERY_CIRCLE): a collider is reported with the signed distance from the circle's centre to its shape
+ * (negative inside) when that distance is below 'radius'. Ascending indices; out_count receives the full count, at
+ * most 'capacity' indices and distances are written. Same validity rule as ag2d_world_query_shape. */
+int32_t ag2d_world_query_circle_contacts(ag2d_world* world, float x, float y, float radius, uint32_t trees,
+                                         uint32_t* out_colliders, float* out_distance, uint32_t capacity,
+                                         uint32_t* out_count);
 
 /* Copies a field into caller memory (host). out_bytes receives the field size; pass dst = NULL to query it.
  * Replaces the reference's SoA viewers (ObjectAPI::getBodies/getColliders, ObjectAPI.h:96-101) and

@@ -615,6 +615,26 @@ extern "C"
         return int64_t(found.size());
     }
 
+    // Colliders a circle touches: the circle query's colliders (as above) passed to
+    // NarrowPhaseCollisionDetector::findCollisionsInCircle (NarrowPhaseCollisionDetector.cpp:153-270). Returns the
+    // count; writes at most 'cap' (collider, signed distance) results in the reference's order.
+    int64_t agref_circle_contacts(void* hp, float x, float y, float r, uint32_t trees, uint32_t* outIdx, float* outSdf,
+                                  uint64_t cap)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        std::vector<ObjectDenseIndex> found;
+        h->sim.getBroadPhaseCollisionDetector().queryCollidersInShape(
+            BroadPhaseInternal::CircleQuery(Vec2{x, y}, r), static_cast<BroadPhaseInternal::BvhTreeTypeFlag>(trees),
+            found);
+        std::vector<std::pair<ObjectDenseIndex, Real>> hits;
+        h->sim.getNarrowPhaseCollisionDetector().findCollisionsInCircle(found, Vec2{x, y}, r, hits);
+        for (size_t i = 0; i < hits.size() && i < cap; i++) {
+            outIdx[i] = uint32_t(hits[i].first);
+            outSdf[i] = float(hits[i].second);
+        }
+        return int64_t(hits.size());
+    }
+
     // The reference's batched rotation cos/sin over an array (FastCosSin.cpp:26-109), SIMD body and scalar tail.
     void agref_fastcossin(const float* in, float* outCos, float* outSin, uint64_t n)
     {

@@ -72,6 +72,8 @@ def lib():
         L.agref_clear_blobs.argtypes = [vp]
         L.agref_query_shape.argtypes = [vp, i32, vp, u32, vp, ctypes.c_uint64]
         L.agref_query_shape.restype = ctypes.c_int64
+        L.agref_circle_contacts.argtypes = [vp, f, f, f, u32, vp, vp, ctypes.c_uint64]
+        L.agref_circle_contacts.restype = ctypes.c_int64
         L.agref_fastcossin.argtypes = [vp, vp, vp, ctypes.c_uint64]
         _lib = L
     return _lib
@@ -178,6 +180,15 @@ class RefSim:
         out = np.empty(max(int(n), 1), np.uint32)
         lib().agref_query_shape(self.h, shape, p.ctypes.data, trees, out.ctypes.data, out.size)
         return out[:int(n)]
+
+    def circle_contacts(self, x: float, y: float, r: float, trees: int = 7):
+        """(colliders, signed distances) the reference's findCollisionsInCircle reports for its circle query."""
+        L = lib()
+        n = L.agref_circle_contacts(self.h, x, y, r, trees, None, None, 0)
+        idx = np.empty(max(int(n), 1), np.uint32)
+        sdf = np.empty(max(int(n), 1), np.float32)
+        L.agref_circle_contacts(self.h, x, y, r, trees, idx.ctypes.data, sdf.ctypes.data, idx.size)
+        return idx[:int(n)], sdf[:int(n)]
 
     @property
     def manifold_count(self) -> int:

@@ -149,6 +149,8 @@ def _load():
     L.ag2d_world_autotune.argtypes = [vp, i32, ctypes.POINTER(Tuning)]
     L.ag2d_world_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
     L.ag2d_world_query_shape.argtypes = [vp, i32, vp, u32, vp, u32, ctypes.POINTER(u32)]
+    L.ag2d_world_query_circle_contacts.argtypes = [vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, u32, vp, vp,
+                                                   u32, ctypes.POINTER(u32)]
     L.ag2d_world_phase_times.argtypes = [vp, vp, vp, i32]
     L.ag2d_world_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.ag2d_batch_create.argtypes = [ctypes.POINTER(vp), u32, ctypes.POINTER(vp)]
@@ -376,6 +378,18 @@ class World:
     def query_circle(self, centre, radius: float, trees: int = TREE_ALL) -> np.ndarray:
         """Colliders whose AABB is within 'radius' of 'centre' (a CircleQuery), ascending indices."""
         return self._query(QUERY_CIRCLE, [centre[0], centre[1], radius], trees)
+
+    def query_circle_contacts(self, centre, radius: float, trees: int = TREE_ALL):
+        """(indices, signed distances) of the colliders the circle touches (findCollisionsInCircle over the circle
+        query's colliders), ascending indices."""
+        n = ctypes.c_uint32()
+        args = (self.h, float(centre[0]), float(centre[1]), float(radius), trees)
+        _check(lib.ag2d_world_query_circle_contacts(*args, None, None, 0, ctypes.byref(n)))
+        idx = np.empty(max(int(n.value), 1), np.uint32)
+        dist = np.empty(max(int(n.value), 1), np.float32)
+        _check(lib.ag2d_world_query_circle_contacts(*args, idx.ctypes.data, dist.ctypes.data, idx.size,
+                                                    ctypes.byref(n)))
+        return idx[:int(n.value)], dist[:int(n.value)]
 
     def set_tuning(self, tuning: dict):
         """Applies launch shapes (a dict as autotune returns); results do not depend on them."""

@@ -118,6 +118,10 @@ __global__ void k_state_flags(const uint8_t* bstate, const uint32_t* cbody, uint
 __global__ void k_scatter_list(const uint32_t* flag, const uint32_t* offset, uint32_t n, uint32_t* list);
 __global__ void k_query_shape(const float4* caabb, const uint32_t* cbody, const uint8_t* bstate, uint32_t n,
                               uint32_t shape, float4 q, uint32_t trees, uint32_t* flag);
+__global__ void k_circle_contacts(DeviceWorld w, float x, float y, float radius, uint32_t trees, uint32_t* flag,
+                                  float* dist);
+__global__ void k_scatter_contacts(const uint32_t* flag, const uint32_t* offset, const float* dist, uint32_t n,
+                                   uint32_t* list, float* listDist);
 
 // Batch repacking (k_repack.cu). A segment copies 'count' elements from [src, ...) of the current array (fromNew
 // 0), or from the staged section of joining world 'src' (fromNew 1), to [dst, ...) of the new array; the deltas

@@ -404,6 +404,7 @@ struct ag2d_world {
     bool hostDirty = true;          // host objects changed since the last upload
     bool listsDirty = true;         // work lists need a rebuild (state changes)
     bool fullPose = true;           // next pose pass covers every collider (first step after an upload)
+    bool aabbValid = false;         // caabb holds the broad phase's AABBs (a step ran, or a state brought them)
     bool otherDirty = true;         // static + sleeping tree must be rebuilt
     uint64_t stepsTaken = 0;
 
@@ -494,6 +495,7 @@ struct ag2d_world {
     DBuf<unsigned long long> stagedSections;   // [joining world][section] byte offsets into 'staging'
     PinnedBuf hostStage, hostOut;              // page-locked copies of the staged blobs and the leaving bodies
     DBuf<uint32_t> queryFlag, queryOffset, queryList, queryCount;   // spatial query scratch
+    DBuf<float> queryDist, queryListDist;
     DBuf<GatherSeg> gatherSegs;
     bool newWorldsPending = false;   // joined worlds take a full pose pass in their first step
     // Shape table sizes of the last upload.
@@ -1129,6 +1131,7 @@ struct ag2d_world {
         hostDirty = false;
         listsDirty = true;
         fullPose = true;
+        aabbValid = false;
         otherDirty = true;
         lastManifolds = 0;
         prevCount = 0;
@@ -1714,6 +1717,7 @@ struct ag2d_world {
                 throw ApiError(AG2D_ERR_CAPACITY, "capacity limit (colours, hash or traversal stack), status " + std::to_string(st));
             }
             fullPose = false;
+            aabbValid = true;
             // The solved manifolds become the next step's warm-start source.
             swap_bufs(manifolds, prevManifolds);
             swap_bufs(color, prevColor);   // this step's colours: next step's hints
@@ -1967,6 +1971,7 @@ int32_t ag2d_world_load_state(ag2d_world* world, const ag2d_state_desc* st)
                                      st->col_aabb_max_y[i]);
             if (nc) CK(cudaMemcpyAsync(w.caabb.p, box.data(), nc * sizeof(float4), cudaMemcpyHostToDevice, w.stream));
             CK(cudaStreamSynchronize(w.stream));
+            w.aabbValid = true;
         }
         // The loaded state replaces any host-created objects.
         w.objects.bodies.clear();
@@ -2204,8 +2209,7 @@ int32_t ag2d_world_query_shape(ag2d_world* world, int32_t shape, const float* pa
         w.ensureUploaded();
         *out_count = 0;
         const uint32_t n = w.nColliders;
-        // fullPose: no step has computed the poses and AABBs of the uploaded state yet.
-        if (n == 0 || w.fullPose || (trees & AG2D_TREE_ALL) == 0) return;
+        if (n == 0 || !w.aabbValid || (trees & AG2D_TREE_ALL) == 0) return;
         const cudaStream_t s = w.stream;
         w.queryFlag.reserve(n);
         w.queryOffset.reserve(n);
@@ -2226,6 +2230,48 @@ int32_t ag2d_world_query_shape(ag2d_world* world, int32_t shape, const float* pa
         const uint32_t m = std::min(count, capacity);
         if (m) {
             CK(cudaMemcpyAsync(out_colliders, w.queryList.p, size_t(m) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        }
+        *out_count = count;
+    });
+}
+
+int32_t ag2d_world_query_circle_contacts(ag2d_world* world, float x, float y, float radius, uint32_t trees,
+                                         uint32_t* out_colliders, float* out_distance, uint32_t capacity,
+                                         uint32_t* out_count)
+{
+    return guarded([&] {
+        if (!world || !out_count) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        if (capacity && (!out_colliders || !out_distance))
+            throw ApiError(AG2D_ERR_INVALID_ARG, "null output with a capacity");
+        CK(cudaSetDevice(world->settings.device));
+        ag2d_world& w = *world;
+        w.ensureUploaded();
+        *out_count = 0;
+        const uint32_t n = w.nColliders;
+        if (n == 0 || !w.aabbValid || (trees & AG2D_TREE_ALL) == 0) return;
+        const cudaStream_t s = w.stream;
+        w.queryFlag.reserve(n);
+        w.queryOffset.reserve(n);
+        w.queryList.reserve(n);
+        w.queryDist.reserve(n);
+        w.queryListDist.reserve(n);
+        w.queryCount.reserve(1);
+        w.scanner.reserve(std::max({w.pairCap, w.nColliders, w.nBodies}));
+        k_circle_contacts<<<w.gridFor(n), 256, 0, s>>>(w.view(), x, y, radius, trees & AG2D_TREE_ALL, w.queryFlag.p,
+                                                       w.queryDist.p);
+        CK(cudaGetLastError());
+        w.scanner.run(w.queryFlag.p, w.queryOffset.p, n, w.queryCount.p, s);
+        k_scatter_contacts<<<w.gridFor(n), 256, 0, s>>>(w.queryFlag.p, w.queryOffset.p, w.queryDist.p, n,
+                                                        w.queryList.p, w.queryListDist.p);
+        CK(cudaGetLastError());
+        uint32_t count = 0;
+        CK(cudaMemcpyAsync(&count, w.queryCount.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        const uint32_t m = std::min(count, capacity);
+        if (m) {
+            CK(cudaMemcpyAsync(out_colliders, w.queryList.p, size_t(m) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(out_distance, w.queryListDist.p, size_t(m) * sizeof(float), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
         }
         *out_count = count;

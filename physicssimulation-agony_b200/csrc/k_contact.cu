@@ -487,6 +487,89 @@ __global__ void k_query_shape(const float4* __restrict__ caabb, const uint32_t* 
     }
 }
 
+// Signed distance from a query circle's centre to one collider, as NarrowPhaseCollisionDetector::
+// findCollisionsInCircle (NarrowPhaseCollisionDetector.cpp:153-270) computes it: circle - centre distance minus the
+// radius; box - the exact box distance field in the box frame; polygon - distance to the support edge's closest
+// point (findSupportEdge / closestPointOnSegment, HelperMethods.h:73-109), or the (negative) separation inside.
+// False where the reference skips the collider or the distance is not below the query radius.
+__device__ __forceinline__ bool circle_contact(const ColliderView& B, V2 pos, float radius, float& sdf)
+{
+    if (B.type == SHAPE_CIRCLE) {
+        const V2 delta = B.pos - pos;
+        const float distSq = dot(delta, delta);
+        const float radiusSum = B.r + radius;
+        if (radiusSum <= 0.0f || distSq >= radiusSum * radiusSum) return false;
+        sdf = sqrtf(distSq) - B.r;
+    } else {
+        const V2 right = V2{B.c, B.s}, up = V2{-B.s, B.c};
+        const V2 d = pos - B.pos;
+        const V2 loc = V2{dot(d, right), dot(d, up)};
+        if (B.type == SHAPE_BOX) {
+            const float dx = fabsf(loc.x) - B.hw, dy = fabsf(loc.y) - B.hh;
+            const float maxD = rfmaxf(dx, dy);
+            if (maxD > 0.0f && maxD >= radius) return false;
+            const float ex = rfmaxf(0.0f, dx), ey = rfmaxf(0.0f, dy);
+            const float outside = sqrtf(ex * ex + ey * ey);
+            const float inside = rfminf(0.0f, maxD);
+            sdf = inside + outside;
+        } else {
+            float maxSep = -FLT_MAX;
+            uint32_t edge = 0;
+            for (uint32_t i = 0; i < B.nv; i++) {
+                const float sep = dot(ld2(B.normals, i), loc - ld2(B.verts, i));
+                if (sep > radius) return false;
+                if (sep > maxSep) { maxSep = sep; edge = i; }
+            }
+            if (maxSep >= ZERO_DIVISION_BOUNDARY) {
+                const V2 a = ld2(B.verts, edge), b = ld2(B.verts, next_index(edge, B.nv));
+                const V2 ab = b - a;
+                const float denom = dot(ab, ab);
+                V2 q = a;
+                if (denom >= ZERO_DIVISION_BOUNDARY_SQUARED) {
+                    const float t = dot(loc - a, ab) / denom;
+                    q = a + ab * rfminf(rfmaxf(t, 0.0f), 1.0f);
+                }
+                const V2 e = loc - q;
+                sdf = sqrtf(dot(e, e));
+            } else {
+                sdf = maxSep;
+            }
+        }
+    }
+    return sdf < radius;
+}
+
+// Circle contacts: the circle query's colliders (k_query_shape's circle test, radius clamped at 0) that the circle
+// itself touches (circle_contact, the radius as given), with their signed distances.
+__global__ void k_circle_contacts(DeviceWorld w, float x, float y, float radius, uint32_t trees,
+                                  uint32_t* __restrict__ flag, float* __restrict__ dist)
+{
+    const float r = rfmaxf(0.0f, radius);
+    const float rr = r * r;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < w.nColliders; c += gridDim.x * blockDim.x) {
+        const uint8_t st = w.bstate[w.cbody[c]];
+        const uint32_t tree = st == STATE_DYNAMIC ? 1u : (st == STATE_STATIC ? 2u : 4u);
+        bool hit = false;
+        float sdf = 0.0f;
+        if (trees & tree) {
+            const float4 b = w.caabb[c];
+            const float dx = rfmaxf(b.x - x, rfmaxf(0.0f, x - b.z));
+            const float dy = rfmaxf(b.y - y, rfmaxf(0.0f, y - b.w));
+            if ((dx * dx + dy * dy) <= rr) hit = circle_contact(collider_view(w, c), V2{x, y}, radius, sdf);
+        }
+        flag[c] = hit ? 1u : 0u;
+        dist[c] = sdf;
+    }
+}
+
+__global__ void k_scatter_contacts(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ offset,
+                                   const float* __restrict__ dist, uint32_t n, uint32_t* __restrict__ list,
+                                   float* __restrict__ listDist)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (flag[i]) { list[offset[i]] = i; listDist[offset[i]] = dist[i]; }
+}
+
 __global__ void k_scatter_list(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ offset, uint32_t n,
                                uint32_t* __restrict__ list)
 {

@@ -185,6 +185,50 @@ def query_fixture(path, n=600, steps=700, queries=24):
     print(f"{os.path.basename(path)}: {len(shapes)} queries, groups {keep['q.col.groupStarts'].tolist()}")
 
 
+def contacts_fixture(path, n=1500, steps=300, queries=60):
+    """Circle contacts (agref_circle_contacts: the circle query's colliders through findCollisionsInCircle) and
+    shape queries on a mixed-shape pile (circles, boxes, polygons in a U container), with the full reference state
+    they ran on, so that a world loaded from it answers the same queries."""
+    scene = scenes.make_c2(n, 2, columns=30)
+    r = refapi.RefSim(scene)
+    r.update(steps)
+    r.dump_state("q.")
+    keep = {k: v for k, v in r.blobs("q.").items() if not k.startswith("q.man.")}
+    rng = np.random.default_rng(21)
+    cparams, ctrees, cidx, csdf, coff = [], [], [], [], [0]
+    sparams, sshape, strees, sidx, soff = [], [], [], [], [0]
+    for _ in range(queries):
+        c = int(rng.integers(0, keep["q.col.worldPosX"].size))   # near a random collider: contacts of every shape
+        x = float(keep["q.col.worldPosX"][c]) + rng.uniform(-2.0, 2.0)
+        y = float(keep["q.col.worldPosY"][c]) + rng.uniform(-2.0, 2.0)
+        rad = rng.uniform(-0.5, 6.0)
+        hw, hh = rng.uniform(0.1, 8.0), rng.uniform(0.1, 8.0)
+        for t in (7, 1, 2, 4, 6):
+            idx, sdf = r.circle_contacts(x, y, rad, t)
+            order = np.argsort(idx, kind="stable")
+            cparams.append((x, y, rad)); ctrees.append(t)
+            cidx.append(idx[order]); csdf.append(sdf[order]); coff.append(coff[-1] + idx.size)
+            for shape, prm in ((0, (x - hw, y - hh, x + hw, y + hh)), (1, (x, y, rad, 0.0))):
+                got = np.sort(r.query_shape(shape, prm[:4] if shape == 0 else prm[:3], t))
+                sparams.append(prm); sshape.append(shape); strees.append(t)
+                sidx.append(got); soff.append(soff[-1] + got.size)
+    keep["c.params"] = np.asarray(cparams, np.float32)
+    keep["c.trees"] = np.asarray(ctrees, np.uint32)
+    keep["c.idx"] = np.concatenate(cidx).astype(np.uint32)
+    keep["c.sdf"] = np.concatenate(csdf).astype(np.float32)
+    keep["c.offsets"] = np.asarray(coff, np.uint32)
+    keep["s.params"] = np.asarray(sparams, np.float32)
+    keep["s.shape"] = np.asarray(sshape, np.uint32)
+    keep["s.trees"] = np.asarray(strees, np.uint32)
+    keep["s.idx"] = np.concatenate(sidx).astype(np.uint32)
+    keep["s.offsets"] = np.asarray(soff, np.uint32)
+    keep["meta.materials"] = np.array([(1.0, 0.0, 0.0)] + list(scene.materials), np.float32)
+    np.savez_compressed(path, **keep)
+    r.close()
+    print(f"{os.path.basename(path)}: {len(ctrees)} circle-contact queries ({keep['c.idx'].size} contacts), "
+          f"{len(sshape)} shape queries, groups {keep['q.col.groupStarts'].tolist()}")
+
+
 def main():
     if not refapi.available():
         sys.exit("oracle/_ref/libagony_ref.so missing: run oracle/ref_build.sh first")
@@ -196,6 +240,7 @@ def main():
     trajectory_fixture(os.path.join(HERE, "traj_c1_n256.npz"))
     ccd_fixture(os.path.join(HERE, "c5_ccd_hit.npz"))
     query_fixture(os.path.join(HERE, "query_c1_n600_step700.npz"))
+    contacts_fixture(os.path.join(HERE, "contacts_c2_n1500_step300.npz"))
 
 
 if __name__ == "__main__":

@@ -60,3 +60,38 @@ def test_query_capacity_and_counts(world):
     assert world.query_circle((0.0, 0.0), -3.0).size <= everything.size   # a negative radius is clamped at 0
     with pytest.raises(ag2d.Ag2dError):
         world._query(7, [0, 0, 1, 1], ag2d.TREE_ALL)
+
+
+@pytest.fixture(scope="module")
+def loaded():
+    """A world holding the reference's own state of a mixed-shape pile (circles, boxes, polygons in a U container,
+    1,500 bodies after 300 steps), collider poses and AABBs included, with the reference's query answers."""
+    g = parity.load("contacts_c2_n1500_step300.npz")
+    w = ag2d.World()
+    w.load_state(g, "q.", g["meta.materials"], with_poses=True)
+    return w, g
+
+
+def test_shape_queries_match_the_reference(loaded):
+    w, g = loaded
+    for k in range(g["s.shape"].size):
+        shape, trees = int(g["s.shape"][k]), int(g["s.trees"][k])
+        params = g["s.params"][k][:4] if shape == 0 else g["s.params"][k][:3]
+        want = g["s.idx"][g["s.offsets"][k]:g["s.offsets"][k + 1]]
+        assert np.array_equal(w._query(shape, params, trees), want), (k, shape, trees)
+
+
+def test_circle_contacts_match_the_reference(loaded):
+    """Same colliders as NarrowPhaseCollisionDetector::findCollisionsInCircle over the reference's circle query;
+    signed distances within 1e-5 relative (the narrow-phase bar for depths)."""
+    w, g = loaded
+    total = 0
+    for k in range(g["c.trees"].size):
+        x, y, r = (float(v) for v in g["c.params"][k])
+        idx, dist = w.query_circle_contacts((x, y), r, int(g["c.trees"][k]))
+        lo, hi = g["c.offsets"][k], g["c.offsets"][k + 1]
+        assert np.array_equal(idx, g["c.idx"][lo:hi]), k
+        want = g["c.sdf"][lo:hi]
+        assert np.allclose(dist, want, rtol=1e-5, atol=1e-6), (k, np.abs(dist - want).max())
+        total += idx.size
+    assert total > 1000

@@ -172,3 +172,18 @@ def test_query_restatement_matches_the_reference():
         assert np.array_equal(got, want), (k, shape, trees)
         nonempty += want.size > 0
     assert nonempty > 20
+
+
+def test_query_restatement_matches_the_reference_on_mixed_shapes():
+    """The same restatement against the reference's shape queries on the mixed-shape pile of the circle-contact
+    fixture (circles, boxes, polygons)."""
+    g = parity.load("contacts_c2_n1500_step300.npz")
+    starts = g["q.col.groupStarts"]
+    idx = np.arange(g["q.col.aabbMinX"].size)
+    tree_bits = np.where(idx < starts[1], 2, np.where(idx < starts[2], 4, 1))
+    for k in range(g["s.shape"].size):
+        shape, trees = int(g["s.shape"][k]), int(g["s.trees"][k])
+        params = g["s.params"][k][:4] if shape == 0 else g["s.params"][k][:3]
+        got = parity.query_leaf_test(g["q.col.aabbMinX"], g["q.col.aabbMinY"], g["q.col.aabbMaxX"],
+                                     g["q.col.aabbMaxY"], tree_bits, shape, params, trees)
+        assert np.array_equal(got, g["s.idx"][g["s.offsets"][k]:g["s.offsets"][k + 1]]), (k, shape, trees)
