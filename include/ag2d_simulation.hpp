@@ -16,6 +16,7 @@
 
 #include "ag2d.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <memory>
@@ -23,6 +24,7 @@
 #include <span>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace ag2d {
@@ -183,6 +185,89 @@ private:
     ag2d_world* world;
 };
 
+struct AABB {
+    Real minX = 0, minY = 0, maxX = 0, maxY = 0;
+};
+
+// Query shapes of the broad phase (CollisionDetection/Broad/QueryShapes.h:8-86) and its tree selection flags
+// (BvhTree.h:26-33).
+namespace BroadPhaseInternal {
+enum class BvhTreeTypeFlag : uint8_t { None = 0, Dynamic = 1, Static = 2, Sleeping = 4, All = 7 };
+constexpr BvhTreeTypeFlag operator|(BvhTreeTypeFlag a, BvhTreeTypeFlag b) noexcept
+{
+    return BvhTreeTypeFlag(uint8_t(a) | uint8_t(b));
+}
+struct AABBQuery {
+    AABB aabb;
+    explicit AABBQuery(const AABB& a) noexcept : aabb(a) {}
+};
+struct CircleQuery {
+    Vec2 pos;
+    Real radius;
+    CircleQuery(Vec2 p, Real r) noexcept : pos(p), radius(r) {}
+};
+}  // namespace BroadPhaseInternal
+
+// The broad phase's spatial queries (BroadPhaseCollisionDetector::queryCollidersInShape,
+// BroadPhaseCollisionDetector.h:164-203). Indices are this library's collider indices; the found set is the
+// reference's, appended in ascending index order.
+class BroadPhaseCollisionDetector {
+public:
+    explicit BroadPhaseCollisionDetector(ag2d_world* w) : world(w) {}
+    void queryCollidersInShape(const BroadPhaseInternal::AABBQuery& q, BroadPhaseInternal::BvhTreeTypeFlag flags,
+                               std::vector<ObjectDenseIndex>& out) const
+    {
+        const float p[4] = {q.aabb.minX, q.aabb.minY, q.aabb.maxX, q.aabb.maxY};
+        run(AG2D_QUERY_AABB, p, flags, out);
+    }
+    void queryCollidersInShape(const BroadPhaseInternal::CircleQuery& q, BroadPhaseInternal::BvhTreeTypeFlag flags,
+                               std::vector<ObjectDenseIndex>& out) const
+    {
+        const float p[4] = {q.pos.x, q.pos.y, q.radius, 0.0f};
+        run(AG2D_QUERY_CIRCLE, p, flags, out);
+    }
+
+private:
+    void run(int32_t shape, const float* p, BroadPhaseInternal::BvhTreeTypeFlag flags,
+             std::vector<ObjectDenseIndex>& out) const
+    {
+        uint32_t n = 0;
+        detail::check(ag2d_world_query_shape(world, shape, p, uint32_t(flags), nullptr, 0, &n));
+        const size_t base = out.size();
+        out.resize(base + n);
+        if (n) detail::check(ag2d_world_query_shape(world, shape, p, uint32_t(flags), out.data() + base, n, &n));
+    }
+    ag2d_world* world;
+};
+
+// The narrow phase's circle test (NarrowPhaseCollisionDetector::findCollisionsInCircle,
+// NarrowPhaseCollisionDetector.cpp:153-270): for each collider of 'collidersToCheck' that the circle touches, its
+// index and the signed distance from the circle's centre, in the order given.
+class NarrowPhaseCollisionDetector {
+public:
+    explicit NarrowPhaseCollisionDetector(ag2d_world* w) : world(w) {}
+    void findCollisionsInCircle(std::span<const ObjectDenseIndex> collidersToCheck, Vec2 pos, Real radius,
+                                std::vector<std::pair<ObjectDenseIndex, Real>>& outColliding) const
+    {
+        // Every collider the circle touches passes the circle query too, so the device's answer over the query's
+        // colliders holds all of them; it is filtered to the colliders given.
+        uint32_t n = 0;
+        detail::check(ag2d_world_query_circle_contacts(world, pos.x, pos.y, radius, AG2D_TREE_ALL, nullptr, nullptr, 0,
+                                                        &n));
+        std::vector<uint32_t> idx(n);
+        std::vector<float> dist(n);
+        if (n) detail::check(ag2d_world_query_circle_contacts(world, pos.x, pos.y, radius, AG2D_TREE_ALL, idx.data(),
+                                                               dist.data(), n, &n));
+        for (ObjectDenseIndex c : collidersToCheck) {
+            const auto it = std::lower_bound(idx.begin(), idx.end(), c);   // ascending indices
+            if (it != idx.end() && *it == c) outColliding.emplace_back(c, Real(dist[size_t(it - idx.begin())]));
+        }
+    }
+
+private:
+    ag2d_world* world;
+};
+
 class Simulation {
 public:
     explicit Simulation(const SimulationSettings& s = {}) : settings(s)
@@ -237,6 +322,10 @@ public:
     }
 
     const SimulationSettings& getSimulationSettings() const noexcept { return settings; }
+    // Simulation::getBroadPhaseCollisionDetector / getNarrowPhaseCollisionDetector (Simulation.h:183-184), for their
+    // query entry points.
+    BroadPhaseCollisionDetector getBroadPhaseCollisionDetector() const noexcept { return BroadPhaseCollisionDetector(world); }
+    NarrowPhaseCollisionDetector getNarrowPhaseCollisionDetector() const noexcept { return NarrowPhaseCollisionDetector(world); }
     ag2d_world* handle() noexcept { return world; }
 
 private:

@@ -1,7 +1,9 @@
 // Scene code in the reference's style (App/Scenes.cpp: create a material, a static ground box and a pile of
 // bodies through ObjectAPI, then Simulation::update) compiled against the C++ facade of libag2d.so.
 // Prints "no-device" and exits 0 when the machine has no CUDA device; otherwise steps the scene and prints
-// "ok <bodies> <most manifolds in one step> <mean y>".
+// "ok <bodies> <most manifolds in one step> <mean y> <colliders a circle query finds> <circle contacts>" after
+// querying the settled pile the way the reference's editor selects (queryCollidersInShape with a CircleQuery, then
+// findCollisionsInCircle over what it found).
 #include "ag2d_simulation.hpp"
 
 #include <algorithm>
@@ -52,6 +54,19 @@ int main()
     const ag2d::BodyView bodies = sim->objects().getBodies();
     double meanY = 0.0;
     for (uint32_t i = 0; i < bodies.getCount(); i++) meanY += bodies.comY[i];
-    std::printf("ok %u %zu %.3f\n", bodies.getCount(), maxManifolds, meanY / double(bodies.getCount()));
+    namespace bp = ag2d::BroadPhaseInternal;
+    std::vector<ag2d::ObjectDenseIndex> found;
+    sim->getBroadPhaseCollisionDetector().queryCollidersInShape(bp::CircleQuery({0.0f, 1.0f}, 3.0f),
+                                                                bp::BvhTreeTypeFlag::All, found);
+    std::vector<std::pair<ag2d::ObjectDenseIndex, ag2d::Real>> touching;
+    sim->getNarrowPhaseCollisionDetector().findCollisionsInCircle(found, {0.0f, 1.0f}, 3.0f, touching);
+    for (const auto& t : touching)
+        if (!(t.second < 3.0f)) return 5;   // a contact is closer than the radius
+    std::vector<ag2d::ObjectDenseIndex> all;
+    sim->getBroadPhaseCollisionDetector().queryCollidersInShape(bp::AABBQuery({-1e6f, -1e6f, 1e6f, 1e6f}),
+                                                                bp::BvhTreeTypeFlag::All, all);
+    if (all.size() != bodies.getCount()) return 6;   // one collider per body, all inside the huge box
+    std::printf("ok %u %zu %.3f %zu %zu\n", bodies.getCount(), maxManifolds, meanY / double(bodies.getCount()),
+                found.size(), touching.size());
     return bodies.getCount() == uint32_t(created) ? 0 : 4;
 }

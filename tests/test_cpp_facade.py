@@ -40,3 +40,5 @@ def test_facade_steps_scene_on_gpu(tmp_path):
     bodies, manifolds, mean_y = int(fields[1]), int(fields[2]), float(fields[3])
     assert bodies == 61 and manifolds > 0
     assert -1.0 < mean_y < 6.0   # the pile has fallen onto the ground (spawned between y = 1 and 8.5)
+    found, touching = int(fields[4]), int(fields[5])   # the editor-style circle query around the pile's base
+    assert 0 < touching <= found
