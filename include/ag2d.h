@@ -315,8 +315,12 @@ int32_t ag2d_server_destroy(ag2d_server* server);
  * static device array of about 3.1 MiB per device, so:
  *  - at most AG2D_SOLVE_NOALLOC_MAX_MANIFOLDS manifolds and AG2D_SOLVE_NOALLOC_MAX_BODIES bodies per call; larger
  *    sizes return AG2D_ERR_CAPACITY with the limit in the error string, before any launch;
- *  - the first call with a device current looks the array's address up (cudaGetSymbolAddress) and so performs
- *    set-up; make it before any stream capture on that device;
+ *  - the array's address belongs to a CUDA context: the first call in each context (the first on a device, and the
+ *    first again after cudaDeviceReset or when another context is made current on that device) looks it up
+ *    (cudaGetSymbolAddress) and caches it under the context's unique id, so that call performs set-up; make it
+ *    before any stream capture in that context;
+ *  - a CUDA error already pending when the call starts (left by the caller's earlier work) is returned as
+ *    AG2D_ERR_CUDA without launching and is left pending, so a launch error reported here is this call's own;
  *  - the kernel clears what it needs at the start of every call: nothing has to start at zero;
  *  - calls that overlap on one device share the array and race: serialise them (one stream, or events).
  * The call is asynchronous on 'stream' (a cudaStream_t, NULL for the default stream) on the current device.

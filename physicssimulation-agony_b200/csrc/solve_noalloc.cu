@@ -2,16 +2,21 @@
 //
 // The scratch the solver needs (constraint records, colours, solving order, uncoloured lists, per-body colouring
 // words) lives in one file-scope __device__ array of fixed size, so a call makes no device allocation. The array's
-// address is looked up once per device with cudaGetSymbolAddress, on the first call made with that device current;
-// later calls only launch. The kernel clears the per-body colouring words it relies on at the start of every call,
-// so nothing in the array has to start at zero. Two calls that overlap on one device share the array and race:
-// callers serialise them (one stream, or an event between streams).
+// address belongs to a CUDA context, not to a device ordinal: it is looked up with cudaGetSymbolAddress on the first
+// call made in each context (the first call on a device, and again after a cudaDeviceReset or under another context
+// made current on that device) and cached under the context's process-unique id; later calls in that context only
+// launch. The kernel clears the per-body colouring words it relies on at the start of every call, so nothing in the
+// array has to start at zero. Two calls that overlap on one device share the array and race: callers serialise them
+// (one stream, or an event between streams).
 #include "ag2d.h"
 #include "ag2d_solver.cuh"
+
+#include <cuda.h>   // driver API types only; the two context queries are reached through cudaGetDriverEntryPoint
 
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 
 namespace ag2d {
 
@@ -76,10 +81,40 @@ void set_last_error(const std::string& message);   // the thread's ag2d_last_err
 
 namespace {
 
-// Scratch address per device ordinal, filled on the first call with that device current.
-constexpr int MAX_DEVICES = 64;
+// Scratch address per CUDA context, keyed by the context's id (cuCtxGetId: unique for the life of the process, so a
+// context created after a reset never finds the address of the one it replaced, even at the same CUcontext value).
 std::mutex g_scratchMutex;
-unsigned char* g_scratchPtr[MAX_DEVICES] = {};
+std::unordered_map<unsigned long long, unsigned char*> g_scratchByContext;
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Id of the calling thread's current context; 0 when no context is current or the driver cannot say (the caller
+// then looks the address up without caching it).
+unsigned long long current_context_id()
+{
+    static CtxGetCurrentFn getCurrent = nullptr;
+    static CtxGetIdFn getId = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            getCurrent = reinterpret_cast<CtxGetCurrentFn>(p);
+        p = nullptr;
+        q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            getId = reinterpret_cast<CtxGetIdFn>(p);
+    });
+    if (!getCurrent || !getId) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (getCurrent(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (getId(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
@@ -112,19 +147,31 @@ int32_t ag2d_solve_noalloc(const ag2d_solve_view* view, ag2d_manifold* manifolds
         !aligned16(view->materials))
         return fail(AG2D_ERR_INVALID_ARG, "manifold, body and material arrays must be 16-byte aligned");
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
-        return fail(AG2D_ERR_NO_DEVICE, "no current CUDA device");
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return fail(AG2D_ERR_NO_DEVICE, "no current CUDA device");
+    // An error left by the caller's earlier work is reported as such and left in place for the caller, so that the
+    // launch check below only ever sees this call's own launch.
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess)
+        return fail(AG2D_ERR_CUDA, std::string("a CUDA error from earlier work is pending (not cleared): ") +
+                                       cudaGetErrorString(pending));
     unsigned char* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_scratchMutex);
-        if (!g_scratchPtr[dev]) {
+        const unsigned long long ctx = current_context_id();
+        const auto hit = ctx ? g_scratchByContext.find(ctx) : g_scratchByContext.end();
+        if (hit != g_scratchByContext.end()) {
+            scratch = hit->second;
+        } else {
+            // Set-up for this context: the device address of the static array as this context maps it.
             void* p = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&p, g_solveScratch);
             if (e != cudaSuccess)
                 return fail(AG2D_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            g_scratchPtr[dev] = static_cast<unsigned char*>(p);
+            scratch = static_cast<unsigned char*>(p);
+            // The lookup may have made the device's primary context current: key by the context now current.
+            const unsigned long long now = current_context_id();
+            if (now) g_scratchByContext[now] = scratch;
         }
-        scratch = g_scratchPtr[dev];
     }
     DeviceWorld w{};
     w.nBodies = view->n_bodies;
