@@ -85,7 +85,14 @@ def parse():
     ap.add_argument("--round-steps", type=int, default=8, help="c5 steps between admission rounds")
     ap.add_argument("--reserve-bodies", type=int, default=4_000_000,
                     help="c5 resident bodies the server sizes its batch for at start-up")
+    ap.add_argument("--window-start", type=int, default=300,
+                    help="c4: first step of the timed window (both arms step every world from rest to it)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="c4: leave out the c3 collision-detection and c5 serving sub-results of the default line")
+    ap.add_argument("--extra-requests", type=int, default=2000, help="c5 arrivals of the default line's c5 part")
     a = ap.parse_args()
+    if a.window_start < a.warmup:
+        ap.error("--window-start must be at least --warmup")
     if a.steps is None:
         a.steps = DEFAULT_STEPS[a.workload]
     if a.bodies is None:
@@ -347,17 +354,87 @@ def cpu_worlds_rate(scene_list, seconds, threads, max_steps=600, ccd=False):
     return done[0] / (time.perf_counter() - t0)
 
 
-def cpu_c4(scene_list, seconds):
+def cpu_worlds_window(scene_list, start, steps, threads, single_thread_worlds=0):
+    """The reference engine over the step window [start, start + steps) of each world, on a pool of host threads
+    (ctypes releases the GIL): every world is built and stepped to `start` untimed, then, after all are there, the
+    pool steps every world through the window and the wall clock of that phase alone is the time. Returns
+    (body-steps/s with `threads` threads, body-steps/s of one thread over the first `single_thread_worlds` worlds
+    or None)."""
+    from oracle import refapi
+    settled = []
+    lock = threading.Lock()
+    work = queue.Queue()
+    for sc in scene_list:
+        work.put(sc)
+
+    def settle():
+        while True:
+            try:
+                sc = work.get_nowait()
+            except queue.Empty:
+                return
+            sim = refapi.RefSim(sc, threads=0)
+            sim.update(start)
+            with lock:
+                settled.append((sc.n, sim))
+    pool = [threading.Thread(target=settle) for _ in range(threads)]
+    for t in pool:
+        t.start()
+    for t in pool:
+        t.join()
+    one = None
+    if single_thread_worlds:
+        # One thread, one world after another, over the window (these worlds are then past it: timed first).
+        sub = settled[:single_thread_worlds]
+        t0 = time.perf_counter()
+        for _, sim in sub:
+            sim.update(steps)
+        one = sum(n for n, _ in sub) * steps / (time.perf_counter() - t0)
+        settled = settled[single_thread_worlds:]
+    for item in settled:
+        work.put(item)
+
+    def run():
+        while True:
+            try:
+                _, sim = work.get_nowait()
+            except queue.Empty:
+                return
+            sim.update(steps)
+    pool = [threading.Thread(target=run) for _ in range(threads)]
+    t0 = time.perf_counter()
+    for t in pool:
+        t.start()
+    for t in pool:
+        t.join()
+    elapsed = time.perf_counter() - t0
+    for _, sim in settled:
+        sim.close()
+    return sum(n for n, _ in settled) * steps / elapsed, one
+
+
+def c4_cpu_sample(scene_list):
+    """Every 4th world of the batch (about a quarter of its bodies, the same size mix)."""
+    stride = 4 if len(scene_list) >= 64 else 1
+    return scene_list[::stride], stride
+
+
+def cpu_c4(scene_list, start, steps):
     from oracle import refapi
     if not refapi.available():
         return None
     threads = host_threads()
-    stride = max(1, len(scene_list) // 256)
-    value = cpu_worlds_rate(scene_list[::stride], seconds, threads)
+    sample, stride = c4_cpu_sample(scene_list)
+    one_worlds = min(64, len(sample) // 4)
+    value, one = cpu_worlds_window(sample, start, steps, threads, one_worlds)
     return {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
             "sample": f"reference engine (oracle/_ref, -O2 -mavx2 -mfma), one single-threaded Simulation per world, "
-                      f"{threads} worlds at a time, every {stride}-th world of the batch stepped from rest in chunks "
-                      f"of 10 steps for {seconds:.0f} s"}
+                      f"every {stride}-th world of the batch ({len(sample)} worlds), each stepped to step {start} "
+                      f"untimed, then steps {start}..{start + steps} timed on {threads} host threads (wall clock of "
+                      f"that phase)",
+            "single_thread": {"value": one, "cores": 1,
+                              "sample": f"the first {one_worlds} of those worlds one after another on one thread, "
+                                        f"same window"}}
 
 
 def cpu_c2(scene, seconds):
@@ -391,6 +468,34 @@ def cpu_c3(scene, reps):
     return {"seconds": statistics.median(times), "pairs": pairs, "manifolds": mans, "threads": threads + 1}
 
 
+def window_name(args):
+    return f"steps {args.window_start}..{args.window_start + args.steps} of every world (stepped from rest)"
+
+
+def reference_c3_extra(args):
+    """The reference's collision-detection pass over the c3 world (the c3 line's CPU number)."""
+    scene = c3_scene(1_000_000)
+    r = cpu_c3(scene, 3)
+    from ag2d import roofline
+    step_b = roofline.broad_narrow_bytes_per_step(scene.n, mean_shape_bytes([scene]), r["pairs"], r["manifolds"])
+    return {"workload": WORKLOADS["c3"], "value": scene.n / r["seconds"], "unit": METRIC,
+            "ms_per_pass": 1e3 * r["seconds"], "pairs": r["pairs"], "manifolds": r["manifolds"],
+            "broadphase_gbs": step_b / r["seconds"] / 1e9, "cores": r["threads"],
+            "sample": "median of 3 collision-detection passes (spatial data, broad, narrow; agref_timed_collide)"}
+
+
+def reference_c5_extra(args):
+    """The reference serving c5 requests: a pool of host threads, one single-threaded Simulation per request."""
+    scene_list = c5_requests(256, 0)
+    threads = host_threads()
+    seconds = 15.0
+    value = cpu_worlds_rate(scene_list, seconds, threads, max_steps=120, ccd=True)
+    return {"workload": WORKLOADS["c5"], "value": value, "unit": METRIC, "cores": threads,
+            "sample": f"the first {len(scene_list)} requests of the stream, one single-threaded Simulation each "
+                      f"(CCD on), {threads} at a time, 120 steps each, {seconds:.0f} s of serving; arrivals are not "
+                      f"replayed on the host, so no latency"}
+
+
 # ---------------------------------------------------------------------------------------------------------------
 # Reference arm
 # ---------------------------------------------------------------------------------------------------------------
@@ -408,16 +513,17 @@ def run_reference(args):
             "data": "synthetic (seeded scene generator, ag2d.scenes)"}
     if args.workload == "c4":
         scene_list = c4_scenes(args.worlds, 0)
-        threads = host_threads()
-        stride = max(1, len(scene_list) // 256)
-        seconds = min(budget, 10.0 * max(args.steps, 1) / 60.0 + 20.0)
-        value = cpu_worlds_rate(scene_list[::stride], seconds, threads)
-        sample = (f"every {stride}-th world, one single-threaded Simulation per world, {threads} at a time, "
-                  f"{seconds:.0f} s of stepping from rest")
+        r = cpu_c4(scene_list, args.window_start, args.steps)
+        value, threads, sample = r["value"], r["cores"], r["sample"]
         bodies = int(sum(s.n for s in scene_list))
         line = dict(base, value=value, steps=args.steps, ms_per_step=1e3 * bodies / value,
                     config={"workload": WORKLOADS["c4"], "worlds": args.worlds, "bodies": bodies,
-                            "ms_per_step": "equivalent time of one step of the whole batch at this rate"})
+                            "window": window_name(args),
+                            "ms_per_step": "equivalent time of one step of the whole batch at this rate"},
+                    single_thread=r["single_thread"])
+        if not args.no_extras:
+            line["c3"] = reference_c3_extra(args)
+            line["c5"] = reference_c5_extra(args)
     elif args.workload == "c2":
         scene = c2_scene(args.bodies)
         threads = max(0, host_threads() - 1)
@@ -474,21 +580,23 @@ def run_c4(args, torch, dist, rank, world_size, local, dev):
         w = ag2d.World(**settings)
         w.add_scene(sc)
         worlds.append(w)
+    start, W, K = args.window_start, args.warmup, args.steps
     batch = ag2d.Batch(worlds)
     e = batch.engine
     stream = torch.cuda.ExternalStream(e.stream(), device=dev)
-    # Launch shapes are tuned on a copy of the batch stepped ahead into the settled part of the run (the contact
-    # count of the first steps is far below the later one's); results do not depend on them.
+    # Untimed: the batch steps from rest to the window's start (the reference arm steps the same worlds the same
+    # way). Launch shapes are tuned on a copy restored from a checkpoint there; results do not depend on them.
+    batch.step(start - W)
     if args.no_autotune:
         tuning = None   # the engine's default launch shapes (the settled-state choice on this workload)
     else:
-        ahead = ag2d.Batch(worlds)
-        ahead.step(args.tune_ahead)
+        ahead = ag2d.Batch.restore(batch.save())
         tuning = ahead.engine.autotune(2)
         ahead.close()
         del ahead
         e.set_tuning(tuning)
-    batch.step(args.warmup)
+    batch.step(W)
+    ckpt = batch.save()   # host checkpoint at the window's start, for the end-to-end run below
     e.set_profiling(True)
     c0 = e.counters()
     if world_size > 1:
@@ -503,13 +611,12 @@ def run_c4(args, torch, dist, rank, world_size, local, dev):
     timer = Timer(torch, stream, dev)
     sampler = ClockSampler(local)
     sampler.start()
-    total_ms = timer.run(lambda: batch.step(1), args.steps, acc)
+    total_ms = timer.run(lambda: batch.step(1), K, acc)
     torch.cuda.synchronize()
     if world_size > 1:
         dist.barrier()
     clocks = sampler.stop()
     c1 = e.counters()
-    K = args.steps
     value, max_s, job_steps = job_rate(torch, dist, world_size, dev, n_bodies * K, total_ms / 1e3)
     max_ms, job_bodies = max_s * 1e3, job_steps / K
     phases = e.phase_times()
@@ -520,23 +627,35 @@ def run_c4(args, torch, dist, rank, world_size, local, dev):
     roof = roofline_line(phases, bytes_by_phase, kernel_of, "c4")
     del batch, e
 
-    # End to end through the C ABI: a batch packed from the host-created worlds and uploaded inside the timed
-    # region, then per step one ag2d_batch_step and a readback of every body's pose (x, y, rotation).
-    e2e_steps = min(K, 200)
+    # End to end through the C ABI, over the same window: the batch restored from the host checkpoint of the
+    # window's start (page-locked; uploaded inside the timed region), then per step one ag2d_batch_step and a read
+    # of every body's pose (x, y, rotation) into page-locked host memory. The read of step k is queued after it
+    # and lands while step k + 1 runs; the loop waits for it before queuing the next (a consumer one frame behind).
+    e2e_steps = K
+    pose_ring = None
     if world_size > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    b2 = ag2d.Batch(worlds)
-    for _ in range(e2e_steps):
+    b2 = ag2d.Batch.restore(ckpt)
+    if tuning:
+        b2.engine.set_tuning(tuning)
+    pose_bytes = b2.engine.field_bytes(ag2d.BODY_POSE)
+    pose_ring = [ag2d.host_empty(pose_bytes), ag2d.host_empty(pose_bytes)]
+    for k in range(e2e_steps):
         b2.step(1)
-        pose = b2.engine.read(ag2d.BODY_POSE)
+        b2.engine.read_wait()
+        b2.engine.read_async(ag2d.BODY_POSE, pose_ring[k & 1])
+    b2.engine.read_wait()
     torch.cuda.synchronize()
     e2e_s = reduce_max(torch, dist, world_size, dev, time.perf_counter() - t0)
     e2e = {"value": job_bodies * e2e_steps / e2e_s, "unit": METRIC,
-           "h2d_bytes_per_step": upload_bytes(scene_list) / e2e_steps, "d2h_bytes_per_step": int(pose.nbytes),
-           "steps": e2e_steps}
-    del b2, pose
+           "h2d_bytes_per_step": ckpt.nbytes / e2e_steps, "d2h_bytes_per_step": int(pose_bytes),
+           "steps": e2e_steps, "window": window_name(args),
+           "timed": "ag2d_batch_restore from a page-locked host checkpoint of the window's start (in the timed "
+                    "region), then per step ag2d_batch_step + ag2d_world_read_async of every body pose into "
+                    "page-locked memory, waited for one step later; wall clock"}
+    del b2, pose_ring
 
     # The same worlds, one launch sequence per world per step (a Simulation per world): every k-th world.
     stride = max(1, len(worlds) // max(1, args.per_world_sample))
@@ -554,23 +673,26 @@ def run_c4(args, torch, dist, rank, world_size, local, dev):
     pw_bodies = sum(scene_list[k].n for k in range(0, len(worlds), stride))
     per_world = reduce_sum(torch, dist, world_size, dev, pw_bodies * pw_steps / pw_s)
     per_world_line = {"value": per_world, "unit": METRIC,
-                      "sample": f"every {stride}-th world ({len(sample)} worlds), {pw_steps} steps each after "
-                                f"{args.warmup} warm-up steps, each world its own ag2d_world_step launch sequence, "
-                                f"wall clock (host launch bound)",
+                      "sample": f"every {stride}-th world ({len(sample)} worlds), steps {args.warmup}.."
+                                f"{args.warmup + pw_steps} from rest, each world its own ag2d_world_step launch "
+                                f"sequence, wall clock (host launch bound; the early steps have fewer contacts "
+                                f"than the batched window, which favours this form)",
                       "batched_over_per_world": value / per_world}
     del sample
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline:
-        cpu = cpu_c4(scene_list, args.cpu_seconds)
+        cpu = cpu_c4(scene_list, start, K)
     return {
-        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world_size, "steps": K, "warmup": args.warmup,
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world_size, "steps": K, "warmup": W,
         "ms_per_step": max_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32", "data": "synthetic (seeded scene generator, ag2d.scenes.make_c4_worlds)",
         "config": {"workload": WORKLOADS["c4"], "worlds_per_gpu": len(scene_list), "bodies_per_gpu": n_bodies,
+                   "window": window_name(args),
                    "parallelism": f"independent worlds x{world_size} GPUs (no step-path collective)",
-                   "autotuned": tuning, "steps_before_timing": f"{args.warmup} warm-up (launch shapes tuned on a copy stepped {args.tune_ahead} "
-                                          f"steps ahead)",
+                   "autotuned": tuning,
+                   "steps_before_timing": f"{start - W} settling steps, launch shapes tuned on a copy restored "
+                                          f"there, then {W} warm-up steps",
                    "l2": "flushed between timed steps (256 MiB write outside the events)",
                    "mean_pairs_per_step": sums["pairs"] / K, "mean_manifolds_per_step": sums["manifolds"] / K},
         "per_world_launch": per_world_line,
@@ -844,6 +966,21 @@ def run_c5(args, torch, dist, rank, world_size, local, dev):
     return line
 
 
+def extra_args(args, workload):
+    """Arguments of a sub-run of the default line: the workload's own defaults, shortened where they are long."""
+    a = argparse.Namespace(**vars(args))
+    a.workload = workload
+    if workload == "c3":
+        a.steps, a.bodies, a.warmup = 20, 1_000_000, max(3, args.warmup)
+    else:
+        a.steps, a.requests, a.cpu_seconds = DEFAULT_STEPS["c5"], args.extra_requests, min(args.cpu_seconds, 10.0)
+    return a
+
+
+def pick(d, keys):
+    return {k: d[k] for k in keys if k in d}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -856,6 +993,22 @@ def run_ours(args):
     dev = torch.device(f"cuda:{local}")
     fn = {"c4": run_c4, "c2": run_c2, "c3": run_c3, "c5": run_c5}[args.workload]
     line = fn(args, torch, dist, rank, world_size, local, dev)
+    if args.workload == "c4" and not args.no_extras:
+        # The rest of the headline metric: broad+narrow GB/s of the 1M-body pass and the serving latency.
+        import gc
+        gc.collect()
+        torch.cuda.synchronize()
+        c3 = run_c3(extra_args(args, "c3"), torch, dist, rank, world_size, local, dev)
+        line["c3"] = pick(c3, ("value", "unit", "ms_per_step", "broadphase_gbs", "roofline", "cpu_baseline",
+                               "e2e", "gpu_launches", "clocks", "phase_ms_per_step"))
+        line["c3"]["config"] = c3["config"]
+        gc.collect()
+        c5 = run_c5(extra_args(args, "c5"), torch, dist, rank, world_size, local, dev)
+        line["c5"] = pick(c5, ("value", "unit", "latency_ms", "serving", "cpu_baseline", "clocks", "config"))
+        line["broadphase_gbs"] = c3["broadphase_gbs"]
+        line["broadphase_roofline_frac"] = c3["roofline"]["frac"]
+        line["serving_p50_ms"] = c5["latency_ms"]["p50"]
+        line["serving_p99_ms"] = c5["latency_ms"]["p99"]
     if rank == 0:
         print(json.dumps(line))
     if world_size > 1:

@@ -246,6 +246,20 @@ int32_t ag2d_world_query_circle_contacts(ag2d_world* world, float x, float y, fl
  * Replaces the reference's SoA viewers (ObjectAPI::getBodies/getColliders, ObjectAPI.h:96-101) and
  * Simulation::getBodyCollisionData (Simulation.h:186). */
 int32_t ag2d_world_read(ag2d_world* world, int32_t field, void* dst, uint64_t capacity_bytes, uint64_t* out_bytes);
+/* Body and collider fields (the reference's per-frame BodySoA / ColliderSoA viewers, ObjectAPI::getBodies /
+ * getColliders, ObjectAPI.h:97-101, read by its renderer every frame) without waiting: the values as they stand
+ * after the work queued so far are packed on the device and copied into 'dst' on a copy stream while the next
+ * steps run. 'dst' must be page-locked (ag2d_host_alloc, cudaHostAlloc or cudaHostRegister) and stay untouched
+ * until ag2d_world_read_wait returns. Up to four reads may be in flight; a fifth waits on the device for the first
+ * one's copy. Phase-tap fields (pairs, manifolds, ...) return AG2D_ERR_UNSUPPORTED. */
+int32_t ag2d_world_read_async(ag2d_world* world, int32_t field, void* dst, uint64_t capacity_bytes,
+                              uint64_t* out_bytes);
+/* Blocks until every ag2d_world_read_async of this world has landed in host memory. */
+int32_t ag2d_world_read_wait(ag2d_world* world);
+/* Page-locked host memory (cudaHostAlloc): destinations for asynchronous reads and checkpoints, one DMA per copy.
+ * No reference counterpart (the reference's state lives in host memory). */
+int32_t ag2d_host_alloc(uint64_t bytes, void** out_ptr);
+int32_t ag2d_host_free(void* ptr);
 /* Overwrites a field from host memory (body state, pairs, manifolds) for phase-level parity runs. */
 int32_t ag2d_world_write(ag2d_world* world, int32_t field, const void* src, uint64_t bytes);
 /* Runs one phase (enum ag2d_phase) on the current device state. */
@@ -266,6 +280,13 @@ int32_t ag2d_batch_engine(ag2d_batch* batch, ag2d_world** out_world);
 int32_t ag2d_batch_read(ag2d_batch* batch, uint32_t world, int32_t field, void* dst, uint64_t capacity_bytes,
                         uint64_t* out_bytes);
 int32_t ag2d_batch_destroy(ag2d_batch* batch);
+/* Checkpoint of a batch: every resident array (body and collider state, shapes, materials, collider poses and
+ * AABBs), the warm-start manifolds with their colours and the world partition, in one self-describing host blob.
+ * Pass dst = NULL to get the size. A batch restored from it steps on exactly as the saved batch does (bit for bit);
+ * a page-locked source (ag2d_host_alloc) goes over in one DMA per array. 'device' < 0 keeps the saved device.
+ * No reference counterpart: the reference keeps its state in host memory and has no save / load of a Simulation. */
+int32_t ag2d_batch_save(ag2d_batch* batch, void* dst, uint64_t capacity_bytes, uint64_t* out_bytes);
+int32_t ag2d_batch_restore(const void* src, uint64_t bytes, int32_t device, ag2d_batch** out_batch);
 
 /* ---- request server: world rollouts served from one resident, continuously repacked batch ----
  * No counterpart in the reference (it steps one Simulation per caller). A server owns one device batch and a host

@@ -144,6 +144,12 @@ def _load():
     L.ag2d_world_body_count.argtypes = [vp, ctypes.POINTER(u32), ctypes.POINTER(u32)]
     L.ag2d_world_read.argtypes = [vp, i32, vp, u64, ctypes.POINTER(u64)]
     L.ag2d_world_write.argtypes = [vp, i32, vp, u64]
+    L.ag2d_world_read_async.argtypes = [vp, i32, vp, u64, ctypes.POINTER(u64)]
+    L.ag2d_world_read_wait.argtypes = [vp]
+    L.ag2d_host_alloc.argtypes = [u64, ctypes.POINTER(vp)]
+    L.ag2d_host_free.argtypes = [vp]
+    L.ag2d_batch_save.argtypes = [vp, vp, u64, ctypes.POINTER(u64)]
+    L.ag2d_batch_restore.argtypes = [vp, u64, i32, ctypes.POINTER(vp)]
     L.ag2d_world_run_phase.argtypes = [vp, i32]
     L.ag2d_world_set_profiling.argtypes = [vp, i32]
     L.ag2d_world_autotune.argtypes = [vp, i32, ctypes.POINTER(Tuning)]
@@ -187,6 +193,47 @@ lib = _Lib()
 def _check(code: int):
     if code != OK:
         raise Ag2dError(code, lib.ag2d_last_error_string().decode(errors="replace"))
+
+
+class _HostBlock:
+    """Page-locked host memory from ag2d_host_alloc, freed with the last array that views it."""
+
+    def __init__(self, nbytes: int):
+        p = ctypes.c_void_p()
+        _check(lib.ag2d_host_alloc(max(int(nbytes), 1), ctypes.byref(p)))
+        self.p = p.value
+        self.nbytes = int(nbytes)
+
+    def __del__(self):
+        try:
+            if self.p:
+                lib.ag2d_host_free(self.p)
+                self.p = None
+        except Exception:
+            pass
+
+
+def host_empty(nbytes: int) -> np.ndarray:
+    """A uint8 array of `nbytes` in page-locked host memory: the destination asynchronous reads require, and the
+    fastest one for reads and checkpoints (one DMA, no staging). View it with .view(dtype) as needed."""
+    block = _HostBlock(nbytes)
+    raw = (ctypes.c_uint8 * max(block.nbytes, 1)).from_address(block.p)
+    raw._ag2d_block = block   # the ctypes array keeps the allocation alive; numpy keeps the ctypes array
+    return np.frombuffer(raw, dtype=np.uint8)[:block.nbytes]
+
+
+def _field_view(buf: np.ndarray, field: int) -> np.ndarray:
+    if field in (MANIFOLDS, PREV_MANIFOLDS):
+        return buf.view(MANIFOLD_DTYPE)
+    if field == PAIRS:
+        return buf.view(np.uint32).reshape(-1, 2)
+    return buf.view(np.uint32 if field in _U32_FIELDS else np.float32)
+
+
+def _out_bytes(out: np.ndarray):
+    if not out.flags["C_CONTIGUOUS"]:
+        raise ValueError("destination must be C-contiguous")
+    return out.ctypes.data, out.nbytes
 
 
 def device_count() -> int:
@@ -421,16 +468,33 @@ class World:
         return int(b.value), int(c.value)
 
     # --- field access ---
-    def read(self, field: int) -> np.ndarray:
+    def field_bytes(self, field: int) -> int:
+        """Bytes a read of `field` returns (body and collider fields: no device access)."""
         n = ctypes.c_uint64()
         _check(lib.ag2d_world_read(self.h, field, None, 0, ctypes.byref(n)))
-        buf = np.empty(int(n.value), dtype=np.uint8)
-        _check(lib.ag2d_world_read(self.h, field, buf.ctypes.data if buf.size else None, buf.size, ctypes.byref(n)))
-        if field in (MANIFOLDS, PREV_MANIFOLDS):
-            return buf.view(MANIFOLD_DTYPE)
-        if field == PAIRS:
-            return buf.view(np.uint32).reshape(-1, 2)
-        return buf.view(np.uint32 if field in _U32_FIELDS else np.float32)
+        return int(n.value)
+
+    def read(self, field: int, out: np.ndarray = None) -> np.ndarray:
+        """A field as a host array; with `out` (any contiguous array large enough, page-locked for the fastest
+        copy) the values land there and a view of its first bytes is returned."""
+        if out is None:
+            out = np.empty(self.field_bytes(field), dtype=np.uint8)
+        ptr, cap = _out_bytes(out)
+        n = ctypes.c_uint64()
+        _check(lib.ag2d_world_read(self.h, field, ptr if cap else None, cap, ctypes.byref(n)))
+        return _field_view(out.reshape(-1).view(np.uint8)[:int(n.value)], field)
+
+    def read_async(self, field: int, out: np.ndarray) -> np.ndarray:
+        """Queues a read of a body or collider field into page-locked `out` (ag2d.host_empty); the copy overlaps the
+        steps that follow. The values are valid after read_wait()."""
+        ptr, cap = _out_bytes(out)
+        n = ctypes.c_uint64()
+        _check(lib.ag2d_world_read_async(self.h, field, ptr, cap, ctypes.byref(n)))
+        return _field_view(out.reshape(-1).view(np.uint8)[:int(n.value)], field)
+
+    def read_wait(self):
+        """Waits until every read_async of this world has landed."""
+        _check(lib.ag2d_world_read_wait(self.h))
 
     def write(self, field: int, data: np.ndarray):
         if field in (MANIFOLDS, PREV_MANIFOLDS):
@@ -451,22 +515,50 @@ class Batch:
         arr = (ctypes.c_void_p * len(worlds))(*[w.h for w in worlds])
         h = ctypes.c_void_p()
         _check(lib.ag2d_batch_create(arr, len(worlds), ctypes.byref(h)))
+        self._adopt(h)
+
+    def _adopt(self, h):
         self.h = h
-        self.n_worlds = len(worlds)
+        n = ctypes.c_uint32()
+        _check(lib.ag2d_batch_world_count(self.h, ctypes.byref(n)))
+        self.n_worlds = int(n.value)
         e = ctypes.c_void_p()
         _check(lib.ag2d_batch_engine(self.h, ctypes.byref(e)))
         self.engine = World._borrowed(e, self)
 
+    @classmethod
+    def restore(cls, blob: np.ndarray, device: int = -1) -> "Batch":
+        """A batch from a checkpoint (Batch.save); it steps on exactly as the saved batch does. A page-locked blob
+        (ag2d.host_empty) goes over in one DMA per array."""
+        ptr, nbytes = _out_bytes(blob)
+        h = ctypes.c_void_p()
+        _check(lib.ag2d_batch_restore(ptr, nbytes, device, ctypes.byref(h)))
+        b = cls.__new__(cls)
+        b._adopt(h)
+        return b
+
+    def save(self, out: np.ndarray = None) -> np.ndarray:
+        """Checkpoint of the whole batch as a uint8 array (page-locked unless `out` is given)."""
+        n = ctypes.c_uint64()
+        _check(lib.ag2d_batch_save(self.h, None, 0, ctypes.byref(n)))
+        if out is None:
+            out = host_empty(int(n.value))
+        ptr, cap = _out_bytes(out)
+        _check(lib.ag2d_batch_save(self.h, ptr, cap, ctypes.byref(n)))
+        return out.reshape(-1).view(np.uint8)[:int(n.value)]
+
     def step(self, steps: int = 1):
         _check(lib.ag2d_batch_step(self.h, steps))
 
-    def read(self, world: int, field: int) -> np.ndarray:
+    def read(self, world: int, field: int, out: np.ndarray = None) -> np.ndarray:
         """A body field, collider field or the manifolds of one world, in that world's own indices."""
         n = ctypes.c_uint64()
-        _check(lib.ag2d_batch_read(self.h, world, field, None, 0, ctypes.byref(n)))
-        buf = np.empty(int(n.value), dtype=np.uint8)
-        _check(lib.ag2d_batch_read(self.h, world, field, buf.ctypes.data if buf.size else None, buf.size,
-                                   ctypes.byref(n)))
+        if out is None:
+            _check(lib.ag2d_batch_read(self.h, world, field, None, 0, ctypes.byref(n)))
+            out = np.empty(int(n.value), dtype=np.uint8)
+        ptr, cap = _out_bytes(out)
+        _check(lib.ag2d_batch_read(self.h, world, field, ptr if cap else None, cap, ctypes.byref(n)))
+        buf = out.reshape(-1).view(np.uint8)[:int(n.value)]
         if field in (MANIFOLDS, PREV_MANIFOLDS):
             return buf.view(MANIFOLD_DTYPE)
         return buf.view(np.uint32 if field in _U32_FIELDS else np.float32)

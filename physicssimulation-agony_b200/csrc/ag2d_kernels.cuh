@@ -140,5 +140,11 @@ cudaError_t launch_gather(T* dst, const T* srcOld, const T* srcNew, const Gather
                           const unsigned long long* sections, uint32_t nsec, uint32_t section);
 __global__ void k_world_of(const uint32_t* starts, uint32_t worlds, uint32_t n, uint32_t* out);
 __global__ void k_fill_u32(uint32_t* out, uint32_t n, uint32_t value);
+// Host reads: how k_extract packs a field (EXTRACT_DIRECT fields are copied as they lie).
+enum ExtractKind : uint32_t {
+    EXTRACT_DIRECT = 0, EXTRACT_F4_COMP, EXTRACT_F4_XYZ, EXTRACT_F2_COMP, EXTRACT_U8_U32, EXTRACT_ISLAND
+};
+__global__ void k_extract(const void* src, uint32_t lo, uint32_t n, uint32_t kind, uint32_t comp, uint32_t bias,
+                          void* out);
 
 }  // namespace ag2d

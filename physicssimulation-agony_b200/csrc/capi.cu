@@ -253,6 +253,28 @@ struct StagedWorld {
     uint64_t sec[NSEC] = {};
 };
 
+// Checkpoint of an engine (ag2d_batch_save / ag2d_batch_restore): a header, then one section per resident array at
+// 256-byte aligned offsets, in device layout with batch-global indices. It holds everything a step reads from the
+// previous one (body and collider state, collider poses and AABBs, the warm-start manifolds with their colours, the
+// world partition), so that a restored engine steps on exactly as the saved one would.
+enum CkptSection : uint32_t {
+    CK_VEL, CK_POS, CK_ROT, CK_WRAP, CK_BOUND, CK_TIMER, CK_STATE, CK_ISLAND,
+    CK_CBODY, CK_CSHAPE, CK_CMAT, CK_COFF, CK_CPOSE, CK_CAABB, CK_CROT, CK_MINEXT,
+    CK_CIRCLE, CK_BOXHALF, CK_POLYOFF, CK_POLYCOUNT, CK_POLYVERTS, CK_POLYNORMALS, CK_MATS, CK_PREV,
+    CK_PREVCOLOR, CK_WBODY, CK_WCOL, NCK
+};
+constexpr char CKPT_MAGIC[8] = {'A', 'G', '2', 'D', 'C', 'K', 'P', 'T'};
+constexpr uint32_t CKPT_VERSION = 1;
+struct CkptHeader {
+    char magic[8];
+    uint32_t version, headerBytes;
+    ag2d_world_settings settings;
+    uint32_t nWorlds, nBodies, nColliders, nCircles, nBoxes, nPolygons, nPolyVerts, nMaterialRows;
+    uint32_t nPrev, nStatic, lastManifolds, reserved;
+    uint64_t totalBytes;
+    uint64_t off[NCK], len[NCK];
+};
+
 // One world's state in the upload format (host arrays), and the warm-start manifolds.
 struct PackedArrays {
     std::vector<float4> vel, pos, co, mats;
@@ -494,6 +516,23 @@ struct ag2d_world {
     DBuf<uint32_t> bk_prevColor;
     DBuf<unsigned long long> stagedSections;   // [joining world][section] byte offsets into 'staging'
     PinnedBuf hostStage, hostOut;              // page-locked copies of the staged blobs and the leaving bodies
+    // Host reads: fields packed on the device (k_extract) into readStage, then copied straight into a page-locked
+    // destination, or through two page-locked halves of readBounce (the copy of one chunk overlaps the host copy
+    // of the previous one) into pageable memory.
+    DBuf<uint8_t> readStage;
+    PinnedBuf readBounce;
+    cudaEvent_t readEv[2] = {nullptr, nullptr};
+    // Asynchronous reads: a ring of device staging buffers; each read packs on the engine stream and copies on
+    // copyStream, so the copy overlaps the steps launched after it.
+    static constexpr int NASYNC = 4;
+    struct AsyncSlot {
+        DBuf<uint8_t> buf;
+        cudaEvent_t packed = nullptr, done = nullptr;
+        bool used = false;
+    };
+    AsyncSlot asyncSlot[NASYNC];
+    uint32_t asyncNext = 0;
+    cudaStream_t copyStream = nullptr;
     DBuf<uint32_t> queryFlag, queryOffset, queryList, queryCount;   // spatial query scratch
     DBuf<float> queryDist, queryListDist;
     DBuf<GatherSeg> gatherSegs;
@@ -930,8 +969,136 @@ struct ag2d_world {
         fullPose = true;
     }
 
+    // Checkpoint layout of the current state (counts from the host's view of the engine; the warm-start count is
+    // read from the device).
+    CkptHeader checkpointLayout()
+    {
+        ensureUploaded();
+        CkptHeader h{};
+        std::memcpy(h.magic, CKPT_MAGIC, sizeof(h.magic));
+        h.version = CKPT_VERSION;
+        h.headerBytes = sizeof(CkptHeader);
+        h.settings = settings;
+        h.nWorlds = nWorlds;
+        h.nBodies = nBodies; h.nColliders = nColliders; h.nCircles = nCircles; h.nBoxes = nBoxes;
+        h.nPolygons = nPolygons; h.nPolyVerts = nPolyVerts; h.nMaterialRows = nMaterialRows;
+        h.nStatic = nStatic;
+        h.lastManifolds = lastManifolds;
+        CK(cudaMemcpyAsync(&h.nPrev, nPrev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        const uint64_t b = nBodies, c = nColliders, m = h.nPrev, wp = uint64_t(nWorlds) + 1;
+        const uint64_t len[NCK] = {
+            b * 16, b * 16, b * 8, b * 4, b * 4, b * 4, b, b * 4,
+            c * 4, c * 4, c * 4, c * 16, c * 16, c * 16, c * 4, c * 4,
+            uint64_t(nCircles) * 4, uint64_t(nBoxes) * 8, uint64_t(nPolygons) * 4, uint64_t(nPolygons) * 4,
+            uint64_t(nPolyVerts) * 8, uint64_t(nPolyVerts) * 8, uint64_t(nMaterialRows) * 16, m * sizeof(Manifold),
+            m * 4, wp * 4, wp * 4};
+        uint64_t at = (sizeof(CkptHeader) + 255) & ~uint64_t(255);
+        for (uint32_t k = 0; k < NCK; k++) {
+            h.off[k] = at;
+            h.len[k] = len[k];
+            at += (len[k] + 255) & ~uint64_t(255);
+        }
+        h.totalBytes = at;
+        return h;
+    }
+
+    // Writes the checkpoint into host memory 'dst' (h.totalBytes bytes): one transfer per section, all on the engine
+    // stream, then one wait.
+    void saveCheckpoint(const CkptHeader& h, uint8_t* dst)
+    {
+        const cudaStream_t s = stream;
+        std::memcpy(dst, &h, sizeof(h));
+        const void* src[NCK] = {bvel.p, bpos.p, brot.p, wrapCount.p, boundRadius.p, sleepTimer.p, bstate.p,
+                                sleepIsland.p, cbody.p, cshape.p, cmat.p, coff.p, cpose.p, caabb.p, cworldRot.p,
+                                minExtent.p, circleRadius.p, boxHalf.p, polyOffset.p, polyCount.p, polyVerts.p,
+                                polyNormals.p, materials.p, prevManifolds.p, prevColor.p, nullptr, nullptr};
+        for (uint32_t k = 0; k < CK_WBODY; k++)
+            if (h.len[k]) CK(cudaMemcpyAsync(dst + h.off[k], src[k], h.len[k], cudaMemcpyDeviceToHost, s));
+        std::vector<uint32_t> bs = hBodyStart, cs = hColStart;
+        if (nWorlds <= 1) { bs = {0, nBodies}; cs = {0, nColliders}; }
+        std::memcpy(dst + h.off[CK_WBODY], bs.data(), h.len[CK_WBODY]);
+        std::memcpy(dst + h.off[CK_WCOL], cs.data(), h.len[CK_WCOL]);
+        CK(cudaStreamSynchronize(s));
+    }
+
+    // Makes this (fresh) engine the state a checkpoint holds: every section goes over as it lies in the blob (one
+    // DMA each from page-locked memory), the world partition and the per-element world ids are rebuilt on the
+    // device, and the next step starts exactly as the saved engine's next step would (work lists and the static
+    // tree are rebuilt from the restored state, as after any change of state).
+    void restoreCheckpoint(const CkptHeader& h, const uint8_t* src)
+    {
+        ensureDevice();
+        const cudaStream_t s = stream;
+        nBodies = h.nBodies; nColliders = h.nColliders; nCircles = h.nCircles; nBoxes = h.nBoxes;
+        nPolygons = h.nPolygons; nPolyVerts = h.nPolyVerts; nMaterialRows = h.nMaterialRows; nStatic = h.nStatic;
+        nWorlds = std::max<uint32_t>(h.nWorlds, 1);
+        auto up = [&](auto& buf, uint32_t k, size_t count) {
+            buf.reserve(std::max<size_t>(count, 1));
+            if (h.len[k]) CK(cudaMemcpyAsync(buf.p, src + h.off[k], h.len[k], cudaMemcpyHostToDevice, s));
+        };
+        up(bvel, CK_VEL, nBodies); up(bpos, CK_POS, nBodies); up(brot, CK_ROT, nBodies);
+        up(wrapCount, CK_WRAP, nBodies); up(boundRadius, CK_BOUND, nBodies); up(sleepTimer, CK_TIMER, nBodies);
+        up(bstate, CK_STATE, nBodies); up(sleepIsland, CK_ISLAND, nBodies);
+        up(cbody, CK_CBODY, nColliders); up(cshape, CK_CSHAPE, nColliders); up(cmat, CK_CMAT, nColliders);
+        up(coff, CK_COFF, nColliders); up(cpose, CK_CPOSE, nColliders); up(caabb, CK_CAABB, nColliders);
+        up(cworldRot, CK_CROT, nColliders); up(minExtent, CK_MINEXT, nColliders);
+        up(circleRadius, CK_CIRCLE, nCircles); up(boxHalf, CK_BOXHALF, nBoxes); up(polyOffset, CK_POLYOFF, nPolygons);
+        up(polyCount, CK_POLYCOUNT, nPolygons); up(polyVerts, CK_POLYVERTS, nPolyVerts);
+        up(polyNormals, CK_POLYNORMALS, nPolyVerts); up(materials, CK_MATS, nMaterialRows);
+        objects.materials.assign(size_t(nMaterialRows) * 3, 0.0f);   // the material count the device view reads
+        const uint32_t* ws = reinterpret_cast<const uint32_t*>(src + h.off[CK_WBODY]);
+        const uint32_t* wc = reinterpret_cast<const uint32_t*>(src + h.off[CK_WCOL]);
+        hBodyStart.assign(ws, ws + nWorlds + 1);
+        hColStart.assign(wc, wc + nWorlds + 1);
+        sizeFor();
+        if (h.nPrev > manifoldCap) reserveCapacities(std::max(h.nPrev, pairCap), h.nPrev);
+        if (h.len[CK_PREV])
+            CK(cudaMemcpyAsync(prevManifolds.p, src + h.off[CK_PREV], h.len[CK_PREV], cudaMemcpyHostToDevice, s));
+        if (h.len[CK_PREVCOLOR])
+            CK(cudaMemcpyAsync(prevColor.p, src + h.off[CK_PREVCOLOR], h.len[CK_PREVCOLOR], cudaMemcpyHostToDevice, s));
+        prevCount = h.nPrev;
+        CK(cudaMemcpyAsync(nPrev.p, &prevCount, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        const uint32_t ones = std::max<uint32_t>(nBodies, 1);
+        k_fill_u32<<<gridFor(ones), 256, 0, s>>>(ccdHit.p, ones, ORDERED_ONE);
+        CK(cudaGetLastError());
+        if (nWorlds > 1) {
+            bodyWorld.reserve(std::max<uint32_t>(nBodies, 1));
+            colWorld.reserve(std::max<uint32_t>(nColliders, 1));
+            worldBodyStart.upload(hBodyStart.data(), hBodyStart.size(), s);
+            worldColStart.upload(hColStart.data(), hColStart.size(), s);
+            if (nBodies) k_world_of<<<gridFor(nBodies), 256, 0, s>>>(worldBodyStart.p, nWorlds, nBodies, bodyWorld.p);
+            if (nColliders)
+                k_world_of<<<gridFor(nColliders), 256, 0, s>>>(worldColStart.p, nWorlds, nColliders, colWorld.p);
+            CK(cudaGetLastError());
+            manSeg.reserve(nWorlds + 1);
+            nextWorld.reserve(2);
+            worldDirty.reserve(nWorlds);
+            CK(cudaMemsetAsync(worldDirty.p, 0, sizeof(uint32_t) * nWorlds, s));
+            setTeams(teamColliders, teamThreads);
+        }
+        CK(cudaStreamSynchronize(s));
+        hostDirty = false;
+        listsDirty = true;
+        otherDirty = true;
+        fullPose = false;
+        aabbValid = true;
+        newWorldsPending = false;
+        manSegFresh = false;
+        hintsReady = false;
+        lastManifolds = h.lastManifolds;
+    }
+
     ~ag2d_world()
     {
+        if (copyStream) cudaStreamSynchronize(copyStream);
+        for (auto& a : asyncSlot) {
+            if (a.packed) cudaEventDestroy(a.packed);
+            if (a.done) cudaEventDestroy(a.done);
+        }
+        for (auto& e : readEv)
+            if (e) cudaEventDestroy(e);
+        if (copyStream) cudaStreamDestroy(copyStream);
         for (auto& e : ev) {
             if (e[0]) cudaEventDestroy(e[0]);
             if (e[1]) cudaEventDestroy(e[1]);
@@ -2097,6 +2264,141 @@ int32_t ag2d_world_body_count(ag2d_world* world, uint32_t* out_bodies, uint32_t*
 
 // Field access ---------------------------------------------------------------------------------------------------
 
+// Host memory the device can copy into directly: page-locked by cudaHostAlloc or cudaHostRegister (any CUDA runtime
+// of the process; the driver tracks it).
+static bool page_locked(const void* p)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// How a per-body or per-collider field is read: its device array and how k_extract packs it.
+struct FieldSpec {
+    const void* src = nullptr;
+    uint32_t kind = EXTRACT_DIRECT, comp = 0;
+    uint32_t outBytes = 4;      // bytes per element as read
+    bool perCollider = false;
+};
+
+static bool field_spec(const ag2d_world& w, int32_t field, FieldSpec& f)
+{
+    auto c4 = [&](const void* p, uint32_t c) { f.src = p; f.kind = EXTRACT_F4_COMP; f.comp = c; };
+    auto c2 = [&](const void* p, uint32_t c) { f.src = p; f.kind = EXTRACT_F2_COMP; f.comp = c; };
+    switch (field) {
+    case AG2D_BODY_COM_X: c4(w.bpos.p, 0); break;
+    case AG2D_BODY_COM_Y: c4(w.bpos.p, 1); break;
+    case AG2D_BODY_ROTATION: c4(w.bpos.p, 2); break;
+    case AG2D_BODY_INV_INERTIA: c4(w.bpos.p, 3); break;
+    case AG2D_BODY_VEL_X: c4(w.bvel.p, 0); break;
+    case AG2D_BODY_VEL_Y: c4(w.bvel.p, 1); break;
+    case AG2D_BODY_ANGULAR_VELOCITY: c4(w.bvel.p, 2); break;
+    case AG2D_BODY_INV_MASS: c4(w.bvel.p, 3); break;
+    case AG2D_BODY_ROT_COS: c2(w.brot.p, 0); break;
+    case AG2D_BODY_ROT_SIN: c2(w.brot.p, 1); break;
+    case AG2D_BODY_WRAP_COUNT: f.src = w.wrapCount.p; break;
+    case AG2D_BODY_SLEEP_TIMER: f.src = w.sleepTimer.p; break;
+    case AG2D_BODY_STATE: f.src = w.bstate.p; f.kind = EXTRACT_U8_U32; break;
+    case AG2D_BODY_SLEEP_ISLAND: f.src = w.sleepIsland.p; f.kind = EXTRACT_ISLAND; break;
+    case AG2D_BODY_POSE: f.src = w.bpos.p; f.kind = EXTRACT_F4_XYZ; f.outBytes = 12; break;
+    case AG2D_COL_WORLD_X: c4(w.cpose.p, 0); f.perCollider = true; break;
+    case AG2D_COL_WORLD_Y: c4(w.cpose.p, 1); f.perCollider = true; break;
+    case AG2D_COL_WORLD_COS: c4(w.cpose.p, 2); f.perCollider = true; break;
+    case AG2D_COL_WORLD_SIN: c4(w.cpose.p, 3); f.perCollider = true; break;
+    case AG2D_COL_WORLD_ROTATION: f.src = w.cworldRot.p; f.perCollider = true; break;
+    case AG2D_COL_AABB_MIN_X: c4(w.caabb.p, 0); f.perCollider = true; break;
+    case AG2D_COL_AABB_MIN_Y: c4(w.caabb.p, 1); f.perCollider = true; break;
+    case AG2D_COL_AABB_MAX_X: c4(w.caabb.p, 2); f.perCollider = true; break;
+    case AG2D_COL_AABB_MAX_Y: c4(w.caabb.p, 3); f.perCollider = true; break;
+    default: return false;
+    }
+    return true;
+}
+
+// Copies 'bytes' of device memory into host memory on the engine stream and waits for them: one transfer into a
+// page-locked destination, else 8 MiB chunks through the two halves of a page-locked bounce buffer, the transfer
+// of chunk c + 1 overlapping the host copy of chunk c.
+static void copy_to_host(ag2d_world& w, void* dst, const void* src, size_t bytes)
+{
+    const cudaStream_t s = w.stream;
+    if (!bytes) return;
+    if (page_locked(dst)) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return;
+    }
+    constexpr size_t CHUNK = size_t(8) << 20;
+    w.readBounce.reserve(2 * CHUNK);
+    for (auto& e : w.readEv)
+        if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    const size_t chunks = (bytes + CHUNK - 1) / CHUNK;
+    auto issue = [&](size_t c) {
+        const size_t off = c * CHUNK, len = std::min(CHUNK, bytes - off);
+        CK(cudaMemcpyAsync(w.readBounce.p + (c & 1) * CHUNK, static_cast<const uint8_t*>(src) + off, len,
+                           cudaMemcpyDeviceToHost, s));
+        CK(cudaEventRecord(w.readEv[c & 1], s));
+    };
+    issue(0);
+    for (size_t c = 0; c < chunks; c++) {
+        // Chunk c + 1 lands in the half whose contents the host copied out in the previous iteration.
+        if (c + 1 < chunks) issue(c + 1);
+        CK(cudaEventSynchronize(w.readEv[c & 1]));
+        const size_t off = c * CHUNK, len = std::min(CHUNK, bytes - off);
+        std::memcpy(static_cast<uint8_t*>(dst) + off, w.readBounce.p + (c & 1) * CHUNK, len);
+    }
+}
+
+// Elements [lo, lo + n) of a field, packed, into host memory 'dst'; 'bias' is subtracted from sleeping-island ids
+// (the first body of a batch's world). Returns the bytes written.
+static uint64_t read_packed(ag2d_world& w, const FieldSpec& f, uint32_t lo, uint32_t n, uint32_t bias, void* dst)
+{
+    const uint64_t bytes = uint64_t(n) * f.outBytes;
+    if (!bytes) return 0;
+    const void* src = static_cast<const uint8_t*>(f.src) + size_t(lo) * f.outBytes;
+    if (f.kind != EXTRACT_DIRECT) {
+        w.readStage.reserve(bytes);
+        k_extract<<<w.gridFor(n), 256, 0, w.stream>>>(f.src, lo, n, f.kind, f.comp, bias, w.readStage.p);
+        CK(cudaGetLastError());
+        src = w.readStage.p;
+    }
+    copy_to_host(w, dst, src, bytes);
+    return bytes;
+}
+
+// Queues a read of elements [lo, lo + n) into page-locked 'dst': packed on the engine stream into a ring slot (a
+// copy of the values as they are after the work queued so far), then copied on copyStream while later steps run.
+static void read_async(ag2d_world& w, const FieldSpec& f, uint32_t lo, uint32_t n, uint32_t bias, void* dst)
+{
+    const uint64_t bytes = uint64_t(n) * f.outBytes;
+    if (!bytes) return;
+    if (!w.copyStream) CK(cudaStreamCreateWithFlags(&w.copyStream, cudaStreamNonBlocking));
+    ag2d_world::AsyncSlot& a = w.asyncSlot[w.asyncNext++ % ag2d_world::NASYNC];
+    if (!a.packed) {
+        CK(cudaEventCreateWithFlags(&a.packed, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&a.done, cudaEventDisableTiming));
+    }
+    if (a.used) {
+        if (a.buf.n < bytes) CK(cudaEventSynchronize(a.done));   // growing frees the buffer its last copy reads
+        else CK(cudaStreamWaitEvent(w.stream, a.done, 0));       // the next pack waits for that copy on the device
+    }
+    a.buf.reserve(bytes);
+    if (f.kind == EXTRACT_DIRECT) {
+        CK(cudaMemcpyAsync(a.buf.p, static_cast<const uint8_t*>(f.src) + size_t(lo) * f.outBytes, bytes,
+                           cudaMemcpyDeviceToDevice, w.stream));
+    } else {
+        k_extract<<<w.gridFor(n), 256, 0, w.stream>>>(f.src, lo, n, f.kind, f.comp, bias, a.buf.p);
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(a.packed, w.stream));
+    CK(cudaStreamWaitEvent(w.copyStream, a.packed, 0));
+    CK(cudaMemcpyAsync(dst, a.buf.p, bytes, cudaMemcpyDeviceToHost, w.copyStream));
+    CK(cudaEventRecord(a.done, w.copyStream));
+    a.used = true;
+}
+
 template <class T>
 static std::vector<T> download(const T* p, size_t n, cudaStream_t s)
 {
@@ -2106,7 +2408,9 @@ static std::vector<T> download(const T* p, size_t n, cudaStream_t s)
     return v;
 }
 
-static std::vector<uint8_t> read_field(ag2d_world& w, int32_t field)
+// The phase-tap fields (Morton order, pairs, manifolds, solve order, colour starts): element count from the device
+// counters where the count lives there. With sizeOnly the bytes are counted but not read.
+static std::vector<uint8_t> read_field(ag2d_world& w, int32_t field, bool sizeOnly, uint64_t* bytesOut)
 {
     const cudaStream_t s = w.stream;
     auto pack = [](const auto& v) {
@@ -2114,82 +2418,26 @@ static std::vector<uint8_t> read_field(ag2d_world& w, int32_t field)
         if (!v.empty()) std::memcpy(out.data(), v.data(), out.size());
         return out;
     };
-    auto comp4 = [&](const DBuf<float4>& b, uint32_t n, int c) {
-        const auto v = download(b.p, n, s);
-        std::vector<float> o(n);
-        for (uint32_t i = 0; i < n; i++) o[i] = c == 0 ? v[i].x : c == 1 ? v[i].y : c == 2 ? v[i].z : v[i].w;
-        return pack(o);
+    auto devCount = [&](const uint32_t* p) {
+        uint32_t n = 0;
+        CK(cudaMemcpyAsync(&n, p, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return n;
     };
-    auto comp2 = [&](const DBuf<float2>& b, uint32_t n, int c) {
-        const auto v = download(b.p, n, s);
-        std::vector<float> o(n);
-        for (uint32_t i = 0; i < n; i++) o[i] = c == 0 ? v[i].x : v[i].y;
-        return pack(o);
+    auto get = [&](const auto* p, size_t n) {
+        *bytesOut = n * sizeof(*p);
+        using T = std::remove_const_t<std::remove_pointer_t<decltype(p)>>;
+        return sizeOnly ? std::vector<uint8_t>() : pack(download(static_cast<const T*>(p), n, s));
     };
-    const uint32_t nb = w.nBodies, nc = w.nColliders;
     switch (field) {
-    case AG2D_BODY_COM_X: return comp4(w.bpos, nb, 0);
-    case AG2D_BODY_COM_Y: return comp4(w.bpos, nb, 1);
-    case AG2D_BODY_ROTATION: return comp4(w.bpos, nb, 2);
-    case AG2D_BODY_VEL_X: return comp4(w.bvel, nb, 0);
-    case AG2D_BODY_VEL_Y: return comp4(w.bvel, nb, 1);
-    case AG2D_BODY_ANGULAR_VELOCITY: return comp4(w.bvel, nb, 2);
-    case AG2D_BODY_ROT_COS: return comp2(w.brot, nb, 0);
-    case AG2D_BODY_ROT_SIN: return comp2(w.brot, nb, 1);
-    case AG2D_BODY_WRAP_COUNT: return pack(download(w.wrapCount.p, nb, s));
-    case AG2D_BODY_SLEEP_TIMER: return pack(download(w.sleepTimer.p, nb, s));
-    case AG2D_BODY_STATE: {
-        const auto v = download(w.bstate.p, nb, s);
-        std::vector<uint32_t> o(v.begin(), v.end());
-        return pack(o);
-    }
-    case AG2D_BODY_SLEEP_ISLAND: return pack(download(w.sleepIsland.p, nb, s));
-    case AG2D_BODY_INV_MASS: return comp4(w.bvel, nb, 3);
-    case AG2D_BODY_INV_INERTIA: return comp4(w.bpos, nb, 3);
-    case AG2D_BODY_POSE: {
-        const auto v = download(w.bpos.p, nb, s);
-        std::vector<float> o(size_t(nb) * 3);
-        for (uint32_t i = 0; i < nb; i++) { o[3 * i] = v[i].x; o[3 * i + 1] = v[i].y; o[3 * i + 2] = v[i].z; }
-        return pack(o);
-    }
-    case AG2D_COL_WORLD_X: return comp4(w.cpose, nc, 0);
-    case AG2D_COL_WORLD_Y: return comp4(w.cpose, nc, 1);
-    case AG2D_COL_WORLD_COS: return comp4(w.cpose, nc, 2);
-    case AG2D_COL_WORLD_SIN: return comp4(w.cpose, nc, 3);
-    case AG2D_COL_WORLD_ROTATION: return pack(download(w.cworldRot.p, nc, s));
-    case AG2D_COL_AABB_MIN_X: return comp4(w.caabb, nc, 0);
-    case AG2D_COL_AABB_MIN_Y: return comp4(w.caabb, nc, 1);
-    case AG2D_COL_AABB_MAX_X: return comp4(w.caabb, nc, 2);
-    case AG2D_COL_AABB_MAX_Y: return comp4(w.caabb, nc, 3);
-    case AG2D_DYN_SORTED: return pack(download(w.dynTree.vals.p, uint32_t(w.dynTree.n), s));
+    case AG2D_DYN_SORTED: return get(w.dynTree.vals.p, uint32_t(w.dynTree.n));
     case AG2D_DYN_MORTON:
-        return pack(download(w.nWorlds > 1 ? w.dynTree.sortedKey.p : w.dynTree.keys.p, uint32_t(w.dynTree.n), s));
-    case AG2D_PAIRS: {
-        uint32_t n = 0;
-        CK(cudaMemcpyAsync(&n, &w.dCounters.p->pairs, 4, cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        return pack(download(w.pairs.p, std::min(n, w.pairCap), s));
-    }
-    case AG2D_MANIFOLDS:
-    case AG2D_PREV_MANIFOLDS: {
-        const bool prev = field == AG2D_PREV_MANIFOLDS;
-        uint32_t n = 0;
-        CK(cudaMemcpyAsync(&n, prev ? w.nPrev.p : w.nManifolds.p, 4, cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        return pack(download(prev ? w.prevManifolds.p : w.manifolds.p, n, s));
-    }
-    case AG2D_SOLVE_ORDER: {
-        uint32_t n = 0;
-        CK(cudaMemcpyAsync(&n, w.nManifolds.p, 4, cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        return pack(download(w.order.p, n, s));
-    }
-    case AG2D_COLOR_STARTS: {
-        StepCounters c;
-        CK(cudaMemcpyAsync(&c, w.dCounters.p, sizeof(c), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        return pack(download(w.colorStart.p, c.colors + 1, s));
-    }
+        return get(w.nWorlds > 1 ? w.dynTree.sortedKey.p : w.dynTree.keys.p, uint32_t(w.dynTree.n));
+    case AG2D_PAIRS: return get(w.pairs.p, std::min(devCount(&w.dCounters.p->pairs), w.pairCap));
+    case AG2D_MANIFOLDS: return get(w.manifolds.p, devCount(w.nManifolds.p));
+    case AG2D_PREV_MANIFOLDS: return get(w.prevManifolds.p, devCount(w.nPrev.p));
+    case AG2D_SOLVE_ORDER: return get(w.order.p, devCount(w.nManifolds.p));
+    case AG2D_COLOR_STARTS: return get(w.colorStart.p, devCount(&w.dCounters.p->colors) + 1);
     default: throw ApiError(AG2D_ERR_INVALID_ARG, "unknown field " + std::to_string(field));
     }
 }
@@ -2284,12 +2532,77 @@ int32_t ag2d_world_read(ag2d_world* world, int32_t field, void* dst, uint64_t ca
         if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
         CK(cudaSetDevice(world->settings.device));
         world->ensureUploaded();
-        const auto bytes = read_field(*world, field);
-        if (out_bytes) *out_bytes = bytes.size();
+        FieldSpec f;
+        if (field_spec(*world, field, f)) {
+            // Body and collider fields: the size needs no device access; the values are packed on the device.
+            const uint32_t n = f.perCollider ? world->nColliders : world->nBodies;
+            const uint64_t bytes = uint64_t(n) * f.outBytes;
+            if (out_bytes) *out_bytes = bytes;
+            if (dst) {
+                if (cap < bytes) throw ApiError(AG2D_ERR_INVALID_ARG, "destination too small");
+                read_packed(*world, f, 0, n, 0, dst);
+            }
+            return;
+        }
+        uint64_t size = 0;
+        const auto bytes = read_field(*world, field, dst == nullptr, &size);
+        if (out_bytes) *out_bytes = size;
         if (dst) {
             if (cap < bytes.size()) throw ApiError(AG2D_ERR_INVALID_ARG, "destination too small");
             if (!bytes.empty()) std::memcpy(dst, bytes.data(), bytes.size());
         }
+    });
+}
+
+int32_t ag2d_world_read_async(ag2d_world* world, int32_t field, void* dst, uint64_t cap, uint64_t* out_bytes)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        CK(cudaSetDevice(world->settings.device));
+        world->ensureUploaded();
+        FieldSpec f;
+        if (!field_spec(*world, field, f))
+            throw ApiError(AG2D_ERR_UNSUPPORTED, "asynchronous reads take body and collider fields");
+        const uint32_t n = f.perCollider ? world->nColliders : world->nBodies;
+        const uint64_t bytes = uint64_t(n) * f.outBytes;
+        if (out_bytes) *out_bytes = bytes;
+        if (!dst || cap < bytes) throw ApiError(AG2D_ERR_INVALID_ARG, "destination missing or too small");
+        if (!page_locked(dst))
+            throw ApiError(AG2D_ERR_INVALID_ARG, "asynchronous reads need a page-locked destination (ag2d_host_alloc)");
+        read_async(*world, f, 0, n, 0, dst);
+    });
+}
+
+int32_t ag2d_world_read_wait(ag2d_world* world)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        if (!world->copyStream) return;
+        CK(cudaSetDevice(world->settings.device));
+        CK(cudaStreamSynchronize(world->copyStream));
+    });
+}
+
+int32_t ag2d_host_alloc(uint64_t bytes, void** out_ptr)
+{
+    return guarded([&] {
+        if (!out_ptr) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        *out_ptr = nullptr;
+        if (bytes == 0) throw ApiError(AG2D_ERR_INVALID_ARG, "zero bytes");
+        const cudaError_t e = cudaHostAlloc(out_ptr, bytes, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            *out_ptr = nullptr;
+            throw ApiError(e == cudaErrorMemoryAllocation ? AG2D_ERR_OOM : AG2D_ERR_CUDA,
+                           std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+        }
+    });
+}
+
+int32_t ag2d_host_free(void* ptr)
+{
+    return guarded([&] {
+        if (ptr) CK(cudaFreeHost(ptr));
     });
 }
 
@@ -2493,23 +2806,22 @@ int32_t ag2d_batch_read(ag2d_batch* batch, uint32_t world, int32_t field, void* 
         CK(cudaSetDevice(e.settings.device));
         const uint32_t b0 = e.hBodyStart[world], b1 = e.hBodyStart[world + 1];
         const uint32_t c0 = e.hColStart[world], c1 = e.hColStart[world + 1];
-        const std::vector<uint8_t> all = read_field(e, field);
+        FieldSpec f;
+        if (field_spec(e, field, f)) {
+            // The world's range only, packed on the device; sleeping-island ids become world-local.
+            const uint32_t lo = f.perCollider ? c0 : b0, hi = f.perCollider ? c1 : b1;
+            const uint64_t bytes = uint64_t(hi - lo) * f.outBytes;
+            if (out_bytes) *out_bytes = bytes;
+            if (dst) {
+                if (cap < bytes) throw ApiError(AG2D_ERR_INVALID_ARG, "destination too small");
+                read_packed(e, f, lo, hi - lo, b0, dst);
+            }
+            return;
+        }
         std::vector<uint8_t> out;
-        auto slice = [&](size_t elemBytes, uint32_t lo, uint32_t hi) {
-            out.assign(all.begin() + size_t(lo) * elemBytes, all.begin() + size_t(hi) * elemBytes);
-        };
-        if (field == AG2D_BODY_POSE) {
-            slice(12, b0, b1);
-        } else if (field == AG2D_BODY_SLEEP_ISLAND) {
-            slice(4, b0, b1);
-            uint32_t* v = reinterpret_cast<uint32_t*>(out.data());
-            for (uint32_t i = 0; i < b1 - b0; i++) if (v[i] != 0xFFFFFFFFu) v[i] -= b0;
-        } else if ((field >= AG2D_BODY_COM_X && field < AG2D_BODY_POSE) || field == AG2D_BODY_INV_MASS ||
-                   field == AG2D_BODY_INV_INERTIA) {
-            slice(4, b0, b1);
-        } else if (field >= AG2D_COL_WORLD_X && field < AG2D_DYN_SORTED) {
-            slice(4, c0, c1);
-        } else if (field == AG2D_MANIFOLDS || field == AG2D_PREV_MANIFOLDS) {
+        if (field == AG2D_MANIFOLDS || field == AG2D_PREV_MANIFOLDS) {
+            uint64_t size = 0;
+            const std::vector<uint8_t> all = read_field(e, field, false, &size);
             const Manifold* m = reinterpret_cast<const Manifold*>(all.data());
             const size_t n = all.size() / sizeof(Manifold);
             std::vector<Manifold> mine;
@@ -2538,6 +2850,50 @@ int32_t ag2d_batch_destroy(ag2d_batch* batch)
     return guarded([&] {
         if (batch && batch->engine) cudaSetDevice(batch->engine->settings.device);
         delete batch;
+    });
+}
+
+int32_t ag2d_batch_save(ag2d_batch* batch, void* dst, uint64_t cap, uint64_t* out_bytes)
+{
+    return guarded([&] {
+        if (!batch) throw ApiError(AG2D_ERR_INVALID_ARG, "null batch");
+        ag2d_world& e = *batch->engine;
+        CK(cudaSetDevice(e.settings.device));
+        const CkptHeader h = e.checkpointLayout();
+        if (out_bytes) *out_bytes = h.totalBytes;
+        if (!dst) return;
+        if (cap < h.totalBytes) throw ApiError(AG2D_ERR_INVALID_ARG, "destination too small");
+        e.saveCheckpoint(h, static_cast<uint8_t*>(dst));
+    });
+}
+
+int32_t ag2d_batch_restore(const void* src, uint64_t bytes, int32_t device, ag2d_batch** out)
+{
+    return guarded([&] {
+        if (!src || !out) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        CkptHeader h;
+        if (bytes < sizeof(h)) throw ApiError(AG2D_ERR_INVALID_ARG, "not a checkpoint (too short)");
+        std::memcpy(&h, src, sizeof(h));
+        if (std::memcmp(h.magic, CKPT_MAGIC, sizeof(h.magic)) != 0 || h.version != CKPT_VERSION ||
+            h.headerBytes != sizeof(CkptHeader))
+            throw ApiError(AG2D_ERR_INVALID_ARG, "not a checkpoint of this library version");
+        if (h.totalBytes > bytes) throw ApiError(AG2D_ERR_INVALID_ARG, "checkpoint truncated");
+        for (uint32_t k = 0; k < NCK; k++)
+            if (h.off[k] > h.totalBytes || h.len[k] > h.totalBytes - h.off[k])
+                throw ApiError(AG2D_ERR_INVALID_ARG, "checkpoint section out of range");
+        if (h.len[CK_WBODY] != (uint64_t(std::max<uint32_t>(h.nWorlds, 1)) + 1) * 4 ||
+            h.len[CK_WCOL] != h.len[CK_WBODY] || h.len[CK_VEL] != uint64_t(h.nBodies) * 16 ||
+            h.len[CK_CBODY] != uint64_t(h.nColliders) * 4)
+            throw ApiError(AG2D_ERR_INVALID_ARG, "checkpoint sizes inconsistent");
+        ag2d_world_settings st = h.settings;
+        if (device >= 0) st.device = device;
+        std::unique_ptr<ag2d_batch> b(new ag2d_batch());
+        b->worlds = std::max<uint32_t>(h.nWorlds, 1);
+        b->engine.reset(new ag2d_world());
+        b->engine->init(st);
+        CK(cudaSetDevice(st.device));
+        b->engine->restoreCheckpoint(h, static_cast<const uint8_t*>(src));
+        *out = b.release();
     });
 }
 

@@ -112,4 +112,40 @@ __global__ void k_fill_u32(uint32_t* __restrict__ out, uint32_t n, uint32_t valu
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) out[e] = value;
 }
 
+// Packs elements [lo, lo + n) of one field into the dense layout a host read returns, so that the transfer carries
+// only the bytes the caller asked for (a float4 record's component is 4 of its 16 bytes).
+__global__ void k_extract(const void* __restrict__ src, uint32_t lo, uint32_t n, uint32_t kind, uint32_t comp,
+                          uint32_t bias, void* __restrict__ out)
+{
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const uint32_t i = lo + e;
+        switch (kind) {
+        case EXTRACT_F4_COMP:
+            static_cast<float*>(out)[e] = static_cast<const float*>(src)[4 * size_t(i) + comp];
+            break;
+        case EXTRACT_F4_XYZ: {
+            const float4 v = static_cast<const float4*>(src)[i];
+            float* o = static_cast<float*>(out) + 3 * size_t(e);
+            o[0] = v.x;
+            o[1] = v.y;
+            o[2] = v.z;
+            break;
+        }
+        case EXTRACT_F2_COMP:
+            static_cast<float*>(out)[e] = static_cast<const float*>(src)[2 * size_t(i) + comp];
+            break;
+        case EXTRACT_U8_U32:
+            static_cast<uint32_t*>(out)[e] = static_cast<const uint8_t*>(src)[i];
+            break;
+        case EXTRACT_ISLAND: {
+            const uint32_t v = static_cast<const uint32_t*>(src)[i];
+            static_cast<uint32_t*>(out)[e] = v == 0xFFFFFFFFu ? v : v - bias;
+            break;
+        }
+        default:
+            break;
+        }
+    }
+}
+
 }  // namespace ag2d
