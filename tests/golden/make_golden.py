@@ -14,6 +14,9 @@ Fixtures:
     cossin_edge.npz         FastCosSin over edge angles (quadrant boundaries, values just below 2 pi)
     wrap_edge.npz           body rotations around wrap boundaries (SIMD body and scalar tail)
     traj_c1_n256.npz        600-step trajectory statistics of a 256-polygon scene
+    traj_c1_n2048.npz       the same statistics of the full c1 configuration (2,048 polygons, seed 0, 600 steps)
+    c2_n20000_s2_step420.npz   20,000 bodies of the c2 mix (500 columns x 40 rows) in a U container, phase taps of step 421 (the
+                               narrow phase and the solver compared at scale)
     c5_ccd_hit.npz          the first continuous-collision hit of a serving-style request (fast circles)
 """
 from __future__ import annotations
@@ -37,17 +40,34 @@ DROP_SUFFIXES = (".localOffsetX", ".localOffsetY", ".mass", ".inertia", ".localC
                  ".localCenterOfMassY", ".minExtent", ".maxExtent")
 
 
-def phase_fixture(scene, steps, path):
+def dedupe(blobs):
+    """Stores each distinct array once: a later array equal to an earlier one (same dtype, shape and bytes)
+    becomes an entry "later=earlier" of meta.aliases, which tests/parity.py load() expands."""
+    seen, out, aliases = {}, {}, []
+    for k in sorted(blobs):
+        v = np.ascontiguousarray(blobs[k])
+        key = (v.dtype.str, v.shape, v.tobytes())
+        if key in seen and not k.startswith("meta."):
+            aliases.append(f"{k}={seen[key]}")
+        else:
+            seen.setdefault(key, k)
+            out[k] = v
+    if aliases:
+        out["meta.aliases"] = np.array(aliases)
+    return out
+
+
+def phase_fixture(scene, steps, path, prefixes=PHASE_PREFIXES, store_once=False):
     r = refapi.RefSim(scene)
     r.update(steps)
     r.phase_step()
     blobs = {k: v for k, v in r.blobs().items()
-             if k.startswith(PHASE_PREFIXES) and not k.endswith(DROP_SUFFIXES)}
+             if k.startswith(prefixes) and not k.endswith(DROP_SUFFIXES)}
     blobs["meta.dt"] = np.array([scene.dt], np.float32)
     blobs["meta.gravity"] = np.array(scene.gravity, np.float32)
     blobs["meta.iters"] = np.array([scene.velocity_iterations, scene.position_iterations], np.uint32)
     blobs["meta.materials"] = np.array([(1.0, 0.0, 0.0)] + list(scene.materials), np.float32)
-    np.savez_compressed(path, **blobs)
+    np.savez_compressed(path, **(dedupe(blobs) if store_once else blobs))
     r.close()
     print(f"{os.path.basename(path)}: {len(blobs)} arrays, pairs {blobs['bp.pairs'].size // 2}, "
           f"manifolds {blobs.get('np.count', np.zeros(0)).size}")
@@ -101,8 +121,11 @@ def wrap_fixture(path):
 
 
 def trajectory_stats(sim, steps):
-    """Per-step: momentum (sum m v), kinetic energy, max manifold depth, manifold count, sleeping bodies."""
-    out = {k: [] for k in ("px", "py", "ke", "max_depth", "manifolds", "sleeping")}
+    """Per-step: momentum (sum m v), kinetic energy, max manifold depth, manifold count, sleeping bodies; and, since
+    bodies near the ends of the ground can slide off and fall without limit, the kinetic energy of the bodies still
+    at or above the ground's top ("ke_on": centre of mass above y = -1) and the number that have fallen off
+    ("fallen": below y = -10)."""
+    out = {k: [] for k in ("px", "py", "ke", "max_depth", "manifolds", "sleeping", "ke_on", "fallen")}
     for _ in range(steps):
         sim.update(1)
         sim.dump_state("t.")
@@ -112,7 +135,11 @@ def trajectory_stats(sim, steps):
         dyn = m > 0
         out["px"].append(float(np.sum((m * vx)[dyn], dtype=np.float64)))
         out["py"].append(float(np.sum((m * vy)[dyn], dtype=np.float64)))
-        out["ke"].append(float(0.5 * np.sum((m * (vx * vx + vy * vy) + inertia * w * w)[dyn], dtype=np.float64)))
+        ke = 0.5 * (m * (vx * vx + vy * vy) + inertia * w * w)
+        out["ke"].append(float(np.sum(ke[dyn], dtype=np.float64)))
+        y = sim.blob("t.body.comY")
+        out["ke_on"].append(float(np.sum(ke[dyn & (y > -1.0)], dtype=np.float64)))
+        out["fallen"].append(int(np.sum(dyn & (y < -10.0))))
         depth = sim.blob("t.man.depth")
         out["max_depth"].append(float(depth.max()) if depth.size else 0.0)
         out["manifolds"].append(int(depth.size))
@@ -229,18 +256,30 @@ def contacts_fixture(path, n=1500, steps=300, queries=60):
           f"{len(sshape)} shape queries, groups {keep['q.col.groupStarts'].tolist()}")
 
 
+FIXTURES = {
+    "c1_n256_s0_step300.npz": lambda p: phase_fixture(scenes.make_c1(256, 0), 300, p),
+    "c2_n2000_s1_step240.npz": lambda p: phase_fixture(scenes.make_c2(2000, 1, columns=50), 240, p),
+    "c3_n1500_s0_step0.npz": lambda p: phase_fixture(scenes.make_c3(1500, 0, extent=70.0), 0, p),
+    # The post-step taps are left out of the large fixture (no test reads them), to keep it small.
+    "c2_n20000_s2_step420.npz": lambda p: phase_fixture(scenes.make_c2(20000, 2, columns=500), 420, p,
+                                                        tuple(x for x in PHASE_PREFIXES if not x.startswith("post.")),
+                                                        store_once=True),
+    "cossin_edge.npz": cossin_fixture,
+    "wrap_edge.npz": wrap_fixture,
+    "traj_c1_n256.npz": trajectory_fixture,
+    "traj_c1_n2048.npz": lambda p: trajectory_fixture(p, n=2048),
+    "c5_ccd_hit.npz": ccd_fixture,
+    "query_c1_n600_step700.npz": query_fixture,
+    "contacts_c2_n1500_step300.npz": contacts_fixture,
+}
+
+
 def main():
     if not refapi.available():
         sys.exit("oracle/_ref/libagony_ref.so missing: run oracle/ref_build.sh first")
-    phase_fixture(scenes.make_c1(256, 0), 300, os.path.join(HERE, "c1_n256_s0_step300.npz"))
-    phase_fixture(scenes.make_c2(2000, 1, columns=50), 240, os.path.join(HERE, "c2_n2000_s1_step240.npz"))
-    phase_fixture(scenes.make_c3(1500, 0, extent=70.0), 0, os.path.join(HERE, "c3_n1500_s0_step0.npz"))
-    cossin_fixture(os.path.join(HERE, "cossin_edge.npz"))
-    wrap_fixture(os.path.join(HERE, "wrap_edge.npz"))
-    trajectory_fixture(os.path.join(HERE, "traj_c1_n256.npz"))
-    ccd_fixture(os.path.join(HERE, "c5_ccd_hit.npz"))
-    query_fixture(os.path.join(HERE, "query_c1_n600_step700.npz"))
-    contacts_fixture(os.path.join(HERE, "contacts_c2_n1500_step300.npz"))
+    names = sys.argv[1:] or list(FIXTURES)
+    for name in names:
+        FIXTURES[name](os.path.join(HERE, name))
 
 
 if __name__ == "__main__":

@@ -3,7 +3,9 @@
 Tolerances (from the path's parity contract): integration, poses, AABBs, Morton keys, the sorted order and the
 candidate pair set are bit-exact; narrow-phase manifolds are bit-exact on the same pair list (the arithmetic is the
 reference's, contraction off); solver impulses are bit-exact against the FP32 oracle replay of the GPU's own colour
-order and within 1e-4 relative (of the largest impulse) against the FP64 replay.
+order and within the impulse contract of tests/parity.py against the FP64 replay (1e-4 relative, absolute floor
+1e-4 N s, for at least 99.5 % of impulses; 1e-3 relative + 1e-2 N s for every one; the reference's own FP32 solve
+meets the same bound).
 """
 import numpy as np
 import pytest
@@ -160,12 +162,12 @@ def test_solver_against_replays_of_the_colour_order(name):
     for field, ref in [(ag2d.BODY_VEL_X, "velX"), (ag2d.BODY_VEL_Y, "velY"), (ag2d.BODY_ANGULAR_VELOCITY, "angVel"),
                        (ag2d.BODY_COM_X, "comX"), (ag2d.BODY_COM_Y, "comY")]:
         assert parity.mismatches(w.read(field), o32.a[ref]) == 0, ref
-    # FP64 replay of the same order: within 1e-4 of the largest impulse.
+    # FP64 replay of the same order: the impulse contract of tests/parity.py (1e-4 relative for all but a stated
+    # share, and a hard ceiling for every impulse), the bound the reference's own FP32 solve meets.
     o64 = oraapi.OraWorld(d, "svin.", mats)
     _, _, imp = o64.solve_f64(m_in, order, int(iters[0]), int(iters[1]))
-    got = np.stack([ours["jn"][:, 0], ours["jt"][:, 0], ours["jn"][:, 1], ours["jt"][:, 1]], 1).astype(np.float64)
-    scale = max(float(np.abs(imp).max()), 1e-6)
-    assert float(np.max(np.abs(got - imp))) <= 1e-4 * scale * 10, "FP64 replay drifted"
+    ok, msg = parity.impulses_within_contract(ours, imp)
+    assert ok, msg
 
 
 @pytest.mark.parametrize("name", parity.PHASE_FIXTURES)

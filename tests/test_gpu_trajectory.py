@@ -1,16 +1,20 @@
-"""600-step trajectory of a 256-polygon drop (c1 mix, seed 0) against the reference engine's own trajectory.
+"""600-step trajectories of polygon drops (c1 mix, seed 0) against the reference engine's own trajectories: 256
+polygons, and the full c1 configuration (2,048 polygons on the 220 m ground box).
 
 The solver's colouring changes the Gauss-Seidel order, so the two runs are not bit-identical and a falling pile
 diverges chaotically in its details. The comparison is on the statistics the parity contract names, each with its
 tolerance written here:
-  - free fall (steps 0-39, before the bodies reach the ground): vertical momentum within 1e-4 relative, kinetic
-    energy within 1e-3 relative (initial overlaps are resolved in another order, nothing else differs);
-  - energy drift: the kinetic-energy peak of the fall within 5 % and reached within 10 steps of the reference's;
-  - momentum: total vertical momentum at its extreme within 5 %; horizontal momentum stays below 3 % of it;
+  - free fall (the steps where the reference's vertical momentum is still exactly -M g dt (k + 1), within 1e-5
+    relative: no body has met the ground yet): vertical momentum within 1e-4 relative, kinetic energy within 1e-3
+    relative (initial overlaps between bodies are resolved in another order, nothing else differs);
+  - energy drift: the kinetic-energy peak of the bodies over the ground within 5 % and reached within 10 steps of
+    the reference's;
+  - momentum: horizontal momentum stays below 3 % of the vertical extreme; the number of bodies that slid off the
+    ends of the ground (and fall without limit, which dominates the total momentum and energy) within 15 % (+3);
   - penetration: the deepest contact after the first 20 steps no more than 1.5 x the reference's deepest (+1 cm);
-  - the settled pile: contact count over the last 100 steps within 20 % of the reference's.
-The reference trajectory (tests/golden/traj_c1_n256.npz) is the compiled reference engine run by
-tests/golden/make_golden.py.
+  - the pile: contact count over the last 100 steps within 20 % of the reference's.
+The reference trajectories (tests/golden/traj_c1_n256.npz, traj_c1_n2048.npz) are the compiled reference engine run
+by tests/golden/make_golden.py.
 """
 import json
 import os
@@ -25,12 +29,15 @@ pytestmark = pytest.mark.gpu
 ag2d = pytest.importorskip("ag2d")
 from ag2d import scenes  # noqa: E402
 
+CASES = {256: "traj_c1_n256.npz", 2048: "traj_c1_n2048.npz"}
+KEYS = ("px", "py", "ke", "max_depth", "manifolds", "sleeping", "ke_on", "fallen")
 
-def _trajectory(steps=600):
-    sc = scenes.make_c1(256, 0)
+
+def _trajectory(n, steps=600):
+    sc = scenes.make_c1(n, 0)
     w = ag2d.World.from_scene(sc)
     w.step(0)
-    out = {k: [] for k in ("px", "py", "ke", "max_depth", "manifolds", "sleeping")}
+    out = {k: [] for k in KEYS}
     inv_m = inv_i = None
     for _ in range(steps):
         w.step(1)
@@ -43,45 +50,60 @@ def _trajectory(steps=600):
         vx = w.read(ag2d.BODY_VEL_X).astype(np.float64)
         vy = w.read(ag2d.BODY_VEL_Y).astype(np.float64)
         om = w.read(ag2d.BODY_ANGULAR_VELOCITY).astype(np.float64)
+        y = w.read(ag2d.BODY_COM_Y).astype(np.float64)
+        ke = 0.5 * (m * (vx * vx + vy * vy) + inertia * om * om)
         out["px"].append(float(np.sum((m * vx)[dyn])))
         out["py"].append(float(np.sum((m * vy)[dyn])))
-        out["ke"].append(float(0.5 * np.sum((m * (vx * vx + vy * vy) + inertia * om * om)[dyn])))
+        out["ke"].append(float(np.sum(ke[dyn])))
+        out["ke_on"].append(float(np.sum(ke[dyn & (y > -1.0)])))
+        out["fallen"].append(int(np.sum(dyn & (y < -10.0))))
         man = w.read(ag2d.PREV_MANIFOLDS)
         out["max_depth"].append(float(man["depth"].max()) if man.size else 0.0)
         out["manifolds"].append(int(man.size))
         out["sleeping"].append(int(np.sum(w.read(ag2d.BODY_STATE) == 1)))
-    return {k: np.asarray(v) for k, v in out.items()}
+    out = {k: np.asarray(v) for k, v in out.items()}
+    out["total_mass"] = float(np.sum(m[dyn]))
+    out["g_dt"] = float(-sc.gravity[1] * sc.dt)
+    return out
 
 
-@pytest.fixture(scope="module")
-def runs():
-    ref = parity.load("traj_c1_n256.npz")
-    gpu = _trajectory()
+@pytest.fixture(scope="module", params=sorted(CASES))
+def runs(request):
+    n = request.param
+    ref = parity.load(CASES[n])
+    gpu = _trajectory(n)
     out_dir = os.environ.get("AG2D_TRAJ_OUT")
     if out_dir:
-        with open(os.path.join(out_dir, "traj_c1_n256_gpu.json"), "w") as f:
-            json.dump({k: v.tolist() for k, v in gpu.items()}, f)
-    return {k: np.asarray(ref[k], np.float64) for k in gpu}, gpu
+        with open(os.path.join(out_dir, f"traj_c1_n{n}_gpu.json"), "w") as f:
+            json.dump({k: (v.tolist() if isinstance(v, np.ndarray) else v) for k, v in gpu.items()}, f)
+    return {k: np.asarray(ref[k], np.float64) for k in KEYS}, gpu
+
+
+def _free_fall_steps(ref, gpu):
+    ideal = -gpu["total_mass"] * gpu["g_dt"] * np.arange(1, ref["py"].size + 1)
+    exact = np.abs(ref["py"] - ideal) <= 1e-5 * np.abs(ideal)
+    return int(np.argmin(exact)) if not exact.all() else exact.size
 
 
 def test_free_fall_matches(runs):
     ref, gpu = runs
-    sl = slice(0, 40)
-    np.testing.assert_allclose(gpu["py"][sl], ref["py"][sl], rtol=1e-4)
-    np.testing.assert_allclose(gpu["ke"][sl], ref["ke"][sl], rtol=1e-3)
+    k = _free_fall_steps(ref, gpu)
+    # 33 steps for 256 polygons; 4 for 2,048, whose 1,808 initial overlaps push bodies onto the ground at once.
+    assert k >= 3, "the reference left free fall within 3 steps"
+    np.testing.assert_allclose(gpu["py"][:k], ref["py"][:k], rtol=1e-4)
+    np.testing.assert_allclose(gpu["ke"][:k], ref["ke"][:k], rtol=1e-3)
 
 
 def test_energy_peak(runs):
     ref, gpu = runs
-    assert abs(gpu["ke"].max() - ref["ke"].max()) <= 0.05 * ref["ke"].max()
-    assert abs(int(np.argmax(gpu["ke"])) - int(np.argmax(ref["ke"]))) <= 10
+    assert abs(gpu["ke_on"].max() - ref["ke_on"].max()) <= 0.05 * ref["ke_on"].max()
+    assert abs(int(np.argmax(gpu["ke_on"])) - int(np.argmax(ref["ke_on"]))) <= 10
 
 
 def test_momentum(runs):
     ref, gpu = runs
-    peak_ref, peak_gpu = ref["py"].min(), gpu["py"].min()
-    assert abs(peak_gpu - peak_ref) <= 0.05 * abs(peak_ref)
-    assert np.abs(gpu["px"]).max() <= 0.03 * abs(peak_gpu)
+    assert np.abs(gpu["px"]).max() <= 0.03 * np.abs(gpu["py"]).max()
+    assert abs(gpu["fallen"][-1] - ref["fallen"][-1]) <= 0.15 * ref["fallen"][-1] + 3
 
 
 def test_penetration(runs):
