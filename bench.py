@@ -17,8 +17,9 @@ Workloads (seeded synthetic scenes, ag2d.scenes):
                 --requests arrivals, reporting aggregate body-steps/s and p50 / p99 completion latency.
 
 One process per GPU (torchrun for N > 1). Worlds exchange nothing on the step path, so each rank advances its own
-batch (rank r's worlds are seeded r * worlds + k): weak scaling with no collective in the step; the whole-job value
-is the sum of all ranks' body-steps over the slowest rank's device time.
+batch: the job's N x 4,096 worlds (seeds 0 ..) are shared out by greedy body-count balancing (largest first, to the
+least-loaded rank): weak scaling with no collective in the step; the whole-job value is the sum of all ranks'
+body-steps over the slowest rank's device time.
 
 Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events on the engine's stream, with a 256 MiB
 write between steps outside the events (L2 flushed); barrier + synchronize around the timed region; the max over
@@ -120,9 +121,19 @@ def host_threads():
 # ---------------------------------------------------------------------------------------------------------------
 # Scenes
 # ---------------------------------------------------------------------------------------------------------------
-def c4_scenes(worlds, seed):
+def c4_shard(worlds_per_rank, rank, world_size):
+    """This rank's worlds of the whole job (worlds_per_rank x world_size worlds, seed 0), balanced by body count
+    over the ranks (weak scaling: the per-rank load stays at one batch's worth)."""
     from ag2d import scenes
-    return scenes.make_c4_worlds(worlds=worlds, seed=seed, processes=max(1, min(32, host_threads())))
+    counts = scenes.c4_counts(worlds_per_rank * world_size, 0)
+    return scenes.shard_by_bodies(counts, world_size)[rank]
+
+
+def c4_scenes(worlds, seed=0, rank=0, world_size=1):
+    from ag2d import scenes
+    subset = None if world_size == 1 else c4_shard(worlds, rank, world_size)
+    return scenes.make_c4_worlds(worlds=worlds * world_size, seed=seed, processes=max(1, min(32, host_threads())),
+                                 subset=subset)
 
 
 def c5_requests(count, seed):
@@ -576,7 +587,7 @@ def run_reference(args):
 # ---------------------------------------------------------------------------------------------------------------
 def run_c4(args, torch, dist, rank, world_size, local, dev):
     import ag2d
-    scene_list = c4_scenes(args.worlds, rank_seed(rank, args.worlds))
+    scene_list = c4_scenes(args.worlds, 0, rank, world_size)
     n_bodies = int(sum(s.n for s in scene_list))
     settings = dict(dt=scene_list[0].dt, velocity_iterations=8, position_iterations=3, gravity=scene_list[0].gravity,
                     device=local)

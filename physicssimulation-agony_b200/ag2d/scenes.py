@@ -183,13 +183,36 @@ def _c4_world(args):
     return make_c1(int(count), world_seed, width=max(20.0, 200.0 * scale), height=max(10.0, 100.0 * scale))
 
 
-def make_c4_worlds(worlds: int = 4096, seed: int = 0, lo: int = 16, hi: int = 2048, processes: int = 1) -> list:
+def c4_counts(worlds: int = 4096, seed: int = 0, lo: int = 16, hi: int = 2048) -> np.ndarray:
+    """Body counts of the batched-worlds workload: log-uniform in [lo, hi], one draw per world."""
+    return log_uniform_counts(np.random.default_rng(seed), worlds, lo, hi)
+
+
+def shard_by_bodies(counts, ranks: int) -> list:
+    """Greedy body-count balancing of independent worlds over ranks: worlds largest first (ties: lower index), each
+    to the rank with the fewest bodies so far (ties: lower rank). Returns each rank's world indices, ascending. The
+    loads differ by at most the largest world's count."""
+    counts = np.asarray(counts, dtype=np.int64)
+    order = sorted(range(counts.size), key=lambda k: (-int(counts[k]), k))
+    load = [0] * ranks
+    out = [[] for _ in range(ranks)]
+    for k in order:
+        r = min(range(ranks), key=lambda j: (load[j], j))
+        out[r].append(k)
+        load[r] += int(counts[k])
+    return [sorted(x) for x in out]
+
+
+def make_c4_worlds(worlds: int = 4096, seed: int = 0, lo: int = 16, hi: int = 2048, processes: int = 1,
+                   subset=None) -> list:
     """Batched worlds: body counts log-uniform in [lo, hi]; world k is make_c1(count_k, seed + k) (c1 shape mix,
     own ground box), with the region scaled so the body density matches c1 (2048 bodies in 200 x 100 m).
+    subset: only these world indices (in that order), e.g. one rank's shard_by_bodies share of the job.
     processes > 1 generates the worlds in a spawned process pool (same worlds: each has its own seed)."""
-    rng = np.random.default_rng(seed)
-    counts = log_uniform_counts(rng, worlds, lo, hi)
-    jobs = [(int(counts[k]), seed + k) for k in range(worlds)]
+    counts = c4_counts(worlds, seed, lo, hi)
+    ks = range(worlds) if subset is None else list(subset)
+    jobs = [(int(counts[k]), seed + k) for k in ks]
+    worlds = len(jobs)
     if processes > 1 and worlds > 1:
         import multiprocessing as mp
         with mp.get_context("spawn").Pool(processes) as pool:
