@@ -18,11 +18,13 @@
 # Flags are the parity build: -O2 -mavx2 -mfma -ffp-contract=off (no fast-math). Explicit FMA intrinsics in
 # the reference's SIMD wrapper still fuse; that is the reference's own arithmetic.
 #
-# Usage: oracle/ref_build.sh [reference_root]   (default /root/reference). Output: oracle/_ref/libagony_ref.so
+# Usage: oracle/ref_build.sh [reference_root]. The reference root is the argument, else $AG2D_REFERENCE_ROOT, else
+# /root/reference (the build container's checkout). Output: oracle/_ref/libagony_ref.so. Exit status 2: no
+# reference checkout there (nothing built).
 set -euo pipefail
 
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF_ROOT="${1:-/root/reference}"
+REF_ROOT="${1:-${AG2D_REFERENCE_ROOT:-/root/reference}}"
 OUT="$HERE/_ref"
 SRC_ENGINE="$REF_ROOT/PhysicsSimulation-Agony/PS_AGONY2D"
 LIB_INC="$REF_ROOT/Libraries/include"
