@@ -273,16 +273,31 @@ class Timer:
         return float(sum(self.ms))
 
 
-def roofline_line(phases, bytes_by_phase, kernel_of, workload):
+def roofline_line(phases, bytes_by_phase, kernel_of, workload, solve_passes=None):
+    """The dominant phase's roofline. For the solver, solve_passes (bytes by pass, whole run) is listed per launch
+    beside the total, with the velocity passes' own fraction (the measurement unit's 192 B per manifold per
+    velocity iteration over the whole kernel's time, a lower bound on what those passes reach)."""
     dominant = max(bytes_by_phase, key=lambda p: phases[p][0])
     peak, peak_kind = measured_peaks()
     dom_ms, dom_calls = phases[dominant]
     achieved = bytes_by_phase[dominant] / max(dom_ms / 1e3, 1e-12) / 1e9
     calls = max(dom_calls, 1)
-    return {"bound": "hbm", "kernel": kernel_of[dominant], "phase": dominant, "achieved": achieved, "peak": peak,
+    traffic = dram_traffic(f"{workload}:{kernel_of[dominant]}")
+    line = {"bound": "hbm", "kernel": kernel_of[dominant], "phase": dominant, "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-            "traffic": dram_traffic(f"{workload}:{kernel_of[dominant]}"),
-            "algorithmic_bytes_per_launch": bytes_by_phase[dominant] / calls, "launch_ms": dom_ms / calls}
+            "traffic": traffic, "algorithmic_bytes_per_launch": bytes_by_phase[dominant] / calls,
+            "launch_ms": dom_ms / calls}
+    if traffic:
+        line["traffic_frac"] = traffic / max(dom_ms / calls / 1e3, 1e-12) / 1e9 / peak   # measured DRAM bytes
+    if dominant == "solve" and solve_passes:
+        line["bytes_per_launch_by_pass"] = {k: v / calls for k, v in solve_passes.items()}
+        line["velocity_passes_frac"] = solve_passes["velocity"] / max(dom_ms / 1e3, 1e-12) / 1e9 / peak
+    return line
+
+
+def solve_passes(manifolds_sum, vi=8, pi=3):
+    from ag2d import roofline
+    return roofline.solve_bytes_breakdown(manifolds_sum, vi, pi)
 
 
 def step_bytes(msb, pairs_sum, manifolds_sum, dyn_bodies, steps, vi=8, pi=3):
@@ -652,7 +667,7 @@ def run_c4(args, torch, dist, rank, world_size, local, dev):
     bytes_by_phase = step_bytes(msb, sums["pairs"], sums["manifolds"], n_bodies - len(scene_list), K)
     kernel_of = {"solve": "k_color_solve_teams", "narrow": "k_narrow", "integrate": "k_integrate",
                  "pose": "k_collider_pose", "sort": "k_sort_pass", "query": "k_query_stash + k_query_emit"}
-    roof = roofline_line(phases, bytes_by_phase, kernel_of, "c4")
+    roof = roofline_line(phases, bytes_by_phase, kernel_of, "c4", solve_passes(sums["manifolds"]))
     del batch, e
 
     # End to end through the C ABI, over the same window: the batch restored from the host checkpoint of the
@@ -768,7 +783,7 @@ def run_c2(args, torch, dist, rank, world_size, local, dev):
     bytes_by_phase = step_bytes(msb, sums["pairs"], sums["manifolds"], nb - int((scene.mass == 0).sum()), K)
     kernel_of = {"solve": "k_color_solve_cluster", "narrow": "k_narrow", "integrate": "k_integrate",
                  "pose": "k_collider_pose", "sort": "k_sort_pass", "query": "k_query_stash + k_query_emit"}
-    roof = roofline_line(phases, bytes_by_phase, kernel_of, "c2")
+    roof = roofline_line(phases, bytes_by_phase, kernel_of, "c2", solve_passes(sums["manifolds"]))
 
     e2e_steps = min(K, 300)
     if world_size > 1:

@@ -90,6 +90,8 @@ typedef struct ag2d_tuning {
     uint32_t narrow_threads;   /* narrow-phase block size */
     float solve_ms, query_ms, narrow_ms;   /* device time per step of each phase at the chosen setting */
     uint32_t team_cons_on_chip;  /* batched solver: a team's constraint records kept in shared memory (1) or not */
+    uint32_t big_team_mode;      /* batched solver, worlds larger than a team: bit 0 = 256-thread CTAs (else 512),
+                                    bit 1 = record loads pipelined one phase ahead */
 } ag2d_tuning;
 
 /* Reference-layout world state for ag2d_world_load_state: every array in the reference's dense order, as its
@@ -113,6 +115,9 @@ typedef struct ag2d_state_desc {
      * them (ColliderSoA worldPos / worldRotationCos / Sin, aabbMin / Max). */
     const float *col_world_x, *col_world_y, *col_world_cos, *col_world_sin;
     const float *col_aabb_min_x, *col_aabb_min_y, *col_aabb_max_x, *col_aabb_max_y;
+    /* Capsules (CapsuleSoA): colliders of shape type 3 index these arrays. */
+    uint32_t n_capsules;
+    const float *capsule_half_length, *capsule_radius;   /* [n_capsules] */
 } ag2d_state_desc;
 
 /* Readable / writable world fields (ag2d_world_read / ag2d_world_write). Body and collider arrays are float32 or
@@ -125,6 +130,7 @@ enum ag2d_field {
     AG2D_BODY_INV_MASS, AG2D_BODY_INV_INERTIA,
     AG2D_COL_WORLD_X = 32, AG2D_COL_WORLD_Y, AG2D_COL_WORLD_ROTATION, AG2D_COL_WORLD_COS, AG2D_COL_WORLD_SIN,
     AG2D_COL_AABB_MIN_X, AG2D_COL_AABB_MIN_Y, AG2D_COL_AABB_MAX_X, AG2D_COL_AABB_MAX_Y,
+    AG2D_COL_BODY /* uint32: the owner body's dense index (read only) */,
     AG2D_DYN_SORTED = 64,   /* dynamic tree: collider indices in Morton order */
     AG2D_DYN_MORTON,        /* dynamic tree: sorted Morton keys */
     AG2D_PAIRS,             /* candidate pairs (uint32 a, b) */
@@ -181,6 +187,22 @@ int32_t ag2d_world_add_box(ag2d_world* world, const ag2d_body_desc* body, float 
                            uint64_t* out_handle);
 int32_t ag2d_world_add_polygon(ag2d_world* world, const ag2d_body_desc* body, const float* vertices_xy,
                                uint32_t vertex_count, uint64_t* out_handle);
+/* ObjectAPI::createBodyH (ObjectAPI.h:61; ObjectManager::createBody, ObjectManager.cpp:71-88): a body with the
+ * descriptor's pose, velocities and mass, the given inertia and local centre of mass, and no collider yet. */
+int32_t ag2d_world_create_body(ag2d_world* world, const ag2d_body_desc* body, float inertia, float com_x,
+                               float com_y, uint64_t* out_handle);
+/* ObjectAPI::create{Circle,Box,Polygon,Capsule}Collider (ObjectAPI.h:29-32; ObjectManager.cpp:90-231): a collider
+ * on an existing body at a local offset and rotation. shape: 0 circle (params[0] radius), 1 box (params = width,
+ * height), 2 polygon (xy / n_vertices: a convex outline, recentred on its centroid with the shift added to the
+ * offset; concave outlines return AG2D_ERR_UNSUPPORTED: the reference would decompose them), 3 capsule (params =
+ * length, radius). The body's mass and inertia stay as created. out_collider: the collider's dense index. */
+int32_t ag2d_world_add_collider(ag2d_world* world, uint64_t body, int32_t shape, float local_x, float local_y,
+                                float local_rotation, uint32_t material, const float* params, const float* xy,
+                                uint32_t n_vertices, uint32_t* out_collider);
+/* ObjectAPI::createCapsuleH (SimulationAPIs/ObjectAPI.h:65; ObjectManager::createCapsule, ObjectManager.cpp:351-388):
+ * a capsule body whose core of 'length' (cap centre to cap centre) lies along the body's x axis, swept by 'radius'. */
+int32_t ag2d_world_add_capsule(ag2d_world* world, const ag2d_body_desc* body, float length, float radius,
+                               uint64_t* out_handle);
 /* Creates 'count' bodies in one call: the same bodies, in the same order, as the matching add_circle / add_box /
  * add_polygon calls (a scene loader's loop over ObjectAPI::create*, ObjectAPI.h:20-45, without a call per body).
  * kinds[i]: 0 circle (params[2i] = radius), 1 box (params[2i], params[2i+1] = width, height), 2 polygon
@@ -191,6 +213,31 @@ int32_t ag2d_world_add_bodies(ag2d_world* world, uint32_t count, const ag2d_body
                               const uint32_t* poly_counts, const float* poly_xy, uint64_t* out_handles);
 /* Dense body index of a handle (ObjectAPI::getBodyIndex, ObjectAPI.h:53), or UINT32_MAX if stale. */
 uint32_t ag2d_world_body_index(ag2d_world* world, uint64_t handle);
+
+/* ---- deferred body commands: ObjectAPI::destroyBody / setBody* (SimulationAPIs/ObjectAPI.h:72-81) ----
+ * Queued in call order and applied at the start of the next step, as the reference applies its command queue in
+ * Simulation::update (Simulation.cpp:39 -> ObjectManager::flushCommands / applyCommand, ObjectManager.cpp:
+ * 638-790), or at once by ag2d_world_flush_commands. A command on a stale handle is dropped when applied. Every
+ * command wakes the body's sleeping island. A position is the body origin's (the centre of mass moves with it); a
+ * rotation is wrapped into [0, 2 pi); mass 0 makes the body static (its velocities zeroed), a positive mass scales
+ * the inertia by new / old mass; an inertia is ignored on a static body. A destroyed body keeps its dense index
+ * with state AG2D_BODY_DESTROYED: it is in no work list or tree, touches nothing, and its handle goes stale (the
+ * reference pops it from its dense arrays instead; handles are what both keep stable). Per world: a batch
+ * engine's worlds take no commands (AG2D_ERR_UNSUPPORTED). */
+enum ag2d_body_state { AG2D_BODY_STATIC = 0, AG2D_BODY_SLEEPING = 1, AG2D_BODY_DYNAMIC = 2, AG2D_BODY_DESTROYED = 3 };
+enum ag2d_command {
+    AG2D_COMMAND_DESTROY = 0, AG2D_COMMAND_POSITION, AG2D_COMMAND_ROTATION, AG2D_COMMAND_VELOCITY,
+    AG2D_COMMAND_ANGULAR_VELOCITY, AG2D_COMMAND_MASS, AG2D_COMMAND_INERTIA
+};
+int32_t ag2d_world_destroy_body(ag2d_world* world, uint64_t body);
+int32_t ag2d_world_set_body_position(ag2d_world* world, uint64_t body, float x, float y);
+int32_t ag2d_world_set_body_rotation(ag2d_world* world, uint64_t body, float rotation);
+int32_t ag2d_world_set_body_velocity(ag2d_world* world, uint64_t body, float vx, float vy);
+int32_t ag2d_world_set_body_angular_velocity(ag2d_world* world, uint64_t body, float angular_velocity);
+int32_t ag2d_world_set_body_mass(ag2d_world* world, uint64_t body, float mass);
+int32_t ag2d_world_set_body_inertia(ag2d_world* world, uint64_t body, float inertia);
+/* Applies the queued commands now (Simulation::flushCommands, Simulation.cpp:453-456). */
+int32_t ag2d_world_flush_commands(ag2d_world* world);
 
 /* Replaces the world with a reference-layout state (parity harness: same inputs as the reference). */
 int32_t ag2d_world_load_state(ag2d_world* world, const ag2d_state_desc* state);

@@ -54,8 +54,31 @@ struct BodyCreateParams {
     Real rotation = 0;
     Real angularVelocity = 0;
     Real mass = 0;          // 0: a static body
-    Real inertia = 0;       // 0: from the shape (the only form the C ABI takes)
+    Real inertia = 0;       // create<Shape>: must be 0 (inertia from the shape); createBody: the body's inertia
+    std::optional<Vec2> centerOfMass = std::nullopt;   // createBody only: local centre of mass (default origin)
     MaterialIndex materialIndex = 0;
+};
+// Collider params (SimulationImpl/ObjectCreateParams.h:26-69): a shape attached to an existing body at a local offset
+// and rotation. Polygons must be convex here (the reference decomposes concave outlines); capsules take the
+// length / radius form.
+struct ColliderCreateParams {
+    Handle bodyHandle;
+    Vec2 localOffset{};
+    Real localRotation = 0;
+    MaterialIndex materialIndex = 0;
+};
+struct CircleColliderCreateParams : ColliderCreateParams {
+    Real radius = 0;
+};
+struct BoxColliderCreateParams : ColliderCreateParams {
+    Vec2 size{};
+};
+struct PolygonColliderCreateParams : ColliderCreateParams {
+    std::span<const Vec2> localVertices;
+};
+struct CapsuleColliderCreateParams : ColliderCreateParams {
+    Real length = 0;
+    Real radius = 0;
 };
 struct CircleCreateParams {
     BodyCreateParams base;
@@ -68,6 +91,13 @@ struct BoxCreateParams {
 struct PolygonCreateParams {
     BodyCreateParams base;
     std::span<Vec2> localVertices;
+};
+// CapsuleCreateParams (SimulationImpl/ObjectCreateParams.h:98-105) without the endpoint form: a core of 'length'
+// along the body's x axis, swept by 'radius'.
+struct CapsuleCreateParams {
+    BodyCreateParams base;
+    Real length = 0;
+    Real radius = 0;
 };
 
 struct FixedClockSettings {
@@ -128,6 +158,7 @@ public:
     std::optional<ObjectDenseIndex> createCircle(const CircleCreateParams& p) { return index(createCircleH(p)); }
     std::optional<ObjectDenseIndex> createBox(const BoxCreateParams& p) { return index(createBoxH(p)); }
     std::optional<ObjectDenseIndex> createPolygon(const PolygonCreateParams& p) { return index(createPolygonH(p)); }
+    std::optional<ObjectDenseIndex> createCapsule(const CapsuleCreateParams& p) { return index(createCapsuleH(p)); }
 
     std::optional<Handle> createCircleH(const CircleCreateParams& p)
     {
@@ -153,6 +184,61 @@ public:
         uint64_t h = 0;
         return created(ag2d_world_add_polygon(world, &d, xy.data(), uint32_t(p.localVertices.size()), &h), h);
     }
+
+    std::optional<Handle> createCapsuleH(const CapsuleCreateParams& p)
+    {
+        if (p.base.inertia != 0) return std::nullopt;
+        const ag2d_body_desc d = detail::desc(p.base);
+        uint64_t h = 0;
+        return created(ag2d_world_add_capsule(world, &d, p.length, p.radius, &h), h);
+    }
+
+    // ObjectAPI::createBody / createBodyH (ObjectAPI.h:28, 61): a body with explicit mass, inertia and centre of
+    // mass and no collider; colliders are attached with create*Collider (ObjectAPI.h:29-32), which return the new
+    // collider's dense index.
+    std::optional<ObjectDenseIndex> createBody(const BodyCreateParams& p) { return index(createBodyH(p)); }
+    std::optional<Handle> createBodyH(const BodyCreateParams& p)
+    {
+        const ag2d_body_desc d = detail::desc(p);
+        const Vec2 com = p.centerOfMass.value_or(Vec2{});
+        uint64_t h = 0;
+        return created(ag2d_world_create_body(world, &d, p.inertia, com.x, com.y, &h), h);
+    }
+    std::optional<ObjectDenseIndex> createCircleCollider(const CircleColliderCreateParams& p)
+    {
+        const float params[2] = {p.radius, 0};
+        return collider(p, 0, params, nullptr, 0);
+    }
+    std::optional<ObjectDenseIndex> createBoxCollider(const BoxColliderCreateParams& p)
+    {
+        const float params[2] = {p.size.x, p.size.y};
+        return collider(p, 1, params, nullptr, 0);
+    }
+    std::optional<ObjectDenseIndex> createPolygonCollider(const PolygonColliderCreateParams& p)
+    {
+        std::vector<float> xy;
+        xy.reserve(p.localVertices.size() * 2);
+        for (const Vec2& v : p.localVertices) { xy.push_back(v.x); xy.push_back(v.y); }
+        return collider(p, 2, nullptr, xy.data(), uint32_t(p.localVertices.size()));
+    }
+    std::optional<ObjectDenseIndex> createCapsuleCollider(const CapsuleColliderCreateParams& p)
+    {
+        const float params[2] = {p.length, p.radius};
+        return collider(p, 3, params, nullptr, 0);
+    }
+
+    // Deferred body commands (ObjectAPI.h:72-81): applied at the start of the next update's first step; stale
+    // handles are dropped then. A destroyed body keeps its dense index with state AG2D_BODY_DESTROYED.
+    void destroyBody(Handle h) { detail::check(ag2d_world_destroy_body(world, h.value)); }
+    void setBodyPosition(Handle h, Vec2 p) { detail::check(ag2d_world_set_body_position(world, h.value, p.x, p.y)); }
+    void setBodyRotation(Handle h, Real r) { detail::check(ag2d_world_set_body_rotation(world, h.value, r)); }
+    void setBodyVelocity(Handle h, Vec2 v) { detail::check(ag2d_world_set_body_velocity(world, h.value, v.x, v.y)); }
+    void setBodyAngularVelocity(Handle h, Real w)
+    {
+        detail::check(ag2d_world_set_body_angular_velocity(world, h.value, w));
+    }
+    void setBodyMass(Handle h, Real m) { detail::check(ag2d_world_set_body_mass(world, h.value, m)); }
+    void setBodyInertia(Handle h, Real i) { detail::check(ag2d_world_set_body_inertia(world, h.value, i)); }
 
     // Dense index of a handle; UINT32_MAX when the handle is stale (ObjectAPI::getBodyIndex, ObjectAPI.h:53).
     ObjectDenseIndex getBodyIndex(Handle h) const noexcept { return ag2d_world_body_index(world, h.value); }
@@ -181,6 +267,19 @@ private:
     {
         if (!h) return std::nullopt;
         return getBodyIndex(*h);
+    }
+    // Failures the reference reports with an empty optional (stale body handle, degenerate or unsupported outline)
+    // come back the same way; others throw.
+    std::optional<ObjectDenseIndex> collider(const ColliderCreateParams& p, int32_t shape, const float* params,
+                                             const float* xy, uint32_t n)
+    {
+        uint32_t c = 0;
+        const int32_t code = ag2d_world_add_collider(world, p.bodyHandle.value, shape, p.localOffset.x,
+                                                     p.localOffset.y, p.localRotation, p.materialIndex, params, xy,
+                                                     n, &c);
+        if (code == AG2D_ERR_INVALID_ARG || code == AG2D_ERR_UNSUPPORTED) return std::nullopt;
+        detail::check(code);
+        return c;
     }
     ag2d_world* world;
 };

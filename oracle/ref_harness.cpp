@@ -27,10 +27,6 @@
 
 using namespace PS_AGONY2D;
 
-// PolygonCapsule.cpp is not compiled (GCC rejects its goto); capsules are in no workload.
-void PS_AGONY2D::NarrowPhaseCollisionDetector::collisionPolygonCapsule(
-    std::span<const ObjectPair>, CacheLineAlignedVector<BodyCollisionData>&) {}
-
 namespace
 {
     // IThreadingBackend (PS_AGONY2D/Threading.h:10-22): every launched task runs on its own pool thread, all
@@ -124,6 +120,7 @@ namespace
         float dt = 1.0f / 60.0f;
         size_t threads = 0;
         std::map<std::string, std::vector<uint8_t>> blobs;
+        std::vector<uint32_t> createdGeneration;   // per body handle slot: its generation when the body was created
 
         template <class T>
         void put(const std::string& name, const T* data, size_t count)
@@ -230,6 +227,9 @@ namespace
         h->putv(p + "poly.counts", counts);
         h->putv(p + "poly.vertices", verts);
         h->putv(p + "poly.normals", norms);
+        h->putv(p + "capsule.colliderIndices", om.capsules.colliderIndices);
+        h->putv(p + "capsule.halfLength", om.capsules.halfLength);
+        h->putv(p + "capsule.radius", om.capsules.radius);
     }
 
     // Manifolds with collider handles resolved to current dense collider indices.
@@ -274,7 +274,10 @@ namespace
     int64_t finishBody(Harness* h, std::optional<ObjectDenseIndex> idx)
     {
         if (!idx) return -1;
-        return int64_t(h->sim.objectManager.bodies.handleAt(*idx).slot);
+        const Handle hd = h->sim.objectManager.bodies.handleAt(*idx);
+        if (h->createdGeneration.size() <= hd.slot) h->createdGeneration.resize(size_t(hd.slot) + 1, 0u);
+        h->createdGeneration[hd.slot] = hd.generation;
+        return int64_t(hd.slot);
     }
 }
 
@@ -360,6 +363,97 @@ extern "C"
         p.base = baseParams(px, py, rot, vx, vy, w, mass, mat);
         p.radius = radius;
         return finishBody(h, h->sim.objects().createCircle(p));
+    }
+
+    int64_t agref_add_capsule(void* hp, float length, float radius, float px, float py, float rot, float vx,
+                              float vy, float w, float mass, uint32_t mat)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        CapsuleCreateParams p;
+        p.base = baseParams(px, py, rot, vx, vy, w, mass, mat);
+        p.length = length;
+        p.radius = radius;
+        return finishBody(h, h->sim.objects().createCapsule(p));
+    }
+
+    // ObjectAPI::createBody + create*Collider (ObjectAPI.h:28-32): a body with explicit mass, inertia and centre of
+    // mass, then colliders on it. Returns the body's handle slot / the collider's dense index, -1 on failure.
+    int64_t agref_create_body(void* hp, float px, float py, float rot, float vx, float vy, float w, float mass,
+                              float inertia, float comX, float comY)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        BodyCreateParams b = baseParams(px, py, rot, vx, vy, w, mass, 0);
+        b.inertia = inertia;
+        b.centerOfMass = Vec2(comX, comY);
+        return finishBody(h, h->sim.objects().createBody(b));
+    }
+    int64_t agref_add_collider(void* hp, uint32_t slot, int32_t shape, float lx, float ly, float lrot, uint32_t mat,
+                               float p0, float p1, const float* xy, uint32_t n);
+
+    // ObjectAPI's deferred body commands (SimulationAPIs/ObjectAPI.h:72-81), by body handle slot: the handle the
+    // body got at creation (so a destroyed body's handle stays stale, even once its slot is reused); the reference
+    // applies them at its next flushCommands (ObjectManager.cpp:638).
+    static Handle bodyHandleOfSlot(Harness* h, uint32_t slot)
+    {
+        return Handle{slot, slot < h->createdGeneration.size() ? h->createdGeneration[slot] : 0u};
+    }
+    void agref_destroy_body(void* hp, uint32_t slot)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        h->sim.objects().destroyBody(bodyHandleOfSlot(h, slot));
+    }
+    // kind: 0 position (a, b), 1 rotation (a), 2 velocity (a, b), 3 angular velocity (a), 4 mass (a), 5 inertia (a).
+    void agref_set_body(void* hp, uint32_t slot, int32_t kind, float a, float b)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        const Handle hd = bodyHandleOfSlot(h, slot);
+        auto& o = h->sim.objects();
+        switch (kind)
+        {
+        case 0: o.setBodyPosition(hd, Vec2(a, b)); break;
+        case 1: o.setBodyRotation(hd, a); break;
+        case 2: o.setBodyVelocity(hd, Vec2(a, b)); break;
+        case 3: o.setBodyAngularVelocity(hd, a); break;
+        case 4: o.setBodyMass(hd, a); break;
+        case 5: o.setBodyInertia(hd, a); break;
+        default: break;
+        }
+    }
+    // Dense body index of a handle slot (UINT32_MAX when destroyed).
+    uint32_t agref_body_index(void* hp, uint32_t slot)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        return h->sim.objectManager.bodies.indexOf(bodyHandleOfSlot(h, slot));
+    }
+
+    int64_t agref_add_collider(void* hp, uint32_t slot, int32_t shape, float lx, float ly, float lrot, uint32_t mat,
+                               float p0, float p1, const float* xy, uint32_t n)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        auto& o = h->sim.objects();
+        const Handle body = bodyHandleOfSlot(h, slot);
+        std::optional<ObjectDenseIndex> c;
+        switch (shape)
+        {
+        case 0: c = o.createCircleCollider({.bodyHandle = body, .localOffset = Vec2(lx, ly), .localRotation = lrot,
+                                            .materialIndex = mat, .radius = p0}); break;
+        case 1: c = o.createBoxCollider({.bodyHandle = body, .localOffset = Vec2(lx, ly), .localRotation = lrot,
+                                         .materialIndex = mat, .size = Vec2(p0, p1)}); break;
+        case 2: {
+            std::vector<Vec2> v(n);
+            for (uint32_t i = 0; i < n; i++) v[i] = Vec2(xy[2 * i], xy[2 * i + 1]);
+            PolygonColliderCreateParams p;
+            p.bodyHandle = body; p.localOffset = Vec2(lx, ly); p.localRotation = lrot; p.materialIndex = mat;
+            p.localVertices = v.data(); p.verticesCount = n;
+            auto r = o.createPolygonCollider(p);
+            if (r) c = r->firstColliderIndex;
+            break;
+        }
+        case 3: c = o.createCapsuleCollider({.bodyHandle = body, .localOffset = Vec2(lx, ly), .localRotation = lrot,
+                                             .materialIndex = mat, .length = p0, .radius = p1}); break;
+        default: break;
+        }
+        return c ? int64_t(*c) : -1;
     }
 
     // Steps through the reference's public entry point, Simulation::update (Simulation.cpp:32-74). With

@@ -48,7 +48,17 @@ def lib():
         L.agref_add_box.argtypes = [vp, f, f, f, f, f, f, f, f, f, u32]
         L.agref_add_circle.restype = i64
         L.agref_add_circle.argtypes = [vp, f, f, f, f, f, f, f, f, u32]
+        L.agref_add_capsule.restype = i64
+        L.agref_add_capsule.argtypes = [vp, f, f, f, f, f, f, f, f, f, u32]
+        L.agref_create_body.restype = i64
+        L.agref_create_body.argtypes = [vp, f, f, f, f, f, f, f, f, f, f]
+        L.agref_add_collider.restype = i64
+        L.agref_add_collider.argtypes = [vp, u32, i32, f, f, f, u32, f, f, vp, u32]
         L.agref_update.argtypes = [vp, i32]
+        L.agref_destroy_body.argtypes = [vp, u32]
+        L.agref_set_body.argtypes = [vp, u32, i32, f, f]
+        L.agref_body_index.restype = u32
+        L.agref_body_index.argtypes = [vp, u32]
         L.agref_timed_update.restype = ctypes.c_double
         L.agref_timed_update.argtypes = [vp, i32]
         L.agref_timed_collide.restype = ctypes.c_double
@@ -111,6 +121,8 @@ class RefSim:
                 slot = L.agref_add_polygon(self.h, v.ctypes.data, v.shape[0], *args)
             elif k == 1:
                 slot = L.agref_add_box(self.h, float(scene.width[i]), float(scene.height[i]), *args)
+            elif k == 3:
+                slot = L.agref_add_capsule(self.h, float(scene.width[i]), float(scene.radius[i]), *args)
             else:
                 slot = L.agref_add_circle(self.h, float(scene.radius[i]), *args)
             if slot < 0:
@@ -127,6 +139,46 @@ class RefSim:
             self.close()
         except Exception:
             pass
+
+    # ObjectAPI deferred body commands, by the handle slot the constructor recorded for scene body i.
+    SET_POSITION, SET_ROTATION, SET_VELOCITY, SET_ANGULAR_VELOCITY, SET_MASS, SET_INERTIA = range(6)
+
+    def destroy_body(self, i: int):
+        lib().agref_destroy_body(self.h, self.body_slots[i])
+
+    def set_body(self, i: int, kind: int, a: float, b: float = 0.0):
+        lib().agref_set_body(self.h, self.body_slots[i], kind, a, b)
+
+    def add_material(self, elasticity: float, static_friction: float, dynamic_friction: float) -> int:
+        """Simulation::addMaterial; the new material's index."""
+        return int(lib().agref_material(self.h, elasticity, static_friction, dynamic_friction))
+
+    def create_body(self, x, y, rotation=0.0, vx=0.0, vy=0.0, w=0.0, mass=1.0, inertia=1.0, com=(0.0, 0.0)) -> int:
+        """ObjectAPI::createBody: a body without colliders. Returns its index in body_slots (like a scene body's)."""
+        slot = lib().agref_create_body(self.h, x, y, rotation, vx, vy, w, mass, inertia, com[0], com[1])
+        if slot < 0:
+            raise ValueError("reference rejected the body")
+        self.body_slots.append(slot)
+        return len(self.body_slots) - 1
+
+    def add_collider(self, i: int, shape: int, offset=(0.0, 0.0), rotation=0.0, material=0, radius=0.0, width=0.0,
+                     height=0.0, length=0.0, vertices=None) -> int:
+        """ObjectAPI::create*Collider on body i (0 circle, 1 box, 2 polygon, 3 capsule); the collider's dense index.
+        material is a material index as returned by the reference (0 = its default material)."""
+        p0, p1 = {0: (radius, 0.0), 1: (width, height), 2: (0.0, 0.0), 3: (length, radius)}[shape]
+        xy, n = None, 0
+        if vertices is not None:
+            v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 2)
+            xy, n = v.ctypes.data, v.shape[0]
+        c = lib().agref_add_collider(self.h, self.body_slots[i], shape, offset[0], offset[1], rotation, material, p0,
+                                     p1, xy, n)
+        if c < 0:
+            raise ValueError("reference rejected the collider")
+        return int(c)
+
+    def body_index(self, i: int) -> int:
+        """Dense index of scene body i now (2**32 - 1 once destroyed)."""
+        return int(lib().agref_body_index(self.h, self.body_slots[i]))
 
     def update(self, steps: int = 1):
         lib().agref_update(self.h, steps)

@@ -28,7 +28,7 @@ BODY_COM_X, BODY_COM_Y, BODY_VEL_X, BODY_VEL_Y, BODY_ROTATION, BODY_ANGULAR_VELO
     BODY_WRAP_COUNT, BODY_SLEEP_TIMER, BODY_STATE, BODY_SLEEP_ISLAND, BODY_POSE, BODY_INV_MASS, \
     BODY_INV_INERTIA = range(1, 16)
 COL_WORLD_X, COL_WORLD_Y, COL_WORLD_ROTATION, COL_WORLD_COS, COL_WORLD_SIN, COL_AABB_MIN_X, COL_AABB_MIN_Y, \
-    COL_AABB_MAX_X, COL_AABB_MAX_Y = range(32, 41)
+    COL_AABB_MAX_X, COL_AABB_MAX_Y, COL_BODY = range(32, 42)
 DYN_SORTED, DYN_MORTON, PAIRS, MANIFOLDS, PREV_MANIFOLDS, SOLVE_ORDER, COLOR_STARTS = range(64, 71)
 # enum ag2d_phase
 PHASE_INTEGRATE, PHASE_SPATIAL_FULL, PHASE_SPATIAL_DYNAMIC, PHASE_BROAD, PHASE_NARROW, PHASE_SOLVE, \
@@ -40,7 +40,7 @@ MANIFOLD_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("nx", "<f4"), ("ny", "<f
                            ("jt1", "<f4")])
 assert MANIFOLD_DTYPE.itemsize == 64
 
-_U32_FIELDS = {BODY_STATE, BODY_SLEEP_ISLAND, DYN_SORTED, DYN_MORTON, SOLVE_ORDER, COLOR_STARTS}
+_U32_FIELDS = {BODY_STATE, BODY_SLEEP_ISLAND, COL_BODY, DYN_SORTED, DYN_MORTON, SOLVE_ORDER, COLOR_STARTS}
 
 
 class Ag2dError(RuntimeError):
@@ -79,7 +79,8 @@ class Counters(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("team_colliders", ctypes.c_uint32), ("team_threads", ctypes.c_uint32), ("query_threads", ctypes.c_uint32),
                 ("narrow_threads", ctypes.c_uint32), ("solve_ms", ctypes.c_float), ("query_ms", ctypes.c_float),
-                ("narrow_ms", ctypes.c_float), ("team_cons_on_chip", ctypes.c_uint32)]
+                ("narrow_ms", ctypes.c_float), ("team_cons_on_chip", ctypes.c_uint32),
+                ("big_team_mode", ctypes.c_uint32)]
 
 
 TIMED_PHASES = ("integrate", "pose", "tree_dynamic", "tree_other", "query", "narrow", "compact", "warm", "wake",
@@ -99,6 +100,8 @@ class ServerStats(ctypes.Structure):
 
 
 REQUEST_WAITING, REQUEST_RUNNING, REQUEST_DONE = 0, 1, 2
+# enum ag2d_body_state (AG2D_BODY_STATE values)
+STATE_STATIC, STATE_SLEEPING, STATE_DYNAMIC, STATE_DESTROYED = 0, 1, 2, 3
 # enum ag2d_tree_flag / ag2d_query_shape
 TREE_DYNAMIC, TREE_STATIC, TREE_SLEEPING, TREE_ALL = 1, 2, 4, 7
 QUERY_AABB, QUERY_CIRCLE = 0, 1
@@ -116,7 +119,8 @@ class StateDesc(ctypes.Structure):
                                   "col_local_rotation", "circle_radius", "box_half_width", "box_half_height",
                                   "poly_count", "poly_vertices", "poly_normals", "materials", "col_world_x",
                                   "col_world_y", "col_world_cos", "col_world_sin", "col_aabb_min_x",
-                                  "col_aabb_min_y", "col_aabb_max_x", "col_aabb_max_y")]
+                                  "col_aabb_min_y", "col_aabb_max_x", "col_aabb_max_y")] + \
+               [("n_capsules", ctypes.c_uint32), ("capsule_half_length", _P), ("capsule_radius", _P)]
 
 
 def _load():
@@ -135,9 +139,21 @@ def _load():
     L.ag2d_world_add_box.argtypes = [vp, ctypes.POINTER(BodyDesc), ctypes.c_float, ctypes.c_float,
                                      ctypes.POINTER(u64)]
     L.ag2d_world_add_polygon.argtypes = [vp, ctypes.POINTER(BodyDesc), vp, u32, ctypes.POINTER(u64)]
+    L.ag2d_world_add_capsule.argtypes = [vp, ctypes.POINTER(BodyDesc), ctypes.c_float, ctypes.c_float,
+                                         ctypes.POINTER(u64)]
     L.ag2d_world_body_index.restype = u32
+    L.ag2d_world_create_body.argtypes = [vp, ctypes.POINTER(BodyDesc), ctypes.c_float, ctypes.c_float,
+                                         ctypes.c_float, ctypes.POINTER(u64)]
+    L.ag2d_world_add_collider.argtypes = [vp, u64, i32, ctypes.c_float, ctypes.c_float, ctypes.c_float, u32, vp, vp,
+                                          u32, ctypes.POINTER(u32)]
     L.ag2d_world_add_bodies.argtypes = [vp, u32, ctypes.POINTER(BodyDesc), vp, vp, vp, vp, vp, vp]
     L.ag2d_world_body_index.argtypes = [vp, u64]
+    L.ag2d_world_destroy_body.argtypes = [vp, u64]
+    for name in ("position", "velocity"):
+        getattr(L, f"ag2d_world_set_body_{name}").argtypes = [vp, u64, ctypes.c_float, ctypes.c_float]
+    for name in ("rotation", "angular_velocity", "mass", "inertia"):
+        getattr(L, f"ag2d_world_set_body_{name}").argtypes = [vp, u64, ctypes.c_float]
+    L.ag2d_world_flush_commands.argtypes = [vp]
     L.ag2d_world_load_state.argtypes = [vp, ctypes.POINTER(StateDesc)]
     L.ag2d_world_step.argtypes = [vp, i32]
     L.ag2d_world_counters.argtypes = [vp, ctypes.POINTER(Counters)]
@@ -306,8 +322,68 @@ class World:
         _check(lib.ag2d_world_add_polygon(self.h, ctypes.byref(d), v.ctypes.data, v.shape[0], ctypes.byref(h)))
         return int(h.value)
 
+    def add_capsule(self, length, radius, x, y, rotation=0.0, vx=0.0, vy=0.0, w=0.0, mass=1.0, material=0) -> int:
+        """A capsule body: a core of `length` along the body's x axis swept by `radius`."""
+        h = ctypes.c_uint64()
+        d = self._desc(x, y, rotation, vx, vy, w, mass, material)
+        _check(lib.ag2d_world_add_capsule(self.h, ctypes.byref(d), length, radius, ctypes.byref(h)))
+        return int(h.value)
+
+    def create_body(self, x, y, rotation=0.0, vx=0.0, vy=0.0, w=0.0, mass=1.0, inertia=1.0, com=(0.0, 0.0)) -> int:
+        """A body with explicit mass, inertia and local centre of mass and no collider yet (ObjectAPI::createBody)."""
+        h = ctypes.c_uint64()
+        d = self._desc(x, y, rotation, vx, vy, w, mass, 0)
+        _check(lib.ag2d_world_create_body(self.h, ctypes.byref(d), inertia, com[0], com[1], ctypes.byref(h)))
+        return int(h.value)
+
+    def add_collider(self, body: int, shape: int, offset=(0.0, 0.0), rotation=0.0, material=0, radius=0.0,
+                     width=0.0, height=0.0, length=0.0, vertices=None) -> int:
+        """Attaches a collider to `body` at a local offset and rotation (ObjectAPI::create*Collider); returns its
+        dense collider index. shape: CIRCLE (radius), BOX (width, height), POLYGON (convex `vertices`, recentred
+        on their centroid), CAPSULE (length, radius)."""
+        params = (ctypes.c_float * 2)()
+        if shape == 0:
+            params[0] = radius
+        elif shape == 1:
+            params[0], params[1] = width, height
+        elif shape == 3:
+            params[0], params[1] = length, radius
+        xy, n = None, 0
+        if vertices is not None:
+            v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 2)
+            xy, n = v.ctypes.data, v.shape[0]
+        out = ctypes.c_uint32()
+        _check(lib.ag2d_world_add_collider(self.h, body, shape, offset[0], offset[1], rotation, material, params,
+                                          xy, n, ctypes.byref(out)))
+        return int(out.value)
+
     def body_index(self, handle: int) -> int:
         return int(lib.ag2d_world_body_index(self.h, handle))
+
+    # --- deferred body commands (ObjectAPI::destroyBody / setBody*): applied at the start of the next step ---
+    def destroy_body(self, handle: int):
+        _check(lib.ag2d_world_destroy_body(self.h, handle))
+
+    def set_body_position(self, handle: int, x: float, y: float):
+        _check(lib.ag2d_world_set_body_position(self.h, handle, x, y))
+
+    def set_body_rotation(self, handle: int, rotation: float):
+        _check(lib.ag2d_world_set_body_rotation(self.h, handle, rotation))
+
+    def set_body_velocity(self, handle: int, vx: float, vy: float):
+        _check(lib.ag2d_world_set_body_velocity(self.h, handle, vx, vy))
+
+    def set_body_angular_velocity(self, handle: int, w: float):
+        _check(lib.ag2d_world_set_body_angular_velocity(self.h, handle, w))
+
+    def set_body_mass(self, handle: int, mass: float):
+        _check(lib.ag2d_world_set_body_mass(self.h, handle, mass))
+
+    def set_body_inertia(self, handle: int, inertia: float):
+        _check(lib.ag2d_world_set_body_inertia(self.h, handle, inertia))
+
+    def flush_commands(self):
+        _check(lib.ag2d_world_flush_commands(self.h))
 
     @classmethod
     def from_scene(cls, scene, device=0, **kw):
@@ -329,9 +405,9 @@ class World:
         d["material"] = np.where(m >= 1, mats[np.clip(m - 1, 0, len(mats) - 1)], 0)
         kinds = np.ascontiguousarray(scene.kind, dtype=np.uint32)
         params = np.zeros((max(n, 1), 2), np.float32)
-        circ, box = kinds == scenes.CIRCLE, kinds == scenes.BOX
-        params[:n, 0] = np.where(circ, scene.radius, np.where(box, scene.width, 0.0))
-        params[:n, 1] = np.where(box, scene.height, 0.0)
+        circ, box, cap = kinds == scenes.CIRCLE, kinds == scenes.BOX, kinds == scenes.CAPSULE
+        params[:n, 0] = np.where(circ, scene.radius, np.where(box | cap, scene.width, 0.0))
+        params[:n, 1] = np.where(box, scene.height, np.where(cap, scene.radius, 0.0))
         offs = np.ascontiguousarray(scene.poly_offset, dtype=np.uint32)
         cnts = np.ascontiguousarray(scene.poly_count, dtype=np.uint32)
         xy = np.ascontiguousarray(scene.poly_xy, dtype=np.float32).reshape(-1)
@@ -367,6 +443,11 @@ class World:
             "box_half_height": g("box.halfHeight", f), "poly_count": g("poly.counts", u),
             "poly_vertices": g("poly.vertices", f), "poly_normals": g("poly.normals", f),
         }
+        for k, name in (("capsule.halfLength", "capsule_half_length"), ("capsule.radius", "capsule_radius")):
+            try:
+                arrays[name] = g(k, f)
+            except KeyError:
+                arrays[name] = np.zeros(0, f)
         mats = np.ascontiguousarray(np.asarray(materials if materials is not None else [(1.0, 0.0, 0.0)],
                                                dtype=np.float32).reshape(-1, 3))
         arrays["materials"] = mats
@@ -385,6 +466,7 @@ class World:
         d.n_boxes = arrays["box_half_width"].size
         d.n_polygons = arrays["poly_count"].size
         d.n_materials = mats.shape[0]
+        d.n_capsules = arrays["capsule_half_length"].size
         for k, v in arrays.items():
             setattr(d, k, v.ctypes.data if v.size else None)
         self._keep = list(arrays.values())

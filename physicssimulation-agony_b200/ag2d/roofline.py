@@ -1,8 +1,9 @@
 """Algorithmic bytes per phase of the collision/contact step (the HBM roofline's numerator).
 
 A phase's algorithmic bytes are the bytes its kernel must move between HBM and the SMs for the work it does, with
-each input read once and each output written once (no re-reads, no scratch): achieved GB/s = these bytes / the
-kernel's measured time, and frac = achieved / the measured HBM copy bandwidth. Per-unit figures follow the device
+each input read once per pass and each output written once (no scratch): achieved GB/s = these bytes / the kernel's
+measured time, and frac = achieved / the measured HBM copy bandwidth. Only the solver makes several dependent passes
+over the same records (see SOLVE_VELOCITY_PER_ITERATION). Per-unit figures follow the device
 layout (csrc/ag2d_world.cuh): body state float4 (16 B) + float4 (16 B) + cos/sin float2 (8 B); collider pose and
 AABB float4 each; manifold 64 B; solver constraint 128 B.
 """
@@ -30,14 +31,29 @@ def narrow_bytes(pairs: float, mean_shape_bytes: float, manifolds: float) -> flo
     return pairs * (8.0 + 2.0 * (20.0 + mean_shape_bytes) + 4.0) + manifolds * 64.0
 
 
+# Solver bytes per manifold. The velocity and position passes are Gauss-Seidel sweeps: each pass depends on the one
+# before, so each reads its constraint again (the unit of the measurement specification: per manifold per velocity
+# iteration 112 B of constraint, 48 B of two bodies' velocity and angular velocity read and written, 32 B of the two
+# contacts' normal and tangent impulses read and written). Preparation, warm start, position passes and the
+# impulse write-back are listed separately, each input read once within its pass.
+SOLVE_VELOCITY_PER_ITERATION = 112 + 48 + 32
+SOLVE_PREP = 64 + 16 + 2 * 32 + 112          # manifold, owners + materials, two bodies' state, constraint written
+SOLVE_WARM = 32 + 48                         # impulses read, two bodies' velocities read and written
+SOLVE_POSITION_PER_ITERATION = 48 + 48       # anchors, normal and penetration; two bodies' x, y, angle read+written
+SOLVE_SCATTER = 16                           # accumulated impulses written back to the manifold
+
+
+def solve_bytes_breakdown(manifolds: float, velocity_iterations: int, position_iterations: int) -> dict:
+    """Algorithmic bytes of one solve, by pass: prep, warm, velocity (the measurement unit's 192 B per manifold per
+    velocity iteration), position, scatter."""
+    m = float(manifolds)
+    return {"prep": m * SOLVE_PREP, "warm": m * SOLVE_WARM,
+            "velocity": m * velocity_iterations * SOLVE_VELOCITY_PER_ITERATION,
+            "position": m * position_iterations * SOLVE_POSITION_PER_ITERATION, "scatter": m * SOLVE_SCATTER}
+
+
 def solve_bytes(manifolds: float, velocity_iterations: int, position_iterations: int) -> float:
-    """Per manifold: constraint build (manifold 64, owners + materials 16, two bodies' float4 x2 64, write 128),
-    warm start (constraint 128, two velocities read + written 64), each velocity iteration (constraint 128,
-    velocities 64, impulses 16), each position iteration (normal/bodies/penetration 24, positions 64, inverse
-    masses 32), scatter (impulses 16 read + 16 written)."""
-    per = (64 + 16 + 64 + 128) + (128 + 64) + velocity_iterations * (128 + 64 + 16) + \
-        position_iterations * (24 + 64 + 32) + 32
-    return manifolds * float(per)
+    return float(sum(solve_bytes_breakdown(manifolds, velocity_iterations, position_iterations).values()))
 
 
 def sort_bytes(keys: float) -> float:

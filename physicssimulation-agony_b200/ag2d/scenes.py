@@ -5,7 +5,8 @@ The reference publishes no scenes or datasets; these generators stand in for its
 distributions each workload names. A scene is a flat, numpy-backed body list that both this library and the
 reference engine can be loaded from, so every comparison starts from bit-identical inputs.
 
-Shape codes follow the reference's ColliderShapeType (PS_AGONY2D/Types/Types.h:35-42): 0 circle, 1 box, 2 polygon.
+Shape codes follow the reference's ColliderShapeType (PS_AGONY2D/Types/Types.h:35-42): 0 circle, 1 box, 2 polygon,
+3 capsule.
 Mass 0 means a static body (ObjectManager::appendBody, PS_AGONY2D/SimulationImpl/ObjectManager.cpp:1285).
 """
 from __future__ import annotations
@@ -15,7 +16,7 @@ import math
 
 import numpy as np
 
-CIRCLE, BOX, POLYGON = 0, 1, 2
+CIRCLE, BOX, POLYGON, CAPSULE = 0, 1, 2, 3
 
 
 @dataclasses.dataclass
@@ -33,8 +34,8 @@ class Scene:
     vy: np.ndarray
     w: np.ndarray
     mass: np.ndarray          # 0 = static
-    radius: np.ndarray        # circles
-    width: np.ndarray         # boxes (full size)
+    radius: np.ndarray        # circles and capsules
+    width: np.ndarray         # boxes (full size); capsules: core length (end cap centre to end cap centre)
     height: np.ndarray
     poly_offset: np.ndarray   # int64, polygons
     poly_count: np.ndarray    # int32, polygons
@@ -149,6 +150,40 @@ def make_c2(n: int = 100_000, seed: int = 0, columns: int = 500, cell: float = 4
             verts = polygon_on_circle(rng, rng.uniform(0.5, 2.0))
             b.add(POLYGON, x, y, mass=polygon_area(verts), verts=verts, material=1)
     return b.build(f"c2_n{n}_s{seed}")
+
+
+def make_capsule_mix(n: int = 1500, seed: int = 0, columns: int = 40, cell: float = 4.8) -> Scene:
+    """Every shape pair, capsules included: n bodies (30% capsules of core length U[0.4,2.4] m and radius
+    U[0.15,0.6] m at random rotations, 25% boxes side U[0.3,1.5], 20% circles r U[0.2,1], 25% 3-8-gons from the c1
+    generator), one per cell of a columns-wide grid above the floor of a static U container, density 1."""
+    rng = np.random.default_rng(seed)
+    b = _Builder([FRICTION_MATERIAL])
+    rows = (n + columns - 1) // columns
+    inner = columns * cell
+    wall_h = rows * cell + 20.0
+    b.add(BOX, 0.0, -1.0, width=inner + 4.0, height=2.0, mass=0.0, material=1)
+    b.add(BOX, -0.5 * inner - 1.0, 0.5 * wall_h, width=2.0, height=wall_h, mass=0.0, material=1)
+    b.add(BOX, 0.5 * inner + 1.0, 0.5 * wall_h, width=2.0, height=wall_h, mass=0.0, material=1)
+    kinds = rng.random(n)
+    for i in range(n):
+        col, row = i % columns, i // columns
+        x = -0.5 * inner + (col + 0.5) * cell
+        y = 0.5 * cell + row * cell
+        u = kinds[i]
+        if u < 0.30:
+            length, r = rng.uniform(0.4, 2.4), rng.uniform(0.15, 0.6)
+            b.add(CAPSULE, x, y, rot=rng.uniform(0.0, math.pi), radius=r, width=length,
+                  mass=length * 2.0 * r + math.pi * r * r, material=1)
+        elif u < 0.55:
+            s = rng.uniform(0.3, 1.5)
+            b.add(BOX, x, y, width=s, height=s, mass=s * s, material=1)
+        elif u < 0.75:
+            r = rng.uniform(0.2, 1.0)
+            b.add(CIRCLE, x, y, radius=r, mass=math.pi * r * r, material=1)
+        else:
+            verts = polygon_on_circle(rng, rng.uniform(0.5, 2.0))
+            b.add(POLYGON, x, y, mass=polygon_area(verts), verts=verts, material=1)
+    return b.build(f"capmix_n{n}_s{seed}")
 
 
 def make_c3(n: int = 1_000_000, seed: int = 0, extent: float = 4000.0) -> Scene:

@@ -64,6 +64,21 @@ __device__ __forceinline__ float ccd_cast_box(V2 q0, V2 dl, float dd, float hw, 
 
 // Convex polygon (local vertices / outward normals) inflated by 'radius': offset half-planes give the entry and
 // exit times; an entry beyond its edge's span is decided by the rounded corner.
+// castCapsule (ContinuousCollisionDetector.cpp:222-240): the slab on q0's side, then the two end circles.
+__device__ __forceinline__ float ccd_cast_capsule(V2 q0, V2 dl, float dd, float halfLength, float capsuleRadius,
+                                                  float radius, float best)
+{
+    const float inflated = capsuleRadius + radius;
+    const float nvy = -copysignf(1.0f, q0.y) * dl.y;
+    const float gap = fabsf(q0.y) - inflated;
+    if (nvy > 0.0f && gap >= 0.0f && gap < best * nvy) {
+        const float time = gap / nvy;
+        if (fabsf(q0.x + dl.x * time) <= halfLength) return time;
+    }
+    const float t = rfminf(ccd_cast_circle(q0.x + halfLength, q0.y, dl.x, dl.y, dd, inflated, best), best);
+    return rfminf(ccd_cast_circle(q0.x - halfLength, q0.y, dl.x, dl.y, dd, inflated, t), t);
+}
+
 __device__ __forceinline__ float ccd_cast_polygon(V2 q0, V2 dl, float dd, const float2* verts, const float2* normals,
                                                   uint32_t count, float radius, float best)
 {

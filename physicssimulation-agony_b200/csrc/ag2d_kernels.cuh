@@ -77,28 +77,63 @@ __global__ void k_lbvh_refit(int n, const int2* child, const int* parent, const 
                              const float4* leafAabb, float4* nodeAabb, float4* meet, NodeRec* rec);
 // Empty marker of a refit meeting slot (min x bits): a NaN no arithmetic produces.
 constexpr uint32_t MEET_EMPTY = 0xFFFFFFFFu;
-__global__ void k_query_stash(TreeView dyn, TreeView other, const uint32_t* cbody, uint32_t* counts, uint2* stash,
-                              uint32_t* status);
-__global__ void k_query_emit(TreeView dyn, TreeView other, const uint32_t* cbody, const uint32_t* counts,
-                             const uint32_t* offsets, const uint2* stash, uint2* pairs, uint32_t pairCap,
-                             uint32_t* status);
+// Pair query: every candidate pair of the dynamic colliders, in query-rank order, into pairs; *total = the count.
+// tileState [tiles + 1] and tileCounter zeroed before the launch (tiles: blockDim.x queries each).
+constexpr uint32_t QUERY_MAX_THREADS = 256;
+__global__ void k_query(TreeView dyn, TreeView other, const uint32_t* cbody, uint2* pairs, uint32_t pairCap,
+                        uint32_t* total, uint32_t* status, uint32_t* tileState, uint32_t* tileCounter);
 __global__ void k_ccd_sweep(DeviceWorld w, const uint32_t* dynCol, uint32_t n, TreeView other, const float4* prevPos,
                             const float4* prevPose, const float* minExtent, uint32_t* hitTime, uint32_t* status);
 __global__ void k_ccd_shift_colliders(DeviceWorld w, const uint32_t* dynCol, uint32_t n, const float4* prevPos,
                                       const uint32_t* hitTime);
 __global__ void k_ccd_shift_bodies(DeviceWorld w, const uint32_t* dynBody, uint32_t n, const float4* prevPos,
                                    uint32_t* hitTime, StepCounters* counters);
-__global__ void k_scan_blocks(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* blockSums, const uint32_t* nDev);
-__global__ void k_scan_add(uint32_t* out, uint32_t n, const uint32_t* blockOffsets, const uint32_t* nDev);
-__global__ void k_scan_total(const uint32_t* in, const uint32_t* out, uint32_t n, uint32_t* total);
+// Decoupled look-back over tiles taken in ticket order: tile t publishes flag << 30 | value in tileState[t] (flag 1:
+// its aggregate, 2: its inclusive prefix) and sums its predecessors' values, read by the calling warp 32 at a time,
+// nearest first, up to the nearest inclusive prefix. A tile only waits on tiles with smaller tickets, all held by
+// running blocks, so the waits end; each is still bounded by SPIN_LIMIT (then STATUS_LOOKBACK_TIMEOUT is set and the
+// partial sum returned). Called by one full warp; returns the exclusive prefix of tile 'tile' (> 0).
+__device__ __forceinline__ uint32_t scan_lookback(uint32_t tile, uint32_t* tileState, uint32_t* status)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    volatile uint32_t* state = tileState;
+    uint32_t prefix = 0, spins = 0;
+    int32_t t = int32_t(tile) - 1;
+    while (t >= 0) {
+        const int32_t idx = t - int32_t(lane);
+        const uint32_t sv = idx >= 0 ? state[idx] : (2u << 30);
+        const uint32_t flag = sv >> 30;
+        const uint32_t inc = __ballot_sync(0xffffffffu, flag == 2u);
+        const uint32_t window = inc ? (((inc & (0u - inc)) << 1) - 1u) : 0xffffffffu;   // lanes up to the nearest
+        if (__ballot_sync(0xffffffffu, flag == 0u) & window) {                             // inclusive prefix
+            if (++spins > SPIN_LIMIT) {
+                if (lane == 0) atomicOr(status, STATUS_LOOKBACK_TIMEOUT);
+                break;
+            }
+            continue;
+        }
+        uint32_t v = ((window >> lane) & 1u) ? (sv & 0x3FFFFFFFu) : 0u;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        prefix += v;
+        if (inc) break;
+        t -= 32;
+    }
+    return prefix;
+}
+
+// Exclusive scan of in[0, min(n, *nDev)) into out (nDev may be null), total = the sum (may be null).
+__global__ void k_scan(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_t* nDev, uint32_t* total,
+                       uint32_t* tileState, uint32_t* tileCounter, uint32_t* status);
 
 // Contact kernels (k_contact.cu).
-constexpr uint32_t NARROW_SMEM_PER_THREAD = 2 * MAX_POLYGON_VERTICES * sizeof(V2) / NARROW_GROUP;
-__global__ void k_narrow(DeviceWorld w, const uint2* pairs, const uint32_t* nPairs, uint32_t pairCap,
-                         Manifold* slots, uint32_t* hit);
-__global__ void k_compact_manifolds(const Manifold* slots, const uint32_t* hit, const uint32_t* offsets,
-                                    const uint32_t* nPairs, uint32_t pairCap, Manifold* out, uint32_t manifoldCap,
-                                    uint32_t* nOut, StepCounters* counters);
+// Per thread: a 64-byte manifold slot, a hit flag and its share of its group's vertex tiles (100 bytes).
+constexpr uint32_t NARROW_SMEM_PER_THREAD =
+    uint32_t(sizeof(Manifold) + sizeof(uint32_t) + 2 * MAX_POLYGON_VERTICES * sizeof(V2) / NARROW_GROUP);
+// Narrow phase + manifold compaction: manifolds of the hit pairs, in pair order, into out; tileState [tiles + 1] and
+// tileCounter zeroed before the launch (tiles: blockDim.x pairs each).
+__global__ void k_narrow(DeviceWorld w, const uint2* pairs, const uint32_t* nPairs, uint32_t pairCap, Manifold* out,
+                         uint32_t manifoldCap, uint32_t* nOut, StepCounters* counters, uint32_t* tileState,
+                         uint32_t* tileCounter);
 __global__ void k_warm_insert(const Manifold* prev, const uint32_t* nPrev, unsigned long long* keys,
                               uint32_t* vals, uint32_t capacity, uint32_t* status);
 constexpr uint32_t WARM_CACHED = 0x80000000u;   // contact-cache value flag: the manifold had a non-zero impulse

@@ -35,7 +35,9 @@ constexpr float ZERO_DIVISION_BOUNDARY_SQUARED = 1e-8f;
 constexpr float SAT_EPSILON = 1e-4f;
 constexpr uint32_t REFERENCE_BODY_TAG = 0x80000000u;
 
-enum ShapeType : uint32_t { SHAPE_CIRCLE = 0, SHAPE_BOX = 1, SHAPE_POLYGON = 2 };
+enum ShapeType : uint32_t { SHAPE_CIRCLE = 0, SHAPE_BOX = 1, SHAPE_POLYGON = 2, SHAPE_CAPSULE = 3 };
+constexpr uint32_t CAPSULE_VERTEX_CONTACT_TAG = 0x40000000u;   // Narrow/Constants.h:40
+constexpr float CAPSULE_PARALLEL_SIN_SQUARED = 1e-3f;          // Narrow/Constants.h:41
 constexpr uint32_t MAX_POLYGON_VERTICES = 16;   // Limits.h:6
 
 // std::fmax / std::fmin as glibc implements them on x86-64 (the reference's build): the first argument if it
@@ -127,8 +129,8 @@ struct ColliderView {
     V2 pos;
     float c, s;            // world rotation cos/sin
     uint32_t type;
-    float r;               // circle radius
-    float hw, hh;          // box half extents
+    float r;               // circle radius; capsule radius
+    float hw, hh;          // box half extents; capsule: hw = half length of the core
     const float2* verts;   // polygon, body-local (centred on the piece centroid)
     const float2* normals;
     uint32_t nv;
@@ -643,9 +645,383 @@ __device__ __forceinline__ bool collide_polygon_polygon_group(const ColliderView
     return __shfl_sync(mask, hit ? 1u : 0u, __ffs(mask) - 1) != 0;
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// Capsules: a core segment of half length hw along the collider's local x axis, swept by radius r
+// (CollisionMethods/*Capsule*.cpp). clampValue (HelperMethods.h:111-114) is fmin(fmax(v, lo), hi).
+// ---------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ float clamp_value(float v, float lo, float hi) { return rfminf(rfmaxf(v, lo), hi); }
+
+// collisionCircleCapsule, the scalar path (CircleCapsule.cpp:148-203). The 8-lane batch (:55-146) computes the same
+// manifold except when the circle's centre lies within ZERO_DIVISION_BOUNDARY of the core, where it picks the
+// fallback normal's side from another expression; this routine takes the scalar one there.
+__device__ __forceinline__ bool collide_circle_capsule(const ColliderView& A, const ColliderView& B, Contact& out)
+{
+    const float radiusA = A.r, halfLengthB = B.hw, radiusB = B.r;
+    const V2 axisB = v2(B.c, B.s);
+    const V2 d = A.pos - B.pos;
+    const float t = clamp_value(dot(d, axisB), -halfLengthB, halfLengthB);
+    const V2 delta = axisB * t - d;
+    const float radiusSum = radiusA + radiusB;
+    const float squaredDistance = dot(delta, delta);
+    if (squaredDistance >= radiusSum * radiusSum) return false;
+    const float distance = sqrtf(squaredDistance);
+    const float depth = radiusSum - distance;
+    V2 normal;
+    if (distance < ZERO_DIVISION_BOUNDARY) normal = flip_if_negative(v2(B.s, -B.c), d.x * B.s + d.y * B.c);
+    else normal = delta * (1.0f / distance);
+    out.n = normal;
+    out.depth = depth;
+    out.count = 1;
+    out.p[0] = A.pos + normal * radiusA;
+    out.id[0] = 0;
+    return true;
+}
+
+// collisionCapsuleCapsule (CapsuleCapsule.cpp:23-157).
+__device__ __forceinline__ bool collide_capsule_capsule(const ColliderView& A, const ColliderView& B, Contact& out)
+{
+    const float halfLengthA = A.hw, halfLengthB = B.hw, radiusA = A.r, radiusB = B.r;
+    const V2 positionA = A.pos, positionB = B.pos;
+    const V2 centerDelta = positionB - positionA;
+    const float radiusSum = radiusA + radiusB;
+    const float reach = halfLengthA + halfLengthB + radiusSum;
+    if (dot(centerDelta, centerDelta) >= reach * reach) return false;
+    const V2 axisA = v2(A.c, A.s), axisB = v2(B.c, B.s);
+    const float b = dot(axisA, axisB);
+    const float centerAlongA = dot(centerDelta, axisA);
+    const float c = -centerAlongA;
+    const float f = -dot(axisB, centerDelta);
+    const float sinSquared = 1.0f - b * b;
+    const bool parallel = sinSquared < CAPSULE_PARALLEL_SIN_SQUARED;
+    const float extentB = fabsf(b) * halfLengthB;
+    const float overlapLo = rfmaxf(-halfLengthA, centerAlongA - extentB);
+    const float overlapHi = rfminf(halfLengthA, centerAlongA + extentB);
+    const bool hasOverlap = parallel && (overlapHi - overlapLo >= ZERO_DIVISION_BOUNDARY);
+    float s, t;
+    if (hasOverlap) {
+        s = 0.5f * (overlapLo + overlapHi);
+        t = clamp_value(b * s + f, -halfLengthB, halfLengthB);
+    } else {
+        s = parallel ? 0.0f : clamp_value((b * f - c) / sinSquared, -halfLengthA, halfLengthA);
+        t = b * s + f;
+        t = clamp_value(t, -halfLengthB, halfLengthB);
+        s = clamp_value(b * t - c, -halfLengthA, halfLengthA);
+    }
+    const V2 pointA = positionA + axisA * s;
+    const V2 pointB = positionB + axisB * t;
+    const V2 delta = pointB - pointA;
+    const float squaredDistance = dot(delta, delta);
+    if (squaredDistance >= radiusSum * radiusSum) return false;
+    V2 normal;
+    float depth;
+    if (squaredDistance >= ZERO_DIVISION_BOUNDARY_SQUARED) {
+        const float distance = sqrtf(squaredDistance);
+        normal = delta * (1.0f / distance);
+        depth = radiusSum - distance;
+    } else {
+        // Core segments intersect: separate along the cheaper of the two side axes.
+        const V2 sideA = v2(-axisA.y, axisA.x), sideB = v2(-axisB.y, axisB.x);
+        const float offsetA = dot(centerDelta, sideA);
+        const float offsetB = dot(centerDelta, sideB);
+        const float depthA = fabsf(dot(axisB, sideA)) * halfLengthB - fabsf(offsetA);
+        const float depthB = fabsf(dot(axisA, sideB)) * halfLengthA - fabsf(offsetB);
+        if (depthA <= depthB) { normal = flip_if_negative(sideA, offsetA); depth = depthA; }
+        else { normal = flip_if_negative(sideB, offsetB); depth = depthB; }
+        depth += radiusSum;
+    }
+    uint32_t count = 0;
+    if (hasOverlap) {
+        // Side by side: one contact at each end of the overlap, if within reach.
+        const V2 sideB = v2(-axisB.y, axisB.x);
+        const float ends[2] = {overlapLo, overlapHi};
+        float minGap = FLT_MAX;
+        for (uint32_t k = 0; k < 2; k++) {
+            const V2 p = positionA + axisA * ends[k];
+            const float gap = fabsf(dot(p - positionB, sideB));
+            if (gap >= radiusSum) continue;
+            out.p[count] = p + normal * radiusA;
+            out.id[count] = k;
+            count++;
+            minGap = rfminf(minGap, gap);
+        }
+        if (count != 0) depth = radiusSum - minGap;
+    }
+    if (count == 0) {
+        out.p[0] = pointA + normal * radiusA;
+        out.id[0] = 2;
+        count = 1;
+    }
+    out.n = normal;
+    out.depth = depth;
+    out.count = count;
+    return true;
+}
+
+// collisionBoxCapsule (BoxCapsule.cpp:26-242): box A, capsule B, normal from the box to the capsule.
+__device__ __forceinline__ bool collide_box_capsule(const ColliderView& A, const ColliderView& B, Contact& out)
+{
+    const V2 halfExtents = v2(A.hw, A.hh);
+    const V2 positionA = A.pos, rightA = v2(A.c, A.s), positionB = B.pos, axisB = v2(B.c, B.s);
+    const float halfLengthB = B.hw, radius = B.r;
+    const V2 upA = v2(-rightA.y, rightA.x);
+    const V2 centerDelta = positionB - positionA;
+    // Capsule pose in box-local space, folded into the +,+ quadrant.
+    const float localX = dot(centerDelta, rightA);
+    const float localY = dot(centerDelta, upA);
+    const float sx = copysignf(1.0f, localX);
+    const float sy = copysignf(1.0f, localY);
+    const V2 center = v2(fabsf(localX), fabsf(localY));
+    const V2 axis = v2((rightA.x * axisB.x + rightA.y * axisB.y) * sx, (rightA.x * axisB.y - rightA.y * axisB.x) * sy);
+    const float absAxisX = fabsf(axis.x), absAxisY = fabsf(axis.y);
+    const float sepX = center.x - halfLengthB * absAxisX - halfExtents.x;
+    const float sepY = center.y - halfLengthB * absAxisY - halfExtents.y;
+    const float faceSeparation = rfmaxf(sepX, sepY);
+    if (faceSeparation >= radius) return false;
+    const V2 sideAxis = v2(-axis.y, axis.x);
+    const float sideOffset = dot(sideAxis, center);
+    const float sideSeparation = fabsf(sideOffset) - (halfExtents.x * absAxisY + halfExtents.y * absAxisX);
+    if (sideSeparation >= radius) return false;
+    const bool sideWins = sideSeparation > faceSeparation + SAT_EPSILON;
+    const bool swap = !sideWins && sepY > sepX;
+    // Working frame: reference face at x = ext.x.
+    const V2 ext = swap ? v2(halfExtents.y, halfExtents.x) : halfExtents;
+    const V2 dir = swap ? v2(axis.y, axis.x) : axis;
+    const V2 mid = swap ? v2(center.y, center.x) : center;
+    const V2 basisX = rightA * sx, basisY = upA * sy;
+    const V2 worldX = swap ? basisY : basisX;
+    const V2 worldY = swap ? basisX : basisY;
+    const V2 halfCore = dir * halfLengthB;
+    const V2 s0 = mid - halfCore, s1 = mid + halfCore;
+    const float length = halfLengthB * 2.0f;
+    auto coreDistSquared = [&](V2 w) {
+        const V2 d = s0 + dir * rfminf(rfmaxf(dot(w - s0, dir), 0.0f), length) - w;
+        return dot(d, d);
+    };
+    V2 normal = v2(1.0f, 0.0f);
+    float depth = 0.0f;
+    uint32_t count = 0;
+    V2 point0 = v2(0.0f, 0.0f), point1 = v2(0.0f, 0.0f);
+    uint32_t id0 = 0, id1 = 0;
+    bool faceContact = false;
+    bool cornerPosX = true, cornerPosY = true;
+    V2 vertexNormal = v2(1.0f, 0.0f);
+    float vertexSeparation = faceSeparation;
+    if (sideWins) {
+        vertexNormal = sideOffset >= 0.0f ? sideAxis : -sideAxis;
+        vertexSeparation = sideSeparation;
+        cornerPosX = vertexNormal.x >= 0.0f;
+        cornerPosY = vertexNormal.y >= 0.0f;
+    } else {
+        do {
+            V2 c0 = s0, c1 = s1;
+            float e0 = s0.x - ext.x, e1 = s1.x - ext.x;
+            if (faceSeparation > 0.0f) {
+                const float minY = rfminf(s0.y, s1.y), maxY = rfmaxf(s0.y, s1.y);
+                if (minY > ext.y) break;
+                const bool beyondLow = minY < -ext.y, beyondHigh = maxY > ext.y;
+                if (beyondLow || beyondHigh) {
+                    const float invDy = 1.0f / (s1.y - s0.y);
+                    const float tA = (-ext.y - s0.y) * invDy;
+                    const float tB = (ext.y - s0.y) * invDy;
+                    const float tLow = rfmaxf(0.0f, rfminf(tA, tB));
+                    const float tHigh = rfminf(1.0f, rfmaxf(tA, tB));
+                    const V2 span = s1 - s0;
+                    c0 = s0 + span * tLow;
+                    c1 = s0 + span * tHigh;
+                    e0 = c0.x - ext.x;
+                    e1 = c1.x - ext.x;
+                    const float minE = rfminf(e0, e1);
+                    const float faceDistSquared = minE * minE;
+                    if (beyondLow && coreDistSquared(v2(ext.x, -ext.y)) + SAT_EPSILON < faceDistSquared) {
+                        cornerPosY = false;
+                        break;
+                    }
+                    if (beyondHigh && coreDistSquared(ext) + SAT_EPSILON < faceDistSquared) break;
+                }
+            }
+            const V2 clipped = c1 - c0;
+            const bool hasSecond = dot(clipped, clipped) >= ZERO_DIVISION_BOUNDARY_SQUARED;
+            const float contactLimit = radius + SAT_EPSILON;
+            const uint32_t faceId = swap ? (sy < 0.0f ? 0u : 2u) : (sx < 0.0f ? 3u : 1u);
+            const uint32_t idBase = REFERENCE_BODY_TAG | (faceId << 1);
+            if (e0 <= contactLimit) { point0 = v2(c0.x - radius, c0.y); id0 = idBase; count = 1; }
+            if (hasSecond && e1 <= contactLimit) {
+                const V2 p = v2(c1.x - radius, c1.y);
+                if (count == 0) { point0 = p; id0 = idBase | 1u; }
+                else { point1 = p; id1 = idBase | 1u; }
+                count++;
+            }
+            if (count == 0) return false;
+            depth = radius - rfminf(e0, e1);
+            faceContact = true;
+        } while (false);
+    }
+    if (!faceContact) {
+        // Single contact between a box corner and the capsule core.
+        const V2 w = v2(cornerPosX ? ext.x : -ext.x, cornerPosY ? ext.y : -ext.y);
+        const V2 q = s0 + dir * rfminf(rfmaxf(dot(w - s0, dir), 0.0f), length);
+        normal = vertexNormal;
+        depth = radius - vertexSeparation;
+        if (vertexSeparation > 0.0f) {
+            const V2 d = q - w;
+            const float distSquared = dot(d, d);
+            if (distSquared >= radius * radius) return false;
+            if (distSquared >= ZERO_DIVISION_BOUNDARY_SQUARED) {
+                const float distance = sqrtf(distSquared);
+                normal = d * (1.0f / distance);
+                depth = radius - distance;
+            }
+        }
+        // Corner id in real box space (undo the swap, then the fold). Corner order: (-,-), (+,-), (+,+), (-,+).
+        const bool foldedPosX = swap ? cornerPosY : cornerPosX;
+        const bool foldedPosY = swap ? cornerPosX : cornerPosY;
+        const bool realPosX = foldedPosX != (sx < 0.0f);
+        const bool realPosY = foldedPosY != (sy < 0.0f);
+        const uint32_t vertexId = (realPosY ? 2u : 0u) | ((realPosX != realPosY) ? 1u : 0u);
+        count = 1;
+        point0 = q - normal * radius;
+        id0 = CAPSULE_VERTEX_CONTACT_TAG | vertexId;
+    }
+    out.n = worldX * normal.x + worldY * normal.y;
+    out.p[0] = positionA + worldX * point0.x + worldY * point0.y;
+    if (count > 1) out.p[1] = positionA + worldX * point1.x + worldY * point1.y;
+    out.id[0] = id0;
+    out.id[1] = id1;
+    out.depth = depth;
+    out.count = count;
+    return true;
+}
+
+// collisionPolygonCapsule (PolygonCapsule.cpp:27-240): polygon A, capsule B, normal from the polygon to the capsule.
+__device__ __forceinline__ bool collide_polygon_capsule(const ColliderView& A, const ColliderView& B, Contact& out)
+{
+    const uint32_t vertexCount = A.nv;
+    const V2 positionA = A.pos, rightA = v2(A.c, A.s), positionB = B.pos, axisB = v2(B.c, B.s);
+    const float halfLengthB = B.hw, radius = B.r;
+    const V2 upA = v2(-rightA.y, rightA.x);
+    const V2 centerDelta = positionB - positionA;
+    const V2 centerLocal = v2(dot(centerDelta, rightA), dot(centerDelta, upA));
+    const V2 axis = v2(rightA.x * axisB.x + rightA.y * axisB.y, rightA.x * axisB.y - rightA.y * axisB.x);
+    const V2 halfCore = axis * halfLengthB;
+    const V2 s0 = centerLocal - halfCore, s1 = centerLocal + halfCore;
+    const float length = halfLengthB * 2.0f;
+    const V2 sideAxis = v2(-axis.y, axis.x);
+    float faceSeparation = -FLT_MAX;
+    uint32_t faceIndex = 0;
+    float minSide = FLT_MAX, maxSide = -FLT_MAX;
+    uint32_t minSideVertex = 0, maxSideVertex = 0;
+    for (uint32_t i = 0; i < vertexCount; i++) {
+        const V2 v = ld2(A.verts, i), n = ld2(A.normals, i);
+        const float separation = rfminf(dot(n, s0 - v), dot(n, s1 - v));
+        if (separation >= radius) return false;
+        if (separation > faceSeparation) { faceSeparation = separation; faceIndex = i; }
+        const float side = dot(v, sideAxis);
+        if (side < minSide) { minSide = side; minSideVertex = i; }
+        if (side > maxSide) { maxSide = side; maxSideVertex = i; }
+    }
+    const float sideOffset = dot(sideAxis, centerLocal);
+    const float sidePlus = sideOffset - maxSide;
+    const float sideMinus = minSide - sideOffset;
+    const float sideSeparation = rfmaxf(sidePlus, sideMinus);
+    if (sideSeparation >= radius) return false;
+    auto coreDistSquared = [&](V2 w) {
+        const V2 d = s0 + axis * rfminf(rfmaxf(dot(w - s0, axis), 0.0f), length) - w;
+        return dot(d, d);
+    };
+    V2 normal = v2(0.0f, 0.0f);
+    float depth = 0.0f;
+    uint32_t count = 0;
+    V2 point0 = v2(0.0f, 0.0f), point1 = v2(0.0f, 0.0f);
+    uint32_t id0 = 0, id1 = 0;
+    bool faceContact = false;
+    uint32_t vertexId = 0;
+    V2 vertexNormal = v2(0.0f, 0.0f);
+    float vertexSeparation = 0.0f;
+    do {
+        if (sideSeparation > faceSeparation + SAT_EPSILON) {
+            const bool onPlusSide = sidePlus >= sideMinus;
+            vertexId = onPlusSide ? maxSideVertex : minSideVertex;
+            vertexNormal = onPlusSide ? sideAxis : -sideAxis;
+            vertexSeparation = sideSeparation;
+            break;
+        }
+        const uint32_t i0 = faceIndex, i1 = next_index(i0, vertexCount);
+        const V2 a = ld2(A.verts, i0), b = ld2(A.verts, i1), n = ld2(A.normals, i0);
+        const V2 tangent = v2(-n.y, n.x);
+        vertexNormal = n;
+        vertexSeparation = faceSeparation;
+        V2 c0 = s0, c1 = s1;
+        float e0 = dot(s0 - a, n), e1 = dot(s1 - a, n);
+        if (faceSeparation > 0.0f) {
+            const float edgeLength = dot(b - a, tangent);
+            const float t0 = dot(s0 - a, tangent), t1 = dot(s1 - a, tangent);
+            const bool beyondStart = rfminf(t0, t1) < 0.0f;
+            const bool beyondEnd = rfmaxf(t0, t1) > edgeLength;
+            if (beyondStart || beyondEnd) {
+                if (clip_segment(c0, c1, a, tangent)) { vertexId = i0; break; }
+                if (clip_segment(c0, c1, b, -tangent)) { vertexId = i1; break; }
+                e0 = dot(c0 - a, n);
+                e1 = dot(c1 - a, n);
+                const float minE = rfminf(e0, e1);
+                const float faceDistSquared = minE * minE;
+                if (beyondStart && coreDistSquared(a) + SAT_EPSILON < faceDistSquared) { vertexId = i0; break; }
+                if (beyondEnd && coreDistSquared(b) + SAT_EPSILON < faceDistSquared) { vertexId = i1; break; }
+            }
+        }
+        const V2 span = c1 - c0;
+        const bool hasSecond = dot(span, span) >= ZERO_DIVISION_BOUNDARY_SQUARED;
+        const float contactLimit = radius + SAT_EPSILON;
+        const uint32_t idBase = REFERENCE_BODY_TAG | (i0 << 1);
+        if (e0 <= contactLimit) { point0 = c0 - n * radius; id0 = idBase; count = 1; }
+        if (hasSecond && e1 <= contactLimit) {
+            const V2 p = c1 - n * radius;
+            if (count == 0) { point0 = p; id0 = idBase | 1u; }
+            else { point1 = p; id1 = idBase | 1u; }
+            count++;
+        }
+        if (count == 0) return false;
+        normal = n;
+        depth = radius - rfminf(e0, e1);
+        faceContact = true;
+    } while (false);
+    if (!faceContact) {
+        const V2 w = ld2(A.verts, vertexId);
+        const V2 q = s0 + axis * rfminf(rfmaxf(dot(w - s0, axis), 0.0f), length);
+        normal = vertexNormal;
+        depth = radius - vertexSeparation;
+        if (vertexSeparation > 0.0f) {
+            const V2 d = q - w;
+            const float distSquared = dot(d, d);
+            if (distSquared >= radius * radius) return false;
+            if (distSquared >= ZERO_DIVISION_BOUNDARY_SQUARED) {
+                const float distance = sqrtf(distSquared);
+                normal = d * (1.0f / distance);
+                depth = radius - distance;
+            }
+        }
+        count = 1;
+        point0 = q - normal * radius;
+        id0 = CAPSULE_VERTEX_CONTACT_TAG | vertexId;
+    }
+    out.n = rightA * normal.x + upA * normal.y;
+    out.p[0] = positionA + rightA * point0.x + upA * point0.y;
+    if (count > 1) out.p[1] = positionA + rightA * point1.x + upA * point1.y;
+    out.id[0] = id0;
+    out.id[1] = id1;
+    out.depth = depth;
+    out.count = count;
+    return true;
+}
+
 // Dispatch on the (ordered) shape-type pair: typeA <= typeB.
 __device__ __forceinline__ bool collide(const ColliderView& A, const ColliderView& B, Contact& out)
 {
+    if (B.type == SHAPE_CAPSULE) {
+        if (A.type == SHAPE_CIRCLE) return collide_circle_capsule(A, B, out);
+        if (A.type == SHAPE_BOX) return collide_box_capsule(A, B, out);
+        if (A.type == SHAPE_POLYGON) return collide_polygon_capsule(A, B, out);
+        return collide_capsule_capsule(A, B, out);
+    }
     if (A.type == SHAPE_CIRCLE) {
         if (B.type == SHAPE_CIRCLE) return collide_circle_circle(A, B, out);
         if (B.type == SHAPE_BOX) return collide_circle_box(A, B, out);

@@ -371,6 +371,92 @@ __device__ __forceinline__ void prefetch_colour(const SolveScratch& s, uint32_t 
     if (c < Sync::ld(s.colorStart + col + 1)) prefetch_l1(s.cons + c);
 }
 
+// Phases of the solve: what a phase does with its records.
+constexpr uint32_t PHASE_WARM = 0, PHASE_VELOCITY = 1, PHASE_POSITION = 2;
+
+// The fields a phase of 'kind' reads from global record c: the head (bodies, count, normal, masses) and, except
+// for a position phase, the rest; a position phase takes the penetration base instead.
+__device__ __forceinline__ void load_record(const Constraint* __restrict__ cons, uint32_t c, uint32_t kind,
+                                            Constraint& k)
+{
+    const float4* q = reinterpret_cast<const float4*>(cons + c);
+    const float4 h0 = q[0], h1 = q[1];
+    k.bodyA = __float_as_uint(h0.x); k.bodyB = __float_as_uint(h0.y); k.count = __float_as_uint(h0.z);
+    k.manifold = __float_as_uint(h0.w);
+    k.nx = h1.x; k.ny = h1.y; k.imA = h1.z; k.imB = h1.w;
+    if (kind == PHASE_POSITION) {
+        k.penBase = cons[c].penBase;
+        return;
+    }
+    const float4 h2 = q[2], j = q[3], r0 = q[4], m0 = q[5], r1 = q[6], m1 = q[7];
+    k.iIA = h2.x; k.iIB = h2.y; k.sf = h2.z; k.df = h2.w;
+    k.jn0 = j.x; k.jt0 = j.y; k.jn1 = j.z; k.jt1 = j.w;
+    k.rAn0 = r0.x; k.rBn0 = r0.y; k.rAt0 = r0.z; k.rBt0 = r0.w;
+    k.nm0 = m0.x; k.tm0 = m0.y; k.bias0 = m0.z; k.penBase = m0.w;
+    k.rAn1 = r1.x; k.rBn1 = r1.y; k.rAt1 = r1.z; k.rBt1 = r1.w;
+    k.nm1 = m1.x; k.tm1 = m1.y; k.bias1 = m1.z; k.pad = m1.w;
+}
+
+// One phase's step on a record held in registers; a velocity step writes the record's impulses back.
+template <class Bodies>
+__device__ __forceinline__ void solve_record(const Bodies& B, Constraint* __restrict__ cons, uint32_t c, uint32_t kind,
+                                             Constraint& k)
+{
+    if (kind == PHASE_WARM) {
+        warm_constraint(B, k);
+    } else if (kind == PHASE_VELOCITY) {
+        velocity_constraint(B, k);
+        *reinterpret_cast<float4*>(&cons[c].jn0) = make_float4(k.jn0, k.jt0, k.jn1, k.jt1);
+    } else {
+        position_constraint(B, k);
+    }
+}
+
+// The warm, velocity and position passes with global records, pipelined: the passes are one sequence of phases
+// (colour-major within each pass, the barrier between phases); in a phase this thread handles the records
+// start + rank, + size, ... of the phase's colour, and the first of them is loaded one phase ahead. A record is
+// written only by the thread that handles it (its impulses), so its load may cross the barrier, which orders the
+// body state alone: the load is in flight while this phase computes and waits. Same arithmetic, same order as the
+// unpipelined passes; more registers (two records live).
+template <class Sync, class Bodies>
+__device__ bool solve_passes_pipelined(const Bodies& B, const SolveScratch& s, uint32_t ncol, uint32_t velIters,
+                                       uint32_t posIters, uint32_t rank, uint32_t size, Sync sync)
+{
+    const uint32_t nPhase = ncol * (1 + velIters + posIters);
+    auto kindOf = [&](uint32_t ph) {
+        const uint32_t p = ph / ncol;
+        return p == 0 ? PHASE_WARM : (p <= velIters ? PHASE_VELOCITY : PHASE_POSITION);
+    };
+    constexpr uint32_t NO_REC = 0xFFFFFFFFu;
+    Constraint nxt;
+    uint32_t cNext = NO_REC;
+    if (nPhase) {
+        const uint32_t c0 = Sync::ld(s.colorStart) + rank;
+        if (c0 < Sync::ld(s.colorStart + 1)) { load_record(s.cons, c0, kindOf(0), nxt); cNext = c0; }
+    }
+    for (uint32_t ph = 0; ph < nPhase; ph++) {
+        const uint32_t col = ph % ncol, kind = kindOf(ph);
+        const uint32_t end = Sync::ld(s.colorStart + col + 1);
+        Constraint k = nxt;
+        uint32_t c = cNext;   // NO_REC (above every end) when this thread has no record in the phase
+        cNext = NO_REC;
+        if (ph + 1 < nPhase) {
+            const uint32_t col2 = (ph + 1) % ncol;
+            const uint32_t c2 = Sync::ld(s.colorStart + col2) + rank;
+            if (c2 < Sync::ld(s.colorStart + col2 + 1)) { load_record(s.cons, c2, kindOf(ph + 1), nxt); cNext = c2; }
+        }
+        while (c < end) {
+            solve_record(B, s.cons, c, kind, k);
+            // One colour: the next phase's record is this one, loaded before this phase's impulses.
+            if (cNext == c) { nxt.jn0 = k.jn0; nxt.jt0 = k.jt0; nxt.jn1 = k.jn1; nxt.jt1 = k.jt1; }
+            c += size;   // a colour larger than the team
+            if (c < end) load_record(s.cons, c, kind, k);
+        }
+        if (!sync()) return false;
+    }
+    return true;
+}
+
 // Colouring followed by the colour-major solve. Colouring runs Jones-Plassmann rounds: in round r every uncoloured
 // manifold whose priority is the largest on each of its dynamic bodies takes the smallest colour not yet taken
 // around its dynamic bodies (first fit); winners of one round share no dynamic body, so the colours stay
@@ -383,7 +469,7 @@ __device__ __forceinline__ void prefetch_colour(const SolveScratch& s, uint32_t 
 // cannot share a dynamic body: their predecessors were coloured together last step, and a body's dynamic flag
 // (finite mass) does not change between steps. The other manifolds run the Jones-Plassmann rounds around the kept
 // colours. With no hints every manifold runs the rounds. s.color holds colour | age << COLOR_AGE_SHIFT.
-template <class Sync, class Bodies>
+template <class Sync, class Bodies, bool PIPELINED = false>
 __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold* __restrict__ m, uint32_t n,
                                 const SolveScratch& s, uint32_t velIters, uint32_t posIters, uint32_t rank,
                                 uint32_t size, Sync sync, uint32_t* __restrict__ outColors, uint32_t* __restrict__ status,
@@ -506,49 +592,58 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
         else s.cons[c] = k;
     }
     if (!sync()) return false;
-    for (uint32_t col = 0; col < ncol; col++) {
-        const uint32_t end = Sync::ld(s.colorStart + col + 1);
-        for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) {
-            if (onChip) {
-                Constraint k;
-                cs.load(c, k);
-                warm_constraint(B, k);
-            } else {
-                warm_constraint(B, s.cons[c]);
-            }
-        }
-        if (!sync()) return false;
-    }
-    for (uint32_t it = 0; it < velIters; it++) {
-        for (uint32_t col = 0; col < ncol; col++) {
-            const uint32_t end = Sync::ld(s.colorStart + col + 1);
-            for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) {
-                Constraint k;
-                if (onChip) cs.load(c, k);
-                else k = s.cons[c];
-                velocity_constraint(B, k);
-                if (onChip) cs.storeImpulses(c, k);
-                else *reinterpret_cast<float4*>(&s.cons[c].jn0) = make_float4(k.jn0, k.jt0, k.jn1, k.jt1);
-            }
-            // The next pass's constraint: from the next colour, or colour 0 of the next iteration.
-            if (!onChip) prefetch_colour<Sync>(s, col + 1 < ncol ? col + 1 : 0, ncol, rank);
-            if (!sync()) return false;
+    bool passesDone = false;
+    if constexpr (PIPELINED) {
+        if (!onChip) {
+            if (!solve_passes_pipelined(B, s, ncol, velIters, posIters, rank, size, sync)) return false;
+            passesDone = true;
         }
     }
-    for (uint32_t it = 0; it < posIters; it++) {
+    if (!passesDone) {
         for (uint32_t col = 0; col < ncol; col++) {
             const uint32_t end = Sync::ld(s.colorStart + col + 1);
             for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) {
                 if (onChip) {
                     Constraint k;
-                    cs.loadHead(c, k);
-                    position_constraint(B, k);
+                    cs.load(c, k);
+                    warm_constraint(B, k);
                 } else {
-                    position_constraint(B, s.cons[c]);
+                    warm_constraint(B, s.cons[c]);
                 }
             }
-            if (!onChip) prefetch_colour<Sync>(s, col + 1 < ncol ? col + 1 : 0, ncol, rank);
             if (!sync()) return false;
+        }
+        for (uint32_t it = 0; it < velIters; it++) {
+            for (uint32_t col = 0; col < ncol; col++) {
+                const uint32_t end = Sync::ld(s.colorStart + col + 1);
+                for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) {
+                    Constraint k;
+                    if (onChip) cs.load(c, k);
+                    else k = s.cons[c];
+                    velocity_constraint(B, k);
+                    if (onChip) cs.storeImpulses(c, k);
+                    else *reinterpret_cast<float4*>(&s.cons[c].jn0) = make_float4(k.jn0, k.jt0, k.jn1, k.jt1);
+                }
+                // The next pass's constraint: from the next colour, or colour 0 of the next iteration.
+                if (!onChip) prefetch_colour<Sync>(s, col + 1 < ncol ? col + 1 : 0, ncol, rank);
+                if (!sync()) return false;
+            }
+        }
+        for (uint32_t it = 0; it < posIters; it++) {
+            for (uint32_t col = 0; col < ncol; col++) {
+                const uint32_t end = Sync::ld(s.colorStart + col + 1);
+                for (uint32_t c = Sync::ld(s.colorStart + col) + rank; c < end; c += size) {
+                    if (onChip) {
+                        Constraint k;
+                        cs.loadHead(c, k);
+                        position_constraint(B, k);
+                    } else {
+                        position_constraint(B, s.cons[c]);
+                    }
+                }
+                if (!onChip) prefetch_colour<Sync>(s, col + 1 < ncol ? col + 1 : 0, ncol, rank);
+                if (!sync()) return false;
+            }
         }
     }
     for (uint32_t c = rank; c < n; c += size) {
@@ -590,7 +685,9 @@ __host__ __device__ constexpr size_t team_smem_bytes(uint32_t bodyCap, uint32_t 
            (size_t(bodyCap) * 16 > size_t(consCap) * CONS_SMEM_BYTES ? size_t(bodyCap) * 16
                                                                        : size_t(consCap) * CONS_SMEM_BYTES);
 }
-constexpr uint32_t BIG_TEAM_THREADS = 512;     // CTA size for a world larger than the team size
+// Launch shapes of the CTAs that solve a world larger than the team size (one world each): threads per CTA and
+// whether the global-record passes are pipelined (solve_passes_pipelined).
+constexpr uint32_t BIG_TEAM_THREADS = 512;
 struct TeamLaunch {
     DeviceWorld w;
     Manifold* m;
@@ -606,10 +703,11 @@ struct TeamLaunch {
     StepCounters* counters;
 };
 // Host side: launches the team solver with 'threads' per CTA; returns the launch error.
-cudaError_t launch_color_solve_teams(uint32_t threads, uint32_t grid, cudaStream_t stream, const TeamLaunch& a);
+cudaError_t launch_color_solve_teams(uint32_t threads, bool pipelined, uint32_t grid, cudaStream_t stream,
+                                     const TeamLaunch& a);
 // Host side: co-resident CTAs per SM of the team solver at this CTA size and shared-memory capacities. Also raises
 // the kernel's dynamic shared-memory limit to TEAM_SMEM_MAX (the limit is per kernel, shared by every engine in the
 // process, so it is never lowered).
-cudaError_t team_solver_blocks_per_sm(uint32_t threads, uint32_t bodyCap, uint32_t consCap, int* out);
+cudaError_t team_solver_blocks_per_sm(uint32_t threads, bool pipelined, uint32_t bodyCap, uint32_t consCap, int* out);
 
 }  // namespace ag2d

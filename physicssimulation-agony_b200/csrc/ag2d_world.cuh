@@ -14,7 +14,8 @@
 
 namespace ag2d {
 
-enum BodyState : uint8_t { STATE_STATIC = 0, STATE_SLEEPING = 1, STATE_DYNAMIC = 2 };
+// STATE_DESTROYED: a body removed by a destroy command; it keeps its slot but is in no work list or tree.
+enum BodyState : uint8_t { STATE_STATIC = 0, STATE_SLEEPING = 1, STATE_DYNAMIC = 2, STATE_DESTROYED = 3 };
 
 // Error bits of the per-step status word (a device-side failure never traps; the host reads this word).
 enum StatusBits : uint32_t {
@@ -90,7 +91,7 @@ struct DeviceWorld {
     float4* caabb;         // minX, minY, maxX, maxY
     // Shapes.
     float* circleRadius;
-    float2* boxHalf;       // halfWidth, halfHeight
+    float2* boxHalf;       // boxes: halfWidth, halfHeight; capsules (the same table): halfLength, radius
     uint32_t* polyOffset;  // into polyVerts / polyNormals
     uint32_t* polyCount;
     float2* polyVerts;

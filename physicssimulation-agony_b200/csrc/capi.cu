@@ -128,39 +128,34 @@ void swap_bufs(DBuf<T>& a, DBuf<T>& b)
 
 inline uint32_t div_up(uint64_t a, uint64_t b) { return uint32_t((a + b - 1) / b); }
 
-// Exclusive scan with per-level block-sum scratch.
+// A device array copied into host memory (synchronised on return).
+template <class T>
+static std::vector<T> download(const T* p, size_t n, cudaStream_t s)
+{
+    std::vector<T> v(n);
+    if (n) CK(cudaMemcpyAsync(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return v;
+}
+
+// Single-pass exclusive scans (k_scan): the tile states and the ticket counter, zeroed before each scan, and the
+// grid of persistent blocks (set from the SM count when the device is first used).
 struct Scanner {
-    std::vector<std::unique_ptr<DBuf<uint32_t>>> levels;
-    void reserve(uint32_t n)
-    {
-        uint32_t m = n, lvl = 0;
-        while (true) {
-            const uint32_t nb = div_up(std::max<uint32_t>(m, 1), SCAN_TILE);
-            if (nb <= 1) break;
-            if (levels.size() <= lvl) levels.emplace_back(new DBuf<uint32_t>());
-            levels[lvl]->reserve(nb);
-            m = nb;
-            lvl++;
-        }
-    }
+    DBuf<uint32_t> state;          // [tiles + 1]: tile states, then the ticket counter
+    uint32_t blocks = 1;
+    uint32_t* status = nullptr;    // where a look-back that gave up is recorded
+    void reserve(uint32_t n) { state.reserve(size_t(div_up(std::max<uint32_t>(n, 1), SCAN_TILE)) + 1); }
     // Exclusive scan of in[0, n) (n the capacity; nDev, if given, the device-side count within it: elements past it
-    // are neither read nor written).
-    void run(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* total, cudaStream_t s, uint32_t lvl = 0,
+    // are neither read nor written); total, if given, receives the sum.
+    void run(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* total, cudaStream_t s,
              const uint32_t* nDev = nullptr)
     {
-        const uint32_t nb = std::max<uint32_t>(div_up(n, SCAN_TILE), 1);
-        uint32_t* sums = nb > 1 ? levels.at(lvl)->p : nullptr;
-        k_scan_blocks<<<nb, SCAN_THREADS, 0, s>>>(in, out, n, sums, nDev);
+        const uint32_t tiles = std::max<uint32_t>(div_up(n, SCAN_TILE), 1);
+        reserve(n);
+        CK(cudaMemsetAsync(state.p, 0, (size_t(tiles) + 1) * sizeof(uint32_t), s));
+        k_scan<<<std::min(tiles, blocks), SCAN_THREADS, 0, s>>>(in, out, n, nDev, total, state.p, state.p + tiles,
+                                                               status);
         CK(cudaGetLastError());
-        if (nb > 1) {
-            run(sums, sums, nb, nullptr, s, lvl + 1);
-            k_scan_add<<<nb, SCAN_THREADS, 0, s>>>(out, n, sums, nDev);
-            CK(cudaGetLastError());
-        }
-        if (total) {
-            k_scan_total<<<1, 32, 0, s>>>(in, out, n, total);
-            CK(cudaGetLastError());
-        }
     }
 };
 
@@ -222,6 +217,8 @@ inline std::vector<float> min_extents(const std::vector<uint32_t>& cs, const std
             me[i] = cr[si];
         } else if (type == SHAPE_BOX) {
             me[i] = host_fmin(bh[si].x, bh[si].y);
+        } else if (type == SHAPE_CAPSULE) {
+            me[i] = bh[si].y;   // setColliderExtents(radius, ...) (ObjectManager.cpp:228)
         } else {
             float r = FLT_MAX;
             for (uint32_t k = 0; k < pc[si]; k++) {
@@ -299,7 +296,8 @@ struct PackedArrays {
         for (uint32_t v : o.cb) cb.push_back(v + bo);
         for (uint32_t v : o.cs) {
             const uint32_t type = shape_type(v), idx = shape_index(v);
-            const uint32_t base = type == SHAPE_CIRCLE ? circ : (type == SHAPE_BOX ? box : poly);
+            const uint32_t base = type == SHAPE_CIRCLE ? circ : (type == SHAPE_POLYGON ? poly : box);   // box table:
+                                                                                                       // boxes, capsules
             cs.push_back((type << 30) | (idx + base));
         }
         for (uint32_t v : o.cm) cm.push_back(v + mat);
@@ -410,6 +408,8 @@ static DeviceInfo probe_device(int device)
         }
     }
     cudaGetLastError();
+    // The narrow phase stages polygons in dynamic shared memory: up to 512 threads x NARROW_SMEM_PER_THREAD.
+    CK(cudaFuncSetAttribute(k_narrow, cudaFuncAttributeMaxDynamicSharedMemorySize, int(512 * NARROW_SMEM_PER_THREAD)));
     // AG2D_SOLVER=grid forces the whole-grid solver (test hook for that variant).
     if (const char* v = std::getenv("AG2D_SOLVER")) {
         if (std::string(v) == "grid") dev.solveCluster = 1;
@@ -417,6 +417,15 @@ static DeviceInfo probe_device(int device)
     cache[device] = dev;
     return dev;
 }
+
+// A deferred body command (ObjectManager::ObjectCommand, SimulationImpl/ObjectManager.h:45): queued by destroy and the
+// setters in call order, applied at the start of the next step (Simulation::update -> flushCommands,
+// Simulation.cpp:39; ObjectManager::applyCommand, ObjectManager.cpp:662-790). Stale handles are dropped.
+struct BodyCommand {
+    int32_t kind;   // AG2D_COMMAND_*
+    uint64_t handle;
+    float a, b;
+};
 
 struct ag2d_world {
     ag2d_world_settings settings{};
@@ -429,8 +438,10 @@ struct ag2d_world {
     bool aabbValid = false;         // caabb holds the broad phase's AABBs (a step ran, or a state brought them)
     bool otherDirty = true;         // static + sleeping tree must be rebuilt
     uint64_t stepsTaken = 0;
+    std::vector<BodyCommand> commands;   // queued body commands, applied by flushCommands
 
     uint32_t nBodies = 0, nColliders = 0, nDynBody = 0, nDynCol = 0, nOther = 0, nStatic = 0;
+    uint32_t nDestroyed = 0;   // bodies removed by destroy commands (still in the arrays, in no list)
     uint32_t pairCap = 0, manifoldCap = 0, hashCap = 0;
     uint32_t lastManifolds = 0;
     uint32_t prevCount = 0;   // manifolds in prevManifolds (the warm-start source), as the host knows them
@@ -462,12 +473,12 @@ struct ag2d_world {
     DBuf<uint32_t> dynBody, dynCol, otherCol, flagA, flagB, flagC, offA, offB, offC, listCounts;
     // Trees and pairs.
     Tree dynTree, otherTree;
-    DBuf<uint32_t> qCounts, qOffsets;
-    DBuf<uint2> qStash;   // QUERY_STASH pairs per dynamic collider
+    DBuf<uint32_t> queryState;   // pair-query tile states ([dynamic colliders / 64 + 1]) and ticket counter
     DBuf<uint2> pairs;
     // Manifolds.
-    DBuf<Manifold> slots, manifolds, prevManifolds;
-    DBuf<uint32_t> hit, hitOffsets, nManifolds, nPrev;
+    DBuf<Manifold> manifolds, prevManifolds;
+    DBuf<uint32_t> nManifolds, nPrev;
+    DBuf<uint32_t> narrowState;   // narrow-phase tile states ([pairCap / 64 + 1]) and ticket counter
     DBuf<unsigned long long> hashKeys;
     DBuf<uint32_t> hashVals;
     // Colouring and solver.
@@ -495,6 +506,8 @@ struct ag2d_world {
     uint32_t nTeams = 0;
     uint32_t teamBlocks = 1;               // co-resident CTAs of the team solver at this shared-memory size
     uint32_t nBigTeams = 0, bigBodyCap = 0, bigBlocks = 1;   // worlds larger than a team, one CTA each
+    uint32_t bigThreads = BIG_TEAM_THREADS;                   // their CTA size (tunable: 256 or 512)
+    bool bigPipelined = false;                                 // their passes pipelined (tunable)
     cudaStream_t sideStream = nullptr;     // the big-world solver runs here, beside the small-team solver
     cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
     uint32_t queryThreads = 256;           // block sizes of the pair query and the narrow phase (tunable)
@@ -612,8 +625,7 @@ struct ag2d_world {
         dynColSimd.reserve(nmax);
         dynTree.reserve(nColliders, nWorlds);
         otherTree.reserve(nColliders, nWorlds);
-        qCounts.reserve(nColliders); qOffsets.reserve(nColliders);
-        qStash.reserve(size_t(std::max<uint32_t>(nColliders, 1)) * QUERY_STASH);
+        queryState.reserve(size_t(div_up(std::max<uint32_t>(nColliders, 1), 64)) + 1);
         bodyMax.reserve(nBodies);
         bodyMask.reserve(nBodies);
         ufParent.reserve(nBodies); ufFlag.reserve(nBodies); wakeIsland.reserve(nBodies);
@@ -874,6 +886,16 @@ struct ag2d_world {
         CK(cudaStreamSynchronize(stream));
     }
 
+    // Launch shape of the CTAs that solve worlds larger than a team: mode bit 0 = 256 threads (else 512), bit 1 =
+    // pipelined global-record passes.
+    uint32_t bigMode() const { return (bigThreads == 256 ? 1u : 0u) | (bigPipelined ? 2u : 0u); }
+    void setBigMode(uint32_t mode)
+    {
+        bigThreads = (mode & 1u) ? 256u : 512u;
+        bigPipelined = (mode & 2u) != 0;
+        if (nWorlds > 1) setTeams(teamColliders, teamThreads);
+    }
+
     // Solver teams: consecutive worlds packed while the team stays within 'colliders' colliders (a larger world is
     // a team of its own), scheduled largest first, each solved by one CTA of 'threads' threads.
     void setTeams(uint32_t colliders, uint32_t threads)
@@ -893,9 +915,9 @@ struct ag2d_world {
         };
         teamConsCap = consFit(teamBodyCap, 3 * colliders);
         int perSm = 0;
-        CK(team_solver_blocks_per_sm(teamThreads, teamBodyCap, teamConsCap, &perSm));
+        CK(team_solver_blocks_per_sm(teamThreads, false, teamBodyCap, teamConsCap, &perSm));
         teamBlocks = uint32_t(std::max(1, perSm) * dev.sms);
-        // Worlds above the team size are teams of their own ("big", solved by BIG_TEAM_THREADS-thread CTAs);
+        // Worlds above the team size are teams of their own ("big", solved by bigThreads-thread CTAs);
         // the others are packed, in order, into teams of up to 'colliders' colliders.
         std::vector<uint32_t> start{0};
         std::vector<uint32_t> big, small;
@@ -927,7 +949,7 @@ struct ag2d_world {
         bigConsCap = consFit(bigBodyCap, 3 * bigMax);
         bigBlocks = 1;
         if (nBigTeams) {
-            CK(team_solver_blocks_per_sm(BIG_TEAM_THREADS, bigBodyCap, bigConsCap, &perSm));
+            CK(team_solver_blocks_per_sm(bigThreads, bigPipelined, bigBodyCap, bigConsCap, &perSm));
             bigBlocks = uint32_t(std::max(1, perSm) * dev.sms);
         }
         std::vector<uint32_t> order(small);
@@ -1141,6 +1163,8 @@ struct ag2d_world {
         CK(cudaMallocHost(reinterpret_cast<void**>(&hCounters), sizeof(StepCounters)));
         std::memset(hCounters, 0, sizeof(StepCounters));
         dCounters.reserve(1);
+        scanner.status = &dCounters.p->status;
+        scanner.blocks = uint32_t(std::max(dev.sms, 1)) * (2048 / SCAN_THREADS);
         bar.reserve(2);
         nManifolds.reserve(1);
         nPrev.reserve(1);
@@ -1157,9 +1181,7 @@ struct ag2d_world {
         pairCap = pairCapNew;
         manifoldCap = manCapNew;
         pairs.reserve(pairCap);
-        slots.reserve(pairCap);
-        hit.reserve(pairCap);
-        hitOffsets.reserve(pairCap);
+        narrowState.reserve(size_t(div_up(pairCap, 64)) + 2);
         // Manifold arrays keep their contents (the previous step's manifolds are the warm-start source).
         auto grow_keep = [&](DBuf<Manifold>& b, uint32_t cap) {
             if (b.n >= cap && b.p) return;
@@ -1285,8 +1307,7 @@ struct ag2d_world {
         otherTree.reserve(nColliders, nWorlds);
         nCircles = uint32_t(cr.size()); nBoxes = uint32_t(bh.size()); nPolygons = uint32_t(po.size());
         nPolyVerts = uint32_t(pv.size()); nMaterialRows = uint32_t(mats.size());
-        qCounts.reserve(nColliders); qOffsets.reserve(nColliders);
-        qStash.reserve(size_t(std::max<uint32_t>(nColliders, 1)) * QUERY_STASH);
+        queryState.reserve(size_t(div_up(std::max<uint32_t>(nColliders, 1), 64)) + 1);
         bodyMax.reserve(nBodies);
         bodyMask.reserve(nBodies);
         ufParent.reserve(nBodies); ufFlag.reserve(nBodies); wakeIsland.reserve(nBodies);
@@ -1575,14 +1596,13 @@ struct ag2d_world {
             return;
         }
         pbegin(4);
-        launches += 2 + scanLaunches(nDynCol) + 1;
+        launches += 1;
         const uint32_t gq = gridFor(nDynCol, queryThreads);
-        k_query_stash<<<gq, queryThreads, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qCounts.p, qStash.p,
-                                                  &dCounters.p->status);
-        CK(cudaGetLastError());
-        scanner.run(qCounts.p, qOffsets.p, nDynCol, total, s);
-        k_query_emit<<<gq, queryThreads, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, qCounts.p, qOffsets.p,
-                                                 qStash.p, pairs.p, pairCap, &dCounters.p->status);
+        const uint32_t tiles = div_up(nDynCol, queryThreads);
+        queryState.reserve(size_t(tiles) + 1);
+        CK(cudaMemsetAsync(queryState.p, 0, (size_t(tiles) + 1) * sizeof(uint32_t), s));
+        k_query<<<gq, queryThreads, 0, s>>>(dynTree.view(), otherTree.view(), cbody.p, pairs.p, pairCap, total,
+                                            &dCounters.p->status, queryState.p, queryState.p + tiles);
         CK(cudaGetLastError());
         pend(4);
     }
@@ -1591,21 +1611,18 @@ struct ag2d_world {
     {
         const cudaStream_t s = stream;
         const uint32_t* nPairs = &dCounters.p->pairs;
-        const uint32_t g = gridFor(pairCap);
+        // Grid sized for the capacity, work bounded by the device-side pair count; the manifolds are compacted in
+        // the same kernel.
         const uint32_t gn = gridFor(pairCap, narrowThreads);
+        const uint32_t tilesCap = std::max<uint32_t>(div_up(pairCap, narrowThreads), 1);
         pbegin(5);
-        k_narrow<<<gn, narrowThreads, narrowThreads * NARROW_SMEM_PER_THREAD, s>>>(view(), pairs.p, nPairs, pairCap,
-                                                                                slots.p, hit.p);
+        CK(cudaMemsetAsync(narrowState.p, 0, (size_t(tilesCap) + 1) * sizeof(uint32_t), s));
+        k_narrow<<<gn, narrowThreads, narrowThreads * NARROW_SMEM_PER_THREAD, s>>>(
+            view(), pairs.p, nPairs, pairCap, manifolds.p, manifoldCap, nManifolds.p, dCounters.p, narrowState.p,
+            narrowState.p + tilesCap);
         CK(cudaGetLastError());
         pend(5);
-        pbegin(6);
-        launches += 1 + scanLaunches(pairCap) + 1 + 2;
-        // Grid sized for the capacity, work bounded by the device-side pair count.
-        scanner.run(hit.p, hitOffsets.p, pairCap, nullptr, s, 0, nPairs);
-        k_compact_manifolds<<<g, 256, 0, s>>>(slots.p, hit.p, hitOffsets.p, nPairs, pairCap, manifolds.p,
-                                               manifoldCap, nManifolds.p, dCounters.p);
-        CK(cudaGetLastError());
-        pend(6);
+        launches += 1;
         if (!warm) return;
         pbegin(7);
         // Warm start from the previous step's manifolds.
@@ -1663,14 +1680,15 @@ struct ag2d_world {
                 CK(cudaStreamWaitEvent(sideStream, forkEvent, 0));
                 const TeamLaunch big{w, mm, manSeg.p, teamWorld.p, teamOrder.p + nTeams, nBigTeams, bigBodyCap,
                                      bigConsCap, scratch, vi, pi, nextWorld.p + 1, ctr};
-                CK(launch_color_solve_teams(BIG_TEAM_THREADS, std::min(nBigTeams, bigBlocks), sideStream, big));
+                CK(launch_color_solve_teams(bigThreads, bigPipelined, std::min(nBigTeams, bigBlocks), sideStream,
+                                            big));
                 launches++;
             }
             if (nTeams) {
                 const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(nTeams, teamBlocks));
                 const TeamLaunch args{w, mm, manSeg.p, teamWorld.p, teamOrder.p, nTeams, teamBodyCap, teamConsCap,
                                       scratch, vi, pi, nextWorld.p, ctr};
-                CK(launch_color_solve_teams(teamThreads, grid, s, args));
+                CK(launch_color_solve_teams(teamThreads, false, grid, s, args));
             }
             if (nBigTeams) {
                 CK(cudaEventRecord(joinEvent, sideStream));
@@ -1728,17 +1746,7 @@ struct ag2d_world {
         pcollect();
     }
 
-    static uint32_t scanLaunches(uint32_t n)
-    {
-        uint32_t k = 0;
-        while (true) {
-            const uint32_t nb = std::max<uint32_t>(div_up(n, SCAN_TILE), 1);
-            k += nb > 1 ? 2 : 1;
-            if (nb <= 1) break;
-            n = nb;
-        }
-        return k;
-    }
+    static uint32_t scanLaunches(uint32_t) { return 1; }   // one k_scan per scan
 
     // Device milliseconds per step of one timed phase over 'steps' real steps.
     double timePhase(int phase, uint32_t steps)
@@ -1784,6 +1792,7 @@ struct ag2d_world {
         };
         out.team_colliders = 0;
         out.team_threads = 0;
+        out.big_team_mode = bigMode();
         out.team_cons_on_chip = consOnChip ? 1 : 0;
         out.solve_ms = 0.0f;
         if (nWorlds > 1) {
@@ -1805,6 +1814,12 @@ struct ag2d_world {
             out.team_threads = r.first & 0x7FFF;
             out.team_cons_on_chip = (r.first >> 15) & 1;
             out.solve_ms = float(r.second);
+            // Worlds larger than a team: CTA size and pipelined passes (modes 0-3, big_team_mode).
+            if (nBigTeams) {
+                const auto rb = pick(10, {0u, 1u, 2u, 3u}, [&](uint32_t mode) { setBigMode(mode); });
+                out.big_team_mode = rb.first;
+                out.solve_ms = float(rb.second);
+            }
         }
         const auto q = pick(4, {64, 128, 256}, [&](uint32_t t) { queryThreads = t; });
         out.query_threads = q.first;
@@ -1814,6 +1829,107 @@ struct ag2d_world {
         out.narrow_ms = float(nr.second);
         profiling = wasProfiling;
         for (int p = 0; p < NPHASE; p++) { phaseMs[p] = 0.0; phaseCalls[p] = 0; evPending[p] = false; }
+    }
+
+    // Applies the queued body commands to the device state, in call order, as ObjectManager::applyCommand does to
+    // the reference's SoA (ObjectManager.cpp:662-790): every command but a stale one wakes the body's sleeping
+    // island first (wakeBody, :1425-1436); a position is given for the body origin and moves the centre of mass
+    // with the rotated local centre of mass; a rotation is wrapped into [0, 2 pi) with std::cos / std::sin of it
+    // stored; a mass of 0 makes the body static (velocities zeroed), a positive one scales the inertia by
+    // new / old mass; an inertia is ignored on a static body; a destroyed body leaves every work list and tree and
+    // its handle goes stale. Body dense indices do not move (the reference's group moves are state flags here).
+    // The next step then rebuilds the work lists and the static tree and poses every collider (spatialDirty).
+    void flushCommands()
+    {
+        if (commands.empty()) return;
+        if (nWorlds > 1) { commands.clear(); throw ApiError(AG2D_ERR_UNSUPPORTED, "body commands are per world"); }
+        ensureUploaded();
+        const cudaStream_t s = stream;
+        std::vector<float4> vel = download(bvel.p, nBodies, s), pos = download(bpos.p, nBodies, s);
+        std::vector<float2> rot = download(brot.p, nBodies, s);
+        std::vector<uint8_t> state = download(bstate.p, nBodies, s);
+        std::vector<float> timer = download(sleepTimer.p, nBodies, s), wraps = download(wrapCount.p, nBodies, s);
+        const std::vector<uint32_t> island = download(sleepIsland.p, nBodies, s);
+        HostObjects& o = objects;
+        auto wake = [&](uint32_t b) {   // the body's whole sleeping island (k_wake_apply's rule)
+            if (state[b] != STATE_SLEEPING) return;
+            const uint32_t root = island[b];
+            for (uint32_t i = 0; i < nBodies; i++)
+                if (state[i] == STATE_SLEEPING && island[i] == root) { state[i] = STATE_DYNAMIC; timer[i] = 0.0f; }
+        };
+        for (const BodyCommand& c : commands) {
+            const uint32_t b = o.indexOf(c.handle);
+            if (b >= nBodies || b >= o.bodies.size() || state[b] == STATE_DESTROYED) continue;
+            HBody& hb = o.bodies[b];
+            wake(b);
+            switch (c.kind) {
+            case AG2D_COMMAND_DESTROY:
+                state[b] = STATE_DESTROYED;
+                o.slotGeneration[uint32_t(c.handle & 0xFFFFFFFFu)]++;
+                break;
+            case AG2D_COMMAND_POSITION: {
+                const float r = pos[b].z, cosR = std::cos(r), sinR = std::sin(r);
+                pos[b].x = c.a + cosR * hb.lcomX - sinR * hb.lcomY;
+                pos[b].y = c.b + sinR * hb.lcomX + cosR * hb.lcomY;
+                break;
+            }
+            case AG2D_COMMAND_ROTATION: {
+                const float twoPi = float(3.14159265358979323846 * 2.0);
+                float r = std::fmod(c.a, twoPi);
+                if (r < 0.0f) r += twoPi;
+                pos[b].z = r;
+                rot[b] = make_float2(std::cos(r), std::sin(r));
+                wraps[b] = 0.0f;
+                break;
+            }
+            case AG2D_COMMAND_VELOCITY: vel[b].x = c.a; vel[b].y = c.b; break;
+            case AG2D_COMMAND_ANGULAR_VELOCITY: vel[b].z = c.a; break;
+            case AG2D_COMMAND_MASS: {   // applyBodyMass (ObjectManager.cpp:867-905)
+                const float newMass = std::fmax(0.0f, c.a);
+                const float oldMass = hb.mass;
+                if (newMass > 0.0f) {
+                    float inertia = hb.inertia;
+                    if (oldMass > 0.0f) inertia *= newMass / oldMass;
+                    hb.mass = newMass;
+                    hb.invMass = 1.0f / newMass;
+                    hb.inertia = inertia;
+                    hb.invInertia = inertia > 0.0f ? 1.0f / inertia : 0.0f;
+                    if (state[b] == STATE_STATIC) { state[b] = STATE_DYNAMIC; timer[b] = 0.0f; }
+                } else {
+                    hb.mass = 0.0f; hb.invMass = 0.0f; hb.inertia = 0.0f; hb.invInertia = 0.0f;
+                    vel[b].x = 0.0f; vel[b].y = 0.0f; vel[b].z = 0.0f;
+                    state[b] = STATE_STATIC;
+                }
+                vel[b].w = hb.invMass;
+                pos[b].w = hb.invInertia;
+                break;
+            }
+            case AG2D_COMMAND_INERTIA: {
+                if (hb.invMass == 0.0f) break;
+                const float inertia = std::fmax(0.0f, c.a);
+                hb.inertia = inertia;
+                hb.invInertia = inertia > 0.0f ? 1.0f / inertia : 0.0f;
+                pos[b].w = hb.invInertia;
+                break;
+            }
+            default: break;
+            }
+        }
+        commands.clear();
+        if (nBodies) {
+            CK(cudaMemcpyAsync(bvel.p, vel.data(), nBodies * sizeof(float4), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(bpos.p, pos.data(), nBodies * sizeof(float4), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(brot.p, rot.data(), nBodies * sizeof(float2), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(bstate.p, state.data(), nBodies, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(sleepTimer.p, timer.data(), nBodies * sizeof(float), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(wrapCount.p, wraps.data(), nBodies * sizeof(float), cudaMemcpyHostToDevice, s));
+            CK(cudaStreamSynchronize(s));
+        }
+        nStatic = uint32_t(std::count(state.begin(), state.end(), uint8_t(STATE_STATIC)));
+        nDestroyed = uint32_t(std::count(state.begin(), state.end(), uint8_t(STATE_DESTROYED)));
+        listsDirty = true;
+        otherDirty = true;
+        fullPose = true;
     }
 
     // One fixed step (Simulation::physicsStep order, Simulation.cpp:255-351).
@@ -1826,6 +1942,7 @@ struct ag2d_world {
             ~HostTimer() { acc += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); }
         } hostTimer{hostMs, tStart};
         ensureUploaded();
+        flushCommands();
         for (int attempt = 0; attempt < 8; attempt++) {
             if (attempt > 0) retries++;
             if (listsDirty) rebuildLists();
@@ -2024,6 +2141,60 @@ int32_t ag2d_world_add_polygon(ag2d_world* world, const ag2d_body_desc* body, co
     });
 }
 
+int32_t ag2d_world_add_capsule(ag2d_world* world, const ag2d_body_desc* body, float length, float radius,
+                               uint64_t* out_handle)
+{
+    return guarded([&] {
+        if (!world || !body) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        pull_state(world);
+        float d[7];
+        body_desc(body, d);
+        uint64_t h = 0;
+        std::string err;
+        if (!world->objects.addCapsule(d, body->material, length, radius, h, err)) throw ApiError(AG2D_ERR_INVALID_ARG, err);
+        world->hostDirty = true;
+        if (out_handle) *out_handle = h;
+    });
+}
+
+int32_t ag2d_world_create_body(ag2d_world* world, const ag2d_body_desc* body, float inertia, float com_x,
+                               float com_y, uint64_t* out_handle)
+{
+    return guarded([&] {
+        if (!world || !body) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        pull_state(world);
+        float d[7];
+        body_desc(body, d);
+        uint64_t h = 0;
+        std::string err;
+        if (!world->objects.addBody(d, inertia, com_x, com_y, h, err)) throw ApiError(AG2D_ERR_INVALID_ARG, err);
+        world->hostDirty = true;
+        if (out_handle) *out_handle = h;
+    });
+}
+
+int32_t ag2d_world_add_collider(ag2d_world* world, uint64_t body, int32_t shape, float local_x, float local_y,
+                                float local_rotation, uint32_t material, const float* params, const float* xy,
+                                uint32_t n_vertices, uint32_t* out_collider)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        if (shape < 0 || shape > 3) throw ApiError(AG2D_ERR_INVALID_ARG, "unknown shape kind");
+        if (shape != SHAPE_POLYGON && !params) throw ApiError(AG2D_ERR_INVALID_ARG, "null shape parameters");
+        const uint32_t b = world->objects.indexOf(body);
+        if (b == 0xFFFFFFFFu) throw ApiError(AG2D_ERR_INVALID_ARG, "stale body handle");
+        pull_state(world);
+        uint32_t c = 0;
+        std::string err;
+        if (!world->objects.addCollider(b, uint32_t(shape), local_x, local_y, local_rotation, material, params, xy,
+                                        n_vertices, c, err))
+            throw ApiError(err.find("not convex") != std::string::npos || err.find("16") != std::string::npos
+                               ? AG2D_ERR_UNSUPPORTED : AG2D_ERR_INVALID_ARG, err);
+        world->hostDirty = true;
+        if (out_collider) *out_collider = c;
+    });
+}
+
 int32_t ag2d_world_add_bodies(ag2d_world* world, uint32_t count, const ag2d_body_desc* bodies,
                               const uint32_t* kinds, const float* params, const uint32_t* poly_offsets,
                               const uint32_t* poly_counts, const float* poly_xy, uint64_t* out_handles)
@@ -2044,6 +2215,9 @@ int32_t ag2d_world_add_bodies(ag2d_world* world, uint32_t count, const ag2d_body
             case SHAPE_BOX:
                 ok = world->objects.addBox(d, bodies[i].material, params[2 * i], params[2 * i + 1], h, err);
                 break;
+            case SHAPE_CAPSULE:
+                ok = world->objects.addCapsule(d, bodies[i].material, params[2 * i], params[2 * i + 1], h, err);
+                break;
             case SHAPE_POLYGON:
                 if (!poly_offsets || !poly_counts || !poly_xy) { err = "polygon without vertex arrays"; break; }
                 ok = world->objects.addPolygon(d, bodies[i].material, poly_xy + 2 * size_t(poly_offsets[i]),
@@ -2063,6 +2237,54 @@ int32_t ag2d_world_add_bodies(ag2d_world* world, uint32_t count, const ag2d_body
 uint32_t ag2d_world_body_index(ag2d_world* world, uint64_t handle)
 {
     return world ? world->objects.indexOf(handle) : 0xFFFFFFFFu;
+}
+
+static int32_t queue_command(ag2d_world* world, int32_t kind, uint64_t handle, float a, float b)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        if (world->nWorlds > 1) throw ApiError(AG2D_ERR_UNSUPPORTED, "body commands are per world");
+        world->commands.push_back(BodyCommand{kind, handle, a, b});
+    });
+}
+
+int32_t ag2d_world_destroy_body(ag2d_world* world, uint64_t body)
+{
+    return queue_command(world, AG2D_COMMAND_DESTROY, body, 0.0f, 0.0f);
+}
+int32_t ag2d_world_set_body_position(ag2d_world* world, uint64_t body, float x, float y)
+{
+    return queue_command(world, AG2D_COMMAND_POSITION, body, x, y);
+}
+int32_t ag2d_world_set_body_rotation(ag2d_world* world, uint64_t body, float rotation)
+{
+    return queue_command(world, AG2D_COMMAND_ROTATION, body, rotation, 0.0f);
+}
+int32_t ag2d_world_set_body_velocity(ag2d_world* world, uint64_t body, float vx, float vy)
+{
+    return queue_command(world, AG2D_COMMAND_VELOCITY, body, vx, vy);
+}
+int32_t ag2d_world_set_body_angular_velocity(ag2d_world* world, uint64_t body, float angular_velocity)
+{
+    return queue_command(world, AG2D_COMMAND_ANGULAR_VELOCITY, body, angular_velocity, 0.0f);
+}
+int32_t ag2d_world_set_body_mass(ag2d_world* world, uint64_t body, float mass)
+{
+    return queue_command(world, AG2D_COMMAND_MASS, body, mass, 0.0f);
+}
+int32_t ag2d_world_set_body_inertia(ag2d_world* world, uint64_t body, float inertia)
+{
+    return queue_command(world, AG2D_COMMAND_INERTIA, body, inertia, 0.0f);
+}
+
+int32_t ag2d_world_flush_commands(ag2d_world* world)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        if (world->commands.empty()) return;
+        CK(cudaSetDevice(world->settings.device));
+        world->flushCommands();
+    });
 }
 
 int32_t ag2d_world_load_state(ag2d_world* world, const ag2d_state_desc* st)
@@ -2102,15 +2324,23 @@ int32_t ag2d_world_load_state(ag2d_world* world, const ag2d_state_desc* st)
         }
         std::vector<uint32_t> cb(nc), cs(nc), cm(nc);
         std::vector<float4> co(nc);
+        const uint32_t nCaps = st->capsule_half_length && st->capsule_radius ? st->n_capsules : 0u;
         for (uint32_t i = 0; i < nc; i++) {
             cb[i] = st->col_body[i];
-            cs[i] = (st->col_shape_type[i] << 30) | st->col_shape_index[i];
+            const uint32_t type = st->col_shape_type[i];
+            if (type > SHAPE_CAPSULE || (type == SHAPE_CAPSULE && st->col_shape_index[i] >= nCaps))
+                throw ApiError(AG2D_ERR_INVALID_ARG, "collider " + std::to_string(i) + ": bad shape");
+            // Capsules follow the boxes in the shared parameter table.
+            const uint32_t idx = st->col_shape_index[i] + (type == SHAPE_CAPSULE ? st->n_boxes : 0u);
+            cs[i] = (type << 30) | idx;
             cm[i] = st->col_material[i];
             co[i] = make_float4(st->col_com_offset_x[i], st->col_com_offset_y[i], st->col_local_rotation[i], 0.0f);
         }
         std::vector<float> cr(st->circle_radius, st->circle_radius + st->n_circles);
-        std::vector<float2> bh(st->n_boxes);
+        std::vector<float2> bh(size_t(st->n_boxes) + nCaps);
         for (uint32_t i = 0; i < st->n_boxes; i++) bh[i] = make_float2(st->box_half_width[i], st->box_half_height[i]);
+        for (uint32_t i = 0; i < nCaps; i++)
+            bh[st->n_boxes + i] = make_float2(st->capsule_half_length[i], st->capsule_radius[i]);
         std::vector<uint32_t> po(st->n_polygons), pc(st->n_polygons);
         uint32_t total = 0;
         for (uint32_t i = 0; i < st->n_polygons; i++) { po[i] = total; pc[i] = st->poly_count[i]; total += pc[i]; }
@@ -2165,7 +2395,7 @@ int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out)
         const StepCounters& c = world->hCounters ? *world->hCounters : none;
         out->status = c.status; out->pairs = c.pairs; out->manifolds = c.manifolds; out->colors = c.colors;
         out->woke = c.woke; out->slept = c.slept; out->warm_hits = c.warmHits;
-        out->sleeping = world->nBodies - world->nDynBody - world->nStatic;
+        out->sleeping = world->nBodies - world->nDynBody - world->nStatic - world->nDestroyed;
         out->ccd_hits = c.ccdHits;
         out->reserved = 0;
         out->steps = world->stepsTaken;
@@ -2209,6 +2439,9 @@ int32_t ag2d_world_set_tuning(ag2d_world* world, const ag2d_tuning* tuning)
         world->queryThreads = t.query_threads;
         world->narrowThreads = t.narrow_threads;
         world->consOnChip = t.team_cons_on_chip != 0;
+        if (t.big_team_mode > 3) throw ApiError(AG2D_ERR_INVALID_ARG, "big_team_mode out of range");
+        world->bigThreads = (t.big_team_mode & 1u) ? 256u : 512u;
+        world->bigPipelined = (t.big_team_mode & 2u) != 0;
         if (t.team_colliders) {
             world->teamColliders = t.team_colliders;
             world->teamThreads = t.team_threads;
@@ -2313,6 +2546,7 @@ static bool field_spec(const ag2d_world& w, int32_t field, FieldSpec& f)
     case AG2D_COL_AABB_MIN_Y: c4(w.caabb.p, 1); f.perCollider = true; break;
     case AG2D_COL_AABB_MAX_X: c4(w.caabb.p, 2); f.perCollider = true; break;
     case AG2D_COL_AABB_MAX_Y: c4(w.caabb.p, 3); f.perCollider = true; break;
+    case AG2D_COL_BODY: f.src = w.cbody.p; f.kind = EXTRACT_ISLAND; f.perCollider = true; break;   // biased like ids
     default: return false;
     }
     return true;
@@ -2399,14 +2633,6 @@ static void read_async(ag2d_world& w, const FieldSpec& f, uint32_t lo, uint32_t 
     a.used = true;
 }
 
-template <class T>
-static std::vector<T> download(const T* p, size_t n, cudaStream_t s)
-{
-    std::vector<T> v(n);
-    if (n) CK(cudaMemcpyAsync(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    return v;
-}
 
 // The phase-tap fields (Morton order, pairs, manifolds, solve order, colour starts): element count from the device
 // counters where the count lives there. With sizeOnly the bytes are counted but not read.

@@ -300,4 +300,108 @@ bool HostObjects::addPolygon(const float* d, uint32_t material, const float* xy,
     return true;
 }
 
+bool HostObjects::addCapsule(const float* d, uint32_t material, float length, float radius, uint64_t& handle,
+                             std::string& err)
+{
+    if (!(length >= 0.0f && radius >= 0.0f)) { err = "capsule length and radius must be >= 0"; return false; }
+    if (material >= materialCount()) material = 0;
+    // ObjectManager::createCapsule (ObjectManager.cpp:351-388) without endpoints; calculateCapsuleInertia
+    // (PhysicsGeometry.cpp:87-113) about the core's centre (centre of mass at the body origin).
+    const float mass = std::fmax(0.0f, d[6]);
+    const float len = std::fmax(0.0f, length), r = std::fmax(0.0f, radius);
+    const float pi = float(3.14159265358979323846);
+    const float rectArea = len * 2.0f * r;
+    const float circleArea = pi * r * r;
+    const float totalArea = rectArea + circleArea;
+    const float rectMass = mass * rectArea / totalArea;
+    const float capMass = mass * circleArea / totalArea;
+    const float diameter = 2.0f * r;
+    const float rectInertia = rectMass * (len * len + diameter * diameter) / 12.0f;
+    const float dist = 4.0f * r / (3.0f * pi);
+    const float capInertia = capMass * (0.5f * r * r + 0.25f * len * len + len * dist);
+    const float inertia = rectInertia + capInertia + mass * 0.0f;
+    const float invMass = mass == 0.0f ? 0.0f : 1.0f / mass;
+    const float invInertia = inertia == 0.0f ? 0.0f : 1.0f / inertia;
+    const uint32_t b = appendBody(d[0], d[1], d[3], d[4], d[2], d[5], mass, invMass, inertia, invInertia, 0.0f, 0.0f);
+    const uint32_t slot = bodies[b].handleSlot;
+    // createCapsuleCollider (ObjectManager.cpp:197-231): half length, radius; extents (radius, half length + radius).
+    const float half = len * 0.5f;
+    boxHalfW.push_back(half);
+    boxHalfH.push_back(r);
+    appendCollider(b, 0.0f, 0.0f, 0.0f, material, 3u, uint32_t(boxHalfW.size() - 1), r, half + r);
+    handle = (uint64_t(slotGeneration[slot]) << 32) | slot;
+    return true;
+}
+
+bool HostObjects::addBody(const float* d, float inertiaIn, float comX, float comY, uint64_t& handle, std::string& err)
+{
+    (void)err;
+    const float mass = std::fmax(0.0f, d[6]);
+    const float inertia = std::fmax(0.0f, inertiaIn);
+    const float invMass = mass == 0.0f ? 0.0f : 1.0f / mass;
+    const float invInertia = inertia == 0.0f ? 0.0f : 1.0f / inertia;
+    const uint32_t b = appendBody(d[0], d[1], d[3], d[4], d[2], d[5], mass, invMass, inertia, invInertia, comX, comY);
+    const uint32_t slot = bodies[b].handleSlot;
+    handle = (uint64_t(slotGeneration[slot]) << 32) | slot;
+    return true;
+}
+
+bool HostObjects::addCollider(uint32_t body, uint32_t type, float locX, float locY, float localRot, uint32_t material,
+                              const float* p, const float* xy, uint32_t n, uint32_t& collider, std::string& err)
+{
+    if (body >= bodies.size()) { err = "stale body handle"; return false; }
+    if (material >= materialCount()) material = 0;
+    switch (type) {
+    case 0: {   // createCircleCollider (:90-112)
+        const float r = std::fmax(0.0f, p[0]);
+        circleRadius.push_back(r);
+        collider = appendCollider(body, locX, locY, localRot, material, 0u, uint32_t(circleRadius.size() - 1), r, r);
+        return true;
+    }
+    case 1: {   // createBoxCollider (:114-139)
+        const float w = std::fmax(0.0f, p[0]), h = std::fmax(0.0f, p[1]);
+        const float hw = w * 0.5f, hh = h * 0.5f;
+        boxHalfW.push_back(hw);
+        boxHalfH.push_back(hh);
+        collider = appendCollider(body, locX, locY, localRot, material, 1u, uint32_t(boxHalfW.size() - 1),
+                                  std::fmin(hw, hh), std::fmax(hw, hh));
+        return true;
+    }
+    case 3: {   // createCapsuleCollider (:197-231)
+        const float len = std::fmax(0.0f, p[0]), r = std::fmax(0.0f, p[1]);
+        const float half = len * 0.5f;
+        boxHalfW.push_back(half);
+        boxHalfH.push_back(r);
+        collider = appendCollider(body, locX, locY, localRot, material, 3u, uint32_t(boxHalfW.size() - 1), r, half + r);
+        return true;
+    }
+    case 2: {   // createPolygonCollider for a convex outline (:141-195) via createConvexPolygonColliderInternal
+        if (!xy || n < 3) { err = "polygon needs at least 3 vertices"; return false; }
+        std::vector<float> outline;
+        if (!prepare_outline(xy, n, outline, err)) return false;
+        float unused = 0, pcx = 0, pcy = 0;
+        if (!polygon_inertia(1.0f, outline, unused, pcx, pcy)) { err = "polygon outline is degenerate"; return false; }
+        for (size_t i = 0; i < outline.size() / 2; i++) { outline[2 * i] -= pcx; outline[2 * i + 1] -= pcy; }
+        const float cosL = std::cos(localRot), sinL = std::sin(localRot);
+        const float offX = locX + (cosL * pcx - sinL * pcy);
+        const float offY = locY + (sinL * pcx + cosL * pcy);
+        HPolygon poly;
+        poly.verts = outline;
+        poly.normals = polygon_normals(outline);
+        float inR = FLT_MAX, outR2 = 0.0f;
+        for (size_t i = 0; i < outline.size() / 2; i++) {
+            const float vx = poly.verts[2 * i], vy = poly.verts[2 * i + 1];
+            inR = std::fmin(inR, poly.normals[2 * i] * vx + poly.normals[2 * i + 1] * vy);
+            outR2 = std::fmax(outR2, vx * vx + vy * vy);
+        }
+        inR = std::fmax(inR, 0.0f);
+        polygons.push_back(std::move(poly));
+        collider = appendCollider(body, offX, offY, localRot, material, 2u, uint32_t(polygons.size() - 1), inR,
+                                  std::sqrt(outR2));
+        return true;
+    }
+    default: err = "unknown shape kind"; return false;
+    }
+}
+
 }  // namespace ag2d

@@ -57,7 +57,7 @@ public:
     std::vector<HBody> bodies;
     std::vector<HCollider> colliders;
     std::vector<float> circleRadius;
-    std::vector<float> boxHalfW, boxHalfH;
+    std::vector<float> boxHalfW, boxHalfH;   // boxes' half extents; capsules share the table: half length, radius
     std::vector<HPolygon> polygons;
     std::vector<float> materials;   // 3 per material
     Groups bodyGroups, colGroups;
@@ -83,6 +83,17 @@ public:
     bool addBox(const float* desc, uint32_t material, float width, float height, uint64_t& handle, std::string& err);
     bool addPolygon(const float* desc, uint32_t material, const float* xy, uint32_t n, uint64_t& handle,
                     std::string& err);
+    bool addCapsule(const float* desc, uint32_t material, float length, float radius, uint64_t& handle,
+                    std::string& err);
+    // ObjectManager::createBody (ObjectManager.cpp:71-88): a body with explicit mass, inertia and local centre of
+    // mass and no collider yet.
+    bool addBody(const float* desc, float inertia, float comX, float comY, uint64_t& handle, std::string& err);
+    // ObjectManager::create{Circle,Box,Polygon,Capsule}Collider (ObjectManager.cpp:90-231): a collider on an
+    // existing body, at a local offset and rotation; p holds radius / (width, height) / (length, radius). Polygons
+    // are convex outlines (xy, n), recentred on their centroid with the shift added to the offset. Returns the
+    // collider's dense index.
+    bool addCollider(uint32_t body, uint32_t type, float locX, float locY, float localRot, uint32_t material,
+                     const float* p, const float* xy, uint32_t n, uint32_t& collider, std::string& err);
 
     uint32_t indexOf(uint64_t handle) const
     {

@@ -21,6 +21,9 @@ __device__ __forceinline__ ColliderView collider_view(const DeviceWorld& w, uint
     } else if (v.type == SHAPE_BOX) {
         const float2 h = w.boxHalf[si];
         v.hw = h.x; v.hh = h.y;
+    } else if (v.type == SHAPE_CAPSULE) {
+        const float2 h = w.boxHalf[si];   // capsules share the table: (half length, radius)
+        v.hw = h.x; v.r = h.y;
     } else {
         const uint32_t off = w.polyOffset[si];
         v.verts = w.polyVerts + off;
@@ -46,25 +49,48 @@ __device__ __forceinline__ void write_slot(const Contact& ct, uint32_t a, uint32
     *slot = m;
 }
 
-// Each warp takes 32 consecutive pairs. Pairs of other shape types run one per lane; then the warp's
-// polygon-polygon pairs run four at a time, one per group of NARROW_GROUP lanes (collide_polygon_polygon_group).
-// Launched with a multiple of 32 threads per block and NARROW_SMEM_PER_THREAD bytes of dynamic shared memory per
-// thread (each group's vertex tiles).
+// Narrow phase with the manifold compaction fused in. Blocks take tiles of blockDim.x consecutive pairs in ticket
+// order (tileState and the ticket counter zeroed before the launch); in a tile each warp takes 32 pairs, one per
+// lane. Pairs of other shape types run one per lane; then the warp's polygon-polygon pairs run four at a time, one
+// per group of NARROW_GROUP lanes (collide_polygon_polygon_group). Each pair's manifold goes to its slot in shared
+// memory; the tile's hits are then counted (warp ballots, then a scan of the warps' counts), its output offset
+// comes from the decoupled look-back over the preceding tiles, and the hit pairs' manifolds are copied straight to
+// their places: manifolds come out in pair order. The last tile writes the manifold count. Launched with a
+// multiple of 32 threads (at most 1024) and NARROW_SMEM_PER_THREAD bytes of dynamic shared memory per thread.
 __global__ void k_narrow(DeviceWorld w, const uint2* __restrict__ pairs, const uint32_t* __restrict__ nPairs,
-                         uint32_t pairCap, Manifold* __restrict__ slots, uint32_t* __restrict__ hit)
+                         uint32_t pairCap, Manifold* __restrict__ out, uint32_t manifoldCap,
+                         uint32_t* __restrict__ nOut, StepCounters* counters, uint32_t* __restrict__ tileState,
+                         uint32_t* __restrict__ tileCounter)
 {
-    extern __shared__ V2 tiles[];   // per group: A's vertices, then B's (in A's frame)
+    extern __shared__ __align__(16) unsigned char narrowSmem[];
+    // [blockDim] manifold slots, [blockDim] hit flags, then per group A's vertices and B's (in A's frame).
+    Manifold* const slot = reinterpret_cast<Manifold*>(narrowSmem);
+    uint32_t* const hitS = reinterpret_cast<uint32_t*>(narrowSmem + blockDim.x * sizeof(Manifold));
+    V2* const tiles = reinterpret_cast<V2*>(narrowSmem + blockDim.x * (sizeof(Manifold) + sizeof(uint32_t)));
+    __shared__ uint32_t warpBase[32];
+    __shared__ uint32_t tileSlot, tileBase;
     const uint32_t n = min(*nPairs, pairCap);
-    const uint32_t lane = threadIdx.x & 31, group = lane / NARROW_GROUP, gl = lane % NARROW_GROUP;
+    if (n == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) { *nOut = 0u; counters->manifolds = 0u; }
+        return;
+    }
+    const uint32_t tiles_n = (n + blockDim.x - 1) / blockDim.x;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
+    const uint32_t group = lane / NARROW_GROUP, gl = lane % NARROW_GROUP;
     const uint32_t gmask = ((1u << NARROW_GROUP) - 1u) << (group * NARROW_GROUP);
-    V2* sA = tiles + (threadIdx.x / NARROW_GROUP) * 2 * MAX_POLYGON_VERTICES;
-    V2* sB = sA + MAX_POLYGON_VERTICES;
-    const uint32_t warps = gridDim.x * (blockDim.x / 32);
-    for (uint32_t tile = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; tile * 32u < n; tile += warps) {
-        const uint32_t p = tile * 32u + lane;
+    V2* const sA = tiles + (threadIdx.x / NARROW_GROUP) * 2 * MAX_POLYGON_VERTICES;
+    V2* const sB = sA + MAX_POLYGON_VERTICES;
+    const uint32_t warpFirst = warp * 32;
+    while (true) {
+        if (threadIdx.x == 0) tileSlot = atomicAdd(tileCounter, 1u);
+        __syncthreads();
+        const uint32_t tile = tileSlot;
+        if (tile >= tiles_n) return;
+        const uint32_t p = tile * blockDim.x + threadIdx.x;
         const bool valid = p < n;
         uint32_t a = 0, b = 0;
         bool pp = false;
+        hitS[threadIdx.x] = 0u;
         if (valid) {
             a = pairs[p].x;
             b = pairs[p].y;
@@ -74,49 +100,73 @@ __global__ void k_narrow(DeviceWorld w, const uint2* __restrict__ pairs, const u
             if (!pp) {
                 const ColliderView A = collider_view(w, a), B = collider_view(w, b);
                 Contact ct;
-                const bool h = collide(A, B, ct);
-                hit[p] = h ? 1u : 0u;
-                if (h) write_slot(ct, a, b, slots + p);
+                if (collide(A, B, ct)) {
+                    hitS[threadIdx.x] = 1u;
+                    write_slot(ct, a, b, slot + threadIdx.x);
+                }
             }
         }
         uint32_t todo = __ballot_sync(0xffffffffu, pp);
         while (todo) {
-            // Group g takes the g-th remaining polygon-polygon lane.
+            // Group g takes the g-th remaining polygon-polygon lane; its leader writes that pair's slot and flag.
             uint32_t pick = todo;
             for (uint32_t k = 0; k < group && pick; k++) pick &= pick - 1;
             const bool has = pick != 0;
             const uint32_t src = has ? uint32_t(__ffs(pick) - 1) : 0u;
             const uint32_t ga = __shfl_sync(0xffffffffu, a, src), gb = __shfl_sync(0xffffffffu, b, src);
-            const uint32_t gp = tile * 32u + src;
             for (uint32_t k = 0; k < 32 / NARROW_GROUP && todo; k++) todo &= todo - 1;
             if (has) {
                 const ColliderView A = collider_view(w, ga), B = collider_view(w, gb);
                 Contact ct;
                 const bool h = collide_polygon_polygon_group(A, B, ct, gl, gmask, sA, sB);
-                if (gl == 0) {
-                    hit[gp] = h ? 1u : 0u;
-                    if (h) write_slot(ct, ga, gb, slots + gp);
+                if (gl == 0 && h) {
+                    hitS[warpFirst + src] = 1u;
+                    write_slot(ct, ga, gb, slot + warpFirst + src);
                 }
                 __syncwarp(gmask);   // the group's tiles are reused by its next pair
             }
         }
+        __syncwarp();
+        const bool h = hitS[threadIdx.x] != 0u;
+        // Output offsets: the tile's hits in pair order after those of the preceding tiles.
+        const uint32_t hits = __ballot_sync(0xffffffffu, h);
+        if (lane == 0) warpBase[warp] = __popc(hits);
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t c = lane < nWarps ? warpBase[lane] : 0u;
+            uint32_t incl = c;
+            for (uint32_t o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const uint32_t aggregate = __shfl_sync(0xffffffffu, incl, 31);
+            if (lane < nWarps) warpBase[lane] = incl - c;
+            volatile uint32_t* state = tileState;
+            uint32_t prefix = 0;
+            if (tile == 0) {
+                if (lane == 0) state[0] = (2u << 30) | aggregate;
+            } else {
+                if (lane == 0) state[tile] = (1u << 30) | aggregate;
+                prefix = scan_lookback(tile, tileState, &counters->status);
+                if (lane == 0) state[tile] = (2u << 30) | (prefix + aggregate);
+            }
+            if (lane == 0) {
+                tileBase = prefix;
+                if (tile == tiles_n - 1) {
+                    const uint32_t total = prefix + aggregate;
+                    counters->manifolds = total;
+                    *nOut = min(total, manifoldCap);
+                    if (total > manifoldCap) atomicOr(&counters->status, STATUS_MANIFOLD_OVERFLOW);
+                }
+            }
+        }
+        __syncthreads();
+        if (h) {
+            const uint32_t o = tileBase + warpBase[warp] + __popc(hits & ((1u << lane) - 1u));
+            if (o < manifoldCap) out[o] = slot[threadIdx.x];
+        }
+        __syncthreads();   // tileSlot, tileBase, warpBase, the slots and the vertex tiles are reused by the next tile
     }
-}
-
-__global__ void k_compact_manifolds(const Manifold* __restrict__ slots, const uint32_t* __restrict__ hit,
-                                    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ nPairs,
-                                    uint32_t pairCap, Manifold* __restrict__ out, uint32_t manifoldCap,
-                                    uint32_t* __restrict__ nOut, StepCounters* counters)
-{
-    const uint32_t n = min(*nPairs, pairCap);
-    const uint32_t total = n ? offsets[n - 1] + hit[n - 1] : 0u;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        *nOut = min(total, manifoldCap);
-        counters->manifolds = total;
-        if (total > manifoldCap) atomicOr(&counters->status, STATUS_MANIFOLD_OVERFLOW);
-    }
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
-        if (hit[p] && offsets[p] < manifoldCap) out[offsets[p]] = slots[p];
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -266,7 +316,7 @@ __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* n
 // colour classes simply merge). Priorities are world-local indices: every world gets the colouring, hence the
 // solving order, it has when stepped on its own, whichever team it is in. A team whose bodies fit the dynamic
 // shared memory (bodyCap bodies) keeps their velocities, poses and colouring words there.
-template <uint32_t THREADS>
+template <uint32_t THREADS, bool PIPELINED>
 __global__ void __launch_bounds__(THREADS) k_color_solve_teams(TeamLaunch a)
 {
     // [bodyCap] velocities, [bodyCap] poses, then 2 x [bodyCap] u64 colouring words, overwritten after colouring by
@@ -310,8 +360,10 @@ __global__ void __launch_bounds__(THREADS) k_color_solve_teams(TeamLaunch a)
             cs.q = teamCache + 2 * a.bodyCap;
             cs.cap = a.consCap;
             cs.base = b0;
-            color_and_solve(w, SharedBodies{vel, pos, maxW, maskW, b0}, m + lo, hi - lo, ls, a.velIters, a.posIters,
-                            threadIdx.x, THREADS, BlockSync{}, &a.counters->colors, &a.counters->status, cs);
+            color_and_solve<BlockSync, SharedBodies, PIPELINED>(w, SharedBodies{vel, pos, maxW, maskW, b0}, m + lo,
+                                                                 hi - lo, ls, a.velIters, a.posIters, threadIdx.x,
+                                                                 THREADS, BlockSync{}, &a.counters->colors,
+                                                                 &a.counters->status, cs);
             __syncthreads();
             for (uint32_t i = threadIdx.x; i < nb; i += THREADS) {
                 w.bvel[b0 + i] = vel[i];
@@ -319,44 +371,52 @@ __global__ void __launch_bounds__(THREADS) k_color_solve_teams(TeamLaunch a)
             }
         } else {
             __syncthreads();
-            color_and_solve(w, GlobalBodies{w.bvel, w.bpos, a.s.bodyMax, a.s.bodyMask}, m + lo, hi - lo, ls,
-                            a.velIters, a.posIters, threadIdx.x, THREADS, BlockSync{}, &a.counters->colors,
-                            &a.counters->status);
+            color_and_solve<BlockSync, GlobalBodies, PIPELINED>(
+                w, GlobalBodies{w.bvel, w.bpos, a.s.bodyMax, a.s.bodyMask}, m + lo, hi - lo, ls, a.velIters,
+                a.posIters, threadIdx.x, THREADS, BlockSync{}, &a.counters->colors, &a.counters->status);
         }
         __syncthreads();
     }
 }
 
-template <uint32_t THREADS>
+template <uint32_t THREADS, bool PIPELINED>
 static cudaError_t team_occupancy(uint32_t bodyCap, uint32_t consCap, int* out)
 {
-    cudaError_t e = cudaFuncSetAttribute(k_color_solve_teams<THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         int(TEAM_SMEM_MAX));
+    cudaError_t e = cudaFuncSetAttribute(k_color_solve_teams<THREADS, PIPELINED>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(TEAM_SMEM_MAX));
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, k_color_solve_teams<THREADS>, THREADS,
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, k_color_solve_teams<THREADS, PIPELINED>, THREADS,
                                                          team_smem_bytes(bodyCap, consCap));
 }
 
-cudaError_t team_solver_blocks_per_sm(uint32_t threads, uint32_t bodyCap, uint32_t consCap, int* out)
+cudaError_t team_solver_blocks_per_sm(uint32_t threads, bool pipelined, uint32_t bodyCap, uint32_t consCap, int* out)
 {
     switch (threads) {
-    case 64: return team_occupancy<64>(bodyCap, consCap, out);
-    case 128: return team_occupancy<128>(bodyCap, consCap, out);
-    case 256: return team_occupancy<256>(bodyCap, consCap, out);
-    case 512: return team_occupancy<512>(bodyCap, consCap, out);
+    case 64: return pipelined ? team_occupancy<64, true>(bodyCap, consCap, out) : team_occupancy<64, false>(bodyCap, consCap, out);
+    case 128: return pipelined ? team_occupancy<128, true>(bodyCap, consCap, out) : team_occupancy<128, false>(bodyCap, consCap, out);
+    case 256: return pipelined ? team_occupancy<256, true>(bodyCap, consCap, out) : team_occupancy<256, false>(bodyCap, consCap, out);
+    case 512: return pipelined ? team_occupancy<512, true>(bodyCap, consCap, out) : team_occupancy<512, false>(bodyCap, consCap, out);
     default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_color_solve_teams(uint32_t threads, uint32_t grid, cudaStream_t stream, const TeamLaunch& a)
+template <uint32_t THREADS>
+static void launch_teams(bool pipelined, uint32_t grid, size_t smem, cudaStream_t stream, const TeamLaunch& a)
+{
+    if (pipelined) k_color_solve_teams<THREADS, true><<<grid, THREADS, smem, stream>>>(a);
+    else k_color_solve_teams<THREADS, false><<<grid, THREADS, smem, stream>>>(a);
+}
+
+cudaError_t launch_color_solve_teams(uint32_t threads, bool pipelined, uint32_t grid, cudaStream_t stream,
+                                     const TeamLaunch& a)
 {
     const size_t smem = team_smem_bytes(a.bodyCap, a.consCap);
     if (smem > TEAM_SMEM_MAX) return cudaErrorInvalidValue;
     switch (threads) {
-    case 64: k_color_solve_teams<64><<<grid, 64, smem, stream>>>(a); break;
-    case 128: k_color_solve_teams<128><<<grid, 128, smem, stream>>>(a); break;
-    case 256: k_color_solve_teams<256><<<grid, 256, smem, stream>>>(a); break;
-    case 512: k_color_solve_teams<512><<<grid, 512, smem, stream>>>(a); break;
+    case 64: launch_teams<64>(pipelined, grid, smem, stream, a); break;
+    case 128: launch_teams<128>(pipelined, grid, smem, stream, a); break;
+    case 256: launch_teams<256>(pipelined, grid, smem, stream, a); break;
+    case 512: launch_teams<512>(pipelined, grid, smem, stream, a); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -450,9 +510,9 @@ __global__ void k_state_flags(const uint8_t* __restrict__ bstate, const uint32_t
     for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nBodies; b += stride)
         bodyDyn[b] = bstate[b] == STATE_DYNAMIC;
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nColliders; c += stride) {
-        const bool dyn = bstate[cbody[c]] == STATE_DYNAMIC;
-        colDyn[c] = dyn;
-        colOther[c] = !dyn;
+        const uint8_t st = bstate[cbody[c]];
+        colDyn[c] = st == STATE_DYNAMIC;
+        colOther[c] = st == STATE_STATIC || st == STATE_SLEEPING;   // destroyed bodies' colliders: neither
     }
 }
 
@@ -469,7 +529,7 @@ __global__ void k_query_shape(const float4* __restrict__ caabb, const uint32_t* 
 {
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         const uint8_t st = bstate[cbody[c]];
-        const uint32_t tree = st == STATE_DYNAMIC ? 1u : (st == STATE_STATIC ? 2u : 4u);
+        const uint32_t tree = st == STATE_DYNAMIC ? 1u : (st == STATE_STATIC ? 2u : (st == STATE_SLEEPING ? 4u : 0u));
         bool hit = false;
         if (trees & tree) {
             const float4 b = caabb[c];
@@ -504,7 +564,16 @@ __device__ __forceinline__ bool circle_contact(const ColliderView& B, V2 pos, fl
         const V2 right = V2{B.c, B.s}, up = V2{-B.s, B.c};
         const V2 d = pos - B.pos;
         const V2 loc = V2{dot(d, right), dot(d, up)};
-        if (B.type == SHAPE_BOX) {
+        if (B.type == SHAPE_CAPSULE) {
+            // Closest point of the core to the query centre (NarrowPhaseCollisionDetector.cpp:245-262).
+            const V2 axis = V2{B.c, B.s};
+            const float t = clamp_value(dot(d, axis), -B.hw, B.hw);
+            const V2 delta = d - axis * t;
+            const float distSquared = dot(delta, delta);
+            const float radiusSum = B.r + radius;
+            if (radiusSum <= 0.0f || distSquared >= radiusSum * radiusSum) return false;
+            sdf = sqrtf(distSquared) - B.r;
+        } else if (B.type == SHAPE_BOX) {
             const float dx = fabsf(loc.x) - B.hw, dy = fabsf(loc.y) - B.hh;
             const float maxD = rfmaxf(dx, dy);
             if (maxD > 0.0f && maxD >= radius) return false;
@@ -548,7 +617,7 @@ __global__ void k_circle_contacts(DeviceWorld w, float x, float y, float radius,
     const float rr = r * r;
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < w.nColliders; c += gridDim.x * blockDim.x) {
         const uint8_t st = w.bstate[w.cbody[c]];
-        const uint32_t tree = st == STATE_DYNAMIC ? 1u : (st == STATE_STATIC ? 2u : 4u);
+        const uint32_t tree = st == STATE_DYNAMIC ? 1u : (st == STATE_STATIC ? 2u : (st == STATE_SLEEPING ? 4u : 0u));
         bool hit = false;
         float sdf = 0.0f;
         if (trees & tree) {

@@ -29,7 +29,8 @@ __device__ __forceinline__ uint32_t remap<uint32_t>(uint32_t v, const GatherSeg&
     case GATHER_BODY: return uint32_t(int32_t(v) + g.dBody);
     case GATHER_SHAPE: {
         const uint32_t type = shape_type(v);
-        const int32_t d = type == SHAPE_CIRCLE ? g.dCircle : (type == SHAPE_BOX ? g.dBox : g.dPoly);
+        // Boxes and capsules share one parameter table.
+        const int32_t d = type == SHAPE_CIRCLE ? g.dCircle : (type == SHAPE_POLYGON ? g.dPoly : g.dBox);
         return (type << 30) | uint32_t(int32_t(shape_index(v)) + d);
     }
     case GATHER_MATERIAL: return uint32_t(int32_t(v) + g.dMat);

@@ -75,6 +75,12 @@ __device__ __forceinline__ float4 collider_aabb(const DeviceWorld& w, uint32_t c
         const float ey = as * h.x + ac * h.y;
         return make_float4(x - ex, y - ey, x + ex, y + ey);
     }
+    case SHAPE_CAPSULE: {   // buildCapsuleAABBs (ColliderAABBBuilder.cpp:138-175): (half length, radius)
+        const float2 h = w.boxHalf[si];
+        const float ex = fabsf(cs) * h.x + h.y;
+        const float ey = fabsf(sn) * h.x + h.y;
+        return make_float4(x - ex, y - ey, x + ex, y + ey);
+    }
     default: {
         const uint32_t off = w.polyOffset[si], nv = w.polyCount[si];
         float mnx = FLT_MAX, mny = FLT_MAX, mxx = -FLT_MAX, mxy = -FLT_MAX;
@@ -718,36 +724,82 @@ __device__ __forceinline__ uint32_t query_one(const TreeView& dyn, const TreeVie
     return count;
 }
 
-// One traversal per query: the count, and the first QUERY_STASH pairs kept in the query's stash slots.
-__global__ void k_query_stash(TreeView dyn, TreeView other, const uint32_t* __restrict__ cbody,
-                              uint32_t* __restrict__ counts, uint2* __restrict__ stash, uint32_t* __restrict__ status)
+// The pair query in one kernel: blocks take tiles of blockDim.x queries (dynamic colliders in sorted rank order) in
+// ticket order (tileState and the ticket counter zeroed before the launch; at most QUERY_MAX_THREADS threads). Each
+// thread traverses once, counting its query's pairs and keeping the first QUERY_STASH in shared memory; the tile
+// scans the counts, takes its output offset from the decoupled look-back over the preceding tiles and writes the
+// kept pairs in place. A query with more pairs than the stash holds traverses again for the rest, after its tile
+// has published its prefix. The pairs come out ordered by query rank, then traversal order; the last tile writes
+// the pair count.
+__global__ void __launch_bounds__(QUERY_MAX_THREADS) k_query(TreeView dyn, TreeView other,
+                                                             const uint32_t* __restrict__ cbody,
+                                                             uint2* __restrict__ pairs, uint32_t pairCap,
+                                                             uint32_t* __restrict__ total,
+                                                             uint32_t* __restrict__ status,
+                                                             uint32_t* __restrict__ tileState,
+                                                             uint32_t* __restrict__ tileCounter)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < dyn.n; i += gridDim.x * blockDim.x) {
-        uint2* mine = stash + size_t(i) * QUERY_STASH;
-        counts[i] = query_one(dyn, other, cbody, i, [&](uint32_t k, uint2 p) { if (k < QUERY_STASH) mine[k] = p; },
-                              status);
-    }
-}
-
-// Pairs to their scanned offsets: copied from the stash, or, for a query with more pairs than the stash holds,
-// written by a second traversal (the same order).
-__global__ void k_query_emit(TreeView dyn, TreeView other, const uint32_t* __restrict__ cbody,
-                             const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offsets,
-                             const uint2* __restrict__ stash, uint2* __restrict__ pairs, uint32_t pairCap,
-                             uint32_t* __restrict__ status)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < dyn.n; i += gridDim.x * blockDim.x) {
-        const uint32_t c = counts[i], out = offsets[i];
-        if (c == 0) continue;
-        if (out + c > pairCap) atomicOr(status, STATUS_PAIR_OVERFLOW);
-        if (c <= QUERY_STASH) {
-            const uint2* mine = stash + size_t(i) * QUERY_STASH;
-            for (uint32_t k = 0; k < c; k++)
-                if (out + k < pairCap) pairs[out + k] = mine[k];
-        } else {
-            query_one(dyn, other, cbody, i, [&](uint32_t k, uint2 p) { if (out + k < pairCap) pairs[out + k] = p; },
-                      status);
+    __shared__ uint2 kept[QUERY_STASH * QUERY_MAX_THREADS];   // [k][thread]
+    __shared__ uint32_t warpBase[QUERY_MAX_THREADS / 32];
+    __shared__ uint32_t tileSlot, tileBase;
+    const uint32_t n = uint32_t(dyn.n);
+    const uint32_t tiles = (n + blockDim.x - 1) / blockDim.x;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
+    while (true) {
+        if (threadIdx.x == 0) tileSlot = atomicAdd(tileCounter, 1u);
+        __syncthreads();
+        const uint32_t tile = tileSlot;
+        if (tile >= tiles) return;
+        const uint32_t i = tile * blockDim.x + threadIdx.x;
+        uint32_t count = 0;
+        if (i < n)
+            count = query_one(dyn, other, cbody, int(i), [&](uint32_t k, uint2 pr) {
+                if (k < QUERY_STASH) kept[k * blockDim.x + threadIdx.x] = pr;
+            }, status);
+        // Block scan of the counts: lane prefix within the warp, then the warps' totals.
+        uint32_t incl = count;
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
         }
+        if (lane == 31) warpBase[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t c = lane < nWarps ? warpBase[lane] : 0u;
+            uint32_t wi = c;
+            for (uint32_t o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += t;
+            }
+            const uint32_t aggregate = __shfl_sync(0xffffffffu, wi, 31);
+            if (lane < nWarps) warpBase[lane] = wi - c;
+            volatile uint32_t* state = tileState;
+            uint32_t prefix = 0;
+            if (tile == 0) {
+                if (lane == 0) state[0] = (2u << 30) | aggregate;
+            } else {
+                if (lane == 0) state[tile] = (1u << 30) | aggregate;
+                prefix = scan_lookback(tile, tileState, status);
+                if (lane == 0) state[tile] = (2u << 30) | (prefix + aggregate);
+            }
+            if (lane == 0) {
+                tileBase = prefix;
+                if (tile == tiles - 1) {
+                    *total = prefix + aggregate;
+                    if (prefix + aggregate > pairCap) atomicOr(status, STATUS_PAIR_OVERFLOW);
+                }
+            }
+        }
+        __syncthreads();
+        const uint32_t out = tileBase + warpBase[warp] + incl - count;
+        const uint32_t keptCount = min(count, QUERY_STASH);
+        for (uint32_t k = 0; k < keptCount; k++)
+            if (out + k < pairCap) pairs[out + k] = kept[k * blockDim.x + threadIdx.x];
+        if (count > QUERY_STASH)
+            query_one(dyn, other, cbody, int(i), [&](uint32_t k, uint2 pr) {
+                if (k >= QUERY_STASH && out + k < pairCap) pairs[out + k] = pr;
+            }, status);
+        __syncthreads();   // tileSlot, tileBase, warpBase and the stash are reused by the next tile
     }
 }
 
@@ -773,6 +825,10 @@ __device__ __forceinline__ float ccd_cast_core(const DeviceWorld& w, uint32_t c,
     case SHAPE_BOX: {
         const float2 h = w.boxHalf[si];
         return ccd_cast_box(q0, dl, dd, h.x, h.y, coreRadius, best);
+    }
+    case SHAPE_CAPSULE: {
+        const float2 h = w.boxHalf[si];
+        return ccd_cast_capsule(q0, dl, dd, h.x, h.y, coreRadius, best);
     }
     default: {
         const uint32_t off = w.polyOffset[si];
@@ -894,65 +950,73 @@ __global__ void k_ccd_shift_bodies(DeviceWorld w, const uint32_t* __restrict__ d
 // Exclusive scan of uint32 (reduce-then-scan, 2048 elements per block); used for pair offsets, compaction and
 // work lists.
 // ---------------------------------------------------------------------------------------------------------------
-__global__ void k_scan_blocks(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t n,
-                              uint32_t* __restrict__ blockSums, const uint32_t* __restrict__ nDev)
+// ---------------------------------------------------------------------------------------------------------------
+// Single-pass exclusive scan (decoupled look-back, scan_lookback). Tiles of SCAN_TILE elements are taken in ticket
+// order by a grid of persistent blocks. tileState and the ticket counter are zeroed before the launch.
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                       uint32_t n, const uint32_t* __restrict__ nDev,
+                                                       uint32_t* __restrict__ total, uint32_t* __restrict__ tileState,
+                                                       uint32_t* __restrict__ tileCounter, uint32_t* __restrict__ status)
 {
-    // nDev: the element count on the device (at most n, the capacity the grid was sized for); blocks past it only
-    // contribute a zero block sum.
+    __shared__ uint32_t warpSums[SCAN_THREADS / 32];
+    __shared__ uint32_t tileSlot, tilePrefix;
     if (nDev) n = min(n, *nDev);
-    if (blockIdx.x * SCAN_TILE >= n && blockIdx.x > 0) {
-        if (threadIdx.x == 0 && blockSums) blockSums[blockIdx.x] = 0u;
+    const uint32_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (n == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0 && total) *total = 0u;
         return;
     }
-    __shared__ uint32_t warpSums[SCAN_THREADS / 32];
-    const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
-    uint32_t v[SCAN_ITEMS];
-    uint32_t sum = 0;
-#pragma unroll
-    for (uint32_t j = 0; j < SCAN_ITEMS; j++) { v[j] = base + j < n ? in[base + j] : 0u; sum += v[j]; }
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t incl = sum;
-    for (uint32_t o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    if (lane == 31) warpSums[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t ws = lane < SCAN_THREADS / 32 ? warpSums[lane] : 0u;
-        uint32_t wi = ws;
-        for (uint32_t o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
-            if (lane >= o) wi += t;
-        }
-        if (lane < SCAN_THREADS / 32) warpSums[lane] = wi - ws;
-        if (lane == SCAN_THREADS / 32 - 1 && blockSums) blockSums[blockIdx.x] = wi;
-    }
-    __syncthreads();
-    uint32_t run = warpSums[warp] + incl - sum;
+    while (true) {
+        if (threadIdx.x == 0) tileSlot = atomicAdd(tileCounter, 1u);
+        __syncthreads();
+        const uint32_t tile = tileSlot;
+        if (tile >= tiles) return;
+        const uint32_t base = tile * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+        uint32_t v[SCAN_ITEMS];
+        uint32_t sum = 0;
 #pragma unroll
-    for (uint32_t j = 0; j < SCAN_ITEMS; j++) {
-        if (base + j < n) out[base + j] = run;
-        run += v[j];
+        for (uint32_t j = 0; j < SCAN_ITEMS; j++) { v[j] = base + j < n ? in[base + j] : 0u; sum += v[j]; }
+        uint32_t incl = sum;
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) warpSums[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t ws = lane < SCAN_THREADS / 32 ? warpSums[lane] : 0u;
+            uint32_t wi = ws;
+            for (uint32_t o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += t;
+            }
+            const uint32_t aggregate = __shfl_sync(0xffffffffu, wi, SCAN_THREADS / 32 - 1);
+            if (lane < SCAN_THREADS / 32) warpSums[lane] = wi - ws;
+            volatile uint32_t* state = tileState;
+            uint32_t prefix = 0;
+            if (tile == 0) {
+                if (lane == 0) state[0] = (2u << 30) | aggregate;
+            } else {
+                if (lane == 0) state[tile] = (1u << 30) | aggregate;
+                prefix = scan_lookback(tile, tileState, status);
+                if (lane == 0) state[tile] = (2u << 30) | (prefix + aggregate);
+            }
+            if (lane == 0) {
+                tilePrefix = prefix;
+                if (total && tile == tiles - 1) *total = prefix + aggregate;
+            }
+        }
+        __syncthreads();
+        uint32_t run = tilePrefix + warpSums[warp] + incl - sum;
+#pragma unroll
+        for (uint32_t j = 0; j < SCAN_ITEMS; j++) {
+            if (base + j < n) out[base + j] = run;
+            run += v[j];
+        }
+        __syncthreads();   // tileSlot and warpSums are reused by the next tile
     }
-}
-
-__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_t* __restrict__ blockOffsets,
-                           const uint32_t* __restrict__ nDev)
-{
-    if (nDev) n = min(n, *nDev);
-    if (blockIdx.x * SCAN_TILE >= n) return;
-    const uint32_t add = blockOffsets[blockIdx.x];
-    const uint32_t base = blockIdx.x * SCAN_TILE;
-    for (uint32_t j = threadIdx.x; j < SCAN_TILE; j += blockDim.x)
-        if (base + j < n) out[base + j] += add;
-}
-
-// total = offsets[n-1] + in[n-1] (0 for n == 0).
-__global__ void k_scan_total(const uint32_t* __restrict__ in, const uint32_t* __restrict__ out, uint32_t n,
-                             uint32_t* __restrict__ total)
-{
-    if (threadIdx.x == 0 && blockIdx.x == 0) *total = n ? out[n - 1] + in[n - 1] : 0u;
 }
 
 }  // namespace ag2d

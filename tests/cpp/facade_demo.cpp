@@ -1,9 +1,10 @@
 // Scene code in the reference's style (App/Scenes.cpp: create a material, a static ground box and a pile of
 // bodies through ObjectAPI, then Simulation::update) compiled against the C++ facade of libag2d.so.
-// Prints "no-device" and exits 0 when the machine has no CUDA device; otherwise steps the scene and prints
-// "ok <bodies> <most manifolds in one step> <mean y> <colliders a circle query finds> <circle contacts>" after
-// querying the settled pile the way the reference's editor selects (queryCollidersInShape with a CircleQuery, then
-// findCollisionsInCircle over what it found).
+// Prints "no-device" and exits 0 when the machine has no CUDA device; otherwise steps the scene (a capsule is
+// created among the pile, and a body with three colliders; once it has settled one body is destroyed and another
+// kicked upwards through ObjectAPI's deferred commands) and prints "ok <bodies> <most manifolds in one step> <mean y> <colliders a circle query finds>
+// <circle contacts> <live bodies>" after querying the settled pile the way the reference's editor selects
+// (queryCollidersInShape with a CircleQuery, then findCollisionsInCircle over what it found).
 #include "ag2d_simulation.hpp"
 
 #include <algorithm>
@@ -42,15 +43,61 @@ int main()
         else ok = sim->objects().createPolygon({b, std::span<ag2d::Vec2>(tri, 3)}).has_value();
         created += ok ? 1 : 0;
     }
+    ag2d::BodyCreateParams cb;
+    cb.position = {0.0f, 10.0f};
+    cb.rotation = 0.3f;
+    cb.mass = 1.0f;
+    cb.materialIndex = mat;
+    const std::optional<ag2d::Handle> capsule = sim->objects().createCapsuleH({cb, 1.5f, 0.3f});
+    if (!capsule) return 7;
+    created++;
+    ag2d::BodyCreateParams gb;
+    gb.position = {8.0f, 10.0f};
+    gb.mass = 1.0f;
+    gb.materialIndex = mat;
+    const std::optional<ag2d::Handle> doomed = sim->objects().createCircleH({gb, 0.5f});
+    if (!doomed) return 8;
+    created++;
+    // A compound body (ObjectAPI::createBody + create*Collider): a bar with a wheel at each end, and an invalid
+    // collider request on a stale handle.
+    ag2d::BodyCreateParams db;
+    db.position = {-4.0f, 12.0f};
+    db.mass = 2.0f;
+    db.inertia = 1.5f;
+    const std::optional<ag2d::Handle> dumbbell = sim->objects().createBodyH(db);
+    if (!dumbbell) return 10;
+    created++;
+    ag2d::BoxColliderCreateParams bar;
+    bar.bodyHandle = *dumbbell;
+    bar.materialIndex = mat;
+    bar.size = {2.0f, 0.2f};
+    if (!sim->objects().createBoxCollider(bar)) return 11;
+    for (float side : {-1.0f, 1.0f}) {
+        ag2d::CircleColliderCreateParams wheel;
+        wheel.bodyHandle = *dumbbell;
+        wheel.localOffset = {side, 0.0f};
+        wheel.materialIndex = mat;
+        wheel.radius = 0.35f;
+        if (!sim->objects().createCircleCollider(wheel)) return 12;
+    }
+    ag2d::CircleColliderCreateParams orphan;
+    orphan.bodyHandle = ag2d::Handle{~0ull};
+    orphan.radius = 1.0f;
+    if (sim->objects().createCircleCollider(orphan)) return 13;   // stale body handle: nullopt
     ag2d::BoxCreateParams bad;
     bad.base.mass = 1.0f;
     bad.size = {-1.0f, 1.0f};
     if (sim->objects().createBox(bad)) return 3;     // invalid shape: nullopt, as in the reference
     size_t maxManifolds = 0;   // the pile settles and falls asleep, so track the most contacts seen
     for (int frame = 0; frame < 120; frame++) {
+        if (frame == 90) {
+            sim->objects().destroyBody(*doomed);
+            sim->objects().setBodyVelocity(*capsule, {0.0f, 3.0f});
+        }
         sim->update(1.0f / 60.0f);
         maxManifolds = std::max(maxManifolds, sim->getBodyCollisionData().size());
     }
+    if (sim->objects().getBodyIndex(*doomed) != UINT32_MAX) return 9;   // the destroyed body's handle is stale
     const ag2d::BodyView bodies = sim->objects().getBodies();
     double meanY = 0.0;
     for (uint32_t i = 0; i < bodies.getCount(); i++) meanY += bodies.comY[i];
@@ -65,8 +112,10 @@ int main()
     std::vector<ag2d::ObjectDenseIndex> all;
     sim->getBroadPhaseCollisionDetector().queryCollidersInShape(bp::AABBQuery({-1e6f, -1e6f, 1e6f, 1e6f}),
                                                                 bp::BvhTreeTypeFlag::All, all);
-    if (all.size() != bodies.getCount()) return 6;   // one collider per body, all inside the huge box
-    std::printf("ok %u %zu %.3f %zu %zu\n", bodies.getCount(), maxManifolds, meanY / double(bodies.getCount()),
-                found.size(), touching.size());
+    // One collider per live body plus the dumbbell's two wheels, all inside the huge box; the destroyed body's
+    // collider is in no tree.
+    if (all.size() != bodies.getCount() - 1 + 2) return 6;
+    std::printf("ok %u %zu %.3f %zu %zu %zu\n", bodies.getCount(), maxManifolds, meanY / double(bodies.getCount()),
+                found.size(), touching.size(), all.size());
     return bodies.getCount() == uint32_t(created) ? 0 : 4;
 }

@@ -15,6 +15,8 @@ Fixtures:
     wrap_edge.npz           body rotations around wrap boundaries (SIMD body and scalar tail)
     traj_c1_n256.npz        600-step trajectory statistics of a 256-polygon scene
     traj_c1_n2048.npz       the same statistics of the full c1 configuration (2,048 polygons, seed 0, 600 steps)
+    capsules_n1500_s0_step300.npz  capsules with circles, boxes and polygons in a U container (every shape pair),
+                               phase taps of step 301
     c2_n20000_s2_step420.npz   20,000 bodies of the c2 mix (500 columns x 40 rows) in a U container, phase taps of step 421 (the
                                narrow phase and the solver compared at scale)
     c5_ccd_hit.npz          the first continuous-collision hit of a serving-style request (fast circles)
@@ -264,6 +266,8 @@ FIXTURES = {
     "c2_n20000_s2_step420.npz": lambda p: phase_fixture(scenes.make_c2(20000, 2, columns=500), 420, p,
                                                         tuple(x for x in PHASE_PREFIXES if not x.startswith("post.")),
                                                         store_once=True),
+    "capsules_n1500_s0_step300.npz": lambda p: phase_fixture(scenes.make_capsule_mix(1500, 0), 300, p,
+                                                            store_once=True),
     "cossin_edge.npz": cossin_fixture,
     "wrap_edge.npz": wrap_fixture,
     "traj_c1_n256.npz": trajectory_fixture,

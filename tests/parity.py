@@ -8,6 +8,10 @@ import numpy as np
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 PHASE_FIXTURES = ("c1_n256_s0_step300.npz", "c2_n2000_s1_step240.npz", "c3_n1500_s0_step0.npz",
                   "c2_n20000_s2_step420.npz")
+# Capsules with every other shape (all ten shape pairs): the CUDA path is compared with the reference's own taps;
+# the C restatement does not restate the capsule routines, so the CPU oracle checks leave this fixture out.
+CAPSULE_FIXTURES = ("capsules_n1500_s0_step300.npz",)
+GPU_PHASE_FIXTURES = PHASE_FIXTURES + CAPSULE_FIXTURES
 
 # Solver impulses against the FP64 replay of the same order (the FP32 replay of the same order is bit-exact; this is
 # the precision contract), on the active contacts' normal and friction impulses:

@@ -66,7 +66,7 @@ COL_FIELDS = [(ag2d.COL_WORLD_X, "worldPosX"), (ag2d.COL_WORLD_Y, "worldPosY"),
               (ag2d.COL_AABB_MIN_Y, "aabbMinY"), (ag2d.COL_AABB_MAX_X, "aabbMaxX"), (ag2d.COL_AABB_MAX_Y, "aabbMaxY")]
 
 
-@pytest.mark.parametrize("name", parity.PHASE_FIXTURES + ("wrap_edge.npz",))
+@pytest.mark.parametrize("name", parity.GPU_PHASE_FIXTURES + ("wrap_edge.npz",))
 def test_integrate_bit_exact(name):
     d, mats = _fixture(name) if name != "wrap_edge.npz" else (parity.load(name), None)
     w = _world(d, mats, "pre.")
@@ -81,7 +81,7 @@ def _spatial(w, d):
         w.run_phase(ag2d.PHASE_SPATIAL_DYNAMIC)
 
 
-@pytest.mark.parametrize("name", parity.PHASE_FIXTURES + ("wrap_edge.npz",))
+@pytest.mark.parametrize("name", parity.GPU_PHASE_FIXTURES + ("wrap_edge.npz",))
 def test_poses_and_aabbs_bit_exact(name):
     d, mats = _fixture(name) if name != "wrap_edge.npz" else (parity.load(name), None)
     w = _world(d, mats, "pre.", body_prefix="int.")
@@ -93,7 +93,7 @@ def test_poses_and_aabbs_bit_exact(name):
         assert parity.mismatches(w.read(field), d["sp.col." + ref]) == 0, ref
 
 
-@pytest.mark.parametrize("name", parity.PHASE_FIXTURES)
+@pytest.mark.parametrize("name", parity.GPU_PHASE_FIXTURES)
 def test_broad_morton_sort_pairs_bit_exact(name):
     d, mats = _fixture(name)
     w = _world(d, mats, "pre.", body_prefix="int.")
@@ -115,7 +115,7 @@ def test_broad_morton_sort_pairs_bit_exact(name):
     assert np.all(p[~both, 0] >= dyn_begin)
 
 
-@pytest.mark.parametrize("name", parity.PHASE_FIXTURES)
+@pytest.mark.parametrize("name", parity.GPU_PHASE_FIXTURES)
 def test_narrow_and_warm_start_bit_exact(name):
     d, mats = _fixture(name)
     w = _world(d, mats, "pre.", body_prefix="int.")
@@ -132,7 +132,7 @@ def test_narrow_and_warm_start_bit_exact(name):
         assert parity.mismatches(parity.active_points(ours, f), parity.active_points(ref, f)) == 0, f
 
 
-@pytest.mark.parametrize("name", parity.PHASE_FIXTURES)
+@pytest.mark.parametrize("name", parity.GPU_PHASE_FIXTURES)
 def test_solver_against_replays_of_the_colour_order(name):
     d, mats = _fixture(name)
     if "svin.man.count" not in d:
@@ -170,7 +170,7 @@ def test_solver_against_replays_of_the_colour_order(name):
     assert ok, msg
 
 
-@pytest.mark.parametrize("name", parity.PHASE_FIXTURES)
+@pytest.mark.parametrize("name", parity.GPU_PHASE_FIXTURES)
 def test_islands_partition(name):
     d, mats = _fixture(name)
     if "svin.man.count" not in d:
