@@ -65,7 +65,7 @@ typedef struct ag2d_counters {
     uint32_t warm_hits;     /* manifolds warm-started */
     uint32_t sleeping;      /* bodies sleeping after the step */
     uint32_t ccd_hits;      /* bodies moved back by continuous collision detection in the last step */
-    uint32_t reserved;
+    uint32_t restored;      /* manifolds of woken islands that joined the last step whole (from the sleep store) */
     uint64_t steps;         /* steps taken by this world */
     uint64_t launches;      /* kernel launches issued by this world so far */
     uint64_t list_rebuilds; /* work-list rebuilds after sleep/wake changes */
@@ -138,6 +138,9 @@ enum ag2d_field {
     AG2D_PREV_MANIFOLDS,    /* previous step's manifolds (warm-start source) */
     AG2D_SOLVE_ORDER,       /* uint32 manifold index per solving slot (colour-major) */
     AG2D_COLOR_STARTS,      /* uint32 [colors + 1] */
+    AG2D_ISLAND_MANIFOLDS,  /* manifolds of sleeping islands, kept until their island wakes (world-grouped) */
+    AG2D_ISLAND_IDS,        /* uint32 island of each stored manifold: the dense index of the island's root body
+                               (writable after AG2D_ISLAND_MANIFOLDS, with the same count) */
 };
 
 /* Manifold record (NarrowPhaseCollisionDetector.h:26-61 with dense collider indices instead of handles). */
@@ -161,6 +164,8 @@ enum ag2d_phase {
     AG2D_PHASE_COLLIDE,            /* collision detection alone: dynamic poses + AABBs, broad, narrow (no warm start) */
     AG2D_PHASE_CCD,                /* continuous collision: sweep fast dynamic colliders against static ones, move
                                       hit bodies back (uses the poses AG2D_PHASE_INTEGRATE recorded) */
+    AG2D_PHASE_WAKE,               /* wake the sleeping islands AG2D_MANIFOLDS touch, then bring their stored
+                                      manifolds into AG2D_MANIFOLDS (Simulation.cpp:440-444) */
 };
 
 /* ---- library ---- */

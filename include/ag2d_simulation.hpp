@@ -165,14 +165,16 @@ public:
         if (p.base.inertia != 0) return std::nullopt;
         const ag2d_body_desc d = detail::desc(p.base);
         uint64_t h = 0;
-        return created(ag2d_world_add_circle(world, &d, p.radius, &h), h);
+        const int32_t code = ag2d_world_add_circle(world, &d, p.radius, &h);
+        return created(code, h);
     }
     std::optional<Handle> createBoxH(const BoxCreateParams& p)
     {
         if (p.base.inertia != 0) return std::nullopt;
         const ag2d_body_desc d = detail::desc(p.base);
         uint64_t h = 0;
-        return created(ag2d_world_add_box(world, &d, p.size.x, p.size.y, &h), h);
+        const int32_t code = ag2d_world_add_box(world, &d, p.size.x, p.size.y, &h);
+        return created(code, h);
     }
     std::optional<Handle> createPolygonH(const PolygonCreateParams& p)
     {
@@ -182,7 +184,8 @@ public:
         xy.reserve(p.localVertices.size() * 2);
         for (const Vec2& v : p.localVertices) { xy.push_back(v.x); xy.push_back(v.y); }
         uint64_t h = 0;
-        return created(ag2d_world_add_polygon(world, &d, xy.data(), uint32_t(p.localVertices.size()), &h), h);
+        const int32_t code = ag2d_world_add_polygon(world, &d, xy.data(), uint32_t(p.localVertices.size()), &h);
+        return created(code, h);
     }
 
     std::optional<Handle> createCapsuleH(const CapsuleCreateParams& p)
@@ -190,7 +193,8 @@ public:
         if (p.base.inertia != 0) return std::nullopt;
         const ag2d_body_desc d = detail::desc(p.base);
         uint64_t h = 0;
-        return created(ag2d_world_add_capsule(world, &d, p.length, p.radius, &h), h);
+        const int32_t code = ag2d_world_add_capsule(world, &d, p.length, p.radius, &h);
+        return created(code, h);
     }
 
     // ObjectAPI::createBody / createBodyH (ObjectAPI.h:28, 61): a body with explicit mass, inertia and centre of
@@ -202,7 +206,8 @@ public:
         const ag2d_body_desc d = detail::desc(p);
         const Vec2 com = p.centerOfMass.value_or(Vec2{});
         uint64_t h = 0;
-        return created(ag2d_world_create_body(world, &d, p.inertia, com.x, com.y, &h), h);
+        const int32_t code = ag2d_world_create_body(world, &d, p.inertia, com.x, com.y, &h);
+        return created(code, h);
     }
     std::optional<ObjectDenseIndex> createCircleCollider(const CircleColliderCreateParams& p)
     {
@@ -257,6 +262,7 @@ public:
 
 private:
     // Invalid shapes (the reference's nullopt cases) return nullopt; anything else is an error.
+    // 'code' is the creating call's result, evaluated before 'h' is read (the call writes h).
     static std::optional<Handle> created(int32_t code, uint64_t h)
     {
         if (code == AG2D_ERR_INVALID_ARG || code == AG2D_ERR_UNSUPPORTED) return std::nullopt;

@@ -264,6 +264,22 @@ namespace
         h->putv(p + "points", pts); h->putv(p + "ids", ids); h->putv(p + "impulses", imp);
     }
 
+    // The sleeping islands' stored manifolds (NarrowPhaseCollisionDetector::islandManifolds), flattened in island
+    // slot order, with each record's sleep island id (slot + FIRST_SLEEP_ISLAND_ID) as <p>islandId.
+    void dumpIslandStore(Harness* h, const std::string& p)
+    {
+        const auto& store = h->sim.narrowPhaseCollisionDetector.islandManifolds;
+        std::vector<BodyCollisionData> flat;
+        std::vector<uint32_t> id;
+        for (size_t slot = 0; slot < store.size(); slot++)
+            for (const BodyCollisionData& d : store[slot]) {
+                flat.push_back(d);
+                id.push_back(uint32_t(slot + FIRST_SLEEP_ISLAND_ID));
+            }
+        dumpManifolds(h, p, flat);
+        h->putv(p + "islandId", id);
+    }
+
     void dumpTree(Harness* h, const std::string& p, BroadPhaseInternal::BvhTreeType type)
     {
         const auto& t = h->sim.broadPhaseCollisionDetector.trees[size_t(type)];
@@ -419,6 +435,13 @@ extern "C"
         default: break;
         }
     }
+    // Simulation::flushCommands (Simulation.cpp:454-461) on its own: the queued commands, the wakes they cause and
+    // the stored manifolds of the woken islands, as the next update would apply them first.
+    void agref_flush_commands(void* hp)
+    {
+        static_cast<Harness*>(hp)->sim.flushCommands();
+    }
+
     // Dense body index of a handle slot (UINT32_MAX when destroyed).
     uint32_t agref_body_index(void* hp, uint32_t slot)
     {
@@ -512,6 +535,7 @@ extern "C"
         dumpBodies(h, p);
         dumpColliders(h, p);
         dumpManifolds(h, p + "man.", h->sim.getBodyCollisionData());
+        dumpIslandStore(h, p + "isle.");
     }
 
     // Overwrites one float field of every body (used to drive the integration/wrap/cos-sin phases with chosen
@@ -553,6 +577,7 @@ extern "C"
         dumpBodies(h, "pre.");
         dumpColliders(h, "pre.");
         dumpManifolds(h, "pre.man.", s.narrowPhaseCollisionDetector.getBodyCollisionData());
+        dumpIslandStore(h, "pre.isle.");
 
         s.simulationRunTimer += dt;
         s.bodyCollisionSolver.resetCollisionData();
@@ -658,6 +683,7 @@ extern "C"
         dumpBodies(h, "post.");
         dumpColliders(h, "post.");
         dumpManifolds(h, "post.man.", s.getBodyCollisionData());
+        dumpIslandStore(h, "post.isle.");
     }
 
     uint64_t agref_blob_size(void* hp, const char* name)

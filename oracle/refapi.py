@@ -54,6 +54,7 @@ def lib():
         L.agref_create_body.argtypes = [vp, f, f, f, f, f, f, f, f, f, f]
         L.agref_add_collider.restype = i64
         L.agref_add_collider.argtypes = [vp, u32, i32, f, f, f, u32, f, f, vp, u32]
+        L.agref_flush_commands.argtypes = [vp]
         L.agref_update.argtypes = [vp, i32]
         L.agref_destroy_body.argtypes = [vp, u32]
         L.agref_set_body.argtypes = [vp, u32, i32, f, f]
@@ -179,6 +180,10 @@ class RefSim:
     def body_index(self, i: int) -> int:
         """Dense index of scene body i now (2**32 - 1 once destroyed)."""
         return int(lib().agref_body_index(self.h, self.body_slots[i]))
+
+    def flush_commands(self):
+        """Applies the queued commands now (the first part of the next update)."""
+        lib().agref_flush_commands(self.h)
 
     def update(self, steps: int = 1):
         lib().agref_update(self.h, steps)

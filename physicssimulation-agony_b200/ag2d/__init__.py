@@ -29,10 +29,11 @@ BODY_COM_X, BODY_COM_Y, BODY_VEL_X, BODY_VEL_Y, BODY_ROTATION, BODY_ANGULAR_VELO
     BODY_INV_INERTIA = range(1, 16)
 COL_WORLD_X, COL_WORLD_Y, COL_WORLD_ROTATION, COL_WORLD_COS, COL_WORLD_SIN, COL_AABB_MIN_X, COL_AABB_MIN_Y, \
     COL_AABB_MAX_X, COL_AABB_MAX_Y, COL_BODY = range(32, 42)
-DYN_SORTED, DYN_MORTON, PAIRS, MANIFOLDS, PREV_MANIFOLDS, SOLVE_ORDER, COLOR_STARTS = range(64, 71)
+DYN_SORTED, DYN_MORTON, PAIRS, MANIFOLDS, PREV_MANIFOLDS, SOLVE_ORDER, COLOR_STARTS, ISLAND_MANIFOLDS, \
+    ISLAND_IDS = range(64, 73)
 # enum ag2d_phase
 PHASE_INTEGRATE, PHASE_SPATIAL_FULL, PHASE_SPATIAL_DYNAMIC, PHASE_BROAD, PHASE_NARROW, PHASE_SOLVE, \
-    PHASE_ISLANDS, PHASE_COLLIDE, PHASE_CCD = range(1, 10)
+    PHASE_ISLANDS, PHASE_COLLIDE, PHASE_CCD, PHASE_WAKE = range(1, 11)
 
 MANIFOLD_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("nx", "<f4"), ("ny", "<f4"), ("depth", "<f4"),
                            ("count", "<u4"), ("id0", "<u4"), ("id1", "<u4"), ("px0", "<f4"), ("py0", "<f4"),
@@ -40,7 +41,8 @@ MANIFOLD_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("nx", "<f4"), ("ny", "<f
                            ("jt1", "<f4")])
 assert MANIFOLD_DTYPE.itemsize == 64
 
-_U32_FIELDS = {BODY_STATE, BODY_SLEEP_ISLAND, COL_BODY, DYN_SORTED, DYN_MORTON, SOLVE_ORDER, COLOR_STARTS}
+_U32_FIELDS = {BODY_STATE, BODY_SLEEP_ISLAND, COL_BODY, DYN_SORTED, DYN_MORTON, SOLVE_ORDER, COLOR_STARTS,
+               ISLAND_IDS}
 
 
 class Ag2dError(RuntimeError):
@@ -71,7 +73,7 @@ class Counters(ctypes.Structure):
     _fields_ = [("status", ctypes.c_uint32), ("pairs", ctypes.c_uint32), ("manifolds", ctypes.c_uint32),
                 ("colors", ctypes.c_uint32), ("woke", ctypes.c_uint32), ("slept", ctypes.c_uint32),
                 ("warm_hits", ctypes.c_uint32), ("sleeping", ctypes.c_uint32), ("ccd_hits", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32), ("steps", ctypes.c_uint64),
+                ("restored", ctypes.c_uint32), ("steps", ctypes.c_uint64),
                 ("launches", ctypes.c_uint64), ("list_rebuilds", ctypes.c_uint64), ("retries", ctypes.c_uint64),
                 ("regrows", ctypes.c_uint64), ("host_ms", ctypes.c_double), ("sync_ms", ctypes.c_double)]
 
@@ -239,7 +241,7 @@ def host_empty(nbytes: int) -> np.ndarray:
 
 
 def _field_view(buf: np.ndarray, field: int) -> np.ndarray:
-    if field in (MANIFOLDS, PREV_MANIFOLDS):
+    if field in (MANIFOLDS, PREV_MANIFOLDS, ISLAND_MANIFOLDS):
         return buf.view(MANIFOLD_DTYPE)
     if field == PAIRS:
         return buf.view(np.uint32).reshape(-1, 2)
@@ -579,10 +581,12 @@ class World:
         _check(lib.ag2d_world_read_wait(self.h))
 
     def write(self, field: int, data: np.ndarray):
-        if field in (MANIFOLDS, PREV_MANIFOLDS):
+        if field in (MANIFOLDS, PREV_MANIFOLDS, ISLAND_MANIFOLDS):
             a = np.ascontiguousarray(data, dtype=MANIFOLD_DTYPE)
         elif field == PAIRS:
             a = np.ascontiguousarray(data, dtype=np.uint32).reshape(-1, 2)
+        elif field in _U32_FIELDS:
+            a = np.ascontiguousarray(data, dtype=np.uint32)
         else:
             a = np.ascontiguousarray(data, dtype=np.float32)
         _check(lib.ag2d_world_write(self.h, field, a.ctypes.data if a.size else None, a.nbytes))
@@ -641,7 +645,7 @@ class Batch:
         ptr, cap = _out_bytes(out)
         _check(lib.ag2d_batch_read(self.h, world, field, ptr if cap else None, cap, ctypes.byref(n)))
         buf = out.reshape(-1).view(np.uint8)[:int(n.value)]
-        if field in (MANIFOLDS, PREV_MANIFOLDS):
+        if field in (MANIFOLDS, PREV_MANIFOLDS, ISLAND_MANIFOLDS):
             return buf.view(MANIFOLD_DTYPE)
         return buf.view(np.uint32 if field in _U32_FIELDS else np.float32)
 

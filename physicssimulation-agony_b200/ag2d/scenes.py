@@ -186,6 +186,31 @@ def make_capsule_mix(n: int = 1500, seed: int = 0, columns: int = 40, cell: floa
     return b.build(f"capmix_n{n}_s{seed}")
 
 
+def make_towers(towers: int = 40, levels: int = 3, drops: int = 12, seed: int = 0, spacing: float = 3.0,
+                drop_height: float = 30.0, group: int = 4) -> Scene:
+    """Sleep and wake: `towers` stacks of `levels` boxes (side U[0.8,1.0]) on a static ground, 3 m apart, each its
+    own island that falls asleep after settling; `drops` circles (r U[0.3,0.5]) fall onto every third tower from
+    drop_height + 8 m x (k // group), so `group` islands wake in the same step, with their stored manifolds."""
+    rng = np.random.default_rng(seed)
+    b = _Builder([FRICTION_MATERIAL])
+    width = towers * spacing + 10.0
+    b.add(BOX, 0.0, -1.0, width=width, height=2.0, mass=0.0, material=1)
+    x0 = -0.5 * (towers - 1) * spacing
+    for t in range(towers):
+        y = 0.0
+        for _ in range(levels):
+            s = rng.uniform(0.8, 1.0)
+            b.add(BOX, x0 + t * spacing + rng.uniform(-0.05, 0.05), y + 0.5 * s + 0.005, width=s, height=s,
+                  mass=s * s, material=1)
+            y += s + 0.01
+    for k in range(drops):
+        t = (3 * k) % towers
+        r = rng.uniform(0.3, 0.5)
+        b.add(CIRCLE, x0 + t * spacing + rng.uniform(-0.2, 0.2), drop_height + 8.0 * (k // group), radius=r,
+              mass=math.pi * r * r, material=1)
+    return b.build(f"towers_{towers}x{levels}_s{seed}")
+
+
 def make_c3(n: int = 1_000_000, seed: int = 0, extent: float = 4000.0) -> Scene:
     """Broad+narrow stress: n bodies, 50% circles / 50% 4-6-gons, size (radius) log-uniform in [0.1, 2] m,
     uniform in an extent x extent box, velocities N(0, 5 m/s), no gravity, no static bodies.

@@ -121,6 +121,18 @@ __device__ __forceinline__ uint32_t scan_lookback(uint32_t tile, uint32_t* tileS
     return prefix;
 }
 
+// Contact-cache key of an unordered collider pair, and its home slot in a power-of-two open-addressing table.
+__device__ __forceinline__ unsigned long long pair_key(uint32_t a, uint32_t b)
+{
+    const uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+    return (static_cast<unsigned long long>(lo) << 32) | hi;
+}
+__device__ __forceinline__ uint32_t slot_of(unsigned long long key, uint32_t capacity)
+{
+    const uint32_t shift = 64u - (31u - __clz(capacity));   // capacity is a power of two
+    return static_cast<uint32_t>((key * 0x9E3779B97F4A7C15ull) >> shift) & (capacity - 1u);
+}
+
 // Exclusive scan of in[0, min(n, *nDev)) into out (nDev may be null), total = the sum (may be null).
 __global__ void k_scan(const uint32_t* in, uint32_t* out, uint32_t n, const uint32_t* nDev, uint32_t* total,
                        uint32_t* tileState, uint32_t* tileCounter, uint32_t* status);
@@ -151,6 +163,50 @@ __global__ void k_island_sleep(DeviceWorld w, uint32_t* parent, const uint32_t* 
 __global__ void k_state_flags(const uint8_t* bstate, const uint32_t* cbody, uint32_t nBodies, uint32_t nColliders,
                               uint32_t* bodyDyn, uint32_t* colDyn, uint32_t* colOther);
 __global__ void k_scatter_list(const uint32_t* flag, const uint32_t* offset, uint32_t n, uint32_t* list);
+
+// Sleeping-island manifold store (k_islands.cu): restore at wake, move at sleep.
+__global__ void k_isle_stage_flags(DeviceWorld w, const Manifold* isle, const uint32_t* isleId, const uint32_t* nIsle,
+                                   const uint32_t* wakeIsland, uint32_t* flag);
+__global__ void k_isle_stage(const Manifold* isle, const uint32_t* nIsle, const uint32_t* flag, const uint32_t* off,
+                             uint32_t* stage, uint32_t* stageSlot, uint32_t* consumed, unsigned long long* keys,
+                             uint32_t* vals, uint32_t capacity, uint32_t* status);
+__global__ void k_isle_take(Manifold* cur, const uint32_t* nCur, const Manifold* isle, const uint32_t* stage,
+                            const uint32_t* nStage, const unsigned long long* keys, const uint32_t* vals,
+                            uint32_t capacity, uint32_t* consumed);
+__global__ void k_isle_unclaimed_flags(const uint32_t* nStage, const uint32_t* consumed, const uint32_t* stageSlot,
+                                       unsigned long long* keys, uint32_t* vals, uint32_t* flag);
+__global__ void k_isle_unclaimed(DeviceWorld w, const Manifold* isle, const uint32_t* nStage, const uint32_t* stage,
+                                 const uint32_t* flag, const uint32_t* off, uint32_t* list, uint32_t* listWorld);
+__global__ void k_isle_append(Manifold* cur, const uint32_t* nCur, uint32_t cap, uint32_t* hint, const Manifold* isle,
+                              const uint32_t* list, const uint32_t* nList, uint32_t* status);
+__global__ void k_isle_merge(DeviceWorld w, const Manifold* cur, const uint32_t* hint, const uint32_t* nCur,
+                             const uint32_t* seg, const Manifold* isle, const uint32_t* list,
+                             const uint32_t* listWorld, const uint32_t* nList, uint32_t cap, Manifold* out,
+                             uint32_t* outHint, uint32_t* status);
+__global__ void k_isle_count(uint32_t* nCur, const uint32_t* nStage, const uint32_t* nList, uint32_t cap,
+                             StepCounters* counters);
+__global__ void k_isle_keep_flags(DeviceWorld w, const Manifold* isle, const uint32_t* isleId, const uint32_t* nIsle,
+                                  const uint32_t* wakeIsland, uint32_t checkAlive, uint32_t* keep);
+__global__ void k_isle_move_flags(DeviceWorld w, const Manifold* m, const uint32_t* nM, uint32_t* stay,
+                                  uint32_t* move, uint32_t* moveIsland);
+__global__ void k_isle_sleep_worlds(DeviceWorld w, const Manifold* isle, const uint32_t* nIsle, const uint32_t* keep,
+                                    const uint32_t* keepOff, const Manifold* m, const uint32_t* nM,
+                                    const uint32_t* move, const uint32_t* moveOff, uint32_t* keepWorld,
+                                    uint32_t* moveWorld);
+__global__ void k_isle_store_scatter(DeviceWorld w, const Manifold* isle, const uint32_t* isleId,
+                                     const uint32_t* nIsle, const uint32_t* keep, const uint32_t* keepOff,
+                                     const uint32_t* nKeep, const Manifold* m, const uint32_t* nM,
+                                     const uint32_t* move, const uint32_t* moveOff, const uint32_t* nMove,
+                                     const uint32_t* moveIsland, const uint32_t* keepWorld, const uint32_t* moveWorld,
+                                     Manifold* isleOut, uint32_t* isleIdOut);
+__global__ void k_isle_store_count(const uint32_t* nKeep, const uint32_t* nMove, uint32_t* nIsle);
+__global__ void k_isle_append_moved(const Manifold* m, const uint32_t* nM, const uint32_t* move,
+                                    const uint32_t* moveOff, const uint32_t* moveIsland, const uint32_t* nIsle,
+                                    Manifold* isle, uint32_t* isleId);
+__global__ void k_isle_add_count(uint32_t* nIsle, const uint32_t* nMove);
+__global__ void k_isle_list_scatter(const Manifold* m, const uint32_t* color, const uint32_t* nM,
+                                    const uint32_t* stay, const uint32_t* stayOff, Manifold* out,
+                                    uint32_t* colorOut);
 __global__ void k_query_shape(const float4* caabb, const uint32_t* cbody, const uint8_t* bstate, uint32_t n,
                               uint32_t shape, float4 q, uint32_t trees, uint32_t* flag);
 __global__ void k_circle_contacts(DeviceWorld w, float x, float y, float radius, uint32_t trees, uint32_t* flag,

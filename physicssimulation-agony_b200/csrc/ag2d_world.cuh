@@ -40,7 +40,10 @@ struct StepCounters {
     uint32_t warmHits;        // manifolds that took warm-start impulses
     uint32_t barrierRounds;   // colouring rounds
     uint32_t ccdHits;         // bodies moved back by continuous collision detection
-    uint32_t pad[6];
+    uint32_t restored;        // sleeping-island manifolds that joined this step's list whole
+    uint32_t stored;          // sleeping-island manifolds held when the step began
+    uint32_t staged;          // of which the woken islands' records taken out by this step's restore
+    uint32_t pad[3];
 };
 
 // Manifold record (64 bytes), NarrowPhaseCollisionDetector.h:26-61 minus the handle union: colliders are stable

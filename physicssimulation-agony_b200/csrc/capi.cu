@@ -234,6 +234,7 @@ inline std::vector<float> min_extents(const std::vector<uint32_t>& cs, const std
 // Element counts of one resident world, per kind of array (a server engine's worlds are consecutive ranges).
 struct WorldExtent {
     uint32_t body = 0, col = 0, circle = 0, box = 0, poly = 0, vert = 0, mat = 0, man = 0, statics = 0;
+    uint32_t isle = 0;   // manifolds of sleeping islands
 };
 
 // A world waiting to join a server batch: all its arrays in one host blob (sections at 64-byte aligned offsets,
@@ -242,7 +243,7 @@ enum StagedSection : uint32_t {
     SEC_VEL, SEC_POS, SEC_ROT, SEC_WRAP, SEC_BOUND, SEC_TIMER, SEC_STATE, SEC_ISLAND,
     SEC_CBODY, SEC_CSHAPE, SEC_CMAT, SEC_COFF, SEC_CPOSE, SEC_CAABB, SEC_CROT, SEC_MINEXT,
     SEC_CIRCLE, SEC_BOXHALF, SEC_POLYOFF, SEC_POLYCOUNT, SEC_POLYVERTS, SEC_POLYNORMALS, SEC_MATS, SEC_PREV,
-    SEC_PREVCOLOR, NSEC
+    SEC_PREVCOLOR, SEC_ISLE, SEC_ISLEID, NSEC
 };
 struct StagedWorld {
     WorldExtent ext;
@@ -258,16 +259,16 @@ enum CkptSection : uint32_t {
     CK_VEL, CK_POS, CK_ROT, CK_WRAP, CK_BOUND, CK_TIMER, CK_STATE, CK_ISLAND,
     CK_CBODY, CK_CSHAPE, CK_CMAT, CK_COFF, CK_CPOSE, CK_CAABB, CK_CROT, CK_MINEXT,
     CK_CIRCLE, CK_BOXHALF, CK_POLYOFF, CK_POLYCOUNT, CK_POLYVERTS, CK_POLYNORMALS, CK_MATS, CK_PREV,
-    CK_PREVCOLOR, CK_WBODY, CK_WCOL, NCK
+    CK_PREVCOLOR, CK_WBODY, CK_WCOL, CK_ISLE, CK_ISLEID, NCK
 };
 constexpr char CKPT_MAGIC[8] = {'A', 'G', '2', 'D', 'C', 'K', 'P', 'T'};
-constexpr uint32_t CKPT_VERSION = 1;
+constexpr uint32_t CKPT_VERSION = 2;
 struct CkptHeader {
     char magic[8];
     uint32_t version, headerBytes;
     ag2d_world_settings settings;
     uint32_t nWorlds, nBodies, nColliders, nCircles, nBoxes, nPolygons, nPolyVerts, nMaterialRows;
-    uint32_t nPrev, nStatic, lastManifolds, reserved;
+    uint32_t nPrev, nStatic, lastManifolds, nIsle;
     uint64_t totalBytes;
     uint64_t off[NCK], len[NCK];
 };
@@ -281,6 +282,8 @@ struct PackedArrays {
     std::vector<uint32_t> isl, cb, cs, cm, po, pc;
     std::vector<Manifold> prev;
     std::vector<uint32_t> pcol;   // colour of each warm-start manifold (empty: none known)
+    std::vector<Manifold> isle;   // manifolds of sleeping islands, and the island (root body) of each
+    std::vector<uint32_t> isleId;
     std::vector<float4> cp;   // collider world poses at the end of the last step (empty: never stepped, zeros)
 
     // Appends another world, shifting its body, collider, shape, vertex and material indices past this one's.
@@ -307,6 +310,8 @@ struct PackedArrays {
         for (Manifold m : o.prev) { m.a += cof; m.b += cof; prev.push_back(m); }
         if (o.pcol.size() == o.prev.size()) cat(pcol, o.pcol);
         else pcol.insert(pcol.end(), o.prev.size(), NO_COLOR);
+        for (Manifold m : o.isle) { m.a += cof; m.b += cof; isle.push_back(m); }
+        for (uint32_t v : o.isleId) isleId.push_back(v == 0xFFFFFFFFu ? v : v + bo);
         if (!o.cp.empty() || !cp.empty()) {
             cp.resize(cof, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
             if (o.cp.empty()) cp.resize(cof + o.cb.size(), make_float4(0.0f, 0.0f, 0.0f, 0.0f));
@@ -330,6 +335,7 @@ StagedWorld stage_world(const PackedArrays& a)
     e.vert = uint32_t(a.pv.size());
     e.mat = uint32_t(a.mats.size());
     e.man = uint32_t(a.prev.size());
+    e.isle = uint32_t(a.isle.size());
     e.statics = uint32_t(std::count(a.state.begin(), a.state.end(), uint8_t(STATE_STATIC)));
     const std::vector<float> me = min_extents(a.cs, a.cr, a.bh, a.po, a.pc, a.pv, a.pn);
     const size_t sizes[NSEC] = {
@@ -338,7 +344,7 @@ StagedWorld stage_world(const PackedArrays& a)
         e.col * 4, e.col * 4, e.col * 4, e.col * sizeof(float4), e.col * sizeof(float4), e.col * sizeof(float4),
         e.col * 4, e.col * 4,
         e.circle * 4, e.box * sizeof(float2), e.poly * 4, e.poly * 4, e.vert * sizeof(float2), e.vert * sizeof(float2),
-        e.mat * sizeof(float4), e.man * sizeof(Manifold), e.man * 4};
+        e.mat * sizeof(float4), e.man * sizeof(Manifold), e.man * 4, e.isle * sizeof(Manifold), e.isle * 4};
     uint64_t off = 0;
     for (uint32_t k = 0; k < NSEC; k++) {
         w.sec[k] = off;
@@ -359,6 +365,8 @@ StagedWorld stage_world(const PackedArrays& a)
     put(SEC_MATS, a.mats.data()); put(SEC_PREV, a.prev.data());
     if (a.pcol.size() == e.man) put(SEC_PREVCOLOR, a.pcol.data());
     else if (e.man) std::memset(w.blob.data() + w.sec[SEC_PREVCOLOR], 0xFF, sizes[SEC_PREVCOLOR]);   // NO_COLOR
+    put(SEC_ISLE, a.isle.data());
+    put(SEC_ISLEID, a.isleId.data());
     return w;
 }
 
@@ -489,6 +497,26 @@ struct ag2d_world {
     bool hintsReady = false;   // this step's lookup wrote the hints
     DBuf<uint4> listA, listB;
     DBuf<unsigned long long> bodyMax, bodyMask;
+    // Manifolds of sleeping islands (k_islands.cu): world-grouped records and the island (root body) of each, with
+    // the back buffers the sleep pass scatters into. isleUpper bounds the count as the host knows it (0: empty).
+    DBuf<Manifold> isle, bk_isle;
+    DBuf<uint32_t> isleId, bk_isleId, nIsle;
+    uint32_t isleUpper = 0;
+    // Restore scratch: staging flags / offsets / indices, the pair-key table (all keys empty between steps), the
+    // unclaimed records and their worlds, and counts [staged, unclaimed, kept, moved, staying].
+    DBuf<uint32_t> isleFlag, isleOff, isleFlag2, isleOff2, isleStage, isleSlot, isleConsumed, isleList, isleListWorld;
+    DBuf<unsigned long long> isleKeys;
+    DBuf<uint32_t> isleVals, isleCounts;
+    uint32_t isleHashCap = 0;
+    // Batches: the step's list with the restored records merged in by world (swapped in as 'manifolds' / 'color').
+    DBuf<Manifold> mergeMan;
+    DBuf<uint32_t> mergeHint;
+    // Sleep pass scratch over the step's list: stay / move flags and offsets, the island of each moving manifold, the
+    // worlds of the kept and moving records, and the compacted list with its colours.
+    DBuf<uint32_t> sleepStay, sleepMove, sleepStayOff, sleepMoveOff, sleepMoveIsland, sleepKeepWorld,
+        sleepMoveWorld, sleepColor;
+    DBuf<Manifold> sleepList;
+    bool prevHoldsSleepers = false;   // the warm-start list still holds records moved to the store (compactPrev)
     DBuf<Constraint> cons;
     DBuf<uint2> pairBodies;
     // Islands.
@@ -514,12 +542,13 @@ struct ag2d_world {
     uint32_t narrowThreads = 256;
     std::vector<uint32_t> hBodyStart, hColStart;     // [nWorlds + 1]
     DBuf<uint32_t> bodyWorld, colWorld, worldBodyStart, worldColStart, manSeg, nextWorld, worldDirty;
+    DBuf<uint32_t> isleSeg;                  // world starts of the sleeping islands' manifolds (server repacks)
     DBuf<uint32_t> teamWorld, teamOrder;     // solver teams: first world of each team; small then big, largest first
     DBuf<uint8_t> dynSimd, dynColSimd;               // SIMD-path flag of each work-list entry
     // Request-server engines: extents of the resident worlds, back buffers the repack gathers into, and the
     // staging upload of joining worlds.
     std::vector<WorldExtent> worldExt;
-    bool manSegFresh = false;   // manSeg describes prevManifolds (a batched step ran since the last repack)
+    bool manSegFresh = false;   // a batched step ran since the last repack (per-world manifold extents changed)
     DBuf<float4> bk_bvel, bk_bpos, bk_coff, bk_cpose, bk_caabb, bk_mats, out_vel, out_pos;
     DBuf<float2> bk_brot, bk_boxHalf, bk_polyVerts, bk_polyNormals;
     DBuf<float> bk_wrap, bk_bound, bk_timer, bk_cworldRot, bk_minExt, bk_circle;
@@ -656,46 +685,63 @@ struct ag2d_world {
             tPrev = now;
         };
         const uint32_t W0 = uint32_t(worldExt.size());
-        // Current extents of the warm-start manifolds.
+        compactPrev();
+        // Current extents of the warm-start manifolds and of the sleeping islands' manifolds (both world-grouped).
         if (W0 == 1) {
-            worldExt[0].man = prevCount;
-        } else if (W0 > 1 && manSegFresh) {
-            std::vector<uint32_t> seg(W0 + 1);
-            CK(cudaMemcpyAsync(seg.data(), manSeg.p, (W0 + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            uint32_t n[2] = {0, 0};
+            CK(cudaMemcpyAsync(n, nPrev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(n + 1, nIsle.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
-            for (uint32_t k = 0; k < W0; k++) worldExt[k].man = seg[k + 1] - seg[k];
+            worldExt[0].man = n[0];
+            worldExt[0].isle = n[1];
+        } else if (W0 > 1 && manSegFresh) {
+            isleSeg.reserve(W0 + 1);
+            const uint32_t g = gridFor(std::max<uint32_t>(manifoldCap, isleUpper));
+            k_manifold_segments<<<g, 256, 0, s>>>(prevManifolds.p, nPrev.p, cbody.p, bodyWorld.p, W0, manSeg.p);
+            k_manifold_segments<<<g, 256, 0, s>>>(isle.p, nIsle.p, cbody.p, bodyWorld.p, W0, isleSeg.p);
+            CK(cudaGetLastError());
+            std::vector<uint32_t> seg(W0 + 1), iseg(W0 + 1);
+            CK(cudaMemcpyAsync(seg.data(), manSeg.p, (W0 + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(iseg.data(), isleSeg.p, (W0 + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            for (uint32_t k = 0; k < W0; k++) {
+                worldExt[k].man = seg[k + 1] - seg[k];
+                worldExt[k].isle = iseg[k + 1] - iseg[k];
+            }
         }
         auto prefix = [](const std::vector<WorldExtent>& ex, uint32_t WorldExtent::*f) {
             std::vector<uint32_t> st(ex.size() + 1, 0);
             for (size_t i = 0; i < ex.size(); i++) st[i + 1] = st[i] + ex[i].*f;
             return st;
         };
-        static constexpr uint32_t WorldExtent::*kinds[8] = {&WorldExtent::body, &WorldExtent::col,
-                                                            &WorldExtent::circle, &WorldExtent::box,
-                                                            &WorldExtent::poly, &WorldExtent::vert,
-                                                            &WorldExtent::mat, &WorldExtent::man};
-        std::vector<uint32_t> oldStart[8], newStart[8];
+        constexpr int NK = 9;
+        static constexpr uint32_t WorldExtent::*kinds[NK] = {&WorldExtent::body, &WorldExtent::col,
+                                                             &WorldExtent::circle, &WorldExtent::box,
+                                                             &WorldExtent::poly, &WorldExtent::vert,
+                                                             &WorldExtent::mat, &WorldExtent::man,
+                                                             &WorldExtent::isle};
+        std::vector<uint32_t> oldStart[NK], newStart[NK];
         std::vector<WorldExtent> next;
         for (uint32_t k : keep) next.push_back(worldExt[k]);
         for (const StagedWorld* w : add) next.push_back(w->ext);
-        for (int c = 0; c < 8; c++) {
+        for (int c = 0; c < NK; c++) {
             oldStart[c] = prefix(worldExt, kinds[c]);
             newStart[c] = prefix(next, kinds[c]);
         }
         // Segments per kind (empty ones left out). A kept world's segment reads the current arrays from its old
         // start; a joining world's reads its staged sections (src = its index among the joining worlds). The
         // deltas shift the indices stored inside the elements to the new starts.
-        std::vector<GatherSeg> segs[8];
+        std::vector<GatherSeg> segs[NK];
         for (size_t j = 0; j < next.size(); j++) {
             const bool fresh = j >= keep.size();
             GatherSeg g{};
             g.fromNew = fresh ? 1u : 0u;
-            int32_t d[8];
-            for (int c = 0; c < 8; c++)
+            int32_t d[NK];
+            for (int c = 0; c < NK; c++)
                 d[c] = int32_t(newStart[c][j]) - (fresh ? 0 : int32_t(oldStart[c][keep[j]]));
             g.dBody = d[0]; g.dCol = d[1]; g.dCircle = d[2]; g.dBox = d[3]; g.dPoly = d[4]; g.dVert = d[5];
             g.dMat = d[6];
-            for (int c = 0; c < 8; c++) {
+            for (int c = 0; c < NK; c++) {
                 g.dst = newStart[c][j];
                 g.src = fresh ? uint32_t(j - keep.size()) : oldStart[c][keep[j]];
                 g.count = next[j].*kinds[c];
@@ -703,12 +749,12 @@ struct ag2d_world {
             }
         }
         std::vector<GatherSeg> allSegs;
-        uint32_t segOff[9] = {0};
-        for (int c = 0; c < 8; c++) {
+        uint32_t segOff[NK + 1] = {0};
+        for (int c = 0; c < NK; c++) {
             segOff[c] = uint32_t(allSegs.size());
             allSegs.insert(allSegs.end(), segs[c].begin(), segs[c].end());
         }
-        segOff[8] = uint32_t(allSegs.size());
+        segOff[NK] = uint32_t(allSegs.size());
         mark("plan");
         gatherSegs.upload(allSegs.data(), allSegs.size(), s);   // empty when every world leaves
         // Staging: each joining world's blob at a 256-byte aligned offset, one transfer each.
@@ -765,6 +811,8 @@ struct ag2d_world {
         run(materials, bk_mats, SEC_MATS, 6, GATHER_PLAIN);
         run(prevManifolds, bk_prev, SEC_PREV, 7, GATHER_PLAIN);
         run(prevColor, bk_prevColor, SEC_PREVCOLOR, 7, GATHER_PLAIN);
+        run(isle, bk_isle, SEC_ISLE, 8, GATHER_PLAIN);
+        run(isleId, bk_isleId, SEC_ISLEID, 8, GATHER_ISLAND);
         mark("gather");
         // Sizes, partition and per-world state.
         worldExt = next;
@@ -778,6 +826,8 @@ struct ag2d_world {
         for (const WorldExtent& e : next) nStatic += e.statics;
         prevCount = newStart[7].back();
         CK(cudaMemcpyAsync(nPrev.p, &prevCount, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        isleUpper = newStart[8].back();
+        CK(cudaMemcpyAsync(nIsle.p, &isleUpper, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
         nWorlds = std::max<uint32_t>(W, 1);
         hBodyStart = newStart[0];
         hColStart = newStart[1];
@@ -1006,15 +1056,17 @@ struct ag2d_world {
         h.nPolygons = nPolygons; h.nPolyVerts = nPolyVerts; h.nMaterialRows = nMaterialRows;
         h.nStatic = nStatic;
         h.lastManifolds = lastManifolds;
+        compactPrev();
         CK(cudaMemcpyAsync(&h.nPrev, nPrev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(&h.nIsle, nIsle.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
-        const uint64_t b = nBodies, c = nColliders, m = h.nPrev, wp = uint64_t(nWorlds) + 1;
+        const uint64_t b = nBodies, c = nColliders, m = h.nPrev, wp = uint64_t(nWorlds) + 1, si = h.nIsle;
         const uint64_t len[NCK] = {
             b * 16, b * 16, b * 8, b * 4, b * 4, b * 4, b, b * 4,
             c * 4, c * 4, c * 4, c * 16, c * 16, c * 16, c * 4, c * 4,
             uint64_t(nCircles) * 4, uint64_t(nBoxes) * 8, uint64_t(nPolygons) * 4, uint64_t(nPolygons) * 4,
             uint64_t(nPolyVerts) * 8, uint64_t(nPolyVerts) * 8, uint64_t(nMaterialRows) * 16, m * sizeof(Manifold),
-            m * 4, wp * 4, wp * 4};
+            m * 4, wp * 4, wp * 4, si * sizeof(Manifold), si * 4};
         uint64_t at = (sizeof(CkptHeader) + 255) & ~uint64_t(255);
         for (uint32_t k = 0; k < NCK; k++) {
             h.off[k] = at;
@@ -1041,6 +1093,9 @@ struct ag2d_world {
         if (nWorlds <= 1) { bs = {0, nBodies}; cs = {0, nColliders}; }
         std::memcpy(dst + h.off[CK_WBODY], bs.data(), h.len[CK_WBODY]);
         std::memcpy(dst + h.off[CK_WCOL], cs.data(), h.len[CK_WCOL]);
+        if (h.len[CK_ISLE]) CK(cudaMemcpyAsync(dst + h.off[CK_ISLE], isle.p, h.len[CK_ISLE], cudaMemcpyDeviceToHost, s));
+        if (h.len[CK_ISLEID])
+            CK(cudaMemcpyAsync(dst + h.off[CK_ISLEID], isleId.p, h.len[CK_ISLEID], cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
     }
 
@@ -1081,6 +1136,10 @@ struct ag2d_world {
             CK(cudaMemcpyAsync(prevColor.p, src + h.off[CK_PREVCOLOR], h.len[CK_PREVCOLOR], cudaMemcpyHostToDevice, s));
         prevCount = h.nPrev;
         CK(cudaMemcpyAsync(nPrev.p, &prevCount, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        up(isle, CK_ISLE, h.nIsle);
+        up(isleId, CK_ISLEID, h.nIsle);
+        isleUpper = h.nIsle;
+        CK(cudaMemcpyAsync(nIsle.p, &isleUpper, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
         const uint32_t ones = std::max<uint32_t>(nBodies, 1);
         k_fill_u32<<<gridFor(ones), 256, 0, s>>>(ccdHit.p, ones, ORDERED_ONE);
         CK(cudaGetLastError());
@@ -1168,11 +1227,34 @@ struct ag2d_world {
         bar.reserve(2);
         nManifolds.reserve(1);
         nPrev.reserve(1);
+        nIsle.reserve(1);
+        isleCounts.reserve(8);
         listCounts.reserve(3);
         colorCount.reserve(COLOR_SLOTS);
         colorStart.reserve(MAX_COLORS + 1);
         CK(cudaMemsetAsync(nPrev.p, 0, sizeof(uint32_t), stream));
         CK(cudaMemsetAsync(nManifolds.p, 0, sizeof(uint32_t), stream));
+        CK(cudaMemsetAsync(nIsle.p, 0, sizeof(uint32_t), stream));
+        CK(cudaMemsetAsync(isleCounts.p, 0, 8 * sizeof(uint32_t), stream));
+    }
+
+    // Restore scratch for a store of up to 'n' records; the key table starts empty (every key ~0, every value ~0).
+    void reserveIsleScratch(uint32_t n)
+    {
+        n = std::max<uint32_t>(n, 1);
+        for (auto* b : {&isleFlag, &isleOff, &isleFlag2, &isleOff2, &isleStage, &isleSlot, &isleConsumed, &isleList,
+                        &isleListWorld, &sleepKeepWorld})
+            b->reserve(n);
+        uint32_t cap = 16;
+        while (cap < 2 * n) cap <<= 1;
+        if (cap > isleHashCap) {
+            isleKeys.reserve(cap);
+            isleVals.reserve(cap);
+            isleHashCap = cap;
+            CK(cudaMemsetAsync(isleKeys.p, 0xFF, sizeof(unsigned long long) * cap, stream));
+            CK(cudaMemsetAsync(isleVals.p, 0xFF, sizeof(uint32_t) * cap, stream));
+        }
+        scanner.reserve(n);
     }
 
     void reserveCapacities(uint32_t pairCapNew, uint32_t manCapNew)
@@ -1253,6 +1335,8 @@ struct ag2d_world {
         for (size_t i = 0; i < a.mats.size(); i++)
             a.mats[i] = make_float4(o.materials[3 * i], o.materials[3 * i + 1], o.materials[3 * i + 2], 0.0f);
         a.prev.clear();
+        a.isle.clear();
+        a.isleId.clear();
     }
 
     // Uploads the host objects as the device state.
@@ -1315,6 +1399,8 @@ struct ag2d_world {
         reserveCapacities(std::max(pairCap, cap), std::max(manifoldCap, cap));
         CK(cudaMemsetAsync(nPrev.p, 0, sizeof(uint32_t), s));
         CK(cudaMemsetAsync(nManifolds.p, 0, sizeof(uint32_t), s));
+        CK(cudaMemsetAsync(nIsle.p, 0, sizeof(uint32_t), s));
+        isleUpper = 0;
         CK(cudaStreamSynchronize(s));
         hostDirty = false;
         listsDirty = true;
@@ -1339,6 +1425,7 @@ struct ag2d_world {
             return;
         }
         ensureUploaded();
+        compactPrev();
         const cudaStream_t s = stream;
         auto get = [&](auto& v, const auto* p, size_t n) {
             v.resize(n);
@@ -1358,6 +1445,11 @@ struct ag2d_world {
         CK(cudaStreamSynchronize(s));
         get(a.prev, prevManifolds.p, np);
         get(a.pcol, prevColor.p, np);
+        uint32_t ni = 0;
+        CK(cudaMemcpyAsync(&ni, nIsle.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        get(a.isle, isle.p, ni);
+        get(a.isleId, isleId.p, ni);
         CK(cudaStreamSynchronize(s));
     }
 
@@ -1653,6 +1745,157 @@ struct ag2d_world {
         pend(8);
     }
 
+    // Manifolds of the islands that woke this step join the list (k_islands.cu, restore): fresh manifolds of their
+    // pairs take the stored impulses; the rest are appended at the end of their world's segment (a batch's list is
+    // merged into mergeMan / mergeHint, which then become 'manifolds' / 'color').
+    void phaseRestore()
+    {
+        if (isleUpper == 0) return;
+        const cudaStream_t s = stream;
+        const DeviceWorld wv = view();
+        reserveIsleScratch(isleUpper);
+        uint32_t* cnt = isleCounts.p;
+        uint32_t* st = &dCounters.p->status;
+        const uint32_t gi = gridFor(isleUpper), gm = gridFor(manifoldCap);
+        k_isle_stage_flags<<<gi, 256, 0, s>>>(wv, isle.p, isleId.p, nIsle.p, wakeIsland.p, isleFlag.p);
+        scanner.run(isleFlag.p, isleOff.p, isleUpper, cnt + 0, s, nIsle.p);
+        k_isle_stage<<<gi, 256, 0, s>>>(isle.p, nIsle.p, isleFlag.p, isleOff.p, isleStage.p, isleSlot.p,
+                                        isleConsumed.p, isleKeys.p, isleVals.p, isleHashCap, st);
+        k_isle_take<<<gm, 256, 0, s>>>(manifolds.p, nManifolds.p, isle.p, isleStage.p, cnt + 0, isleKeys.p, isleVals.p,
+                                       isleHashCap, isleConsumed.p);
+        k_isle_unclaimed_flags<<<gi, 256, 0, s>>>(cnt + 0, isleConsumed.p, isleSlot.p, isleKeys.p, isleVals.p,
+                                                  isleFlag2.p);
+        scanner.run(isleFlag2.p, isleOff2.p, isleUpper, cnt + 1, s, cnt + 0);
+        k_isle_unclaimed<<<gi, 256, 0, s>>>(wv, isle.p, cnt + 0, isleStage.p, isleFlag2.p, isleOff2.p, isleList.p,
+                                            isleListWorld.p);
+        uint32_t* hint = hintsReady ? color.p : nullptr;
+        if (nWorlds > 1) {
+            mergeMan.reserve(manifoldCap);
+            mergeHint.reserve(manifoldCap);
+            k_manifold_segments<<<gm, 256, 0, s>>>(manifolds.p, nManifolds.p, cbody.p, bodyWorld.p, nWorlds, manSeg.p);
+            k_isle_merge<<<gm, 256, 0, s>>>(wv, manifolds.p, hint, nManifolds.p, manSeg.p, isle.p, isleList.p,
+                                            isleListWorld.p, cnt + 1, manifoldCap, mergeMan.p,
+                                            hint ? mergeHint.p : nullptr, st);
+            swap_bufs(manifolds, mergeMan);
+            if (hint) swap_bufs(color, mergeHint);
+            launches += 2;
+        } else {
+            k_isle_append<<<gi, 256, 0, s>>>(manifolds.p, nManifolds.p, manifoldCap, hint, isle.p, isleList.p, cnt + 1,
+                                             st);
+            launches += 1;
+        }
+        k_isle_count<<<1, 32, 0, s>>>(nManifolds.p, cnt + 0, cnt + 1, manifoldCap, dCounters.p);
+        CK(cudaGetLastError());
+        launches += 7;
+    }
+
+    // After a step in which islands woke or fell asleep (k_islands.cu, sleep): the store drops the woken islands'
+    // records and takes the manifolds of the bodies now asleep from the warm-start list ('prevManifolds'). The list
+    // itself keeps those records until it is read (compactPrev): the next step cannot regenerate their pairs (both
+    // bodies asleep, or one asleep and one static), so they warm-start nothing and give no colour hint, and the
+    // next step replaces the list anyway.
+    void phaseSleepStore(uint32_t storedBefore, bool slept, bool removals)
+    {
+        const cudaStream_t s = stream;
+        const DeviceWorld wv = view();
+        const uint32_t listN = std::max<uint32_t>(prevCount, 1), stored = std::max<uint32_t>(storedBefore, 1);
+        const uint64_t need = uint64_t(storedBefore) + (slept ? prevCount : 0);
+        if (need > 0xFFFFFFFFull) throw ApiError(AG2D_ERR_CAPACITY, "sleeping-island store would exceed 2^32 records");
+        // Both store buffers keep one capacity (they trade places), grown together by half again when short, so a
+        // steady store reallocates neither.
+        if (isle.n < need || bk_isle.n < need || isleId.n < need || bk_isleId.n < need || !isle.p || !bk_isle.p) {
+            const size_t cap = std::max<size_t>({size_t(need), size_t(1), isle.n + isle.n / 2});
+            growKeep(isle, cap);
+            growKeep(isleId, cap);
+            DBuf<Manifold> nb;
+            nb.reserve(cap);
+            swap_bufs(bk_isle, nb);
+            DBuf<uint32_t> nbi;
+            nbi.reserve(cap);
+            swap_bufs(bk_isleId, nbi);
+        }
+        reserveIsleScratch(stored);
+        for (auto* b : {&sleepStay, &sleepMove, &sleepMoveOff, &sleepMoveIsland, &sleepMoveWorld}) b->reserve(manifoldCap);
+        scanner.reserve(std::max(listN, stored));
+        uint32_t* cnt = isleCounts.p;
+        const bool batch = nWorlds > 1, checkAlive = nDestroyed > 0;
+        const uint32_t gi = gridFor(stored), gl = gridFor(listN);
+        if (slept) {
+            k_isle_move_flags<<<gl, 256, 0, s>>>(wv, prevManifolds.p, nPrev.p, sleepStay.p, sleepMove.p,
+                                                 sleepMoveIsland.p);
+            scanner.run(sleepMove.p, sleepMoveOff.p, listN, cnt + 3, s, nPrev.p);
+        } else {
+            CK(cudaMemsetAsync(cnt + 3, 0, sizeof(uint32_t), s));
+        }
+        if (!batch && !removals) {
+            // A single world that only gains records: they go after the kept ones, in place.
+            k_isle_append_moved<<<gl, 256, 0, s>>>(prevManifolds.p, nPrev.p, sleepMove.p, sleepMoveOff.p,
+                                                  sleepMoveIsland.p, nIsle.p, isle.p, isleId.p);
+            k_isle_add_count<<<1, 32, 0, s>>>(nIsle.p, cnt + 3);
+            CK(cudaGetLastError());
+            launches += slept ? 4 : 2;
+        } else {
+            k_isle_keep_flags<<<gi, 256, 0, s>>>(wv, isle.p, isleId.p, nIsle.p, wakeIsland.p, checkAlive ? 1u : 0u,
+                                                 isleFlag.p);
+            scanner.run(isleFlag.p, isleOff.p, stored, cnt + 2, s, nIsle.p);
+            if (batch)
+                k_isle_sleep_worlds<<<gridFor(stored + listN), 256, 0, s>>>(wv, isle.p, nIsle.p, isleFlag.p,
+                                                                           isleOff.p, prevManifolds.p, nPrev.p,
+                                                                           slept ? sleepMove.p : nullptr,
+                                                                           sleepMoveOff.p, sleepKeepWorld.p,
+                                                                           sleepMoveWorld.p);
+            k_isle_store_scatter<<<gridFor(stored + listN), 256, 0, s>>>(
+                wv, isle.p, isleId.p, nIsle.p, isleFlag.p, isleOff.p, cnt + 2, prevManifolds.p, nPrev.p,
+                slept ? sleepMove.p : nullptr, sleepMoveOff.p, cnt + 3, sleepMoveIsland.p,
+                batch ? sleepKeepWorld.p : nullptr, batch ? sleepMoveWorld.p : nullptr, bk_isle.p, bk_isleId.p);
+            k_isle_store_count<<<1, 32, 0, s>>>(cnt + 2, cnt + 3, nIsle.p);
+            CK(cudaGetLastError());
+            launches += (slept ? 2 : 0) + (batch ? 5 : 4);
+            swap_bufs(isle, bk_isle);
+            swap_bufs(isleId, bk_isleId);
+        }
+        if (slept) prevHoldsSleepers = true;
+        isleUpper = uint32_t(need);
+    }
+
+    // Drops from the warm-start list the manifolds whose bodies sleep (they are in the store) or were destroyed:
+    // the list as the reference's getBodyCollisionData holds it after a step. Called before the list is read or
+    // packed.
+    void compactPrev()
+    {
+        if (!prevHoldsSleepers) return;
+        prevHoldsSleepers = false;
+        const cudaStream_t s = stream;
+        const uint32_t listN = std::max<uint32_t>(prevCount, 1);
+        for (auto* b : {&sleepStay, &sleepMove, &sleepStayOff, &sleepMoveIsland, &sleepColor}) b->reserve(manifoldCap);
+        sleepList.reserve(manifoldCap);
+        scanner.reserve(listN);
+        uint32_t* cnt = isleCounts.p;
+        k_isle_move_flags<<<gridFor(listN), 256, 0, s>>>(view(), prevManifolds.p, nPrev.p, sleepStay.p, sleepMove.p,
+                                                         sleepMoveIsland.p);
+        scanner.run(sleepStay.p, sleepStayOff.p, listN, cnt + 4, s, nPrev.p);
+        k_isle_list_scatter<<<gridFor(listN), 256, 0, s>>>(prevManifolds.p, prevColor.p, nPrev.p, sleepStay.p,
+                                                           sleepStayOff.p, sleepList.p, sleepColor.p);
+        CK(cudaMemcpyAsync(nPrev.p, cnt + 4, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        CK(cudaGetLastError());
+        launches += 3;
+        swap_bufs(prevManifolds, sleepList);
+        swap_bufs(prevColor, sleepColor);
+        CK(cudaStreamSynchronize(s));
+    }
+
+    // Grows a buffer to at least 'count' elements, keeping its contents.
+    template <class T>
+    void growKeep(DBuf<T>& b, size_t count)
+    {
+        if (b.n >= count && b.p) return;
+        DBuf<T> nb;
+        nb.reserve(count);
+        if (b.p) CK(cudaMemcpyAsync(nb.p, b.p, b.n * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+        CK(cudaStreamSynchronize(stream));
+        swap_bufs(b, nb);
+    }
+
     void phaseSolve()
     {
         const cudaStream_t s = stream;
@@ -1851,16 +2094,30 @@ struct ag2d_world {
         std::vector<float> timer = download(sleepTimer.p, nBodies, s), wraps = download(wrapCount.p, nBodies, s);
         const std::vector<uint32_t> island = download(sleepIsland.p, nBodies, s);
         HostObjects& o = objects;
-        auto wake = [&](uint32_t b) {   // the body's whole sleeping island (k_wake_apply's rule)
-            if (state[b] != STATE_SLEEPING) return;
-            const uint32_t root = island[b];
+        std::vector<uint32_t> wokenRoots;   // islands woken, in waking order
+        auto wakeIsland = [&](uint32_t root) {   // every sleeping body of the island (k_wake_apply's rule)
+            bool any = false;
             for (uint32_t i = 0; i < nBodies; i++)
-                if (state[i] == STATE_SLEEPING && island[i] == root) { state[i] = STATE_DYNAMIC; timer[i] = 0.0f; }
+                if (state[i] == STATE_SLEEPING && island[i] == root) { state[i] = STATE_DYNAMIC; timer[i] = 0.0f; any = true; }
+            if (any) wokenRoots.push_back(root);
         };
+        auto wake = [&](uint32_t b) {
+            if (state[b] == STATE_SLEEPING) wakeIsland(island[b]);
+        };
+        // Static bodies whose pose, mass or existence a command changes (ObjectManager::applyCommand,
+        // ObjectManager.cpp:678-687, and destroyColliderInternal): their colliders count as edited.
+        std::vector<uint8_t> editedBody(nBodies, 0);
+        bool anyEdited = false;
         for (const BodyCommand& c : commands) {
             const uint32_t b = o.indexOf(c.handle);
             if (b >= nBodies || b >= o.bodies.size() || state[b] == STATE_DESTROYED) continue;
             HBody& hb = o.bodies[b];
+            if (state[b] == STATE_STATIC &&
+                (c.kind == AG2D_COMMAND_DESTROY || c.kind == AG2D_COMMAND_POSITION ||
+                 c.kind == AG2D_COMMAND_ROTATION || c.kind == AG2D_COMMAND_MASS)) {
+                editedBody[b] = 1;
+                anyEdited = true;
+            }
             wake(b);
             switch (c.kind) {
             case AG2D_COMMAND_DESTROY:
@@ -1916,6 +2173,7 @@ struct ag2d_world {
             }
         }
         commands.clear();
+        restoreWokenIslands(state, timer, island, wokenRoots, editedBody, anyEdited);
         if (nBodies) {
             CK(cudaMemcpyAsync(bvel.p, vel.data(), nBodies * sizeof(float4), cudaMemcpyHostToDevice, s));
             CK(cudaMemcpyAsync(bpos.p, pos.data(), nBodies * sizeof(float4), cudaMemcpyHostToDevice, s));
@@ -1930,6 +2188,91 @@ struct ag2d_world {
         listsDirty = true;
         otherDirty = true;
         fullPose = true;
+    }
+
+    // The command path's part of Simulation::flushCommands (Simulation.cpp:454-461): islands touching an edited
+    // static body wake (wakeIslandsOfEditedStatics, :463-483, with takeContactsOfColliders,
+    // NarrowPhaseCollisionDetector.cpp:415-456: their stored manifolds with an edited collider are dropped, awake
+    // bodies touching one restart their sleep timers), then the stored manifolds of every woken island join the
+    // warm-start list (wakeContactData, :338-412; none of their pairs can be in that list, so all are appended). A
+    // single world, on the host: body commands are rare.
+    void restoreWokenIslands(std::vector<uint8_t>& state, std::vector<float>& timer, const std::vector<uint32_t>& island,
+                             std::vector<uint32_t>& wokenRoots, const std::vector<uint8_t>& editedBody, bool anyEdited)
+    {
+        const cudaStream_t s = stream;
+        compactPrev();
+        uint32_t counts[2] = {0, 0};
+        CK(cudaMemcpyAsync(counts, nIsle.p, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(counts + 1, nPrev.p, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        const uint32_t ni = counts[0], np = counts[1];
+        if (ni == 0 && !anyEdited) return;
+        std::vector<Manifold> store = download(isle.p, ni, s), prev = download(prevManifolds.p, np, s);
+        std::vector<uint32_t> storeId = download(isleId.p, ni, s), prevCol = download(prevColor.p, np, s);
+        const std::vector<uint32_t> owner = download(cbody.p, nColliders, s);
+        auto edited = [&](uint32_t c) { return c < nColliders && editedBody[owner[c]] != 0; };
+        std::vector<uint8_t> drop(ni, 0);
+        if (anyEdited) {
+            std::vector<uint32_t> hit;   // islands with a stored manifold on an edited collider, in island order
+            for (uint32_t r = 0; r < ni; r++) {
+                if (!edited(store[r].a) && !edited(store[r].b)) continue;
+                drop[r] = 1;
+                if (std::find(hit.begin(), hit.end(), storeId[r]) == hit.end()) hit.push_back(storeId[r]);
+            }
+            std::sort(hit.begin(), hit.end());
+            for (uint32_t root : hit) {
+                bool any = false;
+                for (uint32_t i = 0; i < nBodies; i++)
+                    if (state[i] == STATE_SLEEPING && island[i] == root) { state[i] = STATE_DYNAMIC; timer[i] = 0.0f; any = true; }
+                if (any) wokenRoots.push_back(root);
+            }
+            for (const Manifold& m : prev) {
+                const bool eA = edited(m.a), eB = edited(m.b);
+                if (eA == eB) continue;
+                const uint32_t partner = owner[eA ? m.b : m.a];
+                if (state[partner] == STATE_DYNAMIC) timer[partner] = 0.0f;
+            }
+        }
+        // Woken islands' records (colliders alive) in island order, first record of a pair only.
+        std::vector<uint8_t> woken(nBodies, 0);
+        for (uint32_t root : wokenRoots) if (root < nBodies) woken[root] = 1;
+        auto alive = [&](uint32_t c) { return c < nColliders && state[owner[c]] != STATE_DESTROYED; };
+        std::vector<unsigned long long> keys;
+        bool storeChanged = anyEdited;
+        for (uint32_t root : wokenRoots) {
+            for (uint32_t r = 0; r < ni; r++) {
+                if (drop[r] || storeId[r] != root) continue;
+                drop[r] = 1;
+                storeChanged = true;
+                const Manifold& m = store[r];
+                if (!alive(m.a) || !alive(m.b)) continue;
+                const unsigned long long key = (uint64_t(std::min(m.a, m.b)) << 32) | std::max(m.a, m.b);
+                if (std::find(keys.begin(), keys.end(), key) != keys.end()) continue;
+                keys.push_back(key);
+                prev.push_back(m);
+                prevCol.push_back(NO_COLOR);
+            }
+        }
+        if (!storeChanged) return;
+        std::vector<Manifold> keptRec;
+        std::vector<uint32_t> keptId;
+        for (uint32_t r = 0; r < ni; r++)
+            if (!drop[r]) { keptRec.push_back(store[r]); keptId.push_back(storeId[r]); }
+        const uint32_t nk = uint32_t(keptRec.size()), nnp = uint32_t(prev.size());
+        if (nnp > manifoldCap) reserveCapacities(std::max(nnp, pairCap), nnp);
+        if (nk) {
+            CK(cudaMemcpyAsync(isle.p, keptRec.data(), nk * sizeof(Manifold), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(isleId.p, keptId.data(), nk * 4, cudaMemcpyHostToDevice, s));
+        }
+        if (nnp) {
+            CK(cudaMemcpyAsync(prevManifolds.p, prev.data(), nnp * sizeof(Manifold), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(prevColor.p, prevCol.data(), nnp * 4, cudaMemcpyHostToDevice, s));
+        }
+        CK(cudaMemcpyAsync(nIsle.p, &nk, 4, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(nPrev.p, &nnp, 4, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+        isleUpper = nk;
+        prevCount = nnp;
     }
 
     // One fixed step (Simulation::physicsStep order, Simulation.cpp:255-351).
@@ -1948,6 +2291,7 @@ struct ag2d_world {
             if (listsDirty) rebuildLists();
             const cudaStream_t s = stream;
             CK(cudaMemsetAsync(dCounters.p, 0, sizeof(StepCounters), s));
+            CK(cudaMemcpyAsync(&dCounters.p->stored, nIsle.p, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
             snapshot(false);
             if (settings.ccd && nColliders) {
                 // The poses continuous collision sweeps from; a retried step starts again from the same poses.
@@ -1973,6 +2317,7 @@ struct ag2d_world {
             phaseBroad();
             phaseNarrow();
             phaseWake();
+            phaseRestore();
             phaseSolve();
             phaseIslands();
             readCounters();
@@ -2010,6 +2355,14 @@ struct ag2d_world {
             CK(cudaMemcpyAsync(nPrev.p, nManifolds.p, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
             lastManifolds = hCounters->manifolds;
             prevCount = std::min(lastManifolds, manifoldCap);
+            // The store as the step began (the restore reads it, the sleep pass rewrites it).
+            isleUpper = hCounters->stored;
+            prevHoldsSleepers = false;   // the list is this step's
+            {
+                // Records leave the store when their island woke (staged by the restore) or a collider is gone.
+                const bool removals = hCounters->staged > 0 || (nDestroyed > 0 && hCounters->stored > 0);
+                if (hCounters->slept || removals) phaseSleepStore(hCounters->stored, hCounters->slept > 0, removals);
+            }
             if (hCounters->topoDirty) {
                 // Woken or slept bodies: refresh the poses of every collider at the post-step state (the reference
                 // rebuilds its spatial data in postUpdate, Simulation.cpp:640-647), then the work lists and the
@@ -2397,7 +2750,7 @@ int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out)
         out->woke = c.woke; out->slept = c.slept; out->warm_hits = c.warmHits;
         out->sleeping = world->nBodies - world->nDynBody - world->nStatic - world->nDestroyed;
         out->ccd_hits = c.ccdHits;
-        out->reserved = 0;
+        out->restored = c.restored;
         out->steps = world->stepsTaken;
         out->launches = world->launches;
         out->list_rebuilds = world->listRebuilds;
@@ -2661,9 +3014,11 @@ static std::vector<uint8_t> read_field(ag2d_world& w, int32_t field, bool sizeOn
         return get(w.nWorlds > 1 ? w.dynTree.sortedKey.p : w.dynTree.keys.p, uint32_t(w.dynTree.n));
     case AG2D_PAIRS: return get(w.pairs.p, std::min(devCount(&w.dCounters.p->pairs), w.pairCap));
     case AG2D_MANIFOLDS: return get(w.manifolds.p, devCount(w.nManifolds.p));
-    case AG2D_PREV_MANIFOLDS: return get(w.prevManifolds.p, devCount(w.nPrev.p));
+    case AG2D_PREV_MANIFOLDS: w.compactPrev(); return get(w.prevManifolds.p, devCount(w.nPrev.p));
     case AG2D_SOLVE_ORDER: return get(w.order.p, devCount(w.nManifolds.p));
     case AG2D_COLOR_STARTS: return get(w.colorStart.p, devCount(&w.dCounters.p->colors) + 1);
+    case AG2D_ISLAND_MANIFOLDS: return get(w.isle.p, devCount(w.nIsle.p));
+    case AG2D_ISLAND_IDS: return get(w.isleId.p, devCount(w.nIsle.p));
     default: throw ApiError(AG2D_ERR_INVALID_ARG, "unknown field " + std::to_string(field));
     }
 }
@@ -2869,7 +3224,30 @@ int32_t ag2d_world_write(ag2d_world* world, int32_t field, const void* src, uint
             const bool prev = field == AG2D_PREV_MANIFOLDS;
             if (n) CK(cudaMemcpyAsync(prev ? w.prevManifolds.p : w.manifolds.p, src, bytes, cudaMemcpyHostToDevice, s));
             CK(cudaMemcpyAsync(prev ? w.nPrev.p : w.nManifolds.p, &n, 4, cudaMemcpyHostToDevice, s));
-            if (prev) w.prevCount = n;
+            if (prev) {
+                w.prevCount = n;
+                w.prevHoldsSleepers = false;
+                // Written manifolds carry no solver colour: no colouring hints from them.
+                if (n) CK(cudaMemsetAsync(w.prevColor.p, 0xFF, sizeof(uint32_t) * n, s));
+            }
+            break;
+        }
+        case AG2D_ISLAND_MANIFOLDS: {   // the store's records; their islands follow with AG2D_ISLAND_IDS
+            const uint32_t n = uint32_t(bytes / sizeof(Manifold));
+            w.isle.reserve(std::max<uint32_t>(n, 1));
+            w.isleId.reserve(std::max<uint32_t>(n, 1));
+            if (n) CK(cudaMemcpyAsync(w.isle.p, src, bytes, cudaMemcpyHostToDevice, s));
+            CK(cudaMemsetAsync(w.isleId.p, 0xFF, sizeof(uint32_t) * std::max<uint32_t>(n, 1), s));
+            CK(cudaMemcpyAsync(w.nIsle.p, &n, 4, cudaMemcpyHostToDevice, s));
+            w.isleUpper = n;
+            break;
+        }
+        case AG2D_ISLAND_IDS: {
+            uint32_t n = 0;
+            CK(cudaMemcpyAsync(&n, w.nIsle.p, 4, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            if (bytes != uint64_t(n) * 4) throw ApiError(AG2D_ERR_INVALID_ARG, "one island per stored manifold");
+            if (n) CK(cudaMemcpyAsync(w.isleId.p, src, bytes, cudaMemcpyHostToDevice, s));
             break;
         }
         default: throw ApiError(AG2D_ERR_INVALID_ARG, "field is not writable");
@@ -2912,6 +3290,10 @@ int32_t ag2d_world_run_phase(ag2d_world* world, int32_t phase)
             w.phasePose(false);
             w.phaseBroad();
             w.phaseNarrow(false);
+            break;
+        case AG2D_PHASE_WAKE:
+            w.phaseWake();
+            w.phaseRestore();
             break;
         case AG2D_PHASE_SOLVE: w.phaseSolve(); break;
         case AG2D_PHASE_ISLANDS: w.phaseIslands(); break;
@@ -2991,6 +3373,15 @@ int32_t ag2d_batch_create(ag2d_world* const* worlds, uint32_t count, ag2d_batch*
                                    e.stream));
         CK(cudaMemcpyAsync(e.nPrev.p, &np, sizeof(uint32_t), cudaMemcpyHostToDevice, e.stream));
         e.prevCount = np;
+        const uint32_t ni = uint32_t(all.isle.size());   // sleeping islands' manifolds, world after world
+        e.isle.reserve(std::max<uint32_t>(ni, 1));
+        e.isleId.reserve(std::max<uint32_t>(ni, 1));
+        if (ni) {
+            CK(cudaMemcpyAsync(e.isle.p, all.isle.data(), ni * sizeof(Manifold), cudaMemcpyHostToDevice, e.stream));
+            CK(cudaMemcpyAsync(e.isleId.p, all.isleId.data(), ni * 4, cudaMemcpyHostToDevice, e.stream));
+        }
+        CK(cudaMemcpyAsync(e.nIsle.p, &ni, sizeof(uint32_t), cudaMemcpyHostToDevice, e.stream));
+        e.isleUpper = ni;
         CK(cudaStreamSynchronize(e.stream));
         *out = b.release();
     });
@@ -3060,6 +3451,31 @@ int32_t ag2d_batch_read(ag2d_batch* batch, uint32_t world, int32_t field, void* 
             }
             out.resize(mine.size() * sizeof(Manifold));
             if (!mine.empty()) std::memcpy(out.data(), mine.data(), out.size());
+        } else if (field == AG2D_ISLAND_MANIFOLDS || field == AG2D_ISLAND_IDS) {
+            // The world's stored records (collider indices and island roots made world-local).
+            uint64_t size = 0;
+            const std::vector<uint8_t> rec = read_field(e, AG2D_ISLAND_MANIFOLDS, false, &size);
+            const std::vector<uint8_t> ids = read_field(e, AG2D_ISLAND_IDS, false, &size);
+            const Manifold* m = reinterpret_cast<const Manifold*>(rec.data());
+            const uint32_t* id = reinterpret_cast<const uint32_t*>(ids.data());
+            const size_t n = rec.size() / sizeof(Manifold);
+            std::vector<Manifold> mine;
+            std::vector<uint32_t> mineId;
+            for (size_t i = 0; i < n; i++) {
+                if (m[i].a < c0 || m[i].a >= c1) continue;
+                Manifold x = m[i];
+                x.a -= c0;
+                x.b -= c0;
+                mine.push_back(x);
+                mineId.push_back(id[i] == 0xFFFFFFFFu ? id[i] : id[i] - b0);
+            }
+            if (field == AG2D_ISLAND_MANIFOLDS) {
+                out.resize(mine.size() * sizeof(Manifold));
+                if (!mine.empty()) std::memcpy(out.data(), mine.data(), out.size());
+            } else {
+                out.resize(mineId.size() * 4);
+                if (!mineId.empty()) std::memcpy(out.data(), mineId.data(), out.size());
+            }
         } else {
             throw ApiError(AG2D_ERR_UNSUPPORTED, "field is not readable per world of a batch");
         }
@@ -3109,7 +3525,8 @@ int32_t ag2d_batch_restore(const void* src, uint64_t bytes, int32_t device, ag2d
                 throw ApiError(AG2D_ERR_INVALID_ARG, "checkpoint section out of range");
         if (h.len[CK_WBODY] != (uint64_t(std::max<uint32_t>(h.nWorlds, 1)) + 1) * 4 ||
             h.len[CK_WCOL] != h.len[CK_WBODY] || h.len[CK_VEL] != uint64_t(h.nBodies) * 16 ||
-            h.len[CK_CBODY] != uint64_t(h.nColliders) * 4)
+            h.len[CK_CBODY] != uint64_t(h.nColliders) * 4 || h.len[CK_ISLE] != uint64_t(h.nIsle) * sizeof(Manifold) ||
+            h.len[CK_ISLEID] != uint64_t(h.nIsle) * 4 || h.len[CK_PREV] != uint64_t(h.nPrev) * sizeof(Manifold))
             throw ApiError(AG2D_ERR_INVALID_ARG, "checkpoint sizes inconsistent");
         ag2d_world_settings st = h.settings;
         if (device >= 0) st.device = device;

@@ -201,8 +201,13 @@ uint32_t HostObjects::appendCollider(uint32_t body, float locX, float locY, floa
 {
     // ObjectManager::createColliderInternal + placeNewCollider (ObjectManager.cpp:522-533, 1103-1108); comOffset =
     // localOffset - body local centre of mass (refreshComOffset, :17-22).
+    // The local rotation is stored wrapped into [0, 2pi) (ColliderSoA::append, SoA/ColliderSoA.cpp:25-27); the
+    // polygon recentring before this call used the rotation as given.
+    const float twoPi = 6.28318548f;   // 2 * float(pi)
+    float wrapped = std::fmod(localRot, twoPi);
+    if (wrapped < 0.0f) wrapped += twoPi;
     HCollider c;
-    c.body = body; c.locX = locX; c.locY = locY; c.localRot = localRot; c.material = material;
+    c.body = body; c.locX = locX; c.locY = locY; c.localRot = wrapped; c.material = material;
     c.type = type; c.shape = shape; c.minExtent = minExt; c.maxExtent = maxExt;
     c.comOffX = locX - bodies[body].lcomX;
     c.comOffY = locY - bodies[body].lcomY;

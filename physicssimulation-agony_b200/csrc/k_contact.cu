@@ -176,16 +176,6 @@ __global__ void k_narrow(DeviceWorld w, const uint2* __restrict__ pairs, const u
 // same ordered pair takes the flagged manifold's impulses of the contacts with equal ids (finalizeResults,
 // :749-766). Every new manifold whose pair was there also takes that manifold's colour as its colouring hint.
 // ---------------------------------------------------------------------------------------------------------------
-__device__ __forceinline__ unsigned long long pair_key(uint32_t a, uint32_t b)
-{
-    const uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
-    return (static_cast<unsigned long long>(lo) << 32) | hi;
-}
-__device__ __forceinline__ uint32_t slot_of(unsigned long long key, uint32_t capacity)
-{
-    const uint32_t shift = 64u - (31u - __clz(capacity));   // capacity is a power of two
-    return static_cast<uint32_t>((key * 0x9E3779B97F4A7C15ull) >> shift) & (capacity - 1u);
-}
 
 __global__ void k_warm_insert(const Manifold* __restrict__ prev, const uint32_t* __restrict__ nPrev,
                               unsigned long long* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t capacity,

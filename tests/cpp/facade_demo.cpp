@@ -114,7 +114,10 @@ int main()
                                                                 bp::BvhTreeTypeFlag::All, all);
     // One collider per live body plus the dumbbell's two wheels, all inside the huge box; the destroyed body's
     // collider is in no tree.
-    if (all.size() != bodies.getCount() - 1 + 2) return 6;
+    if (all.size() != bodies.getCount() - 1 + 2) {
+        std::printf("colliders found %zu, bodies %u\n", all.size(), bodies.getCount());
+        return 6;
+    }
     std::printf("ok %u %zu %.3f %zu %zu %zu\n", bodies.getCount(), maxManifolds, meanY / double(bodies.getCount()),
                 found.size(), touching.size(), all.size());
     return bodies.getCount() == uint32_t(created) ? 0 : 4;

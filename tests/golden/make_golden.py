@@ -15,6 +15,9 @@ Fixtures:
     wrap_edge.npz           body rotations around wrap boundaries (SIMD body and scalar tail)
     traj_c1_n256.npz        600-step trajectory statistics of a 256-polygon scene
     traj_c1_n2048.npz       the same statistics of the full c1 configuration (2,048 polygons, seed 0, 600 steps)
+    towers_s0_step33.npz    40 three-box towers: the step in which 36 of them fall asleep (their manifolds go to
+                            the sleeping-island store), with the store after the step
+    towers_s0_step140.npz   the same scene: the step in which four towers wake and their stored manifolds return
     capsules_n1500_s0_step300.npz  capsules with circles, boxes and polygons in a U container (every shape pair),
                                phase taps of step 301
     c2_n20000_s2_step420.npz   20,000 bodies of the c2 mix (500 columns x 40 rows) in a U container, phase taps of step 421 (the
@@ -123,11 +126,12 @@ def wrap_fixture(path):
 
 
 def trajectory_stats(sim, steps):
-    """Per-step: momentum (sum m v), kinetic energy, max manifold depth, manifold count, sleeping bodies; and, since
+    """Per-step: momentum (sum m v), kinetic energy, max manifold depth, manifold count, the manifolds stored for
+    sleeping islands, sleeping bodies; and, since
     bodies near the ends of the ground can slide off and fall without limit, the kinetic energy of the bodies still
     at or above the ground's top ("ke_on": centre of mass above y = -1) and the number that have fallen off
     ("fallen": below y = -10)."""
-    out = {k: [] for k in ("px", "py", "ke", "max_depth", "manifolds", "sleeping", "ke_on", "fallen")}
+    out = {k: [] for k in ("px", "py", "ke", "max_depth", "manifolds", "sleeping", "ke_on", "fallen", "stored")}
     for _ in range(steps):
         sim.update(1)
         sim.dump_state("t.")
@@ -145,6 +149,7 @@ def trajectory_stats(sim, steps):
         depth = sim.blob("t.man.depth")
         out["max_depth"].append(float(depth.max()) if depth.size else 0.0)
         out["manifolds"].append(int(depth.size))
+        out["stored"].append(int(sim.blob("t.isle.count").size))   # manifolds of sleeping islands
         gs = sim.blob("t.body.groupStarts")
         out["sleeping"].append(int(gs[2] - gs[1]))
     return {k: np.asarray(v) for k, v in out.items()}
@@ -268,6 +273,12 @@ FIXTURES = {
                                                         store_once=True),
     "capsules_n1500_s0_step300.npz": lambda p: phase_fixture(scenes.make_capsule_mix(1500, 0), 300, p,
                                                             store_once=True),
+    # Sleeping islands' manifolds: 36 towers fall asleep in step 34 (108 records move to the store); four towers
+    # wake in step 141 (12 stored records join the solver's list).
+    "towers_s0_step33.npz": lambda p: phase_fixture(scenes.make_towers(seed=0), 33, p,
+                                                    PHASE_PREFIXES + ("post.isle.",)),
+    "towers_s0_step140.npz": lambda p: phase_fixture(scenes.make_towers(seed=0), 140, p,
+                                                     PHASE_PREFIXES + ("post.isle.",)),
     "cossin_edge.npz": cossin_fixture,
     "wrap_edge.npz": wrap_fixture,
     "traj_c1_n256.npz": trajectory_fixture,

@@ -109,7 +109,9 @@ def test_autotune_does_not_change_results():
     assert t["team_colliders"] in (128, 256, 512, 1024, 2048) and t["team_threads"] in (64, 128, 256, 512)
     assert t["query_threads"] in (64, 128, 256) and t["narrow_threads"] in (128, 256, 512)
     assert t["team_cons_on_chip"] in (0, 1)
-    plain.step(1 + 19 * 2)
+    # One step, then per candidate one untimed and one timed step; the worlds larger than the chosen team size add
+    # the four large-team modes. The tuned engine's own step count says how many ran.
+    plain.step(int(tuned.counters()["steps"]))
     for k in range(len(sc)):
         for f in BODY_FIELDS:
             assert np.array_equal(_bits(tuned.read(k, f)), _bits(plain.read(k, f))), (k, f)

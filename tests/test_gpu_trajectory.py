@@ -12,7 +12,8 @@ tolerance written here:
   - momentum: horizontal momentum stays below 3 % of the vertical extreme; the number of bodies that slid off the
     ends of the ground (and fall without limit, which dominates the total momentum and energy) within 15 % (+3);
   - penetration: the deepest contact after the first 20 steps no more than 1.5 x the reference's deepest (+1 cm);
-  - the pile: contact count over the last 100 steps within 20 % of the reference's.
+  - the pile: contact count over the last 100 steps (awake manifolds plus those stored for sleeping islands) within
+    20 % of the reference's.
 The reference trajectories (tests/golden/traj_c1_n256.npz, traj_c1_n2048.npz) are the compiled reference engine run
 by tests/golden/make_golden.py.
 """
@@ -30,7 +31,7 @@ ag2d = pytest.importorskip("ag2d")
 from ag2d import scenes  # noqa: E402
 
 CASES = {256: "traj_c1_n256.npz", 2048: "traj_c1_n2048.npz"}
-KEYS = ("px", "py", "ke", "max_depth", "manifolds", "sleeping", "ke_on", "fallen")
+KEYS = ("px", "py", "ke", "max_depth", "manifolds", "sleeping", "ke_on", "fallen", "stored")
 
 
 def _trajectory(n, steps=600):
@@ -60,6 +61,7 @@ def _trajectory(n, steps=600):
         man = w.read(ag2d.PREV_MANIFOLDS)
         out["max_depth"].append(float(man["depth"].max()) if man.size else 0.0)
         out["manifolds"].append(int(man.size))
+        out["stored"].append(int(w.read(ag2d.ISLAND_MANIFOLDS).size))
         out["sleeping"].append(int(np.sum(w.read(ag2d.BODY_STATE) == 1)))
     out = {k: np.asarray(v) for k, v in out.items()}
     out["total_mass"] = float(np.sum(m[dyn]))
@@ -112,6 +114,9 @@ def test_penetration(runs):
 
 
 def test_settled_contacts(runs):
+    # The pile's contacts, awake or held for a sleeping island (whether a quiet pile falls asleep as a whole is a
+    # threshold decision that two solving orders can take differently).
     ref, gpu = runs
-    r, g = ref["manifolds"][-100:].mean(), gpu["manifolds"][-100:].mean()
+    r = (ref["manifolds"] + ref["stored"])[-100:].mean()
+    g = (gpu["manifolds"] + gpu["stored"])[-100:].mean()
     assert abs(g - r) <= 0.2 * r
