@@ -167,16 +167,8 @@ __global__ void k_scatter_list(const uint32_t* flag, const uint32_t* offset, uin
 // Sleeping-island manifold store (k_islands.cu): restore at wake, move at sleep.
 __global__ void k_isle_stage_flags(DeviceWorld w, const Manifold* isle, const uint32_t* isleId, const uint32_t* nIsle,
                                    const uint32_t* wakeIsland, uint32_t* flag);
-__global__ void k_isle_stage(const Manifold* isle, const uint32_t* nIsle, const uint32_t* flag, const uint32_t* off,
-                             uint32_t* stage, uint32_t* stageSlot, uint32_t* consumed, unsigned long long* keys,
-                             uint32_t* vals, uint32_t capacity, uint32_t* status);
-__global__ void k_isle_take(Manifold* cur, const uint32_t* nCur, const Manifold* isle, const uint32_t* stage,
-                            const uint32_t* nStage, const unsigned long long* keys, const uint32_t* vals,
-                            uint32_t capacity, uint32_t* consumed);
-__global__ void k_isle_unclaimed_flags(const uint32_t* nStage, const uint32_t* consumed, const uint32_t* stageSlot,
-                                       unsigned long long* keys, uint32_t* vals, uint32_t* flag);
-__global__ void k_isle_unclaimed(DeviceWorld w, const Manifold* isle, const uint32_t* nStage, const uint32_t* stage,
-                                 const uint32_t* flag, const uint32_t* off, uint32_t* list, uint32_t* listWorld);
+__global__ void k_isle_stage_list(DeviceWorld w, const Manifold* isle, const uint32_t* nIsle, const uint32_t* flag,
+                                  const uint32_t* off, uint32_t* list, uint32_t* listWorld);
 __global__ void k_isle_append(Manifold* cur, const uint32_t* nCur, uint32_t cap, uint32_t* hint, const Manifold* isle,
                               const uint32_t* list, const uint32_t* nList, uint32_t* status);
 __global__ void k_isle_merge(DeviceWorld w, const Manifold* cur, const uint32_t* hint, const uint32_t* nCur,

@@ -34,18 +34,39 @@ struct GlobalBodies {
     __device__ __forceinline__ unsigned long long* maxWord(uint32_t b) const { return maxW + b; }
     __device__ __forceinline__ unsigned long long* maskWord(uint32_t b) const { return maskW + b; }
     static __device__ __forceinline__ unsigned long long ldWord(const unsigned long long* p) { return __ldcg(p); }
+    __device__ __forceinline__ bool stage(uint32_t, uint32_t) const { return false; }
 };
+// Bodies [base, base + count) in shared memory. With 'lazy' set the colouring words occupy the front of the body
+// cache while the team colours (inverse masses then come from global memory), and stage() loads the velocities and
+// poses over them once the colours are known: 32 bytes of shared memory a body instead of 48, so more teams fit on
+// an SM. Otherwise the team loaded the bodies before colouring and the words have a region of their own.
 struct SharedBodies {
     float4* vel;                 // shared: bodies [base, base + count)
     float4* pos;
     unsigned long long* maxW;    // shared, zeroed by the team before colouring
     unsigned long long* maskW;
     uint32_t base;
+    uint32_t count = 0;
+    const float4* gvel = nullptr;   // lazy: the global velocities (inverse masses while colouring)
+    const float4* gpos = nullptr;
     __device__ __forceinline__ float4 v(uint32_t b) const { return vel[b - base]; }
     __device__ __forceinline__ float4 p(uint32_t b) const { return pos[b - base]; }
     __device__ __forceinline__ void setV(uint32_t b, const float4& x) const { vel[b - base] = x; }
     __device__ __forceinline__ void setP(uint32_t b, const float4& x) const { pos[b - base] = x; }
-    __device__ __forceinline__ float invMass(uint32_t b) const { return vel[b - base].w; }
+    __device__ __forceinline__ float invMass(uint32_t b) const
+    {
+        return gvel ? __ldg(&gvel[b].w) : vel[b - base].w;
+    }
+    // Loads the body cache over the colouring words (lazy only); the caller synchronises the team after it.
+    __device__ __forceinline__ bool stage(uint32_t rank, uint32_t size) const
+    {
+        if (!gvel) return false;
+        for (uint32_t i = rank; i < count; i += size) {
+            vel[i] = gvel[base + i];
+            pos[i] = gpos[base + i];
+        }
+        return true;
+    }
     __device__ __forceinline__ unsigned long long* maxWord(uint32_t b) const { return maxW + (b - base); }
     __device__ __forceinline__ unsigned long long* maskWord(uint32_t b) const { return maskW + (b - base); }
     static __device__ __forceinline__ unsigned long long ldWord(const unsigned long long* p)
@@ -581,6 +602,8 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
         s.order[Sync::ld(s.colorStart + c) + atomicAdd(s.colorCount + c, 1u)] = i;
     }
     if (!sync()) return false;
+    // The colouring words are no longer needed: a lazily staged body cache is loaded over them now.
+    if (B.stage(rank, size) && !sync()) return false;
     // Constraint build for every manifold before any velocity changes (computeConstraintData). The records go to
     // shared memory when the team's fit there (the colouring words they overwrite are no longer needed).
     const bool onChip = cs.cap >= n && cs.q != nullptr;
@@ -679,11 +702,14 @@ constexpr uint32_t TEAM_SMEM_MAX = 220 * 1024; // dynamic shared memory of a tea
                                                // all, the kernel's static arrays included)
 // Dynamic shared memory of a team CTA: body velocities and poses, then one region holding first the colouring words
 // (16 B a body) and then the constraint records (CONS_SMEM_BYTES each, consCap of them).
+// With no records on chip (consCap 0) the colouring words share the body cache (SharedBodies, lazy): 32 B a body.
 __host__ __device__ constexpr size_t team_smem_bytes(uint32_t bodyCap, uint32_t consCap)
 {
-    return size_t(bodyCap) * 2 * sizeof(float4) +
-           (size_t(bodyCap) * 16 > size_t(consCap) * CONS_SMEM_BYTES ? size_t(bodyCap) * 16
-                                                                       : size_t(consCap) * CONS_SMEM_BYTES);
+    return consCap == 0 ? size_t(bodyCap) * 2 * sizeof(float4)
+                        : size_t(bodyCap) * 2 * sizeof(float4) +
+                              (size_t(bodyCap) * 16 > size_t(consCap) * CONS_SMEM_BYTES
+                                   ? size_t(bodyCap) * 16
+                                   : size_t(consCap) * CONS_SMEM_BYTES);
 }
 // Launch shapes of the CTAs that solve a world larger than the team size (one world each): threads per CTA and
 // whether the global-record passes are pipelined (solve_passes_pipelined).

@@ -502,12 +502,9 @@ struct ag2d_world {
     DBuf<Manifold> isle, bk_isle;
     DBuf<uint32_t> isleId, bk_isleId, nIsle;
     uint32_t isleUpper = 0;
-    // Restore scratch: staging flags / offsets / indices, the pair-key table (all keys empty between steps), the
-    // unclaimed records and their worlds, and counts [staged, unclaimed, kept, moved, staying].
-    DBuf<uint32_t> isleFlag, isleOff, isleFlag2, isleOff2, isleStage, isleSlot, isleConsumed, isleList, isleListWorld;
-    DBuf<unsigned long long> isleKeys;
-    DBuf<uint32_t> isleVals, isleCounts;
-    uint32_t isleHashCap = 0;
+    // Restore scratch: staging flags and offsets, the staged records and their worlds, and counts [staged, -, kept,
+    // moved, staying].
+    DBuf<uint32_t> isleFlag, isleOff, isleList, isleListWorld, isleCounts;
     // Batches: the step's list with the restored records merged in by world (swapped in as 'manifolds' / 'color').
     DBuf<Manifold> mergeMan;
     DBuf<uint32_t> mergeHint;
@@ -1238,22 +1235,11 @@ struct ag2d_world {
         CK(cudaMemsetAsync(isleCounts.p, 0, 8 * sizeof(uint32_t), stream));
     }
 
-    // Restore scratch for a store of up to 'n' records; the key table starts empty (every key ~0, every value ~0).
+    // Restore and sleep-pass scratch for a store of up to 'n' records.
     void reserveIsleScratch(uint32_t n)
     {
-        n = std::max<uint32_t>(n, 1);
-        for (auto* b : {&isleFlag, &isleOff, &isleFlag2, &isleOff2, &isleStage, &isleSlot, &isleConsumed, &isleList,
-                        &isleListWorld, &sleepKeepWorld})
-            b->reserve(n);
-        uint32_t cap = 16;
-        while (cap < 2 * n) cap <<= 1;
-        if (cap > isleHashCap) {
-            isleKeys.reserve(cap);
-            isleVals.reserve(cap);
-            isleHashCap = cap;
-            CK(cudaMemsetAsync(isleKeys.p, 0xFF, sizeof(unsigned long long) * cap, stream));
-            CK(cudaMemsetAsync(isleVals.p, 0xFF, sizeof(uint32_t) * cap, stream));
-        }
+        n = std::max<uint32_t>({n, manifoldCap / 8, 1u});
+        for (auto* b : {&isleFlag, &isleOff, &isleList, &isleListWorld, &sleepKeepWorld}) b->reserve(n);
         scanner.reserve(n);
     }
 
@@ -1759,34 +1745,26 @@ struct ag2d_world {
         const uint32_t gi = gridFor(isleUpper), gm = gridFor(manifoldCap);
         k_isle_stage_flags<<<gi, 256, 0, s>>>(wv, isle.p, isleId.p, nIsle.p, wakeIsland.p, isleFlag.p);
         scanner.run(isleFlag.p, isleOff.p, isleUpper, cnt + 0, s, nIsle.p);
-        k_isle_stage<<<gi, 256, 0, s>>>(isle.p, nIsle.p, isleFlag.p, isleOff.p, isleStage.p, isleSlot.p,
-                                        isleConsumed.p, isleKeys.p, isleVals.p, isleHashCap, st);
-        k_isle_take<<<gm, 256, 0, s>>>(manifolds.p, nManifolds.p, isle.p, isleStage.p, cnt + 0, isleKeys.p, isleVals.p,
-                                       isleHashCap, isleConsumed.p);
-        k_isle_unclaimed_flags<<<gi, 256, 0, s>>>(cnt + 0, isleConsumed.p, isleSlot.p, isleKeys.p, isleVals.p,
-                                                  isleFlag2.p);
-        scanner.run(isleFlag2.p, isleOff2.p, isleUpper, cnt + 1, s, cnt + 0);
-        k_isle_unclaimed<<<gi, 256, 0, s>>>(wv, isle.p, cnt + 0, isleStage.p, isleFlag2.p, isleOff2.p, isleList.p,
-                                            isleListWorld.p);
+        k_isle_stage_list<<<gi, 256, 0, s>>>(wv, isle.p, nIsle.p, isleFlag.p, isleOff.p, isleList.p, isleListWorld.p);
         uint32_t* hint = hintsReady ? color.p : nullptr;
         if (nWorlds > 1) {
             mergeMan.reserve(manifoldCap);
             mergeHint.reserve(manifoldCap);
             k_manifold_segments<<<gm, 256, 0, s>>>(manifolds.p, nManifolds.p, cbody.p, bodyWorld.p, nWorlds, manSeg.p);
             k_isle_merge<<<gm, 256, 0, s>>>(wv, manifolds.p, hint, nManifolds.p, manSeg.p, isle.p, isleList.p,
-                                            isleListWorld.p, cnt + 1, manifoldCap, mergeMan.p,
+                                            isleListWorld.p, cnt + 0, manifoldCap, mergeMan.p,
                                             hint ? mergeHint.p : nullptr, st);
             swap_bufs(manifolds, mergeMan);
             if (hint) swap_bufs(color, mergeHint);
             launches += 2;
         } else {
-            k_isle_append<<<gi, 256, 0, s>>>(manifolds.p, nManifolds.p, manifoldCap, hint, isle.p, isleList.p, cnt + 1,
+            k_isle_append<<<gi, 256, 0, s>>>(manifolds.p, nManifolds.p, manifoldCap, hint, isle.p, isleList.p, cnt + 0,
                                              st);
             launches += 1;
         }
-        k_isle_count<<<1, 32, 0, s>>>(nManifolds.p, cnt + 0, cnt + 1, manifoldCap, dCounters.p);
+        k_isle_count<<<1, 32, 0, s>>>(nManifolds.p, cnt + 0, cnt + 0, manifoldCap, dCounters.p);
         CK(cudaGetLastError());
-        launches += 7;
+        launches += 4;
     }
 
     // After a step in which islands woke or fell asleep (k_islands.cu, sleep): the store drops the woken islands'
@@ -1804,7 +1782,9 @@ struct ag2d_world {
         // Both store buffers keep one capacity (they trade places), grown together by half again when short, so a
         // steady store reallocates neither.
         if (isle.n < need || bk_isle.n < need || isleId.n < need || bk_isleId.n < need || !isle.p || !bk_isle.p) {
-            const size_t cap = std::max<size_t>({size_t(need), size_t(1), isle.n + isle.n / 2});
+            // Doubling, from an eighth of the manifold capacity: a store that fills as a batch settles
+            // reallocates (a device synchronisation) a few times only.
+            const size_t cap = std::max<size_t>({size_t(need), size_t(manifoldCap / 8), size_t(1), 2 * isle.n});
             growKeep(isle, cap);
             growKeep(isleId, cap);
             DBuf<Manifold> nb;

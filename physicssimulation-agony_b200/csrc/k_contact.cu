@@ -305,9 +305,12 @@ __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* n
 // the world-grouped list, and colours + solves that range as one problem (the worlds share no body, so their
 // colour classes simply merge). Priorities are world-local indices: every world gets the colouring, hence the
 // solving order, it has when stepped on its own, whichever team it is in. A team whose bodies fit the dynamic
-// shared memory (bodyCap bodies) keeps their velocities, poses and colouring words there.
+// shared memory (bodyCap bodies) keeps their velocities, poses and colouring words there. The solver is bound by
+// load latency and barriers, so what counts is how many teams an SM holds at once: the colouring words share the
+// body cache when the records stay in global memory (32 B of shared memory a body), and the unpipelined variant is
+// held to 64 registers a thread (1024 threads an SM).
 template <uint32_t THREADS, bool PIPELINED>
-__global__ void __launch_bounds__(THREADS) k_color_solve_teams(TeamLaunch a)
+__global__ void __launch_bounds__(THREADS, PIPELINED ? 1 : 1024 / THREADS) k_color_solve_teams(TeamLaunch a)
 {
     // [bodyCap] velocities, [bodyCap] poses, then 2 x [bodyCap] u64 colouring words, overwritten after colouring by
     // the constraint records (team_smem_bytes).
@@ -337,11 +340,16 @@ __global__ void __launch_bounds__(THREADS) k_color_solve_teams(TeamLaunch a)
         if (nb <= a.bodyCap) {
             float4* vel = teamCache;
             float4* pos = teamCache + a.bodyCap;
-            auto* maxW = reinterpret_cast<unsigned long long*>(teamCache + 2 * a.bodyCap);
+            // No records on chip: the colouring words sit where the body cache goes and the bodies are loaded after
+            // colouring (SharedBodies, lazy). Otherwise the bodies are loaded now and the words follow them.
+            const bool lazy = a.consCap == 0;
+            auto* maxW = reinterpret_cast<unsigned long long*>(lazy ? teamCache : teamCache + 2 * a.bodyCap);
             unsigned long long* maskW = maxW + a.bodyCap;
             for (uint32_t i = threadIdx.x; i < nb; i += THREADS) {
-                vel[i] = w.bvel[b0 + i];
-                pos[i] = w.bpos[b0 + i];
+                if (!lazy) {
+                    vel[i] = w.bvel[b0 + i];
+                    pos[i] = w.bpos[b0 + i];
+                }
                 maxW[i] = 0ull;
                 maskW[i] = 0ull;
             }
@@ -350,14 +358,19 @@ __global__ void __launch_bounds__(THREADS) k_color_solve_teams(TeamLaunch a)
             cs.q = teamCache + 2 * a.bodyCap;
             cs.cap = a.consCap;
             cs.base = b0;
-            color_and_solve<BlockSync, SharedBodies, PIPELINED>(w, SharedBodies{vel, pos, maxW, maskW, b0}, m + lo,
-                                                                 hi - lo, ls, a.velIters, a.posIters, threadIdx.x,
-                                                                 THREADS, BlockSync{}, &a.counters->colors,
-                                                                 &a.counters->status, cs);
+            SharedBodies sb{vel, pos, maxW, maskW, b0};
+            if (lazy) { sb.count = nb; sb.gvel = w.bvel; sb.gpos = w.bpos; }
+            const bool solved = color_and_solve<BlockSync, SharedBodies, PIPELINED>(
+                w, sb, m + lo, hi - lo, ls, a.velIters, a.posIters, threadIdx.x, THREADS, BlockSync{},
+                &a.counters->colors, &a.counters->status, cs);
             __syncthreads();
-            for (uint32_t i = threadIdx.x; i < nb; i += THREADS) {
-                w.bvel[b0 + i] = vel[i];
-                w.bpos[b0 + i] = pos[i];
+            // A team that gave up (its status bit is set and the step is redone or fails) leaves the bodies alone:
+            // a lazy cache may still hold colouring words.
+            if (solved) {
+                for (uint32_t i = threadIdx.x; i < nb; i += THREADS) {
+                    w.bvel[b0 + i] = vel[i];
+                    w.bpos[b0 + i] = pos[i];
+                }
             }
         } else {
             __syncthreads();

@@ -6,10 +6,13 @@
 // batch and, within a world, in the order the records went to sleep. Two operations per step:
 //
 //  - restore, after the wake pass and before the solver: the records of the islands that woke this step (and whose
-//    colliders still exist) are staged in store order. A table over their pair keys (the first record of a pair
-//    wins) lets every fresh manifold of the same pair take the stored impulses of the contacts with equal ids when
-//    the collider order matches; the staged records no fresh manifold claimed join the step's manifold list whole,
-//    at the end of their world's segment, so the solver and the islands see them this step.
+//    colliders still exist) join the step's manifold list whole, in store order, at the end of their world's
+//    segment, so the solver and the islands see them this step. The reference first lets a manifold generated this
+//    frame for the same pair take the stored impulses (wakeContactData, :371-395); that never happens here: a
+//    stored record's two bodies are in its sleeping island or static until the island wakes, and the pairs of a
+//    frame are found from colliders that were awake when the broad phase ran, before the wake pass. Each pair is
+//    stored at most once (it leaves the warm-start list when it is stored and the store when its island wakes), so
+//    the reference's first-record-of-a-pair rule has nothing to choose either.
 //  - sleep, after a step in which islands woke or fell asleep: the store drops the records of the woken islands and
 //    of destroyed colliders; the step's manifolds with a body that is now asleep move to the store (tagged with that
 //    body's island: body A's when A sleeps, else body B's), the rest stay as the next step's warm-start source.
@@ -56,98 +59,20 @@ __global__ void k_isle_stage_flags(DeviceWorld w, const Manifold* __restrict__ i
     }
 }
 
-// Restore, step 2: staged record j = the j-th flagged store record; its pair key goes into the table (the smallest
-// j of a key wins), the slot it took is remembered for the clean-up.
-__global__ void k_isle_stage(const Manifold* __restrict__ isle, const uint32_t* __restrict__ nIsle,
-                             const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off,
-                             uint32_t* __restrict__ stage, uint32_t* __restrict__ stageSlot,
-                             uint32_t* __restrict__ consumed, unsigned long long* __restrict__ keys,
-                             uint32_t* __restrict__ vals, uint32_t capacity, uint32_t* __restrict__ status)
+// Restore, step 2: the staged records (store indices) in store order, with their worlds.
+__global__ void k_isle_stage_list(DeviceWorld w, const Manifold* __restrict__ isle, const uint32_t* __restrict__ nIsle,
+                                  const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off,
+                                  uint32_t* __restrict__ list, uint32_t* __restrict__ listWorld)
 {
     const uint32_t n = *nIsle;
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         if (!flag[r]) continue;
-        const uint32_t j = off[r];
-        stage[j] = r;
-        consumed[j] = 0u;
-        const Manifold& m = isle[r];
-        const unsigned long long key = pair_key(m.a, m.b);
-        uint32_t s = slot_of(key, capacity);
-        uint32_t probes = 0;
-        for (;;) {
-            const unsigned long long old = atomicCAS(keys + s, ~0ull, key);
-            if (old == ~0ull || old == key) { atomicMin(vals + s, j); break; }
-            s = (s + 1) & (capacity - 1u);
-            if (++probes >= capacity) { atomicOr(status, STATUS_HASH_FULL); s = 0xFFFFFFFFu; break; }
-        }
-        stageSlot[j] = s;
+        list[off[r]] = r;
+        listWorld[off[r]] = record_world(w, isle[r]);
     }
 }
 
-// Restore, step 3: a fresh manifold whose pair is staged claims that record; with the same collider order it takes
-// the stored impulses of its contacts by id.
-__global__ void k_isle_take(Manifold* __restrict__ cur, const uint32_t* __restrict__ nCur,
-                            const Manifold* __restrict__ isle, const uint32_t* __restrict__ stage,
-                            const uint32_t* __restrict__ nStage, const unsigned long long* __restrict__ keys,
-                            const uint32_t* __restrict__ vals, uint32_t capacity, uint32_t* __restrict__ consumed)
-{
-    if (*nStage == 0) return;
-    const uint32_t n = *nCur;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        Manifold& c = cur[i];
-        const unsigned long long key = pair_key(c.a, c.b);
-        uint32_t s = slot_of(key, capacity);
-        uint32_t j = 0xFFFFFFFFu;
-        for (uint32_t probes = 0; probes < capacity; probes++) {
-            const unsigned long long k = keys[s];
-            if (k == key) { j = vals[s]; break; }
-            if (k == ~0ull) break;
-            s = (s + 1) & (capacity - 1u);
-        }
-        if (j == 0xFFFFFFFFu) continue;
-        consumed[j] = 1u;
-        const Manifold st = isle[stage[j]];
-        if (st.a != c.a || st.b != c.b) continue;
-        for (uint32_t k = 0; k < c.count; k++) {
-            const uint32_t id = k == 0 ? c.id0 : c.id1;
-            float jn, jt;
-            if (st.count > 0 && id == st.id0) { jn = st.jn0; jt = st.jt0; }
-            else if (st.count > 1 && id == st.id1) { jn = st.jn1; jt = st.jt1; }
-            else continue;
-            if (k == 0) { c.jn0 = jn; c.jt0 = jt; } else { c.jn1 = jn; c.jt1 = jt; }
-        }
-    }
-}
-
-// Restore, step 4: flags of the staged records no fresh manifold claimed; the table slots are released.
-__global__ void k_isle_unclaimed_flags(const uint32_t* __restrict__ nStage, const uint32_t* __restrict__ consumed,
-                                       const uint32_t* __restrict__ stageSlot, unsigned long long* __restrict__ keys,
-                                       uint32_t* __restrict__ vals, uint32_t* __restrict__ flag)
-{
-    const uint32_t n = *nStage;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        flag[j] = consumed[j] ? 0u : 1u;
-        const uint32_t s = stageSlot[j];
-        if (s != 0xFFFFFFFFu) { keys[s] = ~0ull; vals[s] = 0xFFFFFFFFu; }
-    }
-}
-
-// Restore, step 5: the unclaimed records (store indices) in staging order, with their worlds.
-__global__ void k_isle_unclaimed(DeviceWorld w, const Manifold* __restrict__ isle,
-                                 const uint32_t* __restrict__ nStage, const uint32_t* __restrict__ stage,
-                                 const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off,
-                                 uint32_t* __restrict__ list, uint32_t* __restrict__ listWorld)
-{
-    const uint32_t n = *nStage;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        if (!flag[j]) continue;
-        const uint32_t r = stage[j];
-        list[off[j]] = r;
-        listWorld[off[j]] = record_world(w, isle[r]);
-    }
-}
-
-// Restore, step 6 (a single world): the unclaimed records go after the fresh manifolds, with no colouring hint. A
+// Restore, step 3 (a single world): the staged records go after the fresh manifolds, with no colouring hint. A
 // list that would pass 'cap' records the overflow instead (the step is retried with larger buffers).
 __global__ void k_isle_append(Manifold* __restrict__ cur, const uint32_t* __restrict__ nCur, uint32_t cap,
                               uint32_t* __restrict__ hint, const Manifold* __restrict__ isle,
@@ -165,8 +90,8 @@ __global__ void k_isle_append(Manifold* __restrict__ cur, const uint32_t* __rest
     }
 }
 
-// Restore, step 6 (a batch): fresh manifolds and unclaimed records merged by world into out (the fresh ones of a
-// world first, in their order, then its unclaimed ones in staging order). seg: the fresh list's world starts. The
+// Restore, step 3 (a batch): fresh manifolds and staged records merged by world into out (the fresh ones of a
+// world first, in their order, then its staged ones in store order). seg: the fresh list's world starts. The
 // caller makes out the step's list whatever happens, so every record of out[0, nCur) is written.
 __global__ void k_isle_merge(DeviceWorld w, const Manifold* __restrict__ cur, const uint32_t* __restrict__ hint,
                              const uint32_t* __restrict__ nCur, const uint32_t* __restrict__ seg,
@@ -197,7 +122,7 @@ __global__ void k_isle_merge(DeviceWorld w, const Manifold* __restrict__ cur, co
     }
 }
 
-// Restore, step 7: the list's count takes the appended records (unless the append overflowed).
+// Restore, step 4: the list's count takes the appended records (unless the append overflowed).
 __global__ void k_isle_count(uint32_t* __restrict__ nCur, const uint32_t* __restrict__ nStage,
                              const uint32_t* __restrict__ nList, uint32_t cap, StepCounters* counters)
 {
