@@ -21,11 +21,13 @@ batch: the job's N x 4,096 worlds (seeds 0 ..) are shared out by greedy body-cou
 least-loaded rank): weak scaling with no collective in the step; the whole-job value is the sum of all ranks'
 body-steps over the slowest rank's device time.
 
-Timing: W untimed warm-up steps, then K steps, each bracketed by CUDA events on the engine's stream, with a 256 MiB
-write between steps outside the events (L2 flushed); barrier + synchronize around the timed region; the max over
-ranks. SM clocks are sampled with nvidia-smi during the timed region. The end-to-end number ("e2e") goes through the
-C ABI with host buffers: the bodies created on the host and uploaded inside the timed region, then per step one
-step call and one readback of every body's pose into host memory.
+Timing: c4 steps every world from rest to --window-start - W, then W untimed warm-up steps, then K timed steps
+(both arms time the same window), each bracketed by CUDA events on the engine's stream, with a 256 MiB write
+between steps outside the events (L2 flushed); barrier + synchronize around the timed region; the max over ranks.
+SM clocks are sampled with nvidia-smi during the timed region. The end-to-end number ("e2e") goes through the C ABI
+with host buffers: the batch is restored from a page-locked host checkpoint of the window's start inside the timed
+region, then per step one step call and one asynchronous read of every body's pose into page-locked host memory,
+waited for one step later.
 
 --impl reference times the reference engine itself (oracle/_ref/libagony_ref.so, its own C++ on the host cores,
 all threads) on a bounded sample of the same workload and prints the same line with "impl": "reference".

@@ -147,11 +147,13 @@ __global__ void k_narrow(DeviceWorld w, const uint2* pairs, const uint32_t* nPai
                          uint32_t manifoldCap, uint32_t* nOut, StepCounters* counters, uint32_t* tileState,
                          uint32_t* tileCounter);
 __global__ void k_warm_insert(const Manifold* prev, const uint32_t* nPrev, unsigned long long* keys,
-                              uint32_t* vals, uint32_t capacity, uint32_t* status);
+                              uint32_t* vals, uint32_t capacity, const uint32_t* seg, const uint32_t* colWorld,
+                              uint32_t* status);
 constexpr uint32_t WARM_CACHED = 0x80000000u;   // contact-cache value flag: the manifold had a non-zero impulse
 __global__ void k_warm_lookup(const Manifold* prev, Manifold* cur, const uint32_t* nCur,
                               const unsigned long long* keys, const uint32_t* vals, uint32_t capacity,
-                              StepCounters* counters, const uint32_t* prevColor, uint32_t* hint);
+                              const uint32_t* seg, const uint32_t* colWorld, StepCounters* counters,
+                              const uint32_t* prevColor, uint32_t* hint);
 __global__ void k_wake(DeviceWorld w, const Manifold* m, const uint32_t* nM, uint32_t* wakeIsland,
                        StepCounters* counters);
 __global__ void k_wake_apply(DeviceWorld w, const uint32_t* wakeIsland, StepCounters* counters);

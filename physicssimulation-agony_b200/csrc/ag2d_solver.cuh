@@ -490,6 +490,9 @@ __device__ bool solve_passes_pipelined(const Bodies& B, const SolveScratch& s, u
 // cannot share a dynamic body: their predecessors were coloured together last step, and a body's dynamic flag
 // (finite mass) does not change between steps. The other manifolds run the Jones-Plassmann rounds around the kept
 // colours. With no hints every manifold runs the rounds. s.color holds colour | age << COLOR_AGE_SHIFT.
+// s.pairBodies words: body index | PAIR_DYNAMIC (finite mass) | PAIR_KEPT (first word: colour carried over).
+constexpr uint32_t PAIR_DYNAMIC = 0x80000000u, PAIR_KEPT = 0x40000000u, PAIR_BODY = 0x3FFFFFFFu;
+
 template <class Sync, class Bodies, bool PIPELINED = false>
 __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold* __restrict__ m, uint32_t n,
                                 const SolveScratch& s, uint32_t velIters, uint32_t posIters, uint32_t rank,
@@ -500,7 +503,7 @@ __device__ bool color_and_solve(const DeviceWorld& w, const Bodies& B, Manifold*
     uint32_t* const nColors = s.colorCount + MAX_COLORS + 3;
     // Each manifold's two bodies and whether they are dynamic, looked up once for all colouring rounds; kept
     // colours are counted and marked around their bodies here.
-    constexpr uint32_t DYN = 0x80000000u, KEPT = 0x40000000u;
+    constexpr uint32_t DYN = PAIR_DYNAMIC, KEPT = PAIR_KEPT;
     if (s.hint && !sync()) return false;   // the counters are zeroed before kept colours are counted
     uint32_t keptTop = 0;
     for (uint32_t i = rank; i < n; i += size) {
@@ -727,6 +730,8 @@ struct TeamLaunch {
     uint32_t velIters, posIters;
     uint32_t* nextTeam;
     StepCounters* counters;
+    uint32_t* ufParent;   // non-null: each team also links its islands (union-find over its manifolds, roots the
+                          // smallest body index) into this array, initialised to parent[b] = b before the launch
 };
 // Host side: launches the team solver with 'threads' per CTA; returns the launch error.
 cudaError_t launch_color_solve_teams(uint32_t threads, bool pipelined, uint32_t grid, cudaStream_t stream,

@@ -262,13 +262,14 @@ enum CkptSection : uint32_t {
     CK_PREVCOLOR, CK_WBODY, CK_WCOL, CK_ISLE, CK_ISLEID, NCK
 };
 constexpr char CKPT_MAGIC[8] = {'A', 'G', '2', 'D', 'C', 'K', 'P', 'T'};
-constexpr uint32_t CKPT_VERSION = 2;
+constexpr uint32_t CKPT_VERSION = 3;
 struct CkptHeader {
     char magic[8];
     uint32_t version, headerBytes;
     ag2d_world_settings settings;
     uint32_t nWorlds, nBodies, nColliders, nCircles, nBoxes, nPolygons, nPolyVerts, nMaterialRows;
     uint32_t nPrev, nStatic, lastManifolds, nIsle;
+    uint32_t lastPairs, pad;   // the saved engine's last step: candidate pairs (sizes the restored buffers)
     uint64_t totalBytes;
     uint64_t off[NCK], len[NCK];
 };
@@ -452,6 +453,7 @@ struct ag2d_world {
     uint32_t nDestroyed = 0;   // bodies removed by destroy commands (still in the arrays, in no list)
     uint32_t pairCap = 0, manifoldCap = 0, hashCap = 0;
     uint32_t lastManifolds = 0;
+    uint32_t lastPairs = 0;   // candidate pairs of the last step
     uint32_t prevCount = 0;   // manifolds in prevManifolds (the warm-start source), as the host knows them
 
     // Bodies.
@@ -514,6 +516,7 @@ struct ag2d_world {
         sleepMoveWorld, sleepColor;
     DBuf<Manifold> sleepList;
     bool prevHoldsSleepers = false;   // the warm-start list still holds records moved to the store (compactPrev)
+    bool islandsLinked = false;       // this step's team solver already linked the islands (phaseIslands skips it)
     DBuf<Constraint> cons;
     DBuf<uint2> pairBodies;
     // Islands.
@@ -540,6 +543,8 @@ struct ag2d_world {
     std::vector<uint32_t> hBodyStart, hColStart;     // [nWorlds + 1]
     DBuf<uint32_t> bodyWorld, colWorld, worldBodyStart, worldColStart, manSeg, nextWorld, worldDirty;
     DBuf<uint32_t> isleSeg;                  // world starts of the sleeping islands' manifolds (server repacks)
+    DBuf<uint32_t> prevSeg;                  // world starts of the warm-start list (warm-start table regions)
+    bool prevSegValid = false;               // prevSeg describes prevManifolds as it is
     DBuf<uint32_t> teamWorld, teamOrder;     // solver teams: first world of each team; small then big, largest first
     DBuf<uint8_t> dynSimd, dynColSimd;               // SIMD-path flag of each work-list entry
     // Request-server engines: extents of the resident worlds, back buffers the repack gathers into, and the
@@ -639,7 +644,9 @@ struct ag2d_world {
     }
 
     // Per-body and per-collider work buffers for the current sizes (grow only).
-    void sizeFor()
+    // capsKnown: the pair and manifold capacities were already set (a checkpoint's counts), so the first-upload
+    // guess of INITIAL_PAIRS_PER_COLLIDER a collider is not applied.
+    void sizeFor(bool capsKnown = false)
     {
         snapVel.reserve(nBodies); snapPos.reserve(nBodies); snapRot.reserve(nBodies); snapWrap.reserve(nBodies);
         snapTimer.reserve(nBodies); snapState.reserve(nBodies); snapIsland.reserve(nBodies);
@@ -656,7 +663,7 @@ struct ag2d_world {
         bodyMask.reserve(nBodies);
         ufParent.reserve(nBodies); ufFlag.reserve(nBodies); wakeIsland.reserve(nBodies);
         const uint32_t cap = std::max<uint32_t>(INITIAL_PAIRS_PER_COLLIDER * nColliders, 4096);
-        if (cap > pairCap || cap > manifoldCap)
+        if (!capsKnown && (cap > pairCap || cap > manifoldCap))
             reserveCapacities(std::max(pairCap + pairCap / 2, cap), std::max(manifoldCap + manifoldCap / 2, cap));
         scanner.reserve(std::max({pairCap, nColliders, nBodies}));
     }
@@ -683,6 +690,7 @@ struct ag2d_world {
         };
         const uint32_t W0 = uint32_t(worldExt.size());
         compactPrev();
+        prevSegValid = false;
         // Current extents of the warm-start manifolds and of the sleeping islands' manifolds (both world-grouped).
         if (W0 == 1) {
             uint32_t n[2] = {0, 0};
@@ -1053,6 +1061,7 @@ struct ag2d_world {
         h.nPolygons = nPolygons; h.nPolyVerts = nPolyVerts; h.nMaterialRows = nMaterialRows;
         h.nStatic = nStatic;
         h.lastManifolds = lastManifolds;
+        h.lastPairs = lastPairs;
         compactPrev();
         CK(cudaMemcpyAsync(&h.nPrev, nPrev.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
         CK(cudaMemcpyAsync(&h.nIsle, nIsle.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
@@ -1125,13 +1134,24 @@ struct ag2d_world {
         const uint32_t* wc = reinterpret_cast<const uint32_t*>(src + h.off[CK_WCOL]);
         hBodyStart.assign(ws, ws + nWorlds + 1);
         hColStart.assign(wc, wc + nWorlds + 1);
-        sizeFor();
+        // Buffers sized from the saved engine's last step (three times its pairs and manifolds: above the growth
+        // threshold of twice the count), not from the first-upload guess of pairs a collider.
+        const bool known = h.lastPairs > 0;
+        if (known) {
+            lastManifolds = h.lastManifolds;
+            lastPairs = h.lastPairs;
+            reserveCapacities(uint32_t(std::min<uint64_t>(std::max<uint64_t>(3ull * h.lastPairs, 4096), 1ull << 30)),
+                              uint32_t(std::min<uint64_t>(std::max<uint64_t>({3ull * h.lastManifolds, h.nPrev, 4096}),
+                                                          1ull << 30)));
+        }
+        sizeFor(known);
         if (h.nPrev > manifoldCap) reserveCapacities(std::max(h.nPrev, pairCap), h.nPrev);
         if (h.len[CK_PREV])
             CK(cudaMemcpyAsync(prevManifolds.p, src + h.off[CK_PREV], h.len[CK_PREV], cudaMemcpyHostToDevice, s));
         if (h.len[CK_PREVCOLOR])
             CK(cudaMemcpyAsync(prevColor.p, src + h.off[CK_PREVCOLOR], h.len[CK_PREVCOLOR], cudaMemcpyHostToDevice, s));
         prevCount = h.nPrev;
+        prevSegValid = false;
         CK(cudaMemcpyAsync(nPrev.p, &prevCount, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
         up(isle, CK_ISLE, h.nIsle);
         up(isleId, CK_ISLEID, h.nIsle);
@@ -1238,7 +1258,7 @@ struct ag2d_world {
     // Restore and sleep-pass scratch for a store of up to 'n' records.
     void reserveIsleScratch(uint32_t n)
     {
-        n = std::max<uint32_t>({n, manifoldCap / 8, 1u});
+        n = std::max<uint32_t>(n, 1);
         for (auto* b : {&isleFlag, &isleOff, &isleList, &isleListWorld, &sleepKeepWorld}) b->reserve(n);
         scanner.reserve(n);
     }
@@ -1387,6 +1407,7 @@ struct ag2d_world {
         CK(cudaMemsetAsync(nManifolds.p, 0, sizeof(uint32_t), s));
         CK(cudaMemsetAsync(nIsle.p, 0, sizeof(uint32_t), s));
         isleUpper = 0;
+        prevSegValid = false;
         CK(cudaStreamSynchronize(s));
         hostDirty = false;
         listsDirty = true;
@@ -1710,10 +1731,23 @@ struct ag2d_world {
         while (slotsUsed < 2 * prevCount && slotsUsed < hashCap) slotsUsed <<= 1;
         slotsUsed = std::min(slotsUsed, hashCap);
         CK(cudaMemsetAsync(hashKeys.p, 0xFF, size_t(slotsUsed) * sizeof(unsigned long long), s));
+        // A batch keeps one table region per world (the previous list's world starts, kept from the last step's
+        // solve or recomputed when the list changed since).
+        const uint32_t* seg = nullptr;
+        if (nWorlds > 1) {
+            prevSeg.reserve(nWorlds + 1);
+            if (!prevSegValid) {
+                k_manifold_segments<<<gridFor(manifoldCap), 256, 0, s>>>(prevManifolds.p, nPrev.p, cbody.p,
+                                                                         bodyWorld.p, nWorlds, prevSeg.p);
+                launches++;
+            }
+            seg = prevSeg.p;
+        }
         k_warm_insert<<<gridFor(manifoldCap), 256, 0, s>>>(prevManifolds.p, nPrev.p, hashKeys.p, hashVals.p, slotsUsed,
-                                                           &dCounters.p->status);
+                                                           seg, colWorld.p, &dCounters.p->status);
         k_warm_lookup<<<gridFor(manifoldCap), 256, 0, s>>>(prevManifolds.p, manifolds.p, nManifolds.p, hashKeys.p,
-                                                           hashVals.p, slotsUsed, dCounters.p, prevColor.p, color.p);
+                                                           hashVals.p, slotsUsed, seg, colWorld.p, dCounters.p,
+                                                           prevColor.p, color.p);
         hintsReady = true;
         CK(cudaGetLastError());
         pend(7);
@@ -1782,9 +1816,9 @@ struct ag2d_world {
         // Both store buffers keep one capacity (they trade places), grown together by half again when short, so a
         // steady store reallocates neither.
         if (isle.n < need || bk_isle.n < need || isleId.n < need || bk_isleId.n < need || !isle.p || !bk_isle.p) {
-            // Doubling, from an eighth of the manifold capacity: a store that fills as a batch settles
-            // reallocates (a device synchronisation) a few times only.
-            const size_t cap = std::max<size_t>({size_t(need), size_t(manifoldCap / 8), size_t(1), 2 * isle.n});
+            // Half again on top of the need, at least doubling: a store that fills as a batch settles reallocates
+            // (a device synchronisation) a few times only.
+            const size_t cap = std::max<size_t>({size_t(need) + need / 2, size_t(1024), 2 * isle.n});
             growKeep(isle, cap);
             growKeep(isleId, cap);
             DBuf<Manifold> nb;
@@ -1845,6 +1879,7 @@ struct ag2d_world {
     {
         if (!prevHoldsSleepers) return;
         prevHoldsSleepers = false;
+        prevSegValid = false;
         const cudaStream_t s = stream;
         const uint32_t listN = std::max<uint32_t>(prevCount, 1);
         for (auto* b : {&sleepStay, &sleepMove, &sleepStayOff, &sleepMoveIsland, &sleepColor}) b->reserve(manifoldCap);
@@ -1892,8 +1927,12 @@ struct ag2d_world {
         StepCounters* ctr = dCounters.p;
         pbegin(10);
         if (nWorlds > 1) {
-            // One CTA per world over the world-grouped manifold list.
+            // One CTA per world over the world-grouped manifold list; the teams also link their islands
+            // (phaseIslands then only decides sleep).
             CK(cudaMemsetAsync(nextWorld.p, 0, 2 * sizeof(uint32_t), s));
+            k_island_init<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p);
+            islandsLinked = true;
+            launches++;
             k_manifold_segments<<<gridFor(manifoldCap), 256, 0, s>>>(mm, nm, cbody.p, bodyWorld.p, nWorlds,
                                                                       manSeg.p);
             scratch.prio = prio.p;
@@ -1902,7 +1941,7 @@ struct ag2d_world {
                 CK(cudaEventRecord(forkEvent, s));
                 CK(cudaStreamWaitEvent(sideStream, forkEvent, 0));
                 const TeamLaunch big{w, mm, manSeg.p, teamWorld.p, teamOrder.p + nTeams, nBigTeams, bigBodyCap,
-                                     bigConsCap, scratch, vi, pi, nextWorld.p + 1, ctr};
+                                     bigConsCap, scratch, vi, pi, nextWorld.p + 1, ctr, ufParent.p};
                 CK(launch_color_solve_teams(bigThreads, bigPipelined, std::min(nBigTeams, bigBlocks), sideStream,
                                             big));
                 launches++;
@@ -1910,7 +1949,7 @@ struct ag2d_world {
             if (nTeams) {
                 const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(nTeams, teamBlocks));
                 const TeamLaunch args{w, mm, manSeg.p, teamWorld.p, teamOrder.p, nTeams, teamBodyCap, teamConsCap,
-                                      scratch, vi, pi, nextWorld.p, ctr};
+                                      scratch, vi, pi, nextWorld.p, ctr, ufParent.p};
                 CK(launch_color_solve_teams(teamThreads, false, grid, s, args));
             }
             if (nBigTeams) {
@@ -1950,9 +1989,12 @@ struct ag2d_world {
         const cudaStream_t s = stream;
         const DeviceWorld w = view();
         pbegin(11);
-        launches += 4;
-        k_island_init<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p);
-        k_island_union<<<gridFor(manifoldCap), 256, 0, s>>>(w, manifolds.p, nManifolds.p, ufParent.p);
+        launches += islandsLinked ? 2 : 4;
+        if (!islandsLinked) {
+            k_island_init<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p);
+            k_island_union<<<gridFor(manifoldCap), 256, 0, s>>>(w, manifolds.p, nManifolds.p, ufParent.p);
+        }
+        islandsLinked = false;
         k_island_quiet<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p, settings.dt, settings.sleep_speed,
                                                         settings.sleep_time);
         k_island_sleep<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p, dCounters.p);
@@ -2253,6 +2295,7 @@ struct ag2d_world {
         CK(cudaStreamSynchronize(s));
         isleUpper = nk;
         prevCount = nnp;
+        prevSegValid = false;
     }
 
     // One fixed step (Simulation::physicsStep order, Simulation.cpp:255-351).
@@ -2333,7 +2376,14 @@ struct ag2d_world {
             newWorldsPending = false;
             manSegFresh = nWorlds > 1;
             CK(cudaMemcpyAsync(nPrev.p, nManifolds.p, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+            if (nWorlds > 1) {   // the solve's world starts describe the list that is now the warm-start list
+                prevSeg.reserve(nWorlds + 1);
+                CK(cudaMemcpyAsync(prevSeg.p, manSeg.p, (size_t(nWorlds) + 1) * sizeof(uint32_t),
+                                   cudaMemcpyDeviceToDevice, s));
+                prevSegValid = true;
+            }
             lastManifolds = hCounters->manifolds;
+            lastPairs = hCounters->pairs;
             prevCount = std::min(lastManifolds, manifoldCap);
             // The store as the step began (the restore reads it, the sleep pass rewrites it).
             isleUpper = hCounters->stored;
@@ -3207,6 +3257,7 @@ int32_t ag2d_world_write(ag2d_world* world, int32_t field, const void* src, uint
             if (prev) {
                 w.prevCount = n;
                 w.prevHoldsSleepers = false;
+                w.prevSegValid = false;
                 // Written manifolds carry no solver colour: no colouring hints from them.
                 if (n) CK(cudaMemsetAsync(w.prevColor.p, 0xFF, sizeof(uint32_t) * n, s));
             }

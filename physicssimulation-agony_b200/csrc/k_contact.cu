@@ -177,8 +177,31 @@ __global__ void k_narrow(DeviceWorld w, const uint2* __restrict__ pairs, const u
 // :749-766). Every new manifold whose pair was there also takes that manifold's colour as its colouring hint.
 // ---------------------------------------------------------------------------------------------------------------
 
+// The table: one open-addressing region per world of a batch, [2 seg[w], 2 seg[w + 1]) for the world's
+// seg[w + 1] - seg[w] previous manifolds (seg: the previous list's world starts), so a warm-start probe stays in its
+// world's few kilobytes and hits in cache; a single world (seg null) uses the whole power-of-two table. Which
+// region holds a pair changes nothing but where it is found.
+struct WarmRegion {
+    uint32_t base, size;   // size 0: the world had no manifolds
+    __device__ __forceinline__ uint32_t home(unsigned long long key) const
+    {
+        return base + uint32_t(((key * 0x9E3779B97F4A7C15ull) >> 32) % size);
+    }
+    __device__ __forceinline__ uint32_t next(uint32_t s) const { return s + 1 == base + size ? base : s + 1; }
+};
+__device__ __forceinline__ WarmRegion warm_region(const uint32_t* seg, const uint32_t* colWorld, uint32_t a,
+                                                  uint32_t capacity)
+{
+    if (!seg) return WarmRegion{0u, capacity};
+    const uint32_t wd = colWorld[a];
+    const uint32_t lo = seg[wd], hi = seg[wd + 1];
+    if (hi < lo || 2ull * hi > capacity) return WarmRegion{0u, 0u};   // not a valid segmentation: no region
+    return WarmRegion{2u * lo, 2u * (hi - lo)};
+}
+
 __global__ void k_warm_insert(const Manifold* __restrict__ prev, const uint32_t* __restrict__ nPrev,
                               unsigned long long* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t capacity,
+                              const uint32_t* __restrict__ seg, const uint32_t* __restrict__ colWorld,
                               uint32_t* __restrict__ status)
 {
     const uint32_t n = *nPrev;
@@ -188,33 +211,39 @@ __global__ void k_warm_insert(const Manifold* __restrict__ prev, const uint32_t*
                         uint32_t(m.jt1 != 0.0f) << 3;
         mask &= (1u << (2u * m.count)) - 1u;
         const unsigned long long key = pair_key(m.a, m.b);
-        uint32_t s = slot_of(key, capacity);
+        const WarmRegion r = warm_region(seg, colWorld, m.a, capacity);
+        if (r.size == 0) { atomicOr(status, STATUS_HASH_FULL); continue; }   // cannot happen: m is in its world
+        uint32_t s = r.home(key);
         uint32_t probes = 0;
         for (;;) {
             const unsigned long long old = atomicCAS(keys + s, ~0ull, key);
             if (old == ~0ull || old == key) { vals[s] = i | (mask ? WARM_CACHED : 0u); break; }
-            s = (s + 1) & (capacity - 1u);
-            if (++probes >= capacity) { atomicOr(status, STATUS_HASH_FULL); break; }
+            s = r.next(s);
+            if (++probes >= r.size) { atomicOr(status, STATUS_HASH_FULL); break; }
         }
     }
 }
 
 __global__ void k_warm_lookup(const Manifold* __restrict__ prev, Manifold* __restrict__ cur,
                               const uint32_t* __restrict__ nCur, const unsigned long long* __restrict__ keys,
-                              const uint32_t* __restrict__ vals, uint32_t capacity, StepCounters* counters,
+                              const uint32_t* __restrict__ vals, uint32_t capacity, const uint32_t* __restrict__ seg,
+                              const uint32_t* __restrict__ colWorld, StepCounters* counters,
                               const uint32_t* __restrict__ prevColor, uint32_t* __restrict__ hint)
 {
     const uint32_t n = *nCur;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         Manifold& c = cur[i];
         const unsigned long long key = pair_key(c.a, c.b);
-        uint32_t s = slot_of(key, capacity);
+        const WarmRegion r = warm_region(seg, colWorld, c.a, capacity);
         uint32_t idx = NO_COLOR;
-        for (uint32_t probes = 0; probes < capacity; probes++) {
-            const unsigned long long k = keys[s];
-            if (k == key) { idx = vals[s]; break; }
-            if (k == ~0ull) break;
-            s = (s + 1) & (capacity - 1u);
+        if (r.size) {
+            uint32_t s = r.home(key);
+            for (uint32_t probes = 0; probes < r.size; probes++) {
+                const unsigned long long k = keys[s];
+                if (k == key) { idx = vals[s]; break; }
+                if (k == ~0ull) break;
+                s = r.next(s);
+            }
         }
         if (hint) hint[i] = (idx != NO_COLOR && prevColor) ? prevColor[idx & ~WARM_CACHED] : NO_COLOR;
         if (idx == NO_COLOR || !(idx & WARM_CACHED)) continue;
@@ -309,6 +338,31 @@ __global__ void k_color_solve_grid(DeviceWorld w, Manifold* m, const uint32_t* n
 // load latency and barriers, so what counts is how many teams an SM holds at once: the colouring words share the
 // body cache when the records stay in global memory (32 B of shared memory a body), and the unpipelined variant is
 // held to 64 registers a thread (1024 threads an SM).
+// Union-find over a parent array in shared or global memory (generic addressing; volatile reads see other SMs'
+// links), linking the larger root under the smaller, so every island's root is its smallest body index whatever
+// the order of the links (IslandManager's islands, the same roots k_island_union gives).
+__device__ __forceinline__ uint32_t team_find(uint32_t* par, uint32_t x)
+{
+    volatile uint32_t* p = par;
+    uint32_t px = p[x];
+    for (uint32_t guard = 0; px != x && guard < (1u << 20); guard++) {
+        const uint32_t gp = p[px];
+        if (gp != px) atomicCAS(par + x, px, gp);   // path halving, benign races
+        x = px;
+        px = gp;
+    }
+    return x;
+}
+__device__ __forceinline__ void team_union(uint32_t* par, uint32_t a, uint32_t b)
+{
+    for (uint32_t tries = 0; tries < (1u << 20); tries++) {
+        uint32_t ra = team_find(par, a), rb = team_find(par, b);
+        if (ra == rb) return;
+        if (ra < rb) { const uint32_t t = ra; ra = rb; rb = t; }
+        if (atomicCAS(par + ra, ra, rb) == ra) return;
+    }
+}
+
 template <uint32_t THREADS, bool PIPELINED>
 __global__ void __launch_bounds__(THREADS, PIPELINED ? 1 : 1024 / THREADS) k_color_solve_teams(TeamLaunch a)
 {
@@ -372,11 +426,35 @@ __global__ void __launch_bounds__(THREADS, PIPELINED ? 1 : 1024 / THREADS) k_col
                     w.bpos[b0 + i] = pos[i];
                 }
             }
+            if (solved && a.ufParent) {
+                // The team's islands, in the shared memory the body cache used: links between two dynamic bodies.
+                __syncthreads();
+                uint32_t* par = reinterpret_cast<uint32_t*>(teamCache);
+                for (uint32_t i = threadIdx.x; i < nb; i += THREADS) par[i] = i;
+                __syncthreads();
+                const uint2* pb = a.s.pairBodies + lo;
+                for (uint32_t j = threadIdx.x; j < hi - lo; j += THREADS) {
+                    const uint2 q = pb[j];
+                    if ((q.x & PAIR_DYNAMIC) && (q.y & PAIR_DYNAMIC))
+                        team_union(par, (q.x & PAIR_BODY) - b0, (q.y & PAIR_BODY) - b0);
+                }
+                __syncthreads();
+                for (uint32_t i = threadIdx.x; i < nb; i += THREADS) a.ufParent[b0 + i] = b0 + team_find(par, i);
+            }
         } else {
             __syncthreads();
-            color_and_solve<BlockSync, GlobalBodies, PIPELINED>(
+            const bool solved = color_and_solve<BlockSync, GlobalBodies, PIPELINED>(
                 w, GlobalBodies{w.bvel, w.bpos, a.s.bodyMax, a.s.bodyMask}, m + lo, hi - lo, ls, a.velIters,
                 a.posIters, threadIdx.x, THREADS, BlockSync{}, &a.counters->colors, &a.counters->status);
+            if (solved && a.ufParent) {
+                __syncthreads();
+                const uint2* pb = a.s.pairBodies + lo;
+                for (uint32_t j = threadIdx.x; j < hi - lo; j += THREADS) {
+                    const uint2 q = pb[j];
+                    if ((q.x & PAIR_DYNAMIC) && (q.y & PAIR_DYNAMIC))
+                        team_union(a.ufParent, q.x & PAIR_BODY, q.y & PAIR_BODY);
+                }
+            }
         }
         __syncthreads();
     }
