@@ -354,8 +354,10 @@ public:
     void findCollisionsInCircle(std::span<const ObjectDenseIndex> collidersToCheck, Vec2 pos, Real radius,
                                 std::vector<std::pair<ObjectDenseIndex, Real>>& outColliding) const
     {
-        // Every collider the circle touches passes the circle query too, so the device's answer over the query's
-        // colliders holds all of them; it is filtered to the colliders given.
+        // The device answers over the colliders whose broad-phase AABBs (those of the last step) pass the circle
+        // query, filtered to the colliders given. Between steps the AABBs are current, so that set holds every
+        // collider the circle touches; a collider moved since the last step by a command is only seen from the next
+        // step on (the reference tests every given collider at its current pose).
         uint32_t n = 0;
         detail::check(ag2d_world_query_circle_contacts(world, pos.x, pos.y, radius, AG2D_TREE_ALL, nullptr, nullptr, 0,
                                                         &n));

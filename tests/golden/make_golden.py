@@ -15,6 +15,8 @@ Fixtures:
     wrap_edge.npz           body rotations around wrap boundaries (SIMD body and scalar tail)
     traj_c1_n256.npz        600-step trajectory statistics of a 256-polygon scene
     traj_c1_n2048.npz       the same statistics of the full c1 configuration (2,048 polygons, seed 0, 600 steps)
+    contacts_capsules_n1500_step300.npz  circle contacts and shape queries on a 1,500-body pile with capsules among
+                            circles, boxes and polygons (findCollisionsInCircle's capsule branch)
     towers_s0_step33.npz    40 three-box towers: the step in which 36 of them fall asleep (their manifolds go to
                             the sleeping-island store), with the store after the step
     towers_s0_step140.npz   the same scene: the step in which four towers wake and their stored manifolds return
@@ -219,11 +221,11 @@ def query_fixture(path, n=600, steps=700, queries=24):
     print(f"{os.path.basename(path)}: {len(shapes)} queries, groups {keep['q.col.groupStarts'].tolist()}")
 
 
-def contacts_fixture(path, n=1500, steps=300, queries=60):
+def contacts_fixture(path, n=1500, steps=300, queries=60, capsules=False):
     """Circle contacts (agref_circle_contacts: the circle query's colliders through findCollisionsInCircle) and
-    shape queries on a mixed-shape pile (circles, boxes, polygons in a U container), with the full reference state
-    they ran on, so that a world loaded from it answers the same queries."""
-    scene = scenes.make_c2(n, 2, columns=30)
+    shape queries on a mixed-shape pile (circles, boxes, polygons in a U container; with 'capsules', capsules among
+    them), with the full reference state they ran on, so that a world loaded from it answers the same queries."""
+    scene = scenes.make_capsule_mix(n, 0) if capsules else scenes.make_c2(n, 2, columns=30)
     r = refapi.RefSim(scene)
     r.update(steps)
     r.dump_state("q.")
@@ -286,6 +288,7 @@ FIXTURES = {
     "c5_ccd_hit.npz": ccd_fixture,
     "query_c1_n600_step700.npz": query_fixture,
     "contacts_c2_n1500_step300.npz": contacts_fixture,
+    "contacts_capsules_n1500_step300.npz": lambda p: contacts_fixture(p, capsules=True),
 }
 
 

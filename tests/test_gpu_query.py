@@ -62,11 +62,12 @@ def test_query_capacity_and_counts(world):
         world._query(7, [0, 0, 1, 1], ag2d.TREE_ALL)
 
 
-@pytest.fixture(scope="module")
-def loaded():
-    """A world holding the reference's own state of a mixed-shape pile (circles, boxes, polygons in a U container,
-    1,500 bodies after 300 steps), collider poses and AABBs included, with the reference's query answers."""
-    g = parity.load("contacts_c2_n1500_step300.npz")
+@pytest.fixture(scope="module", params=["contacts_c2_n1500_step300.npz", "contacts_capsules_n1500_step300.npz"])
+def loaded(request):
+    """A world holding the reference's own state of a mixed-shape pile (circles, boxes, polygons in a U container;
+    in the second fixture capsules too, 1,500 bodies after 300 steps), collider poses and AABBs included, with the
+    reference's query answers."""
+    g = parity.load(request.param)
     w = ag2d.World()
     w.load_state(g, "q.", g["meta.materials"], with_poses=True)
     return w, g
