@@ -66,6 +66,8 @@ typedef struct ag2d_counters {
     uint32_t sleeping;      /* bodies sleeping after the step */
     uint32_t ccd_hits;      /* bodies moved back by continuous collision detection in the last step */
     uint32_t restored;      /* manifolds of woken islands that joined the last step whole (from the sleep store) */
+    uint32_t events;        /* collision events recorded in the last step */
+    uint32_t stored;        /* sleeping-island manifolds held when the last step began */
     uint64_t steps;         /* steps taken by this world */
     uint64_t launches;      /* kernel launches issued by this world so far */
     uint64_t list_rebuilds; /* work-list rebuilds after sleep/wake changes */
@@ -166,6 +168,8 @@ enum ag2d_phase {
                                       hit bodies back (uses the poses AG2D_PHASE_INTEGRATE recorded) */
     AG2D_PHASE_WAKE,               /* wake the sleeping islands AG2D_MANIFOLDS touch, then bring their stored
                                       manifolds into AG2D_MANIFOLDS (Simulation.cpp:440-444) */
+    AG2D_PHASE_EVENTS              /* collision events of AG2D_MANIFOLDS from the current velocities (the solver's
+                                      input), into ag2d_world_collision_events; no callback is called */
 };
 
 /* ---- library ---- */
@@ -243,6 +247,46 @@ int32_t ag2d_world_set_body_mass(ag2d_world* world, uint64_t body, float mass);
 int32_t ag2d_world_set_body_inertia(ag2d_world* world, uint64_t body, float inertia);
 /* Applies the queued commands now (Simulation::flushCommands, Simulation.cpp:453-456). */
 int32_t ag2d_world_flush_commands(ag2d_world* world);
+
+/* ---- collision events: Simulation::createCollisionCallback / destroyCollisionCallback /
+ * setColliderCollisionCallback (Simulation.h:169-179, Simulation.cpp:130-171; the table of
+ * SimulationImpl/CollisionCallbackManager.h) ----
+ * A collider with a callback and an impulse threshold gets an event, from its side, for each manifold of a step
+ * whose impact impulse (the largest over the contact points of approach speed along the normal times the normal
+ * effective mass, before solving; BodyCollisionSolver.cpp:320-387) is positive and reaches the threshold. Events
+ * are recorded while collision events are enabled (the default, SimulationSettings::collisionEventsEnabled,
+ * Simulation.h:60) and a callback exists, and after each step the world calls each event's callback in manifold
+ * order, side a before side b (the reference dispatches at the end of physicsStep, Simulation.cpp:174-180, 450;
+ * here after the step's sleep pass). A callback may queue body commands and change callbacks; it may not step
+ * the world. Per world: a batch engine's worlds record no events (AG2D_ERR_UNSUPPORTED). */
+typedef struct ag2d_collision_event {
+    uint32_t self, other;            /* dense collider indices (the reference's collider handles) */
+    uint32_t self_body, other_body;  /* dense body indices */
+    uint64_t self_body_handle;       /* body handles; UINT64_MAX in a world made by ag2d_world_load_state */
+    uint64_t other_body_handle;
+    float point_x, point_y;          /* average of the manifold's contact points */
+    float normal_x, normal_y;        /* from self towards other */
+    float impulse;                   /* the impact impulse */
+    uint16_t callback_id;
+    uint16_t pad;
+} ag2d_collision_event;
+typedef void (*ag2d_collision_callback)(const ag2d_collision_event* event, ag2d_world* world, void* user_data);
+/* A callback slot (ids from 1; a destroyed id is reused first). AG2D_ERR_INVALID_ARG for a null function,
+ * AG2D_ERR_CAPACITY when all 65,535 ids are in use (the reference returns nullopt for both). */
+int32_t ag2d_world_create_collision_callback(ag2d_world* world, ag2d_collision_callback function, void* user_data,
+                                             uint16_t* out_id);
+/* Colliders using the id go back to no callback. AG2D_ERR_INVALID_ARG for id 0 and dead ids (reference: false). */
+int32_t ag2d_world_destroy_collision_callback(ag2d_world* world, uint16_t id);
+/* Id 0 clears the collider's callback (threshold ignored). AG2D_ERR_INVALID_ARG for a collider index out of range,
+ * a dead id, or a threshold that is negative or NaN (reference: false). */
+int32_t ag2d_world_set_collider_collision_callback(ag2d_world* world, uint32_t collider, uint16_t id,
+                                                   float impulse_threshold);
+/* SimulationSettings::collisionEventsEnabled (Simulation.h:59-60): 1 (the default) records events. */
+int32_t ag2d_world_set_collision_events(ag2d_world* world, int32_t enable);
+/* The last step's events, as dispatched (BodyCollisionSolver::getCollisionEvents, BodyCollisionSolver.h:125).
+ * out_count receives the full count; at most 'capacity' events are written. */
+int32_t ag2d_world_collision_events(ag2d_world* world, ag2d_collision_event* out_events, uint32_t capacity,
+                                    uint32_t* out_count);
 
 /* Replaces the world with a reference-layout state (parity harness: same inputs as the reference). */
 int32_t ag2d_world_load_state(ag2d_world* world, const ag2d_state_desc* state);

@@ -6,6 +6,8 @@
 //                                                                     getBodyCollisionData, getSimulationSettings
 //   PS_AGONY2D::ObjectAPI (ObjectAPI.h:14)      ag2d::ObjectAPI       createCircle/Box/Polygon (+ H variants),
 //                                                                     getBodyIndex, getBodies
+//   Simulation collision callbacks              createCollisionCallback, destroyCollisionCallback,
+//   (Simulation.h:169-179)                      setColliderCollisionCallback, getCollisionEvents
 //   SimulationSettings (Simulation.h:50-76)     ag2d::SimulationSettings
 //   FixedClock (SimulationImpl/FixedClock.h)    the same accumulator semantics inside Simulation::update
 //   Body/Circle/Box/PolygonCreateParams         same fields (SimulationImpl/ObjectCreateParams.h:14-95)
@@ -19,6 +21,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <limits>
+#include <map>
 #include <memory>
 #include <optional>
 #include <span>
@@ -109,6 +113,21 @@ struct IntegratorSettings {
     Vec2 gravity{0, Real(-9.81)};
     Real angularVelocityDamping = 1;   // 1: off
 };
+// Collision events (Types/CollisionEvent.h:10-31). Colliders are named by dense index, which is stable in this
+// library (the reference names them by collider handle); bodies by handle.
+using CollisionCallbackIndex = uint16_t;
+inline constexpr Real NO_COLLISION_EVENT_THRESHOLD = std::numeric_limits<Real>::max();
+struct CollisionEvent {
+    ObjectDenseIndex self = 0, other = 0;
+    Handle selfBody, otherBody;
+    Vec2 point;      // average of the manifold's contact points
+    Vec2 normal;     // from self towards other
+    Real impulse = 0;   // impact impulse: max over the contacts of approach speed x normal effective mass, pre-solve
+    CollisionCallbackIndex callbackId = 0;
+};
+class Simulation;
+using CollisionCallback = void (*)(const CollisionEvent& event, Simulation& simulation, void* userData);
+
 struct SimulationSettings {
     FixedClockSettings clockSettings;
     uint32_t collisionVelocitySolvingIterations = 6;
@@ -117,6 +136,7 @@ struct SimulationSettings {
     bool continuousCollisionEnabled = true;
     Real sleepSpeedThreshold = Real(0.1);
     Real sleepTimeThreshold = Real(0.5);
+    bool collisionEventsEnabled = true;        // also requires at least one collision callback
     int device = 0;                            // CUDA device ordinal
 };
 
@@ -402,6 +422,7 @@ public:
     void update(Real deltaTime)
     {
         if (!(deltaTime > 0)) return;
+        detail::check(ag2d_world_set_collision_events(world, settings.collisionEventsEnabled ? 1 : 0));
         accumulator += std::fmin(deltaTime, settings.clockSettings.maxDeltaTimePerUpdateCall);
         const uint32_t steps = uint32_t(std::floor(accumulator / settings.clockSettings.updateInterval));
         accumulator -= Real(steps) * settings.clockSettings.updateInterval;
@@ -429,6 +450,49 @@ public:
     }
 
     const SimulationSettings& getSimulationSettings() const noexcept { return settings; }
+    // collisionEventsEnabled is read at every update; the other fields when the Simulation is constructed.
+    SimulationSettings& getSimulationSettings() noexcept { return settings; }
+
+    // Collision callbacks (Simulation.h:169-179): fired after each step, per collider side, when a manifold's
+    // impact impulse reaches the collider's threshold. nullopt for a null function or a full table.
+    std::optional<CollisionCallbackIndex> createCollisionCallback(CollisionCallback function, void* userData = nullptr)
+    {
+        if (!function) return std::nullopt;
+        auto entry = std::make_unique<CallbackEntry>(CallbackEntry{this, function, userData});
+        uint16_t id = 0;
+        const int32_t rc = ag2d_world_create_collision_callback(world, &Simulation::dispatch, entry.get(), &id);
+        if (rc == AG2D_ERR_CAPACITY) return std::nullopt;
+        detail::check(rc);
+        callbackEntries[id] = std::move(entry);
+        return id;
+    }
+    // Colliders using it are reset to no callback. false for id 0 and dead ids.
+    bool destroyCollisionCallback(CollisionCallbackIndex callbackIndex)
+    {
+        if (ag2d_world_destroy_collision_callback(world, callbackIndex) != AG2D_OK) return false;
+        callbackEntries.erase(callbackIndex);
+        return true;
+    }
+    // Id 0 clears the collider's callback (threshold ignored). false for an invalid collider, a dead id, or a
+    // negative threshold.
+    bool setColliderCollisionCallback(ObjectDenseIndex colliderIndex, CollisionCallbackIndex callbackIndex,
+                                      Real impulseThreshold)
+    {
+        return ag2d_world_set_collider_collision_callback(world, colliderIndex, callbackIndex, impulseThreshold) ==
+               AG2D_OK;
+    }
+    // The last step's events in dispatch order (BodyCollisionSolver::getCollisionEvents, BodyCollisionSolver.h:125).
+    std::vector<CollisionEvent> getCollisionEvents() const
+    {
+        uint32_t n = 0;
+        detail::check(ag2d_world_collision_events(world, nullptr, 0, &n));
+        std::vector<ag2d_collision_event> raw(n);
+        if (n) detail::check(ag2d_world_collision_events(world, raw.data(), n, &n));
+        std::vector<CollisionEvent> out;
+        out.reserve(raw.size());
+        for (const ag2d_collision_event& e : raw) out.push_back(convert(e));
+        return out;
+    }
     // Simulation::getBroadPhaseCollisionDetector / getNarrowPhaseCollisionDetector (Simulation.h:183-184), for their
     // query entry points.
     BroadPhaseCollisionDetector getBroadPhaseCollisionDetector() const noexcept { return BroadPhaseCollisionDetector(world); }
@@ -436,10 +500,36 @@ public:
     ag2d_world* handle() noexcept { return world; }
 
 private:
+    struct CallbackEntry {
+        Simulation* sim;
+        CollisionCallback fn;
+        void* user;
+    };
+    static CollisionEvent convert(const ag2d_collision_event& e)
+    {
+        CollisionEvent ev;
+        ev.self = e.self;
+        ev.other = e.other;
+        ev.selfBody = Handle{e.self_body_handle};
+        ev.otherBody = Handle{e.other_body_handle};
+        ev.point = Vec2{e.point_x, e.point_y};
+        ev.normal = Vec2{e.normal_x, e.normal_y};
+        ev.impulse = e.impulse;
+        ev.callbackId = e.callback_id;
+        return ev;
+    }
+    // The C callback of every id: the entry is copied first, so the user function may destroy its own id.
+    static void dispatch(const ag2d_collision_event* e, ag2d_world*, void* user)
+    {
+        const CallbackEntry entry = *static_cast<const CallbackEntry*>(user);
+        entry.fn(convert(*e), *entry.sim, entry.user);
+    }
+
     SimulationSettings settings;
     ag2d_world* world = nullptr;
     std::unique_ptr<ObjectAPI> api;
     Real accumulator = 0;
+    std::map<CollisionCallbackIndex, std::unique_ptr<CallbackEntry>> callbackEntries;
 };
 
 }  // namespace ag2d

@@ -922,6 +922,59 @@ void ora_solve_f64(ora_world *w, ora_manifold *m, int64_t n, const int64_t *orde
 }
 
 /* ------------------------------------------------------------------------------------------------------------ */
+/* Collision events (Solving/BodyCollisionSolver.cpp:320-387)                                                    */
+/* ------------------------------------------------------------------------------------------------------------ */
+
+int64_t ora_collision_events(const ora_world *w, const ora_manifold *m, int64_t n, const uint32_t *callback,
+                             const float *threshold, ora_event *out, int64_t cap)
+{
+    int64_t k = 0;
+    for (int64_t c = 0; c < n; c++) {
+        const ora_manifold *d = m + c;
+        const uint32_t bA = w->bodyIndex[d->a], bB = w->bodyIndex[d->b];
+        const float cAx = w->comX[bA], cAy = w->comY[bA], cBx = w->comX[bB], cBy = w->comY[bB];
+        const float iIA = w->invInertia[bA], iIB = w->invInertia[bB];
+        const float effMass = w->invMass[bA] + w->invMass[bB];
+        const float vAx = w->velX[bA], vAy = w->velY[bA], wA = w->angVel[bA];
+        const float vBx = w->velX[bB], vBy = w->velY[bB], wB = w->angVel[bB];
+        /* :320-350 the per-point terms of the constraint data; impactImpulse = fmax(impactImpulse, negVn * nm). */
+        float impact = 0.0f;
+        for (uint32_t i = 0; i < d->count; i++) {
+            const float rAx = d->px[i] - cAx, rAy = d->py[i] - cAy, rBx = d->px[i] - cBx, rBy = d->py[i] - cBy;
+            const float rAn = (-rAy) * d->nx + rAx * d->ny;
+            const float rBn = (-rBy) * d->nx + rBx * d->ny;
+            const float nd = effMass + rAn * rAn * iIA + rBn * rBn * iIB;
+            const float nm = nd > 0.0f ? 1.0f / nd : 0.0f;
+            const float negVn = -(((vBx - vAx) * d->nx + (vBy - vAy) * d->ny) + rBn * wB - rAn * wA);
+            impact = rmax_f32(impact, negVn * nm);
+        }
+        /* :353-387 the event of each side whose collider opted in at a threshold the impulse reaches. */
+        if (impact <= 0.0f) continue;
+        const uint32_t cbA = callback[d->a], cbB = callback[d->b];
+        const int fireA = cbA != 0 && impact >= threshold[d->a];
+        const int fireB = cbB != 0 && impact >= threshold[d->b];
+        if (!fireA && !fireB) continue;
+        const float px = d->count > 1 ? (d->px[0] + d->px[1]) * 0.5f : d->px[0];
+        const float py = d->count > 1 ? (d->py[0] + d->py[1]) * 0.5f : d->py[0];
+        if (fireA) {
+            if (k < cap) {
+                ora_event e = {d->a, d->b, bA, bB, cbA, px, py, d->nx, d->ny, impact};
+                out[k] = e;
+            }
+            k++;
+        }
+        if (fireB) {
+            if (k < cap) {
+                ora_event e = {d->b, d->a, bB, bA, cbB, px, py, -d->nx, -d->ny, impact};
+                out[k] = e;
+            }
+            k++;
+        }
+    }
+    return k <= cap ? k : -k;
+}
+
+/* ------------------------------------------------------------------------------------------------------------ */
 /* Islands and sleeping (IslandManager.cpp:7-116; ObjectManager.cpp:1438-1491)                                   */
 /* ------------------------------------------------------------------------------------------------------------ */
 

@@ -97,6 +97,18 @@ void ora_solve_f64(ora_world *w, ora_manifold *m, int64_t n, const int64_t *orde
                    uint32_t pos_iters, double *io_vel /* 3 per body: vx, vy, w */, double *io_pos /* 2 per body */,
                    double *out_impulses /* 4 per manifold */);
 
+/* ---- collision events (BodyCollisionSolver::computeConstraintData, Solving/BodyCollisionSolver.cpp:320-387) ----
+ * For each manifold in list order, the impact impulse from the world's current velocities (the largest over the
+ * contact points of the approach speed along the normal times the normal effective mass, from 0 by std::fmax); a
+ * side fires when its collider's callback id is not 0, the impulse is positive and it reaches the collider's
+ * threshold. Side a's event comes before side b's. Returns the number of events, or -(needed) if cap is too small. */
+typedef struct ora_event {
+    uint32_t self, other, selfBody, otherBody, callback;
+    float px, py, nx, ny, impulse;
+} ora_event;
+int64_t ora_collision_events(const ora_world *w, const ora_manifold *m, int64_t n, const uint32_t *callback,
+                             const float *threshold, ora_event *out, int64_t cap);
+
 /* ---- islands and sleep flags ----
  * Island ids for dynamic bodies from body-pair edges (ids ordered by DSU root, IslandManager.cpp:36-80), then the
  * sleep-timer update and the per-island "all quiet long enough" AND (ObjectManager.cpp:1438-1491).

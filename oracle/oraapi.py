@@ -47,6 +47,10 @@ MANIFOLD_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("nx", "<f4"), ("ny", "<f
                            ("jn", "<f4", 2), ("jt", "<f4", 2)])
 assert MANIFOLD_DTYPE.itemsize == ctypes.sizeof(Manifold)
 
+EVENT_DTYPE = np.dtype([("self", "<u4"), ("other", "<u4"), ("selfBody", "<u4"), ("otherBody", "<u4"),
+                        ("callback", "<u4"), ("px", "<f4"), ("py", "<f4"), ("nx", "<f4"), ("ny", "<f4"),
+                        ("impulse", "<f4")])
+
 _lib = None
 
 
@@ -81,6 +85,8 @@ def lib():
         L.ora_islands.restype = u32
         L.ora_islands.argtypes = [W, vp, i64, vp]
         L.ora_update_sleeping.argtypes = [W, vp, u32, f, f, f, vp]
+        L.ora_collision_events.argtypes = [W, vp, i64, vp, vp, vp, i64]
+        L.ora_collision_events.restype = i64
         _lib = L
     return _lib
 
@@ -216,6 +222,18 @@ class OraWorld:
                             vel_iters, pos_iters, vel.ctypes.data, pos.ctypes.data, imp.ctypes.data)
         assert vel.shape[0] == nb
         return vel, pos, imp[:m.shape[0]]
+
+    def collision_events(self, manifolds: np.ndarray, callback: np.ndarray, threshold: np.ndarray) -> np.ndarray:
+        """Events (EVENT_DTYPE, dense indices) of the manifolds from the world's current velocities, in manifold
+        order with side a first, for colliders opted in by callback id and threshold."""
+        m = np.ascontiguousarray(manifolds)
+        cb = np.ascontiguousarray(callback, dtype=np.uint32)
+        th = np.ascontiguousarray(threshold, dtype=np.float32)
+        out = np.zeros(max(1, 2 * m.shape[0]), EVENT_DTYPE)
+        k = lib().ora_collision_events(self.ref, m.ctypes.data, m.shape[0], cb.ctypes.data, th.ctypes.data,
+                                       out.ctypes.data, out.size)
+        assert k >= 0
+        return out[:k].copy()
 
     def islands(self, body_edges: np.ndarray):
         e = np.ascontiguousarray(body_edges, dtype=np.uint32).reshape(-1, 2)

@@ -121,6 +121,13 @@ namespace
         size_t threads = 0;
         std::map<std::string, std::vector<uint8_t>> blobs;
         std::vector<uint32_t> createdGeneration;   // per body handle slot: its generation when the body was created
+        // Collision events the recording callback received (Types/CollisionEvent.h:18-26), by handle slots.
+        struct Event
+        {
+            uint32_t self, other, selfBody, otherBody, callback;
+            float px, py, nx, ny, impulse;
+        };
+        std::vector<Event> events;
 
         template <class T>
         void put(const std::string& name, const T* data, size_t count)
@@ -206,6 +213,10 @@ namespace
         }
         h->putv(p + "col.handleSlot", slot);
         h->putv(p + "col.handleGen", gen);
+        std::vector<uint32_t> cb(c.getCount());
+        for (size_t i = 0; i < c.getCount(); i++) cb[i] = uint32_t(c.callbackId[i]);
+        h->putv(p + "col.callbackId", cb);
+        h->putv(p + "col.eventThreshold", c.eventThreshold);
 
         h->putv(p + "circle.colliderIndices", om.circles.colliderIndices);
         h->putv(p + "circle.radius", om.circles.radius);
@@ -440,6 +451,57 @@ extern "C"
     void agref_flush_commands(void* hp)
     {
         static_cast<Harness*>(hp)->sim.flushCommands();
+    }
+
+    // Collision callbacks (Simulation::createCollisionCallback / setColliderCollisionCallback /
+    // destroyCollisionCallback, Simulation.cpp:130-171) with one recording function: every event dispatched at the
+    // end of a step (Simulation.cpp:174-180, 450) is kept until agref_dump_events.
+    static void recordEvent(const CollisionEvent& e, Simulation&, void* user)
+    {
+        static_cast<Harness*>(user)->events.push_back(Harness::Event{
+            e.self.slot, e.other.slot, e.selfBody.slot, e.otherBody.slot, uint32_t(e.callbackId),
+            e.point.x, e.point.y, e.normal.x, e.normal.y, e.impulse});
+    }
+    int32_t agref_create_event_callback(void* hp)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        const auto id = h->sim.createCollisionCallback(&recordEvent, h);
+        return id ? int32_t(*id) : -1;
+    }
+    int32_t agref_destroy_event_callback(void* hp, uint32_t id)
+    {
+        return static_cast<Harness*>(hp)->sim.destroyCollisionCallback(CollisionCallbackIndex(id)) ? 1 : 0;
+    }
+    int32_t agref_set_collider_callback(void* hp, uint32_t collider, uint32_t id, float threshold)
+    {
+        return static_cast<Harness*>(hp)->sim.setColliderCollisionCallback(collider, CollisionCallbackIndex(id),
+                                                                          threshold) ? 1 : 0;
+    }
+    void agref_set_events_enabled(void* hp, int32_t enable)
+    {
+        static_cast<Harness*>(hp)->sim.getSimulationSettings().collisionEventsEnabled = enable != 0;
+    }
+    // The recorded events as blobs <prefix>ev.{self,other,selfBody,otherBody,callback} (handle slots, ids) and
+    // ev.{px,py,nx,ny,impulse}, in dispatch order; the record is then cleared.
+    void agref_dump_events(void* hp, const char* prefix)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        const std::string p(prefix);
+        const size_t n = h->events.size();
+        std::vector<uint32_t> u[5];
+        std::vector<float> f[5];
+        for (auto& v : u) v.resize(n);
+        for (auto& v : f) v.resize(n);
+        for (size_t i = 0; i < n; i++)
+        {
+            const auto& e = h->events[i];
+            u[0][i] = e.self; u[1][i] = e.other; u[2][i] = e.selfBody; u[3][i] = e.otherBody; u[4][i] = e.callback;
+            f[0][i] = e.px; f[1][i] = e.py; f[2][i] = e.nx; f[3][i] = e.ny; f[4][i] = e.impulse;
+        }
+        const char* un[5] = {"ev.self", "ev.other", "ev.selfBody", "ev.otherBody", "ev.callback"};
+        const char* fn[5] = {"ev.px", "ev.py", "ev.nx", "ev.ny", "ev.impulse"};
+        for (int k = 0; k < 5; k++) { h->putv(p + un[k], u[k]); h->putv(p + fn[k], f[k]); }
+        h->events.clear();
     }
 
     // Dense body index of a handle slot (UINT32_MAX when destroyed).

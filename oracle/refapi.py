@@ -86,13 +86,22 @@ def lib():
         L.agref_circle_contacts.argtypes = [vp, f, f, f, u32, vp, vp, ctypes.c_uint64]
         L.agref_circle_contacts.restype = ctypes.c_int64
         L.agref_fastcossin.argtypes = [vp, vp, vp, ctypes.c_uint64]
+        L.agref_create_event_callback.restype = i32
+        L.agref_create_event_callback.argtypes = [vp]
+        L.agref_destroy_event_callback.restype = i32
+        L.agref_destroy_event_callback.argtypes = [vp, u32]
+        L.agref_set_collider_callback.restype = i32
+        L.agref_set_collider_callback.argtypes = [vp, u32, u32, f]
+        L.agref_set_events_enabled.argtypes = [vp, i32]
+        L.agref_dump_events.argtypes = [vp, ctypes.c_char_p]
         _lib = L
     return _lib
 
 
 _U32_SUFFIXES = ("bodyIndex", "materialIndex", "shapeType", "shapeIndex", "groupStarts", "handleSlot", "handleGen",
                  "islandId", "sleepIslandId", "colliderIndices", "counts", "colA", "colB", "slotA", "slotB", "count",
-                 "ids", "sorted", "morton", "pairs", "spatialDirty")
+                 "ids", "sorted", "morton", "pairs", "spatialDirty", "callbackId", "self", "other", "selfBody",
+                 "otherBody", "callback")
 
 
 def _dtype_for(name: str):
@@ -246,6 +255,26 @@ class RefSim:
         sdf = np.empty(max(int(n), 1), np.float32)
         L.agref_circle_contacts(self.h, x, y, r, trees, idx.ctypes.data, sdf.ctypes.data, idx.size)
         return idx[:int(n)], sdf[:int(n)]
+
+    def create_event_callback(self) -> int:
+        """A collision callback that records every event it receives (Simulation::createCollisionCallback)."""
+        return int(lib().agref_create_event_callback(self.h))
+
+    def destroy_event_callback(self, cb: int) -> bool:
+        return bool(lib().agref_destroy_event_callback(self.h, cb))
+
+    def set_collider_callback(self, collider: int, cb: int, threshold: float) -> bool:
+        """Simulation::setColliderCollisionCallback on a dense collider index."""
+        return bool(lib().agref_set_collider_callback(self.h, collider, cb, threshold))
+
+    def set_events_enabled(self, enable: bool):
+        lib().agref_set_events_enabled(self.h, 1 if enable else 0)
+
+    def events(self, prefix: str = "e.") -> dict:
+        """The events recorded since the last call (handle slots, points, normals, impulses), in dispatch order."""
+        lib().agref_dump_events(self.h, prefix.encode())
+        return {k[len(prefix) + 3:]: self.blob(k) for k in (prefix + "ev." + n for n in
+                ("self", "other", "selfBody", "otherBody", "callback", "px", "py", "nx", "ny", "impulse"))}
 
     @property
     def manifold_count(self) -> int:

@@ -33,7 +33,7 @@ DYN_SORTED, DYN_MORTON, PAIRS, MANIFOLDS, PREV_MANIFOLDS, SOLVE_ORDER, COLOR_STA
     ISLAND_IDS = range(64, 73)
 # enum ag2d_phase
 PHASE_INTEGRATE, PHASE_SPATIAL_FULL, PHASE_SPATIAL_DYNAMIC, PHASE_BROAD, PHASE_NARROW, PHASE_SOLVE, \
-    PHASE_ISLANDS, PHASE_COLLIDE, PHASE_CCD, PHASE_WAKE = range(1, 11)
+    PHASE_ISLANDS, PHASE_COLLIDE, PHASE_CCD, PHASE_WAKE, PHASE_EVENTS = range(1, 12)
 
 MANIFOLD_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("nx", "<f4"), ("ny", "<f4"), ("depth", "<f4"),
                            ("count", "<u4"), ("id0", "<u4"), ("id1", "<u4"), ("px0", "<f4"), ("py0", "<f4"),
@@ -73,9 +73,26 @@ class Counters(ctypes.Structure):
     _fields_ = [("status", ctypes.c_uint32), ("pairs", ctypes.c_uint32), ("manifolds", ctypes.c_uint32),
                 ("colors", ctypes.c_uint32), ("woke", ctypes.c_uint32), ("slept", ctypes.c_uint32),
                 ("warm_hits", ctypes.c_uint32), ("sleeping", ctypes.c_uint32), ("ccd_hits", ctypes.c_uint32),
-                ("restored", ctypes.c_uint32), ("steps", ctypes.c_uint64),
+                ("restored", ctypes.c_uint32), ("events", ctypes.c_uint32), ("stored", ctypes.c_uint32),
+                ("steps", ctypes.c_uint64),
                 ("launches", ctypes.c_uint64), ("list_rebuilds", ctypes.c_uint64), ("retries", ctypes.c_uint64),
                 ("regrows", ctypes.c_uint64), ("host_ms", ctypes.c_double), ("sync_ms", ctypes.c_double)]
+
+
+class CollisionEvent(ctypes.Structure):
+    """ag2d_collision_event: one collision event from one collider's side (Types/CollisionEvent.h:18-26)."""
+    _fields_ = [("self", ctypes.c_uint32), ("other", ctypes.c_uint32), ("self_body", ctypes.c_uint32),
+                ("other_body", ctypes.c_uint32), ("self_body_handle", ctypes.c_uint64),
+                ("other_body_handle", ctypes.c_uint64), ("point_x", ctypes.c_float), ("point_y", ctypes.c_float),
+                ("normal_x", ctypes.c_float), ("normal_y", ctypes.c_float), ("impulse", ctypes.c_float),
+                ("callback_id", ctypes.c_uint16), ("pad", ctypes.c_uint16)]
+
+
+EVENT_DTYPE = np.dtype([(n, {ctypes.c_uint32: "<u4", ctypes.c_uint64: "<u8", ctypes.c_float: "<f4",
+                             ctypes.c_uint16: "<u2"}[t]) for n, t in CollisionEvent._fields_])
+assert EVENT_DTYPE.itemsize == ctypes.sizeof(CollisionEvent) == 56
+COLLISION_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.POINTER(CollisionEvent), ctypes.c_void_p, ctypes.c_void_p)
+NO_COLLISION_EVENT_THRESHOLD = float(np.finfo(np.float32).max)
 
 
 class Tuning(ctypes.Structure):
@@ -156,6 +173,11 @@ def _load():
     for name in ("rotation", "angular_velocity", "mass", "inertia"):
         getattr(L, f"ag2d_world_set_body_{name}").argtypes = [vp, u64, ctypes.c_float]
     L.ag2d_world_flush_commands.argtypes = [vp]
+    L.ag2d_world_create_collision_callback.argtypes = [vp, COLLISION_CALLBACK, vp, ctypes.POINTER(ctypes.c_uint16)]
+    L.ag2d_world_destroy_collision_callback.argtypes = [vp, ctypes.c_uint16]
+    L.ag2d_world_set_collider_collision_callback.argtypes = [vp, u32, ctypes.c_uint16, ctypes.c_float]
+    L.ag2d_world_set_collision_events.argtypes = [vp, i32]
+    L.ag2d_world_collision_events.argtypes = [vp, vp, u32, ctypes.POINTER(u32)]
     L.ag2d_world_load_state.argtypes = [vp, ctypes.POINTER(StateDesc)]
     L.ag2d_world_step.argtypes = [vp, i32]
     L.ag2d_world_counters.argtypes = [vp, ctypes.POINTER(Counters)]
@@ -386,6 +408,39 @@ class World:
 
     def flush_commands(self):
         _check(lib.ag2d_world_flush_commands(self.h))
+
+    # --- collision events (Simulation::createCollisionCallback / destroyCollisionCallback /
+    # setColliderCollisionCallback, Simulation.h:169-179) ---
+    def create_collision_callback(self, fn) -> int:
+        """Registers fn(event) (a CollisionEvent) to be called after each step for the events of the colliders that
+        use the returned id; returns the id."""
+        def trampoline(ev, _world, _user):
+            fn(ev.contents)
+        c = COLLISION_CALLBACK(trampoline)
+        out = ctypes.c_uint16()
+        _check(lib.ag2d_world_create_collision_callback(self.h, c, None, ctypes.byref(out)))
+        self._callbacks = getattr(self, "_callbacks", {})
+        self._callbacks[int(out.value)] = c   # the C function pointer lives as long as the id
+        return int(out.value)
+
+    def destroy_collision_callback(self, cb: int):
+        _check(lib.ag2d_world_destroy_collision_callback(self.h, cb))
+        getattr(self, "_callbacks", {}).pop(int(cb), None)
+
+    def set_collider_collision_callback(self, collider: int, cb: int, threshold: float = 0.0):
+        _check(lib.ag2d_world_set_collider_collision_callback(self.h, collider, cb, threshold))
+
+    def set_collision_events(self, enable: bool):
+        _check(lib.ag2d_world_set_collision_events(self.h, 1 if enable else 0))
+
+    def collision_events(self) -> np.ndarray:
+        """The last step's events (EVENT_DTYPE records), in the order they were dispatched."""
+        n = ctypes.c_uint32()
+        _check(lib.ag2d_world_collision_events(self.h, None, 0, ctypes.byref(n)))
+        out = np.zeros(int(n.value), EVENT_DTYPE)
+        if out.size:
+            _check(lib.ag2d_world_collision_events(self.h, out.ctypes.data, out.size, ctypes.byref(n)))
+        return out
 
     @classmethod
     def from_scene(cls, scene, device=0, **kw):

@@ -208,6 +208,13 @@ __global__ void k_circle_contacts(DeviceWorld w, float x, float y, float radius,
 __global__ void k_scatter_contacts(const uint32_t* flag, const uint32_t* offset, const float* dist, uint32_t n,
                                    uint32_t* list, float* listDist);
 
+// Collision events (k_events.cu): the events of the manifolds in man[0, min(*nMan, manCap)) whose colliders opted
+// in (cev), appended to ring (counters->events counts them all; STATUS_EVENT_OVERFLOW when more than ringCap).
+// Launched with a multiple of 32 threads a block, before the solver changes the velocities.
+__global__ void k_collision_events(DeviceWorld w, const ColliderEvent* cev, const Manifold* man,
+                                   const uint32_t* nMan, uint32_t manCap, EventRecord* ring, uint32_t ringCap,
+                                   StepCounters* counters);
+
 // Batch repacking (k_repack.cu). A segment copies 'count' elements from [src, ...) of the current array (fromNew
 // 0), or from the staged section of joining world 'src' (fromNew 1), to [dst, ...) of the new array; the deltas
 // shift the indices stored in the elements (new start - source start of that kind of element in the segment's

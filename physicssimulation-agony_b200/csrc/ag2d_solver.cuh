@@ -114,6 +114,29 @@ __device__ __forceinline__ void prep_constraint(const DeviceWorld& w, const Bodi
     k.pad = 0.0f;
 }
 
+// Impact impulse of a manifold for collision events (BodyCollisionSolver.cpp:320-350): the largest over its points
+// of the approach speed along the normal times the normal effective mass, from the velocities the constraint data
+// is built from. The arithmetic is prep_constraint's (rAn, rBn, the normal mass and negVn, in the same order), so
+// the value is the one the reference computes beside its constraint data.
+__device__ __forceinline__ float impact_impulse(const Manifold& m, float4 vA, float4 vB, float4 pA, float4 pB)
+{
+    const float effMass = vA.w + vB.w;
+    float impact = 0.0f;
+#pragma unroll
+    for (uint32_t i = 0; i < 2; i++) {
+        if (i >= m.count) break;
+        const float px = i == 0 ? m.px0 : m.px1, py = i == 0 ? m.py0 : m.py1;
+        const float rAx = px - pA.x, rAy = py - pA.y, rBx = px - pB.x, rBy = py - pB.y;
+        const float rAn = (-rAy) * m.nx + rAx * m.ny;
+        const float rBn = (-rBy) * m.nx + rBx * m.ny;
+        const float nd = effMass + rAn * rAn * pA.w + rBn * rBn * pB.w;
+        const float nm = nd > 0.0f ? 1.0f / nd : 0.0f;
+        const float negVn = -(((vB.x - vA.x) * m.nx + (vB.y - vA.y) * m.ny) + rBn * vB.z - rAn * vA.z);
+        impact = rfmaxf(impact, negVn * nm);   // std::fmax: a NaN product leaves the running value
+    }
+    return impact;
+}
+
 template <class Bodies>
 __device__ __forceinline__ void warm_constraint(const Bodies& B, const Constraint& k)
 {

@@ -26,6 +26,7 @@ enum StatusBits : uint32_t {
     STATUS_COLOR_OVERFLOW = 1u << 4,
     STATUS_HASH_FULL = 1u << 5,
     STATUS_STACK_OVERFLOW = 1u << 6,
+    STATUS_EVENT_OVERFLOW = 1u << 7,
 };
 
 // Counters written by the kernels and read back by the host after each step (one 64-byte transfer).
@@ -43,7 +44,8 @@ struct StepCounters {
     uint32_t restored;        // sleeping-island manifolds that joined this step's list whole
     uint32_t stored;          // sleeping-island manifolds held when the step began
     uint32_t staged;          // of which the woken islands' records taken out by this step's restore
-    uint32_t pad[3];
+    uint32_t events;          // collision events recorded (may exceed the event ring: STATUS_EVENT_OVERFLOW)
+    uint32_t pad[2];
 };
 
 // Manifold record (64 bytes), NarrowPhaseCollisionDetector.h:26-61 minus the handle union: colliders are stable
@@ -58,6 +60,23 @@ struct alignas(16) Manifold {
     float jn0, jt0, jn1, jt1;     // persistent impulse accumulators (warm start)
 };
 static_assert(sizeof(Manifold) == 64, "Manifold is 64 bytes");
+
+// Collision event (48 bytes), one per opted-in collider side of a manifold: the fields of the reference's
+// CollisionEvent (Types/CollisionEvent.h:18-26) with dense indices for the handles, plus the manifold it came from
+// and the side (0: self is the manifold's collider a) so the host can put the events in manifold order.
+struct alignas(16) EventRecord {
+    uint32_t manifold, side, self, other;
+    uint32_t selfBody, otherBody, callback;
+    float impulse;          // impact impulse: max over the points of approach speed x normal effective mass
+    float px, py, nx, ny;   // average of the contact points; the normal from self towards other
+};
+static_assert(sizeof(EventRecord) == 48, "EventRecord is 48 bytes");
+
+// Collider opt-in for collision events: callback id (0: none) and the impulse threshold.
+struct ColliderEvent {
+    uint32_t callback;
+    float threshold;
+};
 
 // Per-constraint solver record (128 bytes), built from a Manifold in solving (colour) order: the fields of
 // BodyCollisionSolver's VelocityHotData, PositionHotData, VelocityConstraintData and FrictionData.

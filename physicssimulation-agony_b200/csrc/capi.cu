@@ -449,6 +449,25 @@ struct ag2d_world {
     uint64_t stepsTaken = 0;
     std::vector<BodyCommand> commands;   // queued body commands, applied by flushCommands
 
+    // Collision callbacks (SimulationImpl/CollisionCallbackManager.h): slot 0 is the permanent "no callback",
+    // destroyed slots are reused last-in first-out.
+    struct CallbackEntry {
+        ag2d_collision_callback fn = nullptr;
+        void* user = nullptr;
+    };
+    std::vector<CallbackEntry> callbacks = std::vector<CallbackEntry>(1);
+    std::vector<uint8_t> callbackAlive = std::vector<uint8_t>(1, 1);
+    std::vector<uint16_t> callbackFree;
+    uint32_t callbacksAlive = 0;          // excluding slot 0
+    bool eventsEnabled = true;            // SimulationSettings::collisionEventsEnabled
+    std::vector<ColliderEvent> loadedOptIn;   // colliders' opt-ins of a world made by load_state (no host colliders)
+    bool optInDirty = true;               // cevent needs an upload
+    uint32_t optInColliders = 0;          // colliders with a callback, as last uploaded
+    bool recording = false;               // this step records events
+    bool dispatching = false;             // callbacks are running (a callback may not step the world)
+    uint32_t eventCap = 0;
+    std::vector<ag2d_collision_event> lastEvents;   // the last step's events, in dispatch order
+
     uint32_t nBodies = 0, nColliders = 0, nDynBody = 0, nDynCol = 0, nOther = 0, nStatic = 0;
     uint32_t nDestroyed = 0;   // bodies removed by destroy commands (still in the arrays, in no list)
     uint32_t pairCap = 0, manifoldCap = 0, hashCap = 0;
@@ -462,6 +481,9 @@ struct ag2d_world {
     DBuf<float> wrapCount, boundRadius, sleepTimer;
     DBuf<uint8_t> bstate;
     DBuf<uint32_t> sleepIsland;
+    // Collision events: per-collider opt-in and the step's event ring.
+    DBuf<ColliderEvent> cevent;
+    DBuf<EventRecord> eventRing;
     // Snapshot of the mutable body state (restored when a step overflows a buffer).
     DBuf<float4> snapVel, snapPos;
     DBuf<float2> snapRot;
@@ -1408,6 +1430,7 @@ struct ag2d_world {
         CK(cudaMemsetAsync(nIsle.p, 0, sizeof(uint32_t), s));
         isleUpper = 0;
         prevSegValid = false;
+        optInDirty = true;
         CK(cudaStreamSynchronize(s));
         hostDirty = false;
         listsDirty = true;
@@ -1911,6 +1934,100 @@ struct ag2d_world {
         swap_bufs(b, nb);
     }
 
+    // Collision events --------------------------------------------------------------------------------------
+    // Colliders the world has: the host's (created worlds) or the device's (a world made by load_state).
+    uint32_t colliderCount() const
+    {
+        return objects.colliders.empty() ? nColliders : uint32_t(objects.colliders.size());
+    }
+    ColliderEvent optIn(uint32_t c) const
+    {
+        if (!objects.colliders.empty()) return ColliderEvent{objects.colliders[c].callback, objects.colliders[c].eventThreshold};
+        return c < loadedOptIn.size() ? loadedOptIn[c] : ColliderEvent{0u, 3.40282347e38f};
+    }
+    void setOptIn(uint32_t c, uint32_t id, float threshold)
+    {
+        if (!objects.colliders.empty()) {
+            objects.colliders[c].callback = id;
+            objects.colliders[c].eventThreshold = threshold;
+        } else {
+            if (loadedOptIn.size() < nColliders) loadedOptIn.resize(nColliders, ColliderEvent{0u, 3.40282347e38f});
+            loadedOptIn[c] = ColliderEvent{id, threshold};
+        }
+        optInDirty = true;
+    }
+    // Uploads the colliders' opt-ins when they changed and sizes the ring (before a recording step).
+    void prepareEvents()
+    {
+        if (optInDirty) {
+            std::vector<ColliderEvent> v(nColliders);
+            uint32_t with = 0;
+            for (uint32_t c = 0; c < nColliders; c++) {
+                v[c] = optIn(c);
+                with += v[c].callback != 0u;
+            }
+            cevent.upload(v.data(), v.size(), stream);
+            optInColliders = with;
+            optInDirty = false;
+        }
+        if (eventCap == 0) {
+            eventCap = 1024;
+            eventRing.reserve(eventCap);
+        }
+    }
+    void phaseEvents()
+    {
+        if (optInColliders == 0 || manifoldCap == 0) return;
+        const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(gridFor(manifoldCap), 4 * dev.sms));
+        k_collision_events<<<grid, 256, 0, stream>>>(view(), cevent.p, manifolds.p, nManifolds.p, manifoldCap,
+                                                      eventRing.p, eventCap, dCounters.p);
+        CK(cudaGetLastError());
+        launches++;
+    }
+    // The step's events from the ring into lastEvents, in manifold order (side a first), with body handles.
+    void collectEvents(uint32_t count)
+    {
+        std::vector<EventRecord> r(count);
+        CK(cudaMemcpyAsync(r.data(), eventRing.p, sizeof(EventRecord) * count, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        std::sort(r.begin(), r.end(), [](const EventRecord& x, const EventRecord& y) {
+            return x.manifold != y.manifold ? x.manifold < y.manifold : x.side < y.side;
+        });
+        auto handleOf = [&](uint32_t b) -> uint64_t {
+            if (b >= objects.bodies.size()) return ~0ull;
+            const uint32_t slot = objects.bodies[b].handleSlot;
+            return (uint64_t(objects.slotGeneration[slot]) << 32) | slot;
+        };
+        lastEvents.resize(count);
+        for (uint32_t k = 0; k < count; k++) {
+            ag2d_collision_event& e = lastEvents[k];
+            e.self = r[k].self; e.other = r[k].other;
+            e.self_body = r[k].selfBody; e.other_body = r[k].otherBody;
+            e.self_body_handle = handleOf(r[k].selfBody);
+            e.other_body_handle = handleOf(r[k].otherBody);
+            e.point_x = r[k].px; e.point_y = r[k].py; e.normal_x = r[k].nx; e.normal_y = r[k].ny;
+            e.impulse = r[k].impulse;
+            e.callback_id = uint16_t(r[k].callback);
+            e.pad = 0;
+        }
+    }
+    // CollisionCallbackManager::invoke over the step's events (Simulation::dispatchCollisionEvents,
+    // Simulation.cpp:174-180): dead ids are skipped; the entry is read before the call, so a callback may create or
+    // destroy callbacks.
+    void dispatchEvents()
+    {
+        if (lastEvents.empty()) return;
+        dispatching = true;
+        struct Reset { bool& f; ~Reset() { f = false; } } reset{dispatching};
+        const std::vector<ag2d_collision_event> events = lastEvents;
+        for (const ag2d_collision_event& e : events) {
+            const uint16_t id = e.callback_id;
+            if (id == 0 || id >= callbacks.size() || !callbackAlive[id]) continue;
+            const CallbackEntry entry = callbacks[id];
+            entry.fn(&e, this, entry.user);
+        }
+    }
+
     void phaseSolve()
     {
         const cudaStream_t s = stream;
@@ -2309,6 +2426,10 @@ struct ag2d_world {
         } hostTimer{hostMs, tStart};
         ensureUploaded();
         flushCommands();
+        // BodyCollisionSolver::resetCollisionData and setCollisionEventRecording (Simulation.cpp:261-266).
+        lastEvents.clear();
+        recording = eventsEnabled && callbacksAlive > 0 && nWorlds <= 1;
+        if (recording) prepareEvents();
         for (int attempt = 0; attempt < 8; attempt++) {
             if (attempt > 0) retries++;
             if (listsDirty) rebuildLists();
@@ -2341,10 +2462,23 @@ struct ag2d_world {
             phaseNarrow();
             phaseWake();
             phaseRestore();
+            if (recording) phaseEvents();
             phaseSolve();
             phaseIslands();
             readCounters();
             const uint32_t st = hCounters->status;
+            if (st & STATUS_EVENT_OVERFLOW) {
+                // The ring was too small for this step's events: grow it and step again from the saved state.
+                snapshot(true);
+                if (nWorlds > 1) CK(cudaMemsetAsync(worldDirty.p, 0, sizeof(uint32_t) * nWorlds, s));
+                fullPose = fullPoseThisStep;
+                otherDirty = true;
+                eventCap = std::max<uint32_t>(2 * hCounters->events, 2 * eventCap);
+                eventRing.reserve(eventCap);
+                regrows++;
+                CK(cudaStreamSynchronize(s));
+                if (!(st & (STATUS_PAIR_OVERFLOW | STATUS_MANIFOLD_OVERFLOW))) continue;
+            }
             if (st & (STATUS_PAIR_OVERFLOW | STATUS_MANIFOLD_OVERFLOW)) {
                 snapshot(true);
                 if (nWorlds > 1) CK(cudaMemsetAsync(worldDirty.p, 0, sizeof(uint32_t) * nWorlds, s));
@@ -2411,6 +2545,7 @@ struct ag2d_world {
                                        : manifoldCap;
                 reserveCapacities(uint32_t(std::min<uint64_t>(p, 1ull << 30)), uint32_t(std::min<uint64_t>(m, 1ull << 30)));
             }
+            if (recording && hCounters->events) collectEvents(hCounters->events);
             stepsTaken++;
             return;
         }
@@ -2753,9 +2888,11 @@ int32_t ag2d_world_load_state(ag2d_world* world, const ag2d_state_desc* st)
             CK(cudaStreamSynchronize(w.stream));
             w.aabbValid = true;
         }
-        // The loaded state replaces any host-created objects.
+        // The loaded state replaces any host-created objects (and their colliders' event opt-ins).
         w.objects.bodies.clear();
         w.objects.colliders.clear();
+        w.loadedOptIn.assign(nc, ColliderEvent{0u, 3.40282347e38f});
+        w.optInDirty = true;
         w.hostDirty = false;
     });
 }
@@ -2766,7 +2903,95 @@ int32_t ag2d_world_step(ag2d_world* world, int32_t steps)
         if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
         if (steps < 0) throw ApiError(AG2D_ERR_INVALID_ARG, "steps must be >= 0");
         CK(cudaSetDevice(world->settings.device));
-        for (int32_t i = 0; i < steps; i++) world->stepOnce();
+        if (world->dispatching) throw ApiError(AG2D_ERR_INVALID_ARG, "a collision callback may not step the world");
+        for (int32_t i = 0; i < steps; i++) {
+            world->stepOnce();
+            world->dispatchEvents();
+        }
+    });
+}
+
+int32_t ag2d_world_create_collision_callback(ag2d_world* world, ag2d_collision_callback function, void* user_data,
+                                             uint16_t* out_id)
+{
+    return guarded([&] {
+        if (!world || !out_id) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        if (!function) throw ApiError(AG2D_ERR_INVALID_ARG, "null callback function");
+        if (world->nWorlds > 1) throw ApiError(AG2D_ERR_UNSUPPORTED, "collision events are per world");
+        ag2d_world& w = *world;
+        uint16_t id;
+        if (!w.callbackFree.empty()) {
+            id = w.callbackFree.back();
+            w.callbackFree.pop_back();
+        } else {
+            if (w.callbacks.size() >= 65535) throw ApiError(AG2D_ERR_CAPACITY, "all collision callback ids are in use");
+            id = uint16_t(w.callbacks.size());
+            w.callbacks.emplace_back();
+            w.callbackAlive.push_back(0);
+        }
+        w.callbacks[id] = ag2d_world::CallbackEntry{function, user_data};
+        w.callbackAlive[id] = 1;
+        w.callbacksAlive++;
+        *out_id = id;
+    });
+}
+
+int32_t ag2d_world_destroy_collision_callback(ag2d_world* world, uint16_t id)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        ag2d_world& w = *world;
+        if (id == 0 || id >= w.callbacks.size() || !w.callbackAlive[id])
+            throw ApiError(AG2D_ERR_INVALID_ARG, "collision callback " + std::to_string(id) + " is not alive");
+        w.callbacks[id] = ag2d_world::CallbackEntry{};
+        w.callbackAlive[id] = 0;
+        w.callbackFree.push_back(id);
+        w.callbacksAlive--;
+        // Colliders using it go back to no callback (Simulation.cpp:140-149).
+        const uint32_t n = w.colliderCount();
+        for (uint32_t c = 0; c < n; c++)
+            if (w.optIn(c).callback == id) w.setOptIn(c, 0u, 3.40282347e38f);
+    });
+}
+
+int32_t ag2d_world_set_collider_collision_callback(ag2d_world* world, uint32_t collider, uint16_t id,
+                                                   float impulse_threshold)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        ag2d_world& w = *world;
+        if (w.nWorlds > 1) throw ApiError(AG2D_ERR_UNSUPPORTED, "collision events are per world");
+        if (collider >= w.colliderCount())
+            throw ApiError(AG2D_ERR_INVALID_ARG, "collider " + std::to_string(collider) + " out of range");
+        if (id == 0) {
+            w.setOptIn(collider, 0u, 3.40282347e38f);
+            return;
+        }
+        if (id >= w.callbacks.size() || !w.callbackAlive[id])
+            throw ApiError(AG2D_ERR_INVALID_ARG, "collision callback " + std::to_string(id) + " is not alive");
+        if (!(impulse_threshold >= 0.0f)) throw ApiError(AG2D_ERR_INVALID_ARG, "threshold must be >= 0");
+        w.setOptIn(collider, id, impulse_threshold);
+    });
+}
+
+int32_t ag2d_world_set_collision_events(ag2d_world* world, int32_t enable)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        world->eventsEnabled = enable != 0;
+    });
+}
+
+int32_t ag2d_world_collision_events(ag2d_world* world, ag2d_collision_event* out_events, uint32_t capacity,
+                                    uint32_t* out_count)
+{
+    return guarded([&] {
+        if (!world || !out_count) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        const auto& ev = world->lastEvents;
+        *out_count = uint32_t(ev.size());
+        const uint32_t k = std::min<uint32_t>(capacity, uint32_t(ev.size()));
+        if (k && !out_events) throw ApiError(AG2D_ERR_INVALID_ARG, "null event buffer");
+        if (k) std::memcpy(out_events, ev.data(), k * sizeof(ag2d_collision_event));
     });
 }
 
@@ -2781,6 +3006,8 @@ int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out)
         out->sleeping = world->nBodies - world->nDynBody - world->nStatic - world->nDestroyed;
         out->ccd_hits = c.ccdHits;
         out->restored = c.restored;
+        out->events = uint32_t(world->lastEvents.size());
+        out->stored = c.stored;
         out->steps = world->stepsTaken;
         out->launches = world->launches;
         out->list_rebuilds = world->listRebuilds;
@@ -3328,6 +3555,20 @@ int32_t ag2d_world_run_phase(ag2d_world* world, int32_t phase)
             break;
         case AG2D_PHASE_SOLVE: w.phaseSolve(); break;
         case AG2D_PHASE_ISLANDS: w.phaseIslands(); break;
+        case AG2D_PHASE_EVENTS:
+            if (w.nWorlds > 1) throw ApiError(AG2D_ERR_UNSUPPORTED, "collision events are per world");
+            w.lastEvents.clear();
+            w.prepareEvents();
+            for (;;) {
+                CK(cudaMemsetAsync(w.dCounters.p, 0, sizeof(StepCounters), w.stream));
+                w.phaseEvents();
+                w.readCounters();
+                if (!(w.hCounters->status & STATUS_EVENT_OVERFLOW)) break;
+                w.eventCap = std::max<uint32_t>(2 * w.hCounters->events, 2 * w.eventCap);
+                w.eventRing.reserve(w.eventCap);
+            }
+            if (w.hCounters->events) w.collectEvents(w.hCounters->events);
+            break;
         default: throw ApiError(AG2D_ERR_INVALID_ARG, "unknown phase");
         }
         w.readCounters();

@@ -35,6 +35,11 @@ struct HCollider {
     uint32_t material = 0;
     uint32_t type = 0, shape = 0;
     float minExtent = 0, maxExtent = 0;
+    // Collision-event opt-in (ColliderSoA callbackId / eventThreshold, SoA/ColliderSoA.cpp:47-48): no callback and
+    // the never-firing threshold (NO_COLLISION_EVENT_THRESHOLD, Types/CollisionEvent.h:15) at creation. It moves
+    // with the collider when the dense order changes.
+    uint32_t callback = 0;
+    float eventThreshold = 3.40282347e38f;
 };
 
 struct HPolygon {

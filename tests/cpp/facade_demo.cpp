@@ -2,8 +2,9 @@
 // bodies through ObjectAPI, then Simulation::update) compiled against the C++ facade of libag2d.so.
 // Prints "no-device" and exits 0 when the machine has no CUDA device; otherwise steps the scene (a capsule is
 // created among the pile, and a body with three colliders; once it has settled one body is destroyed and another
-// kicked upwards through ObjectAPI's deferred commands) and prints "ok <bodies> <most manifolds in one step> <mean y> <colliders a circle query finds>
-// <circle contacts> <live bodies>" after querying the settled pile the way the reference's editor selects
+// kicked upwards through ObjectAPI's deferred commands) and prints "ok <bodies> <most manifolds in one step> <mean y>
+// <colliders a circle query finds> <circle contacts> <colliders in the trees> <impacts on the ground> <largest
+// impact impulse>" after querying the settled pile the way the reference's editor selects
 // (queryCollidersInShape with a CircleQuery, then findCollisionsInCircle over what it found).
 #include "ag2d_simulation.hpp"
 
@@ -30,6 +31,16 @@ int main()
     ground.base.materialIndex = mat;
     ground.size = {40.0f, 2.0f};
     if (!sim->objects().createBox(ground)) return 2;
+    // Impacts on the ground (its collider is the first): counted by a collision callback.
+    struct Impacts { int count = 0; ag2d::Real largest = 0; } impacts;
+    const auto onImpact = [](const ag2d::CollisionEvent& e, ag2d::Simulation&, void* user) {
+        auto* im = static_cast<Impacts*>(user);
+        im->count++;
+        im->largest = std::max(im->largest, e.impulse);
+    };
+    const std::optional<ag2d::CollisionCallbackIndex> impactId = sim->createCollisionCallback(onImpact, &impacts);
+    if (!impactId || !sim->setColliderCollisionCallback(0, *impactId, 0.5f)) return 14;
+    if (sim->setColliderCollisionCallback(0, *impactId, -1.0f)) return 15;   // negative threshold: false
     ag2d::Vec2 tri[3] = {{-0.5f, -0.4f}, {0.5f, -0.4f}, {0.0f, 0.6f}};
     int created = 1;
     for (int i = 0; i < 60; i++) {
@@ -118,7 +129,8 @@ int main()
         std::printf("colliders found %zu, bodies %u\n", all.size(), bodies.getCount());
         return 6;
     }
-    std::printf("ok %u %zu %.3f %zu %zu %zu\n", bodies.getCount(), maxManifolds, meanY / double(bodies.getCount()),
-                found.size(), touching.size(), all.size());
+    std::printf("ok %u %zu %.3f %zu %zu %zu %d %.3f\n", bodies.getCount(), maxManifolds,
+                meanY / double(bodies.getCount()), found.size(), touching.size(), all.size(), impacts.count,
+                double(impacts.largest));
     return bodies.getCount() == uint32_t(created) ? 0 : 4;
 }

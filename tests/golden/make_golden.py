@@ -17,6 +17,8 @@ Fixtures:
     traj_c1_n2048.npz       the same statistics of the full c1 configuration (2,048 polygons, seed 0, 600 steps)
     contacts_capsules_n1500_step300.npz  circle contacts and shape queries on a 1,500-body pile with capsules among
                             circles, boxes and polygons (findCollisionsInCircle's capsule branch)
+    events_c2_n1200.npz     collision events of four steps of a 1,200-body mixed-shape drop (two callbacks, colliders
+                            opted in at several thresholds), with the reference's state before each step
     towers_s0_step33.npz    40 three-box towers: the step in which 36 of them fall asleep (their manifolds go to
                             the sleeping-island store), with the store after the step
     towers_s0_step140.npz   the same scene: the step in which four towers wake and their stored manifolds return
@@ -265,6 +267,52 @@ def contacts_fixture(path, n=1500, steps=300, queries=60, capsules=False):
           f"{len(sshape)} shape queries, groups {keep['q.col.groupStarts'].tolist()}")
 
 
+EVENT_STEPS = (40, 80, 130, 200)
+EVENT_SLEEP_TIME = 1.0e6   # no body falls asleep: each step's state is the whole of what the next step reads
+NEVER = float(np.finfo(np.float32).max)
+
+
+def events_fixture(path, n=1200, steps=EVENT_STEPS):
+    """Collision events (Simulation::setColliderCollisionCallback, events recorded in computeConstraintData and
+    dispatched at the end of the step) on a mixed-shape drop: two recording callbacks, the colliders opted in by
+    dense index (id 1 at threshold 0, id 2 at 0.5, id 1 at 3, none, id 2 never firing), and for each step in
+    'steps' the reference's full state before it ("s<k>.", with each collider's callback id and threshold) and the
+    events it dispatched ("e<k>.ev.*", by handle slot)."""
+    scene = scenes.make_c2(n, 0, columns=30)
+    r = refapi.RefSim(scene, sleep_time=EVENT_SLEEP_TIME)
+    ids = [r.create_event_callback(), r.create_event_callback()]
+    r.dump_state("c.")
+    pattern = [(ids[0], 0.0), (ids[1], 0.5), (ids[0], 3.0), None, (ids[1], NEVER)]
+    for i in range(r.blob("c.col.bodyIndex").size):
+        p = pattern[i % len(pattern)]
+        if p is not None:
+            assert r.set_collider_callback(i, *p)
+    keep, done, counts, r_manifolds = {}, 0, [], []
+    for k in steps:
+        r.update(k - done)
+        done = k + 1
+        r.events()   # the events of the steps before
+        r.dump_state(f"s{k}.")
+        keep.update({key: v for key, v in r.blobs(f"s{k}.").items()
+                     if not key.startswith(f"s{k}.man.") and not key.startswith(f"s{k}.isle.")
+                     and not key.endswith(DROP_SUFFIXES)})
+        assert keep[f"s{k}.body.groupStarts"][1] == keep[f"s{k}.body.groupStarts"][2], "no body may sleep yet"
+        r.update(1)
+        r_manifolds.append(r.manifold_count)
+        ev = r.events(f"e{k}.")
+        keep.update({f"e{k}.ev.{name}": v for name, v in ev.items()})
+        counts.append(ev["self"].size)
+    keep["meta.steps"] = np.asarray(steps, np.uint32)
+    keep["meta.sleep_time"] = np.array([EVENT_SLEEP_TIME], np.float32)
+    keep["meta.dt"] = np.array([scene.dt], np.float32)
+    keep["meta.gravity"] = np.array(scene.gravity, np.float32)
+    keep["meta.iters"] = np.array([scene.velocity_iterations, scene.position_iterations], np.uint32)
+    keep["meta.materials"] = np.array([(1.0, 0.0, 0.0)] + list(scene.materials), np.float32)
+    np.savez_compressed(path, **dedupe(keep))
+    r.close()
+    print(f"{os.path.basename(path)}: events per step {dict(zip(steps, counts))}, manifolds {r_manifolds}")
+
+
 FIXTURES = {
     "c1_n256_s0_step300.npz": lambda p: phase_fixture(scenes.make_c1(256, 0), 300, p),
     "c2_n2000_s1_step240.npz": lambda p: phase_fixture(scenes.make_c2(2000, 1, columns=50), 240, p),
@@ -289,6 +337,7 @@ FIXTURES = {
     "query_c1_n600_step700.npz": query_fixture,
     "contacts_c2_n1500_step300.npz": contacts_fixture,
     "contacts_capsules_n1500_step300.npz": lambda p: contacts_fixture(p, capsules=True),
+    "events_c2_n1200.npz": events_fixture,
 }
 
 

@@ -43,3 +43,5 @@ def test_facade_steps_scene_on_gpu(tmp_path):
     assert -1.0 < mean_y < 6.0   # the pile has fallen onto the ground (spawned between y = 1 and 8.5)
     found, touching = int(fields[4]), int(fields[5])   # the editor-style circle query around the pile's base
     assert 0 < touching <= found
+    impacts, largest = int(fields[7]), float(fields[8])   # collision callback on the ground's collider, threshold 0.5
+    assert impacts > 0 and largest >= 0.5
