@@ -199,6 +199,14 @@ class ClockSampler:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        # nvidia-smi's start-up (driver and NVML initialisation over every GPU of the node) can hold the driver
+        # for a few hundred milliseconds: wait for its first sample so that it is done before the timed region.
+        deadline = time.perf_counter() + 10.0
+        while time.perf_counter() < deadline and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc:
@@ -318,9 +326,11 @@ def step_bytes(msb, pairs_sum, manifolds_sum, dyn_bodies, steps, vi=8, pi=3):
 def diagnostics(c0, c1, per_step, colors_sum, K):
     return {"mean_colors": colors_sum / K, "list_rebuilds": c1["list_rebuilds"] - c0["list_rebuilds"],
             "retries": c1["retries"] - c0["retries"], "regrows": c1["regrows"] - c0["regrows"],
+            "device_allocs": c1["device_allocs"] - c0["device_allocs"],
             "host_ms_per_step": (c1["host_ms"] - c0["host_ms"]) / K,
             "sync_wait_ms_per_step": (c1["sync_ms"] - c0["sync_ms"]) / K,
-            "max_step_ms": max(per_step), "median_step_ms": statistics.median(per_step)}
+            "max_step_ms": max(per_step), "max_step_index": per_step.index(max(per_step)),
+            "median_step_ms": statistics.median(per_step)}
 
 
 def reduce_max(torch, dist, world_size, dev, value):
@@ -670,14 +680,17 @@ def run_c4(args, torch, dist, rank, world_size, local, dev):
     kernel_of = {"solve": "k_color_solve_teams", "narrow": "k_narrow", "integrate": "k_integrate",
                  "pose": "k_collider_pose", "sort": "k_sort_pass", "query": "k_query_stash + k_query_emit"}
     roof = roofline_line(phases, bytes_by_phase, kernel_of, "c4", solve_passes(sums["manifolds"]))
+    pose_bytes = e.field_bytes(ag2d.BODY_POSE)
     del batch, e
 
     # End to end through the C ABI, over the same window: the batch restored from the host checkpoint of the
     # window's start (page-locked; uploaded inside the timed region), then per step one ag2d_batch_step and a read
     # of every body's pose (x, y, rotation) into page-locked host memory. The read of step k is queued after it
     # and lands while step k + 1 runs; the loop waits for it before queuing the next (a consumer one frame behind).
+    # The consumer's two page-locked pose buffers exist before the timed region (a viewer allocates them once).
     e2e_steps = K
-    pose_ring = None
+    pose_ring = [ag2d.host_empty(pose_bytes), ag2d.host_empty(pose_bytes)]
+    allocs0 = ag2d.device_allocs()
     if world_size > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -685,8 +698,7 @@ def run_c4(args, torch, dist, rank, world_size, local, dev):
     b2 = ag2d.Batch.restore(ckpt)
     if tuning:
         b2.engine.set_tuning(tuning)
-    pose_bytes = b2.engine.field_bytes(ag2d.BODY_POSE)
-    pose_ring = [ag2d.host_empty(pose_bytes), ag2d.host_empty(pose_bytes)]
+    allocs_restore = ag2d.device_allocs() - allocs0
     for k in range(e2e_steps):
         b2.step(1)
         b2.engine.read_wait()
@@ -699,7 +711,9 @@ def run_c4(args, torch, dist, rank, world_size, local, dev):
            "steps": e2e_steps, "window": window_name(args),
            "timed": "ag2d_batch_restore from a page-locked host checkpoint of the window's start (in the timed "
                     "region), then per step ag2d_batch_step + ag2d_world_read_async of every body pose into "
-                    "page-locked memory, waited for one step later; wall clock"}
+                    "page-locked memory, waited for one step later; wall clock",
+           "device_allocs": {"restore": allocs_restore,
+                             "steps": ag2d.device_allocs() - allocs0 - allocs_restore}}
     del b2, pose_ring
 
     # The same worlds, one launch sequence per world per step (a Simulation per world): every k-th world.

@@ -75,6 +75,8 @@ typedef struct ag2d_counters {
     uint64_t regrows;       /* capacity growths */
     double host_ms;         /* host wall time spent inside ag2d_world_step so far */
     double sync_ms;         /* of which waiting for the device at the end of steps */
+    uint64_t device_allocs; /* device buffer allocations made by the library in this process so far (each one
+                               synchronises the device; a steady run of steps makes none) */
 } ag2d_counters;
 
 /* Phases timed by ag2d_world_phase_times (index into the returned array). */
@@ -296,6 +298,8 @@ int32_t ag2d_world_load_state(ag2d_world* world, const ag2d_state_desc* state);
 int32_t ag2d_world_step(ag2d_world* world, int32_t steps);
 
 int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out);
+/* Device buffer allocations the library has made in this process so far (ag2d_counters.device_allocs). */
+int32_t ag2d_device_allocs(uint64_t* out);
 
 /* Launch-shape autotuner (no reference counterpart: the reference runs on CPU threads). Times real steps under each
  * candidate solver team size (batches), pair-query and narrow-phase block size and keeps the fastest. A step's

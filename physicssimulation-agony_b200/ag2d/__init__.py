@@ -76,7 +76,8 @@ class Counters(ctypes.Structure):
                 ("restored", ctypes.c_uint32), ("events", ctypes.c_uint32), ("stored", ctypes.c_uint32),
                 ("steps", ctypes.c_uint64),
                 ("launches", ctypes.c_uint64), ("list_rebuilds", ctypes.c_uint64), ("retries", ctypes.c_uint64),
-                ("regrows", ctypes.c_uint64), ("host_ms", ctypes.c_double), ("sync_ms", ctypes.c_double)]
+                ("regrows", ctypes.c_uint64), ("host_ms", ctypes.c_double), ("sync_ms", ctypes.c_double),
+                ("device_allocs", ctypes.c_uint64)]
 
 
 class CollisionEvent(ctypes.Structure):
@@ -181,6 +182,7 @@ def _load():
     L.ag2d_world_load_state.argtypes = [vp, ctypes.POINTER(StateDesc)]
     L.ag2d_world_step.argtypes = [vp, i32]
     L.ag2d_world_counters.argtypes = [vp, ctypes.POINTER(Counters)]
+    L.ag2d_device_allocs.argtypes = [ctypes.POINTER(u64)]
     L.ag2d_world_body_count.argtypes = [vp, ctypes.POINTER(u32), ctypes.POINTER(u32)]
     L.ag2d_world_read.argtypes = [vp, i32, vp, u64, ctypes.POINTER(u64)]
     L.ag2d_world_write.argtypes = [vp, i32, vp, u64]
@@ -228,6 +230,13 @@ class _Lib:
 
 
 lib = _Lib()
+
+
+def device_allocs() -> int:
+    """Device buffer allocations the library has made in this process (ag2d_counters.device_allocs)."""
+    n = ctypes.c_uint64()
+    _check(lib.ag2d_device_allocs(ctypes.byref(n)))
+    return int(n.value)
 
 
 def _check(code: int):

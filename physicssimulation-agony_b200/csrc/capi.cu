@@ -5,6 +5,7 @@
 #include "host_objects.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -66,6 +67,10 @@ int32_t guarded(F&& f)
     }
 }
 
+// Device buffer (re)allocations in this process: a reallocation synchronises the device and fresh memory is slow
+// to map, so a steady step should make none (reported by ag2d_world_counters).
+static std::atomic<uint64_t> g_deviceAllocs{0};
+
 template <class T>
 struct DBuf {
     T* p = nullptr;
@@ -89,6 +94,7 @@ struct DBuf {
         const size_t c = std::max<size_t>(p ? std::max(count, n + n / 2) : count, 1);
         release();
         CK(cudaMalloc(reinterpret_cast<void**>(&p), c * sizeof(T)));
+        g_deviceAllocs.fetch_add(1, std::memory_order_relaxed);
         n = c;
     }
     void upload(const T* src, size_t count, cudaStream_t s)
@@ -1175,6 +1181,14 @@ struct ag2d_world {
         prevCount = h.nPrev;
         prevSegValid = false;
         CK(cudaMemcpyAsync(nPrev.p, &prevCount, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        {
+            // The store at the capacity the sleep pass would grow it to (half again on its size, at least the
+            // manifold capacity), both buffers and the scratch, so the restored engine's steps allocate nothing.
+            const size_t cap = std::max<size_t>({size_t(h.nIsle) + h.nIsle / 2, size_t(manifoldCap), size_t(1024)});
+            for (auto* b : {&isle, &bk_isle}) b->reserve(cap);
+            for (auto* b : {&isleId, &bk_isleId}) b->reserve(cap);
+            reserveIsleScratch(uint32_t(std::min<size_t>(cap, 0xFFFFFFFFu)));
+        }
         up(isle, CK_ISLE, h.nIsle);
         up(isleId, CK_ISLEID, h.nIsle);
         isleUpper = h.nIsle;
@@ -1839,9 +1853,11 @@ struct ag2d_world {
         // Both store buffers keep one capacity (they trade places), grown together by half again when short, so a
         // steady store reallocates neither.
         if (isle.n < need || bk_isle.n < need || isleId.n < need || bk_isleId.n < need || !isle.p || !bk_isle.p) {
-            // Half again on top of the need, at least doubling: a store that fills as a batch settles reallocates
-            // (a device synchronisation) a few times only.
-            const size_t cap = std::max<size_t>({size_t(need) + need / 2, size_t(1024), 2 * isle.n});
+            // Half again on top of the need, at least doubling, and at least the manifold capacity (the store
+            // rarely outgrows the contacts a step can hold): a store that fills as a batch settles reallocates (a
+            // device synchronisation, slow to map) once or twice only, not inside a steady run of steps.
+            const size_t cap = std::max<size_t>({size_t(need) + need / 2, size_t(1024), 2 * isle.n,
+                                                 size_t(manifoldCap)});
             growKeep(isle, cap);
             growKeep(isleId, cap);
             DBuf<Manifold> nb;
@@ -1850,6 +1866,7 @@ struct ag2d_world {
             DBuf<uint32_t> nbi;
             nbi.reserve(cap);
             swap_bufs(bk_isleId, nbi);
+            reserveIsleScratch(uint32_t(std::min<size_t>(cap, 0xFFFFFFFFu)));   // the scratch follows the store
         }
         reserveIsleScratch(stored);
         for (auto* b : {&sleepStay, &sleepMove, &sleepMoveOff, &sleepMoveIsland, &sleepMoveWorld}) b->reserve(manifoldCap);
@@ -2911,6 +2928,14 @@ int32_t ag2d_world_step(ag2d_world* world, int32_t steps)
     });
 }
 
+int32_t ag2d_device_allocs(uint64_t* out)
+{
+    return guarded([&] {
+        if (!out) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        *out = g_deviceAllocs.load(std::memory_order_relaxed);
+    });
+}
+
 int32_t ag2d_world_create_collision_callback(ag2d_world* world, ag2d_collision_callback function, void* user_data,
                                              uint16_t* out_id)
 {
@@ -3006,6 +3031,7 @@ int32_t ag2d_world_counters(ag2d_world* world, ag2d_counters* out)
         out->sleeping = world->nBodies - world->nDynBody - world->nStatic - world->nDestroyed;
         out->ccd_hits = c.ccdHits;
         out->restored = c.restored;
+        out->device_allocs = g_deviceAllocs.load(std::memory_order_relaxed);
         out->events = uint32_t(world->lastEvents.size());
         out->stored = c.stored;
         out->steps = world->stepsTaken;
