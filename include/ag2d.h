@@ -250,6 +250,46 @@ int32_t ag2d_world_set_body_inertia(ag2d_world* world, uint64_t body, float iner
 /* Applies the queued commands now (Simulation::flushCommands, Simulation.cpp:453-456). */
 int32_t ag2d_world_flush_commands(ag2d_world* world);
 
+/* ---- body constraints: ConstraintAPI (SimulationAPIs/ConstraintAPI.h:32-83) for springs, revolute joints and
+ * motors ----
+ * Springs and revolute joints join two bodies at body-local anchors (a soft distance constraint with a rest
+ * length; a soft pin of both anchors together); a motor drives one body's angular velocity toward a target speed
+ * within a torque limit. They are solved between the two halves of the step's integration, each kind in the
+ * reference's dense order (Solving/SpringSolver.cpp, RevoluteJointSolver.cpp, MotorSolver.cpp scheduled by
+ * ConstraintScheduler.cpp:9-80): the same results as the reference's single-threaded solve. Creation wakes the
+ * bodies and returns a handle (AG2D_ERR_INVALID_ARG for a stale body handle: the reference's nullopt); destruction
+ * and the setters are deferred to the next step's command flush, like the body commands, and wake the bodies; a
+ * destroyed body takes its constraints with it. Per world: a batch engine's worlds take no constraints
+ * (AG2D_ERR_UNSUPPORTED). */
+enum ag2d_joint_kind { AG2D_JOINT_SPRING = 0, AG2D_JOINT_REVOLUTE = 1, AG2D_JOINT_MOTOR = 2 };
+typedef struct ag2d_joint_desc {
+    int32_t kind;                    /* ag2d_joint_kind */
+    uint32_t pad;
+    uint64_t body_a, body_b;         /* body handles (a motor uses body_a) */
+    float anchor_a_x, anchor_a_y;    /* body-local anchors (springs and revolute joints) */
+    float anchor_b_x, anchor_b_y;
+    float rest_length;               /* spring */
+    float stiffness, damping;        /* springs and revolute joints */
+    float target_speed, max_torque;  /* motor */
+    float impulse;                   /* motor: accumulated impulse of the last step (read only) */
+} ag2d_joint_desc;
+/* Setter fields (ConstraintAPI::set*, ConstraintAPI.h:71-83): anchors take (a, b) as x, y; lengths, stiffness,
+ * damping and max torque are clamped at 0 when applied. */
+enum ag2d_joint_field {
+    AG2D_JOINT_ANCHOR_A = 0, AG2D_JOINT_ANCHOR_B, AG2D_JOINT_REST_LENGTH, AG2D_JOINT_STIFFNESS, AG2D_JOINT_DAMPING,
+    AG2D_JOINT_TARGET_SPEED, AG2D_JOINT_MAX_TORQUE
+};
+int32_t ag2d_world_create_joint(ag2d_world* world, const ag2d_joint_desc* desc, uint64_t* out_handle);
+int32_t ag2d_world_destroy_joint(ag2d_world* world, int32_t kind, uint64_t handle);
+int32_t ag2d_world_set_joint(ag2d_world* world, int32_t kind, uint64_t handle, int32_t field, float a, float b);
+/* ConstraintAPI::get*DataH (ConstraintAPI.h:86-105): the constraint as stored now. AG2D_ERR_INVALID_ARG if stale. */
+int32_t ag2d_world_joint(ag2d_world* world, int32_t kind, uint64_t handle, ag2d_joint_desc* out);
+/* Constraints of a kind, and the handle of dense index i (ConstraintAPI::get*Handle, ConstraintAPI.h:46-50). */
+int32_t ag2d_world_joint_count(ag2d_world* world, int32_t kind, uint32_t* out_count);
+int32_t ag2d_world_joint_handle(ag2d_world* world, int32_t kind, uint32_t index, uint64_t* out_handle);
+/* IConstraintSystem::iterations of a kind (default 6; ConstraintSystemBase.h:34). */
+int32_t ag2d_world_set_joint_iterations(ag2d_world* world, int32_t kind, uint32_t iterations);
+
 /* ---- collision events: Simulation::createCollisionCallback / destroyCollisionCallback /
  * setColliderCollisionCallback (Simulation.h:169-179, Simulation.cpp:130-171; the table of
  * SimulationImpl/CollisionCallbackManager.h) ----

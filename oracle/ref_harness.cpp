@@ -504,6 +504,40 @@ extern "C"
         h->events.clear();
     }
 
+    // Constraints (ConstraintAPI::createSpring / createRevoluteJoint / createMotor, SimulationAPIs/ConstraintAPI.h:
+    // 32-36) between bodies given by handle slot; returns the constraint's handle slot or -1 (stale body).
+    // kind 0 spring (p: anchorA xy, anchorB xy, rest length, stiffness, damping), 1 revolute joint (anchors,
+    // stiffness, damping), 4 motor (body A only; p: target speed, max torque).
+    int64_t agref_create_joint(void* hp, int32_t kind, uint32_t slotA, uint32_t slotB, const float* p)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        auto& o = h->sim.objectManager;
+        const Handle a = bodyHandleOfSlot(h, slotA), b = bodyHandleOfSlot(h, slotB);
+        std::optional<Handle> r;
+        switch (kind)
+        {
+        case 0: r = o.createSpring({a, b, Vec2(p[0], p[1]), Vec2(p[2], p[3]), p[4], p[5], p[6]}); break;
+        case 1: r = o.createRevoluteJoint({a, b, Vec2(p[0], p[1]), Vec2(p[2], p[3]), p[4], p[5]}); break;
+        case 4: r = o.createMotor({a, p[0], p[1]}); break;
+        default: break;
+        }
+        return r ? int64_t(r->slot) : -1;
+    }
+    // The motors' accumulated impulses and body handle slots in dense order (MotorSoA).
+    uint32_t agref_motor_impulses(void* hp, float* impulse, uint32_t* bodySlot, uint32_t cap)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        auto& sys = h->sim.motorConstraintSystem;
+        const auto view = sys.getViewer();
+        const uint32_t n = uint32_t(sys.getCount());
+        for (uint32_t i = 0; i < n && i < cap; i++)
+        {
+            impulse[i] = view.accumulatedImpulse[i];
+            bodySlot[i] = h->sim.objectManager.bodies.handleAt(view.bodyIndex[i]).slot;
+        }
+        return n;
+    }
+
     // Dense body index of a handle slot (UINT32_MAX when destroyed).
     uint32_t agref_body_index(void* hp, uint32_t slot)
     {

@@ -86,6 +86,10 @@ def lib():
         L.agref_circle_contacts.argtypes = [vp, f, f, f, u32, vp, vp, ctypes.c_uint64]
         L.agref_circle_contacts.restype = ctypes.c_int64
         L.agref_fastcossin.argtypes = [vp, vp, vp, ctypes.c_uint64]
+        L.agref_create_joint.restype = i64
+        L.agref_create_joint.argtypes = [vp, i32, u32, u32, vp]
+        L.agref_motor_impulses.restype = u32
+        L.agref_motor_impulses.argtypes = [vp, vp, vp, u32]
         L.agref_create_event_callback.restype = i32
         L.agref_create_event_callback.argtypes = [vp]
         L.agref_destroy_event_callback.restype = i32
@@ -255,6 +259,18 @@ class RefSim:
         sdf = np.empty(max(int(n), 1), np.float32)
         L.agref_circle_contacts(self.h, x, y, r, trees, idx.ctypes.data, sdf.ctypes.data, idx.size)
         return idx[:int(n)], sdf[:int(n)]
+
+    def create_joint(self, kind: int, a: int, b: int, params) -> int:
+        """A spring (0), revolute joint (1) or motor (4, body a) between bodies given by handle slot."""
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        return int(lib().agref_create_joint(self.h, kind, a, b, p.ctypes.data))
+
+    def motor_impulses(self):
+        """(accumulated impulses, body handle slots) of the motors in dense order."""
+        imp = np.zeros(4096, np.float32)
+        slot = np.zeros(4096, np.uint32)
+        n = int(lib().agref_motor_impulses(self.h, imp.ctypes.data, slot.ctypes.data, imp.size))
+        return imp[:n].copy(), slot[:n].copy()
 
     def create_event_callback(self) -> int:
         """A collision callback that records every event it receives (Simulation::createCollisionCallback)."""

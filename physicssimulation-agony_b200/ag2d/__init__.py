@@ -96,6 +96,20 @@ COLLISION_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.POINTER(CollisionEvent), ctyp
 NO_COLLISION_EVENT_THRESHOLD = float(np.finfo(np.float32).max)
 
 
+# enum ag2d_joint_kind / ag2d_joint_field
+JOINT_SPRING, JOINT_REVOLUTE, JOINT_MOTOR = range(3)
+JOINT_ANCHOR_A, JOINT_ANCHOR_B, JOINT_REST_LENGTH, JOINT_STIFFNESS, JOINT_DAMPING, JOINT_TARGET_SPEED, \
+    JOINT_MAX_TORQUE = range(7)
+
+
+class JointDesc(ctypes.Structure):
+    """ag2d_joint_desc: a spring, revolute joint or motor."""
+    _fields_ = [("kind", ctypes.c_int32), ("pad", ctypes.c_uint32), ("body_a", ctypes.c_uint64),
+                ("body_b", ctypes.c_uint64)] + \
+               [(n, ctypes.c_float) for n in ("anchor_a_x", "anchor_a_y", "anchor_b_x", "anchor_b_y", "rest_length",
+                                              "stiffness", "damping", "target_speed", "max_torque", "impulse")]
+
+
 class Tuning(ctypes.Structure):
     _fields_ = [("team_colliders", ctypes.c_uint32), ("team_threads", ctypes.c_uint32), ("query_threads", ctypes.c_uint32),
                 ("narrow_threads", ctypes.c_uint32), ("solve_ms", ctypes.c_float), ("query_ms", ctypes.c_float),
@@ -174,6 +188,13 @@ def _load():
     for name in ("rotation", "angular_velocity", "mass", "inertia"):
         getattr(L, f"ag2d_world_set_body_{name}").argtypes = [vp, u64, ctypes.c_float]
     L.ag2d_world_flush_commands.argtypes = [vp]
+    L.ag2d_world_create_joint.argtypes = [vp, ctypes.POINTER(JointDesc), ctypes.POINTER(u64)]
+    L.ag2d_world_destroy_joint.argtypes = [vp, i32, u64]
+    L.ag2d_world_set_joint.argtypes = [vp, i32, u64, i32, ctypes.c_float, ctypes.c_float]
+    L.ag2d_world_joint.argtypes = [vp, i32, u64, ctypes.POINTER(JointDesc)]
+    L.ag2d_world_joint_count.argtypes = [vp, i32, ctypes.POINTER(u32)]
+    L.ag2d_world_joint_handle.argtypes = [vp, i32, u32, ctypes.POINTER(u64)]
+    L.ag2d_world_set_joint_iterations.argtypes = [vp, i32, u32]
     L.ag2d_world_create_collision_callback.argtypes = [vp, COLLISION_CALLBACK, vp, ctypes.POINTER(ctypes.c_uint16)]
     L.ag2d_world_destroy_collision_callback.argtypes = [vp, ctypes.c_uint16]
     L.ag2d_world_set_collider_collision_callback.argtypes = [vp, u32, ctypes.c_uint16, ctypes.c_float]
@@ -417,6 +438,48 @@ class World:
 
     def flush_commands(self):
         _check(lib.ag2d_world_flush_commands(self.h))
+
+    # --- body constraints (ConstraintAPI, SimulationAPIs/ConstraintAPI.h:32-105) ---
+    def create_joint(self, kind, body_a, body_b=0, anchor_a=(0.0, 0.0), anchor_b=(0.0, 0.0), rest_length=0.0,
+                     stiffness=0.0, damping=0.0, target_speed=0.0, max_torque=0.0) -> int:
+        d = JointDesc(kind, 0, body_a, body_b, anchor_a[0], anchor_a[1], anchor_b[0], anchor_b[1], rest_length,
+                      stiffness, damping, target_speed, max_torque, 0.0)
+        out = ctypes.c_uint64()
+        _check(lib.ag2d_world_create_joint(self.h, ctypes.byref(d), ctypes.byref(out)))
+        return int(out.value)
+
+    def create_spring(self, body_a, body_b, anchor_a, anchor_b, rest_length, stiffness, damping) -> int:
+        return self.create_joint(JOINT_SPRING, body_a, body_b, anchor_a, anchor_b, rest_length, stiffness, damping)
+
+    def create_revolute_joint(self, body_a, body_b, anchor_a, anchor_b, stiffness, damping) -> int:
+        return self.create_joint(JOINT_REVOLUTE, body_a, body_b, anchor_a, anchor_b, 0.0, stiffness, damping)
+
+    def create_motor(self, body, target_speed, max_torque) -> int:
+        return self.create_joint(JOINT_MOTOR, body, 0, target_speed=target_speed, max_torque=max_torque)
+
+    def destroy_joint(self, kind, handle):
+        _check(lib.ag2d_world_destroy_joint(self.h, kind, handle))
+
+    def set_joint(self, kind, handle, field, a, b=0.0):
+        _check(lib.ag2d_world_set_joint(self.h, kind, handle, field, a, b))
+
+    def joint(self, kind, handle) -> dict:
+        d = JointDesc()
+        _check(lib.ag2d_world_joint(self.h, kind, handle, ctypes.byref(d)))
+        return {n: getattr(d, n) for n, _ in JointDesc._fields_ if n != "pad"}
+
+    def joint_count(self, kind) -> int:
+        n = ctypes.c_uint32()
+        _check(lib.ag2d_world_joint_count(self.h, kind, ctypes.byref(n)))
+        return int(n.value)
+
+    def joint_handle(self, kind, index) -> int:
+        out = ctypes.c_uint64()
+        _check(lib.ag2d_world_joint_handle(self.h, kind, index, ctypes.byref(out)))
+        return int(out.value)
+
+    def set_joint_iterations(self, kind, iterations):
+        _check(lib.ag2d_world_set_joint_iterations(self.h, kind, iterations))
 
     # --- collision events (Simulation::createCollisionCallback / destroyCollisionCallback /
     # setColliderCollisionCallback, Simulation.h:169-179) ---

@@ -43,7 +43,7 @@ struct TreeView {
 
 // Spatial kernels (k_spatial.cu).
 __global__ void k_integrate(DeviceWorld w, const uint32_t* dynBody, const uint8_t* dynSimd, uint32_t nDyn, float dt,
-                            float gx, float gy, float dampHalf);
+                            float gx, float gy, float dampHalf, uint32_t phase);
 __global__ void k_collider_pose(DeviceWorld w, const uint32_t* list, const uint8_t* listSimd, uint32_t n,
                                 const uint32_t* worldMask);
 __global__ void k_bounds_init(uint32_t* bounds, uint32_t worlds);
@@ -207,6 +207,26 @@ __global__ void k_circle_contacts(DeviceWorld w, float x, float y, float radius,
                                   float* dist);
 __global__ void k_scatter_contacts(const uint32_t* flag, const uint32_t* offset, const float* dist, uint32_t n,
                                    uint32_t* list, float* listDist);
+
+// Body constraints (k_joints.cu): springs (kind 0), revolute joints (1) and motors (2), each kind's active
+// constraints in rec[k] grouped by level (level l: [levelStart[k][l], levelStart[k][l + 1])), solver data in
+// data[k], the motors' accumulated impulses by dense index in motorImpulse. One CTA of JOINT_THREADS threads.
+constexpr uint32_t JOINT_KINDS_DEVICE = 3;
+constexpr uint32_t JOINT_THREADS = 1024;
+struct JointLaunch {
+    const JointRec* rec[JOINT_KINDS_DEVICE];
+    JointData* data[JOINT_KINDS_DEVICE];
+    const uint32_t* levelStart[JOINT_KINDS_DEVICE];
+    uint32_t count[JOINT_KINDS_DEVICE];
+    uint32_t levels[JOINT_KINDS_DEVICE];
+    uint32_t iterations[JOINT_KINDS_DEVICE];
+    uint32_t maxIterations;
+    float dt;
+    float* motorImpulse;
+};
+__global__ void k_joints(DeviceWorld w, JointLaunch L);
+// Island links of the active constraints' body pairs (edges[i] = {a, b}), as k_island_union links manifolds.
+__global__ void k_island_union_edges(DeviceWorld w, const uint2* edges, uint32_t n, uint32_t* parent);
 
 // Collision events (k_events.cu): the events of the manifolds in man[0, min(*nMan, manCap)) whose colliders opted
 // in (cev), appended to ring (counters->events counts them all; STATUS_EVENT_OVERFLOW when more than ringCap).

@@ -78,6 +78,26 @@ struct ColliderEvent {
     float threshold;
 };
 
+// Body constraint on the device (springs, revolute joints, motors; SoA/Constraints/*), one per active constraint
+// in solving order: bodies, the constraint's dense index in its system, local anchors and parameters (spring: rest
+// length, stiffness, damping; revolute joint: stiffness, damping; motor: target speed, max torque).
+struct alignas(16) JointRec {
+    uint32_t bodyA, bodyB, index, pad;
+    float ax, ay, bx, by;
+    float p0, p1, p2, p3;
+};
+static_assert(sizeof(JointRec) == 48, "JointRec is 48 bytes");
+
+// Per-constraint solver data (the solvers' ConstraintData, Solving/*Solver.h). Spring: rotated anchors, direction,
+// inverse effective mass (0: skip), bias. Revolute joint: rotated anchors, bias, inverse effective mass matrix
+// (k11, k12, k22; all 0: skip). Motor: inverse inertia (0: skip), inertia, target speed, max impulse, impulse.
+struct alignas(16) JointData {
+    float rAx, rAy, rBx, rBy;
+    float s0, s1, s2, s3;
+    float s4, s5, s6, s7;
+};
+static_assert(sizeof(JointData) == 48, "JointData is 48 bytes");
+
 // Per-constraint solver record (128 bytes), built from a Manifold in solving (colour) order: the fields of
 // BodyCollisionSolver's VelocityHotData, PositionHotData, VelocityConstraintData and FrictionData.
 struct alignas(16) Constraint {

@@ -474,6 +474,20 @@ struct ag2d_world {
     uint32_t eventCap = 0;
     std::vector<ag2d_collision_event> lastEvents;   // the last step's events, in dispatch order
 
+    // Body constraints: device lists rebuilt from the host tables (objects.jointSystems) when these change or
+    // bodies change state; deferred destroys and setters (ConstraintSystemBase::flushImpl) applied with the body
+    // commands.
+    struct JointCommand {
+        int32_t kind, field;   // field < 0: destroy
+        uint64_t handle;
+        float a, b;
+    };
+    std::vector<JointCommand> jointCommands;
+    uint32_t jointActive[JOINT_KINDS] = {0, 0, 0}, jointLevels[JOINT_KINDS] = {0, 0, 0};
+    std::vector<uint32_t> jointLevelHost[JOINT_KINDS];
+    uint32_t nJointEdges = 0, motorsOnDevice = 0;
+    bool jointsDirty = false;   // the device lists need a rebuild before the next step
+
     uint32_t nBodies = 0, nColliders = 0, nDynBody = 0, nDynCol = 0, nOther = 0, nStatic = 0;
     uint32_t nDestroyed = 0;   // bodies removed by destroy commands (still in the arrays, in no list)
     uint32_t pairCap = 0, manifoldCap = 0, hashCap = 0;
@@ -487,6 +501,13 @@ struct ag2d_world {
     DBuf<float> wrapCount, boundRadius, sleepTimer;
     DBuf<uint8_t> bstate;
     DBuf<uint32_t> sleepIsland;
+    // Body constraints on the device: each kind's active constraints in level order, their solver data and level
+    // starts, the motors' accumulated impulses by dense index, the active pairs' bodies for the islands.
+    DBuf<JointRec> jointRec[JOINT_KINDS];
+    DBuf<JointData> jointData[JOINT_KINDS];
+    DBuf<uint32_t> jointLevel[JOINT_KINDS];
+    DBuf<float> motorImpulse, snapMotorImpulse;
+    DBuf<uint2> jointEdges;
     // Collision events: per-collider opt-in and the step's event ring.
     DBuf<ColliderEvent> cevent;
     DBuf<EventRecord> eventRing;
@@ -1445,6 +1466,8 @@ struct ag2d_world {
         isleUpper = 0;
         prevSegValid = false;
         optInDirty = true;
+        motorsOnDevice = 0;
+        jointsDirty = jointTotal() > 0;
         CK(cudaStreamSynchronize(s));
         hostDirty = false;
         listsDirty = true;
@@ -1554,7 +1577,9 @@ struct ag2d_world {
             cp(snapRot.p, brot.p, n * sizeof(float2)); cp(snapWrap.p, wrapCount.p, n * sizeof(float));
             cp(snapTimer.p, sleepTimer.p, n * sizeof(float)); cp(snapState.p, bstate.p, n);
             cp(snapIsland.p, sleepIsland.p, n * sizeof(uint32_t));
+            cp(snapMotorImpulse.p, motorImpulse.p, motorsOnDevice * sizeof(float));
         } else {
+            cp(motorImpulse.p, snapMotorImpulse.p, motorsOnDevice * sizeof(float));
             cp(bvel.p, snapVel.p, n * sizeof(float4)); cp(bpos.p, snapPos.p, n * sizeof(float4));
             cp(brot.p, snapRot.p, n * sizeof(float2)); cp(wrapCount.p, snapWrap.p, n * sizeof(float));
             cp(sleepTimer.p, snapTimer.p, n * sizeof(float)); cp(bstate.p, snapState.p, n);
@@ -1569,12 +1594,22 @@ struct ag2d_world {
         const float dampHalf = (damp >= 0.0f && damp < 1.0f) ? std::pow(damp, settings.dt * 0.5f) : 2.0f;
         if (nDynBody) {
             pbegin(0);
-            k_integrate<<<gridFor(nDynBody), 256, 0, stream>>>(view(), dynBody.p, nWorlds > 1 ? dynSimd.p : nullptr,
-                                                              nDynBody, settings.dt, settings.gravity_x,
-                                                              settings.gravity_y, dampHalf);
+            const uint8_t* simd = nWorlds > 1 ? dynSimd.p : nullptr;
+            if (jointsActive()) {
+                // The constraints between the halves (Simulation::integrateAndApplyConstraints, :392-407).
+                k_integrate<<<gridFor(nDynBody), 256, 0, stream>>>(view(), dynBody.p, simd, nDynBody, settings.dt,
+                                                                  settings.gravity_x, settings.gravity_y, dampHalf, 1u);
+                launchJoints();
+                k_integrate<<<gridFor(nDynBody), 256, 0, stream>>>(view(), dynBody.p, simd, nDynBody, settings.dt,
+                                                                  settings.gravity_x, settings.gravity_y, dampHalf, 2u);
+                launches += 2;
+            } else {
+                k_integrate<<<gridFor(nDynBody), 256, 0, stream>>>(view(), dynBody.p, simd, nDynBody, settings.dt,
+                                                                  settings.gravity_x, settings.gravity_y, dampHalf, 3u);
+                launches++;
+            }
             CK(cudaGetLastError());
             pend(0);
-            launches++;
         }
     }
 
@@ -1951,6 +1986,126 @@ struct ag2d_world {
         swap_bufs(b, nb);
     }
 
+    // Body constraints ---------------------------------------------------------------------------------------
+    uint32_t jointTotal() const
+    {
+        uint32_t n = 0;
+        for (const JointSystem& js : objects.jointSystems) n += uint32_t(js.joints.size());
+        return n;
+    }
+    bool jointsActive() const { return jointActive[0] + jointActive[1] + jointActive[2] > 0; }
+    // The motors' accumulated impulses from the device into the host table (before the table is reordered or read).
+    void pullMotorImpulses()
+    {
+        auto& motors = objects.jointSystems[JOINT_MOTOR].joints;
+        const uint32_t n = std::min<uint32_t>(motorsOnDevice, uint32_t(motors.size()));
+        if (n == 0) return;
+        const std::vector<float> imp = download(motorImpulse.p, n, stream);
+        for (uint32_t i = 0; i < n; i++) motors[i].impulse = imp[i];
+    }
+    // Before the host tables change (their dense order with them): the device impulses are read back first and
+    // stop matching the table until the next rebuild.
+    void beforeJointEdit()
+    {
+        pullMotorImpulses();
+        motorsOnDevice = 0;
+        jointsDirty = true;
+    }
+    // Regroups every constraint by its bodies' states (Sleeping when a body sleeps, Inactive when no body moves,
+    // else Active: ObjectManager.cpp:1207-1220, 1330-1360), then uploads each kind's active constraints grouped by
+    // level: level(j) = 1 + the highest level of the earlier active constraints of the kind (dense order) that
+    // write one of j's moving bodies.
+    void rebuildJoints()
+    {
+        jointsDirty = false;
+        const cudaStream_t s = stream;
+        pullMotorImpulses();
+        const std::vector<uint8_t> state = download(bstate.p, nBodies, s);
+        auto st = [&](uint32_t b) -> uint8_t { return b < state.size() ? state[b] : uint8_t(STATE_DESTROYED); };
+        std::vector<uint32_t> last(std::max<uint32_t>(nBodies, 1));
+        std::vector<uint2> edges;
+        for (uint32_t k = 0; k < JOINT_KINDS; k++) {
+            JointSystem& js = objects.jointSystems[k];
+            std::vector<uint64_t> handles;
+            for (uint32_t i = 0; i < js.joints.size(); i++) handles.push_back(js.handleOf(i));
+            for (const uint64_t h : handles) {
+                const uint32_t i = js.indexOf(h);
+                const HJoint& j = js.joints[i];
+                const uint8_t sa = st(j.bodyA), sb = j.bodyB == NO_BODY ? uint8_t(STATE_STATIC) : st(j.bodyB);
+                const bool sleeping = sa == STATE_SLEEPING || sb == STATE_SLEEPING;
+                const bool moves = sa == STATE_DYNAMIC || sb == STATE_DYNAMIC;
+                const uint32_t g = sleeping ? JGROUP_SLEEPING : (moves ? JGROUP_ACTIVE : JGROUP_INACTIVE);
+                if (js.groupOf(i) != g) js.moveToGroup(i, g);
+            }
+            const uint32_t begin = js.starts[JGROUP_ACTIVE], end = js.starts[JGROUP_UNUSED];
+            std::fill(last.begin(), last.end(), 0u);
+            std::vector<uint32_t> level(end - begin);
+            uint32_t levels = 0;
+            for (uint32_t i = begin; i < end; i++) {
+                const HJoint& j = js.joints[i];
+                uint32_t l = 0;
+                if (st(j.bodyA) == STATE_DYNAMIC) l = std::max(l, last[j.bodyA]);
+                if (j.bodyB != NO_BODY && st(j.bodyB) == STATE_DYNAMIC) l = std::max(l, last[j.bodyB]);
+                level[i - begin] = ++l;
+                if (st(j.bodyA) == STATE_DYNAMIC) last[j.bodyA] = l;
+                if (j.bodyB != NO_BODY && st(j.bodyB) == STATE_DYNAMIC) last[j.bodyB] = l;
+                levels = std::max(levels, l);
+                if (k != JOINT_MOTOR) edges.push_back(make_uint2(j.bodyA, j.bodyB));
+            }
+            // Level-major order, dense order within a level.
+            std::vector<uint32_t> start(levels + 2, 0);
+            for (const uint32_t l : level) start[l + 1]++;
+            for (uint32_t l = 1; l <= levels + 1; l++) start[l] += start[l - 1];
+            std::vector<uint32_t> fill(start.begin(), start.end());
+            std::vector<JointRec> recs(end - begin);
+            for (uint32_t i = begin; i < end; i++) {
+                const HJoint& j = js.joints[i];
+                JointRec r{};
+                r.bodyA = j.bodyA; r.bodyB = j.bodyB == NO_BODY ? j.bodyA : j.bodyB; r.index = i;
+                r.ax = j.anchorAx; r.ay = j.anchorAy; r.bx = j.anchorBx; r.by = j.anchorBy;
+                if (k == JOINT_SPRING) { r.p0 = j.restLength; r.p1 = j.stiffness; r.p2 = j.damping; }
+                else if (k == JOINT_REVOLUTE) { r.p1 = j.stiffness; r.p2 = j.damping; }
+                else { r.p0 = j.targetSpeed; r.p1 = j.maxTorque; }
+                recs[fill[level[i - begin]]++] = r;
+            }
+            jointActive[k] = end - begin;
+            jointLevels[k] = levels;
+            jointLevelHost[k].assign(start.begin() + 1, start.end());   // level l (from 1) starts at [l - 1]
+            jointRec[k].upload(recs.data(), recs.size(), s);
+            jointLevel[k].upload(jointLevelHost[k].data(), jointLevelHost[k].size(), s);
+            jointData[k].reserve(std::max<size_t>(recs.size(), 1));
+        }
+        auto& motors = objects.jointSystems[JOINT_MOTOR].joints;
+        std::vector<float> imp(motors.size());
+        for (size_t i = 0; i < motors.size(); i++) imp[i] = motors[i].impulse;
+        motorImpulse.upload(imp.data(), imp.size(), s);
+        snapMotorImpulse.reserve(std::max<size_t>(imp.size(), 1));
+        motorsOnDevice = uint32_t(imp.size());
+        nJointEdges = uint32_t(edges.size());
+        jointEdges.upload(edges.data(), edges.size(), s);
+        CK(cudaStreamSynchronize(s));
+    }
+    void launchJoints()
+    {
+        JointLaunch L{};
+        uint32_t maxIt = 0;
+        for (uint32_t k = 0; k < JOINT_KINDS; k++) {
+            L.rec[k] = jointRec[k].p;
+            L.data[k] = jointData[k].p;
+            L.levelStart[k] = jointLevel[k].p;
+            L.count[k] = jointActive[k];
+            L.levels[k] = jointLevels[k];
+            L.iterations[k] = objects.jointSystems[k].iterations;
+            if (jointActive[k]) maxIt = std::max(maxIt, L.iterations[k]);
+        }
+        L.maxIterations = maxIt;
+        L.dt = settings.dt;
+        L.motorImpulse = motorImpulse.p;
+        k_joints<<<1, JOINT_THREADS, 0, stream>>>(view(), L);
+        CK(cudaGetLastError());
+        launches++;
+    }
+
     // Collision events --------------------------------------------------------------------------------------
     // Colliders the world has: the host's (created worlds) or the device's (a world made by load_state).
     uint32_t colliderCount() const
@@ -2127,6 +2282,10 @@ struct ag2d_world {
         if (!islandsLinked) {
             k_island_init<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p);
             k_island_union<<<gridFor(manifoldCap), 256, 0, s>>>(w, manifolds.p, nManifolds.p, ufParent.p);
+            if (nJointEdges) {
+                k_island_union_edges<<<gridFor(nJointEdges), 256, 0, s>>>(w, jointEdges.p, nJointEdges, ufParent.p);
+                launches++;
+            }
         }
         islandsLinked = false;
         k_island_quiet<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p, settings.dt, settings.sleep_speed,
@@ -2240,7 +2399,7 @@ struct ag2d_world {
     // The next step then rebuilds the work lists and the static tree and poses every collider (spatialDirty).
     void flushCommands()
     {
-        if (commands.empty()) return;
+        if (commands.empty() && jointCommands.empty()) return;
         if (nWorlds > 1) { commands.clear(); throw ApiError(AG2D_ERR_UNSUPPORTED, "body commands are per world"); }
         ensureUploaded();
         const cudaStream_t s = stream;
@@ -2279,6 +2438,20 @@ struct ag2d_world {
             case AG2D_COMMAND_DESTROY:
                 state[b] = STATE_DESTROYED;
                 o.slotGeneration[uint32_t(c.handle & 0xFFFFFFFFu)]++;
+                // Its constraints go with it, waking their other bodies (ObjectManager.cpp:400-410, 502-520).
+                for (JointSystem& js : o.jointSystems) {
+                    std::vector<uint64_t> doomed;
+                    for (uint32_t i = 0; i < js.joints.size(); i++)
+                        if (js.joints[i].bodyA == b || js.joints[i].bodyB == b) doomed.push_back(js.handleOf(i));
+                    if (doomed.empty()) continue;
+                    beforeJointEdit();
+                    for (const uint64_t h : doomed) {
+                        const uint32_t i = js.indexOf(h);
+                        const uint32_t other = js.joints[i].bodyA == b ? js.joints[i].bodyB : js.joints[i].bodyA;
+                        if (other != NO_BODY && other < nBodies) wake(other);
+                        js.destroy(i);
+                    }
+                }
                 break;
             case AG2D_COMMAND_POSITION: {
                 const float r = pos[b].z, cosR = std::cos(r), sinR = std::sin(r);
@@ -2329,6 +2502,30 @@ struct ag2d_world {
             }
         }
         commands.clear();
+        // Constraint destroys and edits (ConstraintSystemBase::flushImpl, ConstraintSystemBase.h:127-142, and the
+        // systems' flushCommands): stale handles are dropped; the constraint's bodies wake.
+        for (const JointCommand& c : jointCommands) {
+            JointSystem& js = o.jointSystems[c.kind];
+            const uint32_t i = js.indexOf(c.handle);
+            if (i == NO_BODY) continue;
+            beforeJointEdit();
+            HJoint& j = js.joints[i];
+            if (j.bodyA < nBodies) wake(j.bodyA);
+            if (j.bodyB != NO_BODY && j.bodyB < nBodies) wake(j.bodyB);
+            switch (c.field) {
+            case -1: js.destroy(i); break;
+            case AG2D_JOINT_ANCHOR_A: j.anchorAx = c.a; j.anchorAy = c.b; break;
+            case AG2D_JOINT_ANCHOR_B: j.anchorBx = c.a; j.anchorBy = c.b; break;
+            case AG2D_JOINT_REST_LENGTH: j.restLength = std::fmax(0.0f, c.a); break;
+            case AG2D_JOINT_STIFFNESS: j.stiffness = std::fmax(0.0f, c.a); break;
+            case AG2D_JOINT_DAMPING: j.damping = std::fmax(0.0f, c.a); break;
+            case AG2D_JOINT_TARGET_SPEED: j.targetSpeed = c.a; break;
+            case AG2D_JOINT_MAX_TORQUE: j.maxTorque = std::fmax(0.0f, c.a); break;
+            default: break;
+            }
+        }
+        jointCommands.clear();
+        if (jointTotal()) jointsDirty = true;   // body states may have changed: constraint groups with them
         restoreWokenIslands(state, timer, island, wokenRoots, editedBody, anyEdited);
         if (nBodies) {
             CK(cudaMemcpyAsync(bvel.p, vel.data(), nBodies * sizeof(float4), cudaMemcpyHostToDevice, s));
@@ -2443,6 +2640,7 @@ struct ag2d_world {
         } hostTimer{hostMs, tStart};
         ensureUploaded();
         flushCommands();
+        if (jointsDirty) rebuildJoints();
         // BodyCollisionSolver::resetCollisionData and setCollisionEventRecording (Simulation.cpp:261-266).
         lastEvents.clear();
         recording = eventsEnabled && callbacksAlive > 0 && nWorlds <= 1;
@@ -2544,6 +2742,7 @@ struct ag2d_world {
                 const bool removals = hCounters->staged > 0 || (nDestroyed > 0 && hCounters->stored > 0);
                 if (hCounters->slept || removals) phaseSleepStore(hCounters->stored, hCounters->slept > 0, removals);
             }
+            if (hCounters->topoDirty && jointTotal()) jointsDirty = true;   // constraints change group
             if (hCounters->topoDirty) {
                 // Woken or slept bodies: refresh the poses of every collider at the post-step state (the reference
                 // rebuilds its spatial data in postUpdate, Simulation.cpp:640-647), then the work lists and the
@@ -2910,6 +3109,10 @@ int32_t ag2d_world_load_state(ag2d_world* world, const ag2d_state_desc* st)
         w.objects.colliders.clear();
         w.loadedOptIn.assign(nc, ColliderEvent{0u, 3.40282347e38f});
         w.optInDirty = true;
+        for (JointSystem& js : w.objects.jointSystems) js = JointSystem();
+        for (uint32_t k = 0; k < JOINT_KINDS; k++) w.jointActive[k] = w.jointLevels[k] = 0;
+        w.nJointEdges = 0;
+        w.jointsDirty = false;
         w.hostDirty = false;
     });
 }
@@ -2926,6 +3129,116 @@ int32_t ag2d_world_step(ag2d_world* world, int32_t steps)
             world->dispatchEvents();
         }
     });
+}
+
+// Body constraints ------------------------------------------------------------------------------------------
+
+// A body command that only wakes the body's island (constraint creation on a world that has run).
+constexpr int32_t COMMAND_WAKE = 100;
+
+static JointSystem& joint_system(ag2d_world* world, int32_t kind)
+{
+    if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+    if (kind < 0 || kind >= int32_t(JOINT_KINDS)) throw ApiError(AG2D_ERR_INVALID_ARG, "unknown constraint kind");
+    if (world->nWorlds > 1) throw ApiError(AG2D_ERR_UNSUPPORTED, "body constraints are per world");
+    return world->objects.jointSystems[kind];
+}
+
+static uint64_t body_handle_of(const HostObjects& o, uint32_t b)
+{
+    if (b == NO_BODY || b >= o.bodies.size()) return 0;
+    const uint32_t slot = o.bodies[b].handleSlot;
+    return (uint64_t(o.slotGeneration[slot]) << 32) | slot;
+}
+
+int32_t ag2d_world_create_joint(ag2d_world* world, const ag2d_joint_desc* d, uint64_t* out_handle)
+{
+    return guarded([&] {
+        if (!d || !out_handle) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        JointSystem& js = joint_system(world, d->kind);
+        HostObjects& o = world->objects;
+        const bool single = d->kind == AG2D_JOINT_MOTOR;
+        const uint32_t a = o.indexOf(d->body_a), b = single ? NO_BODY : o.indexOf(d->body_b);
+        if (a == 0xFFFFFFFFu || (!single && b == 0xFFFFFFFFu))
+            throw ApiError(AG2D_ERR_INVALID_ARG, "stale body handle");
+        world->beforeJointEdit();
+        HJoint j;
+        j.bodyA = a;
+        j.bodyB = b;
+        j.anchorAx = d->anchor_a_x; j.anchorAy = d->anchor_a_y; j.anchorBx = d->anchor_b_x; j.anchorBy = d->anchor_b_y;
+        j.restLength = d->rest_length; j.stiffness = d->stiffness; j.damping = d->damping;
+        j.targetSpeed = d->target_speed; j.maxTorque = d->max_torque; j.impulse = 0.0f;
+        // refreshConstraintGroup (ObjectManager.cpp:1207-1220): Inactive when no body has mass.
+        const bool inactive = o.bodies[a].invMass == 0.0f && (single || o.bodies[b].invMass == 0.0f);
+        const uint32_t i = js.create(j, inactive ? JGROUP_INACTIVE : JGROUP_ACTIVE);
+        *out_handle = js.handleOf(i);
+        if (!world->hostDirty) {   // the bodies wake (createConstraint, ObjectManager.cpp:451-454) at the flush
+            world->commands.push_back(BodyCommand{COMMAND_WAKE, d->body_a, 0.0f, 0.0f});
+            if (!single) world->commands.push_back(BodyCommand{COMMAND_WAKE, d->body_b, 0.0f, 0.0f});
+        }
+    });
+}
+
+int32_t ag2d_world_destroy_joint(ag2d_world* world, int32_t kind, uint64_t handle)
+{
+    return guarded([&] {
+        joint_system(world, kind);
+        world->jointCommands.push_back(ag2d_world::JointCommand{kind, -1, handle, 0.0f, 0.0f});
+    });
+}
+
+int32_t ag2d_world_set_joint(ag2d_world* world, int32_t kind, uint64_t handle, int32_t field, float a, float b)
+{
+    return guarded([&] {
+        joint_system(world, kind);
+        if (field < AG2D_JOINT_ANCHOR_A || field > AG2D_JOINT_MAX_TORQUE)
+            throw ApiError(AG2D_ERR_INVALID_ARG, "unknown constraint field");
+        world->jointCommands.push_back(ag2d_world::JointCommand{kind, field, handle, a, b});
+    });
+}
+
+int32_t ag2d_world_joint(ag2d_world* world, int32_t kind, uint64_t handle, ag2d_joint_desc* out)
+{
+    return guarded([&] {
+        JointSystem& js = joint_system(world, kind);
+        if (!out) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        const uint32_t i = js.indexOf(handle);
+        if (i == NO_BODY) throw ApiError(AG2D_ERR_INVALID_ARG, "stale constraint handle");
+        if (kind == AG2D_JOINT_MOTOR) world->pullMotorImpulses();
+        const HJoint& j = js.joints[i];
+        *out = ag2d_joint_desc{};
+        out->kind = kind;
+        out->body_a = body_handle_of(world->objects, j.bodyA);
+        out->body_b = body_handle_of(world->objects, j.bodyB);
+        out->anchor_a_x = j.anchorAx; out->anchor_a_y = j.anchorAy;
+        out->anchor_b_x = j.anchorBx; out->anchor_b_y = j.anchorBy;
+        out->rest_length = j.restLength; out->stiffness = j.stiffness; out->damping = j.damping;
+        out->target_speed = j.targetSpeed; out->max_torque = j.maxTorque; out->impulse = j.impulse;
+    });
+}
+
+int32_t ag2d_world_joint_count(ag2d_world* world, int32_t kind, uint32_t* out_count)
+{
+    return guarded([&] {
+        JointSystem& js = joint_system(world, kind);
+        if (!out_count) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        *out_count = uint32_t(js.joints.size());
+    });
+}
+
+int32_t ag2d_world_joint_handle(ag2d_world* world, int32_t kind, uint32_t index, uint64_t* out_handle)
+{
+    return guarded([&] {
+        JointSystem& js = joint_system(world, kind);
+        if (!out_handle) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        if (index >= js.joints.size()) throw ApiError(AG2D_ERR_INVALID_ARG, "constraint index out of range");
+        *out_handle = js.handleOf(index);
+    });
+}
+
+int32_t ag2d_world_set_joint_iterations(ag2d_world* world, int32_t kind, uint32_t iterations)
+{
+    return guarded([&] { joint_system(world, kind).iterations = iterations; });
 }
 
 int32_t ag2d_device_allocs(uint64_t* out)
@@ -3629,6 +3942,8 @@ int32_t ag2d_batch_create(ag2d_world* const* worlds, uint32_t count, ag2d_batch*
         if (!out || !worlds || count == 0) throw ApiError(AG2D_ERR_INVALID_ARG, "a batch needs at least one world");
         for (uint32_t k = 0; k < count; k++) {
             if (!worlds[k]) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+            if (worlds[k]->jointTotal())
+                throw ApiError(AG2D_ERR_UNSUPPORTED, "a world with body constraints cannot join a batch");
             if (!same_settings(worlds[k]->settings, worlds[0]->settings))
                 throw ApiError(AG2D_ERR_INVALID_ARG, "worlds of a batch must share their step settings");
         }
@@ -4032,6 +4347,8 @@ int32_t ag2d_server_submit(ag2d_server* server, ag2d_world* world, uint32_t step
         if (!server || !world) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
         if (!same_settings(world->settings, server->settings.world))
             throw ApiError(AG2D_ERR_INVALID_ARG, "the request's world settings differ from the server's");
+        if (world->jointTotal())
+            throw ApiError(AG2D_ERR_UNSUPPORTED, "a world with body constraints cannot join a batch");
         auto r = std::make_shared<ServerRequest>();
         {
             // Packed on the caller's thread: the server loop only copies the blob to the device.

@@ -150,9 +150,75 @@ uint32_t HostObjects::appendBody(float px, float py, float vx, float vy, float r
     return moveBodyDown(uint32_t(bodies.size() - 1), invMass == 0.0f ? 0u : 2u);
 }
 
+// ---- constraint systems ----
+
+void JointSystem::swap(uint32_t a, uint32_t b)
+{
+    if (a == b) return;
+    std::swap(joints[a], joints[b]);
+    slotIndex[joints[a].handleSlot] = a;
+    slotIndex[joints[b].handleSlot] = b;
+}
+
+uint32_t JointSystem::moveToGroup(uint32_t index, uint32_t target)
+{
+    uint32_t g = groupOf(index);
+    while (g != target) {
+        if (g < target) {   // to the group's last slot, then across the boundary above it
+            const uint32_t last = starts[g + 1] - 1;
+            swap(index, last);
+            index = last;
+            starts[g + 1]--;
+            g++;
+        } else {            // to the group's first slot, then across the boundary below it
+            const uint32_t first = starts[g];
+            swap(index, first);
+            index = first;
+            starts[g]++;
+            g--;
+        }
+    }
+    return index;
+}
+
+uint32_t JointSystem::create(const HJoint& j, uint32_t group)
+{
+    uint32_t slot;
+    if (freeHead != NO_BODY) {
+        slot = freeHead;
+        freeHead = slotIndex[slot];
+    } else {
+        slot = uint32_t(slotIndex.size());
+        slotIndex.push_back(0);
+        slotGeneration.push_back(0);
+    }
+    joints.push_back(j);
+    joints.back().handleSlot = slot;
+    const uint32_t index = uint32_t(joints.size() - 1);
+    slotIndex[slot] = index;   // appended in the unused range, then moved down to its group
+    return moveToGroup(index, group);
+}
+
+void JointSystem::destroy(uint32_t index)
+{
+    if (index >= joints.size()) return;
+    index = moveToGroup(index, JGROUP_UNUSED);
+    swap(index, uint32_t(joints.size() - 1));
+    const uint32_t slot = joints.back().handleSlot;
+    joints.pop_back();
+    slotGeneration[slot]++;
+    slotIndex[slot] = freeHead;
+    freeHead = slot;
+}
+
 void HostObjects::swapBodies(uint32_t a, uint32_t b)
 {
     if (a == b) return;
+    for (JointSystem& js : jointSystems)
+        for (HJoint& j : js.joints) {
+            if (j.bodyA == a) j.bodyA = b; else if (j.bodyA == b) j.bodyA = a;
+            if (j.bodyB == a) j.bodyB = b; else if (j.bodyB == b) j.bodyB = a;
+        }
     std::swap(bodies[a], bodies[b]);
     for (uint32_t c : bodies[a].colliders) colliders[c].body = a;
     for (uint32_t c : bodies[b].colliders) colliders[c].body = b;

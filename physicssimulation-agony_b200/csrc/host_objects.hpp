@@ -57,8 +57,58 @@ struct Groups {
     }
 };
 
+// Constraints between bodies (SimulationImpl/ConstraintSystems/*, SoA/Constraints/*): springs, revolute joints and
+// motors. A system keeps its constraints in the reference's dense order, grouped [Inactive][Sleeping][Active]
+// (ConstraintGroup, ConstraintSystemBase.h:22-24; Inactive: every body static), moved between groups by the same
+// boundary swaps (ObjectManager::moveConstraintToGroup, ObjectManager.cpp:1172-1205), with a handle table whose
+// freed slots are reused last-in first-out with the generation raised (HandleTable.h:30-90).
+enum JointKind : uint32_t { JOINT_SPRING = 0, JOINT_REVOLUTE = 1, JOINT_MOTOR = 2, JOINT_KINDS = 3 };
+enum JointGroup : uint32_t { JGROUP_INACTIVE = 0, JGROUP_SLEEPING = 1, JGROUP_ACTIVE = 2, JGROUP_UNUSED = 3 };
+constexpr uint32_t NO_BODY = 0xFFFFFFFFu;
+
+struct HJoint {
+    uint32_t bodyA = 0, bodyB = NO_BODY;   // dense body indices (motors: bodyA only)
+    float anchorAx = 0, anchorAy = 0, anchorBx = 0, anchorBy = 0;   // body-local anchors
+    float restLength = 0, stiffness = 0, damping = 0;               // spring (revolute: stiffness, damping)
+    float targetSpeed = 0, maxTorque = 0, impulse = 0;              // motor; impulse: accumulated (warm start)
+    uint32_t handleSlot = 0;
+};
+
+struct JointSystem {
+    std::vector<HJoint> joints;
+    uint32_t starts[4] = {0, 0, 0, 0};   // first index of each group; starts[3]: end of the live constraints
+    uint32_t iterations = 6;             // IConstraintSystem::iterations (ConstraintSystemBase.h:34)
+    std::vector<uint32_t> slotIndex, slotGeneration;
+    uint32_t freeHead = NO_BODY;
+
+    uint32_t groupOf(uint32_t i) const
+    {
+        for (uint32_t g = 0; g < 3; g++) if (i >= starts[g] && i < starts[g + 1]) return g;
+        return JGROUP_UNUSED;
+    }
+    uint32_t indexOf(uint64_t handle) const
+    {
+        const uint32_t slot = uint32_t(handle & 0xFFFFFFFFu), gen = uint32_t(handle >> 32);
+        if (slot >= slotIndex.size() || slotGeneration[slot] != gen || slotIndex[slot] == NO_BODY) return NO_BODY;
+        return slotIndex[slot];
+    }
+    uint64_t handleOf(uint32_t i) const
+    {
+        const uint32_t slot = joints[i].handleSlot;
+        return (uint64_t(slotGeneration[slot]) << 32) | slot;
+    }
+    // Appends and moves the constraint to 'group' (createConstraint + refreshConstraintGroup,
+    // ObjectManager.cpp:430-475, 1207-1220). Returns its dense index.
+    uint32_t create(const HJoint& j, uint32_t group);
+    // Moves to the unused group and pops (destroyConstraintInternal, ObjectManager.cpp:502-520).
+    void destroy(uint32_t index);
+    uint32_t moveToGroup(uint32_t index, uint32_t group);
+    void swap(uint32_t a, uint32_t b);
+};
+
 class HostObjects {
 public:
+    JointSystem jointSystems[JOINT_KINDS];
     std::vector<HBody> bodies;
     std::vector<HCollider> colliders;
     std::vector<float> circleRadius;

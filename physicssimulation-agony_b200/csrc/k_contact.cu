@@ -546,6 +546,22 @@ __global__ void k_island_union(DeviceWorld w, const Manifold* __restrict__ m, co
     }
 }
 
+// The active body constraints' links (Simulation.cpp:338-341: islandManager.step over each system's active edges).
+__global__ void k_island_union_edges(DeviceWorld w, const uint2* __restrict__ edges, uint32_t n,
+                                     uint32_t* __restrict__ parent)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t a = edges[i].x, b = edges[i].y;
+        if (w.bstate[a] != STATE_DYNAMIC || w.bstate[b] != STATE_DYNAMIC) continue;
+        for (uint32_t tries = 0; tries < 1u << 20; tries++) {
+            uint32_t ra = uf_find(parent, a), rb = uf_find(parent, b);
+            if (ra == rb) break;
+            if (ra < rb) { const uint32_t t = ra; ra = rb; rb = t; }
+            if (atomicCAS(parent + ra, ra, rb) == ra) break;
+        }
+    }
+}
+
 __global__ void k_island_quiet(DeviceWorld w, uint32_t* __restrict__ parent, uint32_t* __restrict__ flag, float dt,
                                float speedThreshold, float timeThreshold)
 {

@@ -11,9 +11,12 @@ namespace ag2d {
 // 140-299, call order Simulation.cpp:392-407), wrapBodyRotations (LeftOutFunctions.cpp:13-60) and
 // computeRotationCosSin (Integrator.cpp:301-311), fused per dynamic body. Elementwise: HBM-bound at 40 B/body.
 // ---------------------------------------------------------------------------------------------------------------
+// phase: 3 both halves; 1 the first (half kick and damping: Integrator::integratePhase1_VelocityVerlet +
+// dampAngularVelocities); 2 the second (position step, half kick, damping, wrap, cos/sin). The body constraints
+// run between the two (Simulation.cpp:399-404).
 __global__ void k_integrate(DeviceWorld w, const uint32_t* __restrict__ dynBody, const uint8_t* __restrict__ dynSimd,
                             uint32_t nDyn, float dt, float gx, float gy,
-                            float dampHalf /* damping^(dt/2), or >= 1 when damping is off */)
+                            float dampHalf /* damping^(dt/2), or >= 1 when damping is off */, uint32_t phase)
 {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nDyn; k += gridDim.x * blockDim.x) {
         const uint32_t b = dynBody[k];
@@ -24,12 +27,18 @@ __global__ void k_integrate(DeviceWorld w, const uint32_t* __restrict__ dynBody,
         const float gdx = gx * halfDT, gdy = gy * halfDT;
         const bool movable = v.w != 0.0f;
         const bool angMovable = p.w != 0.0f;
-        if (simd) { v.x += movable ? gdx : 0.0f; v.y += movable ? gdy : 0.0f; }
-        else { v.x += gdx * float(movable); v.y += gdy * float(movable); }
-        if (dampHalf < 1.0f) {
-            const float nv = v.z * dampHalf;
-            if (simd) v.z = angMovable ? nv : v.z;
-            else { const float m = float(angMovable); v.z = m * nv + (1.0f - m) * v.z; }
+        if (phase & 1u) {
+            if (simd) { v.x += movable ? gdx : 0.0f; v.y += movable ? gdy : 0.0f; }
+            else { v.x += gdx * float(movable); v.y += gdy * float(movable); }
+            if (dampHalf < 1.0f) {
+                const float nv = v.z * dampHalf;
+                if (simd) v.z = angMovable ? nv : v.z;
+                else { const float m = float(angMovable); v.z = m * nv + (1.0f - m) * v.z; }
+            }
+            if (!(phase & 2u)) {
+                w.bvel[b] = v;
+                continue;
+            }
         }
         p.x = v.x * dt + p.x;
         p.y = v.y * dt + p.y;

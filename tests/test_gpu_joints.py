@@ -1,0 +1,198 @@
+"""Body constraints through the C ABI (ConstraintAPI, SimulationAPIs/ConstraintAPI.h:32-105: springs, revolute joints,
+motors) against the reference engine making the same calls (oracle/ref_harness.cpp: agref_create_joint).
+
+- Free bodies (no colliders, no sleep): a pendulum chain of revolute joints hanging from a static body, a spring
+  ladder, motors driving some links. Every body's position, rotation and velocities equal the reference's bit for bit
+  after 240 steps, and so do the motors' accumulated impulses: the level schedule solves each kind in the
+  reference's dense order.
+- A random constraint graph (2,000 bodies, 6,000 springs and revolute joints, 300 motors, some on static bodies):
+  bit-exact after 60 steps; levels run in parallel with barriers between them.
+- The API: a stale body handle is refused; destroys and edits wait for the next step; destroying a body takes its
+  constraints; constraints between static bodies are inactive; a constrained world cannot join a batch.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ag2d = pytest.importorskip("ag2d")
+from oracle import refapi  # noqa: E402
+
+REF_KIND = {ag2d.JOINT_SPRING: 0, ag2d.JOINT_REVOLUTE: 1, ag2d.JOINT_MOTOR: 4}
+BODY_FIELDS = [(ag2d.BODY_COM_X, "comX"), (ag2d.BODY_COM_Y, "comY"), (ag2d.BODY_VEL_X, "velocityX"),
+               (ag2d.BODY_VEL_Y, "velocityY"), (ag2d.BODY_ROTATION, "rotation"),
+               (ag2d.BODY_ANGULAR_VELOCITY, "angularVelocity")]
+NO_SLEEP = 1.0e6
+
+
+class _Scene:   # the settings RefSim reads; bodies come through create_body
+    n = 0
+    materials = []
+    dt = 1.0 / 60.0
+    velocity_iterations, position_iterations = 8, 3
+    gravity = (0.0, -9.81)
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+
+
+class _Pair:
+    """The reference and this library driven through the same calls."""
+
+    def __init__(self):
+        self.ref = refapi.RefSim(_Scene(), sleep_time=NO_SLEEP)
+        self.w = ag2d.World(dt=_Scene.dt, gravity=_Scene.gravity, sleep_time=NO_SLEEP)
+        self.slots, self.handles = [], []
+        # A static box far below, so that each world has a collider (the constrained bodies have none).
+        self.ref.add_collider(self.ref.create_body(0.0, -1000.0, mass=0.0, inertia=0.0), 1, width=10.0, height=1.0)
+        self.w.add_collider(self.w.create_body(0.0, -1000.0, mass=0.0, inertia=0.0), 1, width=10.0, height=1.0)
+
+    def body(self, x, y, mass=1.0, inertia=0.2, rotation=0.0, vx=0.0, vy=0.0, w=0.0):
+        self.slots.append(self.ref.create_body(x, y, rotation=rotation, vx=vx, vy=vy, w=w, mass=mass,
+                                               inertia=inertia if mass > 0 else 0.0))
+        self.handles.append(self.w.create_body(x, y, rotation=rotation, vx=vx, vy=vy, w=w, mass=mass,
+                                               inertia=inertia if mass > 0 else 0.0))
+        return len(self.slots) - 1
+
+    def joint(self, kind, a, b=None, anchor_a=(0.0, 0.0), anchor_b=(0.0, 0.0), rest=0.0, k=0.0, c=0.0, speed=0.0,
+              torque=0.0):
+        if kind == ag2d.JOINT_SPRING:
+            p = [*anchor_a, *anchor_b, rest, k, c]
+        elif kind == ag2d.JOINT_REVOLUTE:
+            p = [*anchor_a, *anchor_b, k, c]
+        else:
+            p = [speed, torque]
+        slot = self.ref.body_slots   # create_body returns an index into it
+        sb = slot[self.slots[b]] if b is not None else 0
+        assert self.ref.create_joint(REF_KIND[kind], slot[self.slots[a]], sb, p) >= 0
+        return self.w.create_joint(kind, self.handles[a], self.handles[b] if b is not None else 0, anchor_a,
+                                   anchor_b, rest, k, c, speed, torque)
+
+    def step(self, n):
+        self.ref.update(n)
+        self.w.step(n)
+
+    def assert_bodies_equal(self):
+        self.ref.dump_state("j.")
+        ours = {f: self.w.read(f) for f, _ in BODY_FIELDS}
+        for f, name in BODY_FIELDS:
+            theirs = self.ref.blob("j.body." + name)
+            mine = np.array([ours[f][self.w.body_index(h)] for h in self.handles], np.float32)
+            want = np.array([theirs[self.ref.body_index(s)] for s in self.slots], np.float32)
+            bad = np.nonzero(_bits(mine) != _bits(want))[0]
+            assert bad.size == 0, (name, bad[:5], mine[bad[:5]], want[bad[:5]])
+
+    def close(self):
+        self.ref.close()
+        self.w.close()
+
+
+@pytest.fixture
+def pair():
+    if not refapi.available():
+        pytest.skip("the compiled reference (oracle/_ref) is not present")
+    p = _Pair()
+    yield p
+    p.close()
+
+
+def test_chain_ladder_and_motors_match_the_reference_bit_for_bit(pair):
+    anchor = pair.body(0.0, 20.0, mass=0.0)
+    prev = anchor
+    links = []
+    for k in range(12):   # a pendulum chain starting horizontal
+        b = pair.body(1.0 + k, 20.0, mass=1.0 + 0.1 * k, inertia=0.1)
+        pair.joint(ag2d.JOINT_REVOLUTE, prev, b, (0.5, 0.0) if prev != anchor else (0.0, 0.0), (-0.5, 0.0),
+                   k=5.0e4, c=50.0)
+        links.append(b)
+        prev = b
+    rails = [pair.body(30.0 + 1.5 * k, 10.0, mass=2.0, inertia=0.4, vx=0.3 * k) for k in range(8)]
+    rails2 = [pair.body(30.0 + 1.5 * k, 8.0, mass=1.0, inertia=0.3, w=0.2) for k in range(8)]
+    top = pair.body(40.0, 14.0, mass=0.0)
+    for a, b in zip(rails, rails[1:]):
+        pair.joint(ag2d.JOINT_SPRING, a, b, (0.2, 0.1), (-0.2, 0.0), rest=1.4, k=300.0, c=4.0)
+    for a, b in zip(rails, rails2):
+        pair.joint(ag2d.JOINT_SPRING, a, b, (0.0, -0.1), (0.0, 0.1), rest=2.0, k=800.0, c=10.0)
+    pair.joint(ag2d.JOINT_SPRING, top, rails[3], (0.0, 0.0), (0.0, 0.2), rest=3.0, k=2000.0, c=30.0)
+    motors = [pair.joint(ag2d.JOINT_MOTOR, b, speed=2.0 - 0.5 * i, torque=5.0 + i) for i, b in
+              enumerate(links[::3] + rails2[::2])]
+    for _ in range(4):
+        pair.step(60)
+        pair.assert_bodies_equal()
+    imp, slot = pair.ref.motor_impulses()
+    index_of_slot = {sl: i for i, sl in enumerate(pair.ref.body_slots)}
+    ours = {pair.w.body_index(pair.handles[pair.slots.index(index_of_slot[s])]): v
+            for s, v in zip(slot.tolist(), imp.tolist())}
+    for h in motors:
+        d = pair.w.joint(ag2d.JOINT_MOTOR, h)
+        b = pair.w.body_index(d["body_a"])
+        assert _bits([d["impulse"]])[0] == _bits([ours[b]])[0]
+    assert pair.w.counters()["status"] == 0
+
+
+def test_random_constraint_graph_matches_the_reference(pair):
+    rng = np.random.default_rng(3)
+    n = 2000
+    for i in range(n):
+        static = i % 50 == 0
+        pair.body(float(rng.uniform(-50, 50)), float(rng.uniform(0, 100)), mass=0.0 if static else
+                  float(rng.uniform(0.5, 3.0)), inertia=float(rng.uniform(0.05, 1.0)),
+                  vx=float(rng.normal(0, 1)), vy=float(rng.normal(0, 1)), w=float(rng.normal(0, 0.5)))
+    for j in range(6000):
+        a, b = rng.choice(n, 2, replace=False).tolist()
+        anchors = (tuple(rng.uniform(-0.5, 0.5, 2).tolist()), tuple(rng.uniform(-0.5, 0.5, 2).tolist()))
+        if j % 2 == 0:
+            pair.joint(ag2d.JOINT_SPRING, a, b, *anchors, rest=float(rng.uniform(0.5, 5.0)),
+                       k=float(rng.uniform(10, 200)), c=float(rng.uniform(0.5, 5.0)))
+        else:
+            pair.joint(ag2d.JOINT_REVOLUTE, a, b, *anchors, k=float(rng.uniform(50, 500)),
+                       c=float(rng.uniform(1.0, 10.0)))
+    for b in rng.choice(n, 300, replace=False).tolist():
+        pair.joint(ag2d.JOINT_MOTOR, b, speed=float(rng.uniform(-3, 3)), torque=float(rng.uniform(0.5, 20)))
+    assert pair.w.joint_count(ag2d.JOINT_SPRING) == 3000 and pair.w.joint_count(ag2d.JOINT_MOTOR) == 300
+    for _ in range(3):
+        pair.step(20)
+        pair.assert_bodies_equal()
+
+
+def test_constraint_api(pair):
+    ground = pair.body(0.0, 0.0, mass=0.0)
+    ground2 = pair.body(5.0, 0.0, mass=0.0)
+    a = pair.body(0.0, 5.0)
+    b = pair.body(2.0, 5.0)
+    w = pair.w
+    s = pair.joint(ag2d.JOINT_SPRING, ground, a, rest=5.0, k=100.0, c=2.0)
+    r = pair.joint(ag2d.JOINT_REVOLUTE, a, b, (1.0, 0.0), (-1.0, 0.0), k=1e4, c=10.0)
+    dead = pair.joint(ag2d.JOINT_SPRING, ground, ground2, rest=1.0, k=10.0, c=1.0)   # inactive: no body moves
+    m = pair.joint(ag2d.JOINT_MOTOR, b, speed=1.0, torque=2.0)
+    with pytest.raises(ag2d.Ag2dError):
+        w.create_joint(ag2d.JOINT_SPRING, pair.handles[a], 12345 << 32)
+    d = w.joint(ag2d.JOINT_SPRING, s)
+    assert (d["rest_length"], d["stiffness"], d["damping"]) == (5.0, 100.0, 2.0)
+    assert w.joint(ag2d.JOINT_SPRING, dead)["body_b"] == pair.handles[ground2]
+    pair.step(30)
+    pair.assert_bodies_equal()
+    # Deferred edits: nothing changes until the next step's flush; negative values are clamped at 0.
+    w.set_joint(ag2d.JOINT_SPRING, s, ag2d.JOINT_REST_LENGTH, -3.0)
+    w.set_joint(ag2d.JOINT_MOTOR, m, ag2d.JOINT_TARGET_SPEED, -2.0)
+    assert w.joint(ag2d.JOINT_SPRING, s)["rest_length"] == 5.0
+    w.step(1)
+    assert w.joint(ag2d.JOINT_SPRING, s)["rest_length"] == 0.0
+    assert w.joint(ag2d.JOINT_MOTOR, m)["target_speed"] == -2.0
+    # Deferred destroy; a stale handle is dropped when the commands are applied.
+    w.destroy_joint(ag2d.JOINT_REVOLUTE, r)
+    w.destroy_joint(ag2d.JOINT_REVOLUTE, r)
+    assert w.joint_count(ag2d.JOINT_REVOLUTE) == 1
+    w.step(1)
+    assert w.joint_count(ag2d.JOINT_REVOLUTE) == 0
+    with pytest.raises(ag2d.Ag2dError):
+        w.joint(ag2d.JOINT_REVOLUTE, r)
+    # Destroying a body takes its constraints.
+    w.destroy_body(pair.handles[b])
+    w.step(1)
+    assert w.joint_count(ag2d.JOINT_MOTOR) == 0 and w.joint_count(ag2d.JOINT_SPRING) == 2
+    # A constrained world cannot join a batch.
+    with pytest.raises(ag2d.Ag2dError):
+        ag2d.Batch([w])
+    assert w.counters()["status"] == 0
