@@ -250,34 +250,43 @@ int32_t ag2d_world_set_body_inertia(ag2d_world* world, uint64_t body, float iner
 /* Applies the queued commands now (Simulation::flushCommands, Simulation.cpp:453-456). */
 int32_t ag2d_world_flush_commands(ag2d_world* world);
 
-/* ---- body constraints: ConstraintAPI (SimulationAPIs/ConstraintAPI.h:32-83) for springs, revolute joints and
- * motors ----
- * Springs and revolute joints join two bodies at body-local anchors (a soft distance constraint with a rest
- * length; a soft pin of both anchors together); a motor drives one body's angular velocity toward a target speed
- * within a torque limit. They are solved between the two halves of the step's integration, each kind in the
- * reference's dense order (Solving/SpringSolver.cpp, RevoluteJointSolver.cpp, MotorSolver.cpp scheduled by
+/* ---- body constraints: ConstraintAPI (SimulationAPIs/ConstraintAPI.h:32-105) ----
+ * Springs, revolute, prismatic and slider joints join two bodies at body-local anchors (a soft distance constraint
+ * with a rest length; a soft pin of both anchors together; a soft lock of the translation across body A's axis and
+ * of the relative angle, with optional hard limits along the axis; the same without the angle lock); a motor drives
+ * one body's angular velocity toward a target speed within a torque limit. They are solved between the two halves of the step's integration, each kind in the
+ * reference's dense order (Solving/SpringSolver.cpp, RevoluteJointSolver.cpp, PrismaticJointSolver.cpp,
+ * SliderJointSolver.cpp, MotorSolver.cpp scheduled by
  * ConstraintScheduler.cpp:9-80): the same results as the reference's single-threaded solve. Creation wakes the
  * bodies and returns a handle (AG2D_ERR_INVALID_ARG for a stale body handle: the reference's nullopt); destruction
  * and the setters are deferred to the next step's command flush, like the body commands, and wake the bodies; a
  * destroyed body takes its constraints with it. Per world: a batch engine's worlds take no constraints
  * (AG2D_ERR_UNSUPPORTED). */
-enum ag2d_joint_kind { AG2D_JOINT_SPRING = 0, AG2D_JOINT_REVOLUTE = 1, AG2D_JOINT_MOTOR = 2 };
+enum ag2d_joint_kind {   /* ConstraintType order */
+    AG2D_JOINT_SPRING = 0, AG2D_JOINT_REVOLUTE = 1, AG2D_JOINT_PRISMATIC = 2, AG2D_JOINT_SLIDER = 3, AG2D_JOINT_MOTOR = 4
+};
 typedef struct ag2d_joint_desc {
     int32_t kind;                    /* ag2d_joint_kind */
-    uint32_t pad;
+    int32_t enable_limit;            /* prismatic / slider: the axis limits are enforced */
     uint64_t body_a, body_b;         /* body handles (a motor uses body_a) */
-    float anchor_a_x, anchor_a_y;    /* body-local anchors (springs and revolute joints) */
+    float anchor_a_x, anchor_a_y;    /* body-local anchors (all but motors) */
     float anchor_b_x, anchor_b_y;
     float rest_length;               /* spring */
-    float stiffness, damping;        /* springs and revolute joints */
+    float stiffness, damping;        /* all but motors */
     float target_speed, max_torque;  /* motor */
-    float impulse;                   /* motor: accumulated impulse of the last step (read only) */
+    float axis_x, axis_y;            /* prismatic / slider: body A's local axis (normalised; zero length: (1, 0)) */
+    float lower_limit, upper_limit;  /* prismatic / slider: limits of the translation along the axis */
+    float reference_angle;           /* prismatic, read only: the relative angle locked at creation */
+    float impulse;                   /* motor, read only: accumulated impulse of the last step */
 } ag2d_joint_desc;
-/* Setter fields (ConstraintAPI::set*, ConstraintAPI.h:71-83): anchors take (a, b) as x, y; lengths, stiffness,
- * damping and max torque are clamped at 0 when applied. */
+/* Setter fields (ConstraintAPI::set* / reset*, ConstraintAPI.h:54-83): anchors and the axis take (a, b) as x, y (an
+ * axis is normalised, a zero-length one is dropped); limits take (a, b) in either order; enable_limit takes a != 0;
+ * the reference-angle reset locks the bodies' current relative angle; rest length, stiffness, damping and max
+ * torque are clamped at 0 when applied. */
 enum ag2d_joint_field {
     AG2D_JOINT_ANCHOR_A = 0, AG2D_JOINT_ANCHOR_B, AG2D_JOINT_REST_LENGTH, AG2D_JOINT_STIFFNESS, AG2D_JOINT_DAMPING,
-    AG2D_JOINT_TARGET_SPEED, AG2D_JOINT_MAX_TORQUE
+    AG2D_JOINT_TARGET_SPEED, AG2D_JOINT_MAX_TORQUE, AG2D_JOINT_AXIS_A, AG2D_JOINT_LIMITS, AG2D_JOINT_ENABLE_LIMIT,
+    AG2D_JOINT_RESET_REFERENCE_ANGLE
 };
 int32_t ag2d_world_create_joint(ag2d_world* world, const ag2d_joint_desc* desc, uint64_t* out_handle);
 int32_t ag2d_world_destroy_joint(ag2d_world* world, int32_t kind, uint64_t handle);

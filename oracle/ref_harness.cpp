@@ -507,7 +507,8 @@ extern "C"
     // Constraints (ConstraintAPI::createSpring / createRevoluteJoint / createMotor, SimulationAPIs/ConstraintAPI.h:
     // 32-36) between bodies given by handle slot; returns the constraint's handle slot or -1 (stale body).
     // kind 0 spring (p: anchorA xy, anchorB xy, rest length, stiffness, damping), 1 revolute joint (anchors,
-    // stiffness, damping), 4 motor (body A only; p: target speed, max torque).
+    // stiffness, damping), 2 prismatic and 3 slider joint (anchors, local axis xy, stiffness, damping, lower and
+    // upper limit, limit enabled), 4 motor (body A only; p: target speed, max torque).
     int64_t agref_create_joint(void* hp, int32_t kind, uint32_t slotA, uint32_t slotB, const float* p)
     {
         auto* h = static_cast<Harness*>(hp);
@@ -518,6 +519,20 @@ extern "C"
         {
         case 0: r = o.createSpring({a, b, Vec2(p[0], p[1]), Vec2(p[2], p[3]), p[4], p[5], p[6]}); break;
         case 1: r = o.createRevoluteJoint({a, b, Vec2(p[0], p[1]), Vec2(p[2], p[3]), p[4], p[5]}); break;
+        case 2: {
+            PrismaticJointConstraintSystem::CreateParams q{a, b, Vec2(p[0], p[1]), Vec2(p[2], p[3]), Vec2(p[4], p[5]),
+                                                           p[6], p[7]};
+            q.lowerLimit = p[8]; q.upperLimit = p[9]; q.enableLimit = p[10] != 0.0f;
+            r = o.createPrismaticJoint(q);
+            break;
+        }
+        case 3: {
+            SliderJointConstraintSystem::CreateParams q{a, b, Vec2(p[0], p[1]), Vec2(p[2], p[3]), Vec2(p[4], p[5]),
+                                                        p[6], p[7]};
+            q.lowerLimit = p[8]; q.upperLimit = p[9]; q.enableLimit = p[10] != 0.0f;
+            r = o.createSliderJoint(q);
+            break;
+        }
         case 4: r = o.createMotor({a, p[0], p[1]}); break;
         default: break;
         }

@@ -97,17 +97,18 @@ NO_COLLISION_EVENT_THRESHOLD = float(np.finfo(np.float32).max)
 
 
 # enum ag2d_joint_kind / ag2d_joint_field
-JOINT_SPRING, JOINT_REVOLUTE, JOINT_MOTOR = range(3)
+JOINT_SPRING, JOINT_REVOLUTE, JOINT_PRISMATIC, JOINT_SLIDER, JOINT_MOTOR = range(5)
 JOINT_ANCHOR_A, JOINT_ANCHOR_B, JOINT_REST_LENGTH, JOINT_STIFFNESS, JOINT_DAMPING, JOINT_TARGET_SPEED, \
-    JOINT_MAX_TORQUE = range(7)
+    JOINT_MAX_TORQUE, JOINT_AXIS_A, JOINT_LIMITS, JOINT_ENABLE_LIMIT, JOINT_RESET_REFERENCE_ANGLE = range(11)
 
 
 class JointDesc(ctypes.Structure):
     """ag2d_joint_desc: a spring, revolute joint or motor."""
-    _fields_ = [("kind", ctypes.c_int32), ("pad", ctypes.c_uint32), ("body_a", ctypes.c_uint64),
+    _fields_ = [("kind", ctypes.c_int32), ("enable_limit", ctypes.c_int32), ("body_a", ctypes.c_uint64),
                 ("body_b", ctypes.c_uint64)] + \
                [(n, ctypes.c_float) for n in ("anchor_a_x", "anchor_a_y", "anchor_b_x", "anchor_b_y", "rest_length",
-                                              "stiffness", "damping", "target_speed", "max_torque", "impulse")]
+                                              "stiffness", "damping", "target_speed", "max_torque", "axis_x",
+                                              "axis_y", "lower_limit", "upper_limit", "reference_angle", "impulse")]
 
 
 class Tuning(ctypes.Structure):
@@ -441,9 +442,11 @@ class World:
 
     # --- body constraints (ConstraintAPI, SimulationAPIs/ConstraintAPI.h:32-105) ---
     def create_joint(self, kind, body_a, body_b=0, anchor_a=(0.0, 0.0), anchor_b=(0.0, 0.0), rest_length=0.0,
-                     stiffness=0.0, damping=0.0, target_speed=0.0, max_torque=0.0) -> int:
-        d = JointDesc(kind, 0, body_a, body_b, anchor_a[0], anchor_a[1], anchor_b[0], anchor_b[1], rest_length,
-                      stiffness, damping, target_speed, max_torque, 0.0)
+                     stiffness=0.0, damping=0.0, target_speed=0.0, max_torque=0.0, axis=(1.0, 0.0),
+                     limits=(0.0, 0.0), enable_limit=False) -> int:
+        d = JointDesc(kind, 1 if enable_limit else 0, body_a, body_b, anchor_a[0], anchor_a[1], anchor_b[0],
+                      anchor_b[1], rest_length, stiffness, damping, target_speed, max_torque, axis[0], axis[1],
+                      limits[0], limits[1], 0.0, 0.0)
         out = ctypes.c_uint64()
         _check(lib.ag2d_world_create_joint(self.h, ctypes.byref(d), ctypes.byref(out)))
         return int(out.value)
@@ -466,7 +469,7 @@ class World:
     def joint(self, kind, handle) -> dict:
         d = JointDesc()
         _check(lib.ag2d_world_joint(self.h, kind, handle, ctypes.byref(d)))
-        return {n: getattr(d, n) for n, _ in JointDesc._fields_ if n != "pad"}
+        return {n: getattr(d, n) for n, _ in JointDesc._fields_}
 
     def joint_count(self, kind) -> int:
         n = ctypes.c_uint32()

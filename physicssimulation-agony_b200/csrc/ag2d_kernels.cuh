@@ -208,10 +208,11 @@ __global__ void k_circle_contacts(DeviceWorld w, float x, float y, float radius,
 __global__ void k_scatter_contacts(const uint32_t* flag, const uint32_t* offset, const float* dist, uint32_t n,
                                    uint32_t* list, float* listDist);
 
-// Body constraints (k_joints.cu): springs (kind 0), revolute joints (1) and motors (2), each kind's active
+// Body constraints (k_joints.cu): springs (kind 0), revolute (1), prismatic (2) and slider (3) joints and motors
+// (4), the reference's ConstraintType order, each kind's active
 // constraints in rec[k] grouped by level (level l: [levelStart[k][l], levelStart[k][l + 1])), solver data in
 // data[k], the motors' accumulated impulses by dense index in motorImpulse. One CTA of JOINT_THREADS threads.
-constexpr uint32_t JOINT_KINDS_DEVICE = 3;
+constexpr uint32_t JOINT_KINDS_DEVICE = 5;
 constexpr uint32_t JOINT_THREADS = 1024;
 struct JointLaunch {
     const JointRec* rec[JOINT_KINDS_DEVICE];

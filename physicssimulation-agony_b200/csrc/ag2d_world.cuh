@@ -78,25 +78,25 @@ struct ColliderEvent {
     float threshold;
 };
 
-// Body constraint on the device (springs, revolute joints, motors; SoA/Constraints/*), one per active constraint
-// in solving order: bodies, the constraint's dense index in its system, local anchors and parameters (spring: rest
-// length, stiffness, damping; revolute joint: stiffness, damping; motor: target speed, max torque).
+// Body constraint on the device (SoA/Constraints/*), one per active constraint in solving order: bodies, the
+// constraint's dense index in its system, flags (bit 0: the axis limit is enabled), local anchors and parameters.
+// Spring: p0 rest length, p1 stiffness, p2 damping. Revolute joint: p1 stiffness, p2 damping. Prismatic and slider
+// joints: p0, p1 the local axis of body A (unit), p2 stiffness, p3 damping, p4 lower limit, p5 upper limit,
+// p6 reference angle (prismatic). Motor: p0 target speed, p1 max torque.
 struct alignas(16) JointRec {
-    uint32_t bodyA, bodyB, index, pad;
+    uint32_t bodyA, bodyB, index, flags;
     float ax, ay, bx, by;
-    float p0, p1, p2, p3;
+    float p[8];
 };
-static_assert(sizeof(JointRec) == 48, "JointRec is 48 bytes");
+static_assert(sizeof(JointRec) == 64, "JointRec is 64 bytes");
 
-// Per-constraint solver data (the solvers' ConstraintData, Solving/*Solver.h). Spring: rotated anchors, direction,
-// inverse effective mass (0: skip), bias. Revolute joint: rotated anchors, bias, inverse effective mass matrix
-// (k11, k12, k22; all 0: skip). Motor: inverse inertia (0: skip), inertia, target speed, max impulse, impulse.
+// Per-constraint solver data (the solvers' ConstraintData, Solving/*Solver.h): rotated anchors, then per kind
+// the fields listed beside the kernel that fills them (k_joints.cu).
 struct alignas(16) JointData {
     float rAx, rAy, rBx, rBy;
-    float s0, s1, s2, s3;
-    float s4, s5, s6, s7;
+    float s[20];
 };
-static_assert(sizeof(JointData) == 48, "JointData is 48 bytes");
+static_assert(sizeof(JointData) == 96, "JointData is 96 bytes");
 
 // Per-constraint solver record (128 bytes), built from a Manifold in solving (colour) order: the fields of
 // BodyCollisionSolver's VelocityHotData, PositionHotData, VelocityConstraintData and FrictionData.

@@ -433,6 +433,26 @@ static DeviceInfo probe_device(int device)
     return dev;
 }
 
+// ConstraintSystemBase::normalizeAxis (ConstraintSystemBase.h:144-152): false for a (near) zero-length axis.
+static bool normalize_axis(float& x, float& y)
+{
+    const float lenSq = x * x + y * y;
+    if (!(lenSq > 1e-12f)) return false;
+    const float len = std::sqrt(lenSq);
+    x = x / len;
+    y = y / len;
+    return true;
+}
+
+// PrismaticJointConstraintSystem::computeReferenceAngle (PrismaticJointConstraintSystem.h:118-125).
+static float reference_angle(float rotA, float rotB)
+{
+    const float pi = 3.14159265358979323846f, twoPi = 2.0f * pi;
+    float a = rotB - rotA;
+    a -= twoPi * std::floor((a + pi) / twoPi);
+    return a;
+}
+
 // A deferred body command (ObjectManager::ObjectCommand, SimulationImpl/ObjectManager.h:45): queued by destroy and the
 // setters in call order, applied at the start of the next step (Simulation::update -> flushCommands,
 // Simulation.cpp:39; ObjectManager::applyCommand, ObjectManager.cpp:662-790). Stale handles are dropped.
@@ -483,7 +503,7 @@ struct ag2d_world {
         float a, b;
     };
     std::vector<JointCommand> jointCommands;
-    uint32_t jointActive[JOINT_KINDS] = {0, 0, 0}, jointLevels[JOINT_KINDS] = {0, 0, 0};
+    uint32_t jointActive[JOINT_KINDS] = {}, jointLevels[JOINT_KINDS] = {};
     std::vector<uint32_t> jointLevelHost[JOINT_KINDS];
     uint32_t nJointEdges = 0, motorsOnDevice = 0;
     bool jointsDirty = false;   // the device lists need a rebuild before the next step
@@ -1993,7 +2013,11 @@ struct ag2d_world {
         for (const JointSystem& js : objects.jointSystems) n += uint32_t(js.joints.size());
         return n;
     }
-    bool jointsActive() const { return jointActive[0] + jointActive[1] + jointActive[2] > 0; }
+    bool jointsActive() const
+    {
+        for (uint32_t k = 0; k < JOINT_KINDS; k++) if (jointActive[k]) return true;
+        return false;
+    }
     // The motors' accumulated impulses from the device into the host table (before the table is reordered or read).
     void pullMotorImpulses()
     {
@@ -2063,9 +2087,14 @@ struct ag2d_world {
                 JointRec r{};
                 r.bodyA = j.bodyA; r.bodyB = j.bodyB == NO_BODY ? j.bodyA : j.bodyB; r.index = i;
                 r.ax = j.anchorAx; r.ay = j.anchorAy; r.bx = j.anchorBx; r.by = j.anchorBy;
-                if (k == JOINT_SPRING) { r.p0 = j.restLength; r.p1 = j.stiffness; r.p2 = j.damping; }
-                else if (k == JOINT_REVOLUTE) { r.p1 = j.stiffness; r.p2 = j.damping; }
-                else { r.p0 = j.targetSpeed; r.p1 = j.maxTorque; }
+                if (k == JOINT_SPRING) { r.p[0] = j.restLength; r.p[1] = j.stiffness; r.p[2] = j.damping; }
+                else if (k == JOINT_REVOLUTE) { r.p[1] = j.stiffness; r.p[2] = j.damping; }
+                else if (k == JOINT_MOTOR) { r.p[0] = j.targetSpeed; r.p[1] = j.maxTorque; }
+                else {
+                    r.p[0] = j.axisX; r.p[1] = j.axisY; r.p[2] = j.stiffness; r.p[3] = j.damping;
+                    r.p[4] = j.lowerLimit; r.p[5] = j.upperLimit; r.p[6] = j.referenceAngle;
+                    r.flags = j.enableLimit ? 1u : 0u;
+                }
                 recs[fill[level[i - begin]]++] = r;
             }
             jointActive[k] = end - begin;
@@ -2521,6 +2550,17 @@ struct ag2d_world {
             case AG2D_JOINT_DAMPING: j.damping = std::fmax(0.0f, c.a); break;
             case AG2D_JOINT_TARGET_SPEED: j.targetSpeed = c.a; break;
             case AG2D_JOINT_MAX_TORQUE: j.maxTorque = std::fmax(0.0f, c.a); break;
+            case AG2D_JOINT_AXIS_A: {
+                float x = c.a, y = c.b;
+                if (normalize_axis(x, y)) { j.axisX = x; j.axisY = y; }
+                break;
+            }
+            case AG2D_JOINT_LIMITS: j.lowerLimit = std::fmin(c.a, c.b); j.upperLimit = std::fmax(c.a, c.b); break;
+            case AG2D_JOINT_ENABLE_LIMIT: j.enableLimit = c.a != 0.0f; break;
+            case AG2D_JOINT_RESET_REFERENCE_ANGLE:
+                if (j.bodyB != NO_BODY && j.bodyA < nBodies && j.bodyB < nBodies)
+                    j.referenceAngle = reference_angle(pos[j.bodyA].z, pos[j.bodyB].z);
+                break;
             default: break;
             }
         }
@@ -3168,6 +3208,22 @@ int32_t ag2d_world_create_joint(ag2d_world* world, const ag2d_joint_desc* d, uin
         j.anchorAx = d->anchor_a_x; j.anchorAy = d->anchor_a_y; j.anchorBx = d->anchor_b_x; j.anchorBy = d->anchor_b_y;
         j.restLength = d->rest_length; j.stiffness = d->stiffness; j.damping = d->damping;
         j.targetSpeed = d->target_speed; j.maxTorque = d->max_torque; j.impulse = 0.0f;
+        j.axisX = d->axis_x; j.axisY = d->axis_y;
+        if (!normalize_axis(j.axisX, j.axisY)) { j.axisX = 1.0f; j.axisY = 0.0f; }   // sanitizeAxis
+        j.lowerLimit = d->lower_limit; j.upperLimit = d->upper_limit; j.enableLimit = d->enable_limit != 0;
+        if (d->kind == AG2D_JOINT_PRISMATIC) {
+            // The bodies' rotations now: the host's before the first upload, else the device's.
+            float ra = o.bodies[a].rot, rb = o.bodies[b].rot;
+            if (!world->hostDirty) {
+                CK(cudaSetDevice(world->settings.device));
+                float4 pa, pb;
+                CK(cudaMemcpy(&pa, world->bpos.p + a, sizeof(float4), cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(&pb, world->bpos.p + b, sizeof(float4), cudaMemcpyDeviceToHost));
+                ra = pa.z;
+                rb = pb.z;
+            }
+            j.referenceAngle = reference_angle(ra, rb);
+        }
         // refreshConstraintGroup (ObjectManager.cpp:1207-1220): Inactive when no body has mass.
         const bool inactive = o.bodies[a].invMass == 0.0f && (single || o.bodies[b].invMass == 0.0f);
         const uint32_t i = js.create(j, inactive ? JGROUP_INACTIVE : JGROUP_ACTIVE);
@@ -3191,7 +3247,7 @@ int32_t ag2d_world_set_joint(ag2d_world* world, int32_t kind, uint64_t handle, i
 {
     return guarded([&] {
         joint_system(world, kind);
-        if (field < AG2D_JOINT_ANCHOR_A || field > AG2D_JOINT_MAX_TORQUE)
+        if (field < AG2D_JOINT_ANCHOR_A || field > AG2D_JOINT_RESET_REFERENCE_ANGLE)
             throw ApiError(AG2D_ERR_INVALID_ARG, "unknown constraint field");
         world->jointCommands.push_back(ag2d_world::JointCommand{kind, field, handle, a, b});
     });
@@ -3214,6 +3270,9 @@ int32_t ag2d_world_joint(ag2d_world* world, int32_t kind, uint64_t handle, ag2d_
         out->anchor_b_x = j.anchorBx; out->anchor_b_y = j.anchorBy;
         out->rest_length = j.restLength; out->stiffness = j.stiffness; out->damping = j.damping;
         out->target_speed = j.targetSpeed; out->max_torque = j.maxTorque; out->impulse = j.impulse;
+        out->axis_x = j.axisX; out->axis_y = j.axisY;
+        out->lower_limit = j.lowerLimit; out->upper_limit = j.upperLimit; out->enable_limit = j.enableLimit ? 1 : 0;
+        out->reference_angle = j.referenceAngle;
     });
 }
 

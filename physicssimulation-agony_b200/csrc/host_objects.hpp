@@ -57,12 +57,14 @@ struct Groups {
     }
 };
 
-// Constraints between bodies (SimulationImpl/ConstraintSystems/*, SoA/Constraints/*): springs, revolute joints and
-// motors. A system keeps its constraints in the reference's dense order, grouped [Inactive][Sleeping][Active]
+// Constraints between bodies (SimulationImpl/ConstraintSystems/*, SoA/Constraints/*): springs, revolute, prismatic
+// and slider joints, motors. A system keeps its constraints in the reference's dense order, grouped [Inactive][Sleeping][Active]
 // (ConstraintGroup, ConstraintSystemBase.h:22-24; Inactive: every body static), moved between groups by the same
 // boundary swaps (ObjectManager::moveConstraintToGroup, ObjectManager.cpp:1172-1205), with a handle table whose
 // freed slots are reused last-in first-out with the generation raised (HandleTable.h:30-90).
-enum JointKind : uint32_t { JOINT_SPRING = 0, JOINT_REVOLUTE = 1, JOINT_MOTOR = 2, JOINT_KINDS = 3 };
+enum JointKind : uint32_t {
+    JOINT_SPRING = 0, JOINT_REVOLUTE = 1, JOINT_PRISMATIC = 2, JOINT_SLIDER = 3, JOINT_MOTOR = 4, JOINT_KINDS = 5
+};
 enum JointGroup : uint32_t { JGROUP_INACTIVE = 0, JGROUP_SLEEPING = 1, JGROUP_ACTIVE = 2, JGROUP_UNUSED = 3 };
 constexpr uint32_t NO_BODY = 0xFFFFFFFFu;
 
@@ -71,6 +73,10 @@ struct HJoint {
     float anchorAx = 0, anchorAy = 0, anchorBx = 0, anchorBy = 0;   // body-local anchors
     float restLength = 0, stiffness = 0, damping = 0;               // spring (revolute: stiffness, damping)
     float targetSpeed = 0, maxTorque = 0, impulse = 0;              // motor; impulse: accumulated (warm start)
+    float axisX = 1, axisY = 0;                                       // prismatic / slider: body A's local axis
+    float referenceAngle = 0;                                         // prismatic: locked relative angle
+    float lowerLimit = 0, upperLimit = 0;                             // prismatic / slider: axis limits
+    bool enableLimit = false;
     uint32_t handleSlot = 0;
 };
 

@@ -2,10 +2,11 @@
 motors) against the reference engine making the same calls (oracle/ref_harness.cpp: agref_create_joint).
 
 - Free bodies (no colliders, no sleep): a pendulum chain of revolute joints hanging from a static body, a spring
-  ladder, motors driving some links. Every body's position, rotation and velocities equal the reference's bit for bit
+  ladder, a piston on a limited prismatic joint, a carriage on a limited slider joint, motors driving some links. Every body's position, rotation and velocities equal the reference's bit for bit
   after 240 steps, and so do the motors' accumulated impulses: the level schedule solves each kind in the
   reference's dense order.
-- A random constraint graph (2,000 bodies, 6,000 springs and revolute joints, 300 motors, some on static bodies):
+- A random constraint graph (2,000 bodies, 6,000 springs and revolute, prismatic and slider joints with and without
+  limits, 300 motors, some on static bodies):
   bit-exact after 60 steps; levels run in parallel with barriers between them.
 - The API: a stale body handle is refused; destroys and edits wait for the next step; destroying a body takes its
   constraints; constraints between static bodies are inactive; a constrained world cannot join a batch.
@@ -18,7 +19,8 @@ pytestmark = pytest.mark.gpu
 ag2d = pytest.importorskip("ag2d")
 from oracle import refapi  # noqa: E402
 
-REF_KIND = {ag2d.JOINT_SPRING: 0, ag2d.JOINT_REVOLUTE: 1, ag2d.JOINT_MOTOR: 4}
+REF_KIND = {ag2d.JOINT_SPRING: 0, ag2d.JOINT_REVOLUTE: 1, ag2d.JOINT_PRISMATIC: 2, ag2d.JOINT_SLIDER: 3,
+            ag2d.JOINT_MOTOR: 4}
 BODY_FIELDS = [(ag2d.BODY_COM_X, "comX"), (ag2d.BODY_COM_Y, "comY"), (ag2d.BODY_VEL_X, "velocityX"),
                (ag2d.BODY_VEL_Y, "velocityY"), (ag2d.BODY_ROTATION, "rotation"),
                (ag2d.BODY_ANGULAR_VELOCITY, "angularVelocity")]
@@ -56,18 +58,20 @@ class _Pair:
         return len(self.slots) - 1
 
     def joint(self, kind, a, b=None, anchor_a=(0.0, 0.0), anchor_b=(0.0, 0.0), rest=0.0, k=0.0, c=0.0, speed=0.0,
-              torque=0.0):
+              torque=0.0, axis=(1.0, 0.0), limits=(0.0, 0.0), enable_limit=False):
         if kind == ag2d.JOINT_SPRING:
             p = [*anchor_a, *anchor_b, rest, k, c]
         elif kind == ag2d.JOINT_REVOLUTE:
             p = [*anchor_a, *anchor_b, k, c]
+        elif kind in (ag2d.JOINT_PRISMATIC, ag2d.JOINT_SLIDER):
+            p = [*anchor_a, *anchor_b, *axis, k, c, *limits, 1.0 if enable_limit else 0.0]
         else:
             p = [speed, torque]
         slot = self.ref.body_slots   # create_body returns an index into it
         sb = slot[self.slots[b]] if b is not None else 0
         assert self.ref.create_joint(REF_KIND[kind], slot[self.slots[a]], sb, p) >= 0
         return self.w.create_joint(kind, self.handles[a], self.handles[b] if b is not None else 0, anchor_a,
-                                   anchor_b, rest, k, c, speed, torque)
+                                   anchor_b, rest, k, c, speed, torque, axis, limits, enable_limit)
 
     def step(self, n):
         self.ref.update(n)
@@ -115,8 +119,19 @@ def test_chain_ladder_and_motors_match_the_reference_bit_for_bit(pair):
     for a, b in zip(rails, rails2):
         pair.joint(ag2d.JOINT_SPRING, a, b, (0.0, -0.1), (0.0, 0.1), rest=2.0, k=800.0, c=10.0)
     pair.joint(ag2d.JOINT_SPRING, top, rails[3], (0.0, 0.0), (0.0, 0.2), rest=3.0, k=2000.0, c=30.0)
+    # A piston on a prismatic joint (limits hit while it falls) and a slider carriage on a tilted static rail.
+    base = pair.body(60.0, 12.0, mass=0.0, rotation=0.2)
+    piston = pair.body(60.5, 12.0, mass=1.5, inertia=0.3, rotation=0.5, w=1.0)
+    pair.joint(ag2d.JOINT_PRISMATIC, base, piston, (0.2, 0.0), (0.0, 0.1), k=2.0e4, c=40.0, axis=(1.0, 2.0),
+               limits=(-1.5, 0.5), enable_limit=True)
+    rail = pair.body(80.0, 12.0, mass=0.0, rotation=-0.4)
+    carriage = pair.body(81.0, 12.5, mass=2.0, inertia=0.5, vx=1.0)
+    pair.joint(ag2d.JOINT_SLIDER, rail, carriage, (0.0, 0.0), (0.0, -0.2), k=1.0e4, c=20.0, axis=(3.0, 0.5),
+               limits=(-4.0, 2.0), enable_limit=True)
+    tail = pair.body(82.0, 11.0, mass=0.5, inertia=0.1)
+    pair.joint(ag2d.JOINT_PRISMATIC, carriage, tail, (0.3, 0.0), (0.0, 0.0), k=5.0e3, c=5.0, axis=(0.0, 1.0))
     motors = [pair.joint(ag2d.JOINT_MOTOR, b, speed=2.0 - 0.5 * i, torque=5.0 + i) for i, b in
-              enumerate(links[::3] + rails2[::2])]
+              enumerate(links[::3] + rails2[::2] + [piston])]
     for _ in range(4):
         pair.step(60)
         pair.assert_bodies_equal()
@@ -142,15 +157,21 @@ def test_random_constraint_graph_matches_the_reference(pair):
     for j in range(6000):
         a, b = rng.choice(n, 2, replace=False).tolist()
         anchors = (tuple(rng.uniform(-0.5, 0.5, 2).tolist()), tuple(rng.uniform(-0.5, 0.5, 2).tolist()))
-        if j % 2 == 0:
+        if j % 4 == 0:
             pair.joint(ag2d.JOINT_SPRING, a, b, *anchors, rest=float(rng.uniform(0.5, 5.0)),
                        k=float(rng.uniform(10, 200)), c=float(rng.uniform(0.5, 5.0)))
-        else:
+        elif j % 4 == 1:
             pair.joint(ag2d.JOINT_REVOLUTE, a, b, *anchors, k=float(rng.uniform(50, 500)),
                        c=float(rng.uniform(1.0, 10.0)))
+        else:
+            lo = float(rng.uniform(-3, 0))
+            pair.joint(ag2d.JOINT_PRISMATIC if j % 4 == 2 else ag2d.JOINT_SLIDER, a, b, *anchors,
+                       k=float(rng.uniform(50, 500)), c=float(rng.uniform(1.0, 10.0)),
+                       axis=tuple(rng.normal(0, 1, 2).tolist()), limits=(lo, lo + float(rng.uniform(0.5, 4))),
+                       enable_limit=bool(j % 3))
     for b in rng.choice(n, 300, replace=False).tolist():
         pair.joint(ag2d.JOINT_MOTOR, b, speed=float(rng.uniform(-3, 3)), torque=float(rng.uniform(0.5, 20)))
-    assert pair.w.joint_count(ag2d.JOINT_SPRING) == 3000 and pair.w.joint_count(ag2d.JOINT_MOTOR) == 300
+    assert pair.w.joint_count(ag2d.JOINT_SLIDER) == 1500 and pair.w.joint_count(ag2d.JOINT_MOTOR) == 300
     for _ in range(3):
         pair.step(20)
         pair.assert_bodies_equal()
@@ -171,13 +192,21 @@ def test_constraint_api(pair):
     d = w.joint(ag2d.JOINT_SPRING, s)
     assert (d["rest_length"], d["stiffness"], d["damping"]) == (5.0, 100.0, 2.0)
     assert w.joint(ag2d.JOINT_SPRING, dead)["body_b"] == pair.handles[ground2]
+    pz = pair.joint(ag2d.JOINT_PRISMATIC, ground, a, axis=(3.0, 4.0), k=100.0, c=1.0)   # axis normalised
+    dp = w.joint(ag2d.JOINT_PRISMATIC, pz)
+    assert (dp["axis_x"], dp["axis_y"]) == (float(np.float32(3.0) / np.float32(5.0)),
+                                            float(np.float32(4.0) / np.float32(5.0)))
     pair.step(30)
     pair.assert_bodies_equal()
     # Deferred edits: nothing changes until the next step's flush; negative values are clamped at 0.
     w.set_joint(ag2d.JOINT_SPRING, s, ag2d.JOINT_REST_LENGTH, -3.0)
     w.set_joint(ag2d.JOINT_MOTOR, m, ag2d.JOINT_TARGET_SPEED, -2.0)
+    w.set_joint(ag2d.JOINT_PRISMATIC, pz, ag2d.JOINT_LIMITS, 2.0, -1.0)    # either order
+    w.set_joint(ag2d.JOINT_PRISMATIC, pz, ag2d.JOINT_AXIS_A, 0.0, 0.0)     # zero length: dropped
     assert w.joint(ag2d.JOINT_SPRING, s)["rest_length"] == 5.0
     w.step(1)
+    dp = w.joint(ag2d.JOINT_PRISMATIC, pz)
+    assert (dp["lower_limit"], dp["upper_limit"]) == (-1.0, 2.0) and dp["axis_y"] > 0.79
     assert w.joint(ag2d.JOINT_SPRING, s)["rest_length"] == 0.0
     assert w.joint(ag2d.JOINT_MOTOR, m)["target_speed"] == -2.0
     # Deferred destroy; a stale handle is dropped when the commands are applied.
@@ -192,6 +221,7 @@ def test_constraint_api(pair):
     w.destroy_body(pair.handles[b])
     w.step(1)
     assert w.joint_count(ag2d.JOINT_MOTOR) == 0 and w.joint_count(ag2d.JOINT_SPRING) == 2
+    assert w.joint_count(ag2d.JOINT_PRISMATIC) == 1
     # A constrained world cannot join a batch.
     with pytest.raises(ag2d.Ag2dError):
         ag2d.Batch([w])
