@@ -6,6 +6,8 @@
 //                                                                     getBodyCollisionData, getSimulationSettings
 //   PS_AGONY2D::ObjectAPI (ObjectAPI.h:14)      ag2d::ObjectAPI       createCircle/Box/Polygon (+ H variants),
 //                                                                     getBodyIndex, getBodies
+//   ConstraintAPI (ConstraintAPI.h:13)          ag2d::ConstraintAPI   create/destroy springs, revolute, prismatic
+//                                                                     and slider joints, motors; their setters
 //   Simulation collision callbacks              createCollisionCallback, destroyCollisionCallback,
 //   (Simulation.h:169-179)                      setColliderCollisionCallback, getCollisionEvents
 //   SimulationSettings (Simulation.h:50-76)     ag2d::SimulationSettings
@@ -125,6 +127,42 @@ struct CollisionEvent {
     Real impulse = 0;   // impact impulse: max over the contacts of approach speed x normal effective mass, pre-solve
     CollisionCallbackIndex callbackId = 0;
 };
+// Constraint creation parameters (SimulationImpl/ConstraintSystems/*ConstraintSystem.h: CreateParams), under the
+// reference's class names.
+struct SpringConstraintSystem {
+    struct CreateParams {
+        Handle bodyHandleA, bodyHandleB;
+        Vec2 localAnchorA, localAnchorB;
+        Real restLength = 0, stiffness = 0, damping = 0;
+    };
+};
+struct RevoluteJointConstraintSystem {
+    struct CreateParams {
+        Handle bodyHandleA, bodyHandleB;
+        Vec2 localAnchorA, localAnchorB;
+        Real stiffness = 0, damping = 0;
+    };
+};
+struct PrismaticJointConstraintSystem {
+    struct CreateParams {
+        Handle bodyHandleA, bodyHandleB;
+        Vec2 localAnchorA, localAnchorB;
+        Vec2 localAxisA{1, 0};
+        Real stiffness = 0, damping = 0;
+        Real lowerLimit = 0, upperLimit = 0;
+        bool enableLimit = false;
+    };
+};
+struct SliderJointConstraintSystem {
+    using CreateParams = PrismaticJointConstraintSystem::CreateParams;
+};
+struct MotorConstraintSystem {
+    struct CreateParams {
+        Handle bodyHandle;
+        Real targetSpeed = 0, maxTorque = 0;
+    };
+};
+
 class Simulation;
 using CollisionCallback = void (*)(const CollisionEvent& event, Simulation& simulation, void* userData);
 
@@ -395,6 +433,108 @@ private:
     ag2d_world* world;
 };
 
+// ConstraintAPI (SimulationAPIs/ConstraintAPI.h:13-105): creation returns a handle (nullopt for a stale body
+// handle); destroys and edits are deferred to the next step, as in the reference.
+class ConstraintAPI {
+public:
+    explicit ConstraintAPI(ag2d_world* w) : world(w) {}
+    ConstraintAPI(const ConstraintAPI&) = delete;
+    ConstraintAPI& operator=(const ConstraintAPI&) = delete;
+
+    std::optional<Handle> createSpring(const SpringConstraintSystem::CreateParams& p)
+    {
+        ag2d_joint_desc d = pair(AG2D_JOINT_SPRING, p.bodyHandleA, p.bodyHandleB, p.localAnchorA, p.localAnchorB);
+        d.rest_length = p.restLength; d.stiffness = p.stiffness; d.damping = p.damping;
+        return create(d);
+    }
+    std::optional<Handle> createRevoluteJoint(const RevoluteJointConstraintSystem::CreateParams& p)
+    {
+        ag2d_joint_desc d = pair(AG2D_JOINT_REVOLUTE, p.bodyHandleA, p.bodyHandleB, p.localAnchorA, p.localAnchorB);
+        d.stiffness = p.stiffness; d.damping = p.damping;
+        return create(d);
+    }
+    std::optional<Handle> createPrismaticJoint(const PrismaticJointConstraintSystem::CreateParams& p)
+    {
+        return create(axisJoint(AG2D_JOINT_PRISMATIC, p));
+    }
+    std::optional<Handle> createSliderJoint(const SliderJointConstraintSystem::CreateParams& p)
+    {
+        return create(axisJoint(AG2D_JOINT_SLIDER, p));
+    }
+    std::optional<Handle> createMotor(const MotorConstraintSystem::CreateParams& p)
+    {
+        ag2d_joint_desc d{};
+        d.kind = AG2D_JOINT_MOTOR;
+        d.body_a = p.bodyHandle.value;
+        d.target_speed = p.targetSpeed; d.max_torque = p.maxTorque;
+        return create(d);
+    }
+    void destroySpring(Handle h) { destroy(AG2D_JOINT_SPRING, h); }
+    void destroyRevoluteJoint(Handle h) { destroy(AG2D_JOINT_REVOLUTE, h); }
+    void destroyPrismaticJoint(Handle h) { destroy(AG2D_JOINT_PRISMATIC, h); }
+    void destroySliderJoint(Handle h) { destroy(AG2D_JOINT_SLIDER, h); }
+    void destroyMotor(Handle h) { destroy(AG2D_JOINT_MOTOR, h); }
+
+    void setSpringRestLength(Handle h, Real v) { set(AG2D_JOINT_SPRING, h, AG2D_JOINT_REST_LENGTH, v); }
+    void setSpringStiffness(Handle h, Real v) { set(AG2D_JOINT_SPRING, h, AG2D_JOINT_STIFFNESS, v); }
+    void setSpringDamping(Handle h, Real v) { set(AG2D_JOINT_SPRING, h, AG2D_JOINT_DAMPING, v); }
+    void setRevoluteJointStiffness(Handle h, Real v) { set(AG2D_JOINT_REVOLUTE, h, AG2D_JOINT_STIFFNESS, v); }
+    void setRevoluteJointDamping(Handle h, Real v) { set(AG2D_JOINT_REVOLUTE, h, AG2D_JOINT_DAMPING, v); }
+    void setPrismaticJointLimits(Handle h, Real lower, Real upper)
+    {
+        set(AG2D_JOINT_PRISMATIC, h, AG2D_JOINT_LIMITS, lower, upper);
+    }
+    void setPrismaticJointEnableLimit(Handle h, bool e) { set(AG2D_JOINT_PRISMATIC, h, AG2D_JOINT_ENABLE_LIMIT, e); }
+    void resetPrismaticJointReferenceAngle(Handle h) { set(AG2D_JOINT_PRISMATIC, h, AG2D_JOINT_RESET_REFERENCE_ANGLE, 0); }
+    void setSliderJointLimits(Handle h, Real lower, Real upper)
+    {
+        set(AG2D_JOINT_SLIDER, h, AG2D_JOINT_LIMITS, lower, upper);
+    }
+    void setSliderJointEnableLimit(Handle h, bool e) { set(AG2D_JOINT_SLIDER, h, AG2D_JOINT_ENABLE_LIMIT, e); }
+    void setMotorTargetSpeed(Handle h, Real v) { set(AG2D_JOINT_MOTOR, h, AG2D_JOINT_TARGET_SPEED, v); }
+    void setMotorMaxTorque(Handle h, Real v) { set(AG2D_JOINT_MOTOR, h, AG2D_JOINT_MAX_TORQUE, v); }
+
+    // The constraint as stored now (get*DataH); nullopt if stale. The motor's accumulated impulse is in 'impulse'.
+    std::optional<ag2d_joint_desc> getData(int32_t kind, Handle h) const
+    {
+        ag2d_joint_desc d{};
+        if (ag2d_world_joint(world, kind, h.value, &d) != AG2D_OK) return std::nullopt;
+        return d;
+    }
+
+private:
+    static ag2d_joint_desc pair(int32_t kind, Handle a, Handle b, Vec2 anchorA, Vec2 anchorB)
+    {
+        ag2d_joint_desc d{};
+        d.kind = kind;
+        d.body_a = a.value; d.body_b = b.value;
+        d.anchor_a_x = anchorA.x; d.anchor_a_y = anchorA.y; d.anchor_b_x = anchorB.x; d.anchor_b_y = anchorB.y;
+        return d;
+    }
+    static ag2d_joint_desc axisJoint(int32_t kind, const PrismaticJointConstraintSystem::CreateParams& p)
+    {
+        ag2d_joint_desc d = pair(kind, p.bodyHandleA, p.bodyHandleB, p.localAnchorA, p.localAnchorB);
+        d.axis_x = p.localAxisA.x; d.axis_y = p.localAxisA.y;
+        d.stiffness = p.stiffness; d.damping = p.damping;
+        d.lower_limit = p.lowerLimit; d.upper_limit = p.upperLimit; d.enable_limit = p.enableLimit ? 1 : 0;
+        return d;
+    }
+    std::optional<Handle> create(const ag2d_joint_desc& d)
+    {
+        uint64_t h = 0;
+        const int32_t rc = ag2d_world_create_joint(world, &d, &h);
+        if (rc == AG2D_ERR_INVALID_ARG) return std::nullopt;
+        detail::check(rc);
+        return Handle{h};
+    }
+    void destroy(int32_t kind, Handle h) { detail::check(ag2d_world_destroy_joint(world, kind, h.value)); }
+    void set(int32_t kind, Handle h, int32_t field, Real a, Real b = 0)
+    {
+        detail::check(ag2d_world_set_joint(world, kind, h.value, field, a, b));
+    }
+    ag2d_world* world;
+};
+
 class Simulation {
 public:
     explicit Simulation(const SimulationSettings& s = {}) : settings(s)
@@ -412,6 +552,7 @@ public:
         w.device = s.device;
         detail::check(ag2d_world_create(&w, &world));
         api = std::make_unique<ObjectAPI>(world);
+        constraintApi = std::make_unique<ConstraintAPI>(world);
     }
     ~Simulation() { ag2d_world_destroy(world); }
     Simulation(const Simulation&) = delete;
@@ -437,6 +578,8 @@ public:
     }
 
     ObjectAPI& objects() noexcept { return *api; }
+    // Simulation::constraints (Simulation.h:201-202).
+    ConstraintAPI& constraints() noexcept { return *constraintApi; }
     const ObjectAPI& objects() const noexcept { return *api; }
 
     // The manifolds of the last step (Simulation::getBodyCollisionData, Simulation.h:186), as host copies.
@@ -528,6 +671,7 @@ private:
     SimulationSettings settings;
     ag2d_world* world = nullptr;
     std::unique_ptr<ObjectAPI> api;
+    std::unique_ptr<ConstraintAPI> constraintApi;
     Real accumulator = 0;
     std::map<CollisionCallbackIndex, std::unique_ptr<CallbackEntry>> callbackEntries;
 };

@@ -91,6 +91,33 @@ int main()
         wheel.radius = 0.35f;
         if (!sim->objects().createCircleCollider(wheel)) return 12;
     }
+    // A swinging chain (ConstraintAPI): three links on revolute joints from a static hook, a motor on the last.
+    ag2d::BodyCreateParams hb;
+    hb.position = {14.0f, 14.0f};
+    const std::optional<ag2d::Handle> hook = sim->objects().createBodyH(hb);
+    if (!hook) return 16;
+    created++;
+    ag2d::Handle prevLink = *hook;
+    for (int k = 0; k < 3; k++) {
+        ag2d::BodyCreateParams lb;
+        lb.position = {15.0f + float(k), 14.0f};
+        lb.mass = 1.0f;
+        lb.inertia = 0.1f;
+        const std::optional<ag2d::Handle> link = sim->objects().createBodyH(lb);
+        if (!link) return 17;
+        created++;
+        ag2d::RevoluteJointConstraintSystem::CreateParams jp;
+        jp.bodyHandleA = prevLink;
+        jp.bodyHandleB = *link;
+        jp.localAnchorA = {k == 0 ? 0.0f : 0.5f, 0.0f};
+        jp.localAnchorB = {-0.5f, 0.0f};
+        jp.stiffness = 1.0e4f;
+        jp.damping = 20.0f;
+        if (!sim->constraints().createRevoluteJoint(jp)) return 18;
+        prevLink = *link;
+    }
+    if (!sim->constraints().createMotor({prevLink, 3.0f, 10.0f})) return 19;
+    if (sim->constraints().createMotor({ag2d::Handle{~0ull}, 1.0f, 1.0f})) return 20;   // stale body: nullopt
     ag2d::CircleColliderCreateParams orphan;
     orphan.bodyHandle = ag2d::Handle{~0ull};
     orphan.radius = 1.0f;
@@ -124,8 +151,8 @@ int main()
     sim->getBroadPhaseCollisionDetector().queryCollidersInShape(bp::AABBQuery({-1e6f, -1e6f, 1e6f, 1e6f}),
                                                                 bp::BvhTreeTypeFlag::All, all);
     // One collider per live body plus the dumbbell's two wheels, all inside the huge box; the destroyed body's
-    // collider is in no tree.
-    if (all.size() != bodies.getCount() - 1 + 2) {
+    // collider is in no tree, and the hook and the chain's three links have none.
+    if (all.size() != bodies.getCount() - 1 + 2 - 4) {
         std::printf("colliders found %zu, bodies %u\n", all.size(), bodies.getCount());
         return 6;
     }

@@ -226,3 +226,65 @@ def test_constraint_api(pair):
     with pytest.raises(ag2d.Ag2dError):
         ag2d.Batch([w])
     assert w.counters()["status"] == 0
+
+
+def test_constrained_bodies_sleep_and_wake_as_one_island(pair):
+    """A chain on revolute joints lying on the ground (circle colliders too small to touch each other) settles; its
+    links fall asleep in the same step, as one island with the joints as links, and a ball dropped on one end wakes
+    all of them in the same step. Both engines settle the chain to the same heights within 5 mm."""
+    w, ref = pair.w, pair.ref
+    rm, wm = ref.add_material(0.0, 0.6, 0.5), w.add_material(0.0, 0.6, 0.5)   # no bounce, friction
+    ground = pair.body(0.0, -1.0, mass=0.0)
+    ref.add_collider(pair.slots[ground], 1, material=rm, width=60.0, height=2.0)
+    w.add_collider(pair.handles[ground], 1, material=wm, width=60.0, height=2.0)
+    links = []
+    for k in range(6):
+        b = pair.body(-3.0 + k, 0.3, mass=1.0, inertia=0.05)
+        ref.add_collider(pair.slots[b], 0, material=rm, radius=0.3)
+        w.add_collider(pair.handles[b], 0, material=wm, radius=0.3)
+        if links:
+            pair.joint(ag2d.JOINT_REVOLUTE, links[-1], b, (0.5, 0.0), (-0.5, 0.0), k=1.0e4, c=20.0)
+        links.append(b)
+    w_sleep = pair.w   # the pair's worlds never sleep; this test needs a world that does
+    w2 = ag2d.World(dt=_Scene.dt, gravity=_Scene.gravity)
+    m2 = w2.add_material(0.0, 0.6, 0.5)
+    g2 = w2.create_body(0.0, -1.0, mass=0.0, inertia=0.0)
+    w2.add_collider(g2, 1, material=m2, width=60.0, height=2.0)
+    hs = []
+    for k in range(6):
+        h = w2.create_body(-3.0 + k, 0.3, mass=1.0, inertia=0.05)
+        w2.add_collider(h, 0, material=m2, radius=0.3)
+        if hs:
+            w2.create_joint(ag2d.JOINT_REVOLUTE, hs[-1], h, (0.5, 0.0), (-0.5, 0.0), 0.0, 1.0e4, 20.0)
+        hs.append(h)
+    idx = [w2.body_index(h) for h in hs]
+    slept_at = None
+    for step in range(1, 601):
+        w2.step(1)
+        st = w2.read(ag2d.BODY_STATE)[idx]
+        assert len(set(st.tolist())) == 1, (step, st)   # one island: all asleep or all awake
+        if st[0] == 1:
+            slept_at = step
+            break
+    assert slept_at is not None, "the chain never fell asleep"
+    ball = w2.create_body(-3.0, 3.0, vy=-4.0, mass=2.0, inertia=0.1)
+    w2.add_collider(ball, 0, material=m2, radius=0.3)
+    woke = False
+    for _ in range(120):
+        w2.step(1)
+        st = w2.read(ag2d.BODY_STATE)[idx]
+        assert len(set(st.tolist())) == 1, st
+        if st[0] == 2:
+            woke = True
+            break
+    assert woke, "the ball did not wake the chain"
+    assert w2.counters()["status"] == 0
+    w2.close()
+    # The never-sleeping pair settles to the reference's heights.
+    del w_sleep
+    pair.step(300)
+    ref.dump_state("s.")
+    cy = w.read(ag2d.BODY_COM_Y)
+    ry = ref.blob("s.body.comY")
+    for b in links:
+        assert abs(float(cy[w.body_index(pair.handles[b])]) - float(ry[ref.body_index(pair.slots[b])])) < 5e-3
