@@ -538,6 +538,36 @@ extern "C"
         }
         return r ? int64_t(r->slot) : -1;
     }
+    // A constraint system's dense order as handles (slot, generation) and its group starts (Inactive, Sleeping,
+    // Active, end): ConstraintAPI::get*Handle over every dense index. Returns the count.
+    uint32_t agref_joint_order(void* hp, int32_t kind, uint32_t* slot, uint32_t* gen, uint32_t* starts, uint32_t cap)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        IConstraintSystem* sys = h->sim.constraintSystems[size_t(kind)];
+        const uint32_t n = uint32_t(sys->getCount());
+        for (uint32_t i = 0; i < n && i < cap; i++)
+        {
+            Handle hd{};
+            switch (kind)
+            {
+            case 0: hd = h->sim.springConstraintSystem.handleAt(i); break;
+            case 1: hd = h->sim.jointConstraintSystem.handleAt(i); break;
+            case 2: hd = h->sim.prismaticJointConstraintSystem.handleAt(i); break;
+            case 3: hd = h->sim.sliderJointConstraintSystem.handleAt(i); break;
+            default: hd = h->sim.motorConstraintSystem.handleAt(i); break;
+            }
+            slot[i] = hd.slot;
+            gen[i] = hd.generation;
+        }
+        for (int g = 0; g < 4; g++) starts[g] = sys->groupStarts[g];
+        return n;
+    }
+    // Deferred constraint destroy (ConstraintAPI::destroy*, applied at the next flush).
+    void agref_destroy_joint(void* hp, int32_t kind, uint32_t slot, uint32_t gen)
+    {
+        static_cast<Harness*>(hp)->sim.objectManager.destroyConstraint(ConstraintType(kind), Handle{slot, gen});
+    }
+
     // The motors' accumulated impulses and body handle slots in dense order (MotorSoA).
     uint32_t agref_motor_impulses(void* hp, float* impulse, uint32_t* bodySlot, uint32_t cap)
     {

@@ -88,6 +88,9 @@ def lib():
         L.agref_fastcossin.argtypes = [vp, vp, vp, ctypes.c_uint64]
         L.agref_create_joint.restype = i64
         L.agref_create_joint.argtypes = [vp, i32, u32, u32, vp]
+        L.agref_joint_order.restype = u32
+        L.agref_joint_order.argtypes = [vp, i32, vp, vp, vp, u32]
+        L.agref_destroy_joint.argtypes = [vp, i32, u32, u32]
         L.agref_motor_impulses.restype = u32
         L.agref_motor_impulses.argtypes = [vp, vp, vp, u32]
         L.agref_create_event_callback.restype = i32
@@ -264,6 +267,18 @@ class RefSim:
         """A spring (0), revolute joint (1) or motor (4, body a) between bodies given by handle slot."""
         p = np.ascontiguousarray(params, dtype=np.float32)
         return int(lib().agref_create_joint(self.h, kind, a, b, p.ctypes.data))
+
+    def joint_order(self, kind: int):
+        """(handle slots, generations, group starts) of a constraint system in dense order."""
+        slot = np.zeros(65536, np.uint32)
+        gen = np.zeros(65536, np.uint32)
+        starts = np.zeros(4, np.uint32)
+        n = int(lib().agref_joint_order(self.h, kind, slot.ctypes.data, gen.ctypes.data, starts.ctypes.data,
+                                        slot.size))
+        return slot[:n].copy(), gen[:n].copy(), starts
+
+    def destroy_joint(self, kind: int, slot: int, gen: int):
+        lib().agref_destroy_joint(self.h, kind, slot, gen)
 
     def motor_impulses(self):
         """(accumulated impulses, body handle slots) of the motors in dense order."""

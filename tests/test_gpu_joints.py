@@ -288,3 +288,34 @@ def test_constrained_bodies_sleep_and_wake_as_one_island(pair):
     ry = ref.blob("s.body.comY")
     for b in links:
         assert abs(float(cy[w.body_index(pair.handles[b])]) - float(ry[ref.body_index(pair.slots[b])])) < 5e-3
+
+
+def test_constraint_dense_order_and_handles_match_the_reference(pair):
+    """The host's constraint tables follow the reference's: the dense order after group moves (a constraint between
+    static bodies goes to the inactive group in front, by boundary swaps), handles (slot and generation) and the
+    reuse of a destroyed constraint's slot (last freed first, generation raised)."""
+    w, ref = pair.w, pair.ref
+    statics = [pair.body(float(i), 0.0, mass=0.0) for i in range(3)]
+    movers = [pair.body(float(i), 5.0) for i in range(6)]
+
+    def same_order():
+        slots, gens, _ = ref.joint_order(0)
+        ours = [w.joint_handle(ag2d.JOINT_SPRING, i) for i in range(w.joint_count(ag2d.JOINT_SPRING))]
+        assert [h & 0xFFFFFFFF for h in ours] == slots.tolist()
+        assert [h >> 32 for h in ours] == gens.tolist()
+
+    plan = [(statics[0], movers[0]), (statics[0], statics[1]), (movers[1], movers[2]), (statics[1], statics[2]),
+            (movers[3], statics[2]), (statics[2], statics[0]), (movers[4], movers[5])]
+    hs = [pair.joint(ag2d.JOINT_SPRING, a, b, rest=1.0, k=10.0, c=1.0) for a, b in plan]
+    same_order()
+    for h in (hs[2], hs[1], hs[5]):   # active, inactive, inactive
+        w.destroy_joint(ag2d.JOINT_SPRING, h)
+        ref.destroy_joint(0, h & 0xFFFFFFFF, h >> 32)
+    pair.step(1)
+    same_order()
+    more = [pair.joint(ag2d.JOINT_SPRING, a, b, rest=1.0, k=10.0, c=1.0)
+            for a, b in ((statics[1], statics[0]), (movers[2], movers[0]), (movers[5], statics[1]))]
+    assert [h & 0xFFFFFFFF for h in more] == [hs[5] & 0xFFFFFFFF, hs[1] & 0xFFFFFFFF, hs[2] & 0xFFFFFFFF]
+    same_order()
+    pair.step(30)
+    pair.assert_bodies_equal()
