@@ -436,6 +436,9 @@ int32_t ag2d_batch_destroy(ag2d_batch* batch);
  * No reference counterpart: the reference keeps its state in host memory and has no save / load of a Simulation. */
 int32_t ag2d_batch_save(ag2d_batch* batch, void* dst, uint64_t capacity_bytes, uint64_t* out_bytes);
 int32_t ag2d_batch_restore(const void* src, uint64_t bytes, int32_t device, ag2d_batch** out_batch);
+/* Loads a checkpoint into an existing batch (same settings), reusing its device buffers where they are large
+ * enough: the upload of a resident engine (a server between jobs), without allocating. */
+int32_t ag2d_batch_load(ag2d_batch* batch, const void* src, uint64_t bytes);
 
 /* ---- request server: world rollouts served from one resident, continuously repacked batch ----
  * No counterpart in the reference (it steps one Simulation per caller). A server owns one device batch and a host

@@ -214,6 +214,7 @@ def _load():
     L.ag2d_host_free.argtypes = [vp]
     L.ag2d_batch_save.argtypes = [vp, vp, u64, ctypes.POINTER(u64)]
     L.ag2d_batch_restore.argtypes = [vp, u64, i32, ctypes.POINTER(vp)]
+    L.ag2d_batch_load.argtypes = [vp, vp, u64]
     L.ag2d_world_run_phase.argtypes = [vp, i32]
     L.ag2d_world_set_profiling.argtypes = [vp, i32]
     L.ag2d_world_autotune.argtypes = [vp, i32, ctypes.POINTER(Tuning)]
@@ -752,6 +753,11 @@ class Batch:
         b = cls.__new__(cls)
         b._adopt(h)
         return b
+
+    def load(self, blob: np.ndarray):
+        """Replaces this batch's state by a checkpoint (same settings), reusing its device buffers."""
+        ptr, nbytes = _out_bytes(blob)
+        _check(lib.ag2d_batch_load(self.h, ptr, nbytes))
 
     def save(self, out: np.ndarray = None) -> np.ndarray:
         """Checkpoint of the whole batch as a uint8 array (page-locked unless `out` is given)."""

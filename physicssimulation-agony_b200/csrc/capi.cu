@@ -4181,25 +4181,32 @@ int32_t ag2d_batch_save(ag2d_batch* batch, void* dst, uint64_t cap, uint64_t* ou
     });
 }
 
+// The header of a checkpoint blob, checked against its size and section table.
+static CkptHeader checked_checkpoint(const void* src, uint64_t bytes)
+{
+    CkptHeader h;
+    if (bytes < sizeof(h)) throw ApiError(AG2D_ERR_INVALID_ARG, "not a checkpoint (too short)");
+    std::memcpy(&h, src, sizeof(h));
+    if (std::memcmp(h.magic, CKPT_MAGIC, sizeof(h.magic)) != 0 || h.version != CKPT_VERSION ||
+        h.headerBytes != sizeof(CkptHeader))
+        throw ApiError(AG2D_ERR_INVALID_ARG, "not a checkpoint of this library version");
+    if (h.totalBytes > bytes) throw ApiError(AG2D_ERR_INVALID_ARG, "checkpoint truncated");
+    for (uint32_t k = 0; k < NCK; k++)
+        if (h.off[k] > h.totalBytes || h.len[k] > h.totalBytes - h.off[k])
+            throw ApiError(AG2D_ERR_INVALID_ARG, "checkpoint section out of range");
+    if (h.len[CK_WBODY] != (uint64_t(std::max<uint32_t>(h.nWorlds, 1)) + 1) * 4 ||
+        h.len[CK_WCOL] != h.len[CK_WBODY] || h.len[CK_VEL] != uint64_t(h.nBodies) * 16 ||
+        h.len[CK_CBODY] != uint64_t(h.nColliders) * 4 || h.len[CK_ISLE] != uint64_t(h.nIsle) * sizeof(Manifold) ||
+        h.len[CK_ISLEID] != uint64_t(h.nIsle) * 4 || h.len[CK_PREV] != uint64_t(h.nPrev) * sizeof(Manifold))
+        throw ApiError(AG2D_ERR_INVALID_ARG, "checkpoint sizes inconsistent");
+    return h;
+}
+
 int32_t ag2d_batch_restore(const void* src, uint64_t bytes, int32_t device, ag2d_batch** out)
 {
     return guarded([&] {
         if (!src || !out) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
-        CkptHeader h;
-        if (bytes < sizeof(h)) throw ApiError(AG2D_ERR_INVALID_ARG, "not a checkpoint (too short)");
-        std::memcpy(&h, src, sizeof(h));
-        if (std::memcmp(h.magic, CKPT_MAGIC, sizeof(h.magic)) != 0 || h.version != CKPT_VERSION ||
-            h.headerBytes != sizeof(CkptHeader))
-            throw ApiError(AG2D_ERR_INVALID_ARG, "not a checkpoint of this library version");
-        if (h.totalBytes > bytes) throw ApiError(AG2D_ERR_INVALID_ARG, "checkpoint truncated");
-        for (uint32_t k = 0; k < NCK; k++)
-            if (h.off[k] > h.totalBytes || h.len[k] > h.totalBytes - h.off[k])
-                throw ApiError(AG2D_ERR_INVALID_ARG, "checkpoint section out of range");
-        if (h.len[CK_WBODY] != (uint64_t(std::max<uint32_t>(h.nWorlds, 1)) + 1) * 4 ||
-            h.len[CK_WCOL] != h.len[CK_WBODY] || h.len[CK_VEL] != uint64_t(h.nBodies) * 16 ||
-            h.len[CK_CBODY] != uint64_t(h.nColliders) * 4 || h.len[CK_ISLE] != uint64_t(h.nIsle) * sizeof(Manifold) ||
-            h.len[CK_ISLEID] != uint64_t(h.nIsle) * 4 || h.len[CK_PREV] != uint64_t(h.nPrev) * sizeof(Manifold))
-            throw ApiError(AG2D_ERR_INVALID_ARG, "checkpoint sizes inconsistent");
+        const CkptHeader h = checked_checkpoint(src, bytes);
         ag2d_world_settings st = h.settings;
         if (device >= 0) st.device = device;
         std::unique_ptr<ag2d_batch> b(new ag2d_batch());
@@ -4209,6 +4216,22 @@ int32_t ag2d_batch_restore(const void* src, uint64_t bytes, int32_t device, ag2d
         CK(cudaSetDevice(st.device));
         b->engine->restoreCheckpoint(h, static_cast<const uint8_t*>(src));
         *out = b.release();
+    });
+}
+
+int32_t ag2d_batch_load(ag2d_batch* batch, const void* src, uint64_t bytes)
+{
+    return guarded([&] {
+        if (!batch || !src) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        const CkptHeader h = checked_checkpoint(src, bytes);
+        ag2d_world& e = *batch->engine;
+        ag2d_world_settings st = h.settings;
+        st.device = e.settings.device;
+        if (!same_settings(st, e.settings))
+            throw ApiError(AG2D_ERR_INVALID_ARG, "the checkpoint's settings differ from the batch's");
+        CK(cudaSetDevice(e.settings.device));
+        batch->worlds = std::max<uint32_t>(h.nWorlds, 1);
+        e.restoreCheckpoint(h, static_cast<const uint8_t*>(src));
     });
 }
 

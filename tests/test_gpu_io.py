@@ -124,3 +124,24 @@ def test_checkpoint_restore_steps_on_bit_exact(pinned):
         ag2d.Batch.restore(bad)
     with pytest.raises(ag2d.Ag2dError):
         ag2d.Batch.restore(blob[:blob.nbytes // 2])
+
+
+def test_checkpoint_loaded_into_a_running_batch_steps_on_bit_exact():
+    """ag2d_batch_load: a batch that has run on loads another state of the same worlds and steps on exactly as the
+    batch the checkpoint came from, without allocating device memory when its buffers are large enough."""
+    batch = ag2d.Batch(_worlds(seed=34))
+    batch.step(150)
+    blob = batch.save()
+    other = ag2d.Batch.restore(blob)
+    other.step(37)                  # a different state, buffers warm
+    allocs = ag2d.device_allocs()
+    other.load(blob)
+    assert ag2d.device_allocs() == allocs
+    batch.step(40)
+    other.step(40)
+    for k in range(batch.n_worlds):
+        for f in BODY_FIELDS + COL_FIELDS:
+            assert np.array_equal(_bits(other.read(k, f)), _bits(batch.read(k, f))), (k, f)
+        mg, mw = other.read(k, ag2d.PREV_MANIFOLDS), batch.read(k, ag2d.PREV_MANIFOLDS)
+        assert np.array_equal(mg.view(np.uint8), mw.view(np.uint8)), k
+    assert other.counters()["status"] == 0
