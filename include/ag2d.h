@@ -260,8 +260,9 @@ int32_t ag2d_world_flush_commands(ag2d_world* world);
  * ConstraintScheduler.cpp:9-80): the same results as the reference's single-threaded solve. Creation wakes the
  * bodies and returns a handle (AG2D_ERR_INVALID_ARG for a stale body handle: the reference's nullopt); destruction
  * and the setters are deferred to the next step's command flush, like the body commands, and wake the bodies; a
- * destroyed body takes its constraints with it. Per world: a batch engine's worlds take no constraints
- * (AG2D_ERR_UNSUPPORTED). */
+ * destroyed body takes its constraints with it. These calls are per world (a batch's engine returns
+ * AG2D_ERR_UNSUPPORTED); worlds with constraints can form a batch (each steps as alone), but not join a server or
+ * a checkpoint. */
 enum ag2d_joint_kind {   /* ConstraintType order */
     AG2D_JOINT_SPRING = 0, AG2D_JOINT_REVOLUTE = 1, AG2D_JOINT_PRISMATIC = 2, AG2D_JOINT_SLIDER = 3, AG2D_JOINT_MOTOR = 4
 };

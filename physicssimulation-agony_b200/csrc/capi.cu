@@ -2311,10 +2311,10 @@ struct ag2d_world {
         if (!islandsLinked) {
             k_island_init<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p);
             k_island_union<<<gridFor(manifoldCap), 256, 0, s>>>(w, manifolds.p, nManifolds.p, ufParent.p);
-            if (nJointEdges) {
-                k_island_union_edges<<<gridFor(nJointEdges), 256, 0, s>>>(w, jointEdges.p, nJointEdges, ufParent.p);
-                launches++;
-            }
+        }
+        if (nJointEdges) {   // after the teams' links too: union-find links in any order
+            k_island_union_edges<<<gridFor(nJointEdges), 256, 0, s>>>(w, jointEdges.p, nJointEdges, ufParent.p);
+            launches++;
         }
         islandsLinked = false;
         k_island_quiet<<<gridFor(nBodies), 256, 0, s>>>(w, ufParent.p, ufFlag.p, settings.dt, settings.sleep_speed,
@@ -4001,8 +4001,6 @@ int32_t ag2d_batch_create(ag2d_world* const* worlds, uint32_t count, ag2d_batch*
         if (!out || !worlds || count == 0) throw ApiError(AG2D_ERR_INVALID_ARG, "a batch needs at least one world");
         for (uint32_t k = 0; k < count; k++) {
             if (!worlds[k]) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
-            if (worlds[k]->jointTotal())
-                throw ApiError(AG2D_ERR_UNSUPPORTED, "a world with body constraints cannot join a batch");
             if (!same_settings(worlds[k]->settings, worlds[0]->settings))
                 throw ApiError(AG2D_ERR_INVALID_ARG, "worlds of a batch must share their step settings");
         }
@@ -4054,6 +4052,34 @@ int32_t ag2d_batch_create(ag2d_world* const* worlds, uint32_t count, ag2d_batch*
         }
         CK(cudaMemcpyAsync(e.nIsle.p, &ni, sizeof(uint32_t), cudaMemcpyHostToDevice, e.stream));
         e.isleUpper = ni;
+        // Body constraints, world after world within each group (so each world's active constraints keep their
+        // order), bodies shifted to the batch's indices; the engine owns new handles.
+        for (uint32_t kind = 0; kind < JOINT_KINDS; kind++) {
+            JointSystem& dst = e.objects.jointSystems[kind];
+            for (uint32_t k = 0; k < count; k++) {
+                CK(cudaSetDevice(worlds[k]->settings.device));
+                if (kind == JOINT_MOTOR) worlds[k]->pullMotorImpulses();
+            }
+            CK(cudaSetDevice(e.settings.device));
+            for (uint32_t g = 0; g < 3; g++) {
+                for (uint32_t k = 0; k < count; k++) {
+                    const JointSystem& js = worlds[k]->objects.jointSystems[kind];
+                    for (uint32_t i = js.starts[g]; i < js.starts[g + 1]; i++) {
+                        HJoint j = js.joints[i];
+                        j.bodyA += bodyStart[k];
+                        if (j.bodyB != NO_BODY) j.bodyB += bodyStart[k];
+                        j.handleSlot = uint32_t(dst.joints.size());
+                        dst.slotIndex.push_back(j.handleSlot);
+                        dst.slotGeneration.push_back(0);
+                        dst.joints.push_back(j);
+                    }
+                }
+                dst.starts[g + 1] = uint32_t(dst.joints.size());
+            }
+            dst.starts[JGROUP_UNUSED] = uint32_t(dst.joints.size());
+            dst.iterations = worlds[0]->objects.jointSystems[kind].iterations;
+        }
+        e.jointsDirty = e.jointTotal() > 0;
         CK(cudaStreamSynchronize(e.stream));
         *out = b.release();
     });
@@ -4172,6 +4198,7 @@ int32_t ag2d_batch_save(ag2d_batch* batch, void* dst, uint64_t cap, uint64_t* ou
     return guarded([&] {
         if (!batch) throw ApiError(AG2D_ERR_INVALID_ARG, "null batch");
         ag2d_world& e = *batch->engine;
+        if (e.jointTotal()) throw ApiError(AG2D_ERR_UNSUPPORTED, "checkpoints hold no body constraints");
         CK(cudaSetDevice(e.settings.device));
         const CkptHeader h = e.checkpointLayout();
         if (out_bytes) *out_bytes = h.totalBytes;

@@ -9,7 +9,8 @@ motors) against the reference engine making the same calls (oracle/ref_harness.c
   limits, 300 motors, some on static bodies):
   bit-exact after 60 steps; levels run in parallel with barriers between them.
 - The API: a stale body handle is refused; destroys and edits wait for the next step; destroying a body takes its
-  constraints; constraints between static bodies are inactive; a constrained world cannot join a batch.
+  constraints; constraints between static bodies are inactive; a batch's engine takes no constraint calls.
+- Jointed worlds in one batch step exactly as each world alone.
 """
 import numpy as np
 import pytest
@@ -222,9 +223,10 @@ def test_constraint_api(pair):
     w.step(1)
     assert w.joint_count(ag2d.JOINT_MOTOR) == 0 and w.joint_count(ag2d.JOINT_SPRING) == 2
     assert w.joint_count(ag2d.JOINT_PRISMATIC) == 1
-    # A constrained world cannot join a batch.
+    # The constraint API is per world: a batch's engine takes none.
+    batch = ag2d.Batch([w])
     with pytest.raises(ag2d.Ag2dError):
-        ag2d.Batch([w])
+        batch.engine.create_joint(ag2d.JOINT_MOTOR, pair.handles[a], target_speed=1.0, max_torque=1.0)
     assert w.counters()["status"] == 0
 
 
@@ -319,3 +321,48 @@ def test_constraint_dense_order_and_handles_match_the_reference(pair):
     same_order()
     pair.step(30)
     pair.assert_bodies_equal()
+
+
+def _jointed_world(seed):
+    """A ground box, a pile of boxes and a few jointed contraptions (chain, ladder, piston, motorised wheel)."""
+    rng = np.random.default_rng(seed)
+    w = ag2d.World(dt=_Scene.dt, gravity=_Scene.gravity)
+    mat = w.add_material(0.1, 0.6, 0.5)
+    g = w.create_body(0.0, -1.0, mass=0.0, inertia=0.0)
+    w.add_collider(g, 1, material=mat, width=80.0, height=2.0)
+    for i in range(int(rng.integers(10, 40))):
+        b = w.create_body(float(rng.uniform(-20, 20)), float(rng.uniform(1, 15)), mass=1.0, inertia=0.2)
+        w.add_collider(b, 1, material=mat, width=0.8, height=0.8)
+    hook = w.create_body(float(rng.uniform(-10, 10)), 20.0, mass=0.0, inertia=0.0)
+    prev = hook
+    for k in range(int(rng.integers(3, 9))):
+        b = w.create_body(w.read(ag2d.BODY_COM_X)[w.body_index(hook)] + 1.0 + k, 20.0, mass=1.0, inertia=0.1)
+        w.create_joint(ag2d.JOINT_REVOLUTE, prev, b, (0.5, 0.0) if prev != hook else (0.0, 0.0), (-0.5, 0.0), 0.0,
+                       2.0e4, 30.0)
+        prev = b
+    w.create_joint(ag2d.JOINT_MOTOR, prev, 0, target_speed=float(rng.uniform(-3, 3)), max_torque=8.0)
+    a = w.create_body(-25.0, 6.0, mass=2.0, inertia=0.5)
+    b = w.create_body(-23.0, 6.0, mass=1.0, inertia=0.3)
+    w.add_collider(a, 0, material=mat, radius=0.5)
+    w.add_collider(b, 0, material=mat, radius=0.5)
+    w.create_joint(ag2d.JOINT_SPRING, a, b, (0.2, 0.0), (-0.2, 0.0), 1.8, 400.0, 5.0)
+    w.create_joint(ag2d.JOINT_SLIDER, g, a, (-25.0, 1.0), (0.0, 0.0), 0.0, 5.0e3, 20.0, axis=(0.0, 1.0),
+                   limits=(2.0, 8.0), enable_limit=True)
+    w.create_joint(ag2d.JOINT_PRISMATIC, a, b, (0.0, 0.0), (0.0, 0.0), 0.0, 3.0e3, 10.0, axis=(1.0, 0.2))
+    return w
+
+
+def test_batched_jointed_worlds_match_each_world_alone():
+    """Worlds with body constraints in one batch step exactly as each world alone: the constraints of every world
+    keep their order in the batch's tables and the level schedule never mixes worlds' bodies."""
+    alone = [_jointed_world(s) for s in range(5)]
+    batch = ag2d.Batch([_jointed_world(s) for s in range(5)])
+    for w in alone:
+        w.step(150)
+    batch.step(150)
+    for k, w in enumerate(alone):
+        for f, _ in BODY_FIELDS:
+            assert np.array_equal(_bits(batch.read(k, f)), _bits(w.read(f))), (k, f)
+    assert batch.counters()["status"] == 0
+    with pytest.raises(ag2d.Ag2dError):
+        batch.save()   # checkpoints hold no body constraints
