@@ -660,6 +660,12 @@ struct ag2d_world {
     // Per-phase device timers (CUDA events on the world's stream) and the count of kernel launches.
     static constexpr int NPHASE = 15;
     bool profiling = false;
+    // The collision-detection pass (AG2D_PHASE_COLLIDE) as a captured CUDA graph, replayed while its launch shapes
+    // hold (list sizes, capacities, block sizes, whether the static tree is rebuilt).
+    cudaGraphExec_t collideExec = nullptr;
+    uint64_t collideKey[8] = {};
+    uint64_t collideSeen[8] = {};   // the shape of the last pass run without a graph
+    uint64_t collideLaunches = 0;
     cudaEvent_t ev[NPHASE][2] = {};
     bool evPending[NPHASE] = {};
     double phaseMs[NPHASE] = {};
@@ -1266,6 +1272,7 @@ struct ag2d_world {
 
     ~ag2d_world()
     {
+        if (collideExec) cudaGraphExecDestroy(collideExec);
         if (copyStream) cudaStreamSynchronize(copyStream);
         for (auto& a : asyncSlot) {
             if (a.packed) cudaEventDestroy(a.packed);
@@ -3941,12 +3948,57 @@ int32_t ag2d_world_run_phase(ag2d_world* world, int32_t phase)
             w.phaseBroad();
             break;
         case AG2D_PHASE_NARROW: w.phaseNarrow(); break;
-        case AG2D_PHASE_COLLIDE:
-            CK(cudaMemsetAsync(w.dCounters.p, 0, sizeof(StepCounters), w.stream));
-            w.phasePose(false);
-            w.phaseBroad();
-            w.phaseNarrow(false);
+        case AG2D_PHASE_COLLIDE: {
+            auto pass = [&] {
+                CK(cudaMemsetAsync(w.dCounters.p, 0, sizeof(StepCounters), w.stream));
+                w.phasePose(false);
+                w.phaseBroad();
+                w.phaseNarrow(false);
+            };
+            if (w.profiling) {   // the phase timers record events between the launches: no graph
+                pass();
+                break;
+            }
+            // The pass's launches depend on these only; the kernels read their counts on the device.
+            auto shape = [&](uint64_t* k) {
+                const uint64_t v[8] = {w.nDynCol, w.nOther, w.pairCap, w.manifoldCap, w.queryThreads,
+                                       w.narrowThreads, uint64_t(w.otherDirty), uint64_t(w.nColliders)};
+                std::copy(v, v + 8, k);
+            };
+            uint64_t key[8];
+            shape(key);
+            if (w.collideExec && std::equal(key, key + 8, w.collideKey)) {
+                CK(cudaGraphLaunch(w.collideExec, w.stream));
+                w.launches += w.collideLaunches;
+                break;
+            }
+            if (w.collideExec) { CK(cudaGraphExecDestroy(w.collideExec)); w.collideExec = nullptr; }
+            if (!std::equal(key, key + 8, w.collideSeen)) {
+                // A new shape: one pass as it is (it may grow buffers or rebuild the static tree), remembered.
+                pass();
+                shape(w.collideSeen);
+                break;
+            }
+            // The second pass of a shape: captured (nothing left to allocate), then replayed while the shape holds.
+            const uint64_t before = w.launches;
+            cudaGraph_t graph = nullptr;
+            CK(cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                pass();
+            } catch (...) {
+                cudaStreamEndCapture(w.stream, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            CK(cudaStreamEndCapture(w.stream, &graph));
+            const cudaError_t ie = cudaGraphInstantiate(&w.collideExec, graph, 0);
+            cudaGraphDestroy(graph);
+            CK(ie);
+            w.collideLaunches = w.launches - before;
+            std::copy(key, key + 8, w.collideKey);
+            CK(cudaGraphLaunch(w.collideExec, w.stream));
             break;
+        }
         case AG2D_PHASE_WAKE:
             w.phaseWake();
             w.phaseRestore();
