@@ -147,6 +147,20 @@ int main()
     sim->getNarrowPhaseCollisionDetector().findCollisionsInCircle(found, {0.0f, 1.0f}, 3.0f, touching);
     for (const auto& t : touching)
         if (!(t.second < 3.0f)) return 5;   // a contact is closer than the radius
+    // A collidersToCheck that is not a circle query's output (every other one of them): exactly the full answer's
+    // contacts among those colliders.
+    std::vector<ag2d::ObjectDenseIndex> half;
+    for (size_t i = 0; i < found.size(); i += 2) half.push_back(found[i]);
+    std::vector<std::pair<ag2d::ObjectDenseIndex, ag2d::Real>> touchingHalf;
+    sim->getNarrowPhaseCollisionDetector().findCollisionsInCircle(half, {0.0f, 1.0f}, 3.0f, touchingHalf);
+    {
+        size_t expect = 0;
+        for (const auto& t : touching)
+            if (std::find(half.begin(), half.end(), t.first) != half.end()) expect++;
+        if (touchingHalf.size() != expect) return 21;
+        for (const auto& t : touchingHalf)
+            if (std::find(half.begin(), half.end(), t.first) == half.end()) return 22;
+    }
     std::vector<ag2d::ObjectDenseIndex> all;
     sim->getBroadPhaseCollisionDetector().queryCollidersInShape(bp::AABBQuery({-1e6f, -1e6f, 1e6f, 1e6f}),
                                                                 bp::BvhTreeTypeFlag::All, all);
