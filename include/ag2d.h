@@ -238,7 +238,11 @@ uint32_t ag2d_world_body_index(ag2d_world* world, uint64_t handle);
 enum ag2d_body_state { AG2D_BODY_STATIC = 0, AG2D_BODY_SLEEPING = 1, AG2D_BODY_DYNAMIC = 2, AG2D_BODY_DESTROYED = 3 };
 enum ag2d_command {
     AG2D_COMMAND_DESTROY = 0, AG2D_COMMAND_POSITION, AG2D_COMMAND_ROTATION, AG2D_COMMAND_VELOCITY,
-    AG2D_COMMAND_ANGULAR_VELOCITY, AG2D_COMMAND_MASS, AG2D_COMMAND_INERTIA
+    AG2D_COMMAND_ANGULAR_VELOCITY, AG2D_COMMAND_MASS, AG2D_COMMAND_INERTIA, AG2D_COMMAND_LOCAL_CENTER_OF_MASS,
+    AG2D_COMMAND_RECOMPUTE_INERTIA, AG2D_COMMAND_MASS_FROM_DENSITY,
+    /* collider commands (the handle field holds the collider's dense index) */
+    AG2D_COMMAND_COLLIDER_OFFSET = 16, AG2D_COMMAND_COLLIDER_ROTATION, AG2D_COMMAND_COLLIDER_MATERIAL,
+    AG2D_COMMAND_CIRCLE_RADIUS, AG2D_COMMAND_BOX_SIZE, AG2D_COMMAND_CAPSULE_SHAPE
 };
 int32_t ag2d_world_destroy_body(ag2d_world* world, uint64_t body);
 int32_t ag2d_world_set_body_position(ag2d_world* world, uint64_t body, float x, float y);
@@ -247,6 +251,21 @@ int32_t ag2d_world_set_body_velocity(ag2d_world* world, uint64_t body, float vx,
 int32_t ag2d_world_set_body_angular_velocity(ag2d_world* world, uint64_t body, float angular_velocity);
 int32_t ag2d_world_set_body_mass(ag2d_world* world, uint64_t body, float mass);
 int32_t ag2d_world_set_body_inertia(ag2d_world* world, uint64_t body, float inertia);
+/* ObjectAPI::setBodyLocalCenterOfMass / recomputeBodyInertia / setBodyMassFromDensity (ObjectAPI.h:82-84;
+ * ObjectManager.cpp:751-775, 907-970): the body origin stays put and the centre of mass moves with the local
+ * centre; the inertia from the colliders' shapes at the body's mass (parallel axis to the centre of mass); the mass
+ * from a density times the colliders' area. */
+int32_t ag2d_world_set_body_local_center_of_mass(ag2d_world* world, uint64_t body, float x, float y);
+int32_t ag2d_world_recompute_body_inertia(ag2d_world* world, uint64_t body);
+int32_t ag2d_world_set_body_mass_from_density(ag2d_world* world, uint64_t body, float density);
+/* ObjectAPI::setColliderLocalOffset / setColliderLocalRotation / setColliderMaterial / setCircleRadius /
+ * setBoxSize / setCapsuleShape (ObjectAPI.h:86-91; ObjectManager.cpp:785-850) by dense collider index, deferred
+ * like the body commands: field AG2D_COMMAND_COLLIDER_OFFSET (a, b), _ROTATION (a, wrapped into [0, 2 pi)),
+ * _MATERIAL (a as the index; an unknown index becomes 0), _CIRCLE_RADIUS (a), _BOX_SIZE (a, b: width, height),
+ * _CAPSULE_SHAPE (a, b: length, radius); sizes are clamped at 0, a shape setter on another shape does nothing.
+ * The collider's body wakes; the body's bound radius follows. */
+int32_t ag2d_world_set_collider(ag2d_world* world, uint32_t collider, int32_t command, float a, float b);
+
 /* Applies the queued commands now (Simulation::flushCommands, Simulation.cpp:453-456). */
 int32_t ag2d_world_flush_commands(ag2d_world* world);
 

@@ -302,6 +302,29 @@ public:
     }
     void setBodyMass(Handle h, Real m) { detail::check(ag2d_world_set_body_mass(world, h.value, m)); }
     void setBodyInertia(Handle h, Real i) { detail::check(ag2d_world_set_body_inertia(world, h.value, i)); }
+    void setBodyLocalCenterOfMass(Handle h, Vec2 c)
+    {
+        detail::check(ag2d_world_set_body_local_center_of_mass(world, h.value, c.x, c.y));
+    }
+    void recomputeBodyInertia(Handle h) { detail::check(ag2d_world_recompute_body_inertia(world, h.value)); }
+    void setBodyMassFromDensity(Handle h, Real d)
+    {
+        detail::check(ag2d_world_set_body_mass_from_density(world, h.value, d));
+    }
+    // Collider setters (ObjectAPI.h:86-91) by dense collider index (the reference takes the collider's handle;
+    // collider indices are stable here). Deferred to the next step like the body commands.
+    void setColliderLocalOffset(ObjectDenseIndex c, Vec2 o) { collider(c, AG2D_COMMAND_COLLIDER_OFFSET, o.x, o.y); }
+    void setColliderLocalRotation(ObjectDenseIndex c, Real r) { collider(c, AG2D_COMMAND_COLLIDER_ROTATION, r, 0); }
+    void setColliderMaterial(ObjectDenseIndex c, MaterialIndex m)
+    {
+        collider(c, AG2D_COMMAND_COLLIDER_MATERIAL, Real(m), 0);
+    }
+    void setCircleRadius(ObjectDenseIndex c, Real r) { collider(c, AG2D_COMMAND_CIRCLE_RADIUS, r, 0); }
+    void setBoxSize(ObjectDenseIndex c, Vec2 size) { collider(c, AG2D_COMMAND_BOX_SIZE, size.x, size.y); }
+    void setCapsuleShape(ObjectDenseIndex c, Real length, Real radius)
+    {
+        collider(c, AG2D_COMMAND_CAPSULE_SHAPE, length, radius);
+    }
 
     // Dense index of a handle; UINT32_MAX when the handle is stale (ObjectAPI::getBodyIndex, ObjectAPI.h:53).
     ObjectDenseIndex getBodyIndex(Handle h) const noexcept { return ag2d_world_body_index(world, h.value); }
@@ -319,6 +342,10 @@ public:
     }
 
 private:
+    void collider(ObjectDenseIndex c, int32_t command, Real a, Real b)
+    {
+        detail::check(ag2d_world_set_collider(world, c, command, a, b));
+    }
     // Invalid shapes (the reference's nullopt cases) return nullopt; anything else is an error.
     // 'code' is the creating call's result, evaluated before 'h' is read (the call writes h).
     static std::optional<Handle> created(int32_t code, uint64_t h)

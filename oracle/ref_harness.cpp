@@ -429,7 +429,8 @@ extern "C"
         auto* h = static_cast<Harness*>(hp);
         h->sim.objects().destroyBody(bodyHandleOfSlot(h, slot));
     }
-    // kind: 0 position (a, b), 1 rotation (a), 2 velocity (a, b), 3 angular velocity (a), 4 mass (a), 5 inertia (a).
+    // kind: 0 position (a, b), 1 rotation (a), 2 velocity (a, b), 3 angular velocity (a), 4 mass (a), 5 inertia (a),
+    // 6 local centre of mass (a, b), 7 recompute inertia, 8 mass from density (a).
     void agref_set_body(void* hp, uint32_t slot, int32_t kind, float a, float b)
     {
         auto* h = static_cast<Harness*>(hp);
@@ -443,6 +444,27 @@ extern "C"
         case 3: o.setBodyAngularVelocity(hd, a); break;
         case 4: o.setBodyMass(hd, a); break;
         case 5: o.setBodyInertia(hd, a); break;
+        case 6: o.setBodyLocalCenterOfMass(hd, Vec2(a, b)); break;
+        case 7: o.recomputeBodyInertia(hd); break;
+        case 8: o.setBodyMassFromDensity(hd, a); break;
+        default: break;
+        }
+    }
+    // ObjectAPI's collider setters (SimulationAPIs/ObjectAPI.h:86-91) on the collider at a dense index now:
+    // kind 0 local offset (a, b), 1 local rotation, 2 material (a), 3 circle radius, 4 box size, 5 capsule shape.
+    void agref_set_collider(void* hp, uint32_t index, int32_t kind, float a, float b)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        auto& o = h->sim.objects();
+        const Handle hd = h->sim.objectManager.colliders.handleAt(index);
+        switch (kind)
+        {
+        case 0: o.setColliderLocalOffset(hd, Vec2(a, b)); break;
+        case 1: o.setColliderLocalRotation(hd, a); break;
+        case 2: o.setColliderMaterial(hd, MaterialIndex(a)); break;
+        case 3: o.setCircleRadius(hd, a); break;
+        case 4: o.setBoxSize(hd, Vec2(a, b)); break;
+        case 5: o.setCapsuleShape(hd, a, b); break;
         default: break;
         }
     }

@@ -58,6 +58,7 @@ def lib():
         L.agref_update.argtypes = [vp, i32]
         L.agref_destroy_body.argtypes = [vp, u32]
         L.agref_set_body.argtypes = [vp, u32, i32, f, f]
+        L.agref_set_collider.argtypes = [vp, u32, i32, f, f]
         L.agref_body_index.restype = u32
         L.agref_body_index.argtypes = [vp, u32]
         L.agref_timed_update.restype = ctypes.c_double
@@ -192,6 +193,10 @@ class RefSim:
         if c < 0:
             raise ValueError("reference rejected the collider")
         return int(c)
+
+    def set_collider(self, index: int, kind: int, a: float, b: float = 0.0):
+        """A collider setter on the collider at dense index 'index' (applied at the next flush)."""
+        lib().agref_set_collider(self.h, index, kind, a, b)
 
     def body_index(self, i: int) -> int:
         """Dense index of scene body i now (2**32 - 1 once destroyed)."""

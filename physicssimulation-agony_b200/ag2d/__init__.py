@@ -32,6 +32,9 @@ COL_WORLD_X, COL_WORLD_Y, COL_WORLD_ROTATION, COL_WORLD_COS, COL_WORLD_SIN, COL_
 DYN_SORTED, DYN_MORTON, PAIRS, MANIFOLDS, PREV_MANIFOLDS, SOLVE_ORDER, COLOR_STARTS, ISLAND_MANIFOLDS, \
     ISLAND_IDS = range(64, 73)
 # enum ag2d_phase
+# enum ag2d_command: collider setters (by dense collider index)
+COMMAND_COLLIDER_OFFSET, COMMAND_COLLIDER_ROTATION, COMMAND_COLLIDER_MATERIAL, COMMAND_CIRCLE_RADIUS, \
+    COMMAND_BOX_SIZE, COMMAND_CAPSULE_SHAPE = range(16, 22)
 PHASE_INTEGRATE, PHASE_SPATIAL_FULL, PHASE_SPATIAL_DYNAMIC, PHASE_BROAD, PHASE_NARROW, PHASE_SOLVE, \
     PHASE_ISLANDS, PHASE_COLLIDE, PHASE_CCD, PHASE_WAKE, PHASE_EVENTS = range(1, 12)
 
@@ -189,6 +192,10 @@ def _load():
     for name in ("rotation", "angular_velocity", "mass", "inertia"):
         getattr(L, f"ag2d_world_set_body_{name}").argtypes = [vp, u64, ctypes.c_float]
     L.ag2d_world_flush_commands.argtypes = [vp]
+    L.ag2d_world_set_body_local_center_of_mass.argtypes = [vp, u64, ctypes.c_float, ctypes.c_float]
+    L.ag2d_world_recompute_body_inertia.argtypes = [vp, u64]
+    L.ag2d_world_set_body_mass_from_density.argtypes = [vp, u64, ctypes.c_float]
+    L.ag2d_world_set_collider.argtypes = [vp, u32, i32, ctypes.c_float, ctypes.c_float]
     L.ag2d_world_create_joint.argtypes = [vp, ctypes.POINTER(JointDesc), ctypes.POINTER(u64)]
     L.ag2d_world_destroy_joint.argtypes = [vp, i32, u64]
     L.ag2d_world_set_joint.argtypes = [vp, i32, u64, i32, ctypes.c_float, ctypes.c_float]
@@ -437,6 +444,19 @@ class World:
 
     def set_body_inertia(self, handle: int, inertia: float):
         _check(lib.ag2d_world_set_body_inertia(self.h, handle, inertia))
+
+    def set_body_local_center_of_mass(self, handle: int, x: float, y: float):
+        _check(lib.ag2d_world_set_body_local_center_of_mass(self.h, handle, x, y))
+
+    def recompute_body_inertia(self, handle: int):
+        _check(lib.ag2d_world_recompute_body_inertia(self.h, handle))
+
+    def set_body_mass_from_density(self, handle: int, density: float):
+        _check(lib.ag2d_world_set_body_mass_from_density(self.h, handle, density))
+
+    def set_collider(self, collider: int, command: int, a: float, b: float = 0.0):
+        """A deferred collider setter (COMMAND_COLLIDER_OFFSET ... COMMAND_CAPSULE_SHAPE) by dense index."""
+        _check(lib.ag2d_world_set_collider(self.h, collider, command, a, b))
 
     def flush_commands(self):
         _check(lib.ag2d_world_flush_commands(self.h))

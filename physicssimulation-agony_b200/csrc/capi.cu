@@ -2459,17 +2459,88 @@ struct ag2d_world {
         // ObjectManager.cpp:678-687, and destroyColliderInternal): their colliders count as edited.
         std::vector<uint8_t> editedBody(nBodies, 0);
         bool anyEdited = false;
+        // applyBodyMass (ObjectManager.cpp:867-905).
+        auto applyMass = [&](uint32_t b, float m) {
+            HBody& hb = o.bodies[b];
+            const float newMass = std::fmax(0.0f, m);
+            const float oldMass = hb.mass;
+            if (newMass > 0.0f) {
+                float inertia = hb.inertia;
+                if (oldMass > 0.0f) inertia *= newMass / oldMass;
+                hb.mass = newMass;
+                hb.invMass = 1.0f / newMass;
+                hb.inertia = inertia;
+                hb.invInertia = inertia > 0.0f ? 1.0f / inertia : 0.0f;
+                if (state[b] == STATE_STATIC) { state[b] = STATE_DYNAMIC; timer[b] = 0.0f; }
+            } else {
+                hb.mass = 0.0f; hb.invMass = 0.0f; hb.inertia = 0.0f; hb.invInertia = 0.0f;
+                vel[b].x = 0.0f; vel[b].y = 0.0f; vel[b].z = 0.0f;
+                state[b] = STATE_STATIC;
+            }
+            vel[b].w = hb.invMass;
+            pos[b].w = hb.invInertia;
+        };
+        std::vector<uint32_t> editedColliders, reachBodies;   // device collider records and bound radii to refresh
+        const float twoPi = float(3.14159265358979323846 * 2.0);
+        auto wrap = [&](float r) { r = std::fmod(r, twoPi); if (r < 0.0f) r += twoPi; return r; };
         for (const BodyCommand& c : commands) {
-            const uint32_t b = o.indexOf(c.handle);
+            const bool colliderCmd = c.kind >= AG2D_COMMAND_COLLIDER_OFFSET && c.kind <= AG2D_COMMAND_CAPSULE_SHAPE;
+            const uint32_t ci = colliderCmd ? uint32_t(c.handle) : 0xFFFFFFFFu;
+            if (colliderCmd && ci >= o.colliders.size()) continue;
+            const uint32_t b = colliderCmd ? o.colliders[ci].body : o.indexOf(c.handle);
             if (b >= nBodies || b >= o.bodies.size() || state[b] == STATE_DESTROYED) continue;
             HBody& hb = o.bodies[b];
             if (state[b] == STATE_STATIC &&
-                (c.kind == AG2D_COMMAND_DESTROY || c.kind == AG2D_COMMAND_POSITION ||
-                 c.kind == AG2D_COMMAND_ROTATION || c.kind == AG2D_COMMAND_MASS)) {
-                editedBody[b] = 1;
+                (colliderCmd || c.kind == AG2D_COMMAND_DESTROY || c.kind == AG2D_COMMAND_POSITION ||
+                 c.kind == AG2D_COMMAND_ROTATION || c.kind == AG2D_COMMAND_MASS ||
+                 c.kind == AG2D_COMMAND_LOCAL_CENTER_OF_MASS || c.kind == AG2D_COMMAND_MASS_FROM_DENSITY)) {
+                editedBody[b] = 1;   // markStaticColliderEdited
                 anyEdited = true;
             }
             wake(b);
+            if (colliderCmd) {   // ObjectManager::applyCommand's collider branch (ObjectManager.cpp:785-852)
+                HCollider& k = o.colliders[ci];
+                bool shapeEdit = false;
+                switch (c.kind) {
+                case AG2D_COMMAND_COLLIDER_OFFSET:
+                    k.locX = c.a; k.locY = c.b;
+                    k.comOffX = k.locX - hb.lcomX; k.comOffY = k.locY - hb.lcomY;
+                    break;
+                case AG2D_COMMAND_COLLIDER_ROTATION: k.localRot = wrap(c.a); break;
+                case AG2D_COMMAND_COLLIDER_MATERIAL: {
+                    const float idx = c.a;
+                    k.material = (idx >= 0.0f && idx < float(o.materialCount())) ? uint32_t(idx) : 0u;
+                    break;
+                }
+                case AG2D_COMMAND_CIRCLE_RADIUS:
+                    if (k.type != SHAPE_CIRCLE) break;
+                    o.circleRadius[k.shape] = std::fmax(0.0f, c.a);
+                    k.minExtent = k.maxExtent = o.circleRadius[k.shape];
+                    shapeEdit = true;
+                    break;
+                case AG2D_COMMAND_BOX_SIZE:
+                    if (k.type != SHAPE_BOX) break;
+                    o.boxHalfW[k.shape] = std::fmax(0.0f, c.a) * 0.5f;
+                    o.boxHalfH[k.shape] = std::fmax(0.0f, c.b) * 0.5f;
+                    k.minExtent = std::fmin(o.boxHalfW[k.shape], o.boxHalfH[k.shape]);
+                    k.maxExtent = std::fmax(o.boxHalfW[k.shape], o.boxHalfH[k.shape]);
+                    shapeEdit = true;
+                    break;
+                case AG2D_COMMAND_CAPSULE_SHAPE:
+                    if (k.type != SHAPE_CAPSULE) break;
+                    o.boxHalfW[k.shape] = std::fmax(0.0f, c.a) * 0.5f;
+                    o.boxHalfH[k.shape] = std::fmax(0.0f, c.b);
+                    k.minExtent = o.boxHalfH[k.shape];
+                    k.maxExtent = o.boxHalfW[k.shape] + o.boxHalfH[k.shape];
+                    shapeEdit = true;
+                    break;
+                default: break;
+                }
+                (void)shapeEdit;
+                editedColliders.push_back(ci);
+                reachBodies.push_back(b);
+                continue;
+            }
             switch (c.kind) {
             case AG2D_COMMAND_DESTROY:
                 state[b] = STATE_DESTROYED;
@@ -2506,24 +2577,47 @@ struct ag2d_world {
             }
             case AG2D_COMMAND_VELOCITY: vel[b].x = c.a; vel[b].y = c.b; break;
             case AG2D_COMMAND_ANGULAR_VELOCITY: vel[b].z = c.a; break;
-            case AG2D_COMMAND_MASS: {   // applyBodyMass (ObjectManager.cpp:867-905)
-                const float newMass = std::fmax(0.0f, c.a);
-                const float oldMass = hb.mass;
-                if (newMass > 0.0f) {
-                    float inertia = hb.inertia;
-                    if (oldMass > 0.0f) inertia *= newMass / oldMass;
-                    hb.mass = newMass;
-                    hb.invMass = 1.0f / newMass;
-                    hb.inertia = inertia;
-                    hb.invInertia = inertia > 0.0f ? 1.0f / inertia : 0.0f;
-                    if (state[b] == STATE_STATIC) { state[b] = STATE_DYNAMIC; timer[b] = 0.0f; }
-                } else {
-                    hb.mass = 0.0f; hb.invMass = 0.0f; hb.inertia = 0.0f; hb.invInertia = 0.0f;
-                    vel[b].x = 0.0f; vel[b].y = 0.0f; vel[b].z = 0.0f;
-                    state[b] = STATE_STATIC;
+            case AG2D_COMMAND_MASS: applyMass(b, c.a); break;
+            case AG2D_COMMAND_LOCAL_CENTER_OF_MASS: {   // ObjectManager.cpp:751-771: the origin stays put
+                const float r = pos[b].z, cosR = std::cos(r), sinR = std::sin(r);
+                const float dx = c.a - hb.lcomX, dy = c.b - hb.lcomY;
+                pos[b].x += cosR * dx - sinR * dy;
+                pos[b].y += sinR * dx + cosR * dy;
+                hb.lcomX = c.a;
+                hb.lcomY = c.b;
+                for (const uint32_t k : hb.colliders) {
+                    o.colliders[k].comOffX = o.colliders[k].locX - hb.lcomX;
+                    o.colliders[k].comOffY = o.colliders[k].locY - hb.lcomY;
+                    editedColliders.push_back(k);
                 }
-                vel[b].w = hb.invMass;
+                reachBodies.push_back(b);
+                break;
+            }
+            case AG2D_COMMAND_RECOMPUTE_INERTIA: {   // ObjectManager.cpp:917-970
+                const float mass = hb.mass;
+                if (mass <= 0.0f) break;
+                float totalArea = 0.0f;
+                for (const uint32_t k : hb.colliders) totalArea += o.colliderArea(k);
+                if (totalArea <= 0.0f) break;
+                const float massPerArea = mass / totalArea;
+                float inertia = 0.0f;
+                for (const uint32_t k : hb.colliders) {
+                    const float area = o.colliderArea(k);
+                    if (area <= 0.0f) continue;
+                    const float m = massPerArea * area;
+                    const float dx = o.colliders[k].comOffX, dy = o.colliders[k].comOffY;
+                    inertia += o.colliderOwnInertia(k, m) + m * (dx * dx + dy * dy);
+                }
+                hb.inertia = inertia;
+                hb.invInertia = inertia > 0.0f ? 1.0f / inertia : 0.0f;
                 pos[b].w = hb.invInertia;
+                break;
+            }
+            case AG2D_COMMAND_MASS_FROM_DENSITY: {   // ObjectManager.cpp:907-915
+                float totalArea = 0.0f;
+                for (const uint32_t k : hb.colliders) totalArea += o.colliderArea(k);
+                if (totalArea <= 0.0f) break;
+                applyMass(b, std::fmax(0.0f, c.a) * totalArea);
                 break;
             }
             case AG2D_COMMAND_INERTIA: {
@@ -2538,6 +2632,26 @@ struct ag2d_world {
             }
         }
         commands.clear();
+        // Collider records and shape parameters the commands changed, and the bound radii that follow.
+        for (const uint32_t k : editedColliders) {
+            const HCollider& hc = o.colliders[k];
+            const float4 off = make_float4(hc.comOffX, hc.comOffY, hc.localRot, 0.0f);
+            CK(cudaMemcpyAsync(coff.p + k, &off, sizeof(float4), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(cmat.p + k, &hc.material, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(minExtent.p + k, &hc.minExtent, sizeof(float), cudaMemcpyHostToDevice, s));
+            if (hc.type == SHAPE_CIRCLE)
+                CK(cudaMemcpyAsync(circleRadius.p + hc.shape, &o.circleRadius[hc.shape], sizeof(float),
+                                   cudaMemcpyHostToDevice, s));
+            else if (hc.type == SHAPE_BOX || hc.type == SHAPE_CAPSULE) {
+                const float2 h = make_float2(o.boxHalfW[hc.shape], o.boxHalfH[hc.shape]);
+                CK(cudaMemcpyAsync(boxHalf.p + hc.shape, &h, sizeof(float2), cudaMemcpyHostToDevice, s));
+            }
+            CK(cudaStreamSynchronize(s));   // the sources are this loop's locals
+        }
+        for (const uint32_t b : reachBodies) {
+            o.bodies[b].boundRadius = o.boundRadiusOf(b);
+            CK(cudaMemcpyAsync(boundRadius.p + b, &o.bodies[b].boundRadius, sizeof(float), cudaMemcpyHostToDevice, s));
+        }
         // Constraint destroys and edits (ConstraintSystemBase::flushImpl, ConstraintSystemBase.h:127-142, and the
         // systems' flushCommands): stale handles are dropped; the constraint's bodies wake.
         for (const JointCommand& c : jointCommands) {
@@ -3058,11 +3172,32 @@ int32_t ag2d_world_set_body_inertia(ag2d_world* world, uint64_t body, float iner
     return queue_command(world, AG2D_COMMAND_INERTIA, body, inertia, 0.0f);
 }
 
+int32_t ag2d_world_set_body_local_center_of_mass(ag2d_world* world, uint64_t body, float x, float y)
+{
+    return queue_command(world, AG2D_COMMAND_LOCAL_CENTER_OF_MASS, body, x, y);
+}
+int32_t ag2d_world_recompute_body_inertia(ag2d_world* world, uint64_t body)
+{
+    return queue_command(world, AG2D_COMMAND_RECOMPUTE_INERTIA, body, 0.0f, 0.0f);
+}
+int32_t ag2d_world_set_body_mass_from_density(ag2d_world* world, uint64_t body, float density)
+{
+    return queue_command(world, AG2D_COMMAND_MASS_FROM_DENSITY, body, density, 0.0f);
+}
+int32_t ag2d_world_set_collider(ag2d_world* world, uint32_t collider, int32_t command, float a, float b)
+{
+    if (command < AG2D_COMMAND_COLLIDER_OFFSET || command > AG2D_COMMAND_CAPSULE_SHAPE) {
+        g_error = "unknown collider command";
+        return AG2D_ERR_INVALID_ARG;
+    }
+    return queue_command(world, command, uint64_t(collider), a, b);
+}
+
 int32_t ag2d_world_flush_commands(ag2d_world* world)
 {
     return guarded([&] {
         if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
-        if (world->commands.empty()) return;
+        if (world->commands.empty() && world->jointCommands.empty()) return;
         CK(cudaSetDevice(world->settings.device));
         world->flushCommands();
     });

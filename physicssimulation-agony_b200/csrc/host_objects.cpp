@@ -476,3 +476,72 @@ bool HostObjects::addCollider(uint32_t body, uint32_t type, float locX, float lo
 }
 
 }  // namespace ag2d
+
+namespace ag2d {
+
+float HostObjects::colliderArea(uint32_t c) const
+{
+    const HCollider& k = colliders[c];
+    const float pi = float(3.14159265358979323846);
+    switch (k.type) {
+    case 0: { const float r = circleRadius[k.shape]; return pi * r * r; }
+    case 1: return (boxHalfW[k.shape] * 2.0f) * (boxHalfH[k.shape] * 2.0f);
+    case 3: {
+        const float len = boxHalfW[k.shape] * 2.0f, r = boxHalfH[k.shape];
+        return len * 2.0f * r + pi * r * r;
+    }
+    case 2: {
+        const std::vector<float>& v = polygons[k.shape].verts;
+        const size_t n = v.size() / 2;
+        if (n < 3) return 0.0f;
+        float twice = 0.0f;
+        for (size_t i = 0; i < n; i++) {
+            const size_t j = i + 1 == n ? 0 : i + 1;
+            twice += v[2 * i] * v[2 * j + 1] - v[2 * j] * v[2 * i + 1];
+        }
+        return std::fmax(0.0f, twice * 0.5f);
+    }
+    default: return 0.0f;
+    }
+}
+
+float HostObjects::colliderOwnInertia(uint32_t c, float m) const
+{
+    const HCollider& k = colliders[c];
+    switch (k.type) {
+    case 0: { const float r = circleRadius[k.shape]; return (0.5f * (r * r) + 0.0f) * m; }
+    case 1: {
+        const float w = boxHalfW[k.shape] * 2.0f, h = boxHalfH[k.shape] * 2.0f;
+        return m * (float(1.0 / 12.0) * (w * w + h * h) + 0.0f);
+    }
+    case 3: {
+        const float len = boxHalfW[k.shape] * 2.0f, r = boxHalfH[k.shape];
+        const float pi = float(3.14159265358979323846);
+        const float rectArea = len * 2.0f * r, circleArea = pi * r * r, totalArea = rectArea + circleArea;
+        const float rectMass = m * rectArea / totalArea, capMass = m * circleArea / totalArea;
+        const float diameter = 2.0f * r;
+        const float rectInertia = rectMass * (len * len + diameter * diameter) / 12.0f;
+        const float dist = 4.0f * r / (3.0f * pi);
+        const float capInertia = capMass * (0.5f * r * r + 0.25f * len * len + len * dist);
+        return rectInertia + capInertia + m * 0.0f;
+    }
+    case 2: {
+        float inertia = 0.0f, cx = 0.0f, cy = 0.0f;
+        polygon_inertia(m, polygons[k.shape].verts, inertia, cx, cy);
+        return inertia;
+    }
+    default: return 0.0f;
+    }
+}
+
+float HostObjects::boundRadiusOf(uint32_t b) const
+{
+    float radius = 0.0f;
+    for (const uint32_t c : bodies[b].colliders) {
+        const float x = colliders[c].comOffX, y = colliders[c].comOffY;
+        radius = std::fmax(radius, std::sqrt(x * x + y * y) + colliders[c].maxExtent);
+    }
+    return radius;
+}
+
+}  // namespace ag2d

@@ -156,6 +156,14 @@ public:
     bool addCollider(uint32_t body, uint32_t type, float locX, float locY, float localRot, uint32_t material,
                      const float* p, const float* xy, uint32_t n, uint32_t& collider, std::string& err);
 
+    // colliderArea (ObjectManager.cpp:593-612) with PhysicsGeometry's areas (PhysicsGeometry.cpp:115-144).
+    float colliderArea(uint32_t c) const;
+    // A collider's inertia about its own origin for mass m (PhysicsGeometry::calculate*Inertia at the origin, as
+    // ObjectManager::recomputeBodyInertia takes them, ObjectManager.cpp:917-970).
+    float colliderOwnInertia(uint32_t c, float m) const;
+    // refreshBoundRadius (ObjectManager.cpp:37-43): the farthest reach of the body's colliders from its centre.
+    float boundRadiusOf(uint32_t b) const;
+
     uint32_t indexOf(uint64_t handle) const
     {
         const uint32_t slot = uint32_t(handle & 0xFFFFFFFFu), gen = uint32_t(handle >> 32);
