@@ -242,7 +242,7 @@ enum ag2d_command {
     AG2D_COMMAND_RECOMPUTE_INERTIA, AG2D_COMMAND_MASS_FROM_DENSITY,
     /* collider commands (the handle field holds the collider's dense index) */
     AG2D_COMMAND_COLLIDER_OFFSET = 16, AG2D_COMMAND_COLLIDER_ROTATION, AG2D_COMMAND_COLLIDER_MATERIAL,
-    AG2D_COMMAND_CIRCLE_RADIUS, AG2D_COMMAND_BOX_SIZE, AG2D_COMMAND_CAPSULE_SHAPE
+    AG2D_COMMAND_CIRCLE_RADIUS, AG2D_COMMAND_BOX_SIZE, AG2D_COMMAND_CAPSULE_SHAPE, AG2D_COMMAND_POLYGON_SHAPE
 };
 int32_t ag2d_world_destroy_body(ag2d_world* world, uint64_t body);
 int32_t ag2d_world_set_body_position(ag2d_world* world, uint64_t body, float x, float y);
@@ -265,6 +265,13 @@ int32_t ag2d_world_set_body_mass_from_density(ag2d_world* world, uint64_t body, 
  * _CAPSULE_SHAPE (a, b: length, radius); sizes are clamped at 0, a shape setter on another shape does nothing.
  * The collider's body wakes; the body's bound radius follows. */
 int32_t ag2d_world_set_collider(ag2d_world* world, uint32_t collider, int32_t command, float a, float b);
+/* ObjectAPI::setPolygonShape (ObjectAPI.h:93; ObjectManager.cpp:622-636, 838-857): n collider-local vertices (xy
+ * pairs) replace a polygon collider's outline. The outline is prepared at once as at creation (duplicates and
+ * straight vertices dropped, made counter-clockwise); a degenerate or concave outline, or one of more than 16
+ * vertices, is refused (AG2D_ERR_INVALID_ARG, the reference's false). At the next flush it is recentred on its
+ * centroid, the shift added to the collider's offset (the body's mass and inertia are kept); on another shape it
+ * does nothing. */
+int32_t ag2d_world_set_polygon_shape(ag2d_world* world, uint32_t collider, const float* xy, uint32_t n);
 
 /* Applies the queued commands now (Simulation::flushCommands, Simulation.cpp:453-456). */
 int32_t ag2d_world_flush_commands(ag2d_world* world);

@@ -325,6 +325,18 @@ public:
     {
         collider(c, AG2D_COMMAND_CAPSULE_SHAPE, length, radius);
     }
+    // ObjectAPI::setPolygonShape (ObjectAPI.h:93): false, with nothing queued, for an outline the reference refuses
+    // (fewer than 3 vertices, degenerate, concave, more than 16 vertices).
+    bool setPolygonShape(ObjectDenseIndex c, std::span<const Vec2> localVertices)
+    {
+        std::vector<float> xy;
+        xy.reserve(localVertices.size() * 2);
+        for (const Vec2& v : localVertices) { xy.push_back(v.x); xy.push_back(v.y); }
+        const int32_t code = ag2d_world_set_polygon_shape(world, c, xy.data(), uint32_t(localVertices.size()));
+        if (code == AG2D_ERR_INVALID_ARG) return false;
+        detail::check(code);
+        return true;
+    }
 
     // Dense index of a handle; UINT32_MAX when the handle is stale (ObjectAPI::getBodyIndex, ObjectAPI.h:53).
     ObjectDenseIndex getBodyIndex(Handle h) const noexcept { return ag2d_world_body_index(world, h.value); }

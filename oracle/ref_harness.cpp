@@ -468,6 +468,15 @@ extern "C"
         default: break;
         }
     }
+    // ObjectAPI::setPolygonShape (ObjectAPI.h:93) on the collider at dense index 'index': 1 if queued.
+    int32_t agref_set_polygon(void* hp, uint32_t index, const float* xy, uint32_t n)
+    {
+        auto* h = static_cast<Harness*>(hp);
+        const Handle hd = h->sim.objectManager.colliders.handleAt(index);
+        std::vector<Vec2> v(n);
+        for (uint32_t i = 0; i < n; i++) v[i] = Vec2(xy[2 * i], xy[2 * i + 1]);
+        return h->sim.objects().setPolygonShape(hd, std::span<const Vec2>(v.data(), v.size())) ? 1 : 0;
+    }
     // Simulation::flushCommands (Simulation.cpp:454-461) on its own: the queued commands, the wakes they cause and
     // the stored manifolds of the woken islands, as the next update would apply them first.
     void agref_flush_commands(void* hp)

@@ -59,6 +59,8 @@ def lib():
         L.agref_destroy_body.argtypes = [vp, u32]
         L.agref_set_body.argtypes = [vp, u32, i32, f, f]
         L.agref_set_collider.argtypes = [vp, u32, i32, f, f]
+        L.agref_set_polygon.argtypes = [vp, u32, ctypes.POINTER(ctypes.c_float), u32]
+        L.agref_set_polygon.restype = i32
         L.agref_body_index.restype = u32
         L.agref_body_index.argtypes = [vp, u32]
         L.agref_timed_update.restype = ctypes.c_double
@@ -197,6 +199,12 @@ class RefSim:
     def set_collider(self, index: int, kind: int, a: float, b: float = 0.0):
         """A collider setter on the collider at dense index 'index' (applied at the next flush)."""
         lib().agref_set_collider(self.h, index, kind, a, b)
+
+    def set_polygon(self, index: int, xy) -> bool:
+        """ObjectAPI::setPolygonShape on the collider at dense index 'index' (applied at the next flush)."""
+        v = np.ascontiguousarray(np.asarray(xy, np.float32).reshape(-1))
+        return bool(lib().agref_set_polygon(self.h, index, v.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                            v.size // 2))
 
     def body_index(self, i: int) -> int:
         """Dense index of scene body i now (2**32 - 1 once destroyed)."""

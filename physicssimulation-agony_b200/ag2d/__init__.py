@@ -34,7 +34,7 @@ DYN_SORTED, DYN_MORTON, PAIRS, MANIFOLDS, PREV_MANIFOLDS, SOLVE_ORDER, COLOR_STA
 # enum ag2d_phase
 # enum ag2d_command: collider setters (by dense collider index)
 COMMAND_COLLIDER_OFFSET, COMMAND_COLLIDER_ROTATION, COMMAND_COLLIDER_MATERIAL, COMMAND_CIRCLE_RADIUS, \
-    COMMAND_BOX_SIZE, COMMAND_CAPSULE_SHAPE = range(16, 22)
+    COMMAND_BOX_SIZE, COMMAND_CAPSULE_SHAPE, COMMAND_POLYGON_SHAPE = range(16, 23)
 PHASE_INTEGRATE, PHASE_SPATIAL_FULL, PHASE_SPATIAL_DYNAMIC, PHASE_BROAD, PHASE_NARROW, PHASE_SOLVE, \
     PHASE_ISLANDS, PHASE_COLLIDE, PHASE_CCD, PHASE_WAKE, PHASE_EVENTS = range(1, 12)
 
@@ -196,6 +196,7 @@ def _load():
     L.ag2d_world_recompute_body_inertia.argtypes = [vp, u64]
     L.ag2d_world_set_body_mass_from_density.argtypes = [vp, u64, ctypes.c_float]
     L.ag2d_world_set_collider.argtypes = [vp, u32, i32, ctypes.c_float, ctypes.c_float]
+    L.ag2d_world_set_polygon_shape.argtypes = [vp, u32, ctypes.POINTER(ctypes.c_float), u32]
     L.ag2d_world_create_joint.argtypes = [vp, ctypes.POINTER(JointDesc), ctypes.POINTER(u64)]
     L.ag2d_world_destroy_joint.argtypes = [vp, i32, u64]
     L.ag2d_world_set_joint.argtypes = [vp, i32, u64, i32, ctypes.c_float, ctypes.c_float]
@@ -457,6 +458,17 @@ class World:
     def set_collider(self, collider: int, command: int, a: float, b: float = 0.0):
         """A deferred collider setter (COMMAND_COLLIDER_OFFSET ... COMMAND_CAPSULE_SHAPE) by dense index."""
         _check(lib.ag2d_world_set_collider(self.h, collider, command, a, b))
+
+    def set_polygon_shape(self, collider: int, xy) -> bool:
+        """ObjectAPI::setPolygonShape: new collider-local vertices for a polygon collider, applied at the next
+        step. False, with nothing queued, for an outline the reference refuses (degenerate, concave, > 16)."""
+        v = np.ascontiguousarray(np.asarray(xy, np.float32).reshape(-1, 2))
+        code = lib.ag2d_world_set_polygon_shape(self.h, collider, v.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                                v.shape[0])
+        if code == ERR_INVALID_ARG:
+            return False
+        _check(code)
+        return True
 
     def flush_commands(self):
         _check(lib.ag2d_world_flush_commands(self.h))

@@ -460,6 +460,7 @@ struct BodyCommand {
     int32_t kind;   // AG2D_COMMAND_*
     uint64_t handle;
     float a, b;
+    uint32_t slot = 0;   // AG2D_COMMAND_POLYGON_SHAPE: the outline's index in pendingPolygons
 };
 
 struct ag2d_world {
@@ -474,6 +475,7 @@ struct ag2d_world {
     bool otherDirty = true;         // static + sleeping tree must be rebuilt
     uint64_t stepsTaken = 0;
     std::vector<BodyCommand> commands;   // queued body commands, applied by flushCommands
+    std::vector<std::vector<float>> pendingPolygons;   // prepared outlines the queued polygon commands name
 
     // Collision callbacks (SimulationImpl/CollisionCallbackManager.h): slot 0 is the permanent "no callback",
     // destroyed slots are reused last-in first-out.
@@ -663,8 +665,8 @@ struct ag2d_world {
     // The collision-detection pass (AG2D_PHASE_COLLIDE) as a captured CUDA graph, replayed while its launch shapes
     // hold (list sizes, capacities, block sizes, whether the static tree is rebuilt).
     cudaGraphExec_t collideExec = nullptr;
-    uint64_t collideKey[8] = {};
-    uint64_t collideSeen[8] = {};   // the shape of the last pass run without a graph
+    uint64_t collideKey[9] = {};
+    uint64_t collideSeen[9] = {};   // the shape of the last pass run without a graph
     uint64_t collideLaunches = 0;
     cudaEvent_t ev[NPHASE][2] = {};
     bool evPending[NPHASE] = {};
@@ -2481,10 +2483,11 @@ struct ag2d_world {
             pos[b].w = hb.invInertia;
         };
         std::vector<uint32_t> editedColliders, reachBodies;   // device collider records and bound radii to refresh
+        bool polygonsEdited = false;                          // the packed polygon tables need a new upload
         const float twoPi = float(3.14159265358979323846 * 2.0);
         auto wrap = [&](float r) { r = std::fmod(r, twoPi); if (r < 0.0f) r += twoPi; return r; };
         for (const BodyCommand& c : commands) {
-            const bool colliderCmd = c.kind >= AG2D_COMMAND_COLLIDER_OFFSET && c.kind <= AG2D_COMMAND_CAPSULE_SHAPE;
+            const bool colliderCmd = c.kind >= AG2D_COMMAND_COLLIDER_OFFSET && c.kind <= AG2D_COMMAND_POLYGON_SHAPE;
             const uint32_t ci = colliderCmd ? uint32_t(c.handle) : 0xFFFFFFFFu;
             if (colliderCmd && ci >= o.colliders.size()) continue;
             const uint32_t b = colliderCmd ? o.colliders[ci].body : o.indexOf(c.handle);
@@ -2534,6 +2537,30 @@ struct ag2d_world {
                     k.maxExtent = o.boxHalfW[k.shape] + o.boxHalfH[k.shape];
                     shapeEdit = true;
                     break;
+                case AG2D_COMMAND_POLYGON_SHAPE: {   // ObjectManager.cpp:838-857: recentred on its centroid
+                    if (k.type != SHAPE_POLYGON || c.slot >= pendingPolygons.size()) break;
+                    std::vector<float> v = pendingPolygons[c.slot];
+                    float unused = 0.0f, cx = 0.0f, cy = 0.0f;
+                    polygon_inertia(1.0f, v, unused, cx, cy);
+                    for (size_t i = 0; i < v.size() / 2; i++) { v[2 * i] -= cx; v[2 * i + 1] -= cy; }
+                    const float cosL = std::cos(k.localRot), sinL = std::sin(k.localRot);
+                    k.locX += cosL * cx - sinL * cy;
+                    k.locY += sinL * cx + cosL * cy;
+                    k.comOffX = k.locX - hb.lcomX; k.comOffY = k.locY - hb.lcomY;
+                    HPolygon& poly = o.polygons[k.shape];
+                    poly.verts = v;
+                    poly.normals = polygon_normals(v);
+                    float inR = FLT_MAX, outR2 = 0.0f;
+                    for (size_t i = 0; i < v.size() / 2; i++) {
+                        const float vx = poly.verts[2 * i], vy = poly.verts[2 * i + 1];
+                        inR = std::fmin(inR, poly.normals[2 * i] * vx + poly.normals[2 * i + 1] * vy);
+                        outR2 = std::fmax(outR2, vx * vx + vy * vy);
+                    }
+                    k.minExtent = std::fmax(inR, 0.0f);
+                    k.maxExtent = std::sqrt(outR2);
+                    polygonsEdited = true;
+                    break;
+                }
                 default: break;
                 }
                 (void)shapeEdit;
@@ -2632,6 +2659,23 @@ struct ag2d_world {
             }
         }
         commands.clear();
+        pendingPolygons.clear();
+        if (polygonsEdited) {   // vertex counts may change: the packed tables are rebuilt whole
+            std::vector<uint32_t> po, pc;
+            std::vector<float2> pv, pn;
+            for (const HPolygon& p : o.polygons) {
+                po.push_back(uint32_t(pv.size()));
+                pc.push_back(uint32_t(p.verts.size() / 2));
+                for (size_t k = 0; k < p.verts.size() / 2; k++) {
+                    pv.push_back(make_float2(p.verts[2 * k], p.verts[2 * k + 1]));
+                    pn.push_back(make_float2(p.normals[2 * k], p.normals[2 * k + 1]));
+                }
+            }
+            polyOffset.upload(po.data(), po.size(), s); polyCount.upload(pc.data(), pc.size(), s);
+            polyVerts.upload(pv.data(), pv.size(), s); polyNormals.upload(pn.data(), pn.size(), s);
+            nPolyVerts = uint32_t(pv.size());
+            CK(cudaStreamSynchronize(s));
+        }
         // Collider records and shape parameters the commands changed, and the bound radii that follow.
         for (const uint32_t k : editedColliders) {
             const HCollider& hc = o.colliders[k];
@@ -3186,11 +3230,27 @@ int32_t ag2d_world_set_body_mass_from_density(ag2d_world* world, uint64_t body, 
 }
 int32_t ag2d_world_set_collider(ag2d_world* world, uint32_t collider, int32_t command, float a, float b)
 {
-    if (command < AG2D_COMMAND_COLLIDER_OFFSET || command > AG2D_COMMAND_CAPSULE_SHAPE) {
+    if (command < AG2D_COMMAND_COLLIDER_OFFSET || command > AG2D_COMMAND_CAPSULE_SHAPE) {   // polygons: below
         g_error = "unknown collider command";
         return AG2D_ERR_INVALID_ARG;
     }
     return queue_command(world, command, uint64_t(collider), a, b);
+}
+
+int32_t ag2d_world_set_polygon_shape(ag2d_world* world, uint32_t collider, const float* xy, uint32_t n)
+{
+    return guarded([&] {
+        if (!world) throw ApiError(AG2D_ERR_INVALID_ARG, "null world");
+        if (world->nWorlds > 1) throw ApiError(AG2D_ERR_UNSUPPORTED, "body commands are per world");
+        if (!xy || n < 3) throw ApiError(AG2D_ERR_INVALID_ARG, "polygon needs at least 3 vertices");
+        std::vector<float> outline;
+        std::string err;
+        if (!prepare_outline(xy, n, outline, err)) throw ApiError(AG2D_ERR_INVALID_ARG, err);
+        BodyCommand c{AG2D_COMMAND_POLYGON_SHAPE, uint64_t(collider), 0.0f, 0.0f};
+        c.slot = uint32_t(world->pendingPolygons.size());
+        world->pendingPolygons.push_back(std::move(outline));
+        world->commands.push_back(c);
+    });
 }
 
 int32_t ag2d_world_flush_commands(ag2d_world* world)
@@ -4096,19 +4156,21 @@ int32_t ag2d_world_run_phase(ag2d_world* world, int32_t phase)
             }
             // The pass's launches depend on these only; the kernels read their counts on the device.
             auto shape = [&](uint64_t* k) {
-                const uint64_t v[8] = {w.nDynCol, w.nOther, w.pairCap, w.manifoldCap, w.queryThreads,
-                                       w.narrowThreads, uint64_t(w.otherDirty), uint64_t(w.nColliders)};
-                std::copy(v, v + 8, k);
+                // Any device reallocation (a buffer a captured kernel points at) changes the allocation count.
+                const uint64_t v[9] = {w.nDynCol, w.nOther, w.pairCap, w.manifoldCap, w.queryThreads,
+                                       w.narrowThreads, uint64_t(w.otherDirty), uint64_t(w.nColliders),
+                                       g_deviceAllocs.load(std::memory_order_relaxed)};
+                std::copy(v, v + 9, k);
             };
-            uint64_t key[8];
+            uint64_t key[9];
             shape(key);
-            if (w.collideExec && std::equal(key, key + 8, w.collideKey)) {
+            if (w.collideExec && std::equal(key, key + 9, w.collideKey)) {
                 CK(cudaGraphLaunch(w.collideExec, w.stream));
                 w.launches += w.collideLaunches;
                 break;
             }
             if (w.collideExec) { CK(cudaGraphExecDestroy(w.collideExec)); w.collideExec = nullptr; }
-            if (!std::equal(key, key + 8, w.collideSeen)) {
+            if (!std::equal(key, key + 9, w.collideSeen)) {
                 // A new shape: one pass as it is (it may grow buffers or rebuild the static tree), remembered.
                 pass();
                 shape(w.collideSeen);
@@ -4130,7 +4192,7 @@ int32_t ag2d_world_run_phase(ag2d_world* world, int32_t phase)
             cudaGraphDestroy(graph);
             CK(ie);
             w.collideLaunches = w.launches - before;
-            std::copy(key, key + 8, w.collideKey);
+            std::copy(key, key + 9, w.collideKey);
             CK(cudaGraphLaunch(w.collideExec, w.stream));
             break;
         }

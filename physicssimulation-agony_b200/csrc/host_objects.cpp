@@ -57,6 +57,8 @@ std::vector<float> filter_duplicates(const float* xy, uint32_t n)
     return out;
 }
 
+}  // namespace
+
 // PhysicsGeometry::preparePolygonOutline (PhysicsGeometry.cpp:275-312) for convex outlines: dedupe, strip
 // straight vertices, make CCW, reject degenerate. Non-convex outlines are rejected (the reference would
 // decompose them into convex pieces: PolygonDecomposition.cpp).
@@ -126,8 +128,6 @@ std::vector<float> polygon_normals(const std::vector<float>& v)
     }
     return nrm;
 }
-
-}  // namespace
 
 uint32_t HostObjects::appendBody(float px, float py, float vx, float vy, float rot, float w, float mass,
                                  float invMass, float inertia, float invInertia, float lcomX, float lcomY)

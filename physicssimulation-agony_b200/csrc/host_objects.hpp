@@ -186,4 +186,11 @@ private:
 // Returns false for a degenerate (or clockwise) outline.
 bool polygon_inertia(float mass, const std::vector<float>& xy, float& inertia, float& cx, float& cy);
 
+// PhysicsGeometry::preparePolygonOutline (PhysicsGeometry.cpp:275-312) for convex outlines of at most 16 vertices
+// (xy pairs); false with a reason otherwise.
+bool prepare_outline(const float* xy, uint32_t n, std::vector<float>& out, std::string& err);
+
+// PolygonGeometry::computeNormals (SoA/Shapes/PolygonSoA.cpp:14-30): outward unit edge normals as xy pairs.
+std::vector<float> polygon_normals(const std::vector<float>& v);
+
 }  // namespace ag2d

@@ -54,6 +54,10 @@ int main()
         else ok = sim->objects().createPolygon({b, std::span<ag2d::Vec2>(tri, 3)}).has_value();
         created += ok ? 1 : 0;
     }
+    // ObjectAPI::setPolygonShape on the first triangle's collider: a square is queued, a concave dart refused.
+    ag2d::Vec2 square[4] = {{-0.4f, -0.4f}, {0.4f, -0.4f}, {0.4f, 0.4f}, {-0.4f, 0.4f}};
+    ag2d::Vec2 dart[4] = {{0.0f, 0.0f}, {1.0f, 0.5f}, {0.0f, 0.2f}, {-1.0f, 0.5f}};
+    if (!sim->objects().setPolygonShape(3, square) || sim->objects().setPolygonShape(3, dart)) return 40;
     ag2d::BodyCreateParams cb;
     cb.position = {0.0f, 10.0f};
     cb.rotation = 0.3f;

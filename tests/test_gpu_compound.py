@@ -176,8 +176,9 @@ def test_compound_bodies_land_like_the_reference():
 def test_body_and_collider_setters_match_the_reference():
     """ObjectAPI's remaining setters in free flight (ObjectAPI.h:82-91): a body's local centre of mass moved, its
     inertia recomputed from its colliders, its mass set from a density; a collider's offset, rotation and material,
-    a circle's radius, a box's size and a capsule's shape changed. In each of the 30 steps after the edits every body
-    field and every collider's pose and AABB equal the reference's bit for bit."""
+    a circle's radius, a box's size, a capsule's shape and two polygons' outlines changed (ObjectAPI.h:93; refused
+    outlines refused on both sides). In each of the 30 steps after the edits every body field and every collider's
+    pose and AABB equal the reference's bit for bit."""
     if not refapi.available():
         pytest.skip("the compiled reference (oracle/_ref) is not present")
     poses = [(12.0 * k, 20.0 + 3.0 * k, 0.3 * k, 1.5 - 0.7 * k) for k in range(len(BODIES))]
@@ -208,6 +209,16 @@ def test_body_and_collider_setters_match_the_reference():
     for c, ours, theirs, a, b in edits:
         w.set_collider(c, ours, a, b)
         ref.set_collider(cmap[c], theirs, a, b)
+    # Polygon outlines (setPolygonShape): off-centre ones, so the recentring shift goes into the offset (rotated by
+    # the collider's local rotation on body 2); on a circle nothing happens; refused outlines queue nothing.
+    quad = [(0.2, 0.1), (1.4, 0.3), (1.2, 1.2), (0.1, 0.9)]
+    penta = [(0.5 + 0.8 * np.cos(t), -0.2 + 0.8 * np.sin(t)) for t in np.arange(5) * 2 * np.pi / 5]
+    for c, xy in ((cols[2][1], quad), (cols[4][0], penta), (cols[0][1], quad)):
+        assert w.set_polygon_shape(c, xy) and ref.set_polygon(cmap[c], xy)
+    concave = [(0.0, 0.0), (2.0, 0.0), (1.0, 0.3), (2.0, 1.0), (0.0, 1.0)]
+    many = [(np.cos(t), np.sin(t)) for t in np.arange(17) * 2 * np.pi / 17]
+    for xy in (concave, many, [(0.0, 0.0), (1.0, 0.0)], [(0.0, 0.0), (1.0, 0.0), (2.0, 0.0)]):
+        assert not w.set_polygon_shape(cols[4][0], xy) and not ref.set_polygon(cmap[cols[4][0]], xy)
     w.recompute_body_inertia(hs[3])    # after its collider moved
     ref.set_body(rids[3], 7, 0.0)
     for step in range(30):
