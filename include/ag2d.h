@@ -191,7 +191,7 @@ int32_t ag2d_world_add_material(ag2d_world* world, float elasticity, float stati
 /* ObjectAPI::createCircleH / createBoxH / createPolygonH (SimulationAPIs/ObjectAPI.h:61-65;
  * ObjectManager::createCircle/createBox/createPolygon, SimulationImpl/ObjectManager.cpp:233-349). Mass, inertia,
  * centre of mass and polygon recentring follow the reference's PhysicsGeometry. Polygons must be convex after
- * outline cleaning (concave decomposition is not provided: AG2D_ERR_UNSUPPORTED). The handle is
+ * outline cleaning, concave outlines split into convex pieces, one collider each. The handle is
  * (generation << 32) | slot and stays valid across other creations. */
 int32_t ag2d_world_add_circle(ag2d_world* world, const ag2d_body_desc* body, float radius, uint64_t* out_handle);
 int32_t ag2d_world_add_box(ag2d_world* world, const ag2d_body_desc* body, float width, float height,
@@ -205,7 +205,7 @@ int32_t ag2d_world_create_body(ag2d_world* world, const ag2d_body_desc* body, fl
 /* ObjectAPI::create{Circle,Box,Polygon,Capsule}Collider (ObjectAPI.h:29-32; ObjectManager.cpp:90-231): a collider
  * on an existing body at a local offset and rotation. shape: 0 circle (params[0] radius), 1 box (params = width,
  * height), 2 polygon (xy / n_vertices: a convex outline, recentred on its centroid with the shift added to the
- * offset; concave outlines return AG2D_ERR_UNSUPPORTED: the reference would decompose them), 3 capsule (params =
+ * offset; a concave outline becomes one collider per convex piece, the first returned), 3 capsule (params =
  * length, radius). The body's mass and inertia stay as created. out_collider: the collider's dense index. */
 int32_t ag2d_world_add_collider(ag2d_world* world, uint64_t body, int32_t shape, float local_x, float local_y,
                                 float local_rotation, uint32_t material, const float* params, const float* xy,
@@ -272,6 +272,14 @@ int32_t ag2d_world_set_collider(ag2d_world* world, uint32_t collider, int32_t co
  * centroid, the shift added to the collider's offset (the body's mass and inertia are kept); on another shape it
  * does nothing. */
 int32_t ag2d_world_set_polygon_shape(ag2d_world* world, uint32_t collider, const float* xy, uint32_t n);
+/* PhysicsGeometry::preparePolygonOutline + decomposeConcave (Bayazit, ear clipping when no diagonal is valid) +
+ * limitConvexPieceVertexCount (fan, 16 vertices) (PhysicsGeometry.cpp:175-212, PolygonDecomposition.cpp:704-831):
+ * the convex pieces polygon creation makes from an outline, on the host (no device needed). Writes *out_pieces,
+ * then the pieces' vertex counts and their vertices (xy pairs, one piece after another); AG2D_ERR_CAPACITY with
+ * *out_pieces set when the arrays are too small; AG2D_ERR_INVALID_ARG for a degenerate or self-intersecting
+ * outline. */
+int32_t ag2d_decompose_polygon(const float* xy, uint32_t n, float* out_xy, uint32_t out_capacity,
+                               uint32_t* piece_counts, uint32_t piece_capacity, uint32_t* out_pieces);
 
 /* Applies the queued commands now (Simulation::flushCommands, Simulation.cpp:453-456). */
 int32_t ag2d_world_flush_commands(ag2d_world* world);

@@ -65,7 +65,7 @@ struct BodyCreateParams {
     MaterialIndex materialIndex = 0;
 };
 // Collider params (SimulationImpl/ObjectCreateParams.h:26-69): a shape attached to an existing body at a local offset
-// and rotation. Polygons must be convex here (the reference decomposes concave outlines); capsules take the
+// and rotation. Concave polygons become one collider per convex piece, as in the reference; capsules take the
 // length / radius form.
 struct ColliderCreateParams {
     Handle bodyHandle;

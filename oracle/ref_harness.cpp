@@ -12,6 +12,8 @@
 #include "PS_AGONY2D/FastCosSin.h"
 #include "PS_AGONY2D/Threading.h"
 #include "PS_AGONY2D/SimulationImpl/LeftOutFunctions.h"
+#include "PS_AGONY2D/SimulationImpl/PhysicsGeometry.h"
+#include "PS_AGONY2D/SimulationImpl/PolygonDecomposition.h"
 
 #include <atomic>
 #include <chrono>
@@ -476,6 +478,28 @@ extern "C"
         std::vector<Vec2> v(n);
         for (uint32_t i = 0; i < n; i++) v[i] = Vec2(xy[2 * i], xy[2 * i + 1]);
         return h->sim.objects().setPolygonShape(hd, std::span<const Vec2>(v.data(), v.size())) ? 1 : 0;
+    }
+    // PhysicsGeometry::preparePolygonOutline + decomposeConcave (default method) + limitConvexPieceVertexCount
+    // (16, default method): the pieces polygon creation makes. Returns the piece count (-1: outline refused); the
+    // counts and vertices are written while they fit.
+    int32_t agref_decompose(const float* xy, uint32_t n, float* out, uint32_t cap, uint32_t* counts, uint32_t pcap)
+    {
+        std::vector<Vec2> v(n);
+        for (uint32_t i = 0; i < n; i++) v[i] = Vec2(xy[2 * i], xy[2 * i + 1]);
+        auto outline = PhysicsGeometry::preparePolygonOutline(std::span<const Vec2>(v.data(), v.size()));
+        if (!outline) return -1;
+        auto pieces = PhysicsGeometry::decomposeConcave(*outline, PhysicsGeometry::ConcaveDecompositionMethod::Bayazit);
+        PhysicsGeometry::limitConvexPieceVertexCount(pieces, MAX_POLYGON_VERTEX_COUNT,
+                                                     PhysicsGeometry::ConvexDecompositionMethod::Fan);
+        uint32_t at = 0;
+        for (size_t k = 0; k < pieces.size(); k++) {
+            if (k < pcap) counts[k] = uint32_t(pieces[k].size());
+            for (const Vec2& p : pieces[k]) {
+                if (at < cap) { out[2 * at] = p.x; out[2 * at + 1] = p.y; }
+                at++;
+            }
+        }
+        return int32_t(pieces.size());
     }
     // Simulation::flushCommands (Simulation.cpp:454-461) on its own: the queued commands, the wakes they cause and
     // the stored manifolds of the woken islands, as the next update would apply them first.

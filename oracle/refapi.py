@@ -61,6 +61,9 @@ def lib():
         L.agref_set_collider.argtypes = [vp, u32, i32, f, f]
         L.agref_set_polygon.argtypes = [vp, u32, ctypes.POINTER(ctypes.c_float), u32]
         L.agref_set_polygon.restype = i32
+        L.agref_decompose.argtypes = [ctypes.POINTER(ctypes.c_float), u32, ctypes.POINTER(ctypes.c_float), u32,
+                                      ctypes.POINTER(ctypes.c_uint32), u32]
+        L.agref_decompose.restype = i32
         L.agref_body_index.restype = u32
         L.agref_body_index.argtypes = [vp, u32]
         L.agref_timed_update.restype = ctypes.c_double
@@ -331,3 +334,21 @@ def fastcossin(angles: np.ndarray):
     s = np.empty_like(a)
     lib().agref_fastcossin(a.ctypes.data, c.ctypes.data, s.ctypes.data, a.size)
     return c, s
+
+
+def decompose(xy):
+    """The reference's convex pieces for an outline (preparePolygonOutline, decomposeConcave, the 16-vertex limit):
+    a list of (k, 2) float32 arrays, or None when the outline is refused."""
+    v = np.ascontiguousarray(np.asarray(xy, np.float32).reshape(-1))
+    out = np.zeros(4096, np.float32)
+    counts = np.zeros(512, np.uint32)
+    f = ctypes.POINTER(ctypes.c_float)
+    k = lib().agref_decompose(v.ctypes.data_as(f), v.size // 2, out.ctypes.data_as(f), out.size // 2,
+                              counts.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), counts.size)
+    if k < 0:
+        return None
+    pieces, at = [], 0
+    for c in counts[:k].tolist():
+        pieces.append(out[2 * at:2 * (at + c)].reshape(-1, 2).copy())
+        at += c
+    return pieces

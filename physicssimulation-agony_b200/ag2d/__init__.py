@@ -197,6 +197,8 @@ def _load():
     L.ag2d_world_set_body_mass_from_density.argtypes = [vp, u64, ctypes.c_float]
     L.ag2d_world_set_collider.argtypes = [vp, u32, i32, ctypes.c_float, ctypes.c_float]
     L.ag2d_world_set_polygon_shape.argtypes = [vp, u32, ctypes.POINTER(ctypes.c_float), u32]
+    L.ag2d_decompose_polygon.argtypes = [ctypes.POINTER(ctypes.c_float), u32, ctypes.POINTER(ctypes.c_float), u32,
+                                         ctypes.POINTER(u32), u32, ctypes.POINTER(u32)]
     L.ag2d_world_create_joint.argtypes = [vp, ctypes.POINTER(JointDesc), ctypes.POINTER(u64)]
     L.ag2d_world_destroy_joint.argtypes = [vp, i32, u64]
     L.ag2d_world_set_joint.argtypes = [vp, i32, u64, i32, ctypes.c_float, ctypes.c_float]

@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
               "-Xcompiler", "-fPIC,-ffp-contract=off", f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
 CU_SOURCES = ["k_spatial.cu", "k_contact.cu", "k_islands.cu", "k_events.cu", "k_joints.cu", "k_repack.cu", "capi.cu", "solve_noalloc.cu"]
-CPP_SOURCES = ["host_objects.cpp"]
+CPP_SOURCES = ["host_objects.cpp", "polygon_decompose.cpp"]
 HEADERS = ["ag2d_math.cuh", "ag2d_world.cuh", "ag2d_kernels.cuh", "ag2d_solver.cuh", "ag2d_ccd.cuh", "host_objects.hpp"]
 
 

@@ -3072,8 +3072,7 @@ int32_t ag2d_world_add_polygon(ag2d_world* world, const ag2d_body_desc* body, co
         uint64_t h = 0;
         std::string err;
         if (!world->objects.addPolygon(d, body->material, xy, n, h, err)) {
-            throw ApiError(err.find("not convex") != std::string::npos || err.find("16") != std::string::npos
-                               ? AG2D_ERR_UNSUPPORTED : AG2D_ERR_INVALID_ARG, err);
+            throw ApiError(AG2D_ERR_INVALID_ARG, err);
         }
         world->hostDirty = true;
         if (out_handle) *out_handle = h;
@@ -3127,8 +3126,7 @@ int32_t ag2d_world_add_collider(ag2d_world* world, uint64_t body, int32_t shape,
         std::string err;
         if (!world->objects.addCollider(b, uint32_t(shape), local_x, local_y, local_rotation, material, params, xy,
                                         n_vertices, c, err))
-            throw ApiError(err.find("not convex") != std::string::npos || err.find("16") != std::string::npos
-                               ? AG2D_ERR_UNSUPPORTED : AG2D_ERR_INVALID_ARG, err);
+            throw ApiError(AG2D_ERR_INVALID_ARG, err);
         world->hostDirty = true;
         if (out_collider) *out_collider = c;
     });
@@ -3161,8 +3159,6 @@ int32_t ag2d_world_add_bodies(ag2d_world* world, uint32_t count, const ag2d_body
                 if (!poly_offsets || !poly_counts || !poly_xy) { err = "polygon without vertex arrays"; break; }
                 ok = world->objects.addPolygon(d, bodies[i].material, poly_xy + 2 * size_t(poly_offsets[i]),
                                                poly_counts[i], h, err);
-                if (!ok && (err.find("not convex") != std::string::npos || err.find("16") != std::string::npos))
-                    code = AG2D_ERR_UNSUPPORTED;
                 break;
             default: err = "unknown shape kind"; break;
             }
@@ -3250,6 +3246,31 @@ int32_t ag2d_world_set_polygon_shape(ag2d_world* world, uint32_t collider, const
         c.slot = uint32_t(world->pendingPolygons.size());
         world->pendingPolygons.push_back(std::move(outline));
         world->commands.push_back(c);
+    });
+}
+
+int32_t ag2d_decompose_polygon(const float* xy, uint32_t n, float* out_xy, uint32_t out_capacity,
+                               uint32_t* piece_counts, uint32_t piece_capacity, uint32_t* out_pieces)
+{
+    return guarded([&] {
+        if (!xy || !out_pieces) throw ApiError(AG2D_ERR_INVALID_ARG, "null argument");
+        if (n < 3) throw ApiError(AG2D_ERR_INVALID_ARG, "polygon needs at least 3 vertices");
+        std::vector<float> outline;
+        std::string err;
+        if (!prepare_outline_any(xy, n, outline, err)) throw ApiError(AG2D_ERR_INVALID_ARG, err);
+        const std::vector<std::vector<float>> pieces = decompose_outline(outline, 16);
+        size_t verts = 0;
+        for (const auto& p : pieces) verts += p.size() / 2;
+        *out_pieces = uint32_t(pieces.size());
+        if (pieces.size() > piece_capacity || verts > out_capacity || !piece_counts || !out_xy)
+            throw ApiError(AG2D_ERR_CAPACITY, "output arrays too small: " + std::to_string(pieces.size()) +
+                                                  " pieces, " + std::to_string(verts) + " vertices");
+        size_t at = 0;
+        for (size_t k = 0; k < pieces.size(); k++) {
+            piece_counts[k] = uint32_t(pieces[k].size() / 2);
+            std::copy(pieces[k].begin(), pieces[k].end(), out_xy + 2 * at);
+            at += pieces[k].size() / 2;
+        }
     });
 }
 

@@ -59,10 +59,9 @@ std::vector<float> filter_duplicates(const float* xy, uint32_t n)
 
 }  // namespace
 
-// PhysicsGeometry::preparePolygonOutline (PhysicsGeometry.cpp:275-312) for convex outlines: dedupe, strip
-// straight vertices, make CCW, reject degenerate. Non-convex outlines are rejected (the reference would
-// decompose them into convex pieces: PolygonDecomposition.cpp).
-bool prepare_outline(const float* xy, uint32_t n, std::vector<float>& out, std::string& err)
+// PhysicsGeometry::preparePolygonOutline (PhysicsGeometry.cpp:175-212): dedupe, strip straight vertices, make CCW,
+// reject degenerate and non-simple outlines.
+bool prepare_outline_any(const float* xy, uint32_t n, std::vector<float>& out, std::string& err)
 {
     out = filter_duplicates(xy, n);
     bool removed = true;
@@ -95,13 +94,15 @@ bool prepare_outline(const float* xy, uint32_t n, std::vector<float>& out, std::
         out.swap(rev);
     }
     if (std::abs(area2) * 0.5f <= std::numeric_limits<float>::epsilon()) { err = "polygon outline is degenerate"; return false; }
-    for (size_t i = 0; i < m; i++) {
-        const size_t j = (i + 1) % m, k = (i + 2) % m;
-        const float ax = out[2 * j] - out[2 * i], ay = out[2 * j + 1] - out[2 * i + 1];
-        const float bx = out[2 * k] - out[2 * j], by = out[2 * k + 1] - out[2 * j + 1];
-        if (ax * by - ay * bx < 0.0f) { err = "polygon is not convex (concave decomposition is not provided)"; return false; }
-    }
-    if (m > 16) { err = "polygon has more than 16 vertices (MAX_POLYGON_VERTEX_COUNT)"; return false; }
+    if (!outline_is_simple(out)) { err = "polygon outline is self-intersecting"; return false; }
+    return true;
+}
+
+bool prepare_outline(const float* xy, uint32_t n, std::vector<float>& out, std::string& err)
+{
+    if (!prepare_outline_any(xy, n, out, err)) return false;
+    if (out.size() / 2 > 16) { err = "polygon has more than 16 vertices (MAX_POLYGON_VERTEX_COUNT)"; return false; }
+    if (!outline_is_convex(out)) { err = "polygon is not convex"; return false; }
     return true;
 }
 
@@ -334,12 +335,15 @@ bool HostObjects::addPolygon(const float* d, uint32_t material, const float* xy,
     // ObjectManager::createPolygon (ObjectManager.cpp:286-349) via PhysicsGeometry::buildPolygon (:361-400).
     const float mass = std::fmax(0.0f, d[6]);
     std::vector<float> outline;
-    if (!prepare_outline(xy, n, outline, err)) return false;
+    if (!prepare_outline_any(xy, n, outline, err)) return false;
     float inertia = 0, tcx = 0, tcy = 0;
     if (!polygon_inertia(mass, outline, inertia, tcx, tcy)) { err = "polygon outline is degenerate"; return false; }
     const float needX = tcx - tcx, needY = tcy - tcy;   // requested pivot defaults to the true centre of mass
     for (size_t i = 0; i < outline.size() / 2; i++) { outline[2 * i] -= tcx; outline[2 * i + 1] -= tcy; }
     inertia = inertia + mass * (needX * needX + needY * needY);
+    // Convex pieces of the centred outline (decomposeConcave + limitConvexPieceVertexCount), one collider each.
+    std::vector<std::vector<float>> pieces = decompose_outline(outline, 16);
+    if (pieces.empty()) { err = "decomposition produced no pieces"; return false; }
     const float cosR = std::cos(d[2]), sinR = std::sin(d[2]);
     const float ox = d[0] + (cosR * tcx - sinR * tcy);
     const float oy = d[1] + (sinR * tcx + cosR * tcy);
@@ -347,14 +351,22 @@ bool HostObjects::addPolygon(const float* d, uint32_t material, const float* xy,
     const float invInertia = inertia == 0.0f ? 0.0f : 1.0f / inertia;
     const uint32_t b = appendBody(ox, oy, d[3], d[4], d[2], d[5], mass, invMass, inertia, invInertia, needX, needY);
     const uint32_t slot = bodies[b].handleSlot;
-    // createConvexPolygonColliderInternal (ObjectManager.cpp:535-562): recentre the piece on its own centroid and
-    // move the shift into the local offset; extents are the in-radius and out-radius about the new origin.
+    for (const std::vector<float>& piece : pieces) appendPolygonPiece(b, 0.0f, 0.0f, 0.0f, material, piece);
+    handle = (uint64_t(slotGeneration[slot]) << 32) | slot;
+    return true;
+}
+
+// createConvexPolygonColliderInternal (ObjectManager.cpp:535-562): recentre the piece on its own centroid and move
+// the shift into the local offset; extents are the in-radius and out-radius about the new origin.
+uint32_t HostObjects::appendPolygonPiece(uint32_t b, float offX, float offY, float localRot, uint32_t material,
+                                         std::vector<float> outline)
+{
     float unused = 0, pcx = 0, pcy = 0;
     polygon_inertia(1.0f, outline, unused, pcx, pcy);
     for (size_t i = 0; i < outline.size() / 2; i++) { outline[2 * i] -= pcx; outline[2 * i + 1] -= pcy; }
-    const float cosL = std::cos(0.0f), sinL = std::sin(0.0f);
-    const float locX = 0.0f + (cosL * pcx - sinL * pcy);
-    const float locY = 0.0f + (sinL * pcx + cosL * pcy);
+    const float cosL = std::cos(localRot), sinL = std::sin(localRot);
+    const float locX = offX + (cosL * pcx - sinL * pcy);
+    const float locY = offY + (sinL * pcx + cosL * pcy);
     HPolygon poly;
     poly.verts = outline;
     poly.normals = polygon_normals(outline);
@@ -366,9 +378,8 @@ bool HostObjects::addPolygon(const float* d, uint32_t material, const float* xy,
     }
     inR = std::fmax(inR, 0.0f);
     polygons.push_back(std::move(poly));
-    appendCollider(b, locX, locY, 0.0f, material, 2u, uint32_t(polygons.size() - 1), inR, std::sqrt(outR2));
-    handle = (uint64_t(slotGeneration[slot]) << 32) | slot;
-    return true;
+    return appendCollider(b, locX, locY, localRot, material, 2u, uint32_t(polygons.size() - 1), inR,
+                          std::sqrt(outR2));
 }
 
 bool HostObjects::addCapsule(const float* d, uint32_t material, float length, float radius, uint64_t& handle,
@@ -446,29 +457,14 @@ bool HostObjects::addCollider(uint32_t body, uint32_t type, float locX, float lo
         collider = appendCollider(body, locX, locY, localRot, material, 3u, uint32_t(boxHalfW.size() - 1), r, half + r);
         return true;
     }
-    case 2: {   // createPolygonCollider for a convex outline (:141-195) via createConvexPolygonColliderInternal
+    case 2: {   // createPolygonCollider (:141-195): one collider per convex piece, the first returned
         if (!xy || n < 3) { err = "polygon needs at least 3 vertices"; return false; }
         std::vector<float> outline;
-        if (!prepare_outline(xy, n, outline, err)) return false;
-        float unused = 0, pcx = 0, pcy = 0;
-        if (!polygon_inertia(1.0f, outline, unused, pcx, pcy)) { err = "polygon outline is degenerate"; return false; }
-        for (size_t i = 0; i < outline.size() / 2; i++) { outline[2 * i] -= pcx; outline[2 * i + 1] -= pcy; }
-        const float cosL = std::cos(localRot), sinL = std::sin(localRot);
-        const float offX = locX + (cosL * pcx - sinL * pcy);
-        const float offY = locY + (sinL * pcx + cosL * pcy);
-        HPolygon poly;
-        poly.verts = outline;
-        poly.normals = polygon_normals(outline);
-        float inR = FLT_MAX, outR2 = 0.0f;
-        for (size_t i = 0; i < outline.size() / 2; i++) {
-            const float vx = poly.verts[2 * i], vy = poly.verts[2 * i + 1];
-            inR = std::fmin(inR, poly.normals[2 * i] * vx + poly.normals[2 * i + 1] * vy);
-            outR2 = std::fmax(outR2, vx * vx + vy * vy);
-        }
-        inR = std::fmax(inR, 0.0f);
-        polygons.push_back(std::move(poly));
-        collider = appendCollider(body, offX, offY, localRot, material, 2u, uint32_t(polygons.size() - 1), inR,
-                                  std::sqrt(outR2));
+        if (!prepare_outline_any(xy, n, outline, err)) return false;
+        std::vector<std::vector<float>> pieces = decompose_outline(outline, 16);
+        if (pieces.empty()) { err = "decomposition produced no pieces"; return false; }
+        collider = appendPolygonPiece(body, locX, locY, localRot, material, pieces[0]);
+        for (size_t k = 1; k < pieces.size(); k++) appendPolygonPiece(body, locX, locY, localRot, material, pieces[k]);
         return true;
     }
     default: err = "unknown shape kind"; return false;

@@ -176,6 +176,8 @@ private:
                         float inertia, float invInertia, float lcomX, float lcomY);
     uint32_t appendCollider(uint32_t body, float locX, float locY, float localRot, uint32_t material, uint32_t type,
                             uint32_t shape, float minExt, float maxExt);
+    uint32_t appendPolygonPiece(uint32_t body, float offX, float offY, float localRot, uint32_t material,
+                                std::vector<float> outline);
     void swapBodies(uint32_t a, uint32_t b);
     void swapColliders(uint32_t a, uint32_t b);
     uint32_t moveBodyDown(uint32_t index, uint32_t target);
@@ -186,9 +188,22 @@ private:
 // Returns false for a degenerate (or clockwise) outline.
 bool polygon_inertia(float mass, const std::vector<float>& xy, float& inertia, float& cx, float& cy);
 
-// PhysicsGeometry::preparePolygonOutline (PhysicsGeometry.cpp:275-312) for convex outlines of at most 16 vertices
-// (xy pairs); false with a reason otherwise.
+// PhysicsGeometry::preparePolygonOutline (PhysicsGeometry.cpp:175-212): duplicates and straight vertices dropped,
+// made counter-clockwise; false with a reason for a degenerate or non-simple outline. Concave outlines pass.
+bool prepare_outline_any(const float* xy, uint32_t n, std::vector<float>& out, std::string& err);
+
+// prepare_outline_any for a convex outline of at most 16 vertices (ObjectManager::queueColliderPolygon's checks,
+// ObjectManager.cpp:622-636); false with a reason otherwise.
 bool prepare_outline(const float* xy, uint32_t n, std::vector<float>& out, std::string& err);
+
+// isConvexPolygon and isSimplePolygon (PolygonDecomposition.cpp:618-671) on xy pairs.
+bool outline_is_convex(const std::vector<float>& xy);
+bool outline_is_simple(const std::vector<float>& xy);
+
+// PhysicsGeometry::decomposeConcave with the Bayazit method (ear clipping when it finds no diagonal), then
+// limitConvexPieceVertexCount with the fan split (PolygonDecomposition.cpp:704-831): convex pieces (xy pairs, the
+// prepared outline's vertices) of at most maxVertices vertices each.
+std::vector<std::vector<float>> decompose_outline(const std::vector<float>& xy, size_t maxVertices);
 
 // PolygonGeometry::computeNormals (SoA/Shapes/PolygonSoA.cpp:14-30): outward unit edge normals as xy pairs.
 std::vector<float> polygon_normals(const std::vector<float>& v);
