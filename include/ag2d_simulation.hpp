@@ -82,6 +82,10 @@ struct BoxColliderCreateParams : ColliderCreateParams {
 struct PolygonColliderCreateParams : ColliderCreateParams {
     std::span<const Vec2> localVertices;
 };
+struct PolygonColliderCreateResult {
+    ObjectDenseIndex firstColliderIndex{0};
+    size_t colliderCount{0};
+};
 struct CapsuleColliderCreateParams : ColliderCreateParams {
     Real length = 0;
     Real radius = 0;
@@ -277,12 +281,19 @@ public:
         const float params[2] = {p.size.x, p.size.y};
         return collider(p, 1, params, nullptr, 0);
     }
-    std::optional<ObjectDenseIndex> createPolygonCollider(const PolygonColliderCreateParams& p)
+    // The first piece's index and the number of convex pieces (colliders) the outline became
+    // (PolygonColliderCreateResult, ObjectCreateParams.h:71-75); the pieces follow the first in the body's colliders.
+    std::optional<PolygonColliderCreateResult> createPolygonCollider(const PolygonColliderCreateParams& p)
     {
         std::vector<float> xy;
         xy.reserve(p.localVertices.size() * 2);
         for (const Vec2& v : p.localVertices) { xy.push_back(v.x); xy.push_back(v.y); }
-        return collider(p, 2, nullptr, xy.data(), uint32_t(p.localVertices.size()));
+        const uint32_t n = uint32_t(p.localVertices.size());
+        const std::optional<ObjectDenseIndex> first = collider(p, 2, nullptr, xy.data(), n);
+        if (!first) return std::nullopt;
+        uint32_t pieces = 0;   // the count alone: no output arrays (AG2D_ERR_CAPACITY with the count written)
+        ag2d_decompose_polygon(xy.data(), n, nullptr, 0, nullptr, 0, &pieces);
+        return PolygonColliderCreateResult{*first, size_t(pieces)};
     }
     std::optional<ObjectDenseIndex> createCapsuleCollider(const CapsuleColliderCreateParams& p)
     {

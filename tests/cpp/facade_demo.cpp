@@ -95,6 +95,14 @@ int main()
         wheel.radius = 0.35f;
         if (!sim->objects().createCircleCollider(wheel)) return 12;
     }
+    // A concave bracket on the bar: split into convex pieces, one collider each.
+    ag2d::Vec2 bracket[6] = {{-0.6f, 0.1f}, {0.6f, 0.1f}, {0.6f, 0.7f}, {0.4f, 0.7f}, {0.4f, 0.3f}, {-0.6f, 0.3f}};
+    ag2d::PolygonColliderCreateParams bracketParams;
+    bracketParams.bodyHandle = *dumbbell;
+    bracketParams.materialIndex = mat;
+    bracketParams.localVertices = std::span<const ag2d::Vec2>(bracket, 6);
+    const auto pieces = sim->objects().createPolygonCollider(bracketParams);
+    if (!pieces || pieces->colliderCount < 2) return 41;
     // A swinging chain (ConstraintAPI): three links on revolute joints from a static hook, a motor on the last.
     ag2d::BodyCreateParams hb;
     hb.position = {14.0f, 14.0f};
@@ -168,9 +176,9 @@ int main()
     std::vector<ag2d::ObjectDenseIndex> all;
     sim->getBroadPhaseCollisionDetector().queryCollidersInShape(bp::AABBQuery({-1e6f, -1e6f, 1e6f, 1e6f}),
                                                                 bp::BvhTreeTypeFlag::All, all);
-    // One collider per live body plus the dumbbell's two wheels, all inside the huge box; the destroyed body's
-    // collider is in no tree, and the hook and the chain's three links have none.
-    if (all.size() != bodies.getCount() - 1 + 2 - 4) {
+    // One collider per live body plus the dumbbell's two wheels and the bracket's pieces, all inside the huge box;
+    // the destroyed body's collider is in no tree, and the hook and the chain's three links have none.
+    if (all.size() != bodies.getCount() - 1 + 2 - 4 + pieces->colliderCount) {
         std::printf("colliders found %zu, bodies %u\n", all.size(), bodies.getCount());
         return 6;
     }

@@ -40,7 +40,8 @@ def test_facade_steps_scene_on_gpu(tmp_path):
     bodies, manifolds, mean_y = int(fields[1]), int(fields[2]), float(fields[3])
     assert bodies == 68 and manifolds > 0   # ground, 60 pile bodies, a capsule, a destroyed circle, a dumbbell,
     #                                         a static hook and a three-link chain on revolute joints
-    assert int(fields[6]) == 65             # colliders in the trees: 63 live bodies, two more on the dumbbell
+    assert int(fields[6]) == 67             # colliders in the trees: 63 live bodies, four more on the dumbbell
+    #                                         (its two wheels and the two convex pieces of its concave bracket)
     assert -1.0 < mean_y < 6.0   # the pile has fallen onto the ground (spawned between y = 1 and 8.5)
     found, touching = int(fields[4]), int(fields[5])   # the editor-style circle query around the pile's base
     assert 0 < touching <= found
